@@ -1,0 +1,296 @@
+"""Benchmark of the exposure hot path: scenario x trade revaluations per second.
+
+Workload (default): the multi-factor correlated book of zlatko_b200.configs.config1_book -- 1,000 trades
+(600 swaps, 300 FX forwards, 100 FX options) in 100 collateralised netting sets of Zipf(1.2) sizes,
+100,000 paths, 120 monthly reporting dates to 10y (241 simulation dates with the margin-call dates),
+synthetic seeded data.  One step = the fused simulate -> revalue -> net -> collateralise -> reduce kernel
+over every netting set, the reduction of the per-tile partials, and the row statistics (PFE 97.5% and
+means) of every netting set and reporting date.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zlatko|reference] [--paths P]
+
+value   revaluations/s = paths x simulation dates x trades / device time of a step (CUDA events on the
+        library's stream; inputs resident in HBM; L2 flushed between steps).
+e2e     the same metric through the public C ABI (zk_run_plans): plan tables copied host -> device and
+        statistics device -> host inside the timed region, wall clock of the blocking call.
+--impl reference: the reference's own FP32 CPU kernels (gpu::runFusedReference, compiled from the
+        reference sources into oracle/_ref) on the host cores, on a bounded sample of paths.
+N > 1: replicas (the path runs on one GPU by design); every rank runs the workload, value = all ranks'
+        revaluations / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "scenario x trade revaluations/s"
+UNIT = "revals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="zlatko", choices=["zlatko", "reference"])
+    ap.add_argument("--paths", type=int, default=100_000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(paths: int):
+    """DRAM bytes of one fused-kernel launch from the committed ncu summary, scaled by paths."""
+    path = os.path.join(ROOT, "profiles", "fused_exposure_book100.txt")
+    if not os.path.exists(path):
+        return None
+    ref_paths, ref_bytes = None, None
+    for line in open(path):
+        if line.startswith("capture_paths:"):
+            ref_paths = float(line.split(":")[1])
+        if line.startswith("dram_bytes_per_launch:"):
+            ref_bytes = float(line.split(":")[1])
+    if not ref_paths or not ref_bytes:
+        return None
+    return ref_bytes * paths / ref_paths
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def workload(paths: int):
+    from zlatko_b200 import configs, gpu
+
+    m, books, opts, trades = configs.config1_book(paths)
+    t0 = time.perf_counter()
+    plans = [gpu.compile(m, b, opts) for b in books]
+    compile_s = time.perf_counter() - t0
+    return m, books, opts, trades, plans, compile_s
+
+
+def cpu_reference(plans, trades: int, target_s: float, steps: int = 1):
+    """The reference's FP32 CPU kernels (runFusedReference) on all host threads over a bounded sample of
+    paths of every netting set's plan.  Returns (revals/s, sample paths, threads, seconds)."""
+    from oracle import ref
+
+    threads = os.cpu_count() or 1
+    nT = plans[0].num_dates
+
+    def run(paths):
+        rps = [ref.plan_from_buffers(p.header, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
+                                     p.num_outputs, p.times, p.reporting, num_paths=paths) for p in plans]
+        t0 = time.perf_counter()
+        for rp in rps:
+            ref.run_fused(rp, threads)
+        return time.perf_counter() - t0
+
+    probe = 256
+    dt = run(probe)
+    paths = int(max(probe, min(64 * probe, probe * target_s / max(dt, 1e-3))) // 64 * 64)
+    times = [run(paths) for _ in range(steps)]
+    dt = float(np.median(times))
+    return paths * nT * trades / dt, paths, threads, dt, times
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        _, _, _, trades, plans, _ = workload(a.paths)
+        per_step = max(2.0, a.cpu_seconds / max(a.steps, 1))
+        for _ in range(min(a.warmup, 1)):
+            cpu_reference(plans, trades, 1.0)
+        value, paths, threads, dt, times = cpu_reference(plans, trades, per_step, steps=a.steps)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "config1_book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
+                                       "HW1F + 2 FX + CIR++, 241 simulation dates", "paths_per_step": paths},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": f"{paths} paths of each of the 100 netting sets per step (of {a.paths})"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    device = torch.cuda.current_device()
+    from zlatko_b200 import gpu
+    from zlatko_b200._native import lib
+
+    m, books, opts, trades, plans, compile_s = workload(a.paths)
+    nT, nP = plans[0].num_dates, plans[0].num_paths
+    revals = float(nP) * nT * trades
+    ctx = gpu.Context(device)
+    batch = ctx.batch(plans)
+    info = batch.info()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(max(a.warmup, 3)):
+        batch.execute()
+    batch.read()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms, sim_ms, fused_ms, reduce_ms, rows_ms = [], [], [], [], []
+    with ClockSampler(device) as clocks:
+        torch.cuda.synchronize()
+        for _ in range(a.steps):
+            flush.zero_()  # L2 flush between steps (outside the step's events)
+            torch.cuda.synchronize()
+            batch.execute()
+            ms = batch.timings()
+            sim_ms.append(ms[0]), fused_ms.append(ms[1]), reduce_ms.append(ms[2]), rows_ms.append(ms[3])
+            step_ms.append(float(ms.sum()))
+        torch.cuda.synchronize()
+        # e2e through the public C ABI: host plan tables in, host statistics out.
+        for _ in range(a.warmup):
+            ctx.run_many(plans)
+        e2e_s = []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            ctx.run_many(plans)
+            e2e_s.append(time.perf_counter() - t0)
+    t_step = float(np.sum(step_ms)) / 1e3
+    t_e2e = float(np.sum(e2e_s))
+    if dist:
+        t = torch.tensor([t_step, t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step, t_e2e = float(t[0]), float(t[1])
+    total = revals * world * a.steps
+    value = total / t_step
+    e2e = total / t_e2e
+
+    peak, peak_kind = peaks()
+    fused_s = float(np.mean(fused_ms)) / 1e3
+    nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
+    cube_bytes = (2 + nA + nC) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
+    alg_bytes = sum(p.rows_total * nP * 4 + ((nP + 127) // 128) * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
+    ex2 = C_ex2 = None
+    try:
+        import ctypes as C
+
+        g = C.c_double()
+        if lib().zk_peak_ex2(device, C.byref(g)) == 0:
+            C_ex2 = g.value * 1e9
+    except Exception:
+        C_ex2 = None
+    exp_per_launch = float(info.exp_evaluations) * nP  # one ex2 per bond-like term and path
+    h2d = info.table_bytes + sum(p.indices.size * 4 for p in plans)
+    d2h = sum((p.sums_len() + p.values_len()) * 4 for p in plans)
+
+    if rank == 0:
+        cpu = None
+        try:
+            cv, cpaths, cthreads, cdt, _ = cpu_reference(plans, trades, a.cpu_seconds / 2)
+            cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": "reference",
+                   "sample": f"{cpaths} of {nP} paths of all 100 netting sets (gpu::runFusedReference, {cthreads} threads)"}
+        except Exception as exc:  # pragma: no cover
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": t_step / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config1_book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
+                                   "HW1F + 2 FX + CIR++, 241 simulation dates", "paths": nP, "simulation_dates": nT,
+                       "trades": trades, "netting_sets": len(plans), "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(info.kernels_per_execute) * a.steps,
+            "kernel_ms": {"simulate": float(np.mean(sim_ms)), "revalue": float(np.mean(fused_ms)), "reduce": float(np.mean(reduce_ms)),
+                          "row_stats": float(np.mean(rows_ms))},
+            "roofline": {"bound": "hbm", "achieved": alg_bytes / fused_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg_bytes / fused_s / 1e9 / peak, "traffic": traffic_per_launch(nP),
+                         "note": f"revalue kernel (the dominant one); peak of {peak_kind}; algorithmic bytes = factor cube read "
+                                 "once + PFE rows written + per-tile partials + plan tables"},
+            "roofline_mufu": {"bound": "sfu", "achieved": exp_per_launch / fused_s / 1e9 if C_ex2 else None,
+                              "peak": C_ex2 / 1e9 if C_ex2 else None, "unit": "G ex2/s",
+                              "frac": exp_per_launch / fused_s / C_ex2 if C_ex2 else None},
+            "clocks": clocks.summary(),
+            "plan_compile_s": compile_s,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    batch.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

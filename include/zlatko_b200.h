@@ -1,0 +1,159 @@
+/* zlatko_b200: the counterparty-exposure hot path of svr-net/zlatko on one NVIDIA B200 (sm_100a).
+ *
+ * The reference compiles a netting set into a gpu::FusedPlan (flat tables) and hands it to a
+ * backend functor that returns a gpu::FusedOutput (src/app/analyses.cpp:2148-2177, the seam of
+ * analyseFused; the two reference backends are the WebGPU read-back at analyses.cpp:2179 and
+ * runFusedReference at analyses.cpp:2196).  This library is a third backend behind that seam:
+ * it takes the plan's buffers verbatim and fills the output in the reference's layout.
+ *
+ * Every entry point returns a zk_status and never throws across the ABI; zk_last_error() gives the
+ * message.  ZK_ERR_INVALID_PLAN and ZK_ERR_UNSUPPORTED are the cases where the reference throws
+ * std::invalid_argument (PlanView, src/gpu/fused_reference.cpp:64-75; finishFused :473-478;
+ * compile, src/gpu/fused_exposure.cpp:219-230).  Calls on one context are serialised on the
+ * context's stream; a context is not thread-safe (guard it with a mutex or use one per thread).
+ * There is no CPU fallback: without a CUDA device zk_context_create fails with ZK_ERR_NO_DEVICE.
+ */
+#ifndef ZLATKO_B200_H
+#define ZLATKO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZK_ABI_VERSION 1
+
+typedef enum zk_status {
+  ZK_OK = 0,
+  ZK_ERR_INVALID_ARGUMENT = 1, /* null pointer, wrong buffer length */
+  ZK_ERR_INVALID_PLAN = 2,     /* malformed or inconsistent plan tables */
+  ZK_ERR_UNSUPPORTED = 3,      /* a plan feature this build does not run (message says which) */
+  ZK_ERR_OUT_OF_MEMORY = 4,
+  ZK_ERR_CUDA = 5,             /* a CUDA runtime error (launch failure, ...) */
+  ZK_ERR_DEVICE_TIMEOUT = 6,   /* a bounded wait inside a kernel gave up; the context stays usable */
+  ZK_ERR_NO_DEVICE = 7
+} zk_status;
+
+typedef struct zk_context zk_context;
+
+/* The GPU buffers of a reference gpu::FusedPlan (include/ccr/gpu/fused_exposure.hpp:152-226), in
+ * the reference's exact binary layout.  All lengths count elements. */
+typedef struct zk_plan_view {
+  const uint32_t* header;  size_t header_len;   /* kHeaderWords = 32 (fused_kernels.cpp:32-41)           */
+  const uint32_t* indices; size_t indices_len;  /* termStart[nT+1] | callIndex[nT] | reportingSlot[nT] | imTarget[nT] */
+  const float* params;     size_t params_len;   /* kParamCount = 84: CIR x2 | CSA | spots | Cholesky 8x8 | collateral */
+  const float* steps;      size_t steps_len;    /* nT * kStepStride (24)                                  */
+  const float* terms;      size_t terms_len;    /* numTerms * kTermStride (8)                             */
+  const float* requests;   size_t requests_len; /* numRequests * kRequestStride (8)                       */
+  uint32_t rows_total;                          /* FusedPlan::rows.total                                  */
+  uint32_t num_outputs;                         /* FusedPlan::numOutputs                                  */
+} zk_plan_view;
+
+/* gpu::FusedOutput (fused_exposure.hpp:223-226): sums[nT * statsPerDate] (already divided by the
+ * number of paths) and values[max(1, numOutputs)].  The caller owns both buffers. */
+typedef struct zk_output {
+  float* sums;   size_t sums_len;
+  float* values; size_t values_len;
+} zk_output;
+
+/* Double-precision plan (the FP64 mode): the same layout with double tables, as produced by
+ * zk_compile.  The reference's own plans are single precision; this mode exists to check the
+ * kernels against the reference's FP64 ExposureEngine on identical normals. */
+typedef struct zk_plan_view_f64 {
+  const uint32_t* header;  size_t header_len;
+  const uint32_t* indices; size_t indices_len;
+  const double* params;    size_t params_len;
+  const double* steps;     size_t steps_len;
+  const double* terms;     size_t terms_len;
+  const double* requests;  size_t requests_len;
+  uint32_t rows_total;
+  uint32_t num_outputs;
+} zk_plan_view_f64;
+
+typedef struct zk_output_f64 {
+  double* sums;   size_t sums_len;
+  double* values; size_t values_len;
+} zk_output_f64;
+
+/* ---- context ---------------------------------------------------------------------------------- */
+zk_status zk_context_create(int device, zk_context** out);
+void zk_context_destroy(zk_context* ctx);
+const char* zk_last_error(const zk_context* ctx);
+int zk_abi_version(void);
+/* Runs the context's work on `stream` (a cudaStream_t; NULL: the context's own stream). */
+zk_status zk_context_set_stream(zk_context* ctx, void* stream);
+
+/* ---- the drop-in backend ------------------------------------------------------------------------ */
+/* Replaces gpu::runFusedReference(plan) (src/gpu/fused_reference.cpp:628-630): the fused-exposure,
+ * reduce-partials and row-statistics kernels (src/gpu/fused_kernels.cpp:224-530, :538-563,
+ * :565-771) on the GPU.  Host buffers in, host buffers out. */
+zk_status zk_run_plan(zk_context* ctx, const zk_plan_view* plan, zk_output* out);
+
+/* Many plans in one launch (the reference's book mode, analyses.cpp:1604-2050 runs one plan per
+ * netting set).  Plans that share the scenario (paths, dates, models, seed, Cholesky) share one
+ * simulation of the risk factors on the GPU; the rest run as separate launches. */
+zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_output* outs);
+
+/* Replaces gpu::runAmcStates (src/gpu/fused_reference.cpp:609-626): x and the deflator on every date
+ * ([date][path]) and the exercise value of every Bermudan exercise ([row][path], rows in Bermudan
+ * then exercise order; exercise_rows must equal the plan's total number of exercise dates). */
+zk_status zk_amc_states(zk_context* ctx, const zk_plan_view* plan, float* x, float* deflator, float* exercise,
+                        size_t exercise_rows);
+
+/* FP64 mode.  `normals` (nullable) injects the standard normals instead of the counter-based
+ * generator: normals[((j - 1) * nNormals + k) * streams + s] is normal k of step j on stream s; path p
+ * reads stream p >> 1 with sign (-1)^(p & 1) when the plan is antithetic, else stream p.  `rows`
+ * (nullable, rows_total * nP doubles) receives the per-path rows the fused kernel writes. */
+zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams,
+                          zk_output_f64* out, double* rows);
+/* FP32 with injected normals (converted to float), for the error of the FP32 path against FP64. */
+zk_status zk_run_plan_injected(zk_context* ctx, const zk_plan_view* plan, const double* normals, size_t streams,
+                               zk_output* out, float* rows);
+
+/* ---- device-resident batches (inputs uploaded once; used to time the kernels alone) -------------- */
+typedef struct zk_batch zk_batch;
+typedef struct zk_batch_info {
+  uint64_t num_plans, num_launch_groups, num_paths, num_dates, num_trades_hint;
+  uint64_t num_terms;            /* term records over all plans and dates                         */
+  uint64_t term_evaluations;     /* sum over plans and dates of the terms a path evaluates         */
+  uint64_t exp_evaluations;      /* of which need an exponential                                  */
+  uint64_t table_bytes;          /* bytes of plan tables on the device                            */
+  uint64_t row_bytes;            /* bytes of per-path rows (PFE inputs) written per execute        */
+  uint64_t kernels_per_execute;  /* kernel launches of one zk_batch_execute                         */
+} zk_batch_info;
+
+zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out);
+zk_status zk_batch_execute(zk_batch* b);
+/* Milliseconds of the last execute by kernel: [0] risk-factor simulation, [1] revalue / net /
+ * collateralise / reduce per tile, [2] reduce of the partials, [3] row statistics, measured with CUDA
+ * events on the context stream. */
+zk_status zk_batch_timings(const zk_batch* b, float* ms4);
+zk_status zk_batch_read(zk_batch* b, zk_output* outs);
+zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info);
+void zk_batch_destroy(zk_batch* b);
+
+/* Measured rate of the special-function unit's ex2 (billions per second on the whole GPU), the ceiling
+ * of the fused kernel's bond exponentials (a roofline denominator; not part of the reference). */
+zk_status zk_peak_ex2(int device, double* giga_per_s);
+
+/* ---- plan compiler (host, C++17) ------------------------------------------------------------------ */
+/* Restates gpu::compile (src/gpu/fused_exposure.cpp:214-707) from the flat model / netting-set /
+ * options arrays of zlatko_b200/spec.py, in double precision, without the reference's per-plan caps
+ * on swaps.  zk_plan_view_of gives the single-precision tables (the reference's layout). */
+typedef struct zk_plan zk_plan;
+zk_status zk_compile(const double* model, size_t model_len, const double* netting_set, size_t ns_len,
+                     const double* options, size_t options_len, zk_plan** out, char* err, size_t err_len);
+zk_status zk_plan_view_of(const zk_plan* p, zk_plan_view* view);
+zk_status zk_plan_view_f64_of(const zk_plan* p, zk_plan_view_f64* view);
+/* Simulation dates (nT) and reporting-date indices (nR) of a compiled plan. */
+zk_status zk_plan_dates(const zk_plan* p, double* times, size_t nT, uint64_t* reporting, size_t nR);
+/* Number of simulation dates, reporting dates, stats per date, trades, bermudans, exercise rows. */
+zk_status zk_plan_sizes(const zk_plan* p, uint64_t* sizes6);
+void zk_plan_destroy(zk_plan* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZLATKO_B200_H */

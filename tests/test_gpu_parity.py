@@ -1,0 +1,221 @@
+"""GPU parity: the CUDA kernels (zk_run_plan) against the reference's FP32 CPU kernels (runFusedReference)
+on the same plans, and the FP64 mode against the reference's FP64 ExposureEngine on the same normals.
+
+Tolerances.  The FP32 kernels draw the same counter-based normals as the reference; the two differ only
+by the rounding of single-precision transcendental functions (CUDA's against glibc's), so statistics
+agree to about 1e-6 of their scale; the tests allow 2e-4 of each statistic's scale (and 1e-3 for the
+few path-level view statistics that sit on a histogram edge).  FP64 mode: 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle import ref
+from setups import bermudan, gpu_model, gpu_netting_set, gpu_setup, swap_book
+from zlatko_b200 import gpu
+from zlatko_b200 import spec as S
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")]
+
+RTOL = 2e-4
+
+
+def as_plan(r: ref.RefPlan) -> gpu.Plan:
+    return gpu.Plan.from_arrays(r.header, r.indices, r.params, r.steps, r.terms, r.requests, r.rows_total, r.num_outputs,
+                                r.times, r.reporting.astype(np.int64), r.market_survival)
+
+
+def ref_plan(m, ns, o=None):
+    return ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o or S.Options()))
+
+
+def check_sums(plan, sums_g, sums_r, rtol=RTOL):
+    nS = plan.stats_per_date
+    g = np.asarray(sums_g, np.float64).reshape(-1, nS)
+    r = np.asarray(sums_r, np.float64).reshape(-1, nS)
+    floor = 1e-6 * np.abs(r).max()  # statistics that are zero up to rounding noise (e.g. E[D max(V_i, 0)] of a short option)
+    for k in range(nS):
+        scale = max(np.abs(r[:, k]).max(), floor, 1e-30)
+        err = np.abs(g[:, k] - r[:, k]).max()
+        assert err <= rtol * scale, f"statistic {k}: error {err:.3e} vs scale {scale:.3e}"
+
+
+def check_values(plan, vals_g, vals_r, rtol=RTOL):
+    n = max(1, plan.num_outputs)
+    g, r = np.asarray(vals_g[:n], np.float64), np.asarray(vals_r[:n], np.float64)
+    reqs = plan.requests.reshape(-1, 8)
+    for q in reqs:
+        op, count, out = int(q[0]), int(q[3]), int(q[7])
+        width = count if op == 4 else count + 2 if op == 5 else 1
+        a, b = g[out:out + width], r[out:out + width]
+        if op == 5:  # histogram: counts may move across a bin edge by a path or two
+            assert abs(a[:count].sum() - b[:count].sum()) < 0.5
+            assert np.abs(a[:count] - b[:count]).sum() <= max(4.0, 1e-3 * plan.num_paths)
+            continue
+        scale = max(np.abs(r).max() if op in (0, 7) else np.abs(b).max(), 1e-12)
+        assert np.abs(a - b).max() <= max(rtol, 1e-3 if op in (0, 4, 7) else rtol) * scale, (op, a, b)
+
+
+def run_both(ctx, m, ns, o=None):
+    r = ref_plan(m, ns, o)
+    p = as_plan(r)
+    sg, vg = ctx.run(p)
+    sr, vr = ref.run_fused(r)
+    return r, p, (sg, vg), (sr, vr)
+
+
+@pytest.mark.parametrize("csa", [False, True])
+def test_fused_matches_reference_cpu_kernels(ctx, csa):
+    m, ns = gpu_setup(8000, csa)
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+    # The summaries (gpu::summarise of the reference) of both read-backs agree too.
+    a, b = ref.summarise(r, sg, vg), ref.summarise(r, sr, vr)
+    for k in ("ee", "ene", "pfe", "dee", "dene", "mean_survival"):
+        assert np.abs(a[k] - b[k]).max() <= RTOL * max(np.abs(b[k]).max(), 1e-12), k
+    assert abs(a["pathwise_cva_04"] - b["pathwise_cva_04"]) <= RTOL * abs(b["pathwise_cva_04"])
+
+
+def test_per_trade_and_margin_quantile(ctx):
+    m, ns = gpu_setup(8000, False)
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, S.Options(per_trade=True, im_quantile=0.99))
+    assert p.stats_per_date == 24
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+
+
+def test_path_views(ctx):
+    m, ns = gpu_setup(8000, True)
+    o = S.Options(samples=12, histogram_time=2.0, gross=True, collateral_bands=True, trade_views=True)
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, o)
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+
+
+def test_factor_views_probes(ctx):
+    m, _ = gpu_setup(8000, False)
+    o = S.Options(factor_views=True, samples=5, bond_maturity=8.0)
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, S.NettingSet([]), o)
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+
+
+@pytest.mark.parametrize("kind", [1, 2])
+def test_securities_collateral(ctx, kind):
+    m, ns = gpu_setup(8000, True)
+    ns.csa.kind, ns.csa.haircut, ns.csa.bond_maturity, ns.csa.mpr = kind, 0.02 if kind == 1 else 0.15, 10.0, 20.0 / 250.0
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+
+
+@pytest.mark.parametrize("physical", [True, False])
+def test_bermudan_amc_terms(ctx, physical):
+    """Bermudans priced by the reference-fitted policy and continuation terms: the same exercise decisions."""
+    m, ns = gpu_setup(4000, False)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=physical, degree=2))
+    ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=physical, position=-0.5, degree=3))
+    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, S.Options(exercise_views=True, samples=8))
+    check_sums(p, sg, sr, rtol=1e-3)
+    check_values(p, vg, vr, rtol=1e-3)
+
+
+def test_amc_state_pass_matches_reference(ctx):
+    m, ns = gpu_setup(2000, False)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0), degree=3))
+    r = ref_plan(m, ns)
+    p = as_plan(r)
+    rows = int(ref.lib().ref_amc_rows(r.handle))
+    xg, dg, eg = ctx.amc_states(p, rows)
+    xr, dr, er = ref.amc_states(r)
+    assert np.abs(xg - xr).max() <= 1e-5 * np.abs(xr).max()
+    assert np.abs(dg - dr).max() <= 1e-5
+    assert np.abs(eg - er).max() <= 2e-4 * np.abs(er).max()
+
+
+def test_batch_equals_single_plans(ctx):
+    """Netting sets sharing a scenario run in one launch; each result equals its own single-plan run."""
+    m = gpu_model(3000)
+    m.base_grid = [k / 12 for k in range(1, 61)]
+    books = [swap_book(n, seed=s) for n, s in ((3, 1), (7, 2), (1, 3), (12, 4))]
+    books[1].csa = S.Csa(1e5, 1e5, 1e4)
+    plans = [gpu.compile(m, b, S.Options(pfe_quantile=0.975)) for b in books]
+    many = ctx.run_many(plans)
+    for p, (s, v) in zip(plans, many):
+        s1, v1 = ctx.run(p)
+        assert np.array_equal(s, s1) and np.array_equal(v, v1)
+
+
+def test_pfe_is_the_exact_interpolated_quantile(ctx):
+    """The row-statistics kernel returns ccr::quantile of the rows the fused kernel wrote (exactly, up to
+    the final rounding to float)."""
+    m, ns = gpu_setup(5000, True)
+    for level in (0.5, 0.95, 0.975, 0.99):
+        r = ref_plan(m, ns, S.Options(pfe_quantile=level))
+        p = as_plan(r)
+        streams = (p.num_paths + 1) // 2
+        z = np.random.default_rng(11).standard_normal((p.num_dates - 1) * int(p.header[5]) * streams)
+        sums, vals, rows = ctx.run_injected(p, z, streams, rows=True)
+        for k in range(p.num_reporting):
+            # The plan carries the level in single precision (requests are f32), as the reference's kernel reads it.
+            exact = ref.quantile(rows[int(p.header[28]) + k].astype(np.float64), float(np.float32(level)))
+            assert vals[k] == np.float32(exact) or abs(vals[k] - exact) <= 1e-7 * max(abs(exact), 1.0)
+
+
+def test_invalid_plans_are_rejected(ctx):
+    from zlatko_b200._native import ZkError
+
+    m, ns = gpu_setup(500, False)
+    p = as_plan(ref_plan(m, ns))
+    bad = gpu.Plan.from_arrays(p.header[:20], p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
+                               p.num_outputs, p.times, p.reporting)
+    with pytest.raises(ZkError, match="INVALID_PLAN"):
+        ctx.run(bad)
+    t = p.terms.copy().reshape(-1, 8)
+    t[0, 1] = 40.0  # a swap slot beyond 32 on a fixing term
+    t[0, 0] = 3.0
+    bad2 = gpu.Plan.from_arrays(p.header, p.indices, p.params, p.steps, t.reshape(-1), p.requests, p.rows_total,
+                                p.num_outputs, p.times, p.reporting)
+    with pytest.raises(ZkError, match="INVALID_PLAN"):
+        ctx.run(bad2)
+    h = p.header.copy()
+    h[30] = 64  # nested initial margin: not run by this build
+    with pytest.raises(ZkError, match="UNSUPPORTED"):
+        ctx.run(gpu.Plan.from_arrays(h, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total, p.num_outputs,
+                                     p.times, p.reporting))
+    # The context stays usable after errors.
+    s, v = ctx.run(p)
+    assert np.isfinite(s).all()
+
+
+# ---------------------------------------------------------------- FP64 mode against the FP64 engine
+def injected_normals(plan: gpu.Plan, seed: int):
+    streams = (plan.num_paths + 1) // 2
+    z = np.random.default_rng(seed).standard_normal((plan.num_dates - 1) * int(plan.header[5]) * streams)
+    return z, streams
+
+
+@pytest.mark.parametrize("csa", [False, True])
+def test_fp64_matches_engine_on_identical_normals(ctx, csa):
+    m, ns = gpu_setup(2000, csa)
+    o = S.Options(samples=1, pfe_quantile=0.95)
+    p = gpu.compile(m, ns, o)
+    z, streams = injected_normals(p, 5)
+    sums, vals, rows = ctx.run_f64(p, z, streams, rows=True)
+    e = ref.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams)
+    assert np.array_equal(e.times, p.times)
+    res = __import__("zlatko_b200.summary", fromlist=["summarise"]).summarise(p, sums, vals)
+    for k in ("ev", "ee", "ene", "pfe", "dee", "dene"):
+        scale = max(np.abs(e.profile[k]).max(), 1e-12)
+        assert np.abs(res[k] - e.profile[k]).max() <= 1e-9 * scale, k
+    # Per-path netted values, collateral and exposure on every reporting date.
+    H = p.header
+    rep = e.reporting
+    scale = np.abs(e.netted).max()
+    assert np.abs(rows[H[21]:H[21] + len(rep)].T - e.netted[:, rep]).max() <= 1e-9 * scale
+    if csa:
+        coll = rows[H[22]:H[22] + len(rep)].T
+        assert np.abs(coll - e.collateral[:, rep]).max() <= 1e-9 * scale  # every margin call decided the same way
+    # Pathwise CVA with the simulated survival.
+    pcva = 0.6 * np.nansum(res["cva_inc"])
+    assert abs(pcva - e.pathwise_cva_04) <= 1e-9 * abs(e.pathwise_cva_04)

@@ -1,0 +1,759 @@
+// The C ABI of zlatko_b200 (include/zlatko_b200.h): plan validation, batching, device memory and
+// the launch sequence fused-exposure -> reduce -> row statistics.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/zlatko_b200.h"
+#include "zk_kernels.h"
+
+using namespace zk;
+
+struct zk_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  std::string lastError;
+  uint32_t* dErr = nullptr;
+  void* arena = nullptr;  // reusable device memory of zk_run_plan*
+  size_t arenaBytes = 0;
+};
+
+namespace {
+
+struct Failure {
+  zk_status status;
+  std::string message;
+};
+
+Failure fail(zk_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  return {s, buf};
+}
+
+#define ZK_CUDA(call)                                                                        \
+  do {                                                                                       \
+    const cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                                 \
+      if (e_ == cudaErrorMemoryAllocation) throw fail(ZK_ERR_OUT_OF_MEMORY, "%s: %s", #call, cudaGetErrorString(e_)); \
+      throw fail(ZK_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));                       \
+    }                                                                                        \
+  } while (0)
+
+zk_status record(zk_context* ctx, const Failure& f) {
+  if (ctx) ctx->lastError = f.message;
+  return f.status;
+}
+
+template <typename R>
+struct View {
+  const uint32_t* header;
+  size_t header_len;
+  const uint32_t* indices;
+  size_t indices_len;
+  const R* params;
+  size_t params_len;
+  const R* steps;
+  size_t steps_len;
+  const R* terms;
+  size_t terms_len;
+  const R* requests;
+  size_t requests_len;
+  uint32_t rows_total, num_outputs;
+};
+
+View<float> viewOf(const zk_plan_view& v) {
+  return {v.header, v.header_len, v.indices, v.indices_len, v.params, v.params_len, v.steps, v.steps_len,
+          v.terms, v.terms_len, v.requests, v.requests_len, v.rows_total, v.num_outputs};
+}
+View<double> viewOf(const zk_plan_view_f64& v) {
+  return {v.header, v.header_len, v.indices, v.indices_len, v.params, v.params_len, v.steps, v.steps_len,
+          v.terms, v.terms_len, v.requests, v.requests_len, v.rows_total, v.num_outputs};
+}
+
+// A plan after validation, with the quantities the launch needs.
+template <typename R>
+struct Plan {
+  View<R> v;
+  const uint32_t* H;
+  uint32_t nP, nT, nA, nC, sub, nNormals, seed, anti, hasCsa, cpty, nCorr, offCall, offRep, nS, nR, nTr, nBerm;
+  uint32_t rowDV, rowE, rowV, rowC, rowGross, rowTrades, rowEx, rowEP;
+  size_t nTerms, nReq, nIdx;
+  uint32_t nSlots = 0, ring = 1, ctype = 0, stateWords = 0;
+  bool usesAssets = false, probes = false;
+  uint32_t exerciseRows = 0;
+  uint32_t bermRows[kMaxBermudans] = {0, 0, 0, 0};
+  uint64_t termEvals = 0, expEvals = 0;
+};
+
+template <typename R>
+Plan<R> parse(const View<R>& v, size_t index) {
+  Plan<R> p;
+  p.v = v;
+  auto bad = [&](const char* what) { return fail(ZK_ERR_INVALID_PLAN, "plan %zu: %s", index, what); };
+  if (!v.header || v.header_len != static_cast<size_t>(kHeaderWords)) throw bad("malformed plan header (32 words expected)");
+  const uint32_t* H = v.header;
+  p.H = H;
+  p.nP = H[hP], p.nT = H[hT], p.nA = H[hA], p.nC = H[hC], p.sub = H[hSub], p.nNormals = H[hNormals], p.seed = H[hSeed];
+  p.anti = H[hAnti], p.hasCsa = H[hCsa], p.cpty = H[hCpty], p.nCorr = H[hCorr], p.offCall = H[hOffCall], p.offRep = H[hOffRep];
+  p.nS = H[hS], p.nR = H[hR], p.nTr = H[hTr], p.nBerm = H[hBerm];
+  p.rowDV = H[hRowDV], p.rowE = H[hRowE], p.rowV = H[hRowV], p.rowC = H[hRowC], p.rowGross = H[hRowGross];
+  p.rowTrades = H[hRowTrades], p.rowEx = H[hRowEx], p.rowEP = H[hRowEP];
+  if (p.nP == 0 || p.nT == 0) throw bad("empty plan");
+  if (H[hInner] != 0) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the nested initial margin (imInnerPaths > 0) is not run by this build", index);
+  if (!v.params || v.params_len != static_cast<size_t>(kParamCount)) throw bad("params must hold 84 values");
+  if (!v.steps || v.steps_len != static_cast<size_t>(p.nT) * kStepStride) throw bad("steps must hold nT * 24 values");
+  if (p.nA > kMaxAssets) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: at most 4 assets", index);
+  if (p.nC > kMaxCredits) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: at most 2 credits", index);
+  if (p.nCorr != 1 + p.nA + p.nC || p.nCorr > kChol) throw bad("number of correlated factors must be 1 + assets + credits");
+  if (p.sub == 0) throw bad("CIR sub-steps must be positive");
+  if (p.nNormals > kMaxNormals || p.nNormals < p.nCorr + 1 + p.nC * (p.sub - 1)) throw bad("inconsistent number of normals per step");
+  if (p.nC > 0 && p.cpty >= p.nC) throw bad("counterparty index out of range");
+  if (p.offCall != p.nT + 1 || p.offRep != 2 * p.nT + 1) throw bad("index table offsets do not match the reference layout");
+  if (!v.indices || v.indices_len < 3 * static_cast<size_t>(p.nT) + 1) throw bad("index table too short");
+  if (v.terms_len % kTermStride) throw bad("term table length is not a multiple of 8");
+  if (v.requests_len % kRequestStride) throw bad("request table length is not a multiple of 8");
+  if (p.nS < kStatsPerDate) throw bad("statsPerDate below 8");
+  p.nTerms = v.terms_len / kTermStride;
+  p.nReq = v.requests_len / kRequestStride;
+  p.nIdx = v.indices_len;
+  if (p.nTerms > 0 && !v.terms) throw bad("null term table");
+  if (p.nReq > 0 && !v.requests) throw bad("null request table");
+  const uint32_t* I = v.indices;
+  for (uint32_t j = 0; j < p.nT; ++j)
+    if (I[j] > I[j + 1]) throw bad("term starts must not decrease");
+  if (I[p.nT] > p.nTerms) throw bad("term starts beyond the term table");
+  const uint32_t rows = v.rows_total;
+  uint32_t maxLag = 0, maxSlot = 0;
+  bool anySlot = false;
+  for (uint32_t j = 0; j < p.nT; ++j) {
+    const uint32_t c = I[p.offCall + j];
+    if (c > j) throw bad("margin call date after the valuation date");
+    maxLag = std::max(maxLag, j - c);
+    if (I[p.offRep + j] > p.nR) throw bad("reporting slot beyond the reporting dates");
+  }
+  auto rowBlock = [&](uint32_t base, uint64_t n, const char* what) {
+    if (base != kNoRow && static_cast<uint64_t>(base) + n > rows) throw bad(what);
+  };
+  rowBlock(p.rowEP, p.nR, "exposure rows beyond rows_total");
+  rowBlock(p.rowDV, p.nR, "margin rows beyond rows_total");
+  rowBlock(p.rowE, p.nR, "exposure-value rows beyond rows_total");
+  rowBlock(p.rowV, p.nR, "netted rows beyond rows_total");
+  rowBlock(p.rowC, p.nR, "collateral rows beyond rows_total");
+  rowBlock(p.rowGross, p.nR, "gross rows beyond rows_total");
+  rowBlock(p.rowTrades, static_cast<uint64_t>(std::min<uint32_t>(p.nTr, kMaxTradeGroups)) * p.nR, "trade rows beyond rows_total");
+  rowBlock(p.rowEx, std::min<uint32_t>(p.nBerm, kMaxBermudans), "exercise rows beyond rows_total");
+  if (p.rowEP == kNoRow) throw bad("the exposure rows are required");
+  for (size_t t = 0; t < p.nTerms; ++t) {
+    const R* rec = v.terms + t * kTermStride;
+    if (!(rec[0] >= R(0)) || rec[0] >= R(4294967296.0)) throw bad("invalid term code");
+    const uint32_t code = static_cast<uint32_t>(rec[0]), kind = code & 15u;
+    // rec[1] is an index (swap slot, asset, probe selector) except for continuation terms, where it holds
+    // the Bermudan's position.
+    if (kind != kBermContinue && (!(rec[1] >= R(0)) || rec[1] >= R(4294967296.0))) throw bad("invalid term slot");
+    const uint32_t slot = kind == kBermContinue ? 0u : static_cast<uint32_t>(rec[1]);
+    if (kind == kAsset || kind == kOption) p.usesAssets = true;
+    if (kind == kProbe) {
+      const uint32_t what = slot & 15u;
+      if (what == 2 || what == 6) p.usesAssets = true;
+      if (what == 3 || what == 4) p.probes = true;
+    }
+    if (kind == kFixedFloat || kind == kSetFixing || (kind > kProbe) || kind == kBermFloat) {
+      if (slot >= static_cast<uint32_t>(kMaxSwapSlots)) throw bad("swap slot beyond 32");
+      maxSlot = std::max(maxSlot, slot);
+      anySlot = true;
+    }
+    if (kind == kProbe) {
+      if (!(rec[5] >= R(0)) || static_cast<double>(rec[5]) >= static_cast<double>(rows)) throw bad("probe row beyond rows_total");
+    }
+    if (kind == kBermDecide) {
+      const uint32_t bm = std::min((code >> 8u) & 15u, 3u), extra = code >> 12u;
+      p.bermRows[bm] = std::max(p.bermRows[bm], extra + 1);
+    }
+  }
+  for (uint32_t b = 0; b < kMaxBermudans; ++b) p.exerciseRows += p.bermRows[b];
+  for (uint32_t j = 0; j < p.nT; ++j) {
+    for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
+      const uint32_t kind = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]) & 15u;
+      p.termEvals += 1;
+      if (kind != kAsset && kind != kBermDecide && kind != kBermContinue) p.expEvals += 1;
+    }
+  }
+  for (size_t q = 0; q < p.nReq; ++q) {
+    const R* rq = v.requests + q * kRequestStride;
+    const uint32_t op = static_cast<uint32_t>(rq[0]), row = static_cast<uint32_t>(rq[1]), row2 = static_cast<uint32_t>(rq[2]);
+    const uint64_t count = static_cast<uint64_t>(rq[3]), out = static_cast<uint64_t>(rq[7]);
+    if (op > 9) throw bad("unknown row-statistics operation");
+    if (row >= rows) throw bad("request row beyond rows_total");
+    if ((op == 6 || op == 8 || op == 9) && row2 >= rows) throw bad("request row2 beyond rows_total");
+    const uint64_t width = op == 4 ? count : op == 5 ? count + 2 : 1;
+    if (op == 5 && (count == 0 || count > 3072)) throw bad("histogram bins must be 1..3072");
+    if (out + width > std::max<uint32_t>(1, v.num_outputs)) throw bad("request output beyond numOutputs");
+  }
+  p.nSlots = anySlot ? maxSlot + 1 : 0;
+  p.ctype = p.hasCsa ? static_cast<uint32_t>(v.params[16 + kChol * kChol]) : 0u;
+  if (p.ctype > 2) throw bad("unknown collateral type");
+  p.ring = maxLag + 1;
+  if (p.hasCsa && p.ring > static_cast<uint32_t>(kMaxRing))
+    throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the margin-call look-back spans %u dates (at most %d)", index, maxLag, kMaxRing - 1);
+  if (p.ctype == 2) p.usesAssets = true;
+  p.stateWords = p.nSlots + (p.hasCsa ? p.ring * (p.ctype != 0 ? 2 : 1) : 0);
+  return p;
+}
+
+// Plans share a scenario when every input of the risk-factor simulation is identical.
+template <typename R>
+bool sameScenario(const Plan<R>& a, const Plan<R>& b) {
+  if (a.nP != b.nP || a.nT != b.nT || a.nA != b.nA || a.nC != b.nC || a.sub != b.sub || a.nNormals != b.nNormals ||
+      a.seed != b.seed || a.anti != b.anti || a.nCorr != b.nCorr)
+    return false;
+  if (std::memcmp(a.v.params, b.v.params, 8 * sizeof(R)) || std::memcmp(a.v.params + 12, b.v.params + 12, (4 + 64) * sizeof(R)))
+    return false;
+  for (uint32_t j = 0; j < a.nT; ++j)
+    if (std::memcmp(a.v.steps + static_cast<size_t>(j) * kStepStride, b.v.steps + static_cast<size_t>(j) * kStepStride, 22 * sizeof(R)))
+      return false;
+  return true;
+}
+
+size_t alignUp(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+// A set of plans laid out in one device arena, ready to execute.
+template <typename R>
+struct Batch {
+  zk_context* ctx = nullptr;
+  std::vector<Plan<R>> plans;
+  struct Launch {
+    ScenarioArgs<R> sc;
+    CubeArgs<R> cb;
+    std::vector<uint32_t> planIdx;
+    uint32_t numTiles = 0, numFields = 0;
+    size_t stateWordsMax = 0;
+    bool perTrade = false, probes = false;
+    size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
+  };
+  std::vector<Launch> launches;
+  // device offsets per plan
+  struct Dev {
+    size_t idx, terms, steps, req, expo, partials, sums, values;
+  };
+  std::vector<Dev> dev;
+  size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
+  size_t inputBytes = 0, totalBytes = 0, outBegin = 0, outBytes = 0;
+  uint32_t numRowJobs = 0, maxReduceN = 0;
+  std::vector<unsigned char> image;  // host image of the input region
+  unsigned char* base = nullptr;     // device arena
+  bool ownsArena = false;
+  bool sink = false;
+  uint32_t exerciseRows = 0;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float ms[4] = {0, 0, 0, 0};
+  bool timed = false;
+
+  ~Batch() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (ownsArena && base) cudaFree(base);
+  }
+};
+
+
+template <typename R>
+std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams) {
+  auto B = std::make_unique<Batch<R>>();
+  B->ctx = ctx;
+  B->sink = sink;
+  for (size_t i = 0; i < views.size(); ++i) B->plans.push_back(parse(views[i], i));
+  const size_t nPlans = B->plans.size();
+  // ---- launch groups: plans sharing the scenario ----
+  std::vector<int> launchOf(nPlans, -1);
+  for (size_t i = 0; i < nPlans; ++i) {
+    if (launchOf[i] >= 0) continue;
+    typename Batch<R>::Launch L;
+    for (size_t k = i; k < nPlans; ++k)
+      if (launchOf[k] < 0 && sameScenario(B->plans[i], B->plans[k])) {
+        launchOf[k] = static_cast<int>(B->launches.size());
+        L.planIdx.push_back(static_cast<uint32_t>(k));
+      }
+    B->launches.push_back(std::move(L));
+  }
+  if (normals && B->launches.size() != 1) throw fail(ZK_ERR_INVALID_ARGUMENT, "injected normals need plans of one scenario");
+  // ---- per launch: the factor cube shared by its netting sets, one CTA column per netting set ----
+  for (auto& L : B->launches) {
+    for (uint32_t k : L.planIdx) {
+      const auto& P = B->plans[k];
+      L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
+      L.perTrade = L.perTrade || P.nTr > 0;
+      L.probes = L.probes || P.probes;
+    }
+    const Plan<R>& P0 = B->plans[L.planIdx.front()];
+    L.numTiles = (P0.nP + kTile - 1) / kTile;
+    ScenarioArgs<R>& sc = L.sc;
+    sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
+    sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
+    sc.steps = nullptr, sc.normals = nullptr;
+    for (int k = 0; k < 8; ++k) sc.cir[k] = P0.v.params[k];
+    for (int k = 0; k < 4; ++k) sc.spots[k] = P0.v.params[12 + k];
+    for (int k = 0; k < 64; ++k) sc.chol[k] = P0.v.params[16 + k];
+    CubeArgs<R>& cb = L.cb;
+    cb.nP = P0.nP, cb.nT = P0.nT, cb.nA = P0.nA, cb.nC = P0.nC;
+    cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fLnS = 2 + P0.nA + P0.nC, cb.fY = 2 + 2 * P0.nA + P0.nC;
+    cb.probes = L.probes ? 1u : 0u;
+    L.numFields = L.probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC;
+    if (revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8) > 200 * 1024)
+      throw fail(ZK_ERR_UNSUPPORTED, "a netting set needs more shared memory than a CTA has");
+  }
+  if (normals) {
+    const Plan<R>& P0 = B->plans[0];
+    const size_t need = P0.anti ? (P0.nP + 1) / 2 : P0.nP;
+    if (streams < need) throw fail(ZK_ERR_INVALID_ARGUMENT, "injected normals: %zu streams for %zu needed", streams, need);
+  }
+  // ---- arena layout: inputs first (one upload), then device-only scratch, outputs last ----
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off = alignUp(off + std::max<size_t>(bytes, 16)); return o; };
+  B->dev.resize(nPlans);
+  for (size_t i = 0; i < nPlans; ++i) {
+    const auto& P = B->plans[i];
+    auto& D = B->dev[i];
+    D.idx = take(P.nIdx * 4);
+    D.terms = take(P.nTerms * kTermStride * sizeof(R));
+    D.steps = take(static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
+    D.req = take(P.nReq * kRequestStride * sizeof(R));
+  }
+  for (auto& L : B->launches) L.nsOff = take(L.planIdx.size() * sizeof(NsArgs<R>));
+  B->reduceOff = take(nPlans * sizeof(ReduceJob<R>));
+  for (const auto& P : B->plans) B->numRowJobs += static_cast<uint32_t>(P.nReq);
+  B->rowOff = take(B->numRowJobs * sizeof(RowJob<R>));
+  if (sink) {
+    const auto& P = B->plans[0];
+    B->exerciseRows = P.exerciseRows;
+    B->bermRowOff = take(kMaxBermudans * 4);
+  }
+  if (normals) {
+    const auto& P = B->plans[0];
+    B->normalsOff = take(static_cast<size_t>(P.nT - 1) * P.nNormals * streams * sizeof(R));
+  }
+  B->inputBytes = off;
+  for (auto& L : B->launches)
+    L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
+  for (size_t i = 0; i < nPlans; ++i) {
+    const auto& P = B->plans[i];
+    const uint32_t tiles = (P.nP + kTile - 1) / kTile;
+    B->dev[i].expo = take(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
+    B->dev[i].partials = take(static_cast<size_t>(tiles) * P.nT * P.nS * sizeof(R));
+  }
+  if (sink) {
+    const auto& P = B->plans[0];
+    B->sinkOff[0] = take(static_cast<size_t>(P.nT) * P.nP * 4);
+    B->sinkOff[1] = take(static_cast<size_t>(P.nT) * P.nP * 4);
+    B->sinkOff[2] = take(static_cast<size_t>(std::max<uint32_t>(P.exerciseRows, 1)) * P.nP * 4);
+  }
+  B->outBegin = off;
+  for (size_t i = 0; i < nPlans; ++i) {
+    const auto& P = B->plans[i];
+    B->dev[i].sums = take(static_cast<size_t>(P.nT) * P.nS * sizeof(R));
+    B->dev[i].values = take(static_cast<size_t>(std::max<uint32_t>(P.v.num_outputs, 1)) * sizeof(R));
+  }
+  B->outBytes = off - B->outBegin;
+  B->totalBytes = off;
+  return B;
+}
+
+// Fills the host image of the input region, once the arena base is known.
+template <typename R>
+void fillImage(Batch<R>& B, const double* normals, size_t streams) {
+  B.image.assign(B.inputBytes, 0);
+  unsigned char* img = B.image.data();
+  const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
+  auto dptr = [&](size_t o) { return reinterpret_cast<void*>(base + o); };
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    const auto& P = B.plans[i];
+    const auto& D = B.dev[i];
+    std::memcpy(img + D.idx, P.v.indices, P.nIdx * 4);
+    if (P.nTerms) std::memcpy(img + D.terms, P.v.terms, P.nTerms * kTermStride * sizeof(R));
+    std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
+    if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
+  }
+  for (auto& L : B.launches) {
+    std::vector<NsArgs<R>> args(L.planIdx.size());
+    for (size_t k = 0; k < L.planIdx.size(); ++k) {
+      const auto& P = B.plans[L.planIdx[k]];
+      const auto& D = B.dev[L.planIdx[k]];
+      NsArgs<R>& A = args[k];
+      std::memset(&A, 0, sizeof A);
+      A.idx = static_cast<const uint32_t*>(dptr(D.idx));
+      A.terms = static_cast<const R*>(dptr(D.terms));
+      A.steps = static_cast<const R*>(dptr(D.steps));
+      A.expo = static_cast<R*>(dptr(D.expo));
+      A.partials = static_cast<R*>(dptr(D.partials));
+      const R* prm = P.v.params;
+      A.hc = prm[8], A.hb = prm[9], A.mta = prm[10], A.ia = prm[11];
+      A.keepHaircut = R(1) - prm[16 + kChol * kChol + 2];
+      A.hasCsa = P.hasCsa, A.ctype = P.ctype, A.casset = static_cast<uint32_t>(prm[16 + kChol * kChol + 1]);
+      A.cpty = P.nC > 0 ? P.cpty : 0xFFFFFFFFu;
+      A.nS = P.nS, A.nTr = P.nTr, A.nBerm = P.nBerm, A.nR = P.nR;
+      A.rowEP = P.rowEP, A.rowDV = P.rowDV, A.rowE = P.rowE, A.rowV = P.rowV, A.rowC = P.rowC, A.rowGross = P.rowGross;
+      A.rowTrades = P.rowTrades, A.rowEx = P.rowEx;
+      A.offCall = P.offCall, A.offRep = P.offRep, A.nSlots = P.nSlots, A.ring = P.ring;
+      A.usesAssets = P.usesAssets ? 1u : 0u;
+      if (B.sink) {
+        A.sinkX = static_cast<float*>(dptr(B.sinkOff[0]));
+        A.sinkD = static_cast<float*>(dptr(B.sinkOff[1]));
+        A.sinkEx = static_cast<float*>(dptr(B.sinkOff[2]));
+        A.sinkRowOfBermudan = static_cast<const uint32_t*>(dptr(B.bermRowOff));
+      }
+    }
+    std::memcpy(img + L.nsOff, args.data(), args.size() * sizeof(NsArgs<R>));
+    const auto& P0 = B.plans[L.planIdx.front()];
+    L.sc.steps = static_cast<const R*>(dptr(B.dev[L.planIdx.front()].steps));
+    L.sc.normals = normals ? static_cast<const R*>(dptr(B.normalsOff)) : nullptr;
+    L.cb.data = static_cast<R*>(dptr(L.cubeOff));
+    (void)P0;
+  }
+  std::vector<ReduceJob<R>> red(B.plans.size());
+  std::vector<RowJob<R>> rows;
+  rows.reserve(B.numRowJobs);
+  B.maxReduceN = 0;
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    const auto& P = B.plans[i];
+    const auto& D = B.dev[i];
+    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, (P.nP + kTile - 1) / kTile, P.nP, 0};
+    B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
+    for (size_t q = 0; q < P.nReq; ++q)
+      rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),
+                      static_cast<R*>(dptr(D.values)), P.nP, 0});
+  }
+  std::memcpy(img + B.reduceOff, red.data(), red.size() * sizeof(ReduceJob<R>));
+  if (!rows.empty()) std::memcpy(img + B.rowOff, rows.data(), rows.size() * sizeof(RowJob<R>));
+  if (B.sink) {
+    uint32_t offs[kMaxBermudans], acc = 0;
+    for (int b = 0; b < kMaxBermudans; ++b) offs[b] = acc, acc += B.plans[0].bermRows[b];
+    std::memcpy(img + B.bermRowOff, offs, sizeof offs);
+  }
+  if (normals) {
+    const auto& P = B.plans[0];
+    const size_t n = static_cast<size_t>(P.nT - 1) * P.nNormals * streams;
+    R* dst = reinterpret_cast<R*>(img + B.normalsOff);
+    for (size_t k = 0; k < n; ++k) dst[k] = static_cast<R>(normals[k]);
+  }
+}
+
+template <typename R>
+void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normals, size_t streams) {
+  if (useCtxArena) {
+    if (ctx->arenaBytes < B.totalBytes) {
+      if (ctx->arena) cudaFree(ctx->arena);
+      ctx->arena = nullptr;
+      ctx->arenaBytes = 0;
+      ZK_CUDA(cudaMalloc(&ctx->arena, B.totalBytes));
+      ctx->arenaBytes = B.totalBytes;
+    }
+    B.base = static_cast<unsigned char*>(ctx->arena);
+  } else {
+    void* p = nullptr;
+    ZK_CUDA(cudaMalloc(&p, B.totalBytes));
+    B.base = static_cast<unsigned char*>(p);
+    B.ownsArena = true;
+  }
+  fillImage(B, normals, streams);
+  ZK_CUDA(cudaMemcpyAsync(B.base, B.image.data(), B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));
+}
+
+template <typename R>
+void execute(Batch<R>& B) {
+  zk_context* ctx = B.ctx;
+  cudaStream_t s = ctx->stream;
+  if (!B.ev[0])
+    for (auto& e : B.ev) ZK_CUDA(cudaEventCreate(&e));
+  ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, s));
+  ZK_CUDA(cudaEventRecord(B.ev[0], s));
+  const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
+  for (auto& L : B.launches) ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
+  ZK_CUDA(cudaEventRecord(B.ev[1], s));
+  for (auto& L : B.launches)
+    ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
+                             L.numTiles, L.stateWordsMax, L.perTrade, B.sink, s));
+  ZK_CUDA(cudaEventRecord(B.ev[2], s));
+  if (!B.sink) {
+    ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
+    ZK_CUDA(cudaEventRecord(B.ev[3], s));
+    ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff), B.numRowJobs, ctx->dErr, s));
+  } else {
+    ZK_CUDA(cudaEventRecord(B.ev[3], s));
+  }
+  ZK_CUDA(cudaEventRecord(B.ev[4], s));
+  B.timed = true;
+}
+
+template <typename R>
+void finish(Batch<R>& B) {
+  zk_context* ctx = B.ctx;
+  uint32_t err = 0;
+  ZK_CUDA(cudaMemcpyAsync(&err, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (B.timed) {
+    for (int k = 0; k < 4; ++k) ZK_CUDA(cudaEventElapsedTime(&B.ms[k], B.ev[k], B.ev[k + 1]));
+  }
+  if (err == kDevTimeout) throw fail(ZK_ERR_DEVICE_TIMEOUT, "a bounded wait in the fused kernel gave up");
+  if (err != 0) throw fail(ZK_ERR_CUDA, "a kernel reported error %u", err);
+}
+
+template <typename R, typename Out>
+void readOutputs(Batch<R>& B, Out* outs) {
+  std::vector<unsigned char> host(B.outBytes);
+  ZK_CUDA(cudaMemcpyAsync(host.data(), B.base + B.outBegin, B.outBytes, cudaMemcpyDeviceToHost, B.ctx->stream));
+  finish(B);
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    const auto& P = B.plans[i];
+    const auto& D = B.dev[i];
+    const R* sums = reinterpret_cast<const R*>(host.data() + (D.sums - B.outBegin));
+    const R* vals = reinterpret_cast<const R*>(host.data() + (D.values - B.outBegin));
+    const size_t nS = static_cast<size_t>(P.nT) * P.nS, nV = std::max<uint32_t>(P.v.num_outputs, 1);
+    for (size_t k = 0; k < nS; ++k) outs[i].sums[k] = sums[k];
+    for (size_t k = 0; k < nV; ++k) outs[i].values[k] = vals[k];
+  }
+}
+
+template <typename Out>
+void checkOutput(const Out* o, size_t nSums, size_t nValues, size_t i) {
+  if (!o || !o->sums || !o->values) throw fail(ZK_ERR_INVALID_ARGUMENT, "output %zu: null buffer", i);
+  if (o->sums_len != nSums) throw fail(ZK_ERR_INVALID_ARGUMENT, "output %zu: sums must hold nT * statsPerDate = %zu values", i, nSums);
+  if (o->values_len < nValues) throw fail(ZK_ERR_INVALID_ARGUMENT, "output %zu: values must hold max(1, numOutputs) = %zu values", i, nValues);
+}
+
+template <typename R>
+void checkOutputs(const Batch<R>& B, const void* outs, bool f64) {
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    const auto& P = B.plans[i];
+    const size_t nS = static_cast<size_t>(P.nT) * P.nS, nV = std::max<uint32_t>(P.v.num_outputs, 1);
+    if (f64) checkOutput(static_cast<const zk_output_f64*>(outs) + i, nS, nV, i);
+    else checkOutput(static_cast<const zk_output*>(outs) + i, nS, nV, i);
+  }
+}
+
+void requireCtx(zk_context* ctx) {
+  if (!ctx) throw fail(ZK_ERR_INVALID_ARGUMENT, "null context");
+  ZK_CUDA(cudaSetDevice(ctx->device));
+}
+
+}  // namespace
+
+namespace {
+template <typename R, typename ViewT, typename OutT>
+zk_status runInjected(zk_context* ctx, const ViewT* plan, const double* normals, size_t streams, OutT* out, R* rows) {
+  try {
+    requireCtx(ctx);
+    if (!plan || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    auto B = build<R>(ctx, {viewOf(*plan)}, false, normals, streams);
+    checkOutputs(*B, out, sizeof(R) == 8);
+    upload(*B, ctx, true, normals, streams);
+    execute(*B);
+    if (rows) {
+      const auto& P = B->plans[0];
+      ZK_CUDA(cudaMemcpyAsync(rows, B->base + B->dev[0].expo, static_cast<size_t>(P.v.rows_total) * P.nP * sizeof(R),
+                              cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    readOutputs(*B, out);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+}  // namespace
+
+// ================================================================================================
+struct zk_batch {
+  std::unique_ptr<Batch<float>> b;
+};
+
+extern "C" {
+
+int zk_abi_version(void) { return ZK_ABI_VERSION; }
+
+zk_status zk_context_create(int device, zk_context** out) {
+  if (!out) return ZK_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return ZK_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return ZK_ERR_INVALID_ARGUMENT;
+  auto* ctx = new zk_context();
+  ctx->device = device;
+  try {
+    ZK_CUDA(cudaSetDevice(device));
+    ZK_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->ownStream = true;
+    ZK_CUDA(cudaMalloc(&ctx->dErr, 16));
+  } catch (const Failure& f) {
+    delete ctx;
+    return f.status;
+  }
+  *out = ctx;
+  return ZK_OK;
+}
+
+void zk_context_destroy(zk_context* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->arena) cudaFree(ctx->arena);
+  if (ctx->dErr) cudaFree(ctx->dErr);
+  if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* zk_last_error(const zk_context* ctx) { return ctx ? ctx->lastError.c_str() : "null context"; }
+
+zk_status zk_context_set_stream(zk_context* ctx, void* stream) {
+  if (!ctx) return ZK_ERR_INVALID_ARGUMENT;
+  if (stream) {
+    if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->ownStream = false;
+  }
+  return ZK_OK;
+}
+
+zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_output* outs) {
+  try {
+    requireCtx(ctx);
+    if (!plans || !outs || n == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "null or empty plan list");
+    std::vector<View<float>> views;
+    for (size_t i = 0; i < n; ++i) views.push_back(viewOf(plans[i]));
+    auto B = build<float>(ctx, views, false, nullptr, 0);
+    checkOutputs(*B, outs, false);
+    upload(*B, ctx, true, nullptr, 0);
+    execute(*B);
+    readOutputs(*B, outs);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  } catch (const std::exception& e) {
+    return record(ctx, fail(ZK_ERR_CUDA, "%s", e.what()));
+  }
+}
+
+zk_status zk_run_plan(zk_context* ctx, const zk_plan_view* plan, zk_output* out) { return zk_run_plans(ctx, plan, 1, out); }
+
+zk_status zk_amc_states(zk_context* ctx, const zk_plan_view* plan, float* x, float* deflator, float* exercise, size_t exercise_rows) {
+  try {
+    requireCtx(ctx);
+    if (!plan || !x || !deflator) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    auto B = build<float>(ctx, {viewOf(*plan)}, true, nullptr, 0);
+    if (exercise_rows != B->exerciseRows)
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "the plan has %u exercise rows, not %zu", B->exerciseRows, exercise_rows);
+    if (exercise_rows > 0 && !exercise) throw fail(ZK_ERR_INVALID_ARGUMENT, "null exercise buffer");
+    upload(*B, ctx, true, nullptr, 0);
+    execute(*B);
+    const auto& P = B->plans[0];
+    const size_t n = static_cast<size_t>(P.nT) * P.nP;
+    ZK_CUDA(cudaMemcpyAsync(x, B->base + B->sinkOff[0], n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(deflator, B->base + B->sinkOff[1], n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (exercise_rows)
+      ZK_CUDA(cudaMemcpyAsync(exercise, B->base + B->sinkOff[2], exercise_rows * P.nP * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    finish(*B);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
+
+zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams, zk_output_f64* out,
+                          double* rows) {
+  return runInjected<double>(ctx, plan, normals, streams, out, rows);
+}
+
+zk_status zk_run_plan_injected(zk_context* ctx, const zk_plan_view* plan, const double* normals, size_t streams, zk_output* out,
+                               float* rows) {
+  return runInjected<float>(ctx, plan, normals, streams, out, rows);
+}
+
+// ---- device-resident batches ----
+zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out) {
+  try {
+    requireCtx(ctx);
+    if (!plans || !out || n == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "null or empty plan list");
+    std::vector<View<float>> views;
+    for (size_t i = 0; i < n; ++i) views.push_back(viewOf(plans[i]));
+    auto b = std::make_unique<zk_batch>();
+    b->b = build<float>(ctx, views, false, nullptr, 0);
+    upload(*b->b, ctx, false, nullptr, 0);
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_batch_execute(zk_batch* b) {
+  if (!b) return ZK_ERR_INVALID_ARGUMENT;
+  try {
+    ZK_CUDA(cudaSetDevice(b->b->ctx->device));
+    execute(*b->b);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(b->b->ctx, f);
+  }
+}
+
+zk_status zk_batch_timings(const zk_batch* b, float* ms4) {
+  if (!b || !ms4) return ZK_ERR_INVALID_ARGUMENT;
+  try {
+    Batch<float>& B = *b->b;
+    ZK_CUDA(cudaEventSynchronize(B.ev[4]));
+    for (int k = 0; k < 4; ++k) ZK_CUDA(cudaEventElapsedTime(&B.ms[k], B.ev[k], B.ev[k + 1]));
+    for (int i = 0; i < 4; ++i) ms4[i] = B.ms[i];
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(b->b->ctx, f);
+  }
+}
+
+zk_status zk_batch_read(zk_batch* b, zk_output* outs) {
+  if (!b || !outs) return ZK_ERR_INVALID_ARGUMENT;
+  try {
+    checkOutputs(*b->b, outs, false);
+    readOutputs(*b->b, outs);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(b->b->ctx, f);
+  }
+}
+
+zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
+  if (!b || !info) return ZK_ERR_INVALID_ARGUMENT;
+  const Batch<float>& B = *b->b;
+  std::memset(info, 0, sizeof *info);
+  info->num_plans = B.plans.size();
+  info->num_launch_groups = B.launches.size();
+  info->num_paths = B.plans[0].nP;
+  info->num_dates = B.plans[0].nT;
+  for (const auto& P : B.plans) {
+    info->num_terms += P.nTerms;
+    info->term_evaluations += P.termEvals;
+    info->exp_evaluations += P.expEvals;
+    info->table_bytes += P.nIdx * 4 + P.nTerms * 32 + static_cast<uint64_t>(P.nT) * 96 + P.nReq * 32;
+    info->row_bytes += static_cast<uint64_t>(P.nR) * P.nP * 4;
+  }
+  info->kernels_per_execute = 2 * B.launches.size() + 2;
+  return ZK_OK;
+}
+
+void zk_batch_destroy(zk_batch* b) {
+  if (!b) return;
+  if (b->b && b->b->ctx) {
+    cudaSetDevice(b->b->ctx->device);
+    cudaStreamSynchronize(b->b->ctx->stream);
+  }
+  delete b;
+}
+
+}  // extern "C"

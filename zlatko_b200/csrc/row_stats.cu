@@ -1,0 +1,305 @@
+// reduce-partials and row statistics (the reference's second and third kernels,
+// src/gpu/fused_kernels.cpp:538-563 and :565-771; CPU mirror finishFused,
+// src/gpu/fused_reference.cpp:468-607).
+//
+// reduce: one thread per (date, statistic) sums the per-tile partials in tile order with a
+// compensated double-precision sum, so the result does not depend on scheduling.
+//
+// row statistics: one CTA per request.  Quantiles are the *exact* empirical quantile interpolated
+// between order statistics k = floor(p (n - 1)) and k + 1, as ccr::quantile does
+// (include/ccr/core/math.hpp:39-47), found without sorting the row: a min/max pass, a 4096-bin
+// histogram pass that locates the bins of ranks k and k + 1, then either one pass that reads the
+// maximum of k's bin and the minimum of k+1's bin (different bins) or a gather of k's bin into
+// shared memory and a bitonic sort there (same bin; narrowed again if the bin holds more than
+// kCap values).  The reference's histogram kernel interpolates inside the final bin instead and
+// agrees with the exact quantile to about 5e-8 (README.md:182).
+#include <cfloat>
+
+#include "zk_device.cuh"
+#include "zk_kernels.h"
+
+namespace zk {
+
+namespace {
+
+constexpr int kRowThreads = 512;
+constexpr int kRowWarps = kRowThreads / 32;
+constexpr int kBins = 4096;
+constexpr int kCap = 8192;
+constexpr int kMaxRounds = 16;
+constexpr int kHistBins = 3072;  // the reference's histogram-request limit (kPfeBins)
+
+template <typename R>
+struct RowSmem {
+  uint32_t hist[kBins];
+  R cand[kCap];
+  double dsum[kRowWarps];
+  R rmin[kRowWarps], rmax[kRowWarps];
+  uint32_t candCount;
+  uint32_t pick[4];
+  double flo[kMaxRounds], finvw[kMaxRounds];
+  uint32_t fb0[kMaxRounds], fb1[kMaxRounds];
+};
+
+__device__ __forceinline__ double blockSum(double v, double* scratch) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kRowWarps; ++w) s += scratch[w];
+  __syncthreads();
+  return s;  // valid in thread 0
+}
+
+template <typename R>
+__device__ __forceinline__ void blockMinMax(R& lo, R& hi, R* smin, R* smax) {
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) smin[warp] = lo, smax[warp] = hi;
+  __syncthreads();
+  lo = smin[0], hi = smax[0];
+  for (int w = 1; w < kRowWarps; ++w) lo = fmin(lo, smin[w]), hi = fmax(hi, smax[w]);
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t binOf(double v, double lo, double invw) {
+  const double f = (v - lo) * invw;
+  const uint32_t b = f <= 0.0 ? 0u : (f >= static_cast<double>(kBins) ? static_cast<uint32_t>(kBins) : static_cast<uint32_t>(f));
+  return min(b, static_cast<uint32_t>(kBins - 1));
+}
+
+template <typename R>
+__device__ __forceinline__ bool passes(const RowSmem<R>& s, int rounds, double v) {
+  for (int r = 0; r < rounds; ++r) {
+    const uint32_t b = binOf(v, s.flo[r], s.finvw[r]);
+    if (b < s.fb0[r] || b > s.fb1[r]) return false;
+  }
+  return true;
+}
+
+// Bitonic sort of n (<= kCap) values in shared memory, padded with +inf to a power of two.
+template <typename R>
+__device__ void bitonicSort(R* a, uint32_t n) {
+  uint32_t m = 1;
+  while (m < n) m <<= 1;
+  for (uint32_t i = n + threadIdx.x; i < m; i += kRowThreads) a[i] = R(INFINITY);
+  __syncthreads();
+  for (uint32_t size = 2; size <= m; size <<= 1)
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t i = threadIdx.x; i < m; i += kRowThreads) {
+        const uint32_t partner = i ^ stride;
+        if (partner > i) {
+          const bool up = (i & size) == 0;
+          const R ai = a[i], ap = a[partner];
+          if ((ai > ap) == up) a[i] = ap, a[partner] = ai;
+        }
+      }
+      __syncthreads();
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  RowSmem<R>& s = *reinterpret_cast<RowSmem<R>*>(raw);
+  const RowJob<R> J = jobs[blockIdx.x];
+  const R* rq = J.request;
+  const uint32_t op = static_cast<uint32_t>(rq[0]), row = static_cast<uint32_t>(rq[1]), row2 = static_cast<uint32_t>(rq[2]);
+  const uint32_t count = static_cast<uint32_t>(rq[3]);
+  const size_t outAt = static_cast<size_t>(rq[7]);
+  const uint32_t nP = J.nP, tid = threadIdx.x;
+  const R* X = J.expo + static_cast<size_t>(row) * nP;
+  R* out = J.out + outAt;
+
+  if (op == 4) {  // samples: the first `count` paths
+    for (uint32_t i = tid; i < count && i < nP; i += kRowThreads) out[i] = X[i];
+    return;
+  }
+  if (op != 0 && op != 5 && op != 7) {  // means, in double precision
+    const R* Y = J.expo + static_cast<size_t>(row2) * nP;
+    double acc = 0.0;
+    for (uint32_t i = tid; i < nP; i += kRowThreads) {
+      const R x = X[i];
+      R f = x;
+      switch (op) {
+        case 2: f = fmax(x, R(0)); break;
+        case 3: f = fmin(x, R(0)); break;
+        case 6: f = x * Y[i]; break;
+        case 8: f = fmax(x, R(0)) * Y[i]; break;
+        case 9: f = fmin(x, R(0)) * Y[i]; break;
+        default: break;
+      }
+      acc += static_cast<double>(f);
+    }
+    const double total = blockSum(acc, s.dsum);
+    if (tid == 0) out[0] = static_cast<R>(total / static_cast<double>(nP));
+    return;
+  }
+
+  const bool pos = op == 7;
+  auto val = [&](uint32_t i) -> R { const R x = X[i]; return pos ? fmax(x, R(0)) : x; };
+  R lo = R(INFINITY), hi = R(-INFINITY);
+  for (uint32_t i = tid; i < nP; i += kRowThreads) {
+    const R v = val(i);
+    lo = fmin(lo, v), hi = fmax(hi, v);
+  }
+  blockMinMax(lo, hi, s.rmin, s.rmax);
+
+  if (op == 5) {  // histogram of `count` bins on [lo, hi] (the request's range unless lo == hi there)
+    if (rq[5] != rq[6]) lo = rq[5], hi = rq[6];
+    const R span = fmax(hi - lo, R(1e-30));
+    const uint32_t nb = min(count, static_cast<uint32_t>(kHistBins));
+    for (uint32_t b = tid; b < nb; b += kRowThreads) s.hist[b] = 0;
+    __syncthreads();
+    for (uint32_t i = tid; i < nP; i += kRowThreads) {
+      const R f = fmax((X[i] - lo) / span, R(0)) * static_cast<R>(nb);
+      const uint32_t b = min(f >= R(4294967295.0) ? 0xFFFFFFFFu : static_cast<uint32_t>(f), nb - 1);
+      atomicAdd(&s.hist[b], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = tid; b < nb; b += kRowThreads) out[b] = static_cast<R>(s.hist[b]);
+    if (tid == 0) out[nb] = lo, out[nb + 1] = hi;
+    return;
+  }
+
+  // Exact interpolated quantile (ccr::quantile): ranks k and k1 = min(k + 1, n - 1).
+  const double h = static_cast<double>(rq[4]) * static_cast<double>(nP - 1);
+  const uint32_t k = min(static_cast<uint32_t>(floor(h)), nP - 1), k1 = min(k + 1, nP - 1);
+  const double frac = h - static_cast<double>(k);
+  if (!(lo < hi)) {
+    if (tid == 0) out[0] = lo;
+    return;
+  }
+  uint32_t below = 0;
+  int rounds = 0;
+  R vk = lo, vk1 = lo;
+  bool done = false;
+  while (!done) {
+    if (rounds >= kMaxRounds) {
+      if (tid == 0) atomicExch(err, kDevBadTerm), out[0] = R(NAN);
+      return;
+    }
+    // Range of the current candidates (round 0: the whole row, already known).
+    if (rounds > 0) {
+      lo = R(INFINITY), hi = R(-INFINITY);
+      for (uint32_t i = tid; i < nP; i += kRowThreads) {
+        const R v = val(i);
+        if (passes(s, rounds, static_cast<double>(v))) lo = fmin(lo, v), hi = fmax(hi, v);
+      }
+      blockMinMax(lo, hi, s.rmin, s.rmax);
+      if (!(lo < hi)) {  // every candidate has the same value
+        vk = lo, vk1 = lo;
+        break;
+      }
+    }
+    const double dlo = static_cast<double>(lo), invw = static_cast<double>(kBins) / (static_cast<double>(hi) - dlo);
+    for (uint32_t b = tid; b < kBins; b += kRowThreads) s.hist[b] = 0;
+    __syncthreads();
+    for (uint32_t i = tid; i < nP; i += kRowThreads) {
+      const double v = static_cast<double>(val(i));
+      if (passes(s, rounds, v)) atomicAdd(&s.hist[binOf(v, dlo, invw)], 1u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t cum = below, b0 = kBins - 1, b1 = kBins - 1, below0 = below;
+      bool f0 = false;
+      for (uint32_t b = 0; b < kBins; ++b) {
+        const uint32_t c = s.hist[b];
+        if (!f0 && cum + c > k) b0 = b, below0 = cum, f0 = true;
+        if (cum + c > k1) {
+          b1 = b;
+          break;
+        }
+        cum += c;
+      }
+      s.pick[0] = b0, s.pick[1] = b1, s.pick[2] = below0, s.pick[3] = s.hist[b0];
+    }
+    __syncthreads();
+    const uint32_t b0 = s.pick[0], b1 = s.pick[1], below0 = s.pick[2], c0 = s.pick[3];
+    if (b0 != b1) {
+      // k is the largest value of bin b0, k + 1 the smallest of bin b1.
+      R mx = R(-INFINITY), mn = R(INFINITY);
+      for (uint32_t i = tid; i < nP; i += kRowThreads) {
+        const R v = val(i);
+        const double dv = static_cast<double>(v);
+        if (!passes(s, rounds, dv)) continue;
+        const uint32_t b = binOf(dv, dlo, invw);
+        if (b == b0) mx = fmax(mx, v);
+        if (b == b1) mn = fmin(mn, v);
+      }
+      blockMinMax(mn, mx, s.rmin, s.rmax);  // block minimum of mn, block maximum of mx
+      vk = mx, vk1 = mn;
+      done = true;
+    } else if (c0 <= static_cast<uint32_t>(kCap)) {
+      if (tid == 0) s.candCount = 0;
+      __syncthreads();
+      for (uint32_t i = tid; i < nP; i += kRowThreads) {
+        const R v = val(i);
+        const double dv = static_cast<double>(v);
+        if (passes(s, rounds, dv) && binOf(dv, dlo, invw) == b0) s.cand[atomicAdd(&s.candCount, 1u)] = v;
+      }
+      __syncthreads();
+      const uint32_t n = s.candCount;
+      bitonicSort(s.cand, n);
+      vk = s.cand[k - below0];
+      vk1 = s.cand[min(k1 - below0, n - 1)];
+      done = true;
+    } else {
+      if (tid == 0) s.flo[rounds] = dlo, s.finvw[rounds] = invw, s.fb0[rounds] = b0, s.fb1[rounds] = b0;
+      __syncthreads();
+      below = below0;
+      ++rounds;
+    }
+  }
+  if (tid == 0) {
+    const double a = static_cast<double>(vk), b = static_cast<double>(vk1);
+    out[0] = static_cast<R>(a + frac * (b - a));
+  }
+}
+
+template <typename R>
+__global__ void reduceKernel(const ReduceJob<R>* __restrict__ jobs) {
+  const ReduceJob<R> J = jobs[blockIdx.y];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= J.n) return;
+  double sum = 0.0, comp = 0.0;
+  for (uint32_t t = 0; t < J.numTiles; ++t) {
+    const double yv = static_cast<double>(J.partials[static_cast<size_t>(t) * J.n + i]) - comp;
+    const double tv = sum + yv;
+    comp = (tv - sum) - yv;
+    sum = tv;
+  }
+  J.sums[i] = static_cast<R>(sum / static_cast<double>(J.nP));
+}
+
+}  // namespace
+
+template <typename R>
+cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, cudaStream_t stream) {
+  if (numJobs == 0 || maxN == 0) return cudaSuccess;
+  const dim3 grid((maxN + 255) / 256, numJobs);
+  reduceKernel<R><<<grid, 256, 0, stream>>>(jobs);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream) {
+  if (numJobs == 0) return cudaSuccess;
+  const size_t smem = sizeof(RowSmem<R>);
+  cudaError_t e = cudaFuncSetAttribute(rowStatsKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  rowStatsKernel<R><<<numJobs, kRowThreads, smem, stream>>>(jobs, err);
+  return cudaGetLastError();
+}
+
+template cudaError_t launchReduce<float>(const ReduceJob<float>*, uint32_t, uint32_t, cudaStream_t);
+template cudaError_t launchReduce<double>(const ReduceJob<double>*, uint32_t, uint32_t, cudaStream_t);
+template cudaError_t launchRowStats<float>(const RowJob<float>*, uint32_t, uint32_t*, cudaStream_t);
+template cudaError_t launchRowStats<double>(const RowJob<double>*, uint32_t, uint32_t*, cudaStream_t);
+
+}  // namespace zk

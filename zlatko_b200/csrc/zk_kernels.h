@@ -1,0 +1,43 @@
+// Host-visible launchers of the zlatko_b200 kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "zk_device.cuh"
+
+namespace zk {
+
+// Risk factors of every path and date into the factor cube.
+template <typename R>
+cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream);
+
+// Revalue / net / collateralise / reduce: one CTA per (path tile, netting set).
+template <typename R>
+cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
+                          bool perTrade, bool sink, cudaStream_t stream);
+size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64);
+
+// One reduce job per plan: sums[i] = (sum over tiles of partials[tile][i]) / nP for i < n.
+template <typename R>
+struct ReduceJob {
+  const R* partials;
+  R* sums;
+  uint32_t n, numTiles, nP, pad;
+};
+template <typename R>
+cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, cudaStream_t stream);
+
+// One row-statistics job per request (fused_kernels.cpp:565-771): the request record, its plan's rows.
+template <typename R>
+struct RowJob {
+  const R* expo;      // [rows][nP]
+  const R* request;   // 8 words: (op, row, row2, count) (level, lo, hi, out)
+  R* out;             // the plan's values
+  uint32_t nP, pad;
+};
+template <typename R>
+cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream);
+
+}  // namespace zk

@@ -1,0 +1,267 @@
+"""The fused exposure pipeline on a B200, behind the reference's ``ccr::gpu`` interface.
+
+The reference splits the path into ``compile`` (netting set -> FusedPlan), a backend
+``FusedOutput run(const FusedPlan&)`` and ``summarise`` (include/ccr/gpu/fused_exposure.hpp:338-392).
+This module mirrors those three steps over the C ABI:
+
+    plan = compile(model, netting_set, options)        # zk_compile (C++ host compiler)
+    with Context() as ctx:
+        sums, values = ctx.run(plan)                   # zk_run_plan: the CUDA kernels
+    result = summarise(plan, sums, values)             # profiles, CVA increments, survival
+
+``Plan.from_arrays`` wraps the buffers of any reference FusedPlan, so plans compiled by the reference
+itself run unchanged.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import spec as S
+from ._native import BatchInfo, Output, OutputF64, PlanView, PlanViewF64, ZkError, check, lib
+
+STATS_PER_DATE = 8
+H_QUANTILE, H_NUM_REPORTING, H_STATS = 14, 17, 16
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+@dataclass
+class Plan:
+    """The tables of one gpu::FusedPlan, in the reference's binary layout."""
+
+    header: np.ndarray            # uint32[32]
+    indices: np.ndarray           # uint32
+    params: np.ndarray            # float32[84]
+    steps: np.ndarray             # float32[nT * 24]
+    terms: np.ndarray             # float32[numTerms * 8]
+    requests: np.ndarray          # float32[numRequests * 8]
+    rows_total: int
+    num_outputs: int
+    times: np.ndarray             # simulation dates
+    reporting: np.ndarray         # indices of the reporting dates
+    market_survival: Optional[np.ndarray] = None
+    tables64: Optional[Dict[str, np.ndarray]] = None  # double-precision params/steps/terms/requests (zk_compile)
+    exercise_rows: int = 0
+
+    def __post_init__(self):
+        self.header = np.ascontiguousarray(self.header, np.uint32)
+        self.indices = np.ascontiguousarray(self.indices, np.uint32)
+        for k in ("params", "steps", "terms", "requests"):
+            a = np.ascontiguousarray(getattr(self, k), np.float32)
+            setattr(self, k, a if a.size else np.zeros(8, np.float32)[:0])
+        self._keep: List = []
+
+    @property
+    def num_paths(self) -> int:
+        return int(self.header[0])
+
+    @property
+    def num_dates(self) -> int:
+        return int(self.header[1])
+
+    @property
+    def stats_per_date(self) -> int:
+        return int(self.header[H_STATS])
+
+    @property
+    def num_reporting(self) -> int:
+        return int(self.header[H_NUM_REPORTING])
+
+    def sums_len(self) -> int:
+        return self.num_dates * self.stats_per_date
+
+    def values_len(self) -> int:
+        return max(1, self.num_outputs)
+
+    @staticmethod
+    def from_arrays(header, indices, params, steps, terms, requests, rows_total, num_outputs, times, reporting,
+                    market_survival=None) -> "Plan":
+        return Plan(header, indices, params, steps, terms, requests, int(rows_total), int(num_outputs),
+                    np.asarray(times, np.float64), np.asarray(reporting, np.int64), market_survival)
+
+    def view(self) -> PlanView:
+        terms = self.terms if self.terms.size else np.zeros(8, np.float32)
+        reqs = self.requests if self.requests.size else np.zeros(8, np.float32)
+        self._keep = [terms, reqs]
+        return PlanView(_ptr(self.header, C.c_uint32), self.header.size, _ptr(self.indices, C.c_uint32), self.indices.size,
+                        _ptr(self.params, C.c_float), self.params.size, _ptr(self.steps, C.c_float), self.steps.size,
+                        _ptr(terms, C.c_float), self.terms.size, _ptr(reqs, C.c_float), self.requests.size,
+                        self.rows_total, self.num_outputs)
+
+    def view64(self) -> PlanViewF64:
+        if self.tables64 is None:
+            raise ValueError("this plan has no double-precision tables (compile it with zlatko_b200.gpu.compile)")
+        t = self.tables64
+        terms = t["terms"] if t["terms"].size else np.zeros(8)
+        reqs = t["requests"] if t["requests"].size else np.zeros(8)
+        self._keep = [terms, reqs]
+        return PlanViewF64(_ptr(self.header, C.c_uint32), self.header.size, _ptr(self.indices, C.c_uint32), self.indices.size,
+                           _ptr(t["params"], C.c_double), t["params"].size, _ptr(t["steps"], C.c_double), t["steps"].size,
+                           _ptr(terms, C.c_double), t["terms"].size, _ptr(reqs, C.c_double), t["requests"].size,
+                           self.rows_total, self.num_outputs)
+
+
+def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Options] = None) -> Plan:
+    """zk_compile: the host plan compiler (a restatement of gpu::compile, src/gpu/fused_exposure.cpp:214).
+    Raises ValueError where the reference throws std::invalid_argument."""
+    options = options or S.Options()
+    m, n, o = S.encode_model(model), S.encode_netting_set(netting_set), S.encode_options(options)
+    L = lib()
+    h = C.c_void_p()
+    err = C.create_string_buffer(512)
+    st = L.zk_compile(m.ctypes.data, m.size, n.ctypes.data, n.size, o.ctypes.data, o.size, C.byref(h), err, 512)
+    if st != 0:
+        raise ValueError(err.value.decode())
+    try:
+        v, v64 = PlanView(), PlanViewF64()
+        check(L.zk_plan_view_of(h, C.byref(v)))
+        check(L.zk_plan_view_f64_of(h, C.byref(v64)))
+        sizes = (C.c_uint64 * 6)()
+        check(L.zk_plan_sizes(h, sizes))
+        nT, nR = int(sizes[0]), int(sizes[1])
+
+        def arr(p, n, dt):
+            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+
+        times = np.zeros(nT)
+        rep = np.zeros(nR, np.uint64)
+        check(L.zk_plan_dates(h, times.ctypes.data, nT, rep.ctypes.data, nR))
+        plan = Plan(arr(v.header, v.header_len, np.uint32), arr(v.indices, v.indices_len, np.uint32),
+                    arr(v.params, v.params_len, np.float32), arr(v.steps, v.steps_len, np.float32),
+                    arr(v.terms, v.terms_len, np.float32), arr(v.requests, v.requests_len, np.float32),
+                    int(v.rows_total), int(v.num_outputs), times, rep.astype(np.int64))
+        plan.tables64 = {"params": arr(v64.params, v64.params_len, np.float64), "steps": arr(v64.steps, v64.steps_len, np.float64),
+                         "terms": arr(v64.terms, v64.terms_len, np.float64),
+                         "requests": arr(v64.requests, v64.requests_len, np.float64)}
+        plan.exercise_rows = int(sizes[5])
+        if model.credits:
+            from .summary import hazard_survival
+            c = model.credits[options.counterparty]
+            plan.market_survival = np.array([hazard_survival(c.pillars, c.hazards, t) for t in times])
+        else:
+            plan.market_survival = np.ones(nT)
+        return plan
+    finally:
+        L.zk_plan_destroy(h)
+
+
+class Batch:
+    """Plans uploaded once and executed on the device (zk_batch_*): the inputs stay resident in HBM."""
+
+    def __init__(self, ctx: "Context", plans: Sequence[Plan]):
+        self.ctx, self.plans = ctx, list(plans)
+        views = (PlanView * len(self.plans))(*[p.view() for p in self.plans])
+        h = C.c_void_p()
+        check(lib().zk_batch_create(ctx.handle, views, len(self.plans), C.byref(h)), ctx.handle)
+        self.handle = h
+
+    def execute(self) -> None:
+        check(lib().zk_batch_execute(self.handle), self.ctx.handle)
+
+    def timings(self) -> np.ndarray:
+        """Milliseconds of the last execute: simulate, revalue, reduce, row statistics."""
+        ms = (C.c_float * 4)()
+        check(lib().zk_batch_timings(self.handle, ms), self.ctx.handle)
+        return np.array(ms[:], np.float64)
+
+    def info(self) -> BatchInfo:
+        i = BatchInfo()
+        check(lib().zk_batch_info_get(self.handle, C.byref(i)), self.ctx.handle)
+        return i
+
+    def read(self):
+        outs, bufs = self.ctx._outputs(self.plans)
+        check(lib().zk_batch_read(self.handle, outs), self.ctx.handle)
+        return bufs
+
+    def close(self) -> None:
+        if self.handle:
+            lib().zk_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """A zk_context on one GPU.  Calls on one context run in order on its stream."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        h = C.c_void_p()
+        st = lib().zk_context_create(device, C.byref(h))
+        if st != 0:
+            raise ZkError(st, "zk_context_create failed (no CUDA device?)")
+        self.handle = h
+        if stream:
+            check(lib().zk_context_set_stream(h, C.c_void_p(stream)), h)
+
+    def close(self) -> None:
+        if self.handle:
+            lib().zk_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def _outputs(plans: Sequence[Plan], f64: bool = False):
+        T, ct, dt = (OutputF64, C.c_double, np.float64) if f64 else (Output, C.c_float, np.float32)
+        bufs = [(np.zeros(p.sums_len(), dt), np.zeros(p.values_len(), dt)) for p in plans]
+        outs = (T * len(plans))(*[T(_ptr(s, ct), s.size, _ptr(v, ct), v.size) for s, v in bufs])
+        return outs, bufs
+
+    def run(self, plan: Plan):
+        """zk_run_plan: the drop-in for gpu::runFusedReference.  Returns (sums, values) as float32."""
+        return self.run_many([plan])[0]
+
+    def run_many(self, plans: Sequence[Plan]):
+        views = (PlanView * len(plans))(*[p.view() for p in plans])
+        outs, bufs = self._outputs(plans)
+        check(lib().zk_run_plans(self.handle, views, len(plans), outs), self.handle)
+        return bufs
+
+    def amc_states(self, plan: Plan, exercise_rows: int):
+        nT, nP = plan.num_dates, plan.num_paths
+        x = np.zeros(nT * nP, np.float32)
+        d = np.zeros(nT * nP, np.float32)
+        ex = np.zeros(max(exercise_rows, 1) * nP, np.float32)
+        v = plan.view()
+        check(lib().zk_amc_states(self.handle, C.byref(v), x.ctypes.data, d.ctypes.data, ex.ctypes.data, exercise_rows), self.handle)
+        return x.reshape(nT, nP), d.reshape(nT, nP), ex[: exercise_rows * nP].reshape(exercise_rows, nP)
+
+    def run_f64(self, plan: Plan, normals: Optional[np.ndarray] = None, streams: int = 0, rows: bool = False):
+        """FP64 mode (zk_run_plan_f64), optionally on injected normals [step][normal][stream]."""
+        v = plan.view64()
+        outs, bufs = self._outputs([plan], f64=True)
+        z = None if normals is None else np.ascontiguousarray(normals, np.float64)
+        r = np.zeros(plan.rows_total * plan.num_paths) if rows else None
+        check(lib().zk_run_plan_f64(self.handle, C.byref(v), None if z is None else z.ctypes.data, streams, outs,
+                                    None if r is None else r.ctypes.data), self.handle)
+        sums, values = bufs[0]
+        return (sums, values, r.reshape(plan.rows_total, plan.num_paths)) if rows else (sums, values)
+
+    def run_injected(self, plan: Plan, normals: np.ndarray, streams: int, rows: bool = False):
+        """FP32 kernels on injected normals (zk_run_plan_injected)."""
+        v = plan.view()
+        outs, bufs = self._outputs([plan])
+        z = np.ascontiguousarray(normals, np.float64)
+        r = np.zeros(plan.rows_total * plan.num_paths, np.float32) if rows else None
+        check(lib().zk_run_plan_injected(self.handle, C.byref(v), z.ctypes.data, streams, outs,
+                                         None if r is None else r.ctypes.data), self.handle)
+        sums, values = bufs[0]
+        return (sums, values, r.reshape(plan.rows_total, plan.num_paths)) if rows else (sums, values)
+
+    def batch(self, plans: Sequence[Plan]) -> Batch:
+        return Batch(self, plans)
