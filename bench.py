@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--impl", default="zlatko", choices=["zlatko", "reference"])
     ap.add_argument("--paths", type=int, default=100_000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     return ap.parse_args()
 
 
@@ -256,6 +257,8 @@ def main():
     if rank == 0:
         cpu = None
         try:
+            if a.no_cpu:
+                raise RuntimeError("skipped (--no-cpu)")
             cv, cpaths, cthreads, cdt, _ = cpu_reference(plans, trades, a.cpu_seconds / 2)
             cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": "reference",
                    "sample": f"{cpaths} of {nP} paths of all 100 netting sets (gpu::runFusedReference, {cthreads} threads)"}
