@@ -112,6 +112,20 @@ zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const d
 zk_status zk_run_plan_injected(zk_context* ctx, const zk_plan_view* plan, const double* normals, size_t streams,
                                zk_output* out, float* rows);
 
+/* ---- without device allocation (no counterpart in the reference) ----------------------------------- */
+/* For callers that cannot call cudaMalloc: a host that hands all device memory to its own pooling
+ * allocator up front (a serving process, a framework's caching allocator), or a plug-in that runs
+ * inside such a host.  Runs one plan like zk_run_plan (host buffers in and out) but allocates no device
+ * memory and needs no context: every device buffer lives in one fixed array of
+ * ZK_NOALLOC_SCRATCH_BYTES that the library reserves on each GPU where it is loaded and holds until the
+ * process exits.  A plan that needs more scratch is rejected with ZK_ERR_INVALID_ARGUMENT (use
+ * zk_run_plan).  `stream` may be NULL (the legacy default stream).  The first call on a device looks up
+ * the array's device address; make that first call before any stream capture.  Every call reuses the
+ * same array, so calls that overlap on the GPU (on other streams or from other threads) race: the
+ * caller must serialise them.  On failure the message is copied to err (err_len bytes). */
+#define ZK_NOALLOC_SCRATCH_BYTES (32u << 20)
+zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan_view* plan, zk_output* out, char* err, size_t err_len);
+
 /* ---- device-resident batches (inputs uploaded once; used to time the kernels alone) -------------- */
 typedef struct zk_batch zk_batch;
 typedef struct zk_batch_info {

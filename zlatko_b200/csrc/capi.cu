@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -757,3 +758,91 @@ void zk_batch_destroy(zk_batch* b) {
 }
 
 }  // extern "C"
+
+// ================================================================================================
+// Entry point without device allocation.
+//
+// Some callers cannot call cudaMalloc: a host application that hands all device memory to its own
+// pooling allocator up front (a serving process, a framework's caching allocator), or a plug-in that
+// runs inside such a host and is not allowed to allocate behind its back.  zk_run_plan_noalloc runs the
+// same kernels as zk_run_plan for one plan, but every device buffer it needs (the plan tables, the factor
+// cube, the per-tile partials, the path-view rows, the job tables, the error word) lives in the
+// file-scope array below, which the CUDA module reserves when it loads on a device.  It creates no
+// context, stream or event and allocates no device memory; the host builds its upload image in ordinary
+// host memory.
+static __device__ __align__(256) unsigned char zkNoAllocScratch[ZK_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex gNoAllocMutex;
+unsigned char* gNoAllocBase[kNoAllocMaxDevices] = {};
+
+// The device address of zkNoAllocScratch on `device` (current), looked up once per device.  In host code
+// the array's name is only a stand-in; the kernels need this address.
+unsigned char* noAllocBase(int device) {
+  std::lock_guard<std::mutex> lock(gNoAllocMutex);
+  if (!gNoAllocBase[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, zkNoAllocScratch);
+    if (e != cudaSuccess) throw fail(ZK_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch: %s", cudaGetErrorString(e));
+    gNoAllocBase[device] = static_cast<unsigned char*>(p);
+  }
+  return gNoAllocBase[device];
+}
+
+}  // namespace
+
+extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan_view* plan, zk_output* out, char* err,
+                                         size_t err_len) {
+  auto report = [&](const Failure& f) {
+    if (err && err_len) {
+      std::strncpy(err, f.message.c_str(), err_len - 1);
+      err[err_len - 1] = 0;
+    }
+    return f.status;
+  };
+  try {
+    if (!plan || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw fail(ZK_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n || device >= kNoAllocMaxDevices) throw fail(ZK_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    auto B = build<float>(nullptr, {viewOf(*plan)}, false, nullptr, 0);
+    checkOutputs(*B, out, false);
+    const size_t errOff = alignUp(B->totalBytes);
+    if (errOff + 256 > static_cast<size_t>(ZK_NOALLOC_SCRATCH_BYTES))
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "the plan needs %zu bytes of device scratch; zk_run_plan_noalloc has %zu (use zk_run_plan)",
+                 errOff + 256, static_cast<size_t>(ZK_NOALLOC_SCRATCH_BYTES));
+    ZK_CUDA(cudaSetDevice(device));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    B->base = noAllocBase(device);
+    uint32_t* dErr = reinterpret_cast<uint32_t*>(B->base + errOff);
+    fillImage(*B, nullptr, 0);
+    ZK_CUDA(cudaMemcpyAsync(B->base, B->image.data(), B->inputBytes, cudaMemcpyHostToDevice, s));
+    ZK_CUDA(cudaMemsetAsync(dErr, 0, 4, s));  // the array keeps the previous call's contents
+    const uintptr_t base = reinterpret_cast<uintptr_t>(B->base);
+    const auto& L = B->launches.front();
+    ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
+    ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
+                                 L.numTiles, L.stateWordsMax, L.perTrade, false, s));
+    ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, s));
+    ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
+    std::vector<unsigned char> host(B->outBytes);
+    uint32_t devErr = 0;
+    ZK_CUDA(cudaMemcpyAsync(host.data(), B->base + B->outBegin, B->outBytes, cudaMemcpyDeviceToHost, s));
+    ZK_CUDA(cudaMemcpyAsync(&devErr, dErr, 4, cudaMemcpyDeviceToHost, s));
+    ZK_CUDA(cudaStreamSynchronize(s));
+    if (devErr != 0) throw fail(ZK_ERR_CUDA, "a kernel reported error %u", devErr);
+    const auto& P = B->plans[0];
+    const auto& D = B->dev[0];
+    const float* sums = reinterpret_cast<const float*>(host.data() + (D.sums - B->outBegin));
+    const float* vals = reinterpret_cast<const float*>(host.data() + (D.values - B->outBegin));
+    std::memcpy(out->sums, sums, static_cast<size_t>(P.nT) * P.nS * sizeof(float));
+    std::memcpy(out->values, vals, std::max<uint32_t>(P.v.num_outputs, 1) * sizeof(float));
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return report(f);
+  } catch (const std::exception& e) {
+    return report(fail(ZK_ERR_CUDA, "%s", e.what()));
+  }
+}

@@ -265,3 +265,19 @@ class Context:
 
     def batch(self, plans: Sequence[Plan]) -> Batch:
         return Batch(self, plans)
+
+
+NOALLOC_SCRATCH_BYTES = 32 << 20  # ZK_NOALLOC_SCRATCH_BYTES
+
+
+def run_plan_noalloc(plan: Plan, device: int = 0, stream: Optional[int] = None):
+    """zk_run_plan_noalloc: one plan without any device allocation (all scratch in the library's fixed
+    per-device array of NOALLOC_SCRATCH_BYTES).  For callers that may not call cudaMalloc.  Returns
+    (sums, values); raises ZkError for plans that need more scratch than the array holds."""
+    v = plan.view()
+    outs, bufs = Context._outputs([plan])
+    err = C.create_string_buffer(512)
+    st = lib().zk_run_plan_noalloc(device, C.c_void_p(stream) if stream else None, C.byref(v), outs, err, 512)
+    if st != 0:
+        raise ZkError(st, err.value.decode())
+    return bufs[0]
