@@ -60,7 +60,7 @@ def peaks():
 
 def traffic_per_launch(paths: int):
     """DRAM bytes of one fused-kernel launch from the committed ncu summary, scaled by paths."""
-    path = os.path.join(ROOT, "profiles", "fused_exposure_book100.txt")
+    path = os.path.join(ROOT, "profiles", "revalue_book100.txt")
     if not os.path.exists(path):
         return None
     ref_paths, ref_bytes = None, None
@@ -240,7 +240,8 @@ def main():
     fused_s = float(np.mean(fused_ms)) / 1e3
     nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
     cube_bytes = (2 + nA + nC) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
-    alg_bytes = sum(p.rows_total * nP * 4 + ((nP + 127) // 128) * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
+    tiles = (nP + int(info.tile_paths) - 1) // int(info.tile_paths)
+    alg_bytes = sum(p.rows_total * nP * 4 + tiles * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
     ex2 = C_ex2 = None
     try:
         import ctypes as C
@@ -274,6 +275,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(info.kernels_per_execute) * a.steps,
+            "tile_paths": int(info.tile_paths),
             "kernel_ms": {"simulate": float(np.mean(sim_ms)), "revalue": float(np.mean(fused_ms)), "reduce": float(np.mean(reduce_ms)),
                           "row_stats": float(np.mean(rows_ms))},
             "roofline": {"bound": "hbm", "achieved": alg_bytes / fused_s / 1e9, "peak": peak, "unit": "GB/s",

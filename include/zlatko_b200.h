@@ -136,8 +136,10 @@ typedef struct zk_batch_info {
   uint64_t table_bytes;          /* bytes of plan tables on the device                            */
   uint64_t row_bytes;            /* bytes of per-path rows (PFE inputs) written per execute        */
   uint64_t kernels_per_execute;  /* kernel launches of one zk_batch_execute                         */
+  uint64_t tile_paths;           /* paths per revalue CTA, chosen by the autotuner at creation     */
 } zk_batch_info;
 
+/* Uploads the plans and autotunes the tile shape (paths per revalue CTA) on them: a few executes. */
 zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out);
 zk_status zk_batch_execute(zk_batch* b);
 /* Milliseconds of the last execute by kernel: [0] risk-factor simulation, [1] revalue / net /

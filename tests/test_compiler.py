@@ -57,11 +57,29 @@ def test_bermudan_tables(physical):
           skip_amc=True)
 
 
-def test_two_schedule_swaps_and_merging():
-    m = gpu_model(200)
+@pytest.mark.parametrize("csa", [False, True])
+def test_two_schedule_swaps_value_like_the_reference_decomposition(csa):
+    """A swap with annual fixed and semiannual floating legs compiles natively (one running coupon); the
+    reference has one schedule per swap and represents it as float(K=0) + [swap(K) - swap(0)] on the fixed
+    schedule.  The reference's own CPU kernels run both plans on the same normals: same statistics."""
+    m = gpu_model(512)
     m.base_grid = [k / 12 for k in range(1, 61)]
-    ns = swap_book(9)
-    _same(_ref_plan(m, ns, S.Options(pfe_quantile=0.975)), gpu.compile(m, ns, S.Options(pfe_quantile=0.975)))
+    ns = swap_book(9, csa=S.Csa(1e5, 1e5, 1e4) if csa else None)
+    o = S.Options(pfe_quantile=0.975)
+    r = _ref_plan(m, ns, o)
+    p = gpu.compile(m, ns, o)
+    assert p.terms.size < r.terms.size  # fewer terms: one floating leg instead of three
+    assert np.array_equal(r.times, p.times) and r.header[16] == p.header[16]
+    mine = ref.plan_from_buffers(p.header, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
+                                 p.num_outputs, p.times, p.reporting)
+    s1, v1 = ref.run_fused(r)
+    s2, v2 = ref.run_fused(mine)
+    nS = int(p.header[16])
+    a, b = s1.reshape(-1, nS).astype(np.float64), s2.reshape(-1, nS).astype(np.float64)
+    for k in range(nS):
+        scale = max(np.abs(a[:, k]).max(), 1e-6 * np.abs(a).max(), 1e-30)
+        assert np.abs(a[:, k] - b[:, k]).max() <= 1e-4 * scale, k
+    assert np.abs(v1 - v2).max() <= 1e-4 * np.abs(v1).max()
 
 
 def test_beyond_32_swaps_reuses_slots():

@@ -90,6 +90,9 @@ struct Plan {
   size_t nTerms, nReq, nIdx;
   uint32_t nSlots = 0, ring = 1, ctype = 0, stateWords = 0;
   bool usesAssets = false, probes = false;
+  // The term table lowered for the revalue kernel (lowerTerms).
+  std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot, 0
+  std::vector<R> table;         // records of 4 values
   uint32_t exerciseRows = 0;
   uint32_t bermRows[kMaxBermudans] = {0, 0, 0, 0};
   uint64_t termEvals = 0, expEvals = 0;
@@ -207,7 +210,66 @@ Plan<R> parse(const View<R>& v, size_t index) {
     throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the margin-call look-back spans %u dates (at most %d)", index, maxLag, kMaxRing - 1);
   if (p.ctype == 2) p.usesAssets = true;
   p.stateWords = p.nSlots + (p.hasCsa ? p.ring * (p.ctype != 0 ? 2 : 1) : 0);
+  lowerTerms(p);
   return p;
+}
+
+// Lowers a validated plan's term table for the revalue kernel into typed runs of 4-value records, one
+// contiguous block per date, in the order [floating coupons | bond pairs | generic | fixings]:
+//   floating coupon (kFixedFloat):  (c A, p1 A, b, slot)         value += (c A fix[slot] + p1 A) E(b x)
+//   two bonds (kBond):               (c A, b, c' A', b')          value += c A E(b x) + c' A' E(b' x)
+//   generic (any other kind):        the reference's 8-word record in two 4-value records
+//   fixing (kSetFixing):             (A, b, 1 / c, slot)          fix[slot] = (A E(b x) - 1) / c
+// with b = -B log2 e and E = 2^ in single precision, b = -B and E = exp in double.  Fixings stay last, so a
+// running coupon still reads the previous fixing on its fixing date (the reference's merge order).  In
+// per-trade mode every term keeps its trade group in the generic run.  The date descriptor also carries
+// the margin-call index and the reporting slot: the kernel reads one 32-byte record per date.
+template <typename R>
+void lowerTerms(Plan<R>& p) {
+  const uint32_t* I = p.v.indices;
+  const bool typed = p.nTr == 0;
+  const double bScale = sizeof(R) == 4 ? 1.4426950408889634 : 1.0;
+  p.dates.assign(static_cast<size_t>(p.nT) * 8, 0u);
+  p.table.clear();
+  auto units = [&] { return static_cast<uint32_t>(p.table.size() / 4); };
+  auto push4 = [&](double a, double b, double c, double d) {
+    p.table.push_back(static_cast<R>(a)), p.table.push_back(static_cast<R>(b));
+    p.table.push_back(static_cast<R>(c)), p.table.push_back(static_cast<R>(d));
+  };
+  for (uint32_t j = 0; j < p.nT; ++j) {
+    uint32_t* d = &p.dates[static_cast<size_t>(j) * 8];
+    const R* first = p.v.terms + static_cast<size_t>(I[j]) * kTermStride;
+    const R* last = p.v.terms + static_cast<size_t>(I[j + 1]) * kTermStride;
+    auto isFloat = [&](const R* r) { return typed && r[0] == R(kFixedFloat); };
+    auto isBond = [&](const R* r) { return typed && r[0] == R(kBond); };
+    auto isFixing = [&](const R* r) { return typed && r[0] == R(kSetFixing); };
+    d[0] = units();
+    for (const R* r = first; r < last; r += kTermStride)
+      if (isFloat(r)) {
+        const double A = r[3];
+        push4(static_cast<double>(r[2]) * A, static_cast<double>(r[5]) * A, -static_cast<double>(r[4]) * bScale, r[1]);
+      }
+    d[1] = units();
+    double pending[2] = {0, 0};
+    bool half = false;
+    for (const R* r = first; r < last; r += kTermStride)
+      if (isBond(r)) {
+        const double cA = static_cast<double>(r[2]) * static_cast<double>(r[3]), b = -static_cast<double>(r[4]) * bScale;
+        if (!half) pending[0] = cA, pending[1] = b, half = true;
+        else push4(pending[0], pending[1], cA, b), half = false;
+      }
+    if (half) push4(pending[0], pending[1], 0.0, 0.0);  // the odd bond with a zero partner
+    d[2] = units();
+    for (const R* r = first; r < last; r += kTermStride)
+      if (!isFloat(r) && !isBond(r) && !isFixing(r)) p.table.insert(p.table.end(), r, r + kTermStride);
+    d[3] = units();
+    for (const R* r = first; r < last; r += kTermStride)
+      if (isFixing(r)) push4(r[3], -static_cast<double>(r[4]) * bScale, 1.0 / static_cast<double>(r[2]), r[1]);
+    d[4] = units();
+    d[5] = I[p.offCall + j];
+    d[6] = I[p.offRep + j];
+  }
+  if (p.table.empty()) p.table.assign(4, R(0));
 }
 
 // Plans share a scenario when every input of the risk-factor simulation is identical.
@@ -226,6 +288,11 @@ bool sameScenario(const Plan<R>& a, const Plan<R>& b) {
 
 size_t alignUp(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+uint32_t numTilesOf(uint32_t nP, int ppt) {
+  const uint32_t tp = static_cast<uint32_t>(kTile * ppt);
+  return (nP + tp - 1) / tp;
+}
+
 // A set of plans laid out in one device arena, ready to execute.
 template <typename R>
 struct Batch {
@@ -235,7 +302,7 @@ struct Batch {
     ScenarioArgs<R> sc;
     CubeArgs<R> cb;
     std::vector<uint32_t> planIdx;
-    uint32_t numTiles = 0, numFields = 0;
+    uint32_t numFields = 0;
     size_t stateWordsMax = 0;
     bool perTrade = false, probes = false;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
@@ -243,12 +310,14 @@ struct Batch {
   std::vector<Launch> launches;
   // device offsets per plan
   struct Dev {
-    size_t idx, terms, steps, req, expo, partials, sums, values;
+    size_t dates, table, steps, req, expo, partials, sums, values;
   };
   std::vector<Dev> dev;
   size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
   size_t inputBytes = 0, totalBytes = 0, outBegin = 0, outBytes = 0;
   uint32_t numRowJobs = 0, maxReduceN = 0;
+  int ppt = 2;                        // paths per revalue thread: the tile shape (autotuned by zk_batch_create)
+  std::vector<ReduceJob<R>> reduceJobs;  // host copy; numTiles follows ppt
   std::vector<unsigned char> image;  // host image of the input region
   unsigned char* base = nullptr;     // device arena
   bool ownsArena = false;
@@ -295,7 +364,6 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
       L.probes = L.probes || P.probes;
     }
     const Plan<R>& P0 = B->plans[L.planIdx.front()];
-    L.numTiles = (P0.nP + kTile - 1) / kTile;
     ScenarioArgs<R>& sc = L.sc;
     sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
     sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
@@ -308,7 +376,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fLnS = 2 + P0.nA + P0.nC, cb.fY = 2 + 2 * P0.nA + P0.nC;
     cb.probes = L.probes ? 1u : 0u;
     L.numFields = L.probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC;
-    if (revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8) > 200 * 1024)
+    if (revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8, 1) > 200 * 1024)
       throw fail(ZK_ERR_UNSUPPORTED, "a netting set needs more shared memory than a CTA has");
   }
   if (normals) {
@@ -323,8 +391,8 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   for (size_t i = 0; i < nPlans; ++i) {
     const auto& P = B->plans[i];
     auto& D = B->dev[i];
-    D.idx = take(P.nIdx * 4);
-    D.terms = take(P.nTerms * kTermStride * sizeof(R));
+    D.dates = take(P.dates.size() * 4);
+    D.table = take(P.table.size() * sizeof(R));
     D.steps = take(static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
     D.req = take(P.nReq * kRequestStride * sizeof(R));
   }
@@ -346,7 +414,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
   for (size_t i = 0; i < nPlans; ++i) {
     const auto& P = B->plans[i];
-    const uint32_t tiles = (P.nP + kTile - 1) / kTile;
+    const uint32_t tiles = (P.nP + kTile - 1) / kTile;  // the most tiles any tile shape uses
     B->dev[i].expo = take(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
     B->dev[i].partials = take(static_cast<size_t>(tiles) * P.nT * P.nS * sizeof(R));
   }
@@ -377,8 +445,8 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
   for (size_t i = 0; i < B.plans.size(); ++i) {
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    std::memcpy(img + D.idx, P.v.indices, P.nIdx * 4);
-    if (P.nTerms) std::memcpy(img + D.terms, P.v.terms, P.nTerms * kTermStride * sizeof(R));
+    std::memcpy(img + D.dates, P.dates.data(), P.dates.size() * 4);
+    std::memcpy(img + D.table, P.table.data(), P.table.size() * sizeof(R));
     std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
     if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
   }
@@ -389,8 +457,8 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
       const auto& D = B.dev[L.planIdx[k]];
       NsArgs<R>& A = args[k];
       std::memset(&A, 0, sizeof A);
-      A.idx = static_cast<const uint32_t*>(dptr(D.idx));
-      A.terms = static_cast<const R*>(dptr(D.terms));
+      A.dates = static_cast<const uint32_t*>(dptr(D.dates));
+      A.table = static_cast<const R*>(dptr(D.table));
       A.steps = static_cast<const R*>(dptr(D.steps));
       A.expo = static_cast<R*>(dptr(D.expo));
       A.partials = static_cast<R*>(dptr(D.partials));
@@ -425,13 +493,14 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
   for (size_t i = 0; i < B.plans.size(); ++i) {
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, (P.nP + kTile - 1) / kTile, P.nP, 0};
+    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, B.ppt), P.nP, 0};
     B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
     for (size_t q = 0; q < P.nReq; ++q)
       rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),
                       static_cast<R*>(dptr(D.values)), P.nP, 0});
   }
   std::memcpy(img + B.reduceOff, red.data(), red.size() * sizeof(ReduceJob<R>));
+  B.reduceJobs = red;
   if (!rows.empty()) std::memcpy(img + B.rowOff, rows.data(), rows.size() * sizeof(RowJob<R>));
   if (B.sink) {
     uint32_t offs[kMaxBermudans], acc = 0;
@@ -480,7 +549,7 @@ void execute(Batch<R>& B) {
   ZK_CUDA(cudaEventRecord(B.ev[1], s));
   for (auto& L : B.launches)
     ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                             L.numTiles, L.stateWordsMax, L.perTrade, B.sink, s));
+                             numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, B.ppt, s));
   ZK_CUDA(cudaEventRecord(B.ev[2], s));
   if (!B.sink) {
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
@@ -537,6 +606,42 @@ void checkOutputs(const Batch<R>& B, const void* outs, bool f64) {
     if (f64) checkOutput(static_cast<const zk_output_f64*>(outs) + i, nS, nV, i);
     else checkOutput(static_cast<const zk_output*>(outs) + i, nS, nV, i);
   }
+}
+
+// The tile shape: paths per revalue thread (kTile * ppt paths per CTA).  The per-tile partials are laid
+// out for the smallest tile, so any shape fits; the reduce jobs follow the tile count.
+template <typename R>
+void setTileShape(Batch<R>& B, int ppt) {
+  B.ppt = ppt;
+  for (size_t i = 0; i < B.plans.size(); ++i) B.reduceJobs[i].numTiles = numTilesOf(B.plans[i].nP, ppt);
+  ZK_CUDA(cudaMemcpyAsync(B.base + B.reduceOff, B.reduceJobs.data(), B.reduceJobs.size() * sizeof(ReduceJob<R>),
+                          cudaMemcpyHostToDevice, B.ctx->stream));
+  ZK_CUDA(cudaStreamSynchronize(B.ctx->stream));
+}
+
+// Autotuner: times the revalue kernel of this batch once per candidate tile shape (after a warm-up
+// run) with CUDA events and keeps the fastest.  Shapes whose shared memory does not fit are skipped.
+template <typename R>
+void autotune(Batch<R>& B) {
+  const int candidates[3] = {1, 2, 4};
+  const int count = sizeof(R) == 8 ? 2 : 3;
+  float best = 0.0f;
+  int bestPpt = B.ppt;
+  for (int c = 0; c < count; ++c) {
+    const int ppt = candidates[c];
+    bool fits = true;
+    for (const auto& L : B.launches)
+      fits = fits && revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8, ppt) <= 200 * 1024;
+    if (!fits) continue;
+    setTileShape(B, ppt);
+    execute(B);
+    finish(B);
+    execute(B);
+    finish(B);
+    if (bestPpt == B.ppt && best == 0.0f) best = B.ms[1], bestPpt = ppt;
+    if (B.ms[1] < best) best = B.ms[1], bestPpt = ppt;
+  }
+  setTileShape(B, bestPpt);
 }
 
 void requireCtx(zk_context* ctx) {
@@ -687,6 +792,7 @@ zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, 
     b->b = build<float>(ctx, views, false, nullptr, 0);
     upload(*b->b, ctx, false, nullptr, 0);
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    autotune(*b->b);
     *out = b.release();
     return ZK_OK;
   } catch (const Failure& f) {
@@ -745,6 +851,7 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
     info->row_bytes += static_cast<uint64_t>(P.nR) * P.nP * 4;
   }
   info->kernels_per_execute = 2 * B.launches.size() + 2;
+  info->tile_paths = static_cast<uint64_t>(kTile) * B.ppt;
   return ZK_OK;
 }
 
@@ -824,7 +931,7 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     const auto& L = B->launches.front();
     ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
     ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                                 L.numTiles, L.stateWordsMax, L.perTrade, false, s));
+                                 numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, B->ppt, s));
     ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, s));
     ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
     std::vector<unsigned char> host(B->outBytes);

@@ -205,185 +205,360 @@ __global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, 
 }
 
 // ---------------------------------------------------------------------------------------------
-template <typename R, bool kPerTrade, bool kSink>
+// The exponential of a lowered term: 2^(b x) with b = -B log2 e in single precision, e^(b x) with b = -B
+// in double (lowerTerms, capi.cu).
+__device__ __forceinline__ float termExp(float b, float x) { return ex2(b * x); }
+__device__ __forceinline__ double termExp(double b, double x) { return exp(b * x); }
+
+template <typename R> struct Vec4;
+template <> struct Vec4<float> { using T = float4; };
+template <> struct Vec4<double> { using T = double4; };
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ double4 ld4(const double* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Prefetches into L1 the 128-byte lines of one date's lowered terms, one line per thread of the CTA:
+// the next date's block arrives while the current date computes.
+__device__ __forceinline__ void prefetchL1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(__cvta_generic_to_global(p)));
+}
+template <typename R>
+__device__ __forceinline__ void prefetchDate(uint32_t begin, uint32_t end, const R* table, uint32_t tid) {
+  const size_t b = static_cast<size_t>(begin) * 4 * sizeof(R), e = static_cast<size_t>(end) * 4 * sizeof(R);
+  const uint32_t lines = e > b ? static_cast<uint32_t>((e - 1) / 128 - b / 128 + 1) : 0u;
+  if (tid < lines) prefetchL1(reinterpret_cast<const char*>(table) + (b / 128 + tid) * 128);
+}
+
+template <typename R, int PPT>
+__device__ __forceinline__ R pick4(const R (&a)[4][PPT], uint32_t k, int i) {
+  return k == 0 ? a[0][i] : k == 1 ? a[1][i] : k == 2 ? a[2][i] : a[3][i];
+}
+
+// Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
+// statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
+template <typename R, int PPT, bool kPerTrade, bool kSink>
 __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
-  R* red = reinterpret_cast<R*>(smemRaw);               // [2][kWarps][8]
-  R* vtBuf = red + 2 * kWarps * 8;                      // [16][kTile] per-trade values (per-trade mode)
-  R* state = vtBuf + (kPerTrade ? kMaxTradeGroups * kTile : 0);  // fixings [nSlots][kTile] | ring [ring (x2)][kTile]
+  __shared__ NsArgs<R> sA;
+  R* red = reinterpret_cast<R*>(smemRaw);                          // [2][kWarps][8]
+  R* vtBuf = red + 2 * kWarps * 8;                                 // [16][PPT][kTile] per-trade values
+  R* state = vtBuf + (kPerTrade ? kMaxTradeGroups * PPT * kTile : 0);  // fixings [nSlots][PPT][kTile] | ring
 
   const uint32_t n = blockIdx.x % numNs, tile = blockIdx.x / numNs;
-  const NsArgs<R>& A = nsArgs[n];
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  if (tid == 0) sA = nsArgs[n];
+  __syncthreads();
+  const NsArgs<R>& A = sA;  // read from shared memory: no global reloads after the stores below
+  const uint4* __restrict__ dates = reinterpret_cast<const uint4*>(A.dates);
+  const R* __restrict__ table = A.table;
+  R* __restrict__ expo = A.expo;
   const uint32_t nP = cb.nP, nT = cb.nT;
-  const uint32_t p = tile * kTile + tid;
-  const bool active = p < nP;
-  const uint32_t pp = active ? p : nP - 1;  // threads past the last path read a valid path and contribute nothing
-  R* fix = state + tid;
-  R* ring = state + A.nSlots * kTile + tid;
-  for (uint32_t s = 0; s < A.nSlots; ++s) fix[s * kTile] = R(0);
+  const uint32_t nSlots = A.nSlots, ringLen = A.ring, nS = A.nS, ctype = A.ctype;
+  const bool hasCsa = A.hasCsa != 0, usesAssets = A.usesAssets != 0;
+  uint32_t pth[PPT], pp[PPT];
+  bool act[PPT];
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    pth[i] = tile * (kTile * PPT) + i * kTile + tid;
+    act[i] = pth[i] < nP;
+    pp[i] = act[i] ? pth[i] : nP - 1;  // threads past the last path read a valid path and contribute nothing
+  }
+  auto fix = [&](uint32_t slot, int i) -> R& { return state[(slot * PPT + i) * kTile + tid]; };
+  auto ring = [&](uint32_t r, int i) -> R& { return state[((nSlots + r) * PPT + i) * kTile + tid]; };
+  auto vt = [&](uint32_t g, int i) -> R& { return vtBuf[(g * PPT + i) * kTile + tid]; };
+  for (uint32_t s = 0; s < nSlots; ++s)
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) fix(s, i) = R(0);
   const uint32_t nTr = kPerTrade ? min(A.nTr, static_cast<uint32_t>(kMaxTradeGroups)) : 0u;
   const uint32_t fQ = A.cpty < cb.nC ? cb.fQ + A.cpty : 0xFFFFFFFFu;
+  auto cube = [&](uint32_t field, uint32_t j, int i) { return cb.data[(static_cast<size_t>(field) * nT + j) * nP + pp[i]]; };
 
-  R held = R(0), prevDE = R(0), prevQ = R(1), prevRV = R(0);
-  R ex[4] = {R(-1), R(-1), R(-1), R(-1)};  // exercise index of each Bermudan, -1 if not exercised
+  R held[PPT], prevDE[PPT], prevQ[PPT], prevRV[PPT], ex[4][PPT];
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    held[i] = R(0), prevDE[i] = R(0), prevQ[i] = R(1), prevRV[i] = R(0);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) ex[b][i] = R(-1);  // exercise index of each Bermudan, -1 if not exercised
+  }
   uint32_t redBuf = 0;
-  auto cube = [&](uint32_t field, uint32_t j) { return cb.data[(static_cast<size_t>(field) * nT + j) * nP + pp]; };
+
+  // Software pipeline: the factors and the date descriptor of date j + 1 load while date j computes.
+  R nx[PPT], nD[PPT], nQ[PPT], nS4[4][PPT];
+  auto loadFactors = [&](uint32_t j) {
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      nx[i] = cube(0, j, i), nD[i] = cube(1, j, i), nQ[i] = fQ != 0xFFFFFFFFu ? cube(fQ, j, i) : R(1);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) nS4[a][i] = usesAssets && static_cast<uint32_t>(a) < cb.nA ? cube(cb.fS + a, j, i) : R(0);
+    }
+  };
+  loadFactors(0);
+  uint4 nd0 = __ldg(dates), nd1 = __ldg(dates + 1);
+  // The block of the date after next is prefetched one date ahead of use.
+  uint32_t fBeg = nT > 1 ? __ldg(A.dates + 8) : 0u, fEnd = nT > 1 ? __ldg(A.dates + 12) : 0u;
+  prefetchDate<R>(nd0.x, nd1.x, table, tid);
 
   for (uint32_t j = 0; j < nT; ++j) {
-    const R x = cube(0, j), D = cube(1, j);
-    R S[4] = {R(0), R(0), R(0), R(0)};
-    if (A.usesAssets)
+    R x[PPT], D[PPT], Q[PPT], S[4][PPT];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
-        if (static_cast<uint32_t>(a) < cb.nA) S[a] = cube(cb.fS + a, j);
-    const R Q = fQ != 0xFFFFFFFFu ? cube(fQ, j) : R(1);
-    if (kSink && n == 0 && active) {
-      A.sinkX[static_cast<size_t>(j) * nP + p] = static_cast<float>(x);
-      A.sinkD[static_cast<size_t>(j) * nP + p] = static_cast<float>(D);
+    for (int i = 0; i < PPT; ++i) {
+      x[i] = nx[i], D[i] = nD[i], Q[i] = nQ[i];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) S[a][i] = nS4[a][i];
     }
+    const uint4 d0 = nd0, d1 = nd1;
+    if (j + 1 < nT) {
+      loadFactors(j + 1);
+      nd0 = __ldg(dates + 2 * (j + 1)), nd1 = __ldg(dates + 2 * (j + 1) + 1);
+      prefetchDate<R>(fBeg, fEnd, table, tid);
+      if (j + 2 < nT) {
+        fBeg = __ldg(A.dates + 8 * (j + 2)), fEnd = __ldg(A.dates + 8 * (j + 2) + 4);
+      }
+    }
+    if (kSink && n == 0)
+#pragma unroll
+      for (int i = 0; i < PPT; ++i)
+        if (act[i]) {
+          A.sinkX[static_cast<size_t>(j) * nP + pth[i]] = static_cast<float>(x[i]);
+          A.sinkD[static_cast<size_t>(j) * nP + pth[i]] = static_cast<float>(D[i]);
+        }
 
-    R value = R(0);
-    R ev[4] = {R(0), R(0), R(0), R(0)};
+    R value[PPT], ev[4][PPT];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      value[i] = R(0);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) ev[b][i] = R(0);
+    }
+    using R4 = typename Vec4<R>::T;
+    for (uint32_t u = d0.x; u < d0.y; ++u) {  // running floating coupons
+      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+      const uint32_t slot = static_cast<uint32_t>(r.w);
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) value[i] += (r.x * fix(slot, i) + r.y) * termExp(r.z, x[i]);
+    }
+#pragma unroll 2
+    for (uint32_t u = d0.y; u < d0.z; ++u) {  // bonds, two per record
+      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) value[i] += r.x * termExp(r.y, x[i]) + r.z * termExp(r.w, x[i]);
+    }
     if (kPerTrade && A.nTr > 0)
-      for (uint32_t i = 0; i < kMaxTradeGroups; ++i) vtBuf[i * kTile + tid] = R(0);
-    const uint32_t tBegin = __ldg(A.idx + j), tEnd = __ldg(A.idx + j + 1);
-    for (uint32_t t = tBegin; t < tEnd; ++t) {
+      for (uint32_t g = 0; g < kMaxTradeGroups; ++g)
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) vt(g, i) = R(0);
+    for (uint32_t u = d0.z; u < d0.w; u += 2) {  // generic terms: the reference's records
       R rec[8];
-      loadTerm(A.terms + static_cast<size_t>(t) * kTermStride, rec);
+      loadTerm(table + static_cast<size_t>(u) * 4, rec);
       const uint32_t code = static_cast<uint32_t>(rec[0]);
       const uint32_t kind = code & 15u, bm = min((code >> 8u) & 15u, 3u), extra = code >> 12u;
       const uint32_t slot = static_cast<uint32_t>(rec[1]);
-      const R c = rec[2];
-      R term = R(0);
+      const uint32_t grp = min((code >> 4u) & 15u, 15u);
+      const R c = rec[2], nB = -rec[4];
+      R term[PPT];
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) term[i] = R(0);
       switch (kind) {
-        case kBond: term = c * (rec[3] * fastExp(-rec[4] * x)); break;
-        case kFixedFloat: term = (c * fix[slot * kTile] + rec[5]) * (rec[3] * fastExp(-rec[4] * x)); break;
-        case kAsset: term = c * sel4(S, slot & 3u) * rec[3]; break;
-        case kSetFixing: fix[slot * kTile] = (rec[3] * fastExp(-rec[4] * x) - R(1)) / c; break;
-        case kOption: {
-          const R b0 = rec[3] * fastExp(-rec[4] * x), p3 = rec[7];
-          term = c * black(sel4(S, slot & 3u) * rec[5] / b0, rec[6], fabs(p3), b0, p3 > R(0));
+        case kBond:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) term[i] = c * (rec[3] * fastExp(nB * x[i]));
           break;
-        }
-        case kBermExercise: add4(ev, bm, c * (rec[3] * fastExp(-rec[4] * x))); break;
-        case kBermDecide: {
-          const R e = sel4(ev, bm);
-          if (kSink) {
-            if (active) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + p] = static_cast<float>(e);
-          } else if (sel4(ex, bm) < R(0) && e > R(0) && e > amcPoly(rec, x)) {
-            set4(ex, bm, static_cast<R>(extra));
+        case kFixedFloat:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) term[i] = (c * fix(slot, i) + rec[5]) * (rec[3] * fastExp(nB * x[i]));
+          break;
+        case kAsset:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) term[i] = c * pick4<R, PPT>(S, slot & 3u, i) * rec[3];
+          break;
+        case kSetFixing:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) fix(slot, i) = (rec[3] * fastExp(nB * x[i]) - R(1)) / c;
+          break;
+        case kOption: {
+          const R p3 = rec[7];
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R b0 = rec[3] * fastExp(nB * x[i]);
+            term[i] = c * black(pick4<R, PPT>(S, slot & 3u, i) * rec[5] / b0, rec[6], fabs(p3), b0, p3 > R(0));
           }
           break;
         }
+        case kBermExercise:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R v = c * (rec[3] * fastExp(nB * x[i]));
+            if (bm == 0) ev[0][i] += v;
+            else if (bm == 1) ev[1][i] += v;
+            else if (bm == 2) ev[2][i] += v;
+            else ev[3][i] += v;
+          }
+          break;
+        case kBermDecide:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R e = pick4<R, PPT>(ev, bm, i);
+            if (kSink) {
+              if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = static_cast<float>(e);
+            } else if (pick4<R, PPT>(ex, bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
+              const R v = static_cast<R>(extra);
+              if (bm == 0) ex[0][i] = v;
+              else if (bm == 1) ex[1][i] = v;
+              else if (bm == 2) ex[2][i] = v;
+              else ex[3][i] = v;
+            }
+          }
+          break;
         case kBermContinue:
-          if (sel4(ex, bm) < R(0)) term = rec[1] * fmax(amcPoly(rec, x), R(0));
+#pragma unroll
+          for (int i = 0; i < PPT; ++i)
+            if (pick4<R, PPT>(ex, bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
           break;
-        case kBermBond: {
-          const R e = sel4(ex, bm);
-          if (e >= R(0) && e <= static_cast<R>(extra)) term = c * (rec[3] * fastExp(-rec[4] * x));
+        case kBermBond:
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R e = pick4<R, PPT>(ex, bm, i);
+            if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = c * (rec[3] * fastExp(nB * x[i]));
+          }
           break;
-        }
         case kProbe: {
           const uint32_t what = slot & 15u, ix = min(slot >> 4u, 3u), ic = min(ix, 1u);
-          R q;
-          switch (what) {
-            case 0: q = x; break;
-            case 1: q = D; break;
-            case 2: q = sel4(S, ix); break;
-            case 3: q = ix < cb.nA ? cube(cb.fLnS + ix, j) : R(0); break;
-            case 4: q = ic < cb.nC ? cube(cb.fY + ic, j) : R(0); break;
-            case 5: q = ic < cb.nC ? cube(cb.fQ + ic, j) : R(1); break;
-            case 6: q = D * sel4(S, ix); break;
-            default: q = D * (rec[3] * fastExp(-rec[4] * x));
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            R q;
+            switch (what) {
+              case 0: q = x[i]; break;
+              case 1: q = D[i]; break;
+              case 2: q = pick4<R, PPT>(S, ix, i); break;
+              case 3: q = ix < cb.nA ? cube(cb.fLnS + ix, j, i) : R(0); break;
+              case 4: q = ic < cb.nC ? cube(cb.fY + ic, j, i) : R(0); break;
+              case 5: q = ic < cb.nC ? cube(cb.fQ + ic, j, i) : R(1); break;
+              case 6: q = D[i] * pick4<R, PPT>(S, ix, i); break;
+              default: q = D[i] * (rec[3] * fastExp(nB * x[i]));
+            }
+            if (!kSink && act[i]) expo[static_cast<size_t>(static_cast<uint32_t>(rec[5])) * nP + pth[i]] = q + c;
           }
-          if (!kSink && active) A.expo[static_cast<size_t>(static_cast<uint32_t>(rec[5])) * nP + p] = q + c;
           break;
         }
-        default: {  // kBermFloat
-          const R e = sel4(ex, bm);
-          if (e >= R(0) && e <= static_cast<R>(extra)) term = (c * fix[slot * kTile] + rec[5]) * (rec[3] * fastExp(-rec[4] * x));
-        }
+        default:  // kBermFloat
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R e = pick4<R, PPT>(ex, bm, i);
+            if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = (c * fix(slot, i) + rec[5]) * (rec[3] * fastExp(nB * x[i]));
+          }
       }
-      if (kPerTrade && A.nTr > 0) vtBuf[min((code >> 4u) & 15u, 15u) * kTile + tid] += term;
-      else value += term;
+      if (kPerTrade && A.nTr > 0) {
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) vt(grp, i) += term[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) value[i] += term[i];
+      }
     }
-    for (uint32_t i = 0; i < nTr; ++i) value += vtBuf[i * kTile + tid];
+    for (uint32_t u = d0.w; u < d1.x; ++u) {  // fixings, after every use of the previous fixing
+      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+      const uint32_t slot = static_cast<uint32_t>(r.w);
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) fix(slot, i) = (r.x * termExp(r.y, x[i]) - R(1)) * r.z;
+    }
+    for (uint32_t g = 0; g < nTr; ++g)
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) value[i] += vt(g, i);
     if (kSink) continue;
 
     // ---- CSA: collateral called on the value at t - MPR (collateral.cpp:10-47) ----
-    R collateral = R(0);
-    if (A.hasCsa) {
-      R price = R(1);
-      if (A.ctype == 1) price = A.steps[static_cast<size_t>(j) * kStepStride + 22] * rexp(-A.steps[static_cast<size_t>(j) * kStepStride + 23] * x);
-      else if (A.ctype == 2) price = sel4(S, min(A.casset, 3u));
-      ring[(j % A.ring) * kTile] = value;
-      if (A.ctype != 0) ring[(A.ring + j % A.ring) * kTile] = price;
-      const uint32_t callJ = __ldg(A.idx + A.offCall + j);
-      const R vc = callJ != j ? ring[(callJ % A.ring) * kTile] : value;
-      const R pc = callJ != j && A.ctype != 0 ? ring[(A.ring + callJ % A.ring) * kTile] : price;
-      const R keep = A.ctype != 0 ? A.keepHaircut : R(1);
-      R required = R(0);
-      if (vc > A.hc) required += vc - A.hc;
-      if (A.hb >= R(0) && -vc > A.hb) required -= -vc - A.hb;
-      if (j == 0 || fabs(required - held * keep * pc) >= A.mta) held = required / (keep * pc);
-      collateral = held * price + A.ia;
-    }
-    const R e = value - collateral, ep = fmax(e, R(0)), en = fmin(e, R(0));
-    const uint32_t rs = __ldg(A.idx + A.offRep + j);
-    if (active && rs > 0) {
-      const size_t k = rs - 1;
-      R* E = A.expo;
-      E[(A.rowEP + k) * nP + p] = ep;
-      if (A.rowDV != kNoRow) E[(A.rowDV + k) * nP + p] = rs == 1 ? R(0) : fabs(value - prevRV);
-      if (A.rowE != kNoRow) E[(A.rowE + k) * nP + p] = e;
-      if (A.rowV != kNoRow) E[(A.rowV + k) * nP + p] = value;
-      if (A.rowC != kNoRow) E[(A.rowC + k) * nP + p] = collateral;
-      if (A.rowGross != kNoRow) {
-        R gross = R(0);
-        for (uint32_t i = 0; i < nTr; ++i) gross += fmax(vtBuf[i * kTile + tid], R(0));
-        E[(A.rowGross + k) * nP + p] = gross;
-      }
-      if (A.rowTrades != kNoRow)
-        for (uint32_t i = 0; i < nTr; ++i) E[(A.rowTrades + i * A.nR + k) * nP + p] = vtBuf[i * kTile + tid];
-    }
-    if (active && A.rowEx != kNoRow)
-      for (uint32_t i = 0; i < min(A.nBerm, 4u); ++i) A.expo[(A.rowEx + i) * static_cast<size_t>(nP) + p] = sel4(ex, i) < R(0) ? R(-1) : sel4(ex, i);
-    R cvaInc = R(0);
-    if (rs > 0) {
-      prevRV = value;
-      const R de = D * ep;
-      if (j > 0) cvaInc = R(0.5) * (prevDE + de) * (prevQ - Q);
-      prevDE = de;
-      prevQ = Q;
-    }
-
-    // ---- statistics of this date: the netting set's 8, then kTradeStats per trade ----
-    for (uint32_t q = 0; q < A.nS; q += 8) {
-      R v8[8];
-      if (q == 0) {
-        v8[0] = e, v8[1] = ep, v8[2] = en, v8[3] = D * ep, v8[4] = D * en, v8[5] = cvaInc, v8[6] = Q, v8[7] = D;
-      } else {
+    R e[PPT], ep[PPT], en[PPT];
+    const uint32_t callJ = d1.y, rs = d1.z;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint32_t k = q + c - kStatsPerDate, i = k / kTradeStats;
-          v8[c] = (q + c < A.nS && i < nTr) ? tradeStat<R>(k % kTradeStats, vtBuf[i * kTile + tid], value, D) : R(0);
+    for (int i = 0; i < PPT; ++i) {
+      R collateral = R(0);
+      if (hasCsa) {
+        R price = R(1);
+        if (ctype == 1) price = A.steps[static_cast<size_t>(j) * kStepStride + 22] * rexp(-A.steps[static_cast<size_t>(j) * kStepStride + 23] * x[i]);
+        else if (ctype == 2) price = pick4<R, PPT>(S, min(A.casset, 3u), i);
+        ring(j % ringLen, i) = value[i];
+        if (ctype != 0) ring(ringLen + j % ringLen, i) = price;
+        const R vc = callJ != j ? ring(callJ % ringLen, i) : value[i];
+        R required = R(0);
+        if (vc > A.hc) required += vc - A.hc;
+        if (A.hb >= R(0) && -vc > A.hb) required -= -vc - A.hb;
+        if (ctype == 0) {  // cash: one unit is worth one, no division
+          if (j == 0 || fabs(required - held[i]) >= A.mta) held[i] = required;
+          collateral = held[i] + A.ia;
+        } else {
+          const R pc = callJ != j ? ring(ringLen + callJ % ringLen, i) : price;
+          const R keep = A.keepHaircut;
+          if (j == 0 || fabs(required - held[i] * keep * pc) >= A.mta) held[i] = required / (keep * pc);
+          collateral = held[i] * price + A.ia;
         }
       }
-      if (!active) {
+      e[i] = value[i] - collateral, ep[i] = fmax(e[i], R(0)), en[i] = fmin(e[i], R(0));
+      if (act[i] && rs > 0) {
+        const size_t k = rs - 1, pi = pth[i];
+        expo[(A.rowEP + k) * nP + pi] = ep[i];
+        if (A.rowDV != kNoRow) expo[(A.rowDV + k) * nP + pi] = rs == 1 ? R(0) : fabs(value[i] - prevRV[i]);
+        if (A.rowE != kNoRow) expo[(A.rowE + k) * nP + pi] = e[i];
+        if (A.rowV != kNoRow) expo[(A.rowV + k) * nP + pi] = value[i];
+        if (A.rowC != kNoRow) expo[(A.rowC + k) * nP + pi] = collateral;
+        if (A.rowGross != kNoRow) {
+          R gross = R(0);
+          for (uint32_t g = 0; g < nTr; ++g) gross += fmax(vt(g, i), R(0));
+          expo[(A.rowGross + k) * nP + pi] = gross;
+        }
+        if (A.rowTrades != kNoRow)
+          for (uint32_t g = 0; g < nTr; ++g) expo[(A.rowTrades + g * A.nR + k) * nP + pi] = vt(g, i);
+      }
+      if (act[i] && A.rowEx != kNoRow)
+        for (uint32_t b = 0; b < min(A.nBerm, 4u); ++b) {
+          const R v = pick4<R, PPT>(ex, b, i);
+          expo[(A.rowEx + b) * static_cast<size_t>(nP) + pth[i]] = v < R(0) ? R(-1) : v;
+        }
+    }
+    R cvaInc[PPT];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) v8[c] = R(0);
+    for (int i = 0; i < PPT; ++i) {
+      cvaInc[i] = R(0);
+      if (rs > 0) {
+        prevRV[i] = value[i];
+        const R de = D[i] * ep[i];
+        if (j > 0) cvaInc[i] = R(0.5) * (prevDE[i] + de) * (prevQ[i] - Q[i]);
+        prevDE[i] = de;
+        prevQ[i] = Q[i];
+      }
+    }
+
+    // ---- statistics of this date (the thread's PPT paths summed first): the netting set's 8, then
+    // kTradeStats per trade ----
+    for (uint32_t q = 0; q < nS; q += 8) {
+      R v8[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v8[c] = R(0);
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) {
+        if (!act[i]) continue;
+        if (q == 0) {
+          v8[0] += e[i], v8[1] += ep[i], v8[2] += en[i], v8[3] += D[i] * ep[i], v8[4] += D[i] * en[i];
+          v8[5] += cvaInc[i], v8[6] += Q[i], v8[7] += D[i];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const uint32_t k = q + c - kStatsPerDate, g = k / kTradeStats;
+            if (q + c < nS && g < nTr) v8[c] += tradeStat<R>(k % kTradeStats, vt(g, i), value[i], D[i]);
+          }
+        }
       }
       const R s = warpReduceScatter8(v8, lane);
       R* rb = red + redBuf * kWarps * 8;
       if ((lane & 3u) == 0) rb[warp * 8 + statSlotOfLane(lane)] = s;
       __syncthreads();
-      if (tid < 8 && q + tid < A.nS) {
+      if (tid < 8 && q + tid < nS) {
         R sum = R(0);
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) sum += rb[w * 8 + tid];
-        A.partials[(static_cast<size_t>(tile) * nT + j) * A.nS + q + tid] = sum;
+        A.partials[(static_cast<size_t>(tile) * nT + j) * nS + q + tid] = sum;
       }
       redBuf ^= 1u;  // the other buffer next time: one barrier per block of statistics
     }
@@ -398,15 +573,16 @@ cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cud
   return cudaGetLastError();
 }
 
-size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64) {
+size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) {
   const size_t r = f64 ? 8 : 4;
-  return (2 * kWarps * 8 + (perTrade ? kMaxTradeGroups * kTile : 0) + stateWordsMax * kTile) * r;
+  return (2 * kWarps * 8 + (perTrade ? kMaxTradeGroups * ppt * kTile : 0) + stateWordsMax * ppt * kTile) * r;
 }
 
-template <typename R>
-cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, cudaStream_t stream) {
-  const size_t smem = revalueSmemBytes(stateWordsMax, perTrade, sizeof(R) == 8);
+namespace {
+template <typename R, int PPT>
+cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
+                             bool perTrade, bool sink, cudaStream_t stream) {
+  const size_t smem = revalueSmemBytes(stateWordsMax, perTrade, sizeof(R) == 8, PPT);
   const uint64_t blocks = static_cast<uint64_t>(numTiles) * numNs;
   if (blocks == 0) return cudaSuccess;
   if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
@@ -416,16 +592,30 @@ cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32
     kernel<<<static_cast<uint32_t>(blocks), kTile, smem, stream>>>(cb, nsArgs, numNs);
     return cudaGetLastError();
   };
-  if (sink) return go(revalueKernel<R, false, true>);
-  if (perTrade) return go(revalueKernel<R, true, false>);
-  return go(revalueKernel<R, false, false>);
+  if (sink) return go(revalueKernel<R, PPT, false, true>);
+  if (perTrade) return go(revalueKernel<R, PPT, true, false>);
+  return go(revalueKernel<R, PPT, false, false>);
+}
+}  // namespace
+
+template <typename R>
+cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
+                          bool perTrade, bool sink, int ppt, cudaStream_t stream) {
+  switch (ppt) {
+    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
+    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
+    case 4:
+      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
+      return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template cudaError_t launchSimulate<float>(const ScenarioArgs<float>&, const CubeArgs<float>&, cudaStream_t);
 template cudaError_t launchSimulate<double>(const ScenarioArgs<double>&, const CubeArgs<double>&, cudaStream_t);
-template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool,
+template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, int,
                                           cudaStream_t);
-template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool,
+template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool, int,
                                            cudaStream_t);
 
 }  // namespace zk

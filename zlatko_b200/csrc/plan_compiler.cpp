@@ -118,6 +118,11 @@ double Cir::cirSurvival(double t) const {
 std::vector<double> Trade::eventTimes() const {
   switch (kind) {
     case kSwap: return swap.schedule;
+    case kSwapLegs: {
+      std::vector<double> v = swap.schedule;
+      v.insert(v.end(), fixedSchedule.begin(), fixedSchedule.end());
+      return v;
+    }
     case kForward:
     case kOption: return {maturity};
     default: {
@@ -227,18 +232,18 @@ NettingSet decodeNettingSet(const double* a, std::size_t n) {
       t.position = in.d();
       t.degree = in.u();
       if (t.exercise.empty()) throw std::invalid_argument("BermudanSwaption: no exercise dates");
-    } else if (type == 4) {  // two-schedule swap: float(K=0) + fixed leg at K - fixed leg at 0
-      Swap base;
-      base.notional = in.d();
-      base.fixedRate = in.d();
-      base.payFixed = in.d() != 0.0;
-      const std::vector<double> fs = readSeq(in), ls = readSeq(in);
-      Trade f, k1, k0;
-      f.swap = {base.notional, 0.0, base.payFixed, ls};
-      k1.swap = {base.notional, base.fixedRate, base.payFixed, fs};
-      k0.swap = {base.notional, 0.0, !base.payFixed, fs};
-      ns.trades.push_back(f), ns.trades.push_back(k1), ns.trades.push_back(k0);
-      continue;
+    } else if (type == 4) {  // swap with its own fixed and floating schedules
+      t.kind = Trade::kSwapLegs;
+      t.swap.notional = in.d();
+      t.swap.fixedRate = in.d();
+      t.swap.payFixed = in.d() != 0.0;
+      t.fixedSchedule = readSeq(in);
+      t.swap.schedule = readSeq(in);
+      for (const auto* sch : {&t.fixedSchedule, &t.swap.schedule}) {
+        if (sch->size() < 2) throw std::invalid_argument("swap legs: a schedule needs at least two dates");
+        for (std::size_t q = 1; q < sch->size(); ++q)
+          if ((*sch)[q] <= (*sch)[q - 1]) throw std::invalid_argument("swap legs: schedules must be strictly increasing");
+      }
     } else {
       throw std::invalid_argument("netting set: unknown trade type");
     }
@@ -484,6 +489,39 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
             at[j].back().ts = ts, at[j].back().te = te;
             add(j, kBond, 0, -sign * n * k * tau, bondA(t, te), bondB(t, te));
           }
+        }
+      }
+    } else if (tr.kind == Trade::kSwapLegs) {
+      // The floating leg exactly as a swap with a zero fixed rate on its schedule (fixings recovered on the
+      // path, running coupon with one exponential); the fixed leg as one coupon bond per fixed period.  The
+      // value equals the reference's decomposition float(K = 0) + [swap(K) - swap(0)] on the fixed schedule.
+      const double sign = tr.swap.payFixed ? 1.0 : -1.0, n = tr.swap.notional, k = tr.swap.fixedRate;
+      const auto& sch = tr.swap.schedule;
+      const double slot = static_cast<double>(swapSlots++);
+      for (std::size_t i = 1; i < sch.size(); ++i) {
+        const double ts = sch[i - 1], te = sch[i], tau = te - ts;
+        const std::size_t kf = grid.atOrBefore(ts);
+        add(kf, kSetFixing, slot, tau, bondA(grid.t[kf], ts) / bondA(grid.t[kf], te), bondB(grid.t[kf], ts) - bondB(grid.t[kf], te));
+        at[kf].back().ts = ts, at[kf].back().te = te;
+        for (std::size_t j = 0; j < nT; ++j) {
+          const double t = grid.t[j];
+          if (te <= t + 1e-10) continue;
+          if (ts >= t - 1e-10) {
+            add(j, kBond, 0, sign * n, bondA(t, ts), bondB(t, ts));
+            add(j, kBond, 0, -sign * n, bondA(t, te), bondB(t, te));
+          } else {
+            add(j, kFixedFloat, slot, sign * n * tau, bondA(t, te), bondB(t, te));
+            at[j].back().ts = ts, at[j].back().te = te;
+          }
+        }
+      }
+      const auto& fs = tr.fixedSchedule;
+      for (std::size_t i = 1; i < fs.size(); ++i) {
+        const double te = fs[i], tau = te - fs[i - 1];
+        for (std::size_t j = 0; j < nT; ++j) {
+          const double t = grid.t[j];
+          if (te <= t + 1e-10) continue;
+          add(j, kBond, 0, -sign * n * k * tau, bondA(t, te), bondB(t, te));
         }
       }
     } else if (tr.kind == Trade::kForward) {

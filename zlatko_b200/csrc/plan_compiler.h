@@ -66,8 +66,9 @@ struct Swap {
 };
 
 struct Trade {
-  enum Kind { kSwap, kForward, kOption, kBermudan } kind = kSwap;
-  Swap swap;                         // swap, or a Bermudan's underlying
+  enum Kind { kSwap, kForward, kOption, kBermudan, kSwapLegs } kind = kSwap;
+  Swap swap;                         // swap, or a Bermudan's underlying; kSwapLegs: the floating leg's schedule
+  std::vector<double> fixedSchedule; // kSwapLegs: the fixed leg's own schedule
   std::size_t asset = 0;             // forward / option
   double notional = 0, strike = 0, maturity = 0;
   bool call = true;

@@ -9,7 +9,7 @@
 
 namespace zk {
 
-constexpr int kTile = 128;             // paths per CTA of the fused kernel (one path per thread)
+constexpr int kTile = 128;             // threads per CTA of the revalue kernel
 constexpr int kWarps = kTile / 32;
 constexpr int kHeaderWords = 32;
 constexpr int kStepStride = 24;
@@ -70,8 +70,11 @@ struct CubeArgs {
 // ---- one netting set (one plan) inside a launch ----
 template <typename R>
 struct NsArgs {
-  const uint32_t* idx;     // termStart[nT+1] | callIndex[nT] | reportingSlot[nT]
-  const R* terms;          // [numTerms][8]
+  // The plan's term table lowered at upload (lowerTerms in capi.cu): per date a descriptor
+  // {floatBegin, bondBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot, 0} into a table of
+  // 4-value records holding the date's floating coupons, bond pairs, generic 8-word terms and fixings.
+  const uint32_t* dates;   // [nT][8]
+  const R* table;          // [*][4]
   const R* steps;          // this plan's step table (columns 22, 23: collateral bond A, B)
   R* expo;                 // [rowsTotal][nP] rows of the path views
   R* partials;             // [numTiles][nT][nS]
@@ -121,10 +124,17 @@ __device__ __forceinline__ void gauss2(uint32_t stream, uint32_t j, uint32_t k, 
   z1 = r * s;
 }
 
-// Exponentials of the hot term loop.  In single precision the MUFU ex2 unit evaluates
-// 2^(x log2 e) (relative error about 2^-22 for the small arguments of bond terms); double
-// precision uses the correctly rounded-to-1-ulp library exp.
-__device__ __forceinline__ float fastExp(float x) { return exp2f(x * 1.4426950408889634f); }
+// 2^x on the special-function unit (ex2.approx.ftz: relative error about 2^-22).
+__device__ __forceinline__ float ex2(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Exponentials of the hot term loop.  In single precision the special-function unit evaluates
+// 2^(x log2 e) (relative error about 2^-22 for the small arguments of bond terms); double precision
+// uses the library exp (within 1 ulp).
+__device__ __forceinline__ float fastExp(float x) { return ex2(x * 1.4426950408889634f); }
 __device__ __forceinline__ double fastExp(double x) { return exp(x); }
 
 __device__ __forceinline__ float rexp(float x) { return expf(x); }
@@ -139,19 +149,20 @@ __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 // 0.5 erfc(-x / sqrt 2) of the FP64 engine (include/ccr/core/math.hpp:15), its oracle.
 __device__ __forceinline__ float ncdf(float x) {
   const float z = fabsf(x) * 0.70710678f;
-  const float t = 1.0f / (1.0f + 0.3275911f * z);
+  const float t = __fdividef(1.0f, 1.0f + 0.3275911f * z);
   const float poly = ((((1.061405429f * t - 1.453152027f) * t + 1.421413741f) * t - 0.284496736f) * t + 0.254829592f) * t;
-  const float erf = 1.0f - poly * expf(-z * z);
+  const float erf = 1.0f - poly * fastExp(-z * z);
   return x >= 0.0f ? 0.5f * (1.0f + erf) : 0.5f * (1.0f - erf);
 }
 __device__ __forceinline__ double ncdf(double x) { return 0.5 * erfc(-x / 1.4142135623730951); }
 
 // df * Black(F, K, sd), call or put: the reference kernel's guards in single precision
-// (fused_kernels.cpp:209-215), the FP64 engine's in double (math.hpp:24-31).
+// (fused_kernels.cpp:209-215; log, divisions and the erf exponential on the special-function unit),
+// the FP64 engine's in double (math.hpp:24-31).
 __device__ __forceinline__ float black(float F, float K, float sd, float df, bool isCall) {
   const float s = isCall ? 1.0f : -1.0f;
   if (sd <= 1e-7f || F <= 0.0f) return df * fmaxf(s * (F - K), 0.0f);
-  const float d1 = logf(F / K) / sd + 0.5f * sd;
+  const float d1 = __fdividef(__logf(__fdividef(F, K)), sd) + 0.5f * sd;
   const float d2 = d1 - sd;
   return df * s * (F * ncdf(s * d1) - K * ncdf(s * d2));
 }

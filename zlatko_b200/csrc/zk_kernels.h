@@ -13,11 +13,12 @@ namespace zk {
 template <typename R>
 cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream);
 
-// Revalue / net / collateralise / reduce: one CTA per (path tile, netting set).
+// Revalue / net / collateralise / reduce: one CTA per (path tile, netting set); each thread owns `ppt`
+// paths (1, 2 or 4 in single precision, 1 or 2 in double), so a tile holds kTile * ppt paths.
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, cudaStream_t stream);
-size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64);
+                          bool perTrade, bool sink, int ppt, cudaStream_t stream);
+size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt);
 
 // One reduce job per plan: sums[i] = (sum over tiles of partials[tile][i]) / nP for i < n.
 template <typename R>
