@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--paths", type=int, default=100_000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
     return ap.parse_args()
 
 
@@ -198,12 +199,14 @@ def main():
     revals = float(nP) * nT * trades
     ctx = gpu.Context(device)
     batch = ctx.batch(plans)
-    info = batch.info()
+    if a.tile_paths:
+        batch.set_tile_paths(a.tile_paths)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     for _ in range(max(a.warmup, 3)):
-        batch.execute()
+        batch.execute()  # the first execute autotunes the tile shape
     batch.read()
+    info = batch.info()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

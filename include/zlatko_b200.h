@@ -139,9 +139,12 @@ typedef struct zk_batch_info {
   uint64_t tile_paths;           /* paths per revalue CTA, chosen by the autotuner at creation     */
 } zk_batch_info;
 
-/* Uploads the plans and autotunes the tile shape (paths per revalue CTA) on them: a few executes. */
+/* Uploads the plans.  The first zk_batch_execute autotunes the tile shape (paths per revalue CTA) on
+ * them, a few timed runs, unless zk_batch_set_tile_paths pinned one. */
 zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out);
 zk_status zk_batch_execute(zk_batch* b);
+/* Pins the tile shape: paths per revalue CTA, 128 x (1, 2 or 4) in single precision. */
+zk_status zk_batch_set_tile_paths(zk_batch* b, uint64_t tile_paths);
 /* Milliseconds of the last execute by kernel: [0] risk-factor simulation, [1] revalue / net /
  * collateralise / reduce per tile, [2] reduce of the partials, [3] row statistics, measured with CUDA
  * events on the context stream. */

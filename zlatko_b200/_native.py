@@ -65,7 +65,7 @@ class BatchInfo(C.Structure):
 # Every entry point declared in include/zlatko_b200.h.
 EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream",
            "zk_run_plan", "zk_run_plans", "zk_amc_states", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc",
-           "zk_batch_create", "zk_batch_execute", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
+           "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
            "zk_batch_destroy", "zk_peak_ex2", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
            "zk_plan_destroy"]
 
@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         "zk_run_plan_noalloc": (st, [C.c_int, vp, P(PlanView), P(Output), C.c_char_p, sz]),
         "zk_batch_create": (st, [vp, P(PlanView), sz, P(vp)]),
         "zk_batch_execute": (st, [vp]),
+        "zk_batch_set_tile_paths": (st, [vp, C.c_uint64]),
         "zk_batch_timings": (st, [vp, P(C.c_float)]),
         "zk_batch_read": (st, [vp, P(Output)]),
         "zk_batch_info_get": (st, [vp, P(BatchInfo)]),

@@ -91,7 +91,7 @@ struct Plan {
   uint32_t nSlots = 0, ring = 1, ctype = 0, stateWords = 0;
   bool usesAssets = false, probes = false;
   // The term table lowered for the revalue kernel (lowerTerms).
-  std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot, 0
+  std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, assetBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot
   std::vector<R> table;         // records of 4 values
   uint32_t exerciseRows = 0;
   uint32_t bermRows[kMaxBermudans] = {0, 0, 0, 0};
@@ -215,9 +215,10 @@ Plan<R> parse(const View<R>& v, size_t index) {
 }
 
 // Lowers a validated plan's term table for the revalue kernel into typed runs of 4-value records, one
-// contiguous block per date, in the order [floating coupons | bond pairs | generic | fixings]:
+// contiguous block per date, in the order [floating coupons | bond pairs | asset forwards | generic | fixings]:
 //   floating coupon (kFixedFloat):  (c A, p1 A, b, slot)         value += (c A fix[slot] + p1 A) E(b x)
 //   two bonds (kBond):               (c A, b, c' A', b')          value += c A E(b x) + c' A' E(b' x)
+//   asset forward (kAsset):          (c, A, asset, 0)             value += c S[asset] A
 //   generic (any other kind):        the reference's 8-word record in two 4-value records
 //   fixing (kSetFixing):             (A, b, 1 / c, slot)          fix[slot] = (A E(b x) - 1) / c
 // with b = -B log2 e and E = 2^ in single precision, b = -B and E = exp in double.  Fixings stay last, so a
@@ -243,6 +244,7 @@ void lowerTerms(Plan<R>& p) {
     auto isFloat = [&](const R* r) { return typed && r[0] == R(kFixedFloat); };
     auto isBond = [&](const R* r) { return typed && r[0] == R(kBond); };
     auto isFixing = [&](const R* r) { return typed && r[0] == R(kSetFixing); };
+    auto isAsset = [&](const R* r) { return typed && r[0] == R(kAsset); };
     d[0] = units();
     for (const R* r = first; r < last; r += kTermStride)
       if (isFloat(r)) {
@@ -261,13 +263,16 @@ void lowerTerms(Plan<R>& p) {
     if (half) push4(pending[0], pending[1], 0.0, 0.0);  // the odd bond with a zero partner
     d[2] = units();
     for (const R* r = first; r < last; r += kTermStride)
-      if (!isFloat(r) && !isBond(r) && !isFixing(r)) p.table.insert(p.table.end(), r, r + kTermStride);
+      if (isAsset(r)) push4(r[2], r[3], r[1], 0.0);
     d[3] = units();
     for (const R* r = first; r < last; r += kTermStride)
-      if (isFixing(r)) push4(r[3], -static_cast<double>(r[4]) * bScale, 1.0 / static_cast<double>(r[2]), r[1]);
+      if (!isFloat(r) && !isBond(r) && !isFixing(r) && !isAsset(r)) p.table.insert(p.table.end(), r, r + kTermStride);
     d[4] = units();
-    d[5] = I[p.offCall + j];
-    d[6] = I[p.offRep + j];
+    for (const R* r = first; r < last; r += kTermStride)
+      if (isFixing(r)) push4(r[3], -static_cast<double>(r[4]) * bScale, 1.0 / static_cast<double>(r[2]), r[1]);
+    d[5] = units();
+    d[6] = I[p.offCall + j];
+    d[7] = I[p.offRep + j];
   }
   if (p.table.empty()) p.table.assign(4, R(0));
 }
@@ -677,6 +682,7 @@ zk_status runInjected(zk_context* ctx, const ViewT* plan, const double* normals,
 // ================================================================================================
 struct zk_batch {
   std::unique_ptr<Batch<float>> b;
+  bool tuned = false;  // the tile shape was autotuned or pinned
 };
 
 extern "C" {
@@ -792,7 +798,6 @@ zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, 
     b->b = build<float>(ctx, views, false, nullptr, 0);
     upload(*b->b, ctx, false, nullptr, 0);
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
-    autotune(*b->b);
     *out = b.release();
     return ZK_OK;
   } catch (const Failure& f) {
@@ -804,7 +809,29 @@ zk_status zk_batch_execute(zk_batch* b) {
   if (!b) return ZK_ERR_INVALID_ARGUMENT;
   try {
     ZK_CUDA(cudaSetDevice(b->b->ctx->device));
+    if (!b->tuned) {
+      autotune(*b->b);  // first execute: time the tile shapes on this batch, keep the fastest
+      b->tuned = true;
+    }
     execute(*b->b);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(b->b->ctx, f);
+  }
+}
+
+zk_status zk_batch_set_tile_paths(zk_batch* b, uint64_t tile_paths) {
+  if (!b) return ZK_ERR_INVALID_ARGUMENT;
+  try {
+    const uint64_t ppt = tile_paths / kTile;
+    if (tile_paths % kTile || (ppt != 1 && ppt != 2 && ppt != 4))
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "tile_paths must be 128, 256 or 512");
+    for (const auto& L : b->b->launches)
+      if (revalueSmemBytes(L.stateWordsMax, L.perTrade, false, static_cast<int>(ppt)) > 200 * 1024)
+        throw fail(ZK_ERR_UNSUPPORTED, "this tile shape needs more shared memory than a CTA has");
+    ZK_CUDA(cudaSetDevice(b->b->ctx->device));
+    setTileShape(*b->b, static_cast<int>(ppt));
+    b->tuned = true;
     return ZK_OK;
   } catch (const Failure& f) {
     return record(b->b->ctx, f);

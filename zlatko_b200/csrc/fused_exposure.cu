@@ -258,6 +258,8 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
   const uint32_t nP = cb.nP, nT = cb.nT;
   const uint32_t nSlots = A.nSlots, ringLen = A.ring, nS = A.nS, ctype = A.ctype;
   const bool hasCsa = A.hasCsa != 0, usesAssets = A.usesAssets != 0;
+  R* __restrict__ const rowEP = expo + static_cast<size_t>(A.rowEP) * nP;
+  const bool moreRows = A.rowDV != kNoRow || A.rowE != kNoRow || A.rowV != kNoRow || A.rowC != kNoRow;
   uint32_t pth[PPT], pp[PPT];
   bool act[PPT];
 #pragma unroll
@@ -274,32 +276,47 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
     for (int i = 0; i < PPT; ++i) fix(s, i) = R(0);
   const uint32_t nTr = kPerTrade ? min(A.nTr, static_cast<uint32_t>(kMaxTradeGroups)) : 0u;
   const uint32_t fQ = A.cpty < cb.nC ? cb.fQ + A.cpty : 0xFFFFFFFFu;
-  auto cube = [&](uint32_t field, uint32_t j, int i) { return cb.data[(static_cast<size_t>(field) * nT + j) * nP + pp[i]]; };
+  // Factor loads: per path a base pointer, per date an offset j * nP, per field a stride nT * nP.
+  const size_t fieldStride = static_cast<size_t>(nT) * nP;
+  const R* cubeP[PPT];
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) cubeP[i] = cb.data + pp[i];
+  auto cube = [&](uint32_t field, uint32_t j, int i) { return cubeP[i][field * fieldStride + static_cast<size_t>(j) * nP]; };
 
   R held[PPT], prevDE[PPT], prevQ[PPT], prevRV[PPT], ex[4][PPT];
+  // Look-back of at most one date (the margin-call dates t - MPR sit on the grid): the previous date's value
+  // and collateral price in registers instead of the shared-memory ring.
+  const bool shortLook = ringLen <= 2;
+  R vPrev[PPT], pPrev[PPT];
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) vPrev[i] = R(0), pPrev[i] = R(1);
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     held[i] = R(0), prevDE[i] = R(0), prevQ[i] = R(1), prevRV[i] = R(0);
 #pragma unroll
     for (int b = 0; b < 4; ++b) ex[b][i] = R(-1);  // exercise index of each Bermudan, -1 if not exercised
   }
-  uint32_t redBuf = 0;
+  uint32_t redBuf = 0, ringPos = 0;
 
   // Software pipeline: the factors and the date descriptor of date j + 1 load while date j computes.
   R nx[PPT], nD[PPT], nQ[PPT], nS4[4][PPT];
+  const size_t qOff = fQ != 0xFFFFFFFFu ? fQ * fieldStride : 0, sOff = static_cast<size_t>(cb.fS) * fieldStride;
   auto loadFactors = [&](uint32_t j) {
+    const size_t off = static_cast<size_t>(j) * nP;
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
-      nx[i] = cube(0, j, i), nD[i] = cube(1, j, i), nQ[i] = fQ != 0xFFFFFFFFu ? cube(fQ, j, i) : R(1);
+      const R* c = cubeP[i] + off;
+      nx[i] = __ldg(c), nD[i] = __ldg(c + fieldStride), nQ[i] = fQ != 0xFFFFFFFFu ? __ldg(c + qOff) : R(1);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) nS4[a][i] = usesAssets && static_cast<uint32_t>(a) < cb.nA ? cube(cb.fS + a, j, i) : R(0);
+      for (int a = 0; a < 4; ++a)
+        nS4[a][i] = usesAssets && static_cast<uint32_t>(a) < cb.nA ? __ldg(c + sOff + a * fieldStride) : R(0);
     }
   };
   loadFactors(0);
   uint4 nd0 = __ldg(dates), nd1 = __ldg(dates + 1);
   // The block of the date after next is prefetched one date ahead of use.
-  uint32_t fBeg = nT > 1 ? __ldg(A.dates + 8) : 0u, fEnd = nT > 1 ? __ldg(A.dates + 12) : 0u;
-  prefetchDate<R>(nd0.x, nd1.x, table, tid);
+  uint32_t fBeg = nT > 1 ? __ldg(A.dates + 8) : 0u, fEnd = nT > 1 ? __ldg(A.dates + 13) : 0u;
+  prefetchDate<R>(nd0.x, nd1.y, table, tid);
 
   for (uint32_t j = 0; j < nT; ++j) {
     R x[PPT], D[PPT], Q[PPT], S[4][PPT];
@@ -315,7 +332,7 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
       nd0 = __ldg(dates + 2 * (j + 1)), nd1 = __ldg(dates + 2 * (j + 1) + 1);
       prefetchDate<R>(fBeg, fEnd, table, tid);
       if (j + 2 < nT) {
-        fBeg = __ldg(A.dates + 8 * (j + 2)), fEnd = __ldg(A.dates + 8 * (j + 2) + 4);
+        fBeg = __ldg(A.dates + 8 * (j + 2)), fEnd = __ldg(A.dates + 8 * (j + 2) + 5);
       }
     }
     if (kSink && n == 0)
@@ -335,24 +352,30 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
     }
     using R4 = typename Vec4<R>::T;
     for (uint32_t u = d0.x; u < d0.y; ++u) {  // running floating coupons
-      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+      const R4 r = ld4(table + 4 * u);
       const uint32_t slot = static_cast<uint32_t>(r.w);
 #pragma unroll
       for (int i = 0; i < PPT; ++i) value[i] += (r.x * fix(slot, i) + r.y) * termExp(r.z, x[i]);
     }
 #pragma unroll 2
     for (uint32_t u = d0.y; u < d0.z; ++u) {  // bonds, two per record
-      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+      const R4 r = ld4(table + 4 * u);
 #pragma unroll
       for (int i = 0; i < PPT; ++i) value[i] += r.x * termExp(r.y, x[i]) + r.z * termExp(r.w, x[i]);
+    }
+    for (uint32_t u = d0.z; u < d0.w; ++u) {  // asset forwards: (c, A, asset)
+      const R4 r = ld4(table + 4 * u);
+      const uint32_t a = static_cast<uint32_t>(r.z) & 3u;
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) value[i] += r.x * pick4<R, PPT>(S, a, i) * r.y;
     }
     if (kPerTrade && A.nTr > 0)
       for (uint32_t g = 0; g < kMaxTradeGroups; ++g)
 #pragma unroll
         for (int i = 0; i < PPT; ++i) vt(g, i) = R(0);
-    for (uint32_t u = d0.z; u < d0.w; u += 2) {  // generic terms: the reference's records
+    for (uint32_t u = d0.w; u < d1.x; u += 2) {  // generic terms: the reference's records
       R rec[8];
-      loadTerm(table + static_cast<size_t>(u) * 4, rec);
+      loadTerm(table + 4 * u, rec);
       const uint32_t code = static_cast<uint32_t>(rec[0]);
       const uint32_t kind = code & 15u, bm = min((code >> 8u) & 15u, 3u), extra = code >> 12u;
       const uint32_t slot = static_cast<uint32_t>(rec[1]);
@@ -458,8 +481,8 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
         for (int i = 0; i < PPT; ++i) value[i] += term[i];
       }
     }
-    for (uint32_t u = d0.w; u < d1.x; ++u) {  // fixings, after every use of the previous fixing
-      const R4 r = ld4(table + static_cast<size_t>(u) * 4);
+    for (uint32_t u = d1.x; u < d1.y; ++u) {  // fixings, after every use of the previous fixing
+      const R4 r = ld4(table + 4 * u);
       const uint32_t slot = static_cast<uint32_t>(r.w);
 #pragma unroll
       for (int i = 0; i < PPT; ++i) fix(slot, i) = (r.x * termExp(r.y, x[i]) - R(1)) * r.z;
@@ -471,7 +494,10 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
 
     // ---- CSA: collateral called on the value at t - MPR (collateral.cpp:10-47) ----
     R e[PPT], ep[PPT], en[PPT];
-    const uint32_t callJ = d1.y, rs = d1.z;
+    const uint32_t callJ = d1.z, rs = d1.w;
+    // Ring slots without a modulo: ringPos = j mod ringLen, advanced by one per date; the margin-call date
+    // lies j - callJ < ringLen dates back.
+    const uint32_t lag = j - callJ, callPos = ringPos >= lag ? ringPos - lag : ringPos + ringLen - lag;
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
       R collateral = R(0);
@@ -479,9 +505,17 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
         R price = R(1);
         if (ctype == 1) price = A.steps[static_cast<size_t>(j) * kStepStride + 22] * rexp(-A.steps[static_cast<size_t>(j) * kStepStride + 23] * x[i]);
         else if (ctype == 2) price = pick4<R, PPT>(S, min(A.casset, 3u), i);
-        ring(j % ringLen, i) = value[i];
-        if (ctype != 0) ring(ringLen + j % ringLen, i) = price;
-        const R vc = callJ != j ? ring(callJ % ringLen, i) : value[i];
+        R vc, pc = price;
+        if (shortLook) {
+          vc = callJ != j ? vPrev[i] : value[i];
+          if (callJ != j) pc = pPrev[i];
+          vPrev[i] = value[i], pPrev[i] = price;
+        } else {
+          ring(ringPos, i) = value[i];
+          if (ctype != 0) ring(ringLen + ringPos, i) = price;
+          vc = callJ != j ? ring(callPos, i) : value[i];
+          if (ctype != 0 && callJ != j) pc = ring(ringLen + callPos, i);
+        }
         R required = R(0);
         if (vc > A.hc) required += vc - A.hc;
         if (A.hb >= R(0) && -vc > A.hb) required -= -vc - A.hb;
@@ -489,7 +523,6 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
           if (j == 0 || fabs(required - held[i]) >= A.mta) held[i] = required;
           collateral = held[i] + A.ia;
         } else {
-          const R pc = callJ != j ? ring(ringLen + callJ % ringLen, i) : price;
           const R keep = A.keepHaircut;
           if (j == 0 || fabs(required - held[i] * keep * pc) >= A.mta) held[i] = required / (keep * pc);
           collateral = held[i] * price + A.ia;
@@ -497,12 +530,14 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
       }
       e[i] = value[i] - collateral, ep[i] = fmax(e[i], R(0)), en[i] = fmin(e[i], R(0));
       if (act[i] && rs > 0) {
-        const size_t k = rs - 1, pi = pth[i];
-        expo[(A.rowEP + k) * nP + pi] = ep[i];
-        if (A.rowDV != kNoRow) expo[(A.rowDV + k) * nP + pi] = rs == 1 ? R(0) : fabs(value[i] - prevRV[i]);
-        if (A.rowE != kNoRow) expo[(A.rowE + k) * nP + pi] = e[i];
-        if (A.rowV != kNoRow) expo[(A.rowV + k) * nP + pi] = value[i];
-        if (A.rowC != kNoRow) expo[(A.rowC + k) * nP + pi] = collateral;
+        const size_t k = rs - 1, pi = pth[i], at = k * nP + pi;
+        rowEP[at] = ep[i];
+        if (moreRows) {
+          if (A.rowDV != kNoRow) expo[(A.rowDV + k) * nP + pi] = rs == 1 ? R(0) : fabs(value[i] - prevRV[i]);
+          if (A.rowE != kNoRow) expo[(A.rowE + k) * nP + pi] = e[i];
+          if (A.rowV != kNoRow) expo[(A.rowV + k) * nP + pi] = value[i];
+          if (A.rowC != kNoRow) expo[(A.rowC + k) * nP + pi] = collateral;
+        }
         if (A.rowGross != kNoRow) {
           R gross = R(0);
           for (uint32_t g = 0; g < nTr; ++g) gross += fmax(vt(g, i), R(0));
@@ -562,6 +597,7 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
       }
       redBuf ^= 1u;  // the other buffer next time: one barrier per block of statistics
     }
+    ringPos = ringPos + 1 == ringLen ? 0u : ringPos + 1;
   }
 }
 

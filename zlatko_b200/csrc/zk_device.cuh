@@ -71,8 +71,9 @@ struct CubeArgs {
 template <typename R>
 struct NsArgs {
   // The plan's term table lowered at upload (lowerTerms in capi.cu): per date a descriptor
-  // {floatBegin, bondBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot, 0} into a table of
-  // 4-value records holding the date's floating coupons, bond pairs, generic 8-word terms and fixings.
+  // {floatBegin, bondBegin, assetBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot} into a
+  // table of 4-value records holding the date's floating coupons, bond pairs, asset forwards, generic
+  // 8-word terms and fixings.
   const uint32_t* dates;   // [nT][8]
   const R* table;          // [*][4]
   const R* steps;          // this plan's step table (columns 22, 23: collateral bond A, B)

@@ -164,6 +164,10 @@ class Batch:
     def execute(self) -> None:
         check(lib().zk_batch_execute(self.handle), self.ctx.handle)
 
+    def set_tile_paths(self, tile_paths: int) -> None:
+        """Pins the tile shape (paths per revalue CTA: 128, 256 or 512) instead of the autotuned one."""
+        check(lib().zk_batch_set_tile_paths(self.handle, tile_paths), self.ctx.handle)
+
     def timings(self) -> np.ndarray:
         """Milliseconds of the last execute: simulate, revalue, reduce, row statistics."""
         ms = (C.c_float * 4)()
