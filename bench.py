@@ -1,6 +1,6 @@
 """Benchmark of the exposure hot path: scenario x trade revaluations per second.
 
-Workload (default): the multi-factor correlated book of zlatko_b200.configs.config1_book -- 1,000 trades
+Workload (default): the multi-factor correlated book of zlatko_b200.workloads.correlated_csa_book -- 1,000 trades
 (600 swaps, 300 FX forwards, 100 FX options) in 100 collateralised netting sets of Zipf(1.2) sizes,
 100,000 paths, 120 monthly reporting dates to 10y (241 simulation dates with the margin-call dates),
 synthetic seeded data.  One step = the fused simulate -> revalue -> net -> collateralise -> reduce kernel
@@ -120,9 +120,9 @@ class ClockSampler:
 
 
 def workload(paths: int):
-    from zlatko_b200 import configs, gpu
+    from zlatko_b200 import gpu, workloads
 
-    m, books, opts, trades = configs.config1_book(paths)
+    m, books, opts, trades = workloads.correlated_csa_book(paths)
     t0 = time.perf_counter()
     plans = [gpu.compile(m, b, opts) for b in books]
     compile_s = time.perf_counter() - t0
@@ -130,27 +130,45 @@ def workload(paths: int):
 
 
 def cpu_reference(plans, trades: int, target_s: float, steps: int = 1):
-    """The reference's FP32 CPU kernels (runFusedReference) on all host threads over a bounded sample of
-    paths of every netting set's plan.  Returns (revals/s, sample paths, threads, seconds)."""
+    """The reference's FP32 CPU kernels (gpu::runFusedReference, built from the reference's sources into
+    oracle/_ref) on all host threads over a bounded sample of paths of every netting set's plan.  Where that
+    library is absent, the plain-C restatement of the same kernels (oracle/fused_oracle.c, one thread).
+    Returns (revals/s, sample paths, threads, seconds, per-step seconds, kind)."""
     from oracle import ref
 
-    threads = os.cpu_count() or 1
     nT = plans[0].num_dates
+    if ref.available():
+        kind, threads = "reference", os.cpu_count() or 1
 
-    def run(paths):
-        rps = [ref.plan_from_buffers(p.header, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
-                                     p.num_outputs, p.times, p.reporting, num_paths=paths) for p in plans]
-        t0 = time.perf_counter()
-        for rp in rps:
-            ref.run_fused(rp, threads)
-        return time.perf_counter() - t0
+        def run(paths):
+            rps = [ref.plan_from_buffers(p.header, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
+                                         p.num_outputs, p.times, p.reporting, num_paths=paths) for p in plans]
+            t0 = time.perf_counter()
+            for rp in rps:
+                ref.run_fused(rp, threads)
+            return time.perf_counter() - t0
+    else:
+        from oracle import restated
 
-    probe = 256
+        kind, threads = "port", 1
+
+        def run(paths):
+            heads = []
+            for p in plans:
+                h = p.header.copy()
+                h[0], h[15] = paths, (paths + 63) // 64
+                heads.append(h)
+            t0 = time.perf_counter()
+            for p, h in zip(plans, heads):
+                restated.run_fused(h, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total, p.num_outputs)
+            return time.perf_counter() - t0
+
+    probe = 256 if kind == "reference" else 64
     dt = run(probe)
     paths = int(max(probe, min(64 * probe, probe * target_s / max(dt, 1e-3))) // 64 * 64)
     times = [run(paths) for _ in range(steps)]
     dt = float(np.median(times))
-    return paths * nT * trades / dt, paths, threads, dt, times
+    return paths * nT * trades / dt, paths, threads, dt, times, kind
 
 
 def main():
@@ -166,13 +184,13 @@ def main():
         per_step = max(2.0, a.cpu_seconds / max(a.steps, 1))
         for _ in range(min(a.warmup, 1)):
             cpu_reference(plans, trades, 1.0)
-        value, paths, threads, dt, times = cpu_reference(plans, trades, per_step, steps=a.steps)
+        value, paths, threads, dt, times, kind = cpu_reference(plans, trades, per_step, steps=a.steps)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "config1_book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
+                "config": {"workload": "correlated CSA book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
                                        "HW1F + 2 FX + CIR++, 241 simulation dates", "paths_per_step": paths},
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                                  "sample": f"{paths} paths of each of the 100 netting sets per step (of {a.paths})"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -263,16 +281,17 @@ def main():
         try:
             if a.no_cpu:
                 raise RuntimeError("skipped (--no-cpu)")
-            cv, cpaths, cthreads, cdt, _ = cpu_reference(plans, trades, a.cpu_seconds / 2)
-            cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": "reference",
-                   "sample": f"{cpaths} of {nP} paths of all 100 netting sets (gpu::runFusedReference, {cthreads} threads)"}
+            cv, cpaths, cthreads, cdt, _, ckind = cpu_reference(plans, trades, a.cpu_seconds / 2)
+            what = "gpu::runFusedReference" if ckind == "reference" else "the plain-C restatement of it"
+            cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": ckind,
+                   "sample": f"{cpaths} of {nP} paths of all 100 netting sets ({what}, {cthreads} threads)"}
         except Exception as exc:  # pragma: no cover
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": t_step / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "config1_book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
+            "config": {"workload": "correlated CSA book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
                                    "HW1F + 2 FX + CIR++, 241 simulation dates", "paths": nP, "simulation_dates": nT,
                        "trades": trades, "netting_sets": len(plans), "l2": "flushed between steps (256 MB write)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},

@@ -1,0 +1,208 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY: ctypes access to oracle/_ref/liboracle.so, the plain-C restatement of
+the reference's exposure path (oracle/fused_oracle.c, oracle/engine_oracle.c; declared in oracle/oracle.h).
+
+Unlike oracle/ref.py, which needs the reference's sources to build, this library builds from the files of
+this directory alone (``make -C oracle restatement``), so it is the checker wherever the reference is not
+present.  Only tests/, the smoke check and bench.py's CPU-baseline leg may import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_ref", "liboracle.so")
+_lib: Optional[C.CDLL] = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+
+
+def build() -> None:
+    """Builds the restatement with the system C compiler (no reference sources needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "restatement"], check=True)
+
+
+def available() -> bool:
+    return os.path.exists(_LIB_PATH)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not available():
+            build()
+        L = C.CDLL(_LIB_PATH)
+        sz = C.c_size_t
+        L.orc_run_fused.restype = C.c_int
+        L.orc_run_fused.argtypes = [_up, _up, sz, _fp, _fp, _fp, sz, _fp, sz, C.c_uint32, C.c_uint32, _fp, _fp,
+                                    C.c_void_p, C.c_char_p, sz]
+        L.orc_amc_states.restype = C.c_int
+        L.orc_amc_states.argtypes = [_up, _up, _fp, _fp, _fp, C.c_uint32, _up, _fp, _fp, _fp, C.c_char_p, sz]
+        L.orc_engine_run.restype = C.c_int
+        L.orc_engine_run.argtypes = [_dp, sz, _dp, sz, C.c_double, _dp, sz, sz, _dp, _u64p, C.POINTER(C.c_size_t), _dp,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, sz]
+        L.orc_quantile.restype = C.c_double
+        L.orc_quantile.argtypes = [_dp, sz, C.c_double]
+        L.orc_collateral.restype = C.c_int
+        L.orc_collateral.argtypes = [_dp, C.c_void_p, sz, _dp, sz] + [C.c_double] * 5 + [C.c_int, C.c_double, _dp]
+        L.orc_profile.restype = None
+        L.orc_profile.argtypes = [_dp, _dp, sz, _dp, sz, C.c_double, C.c_double, _dp]
+        L.orc_unilateral_cva.restype = C.c_double
+        L.orc_unilateral_cva.argtypes = [_dp, _dp, sz, _dp, _dp, sz, C.c_double]
+        L.orc_bilateral_cva.restype = None
+        L.orc_bilateral_cva.argtypes = [_dp, _dp, _dp, sz, _dp, _dp, sz, _dp, _dp, sz, C.c_double, C.c_double, _dp]
+        L.orc_pathwise_cva.restype = C.c_double
+        L.orc_pathwise_cva.argtypes = [_dp, _dp, _dp, sz, sz, _u64p, sz, C.c_double]
+        _lib = L
+    return _lib
+
+
+def _err() -> C.Array:
+    return C.create_string_buffer(512)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, np.float32)
+
+
+def run_fused(header, indices, params, steps, terms, requests, rows_total: int, num_outputs: int, rows: bool = False):
+    """The fused pipeline in single precision on a plan in the reference's layout (the tables of a
+    zlatko_b200.gpu.Plan, or of the reference's own compile).  Returns (sums, values[, rows])."""
+    h = np.ascontiguousarray(header, np.uint32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    nT, nS, nP = int(h[1]), int(h[16]), int(h[0])
+    t, q = _f32(terms), _f32(requests)
+    sums = np.zeros(nT * nS, np.float32)
+    values = np.zeros(max(1, num_outputs), np.float32)
+    out_rows = np.zeros(max(1, rows_total) * nP, np.float32) if rows else None
+    e = _err()
+    rc = lib().orc_run_fused(h, idx, idx.size, _f32(params), _f32(steps), t, t.size // 8, q, q.size // 8, rows_total,
+                             num_outputs, sums, values, None if out_rows is None else out_rows.ctypes.data_as(C.c_void_p),
+                             e, 512)
+    if rc:
+        raise ValueError(e.value.decode())
+    if rows:
+        return sums, values, out_rows[: rows_total * nP].reshape(rows_total, nP)
+    return sums, values
+
+
+def run_plan(plan, rows: bool = False):
+    """run_fused on a zlatko_b200.gpu.Plan."""
+    return run_fused(plan.header, plan.indices, plan.params, plan.steps, plan.terms, plan.requests, plan.rows_total,
+                     plan.num_outputs, rows)
+
+
+def exercise_offsets(terms) -> np.ndarray:
+    """First exercise row of each of the (up to 4) Bermudans: a Bermudan's rows are its decide terms'
+    exercise indices (code >> 12), in Bermudan then exercise order."""
+    t = np.asarray(terms, np.float32).reshape(-1, 8)
+    code = t[:, 0].astype(np.int64)
+    rows = np.zeros(4, np.int64)
+    for c in code[(code & 15) == 6]:
+        b = min((c >> 8) & 15, 3)
+        rows[b] = max(rows[b], (c >> 12) + 1)
+    return np.concatenate([[0], np.cumsum(rows)]).astype(np.uint32)
+
+
+def amc_states(plan):
+    """gpu::runAmcStates on a zlatko_b200.gpu.Plan: x and deflator [date][path], exercise values [row][path]."""
+    off = exercise_offsets(plan.terms)
+    rows, nT, nP = int(off[-1]), plan.num_dates, plan.num_paths
+    x, d = np.zeros(nT * nP, np.float32), np.zeros(nT * nP, np.float32)
+    ex = np.zeros(max(rows, 1) * nP, np.float32)
+    e = _err()
+    if lib().orc_amc_states(plan.header, plan.indices, _f32(plan.params), _f32(plan.steps), _f32(plan.terms),
+                            plan.rows_total, off, x, d, ex, e, 512):
+        raise ValueError(e.value.decode())
+    return x.reshape(nT, nP), d.reshape(nT, nP), ex[: rows * nP].reshape(rows, nP)
+
+
+@dataclass
+class EngineResult:
+    times: np.ndarray       # simulation grid
+    reporting: np.ndarray   # indices of the reporting dates in it
+    profile: dict           # ev, ee, ene, pfe, dee, dene over the reporting dates
+    netted: np.ndarray      # [path][date]
+    collateral: np.ndarray
+    deflator: np.ndarray
+    survival: np.ndarray    # credit 0, [path][date]
+    pathwise_cva_04: float
+
+
+def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarray, streams: int,
+               num_paths: int) -> EngineResult:
+    """The FP64 exposure engine on injected normals laid out [step][normal][stream]."""
+    cap = 4096
+    times = np.zeros(cap)
+    rep = np.zeros(cap, np.uint64)
+    sizes = (C.c_size_t * 2)()
+    prof = np.zeros(6 * cap)
+    mats = [np.zeros(num_paths * cap) for _ in range(4)]
+    e = _err()
+    z = np.ascontiguousarray(normals, np.float64)
+    m, n = np.ascontiguousarray(model, np.float64), np.ascontiguousarray(ns, np.float64)
+    rc = lib().orc_engine_run(m, m.size, n, n.size, pfe, z, streams, cap, times, rep, sizes, prof,
+                              *[a.ctypes.data_as(C.c_void_p) for a in mats], e, 512)
+    if rc:
+        raise ValueError(e.value.decode())
+    nT, nR = sizes[0], sizes[1]
+    netted, coll, defl, surv = (a[: num_paths * nT].reshape(num_paths, nT) for a in mats)
+    names = ("ev", "ee", "ene", "pfe", "dee", "dene")
+    p = {k: prof[i * nR:(i + 1) * nR].copy() for i, k in enumerate(names)}
+    reporting = rep[:nR].copy()
+    expo = np.ascontiguousarray(netted - coll)
+    pcva = lib().orc_pathwise_cva(expo, np.ascontiguousarray(defl), np.ascontiguousarray(surv), num_paths, nT, reporting,
+                                  nR, 0.4)
+    return EngineResult(times[:nT].copy(), reporting.astype(np.int64), p, netted, coll, defl, surv, pcva)
+
+
+def quantile(values, p: float) -> float:
+    v = np.ascontiguousarray(values, np.float64)
+    return lib().orc_quantile(v, v.size, p)
+
+
+def profile(values: np.ndarray, deflator: np.ndarray, times, q: float, horizon: float) -> dict:
+    v = np.ascontiguousarray(values, np.float64)
+    d = np.ascontiguousarray(deflator, np.float64)
+    t = np.ascontiguousarray(times, np.float64)
+    nP, nT = v.shape
+    out = np.zeros(6 * nT + 3)
+    lib().orc_profile(v, d, nP, t, nT, q, horizon, out)
+    names = ("ev", "ee", "ene", "pfe", "dee", "dene")
+    r = {k: out[i * nT:(i + 1) * nT] for i, k in enumerate(names)}
+    r["epe"], r["eepe"], r["max_pfe"] = out[6 * nT], out[6 * nT + 1], out[6 * nT + 2]
+    return r
+
+
+def collateral(values: np.ndarray, times, hc, ho, mta, ia, mpr, kind=0, haircut=0.0, unit_price=None) -> np.ndarray:
+    v = np.ascontiguousarray(values, np.float64)
+    t = np.ascontiguousarray(times, np.float64)
+    nP, nT = v.shape
+    out = np.zeros((nP, nT))
+    up = None if unit_price is None else np.ascontiguousarray(unit_price, np.float64)
+    if lib().orc_collateral(v, None if up is None else up.ctypes.data_as(C.c_void_p), nP, t, nT, hc, ho, mta, ia, mpr,
+                            kind, haircut, out):
+        raise ValueError("simulateCollateral: invalid collateral agreement")
+    return out
+
+
+def unilateral_cva(times, dee, pillars, hazards, recovery: float) -> float:
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    t, d, p, h = f(times), f(dee), f(pillars), f(hazards)
+    return lib().orc_unilateral_cva(t, d, t.size, p, h, p.size, recovery)
+
+
+def bilateral_cva(times, dee, dene, cpty, own, rc: float, ro: float):
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    out = np.zeros(2)
+    lib().orc_bilateral_cva(f(times), f(dee), f(dene), len(times), f(cpty[0]), f(cpty[1]), len(cpty[0]), f(own[0]),
+                            f(own[1]), len(own[0]), rc, ro, out)
+    return float(out[0]), float(out[1])

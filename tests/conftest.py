@@ -18,15 +18,10 @@ def _ensure_built():
     from zlatko_b200 import build
 
     build.build()
-    ref_lib = os.path.join(ROOT, "oracle", "_ref", "libccr_ref.so")
-    oracle_lib = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
-    if os.path.isdir("/root/reference") or not os.path.exists(ref_lib) or not os.path.exists(oracle_lib):
-        # The GPU box has no reference sources: it uses the prebuilt oracle libraries that travel with the repo.
-        targets = ["ref"] if os.path.isdir("/root/reference") else []
-        if os.path.exists(os.path.join(ROOT, "oracle", "fused_oracle.c")):
-            targets.append("restatement")
-        if targets:
-            subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle")] + targets, check=True)
+    # The plain-C restatement builds anywhere; the reference library only where its sources are (elsewhere the
+    # prebuilt copy that travels with the repository, if any, is used).
+    targets = ["restatement"] + (["ref"] if os.path.isdir("/root/reference") else [])
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle")] + targets, check=True)
 
 
 _ensure_built()

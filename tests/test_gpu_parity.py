@@ -1,31 +1,31 @@
-"""GPU parity: the CUDA kernels (zk_run_plan) against the reference's FP32 CPU kernels (runFusedReference)
-on the same plans, and the FP64 mode against the reference's FP64 ExposureEngine on the same normals.
+"""GPU parity: the CUDA kernels (zk_run_plan and friends) against the oracle.
 
-Tolerances.  The FP32 kernels draw the same counter-based normals as the reference; the two differ only
-by the rounding of single-precision transcendental functions (CUDA's against glibc's), so statistics
-agree to about 1e-6 of their scale; the tests allow 2e-4 of each statistic's scale (and 1e-3 for the
-few path-level view statistics that sit on a histogram edge).  FP64 mode: 1e-9 relative.
+The oracle is the plain-C restatement of the reference's path (oracle/restated.py), which is pinned bit for bit
+to the reference itself (tests/test_oracle_pins.py), plus the golden fixtures the reference computed
+(tests/golden/).  Plans come from this package's compiler (pinned table-for-table to the reference's
+gpu::compile by tests/test_compiler.py) or, where the reference fits something this build does not (the AMC
+regression of a Bermudan), from the reference's own tables stored in a fixture.
+
+Tolerances.  The FP32 kernels draw the same counter-based normals as the reference; the two differ only by the
+rounding of single-precision transcendental functions (CUDA's against glibc's), so statistics agree to about
+1e-6 of their scale; the tests allow 2e-4 of each statistic's scale (and 1e-3 for the few path-level view
+statistics that sit on a histogram edge).  Quantiles are exact on both sides, so they differ only through the
+exposure rows.  FP64 mode against the FP64 engine on identical normals: 1e-9 relative.
 """
+import os
+
 import numpy as np
 import pytest
 
-from oracle import ref
+from oracle import restated
 from setups import bermudan, gpu_model, gpu_netting_set, gpu_setup, swap_book
 from zlatko_b200 import gpu
 from zlatko_b200 import spec as S
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")]
+pytestmark = pytest.mark.gpu
 
 RTOL = 2e-4
-
-
-def as_plan(r: ref.RefPlan) -> gpu.Plan:
-    return gpu.Plan.from_arrays(r.header, r.indices, r.params, r.steps, r.terms, r.requests, r.rows_total, r.num_outputs,
-                                r.times, r.reporting.astype(np.int64), r.market_survival)
-
-
-def ref_plan(m, ns, o=None):
-    return ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o or S.Options()))
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def check_sums(plan, sums_g, sums_r, rtol=RTOL):
@@ -56,29 +56,44 @@ def check_values(plan, vals_g, vals_r, rtol=RTOL):
 
 
 def run_both(ctx, m, ns, o=None):
-    r = ref_plan(m, ns, o)
-    p = as_plan(r)
+    p = gpu.compile(m, ns, o or S.Options())
     sg, vg = ctx.run(p)
-    sr, vr = ref.run_fused(r)
-    return r, p, (sg, vg), (sr, vr)
+    sr, vr = restated.run_plan(p)
+    return p, (sg, vg), (sr, vr)
+
+
+def fixture(name):
+    f = np.load(os.path.join(GOLDEN, name + ".npz"))
+    plan = gpu.Plan.from_arrays(f["header"], f["indices"], f["params"], f["steps"], f["terms"], f["requests"],
+                                int(f["rows_total"]), int(f["num_outputs"]), f["times"], f["reporting"])
+    return f, plan
+
+
+def with_paths(plan: gpu.Plan, n: int) -> gpu.Plan:
+    """The same plan on n paths (header[0]; header[15] is the reference's count of 64-path workgroups)."""
+    h = plan.header.copy()
+    h[0], h[15] = n, (n + 63) // 64
+    return gpu.Plan.from_arrays(h, plan.indices, plan.params, plan.steps, plan.terms, plan.requests, plan.rows_total,
+                                plan.num_outputs, plan.times, plan.reporting)
 
 
 @pytest.mark.parametrize("csa", [False, True])
-def test_fused_matches_reference_cpu_kernels(ctx, csa):
+def test_fused_matches_oracle(ctx, csa):
     m, ns = gpu_setup(8000, csa)
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
     check_sums(p, sg, sr)
     check_values(p, vg, vr)
-    # The summaries (gpu::summarise of the reference) of both read-backs agree too.
-    a, b = ref.summarise(r, sg, vg), ref.summarise(r, sr, vr)
+    # The summaries (EE, PFE, CVA inputs per reporting date) of both read-backs agree too.
+    from zlatko_b200.summary import summarise
+
+    a, b = summarise(p, sg, vg), summarise(p, sr, vr)
     for k in ("ee", "ene", "pfe", "dee", "dene", "mean_survival"):
         assert np.abs(a[k] - b[k]).max() <= RTOL * max(np.abs(b[k]).max(), 1e-12), k
-    assert abs(a["pathwise_cva_04"] - b["pathwise_cva_04"]) <= RTOL * abs(b["pathwise_cva_04"])
 
 
 def test_per_trade_and_margin_quantile(ctx):
     m, ns = gpu_setup(8000, False)
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, S.Options(per_trade=True, im_quantile=0.99))
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, S.Options(per_trade=True, im_quantile=0.99))
     assert p.stats_per_date == 24
     check_sums(p, sg, sr)
     check_values(p, vg, vr)
@@ -87,7 +102,7 @@ def test_per_trade_and_margin_quantile(ctx):
 def test_path_views(ctx):
     m, ns = gpu_setup(8000, True)
     o = S.Options(samples=12, histogram_time=2.0, gross=True, collateral_bands=True, trade_views=True)
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, o)
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, o)
     check_sums(p, sg, sr)
     check_values(p, vg, vr)
 
@@ -95,7 +110,7 @@ def test_path_views(ctx):
 def test_factor_views_probes(ctx):
     m, _ = gpu_setup(8000, False)
     o = S.Options(factor_views=True, samples=5, bond_maturity=8.0)
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, S.NettingSet([]), o)
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, S.NettingSet([]), o)
     check_sums(p, sg, sr)
     check_values(p, vg, vr)
 
@@ -104,30 +119,58 @@ def test_factor_views_probes(ctx):
 def test_securities_collateral(ctx, kind):
     m, ns = gpu_setup(8000, True)
     ns.csa.kind, ns.csa.haircut, ns.csa.bond_maturity, ns.csa.mpr = kind, 0.02 if kind == 1 else 0.15, 10.0, 20.0 / 250.0
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, ns)
     check_sums(p, sg, sr)
     check_values(p, vg, vr)
 
 
+def test_two_schedule_swap_book(ctx):
+    m = gpu_model(6000, seed=3)
+    m.base_grid = [k / 12 for k in range(1, 61)]
+    p, (sg, vg), (sr, vr) = run_both(ctx, m, swap_book(25, seed=9, csa=S.Csa(1e5, 1e5, 1e4)), S.Options(pfe_quantile=0.975))
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr)
+
+
+@pytest.mark.parametrize("name", ["fused_plain", "fused_csa_views", "fused_bond_collateral", "fused_asset_collateral",
+                                  "fused_bermudan", "fused_swap_book"])
+def test_golden_fixtures(ctx, name):
+    """The reference's own tables run on the GPU reproduce the reference's own outputs."""
+    f, p = fixture(name)
+    sg, vg = ctx.run(p)
+    check_sums(p, sg, f["sums"], rtol=1e-3 if name == "fused_bermudan" else RTOL)
+    exact = f["values"].copy()
+    for q in p.requests.reshape(-1, 8):  # quantiles: the exact ccr::quantile of the reference's rows
+        if int(q[0]) in (0, 7):
+            exact[int(q[7])] = f["exact_quantiles"][int(q[7])]
+    check_values(p, vg, exact, rtol=1e-3 if name == "fused_bermudan" else RTOL)
+
+
 @pytest.mark.parametrize("physical", [True, False])
 def test_bermudan_amc_terms(ctx, physical):
-    """Bermudans priced by the reference-fitted policy and continuation terms: the same exercise decisions."""
-    m, ns = gpu_setup(4000, False)
-    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=physical, degree=2))
-    ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=physical, position=-0.5, degree=3))
-    r, p, (sg, vg), (sr, vr) = run_both(ctx, m, ns, S.Options(exercise_views=True, samples=8))
+    """Bermudans priced by the reference-fitted policy and continuation terms: the same exercise decisions as the
+    oracle on the same tables, on 4000 paths."""
+    f, p = fixture("fused_bermudan")
+    p = with_paths(p, 4000)
+    if not physical:  # the same policy, settled in cash: drop the exercised-tail terms of the underlying
+        t = p.terms.reshape(-1, 8).copy()
+        kind = t[:, 0].astype(np.int64) & 15
+        t[(kind == 8) | (kind == 9), 2] = 0.0
+        t[(kind == 9), 5] = 0.0
+        p = gpu.Plan.from_arrays(p.header, p.indices, p.params, p.steps, t.reshape(-1), p.requests, p.rows_total,
+                                 p.num_outputs, p.times, p.reporting)
+    sg, vg = ctx.run(p)
+    sr, vr = restated.run_plan(p)
     check_sums(p, sg, sr, rtol=1e-3)
     check_values(p, vg, vr, rtol=1e-3)
 
 
-def test_amc_state_pass_matches_reference(ctx):
-    m, ns = gpu_setup(2000, False)
-    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0), degree=3))
-    r = ref_plan(m, ns)
-    p = as_plan(r)
-    rows = int(ref.lib().ref_amc_rows(r.handle))
+def test_amc_state_pass_matches_oracle(ctx):
+    f, p = fixture("fused_bermudan")
+    p = with_paths(p, 2000)
+    rows = int(restated.exercise_offsets(p.terms)[-1])
     xg, dg, eg = ctx.amc_states(p, rows)
-    xr, dr, er = ref.amc_states(r)
+    xr, dr, er = restated.amc_states(p)
     assert np.abs(xg - xr).max() <= 1e-5 * np.abs(xr).max()
     assert np.abs(dg - dr).max() <= 1e-5
     assert np.abs(eg - er).max() <= 2e-4 * np.abs(er).max()
@@ -146,27 +189,56 @@ def test_batch_equals_single_plans(ctx):
         assert np.array_equal(s, s1) and np.array_equal(v, v1)
 
 
+def test_results_do_not_depend_on_the_tile_shape(ctx):
+    """Every tile shape the autotuner may pick gives the same bits (the partials are reduced in path order)."""
+    m = gpu_model(5000)
+    m.base_grid = [k / 12 for k in range(1, 61)]
+    plans = [gpu.compile(m, swap_book(9, seed=s, csa=S.Csa(1e5, 1e5, 1e4) if s else None), S.Options()) for s in (0, 1)]
+    out = []
+    for tile in (128, 256, 512):
+        b = ctx.batch(plans)
+        try:
+            b.set_tile_paths(tile)
+            b.execute()
+            out.append(b.read())
+        finally:
+            b.close()
+    for r in out[1:]:
+        for (s0, v0), (s1, v1) in zip(out[0], r):
+            assert np.array_equal(s0, s1) and np.array_equal(v0, v1)
+
+
 def test_pfe_is_the_exact_interpolated_quantile(ctx):
     """The row-statistics kernel returns ccr::quantile of the rows the fused kernel wrote (exactly, up to
     the final rounding to float)."""
     m, ns = gpu_setup(5000, True)
     for level in (0.5, 0.95, 0.975, 0.99):
-        r = ref_plan(m, ns, S.Options(pfe_quantile=level))
-        p = as_plan(r)
+        p = gpu.compile(m, ns, S.Options(pfe_quantile=level))
         streams = (p.num_paths + 1) // 2
         z = np.random.default_rng(11).standard_normal((p.num_dates - 1) * int(p.header[5]) * streams)
         sums, vals, rows = ctx.run_injected(p, z, streams, rows=True)
         for k in range(p.num_reporting):
             # The plan carries the level in single precision (requests are f32), as the reference's kernel reads it.
-            exact = ref.quantile(rows[int(p.header[28]) + k].astype(np.float64), float(np.float32(level)))
+            exact = restated.quantile(rows[int(p.header[28]) + k].astype(np.float64), float(np.float32(level)))
             assert vals[k] == np.float32(exact) or abs(vals[k] - exact) <= 1e-7 * max(abs(exact), 1.0)
+
+
+def test_quantile_edge_cases(ctx):
+    """Rows with ties, one distinct value and very few paths: still the exact interpolated quantile."""
+    for paths in (1, 2, 3, 64, 65):
+        m, _ = gpu_setup(paths, False)
+        p = gpu.compile(m, S.NettingSet([]), S.Options(factor_views=True, samples=min(paths, 3), pfe_quantile=0.95))
+        sg, vg = ctx.run(p)
+        sr, vr = restated.run_plan(p)
+        check_values(p, vg, vr)
+        assert np.isfinite(vg[: max(1, p.num_outputs)]).all()
 
 
 def test_invalid_plans_are_rejected(ctx):
     from zlatko_b200._native import ZkError
 
     m, ns = gpu_setup(500, False)
-    p = as_plan(ref_plan(m, ns))
+    p = gpu.compile(m, ns, S.Options())
     bad = gpu.Plan.from_arrays(p.header[:20], p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total,
                                p.num_outputs, p.times, p.reporting)
     with pytest.raises(ZkError, match="INVALID_PLAN"):
@@ -202,9 +274,11 @@ def test_fp64_matches_engine_on_identical_normals(ctx, csa):
     p = gpu.compile(m, ns, o)
     z, streams = injected_normals(p, 5)
     sums, vals, rows = ctx.run_f64(p, z, streams, rows=True)
-    e = ref.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams)
+    e = restated.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams, m.num_paths)
     assert np.array_equal(e.times, p.times)
-    res = __import__("zlatko_b200.summary", fromlist=["summarise"]).summarise(p, sums, vals)
+    from zlatko_b200.summary import summarise
+
+    res = summarise(p, sums, vals)
     for k in ("ev", "ee", "ene", "pfe", "dee", "dene"):
         scale = max(np.abs(e.profile[k]).max(), 1e-12)
         assert np.abs(res[k] - e.profile[k]).max() <= 1e-9 * scale, k
@@ -219,3 +293,25 @@ def test_fp64_matches_engine_on_identical_normals(ctx, csa):
     # Pathwise CVA with the simulated survival.
     pcva = 0.6 * np.nansum(res["cva_inc"])
     assert abs(pcva - e.pathwise_cva_04) <= 1e-9 * abs(e.pathwise_cva_04)
+
+
+@pytest.mark.parametrize("csa", [False, True])
+def test_fp64_matches_golden_engine(ctx, csa):
+    """The FP64 mode on the normals of a golden engine fixture reproduces the reference engine's profile."""
+    f = np.load(os.path.join(GOLDEN, "engine_csa.npz" if csa else "engine_plain.npz"))
+    m, ns = gpu_setup(256, csa)  # the set-up the fixture was made from
+    assert np.array_equal(S.encode_model(m), f["model"]) and np.array_equal(S.encode_netting_set(ns), f["netting_set"])
+    p = gpu.compile(m, ns, S.Options(samples=1))
+    streams = int(f["streams"])
+    z = np.random.default_rng(int(f["seed"])).standard_normal((p.num_dates - 1) * int(f["num_normals"]) * streams)
+    sums, vals, rows = ctx.run_f64(p, z, streams, rows=True)
+    from zlatko_b200.summary import summarise
+
+    res = summarise(p, sums, vals)
+    for i, k in enumerate(("ev", "ee", "ene", "pfe", "dee", "dene")):
+        scale = max(np.abs(f["profile"][i]).max(), 1e-12)
+        assert np.abs(res[k] - f["profile"][i]).max() <= 1e-9 * scale, k
+    H, nR = p.header, len(f["reporting"])
+    scale = np.abs(f["netted"]).max()
+    assert np.abs(rows[H[21]:H[21] + nR].T - f["netted"]).max() <= 1e-9 * scale
+    assert abs(0.6 * np.nansum(res["cva_inc"]) - float(f["pathwise_cva_04"])) <= 1e-9 * abs(float(f["pathwise_cva_04"]))

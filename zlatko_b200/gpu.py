@@ -111,7 +111,18 @@ def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Optio
     """zk_compile: the host plan compiler (a restatement of gpu::compile, src/gpu/fused_exposure.cpp:214).
     Raises ValueError where the reference throws std::invalid_argument."""
     options = options or S.Options()
-    m, n, o = S.encode_model(model), S.encode_netting_set(netting_set), S.encode_options(options)
+    plan = compile_arrays(S.encode_model(model), S.encode_netting_set(netting_set), S.encode_options(options))
+    if model.credits:
+        from .summary import hazard_survival
+        c = model.credits[options.counterparty]
+        plan.market_survival = np.array([hazard_survival(c.pillars, c.hazards, t) for t in plan.times])
+    return plan
+
+
+def compile_arrays(m: np.ndarray, n: np.ndarray, o: np.ndarray) -> Plan:
+    """zk_compile on the flat model / netting-set / options arrays of zlatko_b200.spec.  The plan's
+    market_survival is that of no default (compile() fills in the counterparty's curve)."""
+    m, n, o = (np.ascontiguousarray(a, np.float64) for a in (m, n, o))
     L = lib()
     h = C.c_void_p()
     err = C.create_string_buffer(512)
@@ -140,12 +151,7 @@ def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Optio
                          "terms": arr(v64.terms, v64.terms_len, np.float64),
                          "requests": arr(v64.requests, v64.requests_len, np.float64)}
         plan.exercise_rows = int(sizes[5])
-        if model.credits:
-            from .summary import hazard_survival
-            c = model.credits[options.counterparty]
-            plan.market_survival = np.array([hazard_survival(c.pillars, c.hazards, t) for t in times])
-        else:
-            plan.market_survival = np.ones(nT)
+        plan.market_survival = np.ones(nT)
         return plan
     finally:
         L.zk_plan_destroy(h)

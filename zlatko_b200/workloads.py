@@ -1,10 +1,10 @@
 """Seeded synthetic workloads of the benchmark configurations (no public dataset exists for this path).
 
-config0_swaps: one uncollateralised netting set of 20 swaps under HW(0.03, 0.01) on a flat 2% curve,
+swap_portfolio: one uncollateralised netting set of 20 swaps under HW(0.03, 0.01) on a flat 2% curve,
     notionals U[1e6, 1e7], fixed rates U[1%, 4%], payer / receiver 50/50, maturities U[1y, 5y],
     annual fixed and semiannual floating legs, 10,000 paths on 60 monthly dates, PFE 97.5%,
     counterparty hazard 1% (CVA with LGD 0.6).
-config1_book: 1,000 trades (600 swaps, 300 FX forwards, 100 FX options) in 100 netting sets of
+correlated_csa_book: 1,000 trades (600 swaps, 300 FX forwards, 100 FX options) in 100 netting sets of
     Zipf(1.2) sizes, each under a two-way CSA (threshold U[0, 5e6], MTA 1e5, MPR 10/250), 100,000
     paths on 120 monthly dates to 10y, HW(a, sigma) with a ~ U[0.01, 0.1], sigma ~ U[0.005, 0.015],
     2 lognormal FX rates (vol U[8%, 15%]) and one CIR++ intensity (kappa 0.5, theta 0.02, xi 0.08)
@@ -73,7 +73,7 @@ def zipf_sizes(total: int, groups: int, s: float) -> List[int]:
     return [int(x) for x in sizes]
 
 
-def config0_swaps(paths: int = 10_000) -> Tuple[S.Model, S.NettingSet, S.Options]:
+def swap_portfolio(paths: int = 10_000) -> Tuple[S.Model, S.NettingSet, S.Options]:
     rng = np.random.default_rng(PORTFOLIO_SEED)
     m = S.Model(curve=S.Curve.flat(0.02), hw_a=0.03, hw_sigma=0.01,
                 credits=[S.Credit(1e-6, 0.0, 0.0, 0.0, [1.0], [0.01], substeps=1)],
@@ -82,7 +82,7 @@ def config0_swaps(paths: int = 10_000) -> Tuple[S.Model, S.NettingSet, S.Options
     return m, ns, S.Options(pfe_quantile=0.975)
 
 
-def config1_book(paths: int = 100_000, netting_sets: int = 100) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
+def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
     """Returns (model, netting sets, options, number of trades)."""
     rng = np.random.default_rng(PORTFOLIO_SEED + 1)
     a, sigma = rng.uniform(0.01, 0.1), rng.uniform(0.005, 0.015)
