@@ -498,7 +498,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
   for (size_t i = 0; i < B.plans.size(); ++i) {
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, B.ppt), P.nP, 0};
+    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP, 0};
     B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
     for (size_t q = 0; q < P.nReq; ++q)
       rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),
@@ -613,15 +613,11 @@ void checkOutputs(const Batch<R>& B, const void* outs, bool f64) {
   }
 }
 
-// The tile shape: paths per revalue thread (kTile * ppt paths per CTA).  The per-tile partials are laid
-// out for the smallest tile, so any shape fits; the reduce jobs follow the tile count.
+// The tile shape: paths per revalue thread (kTile * ppt paths per CTA).  The partials are per 128-path
+// group whatever the shape, so the reduce jobs and the results do not change with it.
 template <typename R>
 void setTileShape(Batch<R>& B, int ppt) {
   B.ppt = ppt;
-  for (size_t i = 0; i < B.plans.size(); ++i) B.reduceJobs[i].numTiles = numTilesOf(B.plans[i].nP, ppt);
-  ZK_CUDA(cudaMemcpyAsync(B.base + B.reduceOff, B.reduceJobs.data(), B.reduceJobs.size() * sizeof(ReduceJob<R>),
-                          cudaMemcpyHostToDevice, B.ctx->stream));
-  ZK_CUDA(cudaStreamSynchronize(B.ctx->stream));
 }
 
 // Autotuner: times the revalue kernel of this batch once per candidate tile shape (after a warm-up

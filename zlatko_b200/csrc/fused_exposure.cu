@@ -15,8 +15,9 @@
 //                    table (warp-uniform loads, served to all 32 lanes by one L1 broadcast), applies
 //                    the CSA with the margin-call look-back kept in a shared-memory ring, writes the
 //                    reporting-date rows and reduces the 8 (+5 per trade) statistics of the date with a
-//                    warp reduce-scatter (9 shuffles) and one cross-warp pass into per-tile partials,
-//                    which the reduce kernel sums in a fixed order (deterministic results).
+//                    warp reduce-scatter (9 shuffles) and one cross-warp pass per 128-path group into
+//                    per-group partials, which the reduce kernel sums in path order: the results are
+//                    deterministic and the same for every tile shape.
 #include "zk_device.cuh"
 #include "zk_kernels.h"
 
@@ -243,8 +244,8 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
   __shared__ NsArgs<R> sA;
-  R* red = reinterpret_cast<R*>(smemRaw);                          // [2][kWarps][8]
-  R* vtBuf = red + 2 * kWarps * 8;                                 // [16][PPT][kTile] per-trade values
+  R* red = reinterpret_cast<R*>(smemRaw);                          // [2][PPT][kWarps][8]
+  R* vtBuf = red + 2 * PPT * kWarps * 8;                           // [16][PPT][kTile] per-trade values
   R* state = vtBuf + (kPerTrade ? kMaxTradeGroups * PPT * kTile : 0);  // fixings [nSlots][PPT][kTile] | ring
 
   const uint32_t n = blockIdx.x % numNs, tile = blockIdx.x / numNs;
@@ -565,35 +566,40 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
       }
     }
 
-    // ---- statistics of this date (the thread's PPT paths summed first): the netting set's 8, then
-    // kTradeStats per trade ----
+    // ---- statistics of this date: the netting set's 8, then kTradeStats per trade, reduced per 128-path
+    // group (slot i of the tile), so the partials and their bits do not depend on the tile shape ----
+    const uint32_t group0 = tile * PPT;
     for (uint32_t q = 0; q < nS; q += 8) {
-      R v8[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) v8[c] = R(0);
+      R* rb = red + redBuf * (PPT * kWarps * 8);
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
-        if (!act[i]) continue;
-        if (q == 0) {
-          v8[0] += e[i], v8[1] += ep[i], v8[2] += en[i], v8[3] += D[i] * ep[i], v8[4] += D[i] * en[i];
-          v8[5] += cvaInc[i], v8[6] += Q[i], v8[7] += D[i];
-        } else {
+        R v8[8];
 #pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const uint32_t k = q + c - kStatsPerDate, g = k / kTradeStats;
-            if (q + c < nS && g < nTr) v8[c] += tradeStat<R>(k % kTradeStats, vt(g, i), value[i], D[i]);
+        for (int c = 0; c < 8; ++c) v8[c] = R(0);
+        if (act[i]) {
+          if (q == 0) {
+            v8[0] = e[i], v8[1] = ep[i], v8[2] = en[i], v8[3] = D[i] * ep[i], v8[4] = D[i] * en[i];
+            v8[5] = cvaInc[i], v8[6] = Q[i], v8[7] = D[i];
+          } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+              const uint32_t k = q + c - kStatsPerDate, g = k / kTradeStats;
+              if (q + c < nS && g < nTr) v8[c] = tradeStat<R>(k % kTradeStats, vt(g, i), value[i], D[i]);
+            }
           }
         }
+        const R s = warpReduceScatter8(v8, lane);
+        if ((lane & 3u) == 0) rb[(i * kWarps + warp) * 8 + statSlotOfLane(lane)] = s;
       }
-      const R s = warpReduceScatter8(v8, lane);
-      R* rb = red + redBuf * kWarps * 8;
-      if ((lane & 3u) == 0) rb[warp * 8 + statSlotOfLane(lane)] = s;
       __syncthreads();
-      if (tid < 8 && q + tid < nS) {
-        R sum = R(0);
+      if (tid < 8 * PPT) {
+        const uint32_t i = tid >> 3, c = tid & 7u;
+        if (q + c < nS && (group0 + i) * kTile < nP) {
+          R sum = R(0);
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) sum += rb[w * 8 + tid];
-        A.partials[(static_cast<size_t>(tile) * nT + j) * nS + q + tid] = sum;
+          for (int w = 0; w < kWarps; ++w) sum += rb[(i * kWarps + w) * 8 + c];
+          A.partials[(static_cast<size_t>(group0 + i) * nT + j) * nS + q + c] = sum;
+        }
       }
       redBuf ^= 1u;  // the other buffer next time: one barrier per block of statistics
     }
@@ -611,7 +617,7 @@ cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cud
 
 size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) {
   const size_t r = f64 ? 8 : 4;
-  return (2 * kWarps * 8 + (perTrade ? kMaxTradeGroups * ppt * kTile : 0) + stateWordsMax * ppt * kTile) * r;
+  return (2 * ppt * kWarps * 8 + (perTrade ? kMaxTradeGroups * ppt * kTile : 0) + stateWordsMax * ppt * kTile) * r;
 }
 
 namespace {
