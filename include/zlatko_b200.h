@@ -91,6 +91,10 @@ zk_status zk_context_set_stream(zk_context* ctx, void* stream);
  * :565-771) on the GPU.  Host buffers in, host buffers out. */
 zk_status zk_run_plan(zk_context* ctx, const zk_plan_view* plan, zk_output* out);
 
+/* zk_run_plan plus the per-path rows the fused kernel wrote, rows[row][path] (rows_total * nP floats): the
+ * exposure slice of the reference's runFusedWorkgroups (FusedSlice::exposure, fused_reference.cpp:426-466). */
+zk_status zk_run_plan_rows(zk_context* ctx, const zk_plan_view* plan, zk_output* out, float* rows);
+
 /* Many plans in one launch (the reference's book mode, analyses.cpp:1604-2050 runs one plan per
  * netting set).  Plans that share the scenario (paths, dates, models, seed, Cholesky) share one
  * simulation of the risk factors on the GPU; the rest run as separate launches. */
@@ -101,6 +105,18 @@ zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_
  * then exercise order; exercise_rows must equal the plan's total number of exercise dates). */
 zk_status zk_amc_states(zk_context* ctx, const zk_plan_view* plan, float* x, float* deflator, float* exercise,
                         size_t exercise_rows);
+
+/* Replaces the Longstaff-Schwartz fit that the reference's gpu::compile runs on its CPU kernels (fitAmc,
+ * src/gpu/fused_exposure.cpp:103-156): the AMC state pass on the GPU, then the policy regression of every
+ * exercise (in-the-money paths, backwards) and the continuation regression of every date, in double
+ * precision with FP64 Cholesky solves, one thread-block cluster per Bermudan.  terms_out (terms_len =
+ * plan->terms_len) receives the plan's term table with the fitted policy and continuation records;
+ * degrees[b] (<= 3) is the regression degree of Bermudan b, num_bermudans the plan's count (header[27]). */
+zk_status zk_fit_amc(zk_context* ctx, const zk_plan_view* plan, const uint32_t* degrees, size_t num_bermudans, float* terms_out,
+                     size_t terms_len);
+/* The same fit in the FP64 mode, on the FP64 state pass (normals as in zk_run_plan_f64; nullable). */
+zk_status zk_fit_amc_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams,
+                         const uint32_t* degrees, size_t num_bermudans, double* terms_out, size_t terms_len);
 
 /* FP64 mode.  `normals` (nullable) injects the standard normals instead of the counter-based
  * generator: normals[((j - 1) * nNormals + k) * streams + s] is normal k of step j on stream s; path p

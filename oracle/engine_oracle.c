@@ -4,11 +4,11 @@
  *                         lognormal_asset.cpp:16-21, cir_intensity.cpp:25-66, matrix.cpp:49-68
  *   grids                 time_grid.cpp:13-66, exposure_engine.cpp:35-48
  *   valuation             interest_rate_swap.cpp:51-83, asset_forward.cpp:13-25, european_option.cpp:21-35,
- *                         math.hpp:15-30 (Black)
+ *                         math.hpp:15-30 (Black), bermudan_swaption.cpp:49-146 (Longstaff-Schwartz on the
+ *                         short-rate state, with the regression of amc_oracle.c)
  *   netting, collateral   exposure_engine.cpp:9-14, collateral.cpp:10-47
  *   statistics and CVA    exposure_profile.cpp:10-83, math.hpp:39-47, cva.cpp:11-77, credit_curve.cpp:23-35
- * The netting-set / model arrays are the flat encodings the package's spec module writes.  Bermudan
- * swaptions (whose engine valuation fits its own regression) are not restated and are rejected. */
+ * The netting-set / model arrays are the flat encodings the package's spec module writes. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -36,11 +36,16 @@ typedef struct {
   Hazard market;
 } Credit;
 typedef struct {
-  int kind; /* 0 swap, 1 forward, 2 option */
+  int kind; /* 0 swap, 1 forward, 2 option, 3 Bermudan swaption on the swap */
   double notional, fixed, strike, maturity;
   int payFixed, call;
   size_t asset, nSched;
   double* sched;
+  /* Bermudan: sorted exercise times, settlement, position, regression degree */
+  size_t nEx;
+  double* ex;
+  int physical, degree;
+  double position;
 } Trade;
 typedef struct {
   int has, type;
@@ -322,8 +327,17 @@ static int read_netting(const double* a, size_t n, Netting* ns, char* err, size_
       ns->tr[ns->nTr++] = swap_of(notional, K, pay, fixed.sched, fixed.nSched);
       ns->tr[ns->nTr++] = swap_of(notional, 0.0, !pay, fixed.sched, fixed.nSched);
       free(fixed.sched), free(flt.sched);
+    } else if (type == 3) {
+      t->kind = 3, t->notional = next(&r), t->fixed = next(&r), t->payFixed = next(&r) != 0.0;
+      read_sched(&r, t);
+      t->nEx = count(&r);
+      t->ex = (double*)calloc(t->nEx + 1, sizeof(double));
+      for (size_t q = 0; q < t->nEx; ++q) t->ex[q] = next(&r);
+      qsort(t->ex, t->nEx, sizeof(double), cmp_d);
+      t->physical = next(&r) != 0.0, t->position = next(&r), t->degree = (int)count(&r);
+      ++ns->nTr;
     } else {
-      return fail(err, len, type == 3 ? "netting set: Bermudan swaptions are not restated" : "netting set: unknown trade type");
+      return fail(err, len, "netting set: unknown trade type");
     }
   }
   if (next(&r) != 0.0) {
@@ -338,7 +352,15 @@ static int read_netting(const double* a, size_t n, Netting* ns, char* err, size_
   if (ns->nTr == 0) return fail(err, len, "ExposureEngine::run: empty netting set");
   for (size_t k = 0; k < ns->nTr; ++k) {
     const Trade* t = &ns->tr[k];
-    if (t->kind == 0) {
+    if (t->kind == 3) {
+      if (t->nEx == 0) return fail(err, len, "BermudanSwaption: no exercise dates");
+      for (size_t q = 0; q < t->nEx; ++q) {
+        int on = 0;
+        for (size_t i = 0; i + 1 < t->nSched; ++i) on |= fabs(t->sched[i] - t->ex[q]) < 1e-8;
+        if (!on) return fail(err, len, "BermudanSwaption: exercise dates must be start dates of the underlying periods");
+      }
+    }
+    if (t->kind == 0 || t->kind == 3) {
       if (t->nSched < 2 || t->sched[0] < 0.0) return fail(err, len, "InterestRateSwap: invalid schedule");
       for (size_t i = 1; i < t->nSched; ++i)
         if (t->sched[i] <= t->sched[i - 1]) return fail(err, len, "InterestRateSwap: schedule must be strictly increasing");
@@ -416,6 +438,80 @@ static void value_at(const Model* m, const Trade* tr, const Grid* g, size_t j, c
     const double fwd = S[tr->asset][p * nT + j] * carry / df;
     out[p] = tr->notional * black(tr->call, fwd, tr->strike, sd, df);
   }
+}
+
+/* A Bermudan swaption on every path and date (bermudan_swaption.cpp:49-146): exercise values of the tail swaps,
+ * backward Longstaff-Schwartz over the exercise dates on the short-rate state, first exercise per path, then
+ * on every date the tail swap (exercised, physical), nothing (exercised, cash) or the regressed continuation. */
+static void bermudan_cube(const Model* m, const Trade* tr, const Grid* g, const double* X, const double* Dm, size_t nP,
+                          double* out, double* exIndex) {
+  const size_t nT = g->n, nE = tr->nEx;
+  size_t* jEx = (size_t*)malloc(nE * sizeof(size_t));
+  Trade* tails = (Trade*)calloc(nE, sizeof(Trade));
+  for (size_t k = 0; k < nE; ++k) {
+    jEx[k] = (size_t)find_time(g, tr->ex[k]);
+    size_t first = 0;
+    while (first < tr->nSched && tr->sched[first] < tr->ex[k] - 1e-10) ++first;
+    tails[k] = swap_of(tr->notional, tr->fixed, tr->payFixed, tr->sched + first, tr->nSched - first);
+  }
+  double* exValue = (double*)malloc(nE * nP * sizeof(double));
+  for (size_t k = 0; k < nE; ++k) value_at(m, &tails[k], g, jEx[k], X, NULL, nP, exValue + k * nP);
+  double* strategy = (double*)calloc((nE + 1) * nP, sizeof(double));
+  unsigned char* exercise = (unsigned char*)calloc(nE * nP, 1);
+  double *realised = (double*)calloc(nP, sizeof(double)), *target = (double*)malloc(nP * sizeof(double));
+  double* x = (double*)malloc(nP * sizeof(double));
+  unsigned char* itm = (unsigned char*)malloc(nP);
+  orc_regression reg;
+  for (size_t k = nE; k-- > 0;) {
+    const size_t j = jEx[k];
+    for (size_t p = 0; p < nP; ++p) {
+      x[p] = X[p * nT + j];
+      target[p] = realised[p] / Dm[p * nT + j];
+      itm[p] = exValue[k * nP + p] > 0.0;
+    }
+    orc_reg_fit(&reg, tr->degree, x, target, itm, nP);
+    for (size_t p = 0; p < nP; ++p) {
+      const double e = exValue[k * nP + p];
+      if (e > 0.0 && e > orc_reg_predict(&reg, x[p])) exercise[k * nP + p] = 1, realised[p] = Dm[p * nT + j] * e;
+    }
+    memcpy(strategy + k * nP, realised, nP * sizeof(double));
+  }
+  for (size_t p = 0; p < nP; ++p) {
+    exIndex[p] = -1.0;
+    for (size_t k = 0; k < nE; ++k)
+      if (exercise[k * nP + p]) {
+        exIndex[p] = (double)k;
+        break;
+      }
+  }
+  double *cont = (double*)malloc(nP * sizeof(double)), *tailv = (double*)malloc(nE * nP * sizeof(double));
+  for (size_t j = 0; j < nT; ++j) {
+    const double t = g->t[j];
+    size_t nextK = 0;
+    while (nextK < nE && tr->ex[nextK] <= t + 1e-10) ++nextK;
+    if (nextK < nE) {
+      for (size_t p = 0; p < nP; ++p) x[p] = X[p * nT + j], target[p] = strategy[nextK * nP + p] / Dm[p * nT + j];
+      orc_reg_fit(&reg, tr->degree, x, target, NULL, nP);
+      for (size_t p = 0; p < nP; ++p) {
+        const double c = orc_reg_predict(&reg, x[p]);
+        cont[p] = c > 0.0 ? c : 0.0;
+      }
+    } else {
+      for (size_t p = 0; p < nP; ++p) cont[p] = 0.0;
+    }
+    if (tr->physical)
+      for (size_t k = 0; k < nextK; ++k) value_at(m, &tails[k], g, j, X, NULL, nP, tailv + k * nP);
+    for (size_t p = 0; p < nP; ++p) {
+      const double k = exIndex[p];
+      double v;
+      if (k >= 0.0 && (size_t)k < nextK) v = tr->physical ? tailv[(size_t)k * nP + p] : 0.0;
+      else v = cont[p];
+      out[p * nT + j] = tr->position * v;
+    }
+  }
+  for (size_t k = 0; k < nE; ++k) free(tails[k].sched);
+  free(tails), free(jEx), free(exValue), free(strategy), free(exercise), free(realised), free(target), free(x);
+  free(itm), free(cont), free(tailv);
 }
 
 static double required_collateral(double v, double hc, double ho) {
@@ -542,13 +638,14 @@ static void free_model(Model* m) {
   free(m->assets), free(m->credits), free(m->corr), free(m->base);
 }
 static void free_netting(Netting* n) {
-  for (size_t k = 0; k < n->nTr; ++k) free(n->tr[k].sched);
+  for (size_t k = 0; k < n->nTr; ++k) free(n->tr[k].sched), free(n->tr[k].ex);
   free(n->tr);
 }
 
 int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, double pfeQuantile, const double* z,
                    size_t streams, size_t cap, double* times, uint64_t* reporting, size_t* sizes, double* profile,
-                   double* netted, double* collateral, double* deflator, double* survival, char* err, size_t errLen) {
+                   double* netted, double* collateral, double* deflator, double* survival, double* exercise, char* err,
+                   size_t errLen) {
   Model m;
   Netting n;
   int rc = read_model(model, nm, &m, err, errLen);
@@ -556,7 +653,7 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
   rc = read_netting(ns, nn, &n, err, errLen);
   if (rc) return free_model(&m), free_netting(&n), rc;
   for (size_t k = 0; k < n.nTr; ++k)
-    if (n.tr[k].kind != 0 && n.tr[k].asset >= m.nA) {
+    if ((n.tr[k].kind == 1 || n.tr[k].kind == 2) && n.tr[k].asset >= m.nA) {
       free_model(&m), free_netting(&n);
       return fail(err, errLen, "ScenarioSet: unknown asset");
     }
@@ -564,7 +661,7 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
   /* Reporting grid: base grid with every trade's event times; simulation grid: plus t - MPR under a CSA
    * (exposure_engine.cpp:35-48, time_grid.cpp:44-55). */
   size_t nEv = m.nBase;
-  for (size_t k = 0; k < n.nTr; ++k) nEv += n.tr[k].kind == 0 ? n.tr[k].nSched : 1;
+  for (size_t k = 0; k < n.nTr; ++k) nEv += n.tr[k].kind == 0 ? n.tr[k].nSched : n.tr[k].kind == 3 ? n.tr[k].nSched + n.tr[k].nEx : 1;
   double* ev = (double*)malloc((nEv + 1) * sizeof(double));
   size_t q = 0;
   for (size_t k = 0; k < m.nBase; ++k) ev[q++] = m.base[k];
@@ -573,10 +670,12 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
   q = base.n;
   free(base.t);
   for (size_t k = 0; k < n.nTr; ++k) {
-    if (n.tr[k].kind == 0)
+    if (n.tr[k].kind == 0 || n.tr[k].kind == 3) {
       for (size_t i = 0; i < n.tr[k].nSched; ++i) ev[q++] = n.tr[k].sched[i];
-    else
+      for (size_t i = 0; n.tr[k].kind == 3 && i < n.tr[k].nEx; ++i) ev[q++] = n.tr[k].ex[i];
+    } else {
       ev[q++] = n.tr[k].maturity;
+    }
   }
   const Grid rep = make_grid(ev, q);
   free(ev);
@@ -666,12 +765,24 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
   {
     double* V = (double*)calloc(nP * nT, sizeof(double));
     double* slice = (double*)malloc(nP * sizeof(double));
-    for (size_t k = 0; k < n.nTr; ++k)
+    double* cube = (double*)malloc(nP * nT * sizeof(double));
+    double* exIdx = (double*)malloc(nP * sizeof(double));
+    size_t berm = 0;
+    for (size_t k = 0; k < n.nTr; ++k) {
+      if (n.tr[k].kind == 3) {
+        bermudan_cube(&m, &n.tr[k], &sim, X, Dm, nP, cube, exIdx);
+        if (exercise) memcpy(exercise + berm * nP, exIdx, nP * sizeof(double));
+        ++berm;
+      }
       for (size_t j = 0; j < nT; ++j) {
-        value_at(&m, &n.tr[k], &sim, j, X, S, nP, slice);
+        if (n.tr[k].kind == 3)
+          for (size_t p = 0; p < nP; ++p) slice[p] = cube[p * nT + j];
+        else
+          value_at(&m, &n.tr[k], &sim, j, X, S, nP, slice);
         for (size_t p = 0; p < nP; ++p) V[p * nT + j] = k == 0 ? slice[p] : V[p * nT + j] + slice[p];
       }
-    free(slice);
+    }
+    free(slice), free(cube), free(exIdx);
     double* C = (double*)calloc(nP * nT, sizeof(double));
     if (n.csa.has) {
       double* price = NULL;

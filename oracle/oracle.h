@@ -5,8 +5,10 @@
  *                     fused-exposure per path, workgroup tree reduction, compensated sum over
  *                     workgroups (src/gpu/fused_reference.cpp:198-607), with the row statistics'
  *                     quantile computed exactly as ccr::quantile (include/ccr/core/math.hpp:39-47).
+ *   orc_amc_states, orc_fit_amc   the AMC state pass and the Longstaff-Schwartz fit of a plan's Bermudans
+ *                     (fused_reference.cpp:609-626, fused_exposure.cpp:103-156; amc_oracle.c).
  *   orc_engine_run    the FP64 exposure engine (src/exposure/exposure_engine.cpp:50-81) on injected
- *                     normals: scenario generation, swap / forward / option valuation, netting,
+ *                     normals: scenario generation, swap / forward / option / Bermudan valuation, netting,
  *                     collateral, exposure profile.
  *   orc_quantile, orc_collateral, orc_profile, orc_unilateral_cva, orc_bilateral_cva: the building
  *                     blocks (math.hpp:39, collateral.cpp:10-47, exposure_profile.cpp:10-60, cva.cpp:11-48).
@@ -32,13 +34,28 @@ int orc_amc_states(const uint32_t* header, const uint32_t* indices, const float*
                    const float* terms, uint32_t rowsTotal, const uint32_t* offsets, float* x, float* deflator,
                    float* exercise, char* err, size_t errLen);
 
+/* PolynomialRegression (regression.cpp:29-98): predict(x) = sum_d coef[d] ((x - center) / scale)^d. */
+typedef struct orc_regression {
+  double center, scale, coef[4];
+  int ncoef;
+} orc_regression;
+void orc_reg_fit(orc_regression* r, int degree, const double* x, const double* y, const unsigned char* mask, size_t n);
+double orc_reg_predict(const orc_regression* r, double x);
+
+/* fitAmc (fused_exposure.cpp:103-156): fills the policy and continuation records of terms in place, from the
+ * AMC pass of the plan; degrees[b] is the regression degree of Bermudan b. */
+int orc_fit_amc(const uint32_t* header, const uint32_t* indices, const float* params, const float* steps, float* terms,
+                uint32_t rowsTotal, const uint32_t* degrees, size_t numBermudans, char* err, size_t errLen);
+
 /* Engine on injected normals z[((j - 1) * nNormals + k) * streams + s].  Sizes: sizes[0] = nT (simulation
  * dates), sizes[1] = nR; times has room for cap dates, reporting for cap indices.  Per-path outputs
- * (nullable) are [path][date] over the simulation grid; survival is that of credit 0.  profile holds
- * EV, EE, ENE, PFE, EE*, ENE* over the reporting dates (6 * nR). */
+ * (nullable) are [path][date] over the simulation grid; survival is that of credit 0; exercise is
+ * [bermudan][path], the first exercise taken (-1: never).  profile holds EV, EE, ENE, PFE, EE*, ENE* over
+ * the reporting dates (6 * nR). */
 int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, double pfeQuantile, const double* normals,
                    size_t streams, size_t cap, double* times, uint64_t* reporting, size_t* sizes, double* profile,
-                   double* netted, double* collateral, double* deflator, double* survival, char* err, size_t errLen);
+                   double* netted, double* collateral, double* deflator, double* survival, double* exercise, char* err,
+                   size_t errLen);
 
 double orc_quantile(const double* v, size_t n, double p);
 /* values, unitPrice (nullable): [path][date]; out: [path][date] collateral held. */

@@ -46,9 +46,13 @@ def lib() -> C.CDLL:
                                     C.c_void_p, C.c_char_p, sz]
         L.orc_amc_states.restype = C.c_int
         L.orc_amc_states.argtypes = [_up, _up, _fp, _fp, _fp, C.c_uint32, _up, _fp, _fp, _fp, C.c_char_p, sz]
+        L.orc_reg_fit.restype = None
+        L.orc_reg_fit.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_void_p, sz]
+        L.orc_fit_amc.restype = C.c_int
+        L.orc_fit_amc.argtypes = [_up, _up, _fp, _fp, _fp, C.c_uint32, _up, sz, C.c_char_p, sz]
         L.orc_engine_run.restype = C.c_int
         L.orc_engine_run.argtypes = [_dp, sz, _dp, sz, C.c_double, _dp, sz, sz, _dp, _u64p, C.POINTER(C.c_size_t), _dp,
-                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, sz]
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, sz]
         L.orc_quantile.restype = C.c_double
         L.orc_quantile.argtypes = [_dp, sz, C.c_double]
         L.orc_collateral.restype = C.c_int
@@ -125,6 +129,32 @@ def amc_states(plan):
     return x.reshape(nT, nP), d.reshape(nT, nP), ex[: rows * nP].reshape(rows, nP)
 
 
+class _Regression(C.Structure):
+    _fields_ = [("center", C.c_double), ("scale", C.c_double), ("coef", C.c_double * 4), ("ncoef", C.c_int)]
+
+
+def fit_regression(x, y, degree: int, mask=None) -> dict:
+    """PolynomialRegression::fit (regression.cpp:33-80): center, scale and coefficients in the standardised
+    regressor."""
+    xs, ys = np.ascontiguousarray(x, np.float64), np.ascontiguousarray(y, np.float64)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    r = _Regression()
+    lib().orc_reg_fit(C.byref(r), degree, xs, ys, None if m is None else m.ctypes.data_as(C.c_void_p), xs.size)
+    return {"center": r.center, "scale": r.scale, "ncoef": r.ncoef, "coef": list(r.coef)[: r.ncoef]}
+
+
+def fit_amc(plan, degrees) -> np.ndarray:
+    """fitAmc on a plan's tables: a copy of the term table with the Bermudans' policy and continuation
+    coefficients fitted (degrees[b]: regression degree of Bermudan b)."""
+    terms = _f32(plan.terms).copy()
+    deg = np.ascontiguousarray(degrees, np.uint32)
+    e = _err()
+    if lib().orc_fit_amc(np.ascontiguousarray(plan.header, np.uint32), np.ascontiguousarray(plan.indices, np.uint32),
+                         _f32(plan.params), _f32(plan.steps), terms, plan.rows_total, deg, deg.size, e, 512):
+        raise ValueError(e.value.decode())
+    return terms
+
+
 @dataclass
 class EngineResult:
     times: np.ndarray       # simulation grid
@@ -135,6 +165,7 @@ class EngineResult:
     deflator: np.ndarray
     survival: np.ndarray    # credit 0, [path][date]
     pathwise_cva_04: float
+    exercise: np.ndarray    # [bermudan][path]: first exercise taken, -1 never
 
 
 def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarray, streams: int,
@@ -146,11 +177,12 @@ def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarra
     sizes = (C.c_size_t * 2)()
     prof = np.zeros(6 * cap)
     mats = [np.zeros(num_paths * cap) for _ in range(4)]
+    exercise = np.full(4 * num_paths, -1.0)
     e = _err()
     z = np.ascontiguousarray(normals, np.float64)
     m, n = np.ascontiguousarray(model, np.float64), np.ascontiguousarray(ns, np.float64)
     rc = lib().orc_engine_run(m, m.size, n, n.size, pfe, z, streams, cap, times, rep, sizes, prof,
-                              *[a.ctypes.data_as(C.c_void_p) for a in mats], e, 512)
+                              *[a.ctypes.data_as(C.c_void_p) for a in mats], exercise.ctypes.data_as(C.c_void_p), e, 512)
     if rc:
         raise ValueError(e.value.decode())
     nT, nR = sizes[0], sizes[1]
@@ -161,7 +193,8 @@ def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarra
     expo = np.ascontiguousarray(netted - coll)
     pcva = lib().orc_pathwise_cva(expo, np.ascontiguousarray(defl), np.ascontiguousarray(surv), num_paths, nT, reporting,
                                   nR, 0.4)
-    return EngineResult(times[:nT].copy(), reporting.astype(np.int64), p, netted, coll, defl, surv, pcva)
+    return EngineResult(times[:nT].copy(), reporting.astype(np.int64), p, netted, coll, defl, surv, pcva,
+                        exercise.reshape(4, num_paths))
 
 
 def quantile(values, p: float) -> float:

@@ -261,3 +261,61 @@ def test_building_blocks_are_the_reference():
     assert restated.unilateral_cva(t, np.abs(v[0]), pil, haz, 0.4) == ref.unilateral_cva(t, np.abs(v[0]), pil, haz, 0.4)
     assert restated.bilateral_cva(t, np.abs(v[0]), -np.abs(v[1]), (pil, haz), ([2.0], [0.01]), 0.4, 0.3) == \
         ref.bilateral_cva(t, np.abs(v[0]), -np.abs(v[1]), (pil, haz), ([2.0], [0.01]), 0.4, 0.3)
+
+
+# ------------------------------------------------------------------ the Longstaff-Schwartz fit
+def test_fit_restatement_reproduces_golden_bermudan_terms():
+    """fitAmc restated (oracle/amc_oracle.c) on the fixture's tables with the fitted records cleared gives back the
+    reference's fitted records bit for bit (degrees 2 and 3, the fixture's Bermudans)."""
+    f = _load("fused_bermudan")
+    terms = f["terms"].reshape(-1, 8).copy()
+    kind = terms[:, 0].astype(np.int64) & 15
+    fitted = (kind == 6) | (kind == 7)
+    terms[fitted, 2:] = 0.0
+    p = gpu.Plan.from_arrays(f["header"], f["indices"], f["params"], f["steps"], terms.reshape(-1), f["requests"],
+                             int(f["rows_total"]), int(f["num_outputs"]), f["times"], f["reporting"])
+    out = restated.fit_amc(p, [2, 3])
+    assert np.array_equal(_bits(out), _bits(f["terms"]))
+
+
+def test_regression_known_answers():
+    """PolynomialRegression (tests/test_core.cpp:37-54 of the reference): a cubic on 50 points is recovered
+    (prediction at 0.7 within 1e-8), and a degenerate regressor falls back to the sample mean."""
+    x = np.array([-2.0 + 0.08 * i for i in range(50)])
+    y = 1.0 - 2.0 * x + 0.5 * x ** 3
+    t = restated.fit_regression(x, y, 3)
+    assert t["ncoef"] == 4
+    z = (0.7 - t["center"]) / t["scale"]
+    pred = sum(c * z ** d for d, c in enumerate(t["coef"]))
+    assert abs(pred - (1.0 - 1.4 + 0.5 * 0.343)) <= 1e-8
+    flat = restated.fit_regression(np.zeros(10), np.arange(1.0, 11.0), 3)
+    assert flat["ncoef"] == 1 and abs(flat["coef"][0] - 5.5) <= 1e-12
+
+
+@needs_ref
+@pytest.mark.parametrize("physical", [True, False])
+def test_fit_restatement_is_the_reference_fit(physical):
+    m, ns = gpu_setup(1700, physical)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=physical, degree=3))
+    ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=not physical, position=-0.5, degree=1, pay=True))
+    ns.trades.append(bermudan(exercise=(1.0,), physical=physical, degree=2))
+    r = ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(S.Options()))
+    p = gpu.compile(m, ns)  # this package's tables: the records still unfitted
+    out = restated.fit_amc(p, p.amc_degrees)
+    assert np.array_equal(_bits(out), _bits(r.terms))
+
+
+@needs_ref
+@pytest.mark.parametrize("csa", [False, True])
+def test_engine_bermudans_are_the_reference_engine(csa):
+    m, ns = gpu_setup(1200, csa)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=True, degree=2))
+    ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=False, position=-0.5, degree=3))
+    p = gpu.compile(m, ns)
+    streams = (m.num_paths + 1) // 2
+    z = np.random.default_rng(4).standard_normal((p.num_dates - 1) * int(p.header[5]) * streams)
+    e1 = ref.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams)
+    e2 = restated.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams, m.num_paths)
+    assert np.array_equal(e1.netted, e2.netted) and np.array_equal(e1.collateral, e2.collateral)
+    for k in e1.profile:
+        assert np.array_equal(e1.profile[k], e2.profile[k]), k

@@ -1,0 +1,250 @@
+// Longstaff-Schwartz fit of the Bermudans of a plan on the GPU: the policy (exercise decision) and the
+// continuation regressions that the fused kernel's AMC terms evaluate.
+//
+// It follows the reference's compile-time fit (fitAmc, src/gpu/fused_exposure.cpp:103-156, with
+// PolynomialRegression, src/core/regression.cpp:29-98): backwards over the exercise dates, a masked
+// (in-the-money) regression of the deflated realised value on the standardised short-rate state, the
+// exercise rule "exercise value > 0 and > regression", and on every date with an exercise ahead an
+// unmasked regression of the value of the policy from the next exercise on.  The degree falls back as the
+// reference's does (degenerate regressor, too few samples) and the ridge is 1e-12 n.
+//
+// B200 layout: one thread-block cluster per Bermudan.  Each CTA owns a fixed strided share of the paths
+// and keeps the realised values of its paths in a global scratch row that only it touches; every pass
+// (moments, Gram, exercise update) is a streaming read of the AMC pass's x, deflator and exercise values.
+// The per-CTA sums are reduced through distributed shared memory on rank 0 in rank order, so the fit is
+// deterministic.  Rank 0 solves the normal equations by an FP64 Cholesky factorisation and broadcasts the
+// coefficients back through DSMEM.  The Gram of a one-dimensional monomial basis is a handful of power
+// moments, an FP64 CUDA-core reduction: the work per path is ~30 flops against 12-20 bytes read.
+#include <cooperative_groups.h>
+
+#include "zk_device.cuh"
+#include "zk_kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace zk {
+
+namespace {
+
+constexpr int kFitThreads = 512;
+constexpr int kFitWarps = kFitThreads / 32;
+constexpr int kMomentVals = 4;   // count, sum x, sum x^2, sum y
+constexpr int kGramVals = 14;    // 10 Gram entries (lower triangle, degree 3) + 4 right-hand sides
+
+struct FitSmem {
+  double warpBuf[kFitWarps][kGramVals];
+  double part[kGramVals];   // this CTA's sums
+  double res[8];            // rank 0: center, scale, degree, c0..c3, status
+};
+
+// Sums V values over the CTA: a fixed shuffle tree per warp, then the warps in order.
+template <int V>
+__device__ __forceinline__ void blockSum(double (&v)[V], FitSmem& s) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < V; ++i)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_xor_sync(0xFFFFFFFFu, v[i], off);
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < V; ++i) s.warpBuf[warp][i] = v[i];
+  __syncthreads();
+  if (threadIdx.x < V) {
+    double t = 0.0;
+    for (int w = 0; w < kFitWarps; ++w) t += s.warpBuf[w][threadIdx.x];
+    s.part[threadIdx.x] = t;
+  }
+}
+
+// Rank 0 sums the cluster's parts in rank order into `tot` (its own shared memory).
+template <int V>
+__device__ __forceinline__ void clusterSum(cg::cluster_group& cl, FitSmem& s, double* tot) {
+  cl.sync();
+  if (cl.block_rank() == 0 && threadIdx.x < V) {
+    double t = 0.0;
+    for (unsigned r = 0; r < cl.num_blocks(); ++r) t += cl.map_shared_rank(s.part, r)[threadIdx.x];
+    tot[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// z^0 .. z^d by repeated multiplication, as the reference's design rows.
+__device__ __forceinline__ void powers(double z, int d, double (&pw)[4]) {
+  pw[0] = 1.0;
+#pragma unroll
+  for (int i = 1; i < 4; ++i) pw[i] = i <= d ? pw[i - 1] * z : 0.0;
+}
+
+__device__ __forceinline__ double predict(const double* res, double x) {
+  const double z = (x - res[0]) / res[1];
+  const int d = static_cast<int>(res[2]);
+  double v = 0.0;
+  for (int i = d; i >= 0; --i) v = v * z + res[3 + i];
+  return v;
+}
+
+// One regression of y = realised / D on x over the CTA's paths (masked by E > 0 when E is given); the
+// result lands in every CTA's `res` copy and, from rank 0, in out[0..5] = center, scale, c0..c3.
+template <typename R>
+__device__ void fitOnce(cg::cluster_group& cl, FitSmem& s, double* res, const R* __restrict__ X, const R* __restrict__ Dj,
+                        const R* __restrict__ Ek, const double* __restrict__ realised, uint32_t nP, int degree, uint32_t first,
+                        uint32_t stride, double* out, uint32_t* err) {
+  __shared__ double tot[kGramVals];
+  // Pass 1: count, sum x, sum x^2, sum y.
+  double m[kMomentVals] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t p = first; p < nP; p += stride) {
+    if (Ek && !(Ek[p] > R(0))) continue;
+    const double x = static_cast<double>(X[p]);
+    m[0] += 1.0, m[1] += x, m[2] += x * x, m[3] += realised[p] / static_cast<double>(Dj[p]);
+  }
+  blockSum(m, s);
+  clusterSum<kMomentVals>(cl, s, tot);
+  if (cl.block_rank() == 0 && threadIdx.x == 0) {
+    const double n = tot[0];
+    double center = 0.0, scale = 1.0;
+    int d = degree;
+    for (int i = 0; i < 4; ++i) s.res[3 + i] = 0.0;
+    if (n == 0.0) {
+      d = -1;  // no sample: the regression predicts 0
+    } else {
+      center = tot[1] / n;
+      const double var = tot[2] / n - center * center;
+      scale = sqrt(var > 0.0 ? var : 0.0);
+      if (scale < 1e-12 * fmax(1.0, fabs(center))) d = 0;
+      if (n < 2.0 * (d + 1)) d = n >= 4.0 ? static_cast<int>(n) / 2 - 1 : 0;
+      if (d == 0) scale = 1.0, s.res[3] = tot[3] / n;
+    }
+    s.res[0] = center, s.res[1] = scale, s.res[2] = d < 0 ? 0.0 : static_cast<double>(d), s.res[7] = static_cast<double>(d);
+  }
+  cl.sync();
+  const double* r0 = cl.map_shared_rank(s.res, 0);
+  if (threadIdx.x < 8) res[threadIdx.x] = r0[threadIdx.x];
+  __syncthreads();
+  const int d = static_cast<int>(res[7]);
+  if (d > 0) {
+    // Pass 2: Gram (lower triangle) and right-hand side of the standardised design.
+    double g[kGramVals];
+#pragma unroll
+    for (int i = 0; i < kGramVals; ++i) g[i] = 0.0;
+    const double c = res[0], sc = res[1];
+    for (uint32_t p = first; p < nP; p += stride) {
+      if (Ek && !(Ek[p] > R(0))) continue;
+      double pw[4];
+      powers((static_cast<double>(X[p]) - c) / sc, d, pw);
+      const double y = realised[p] / static_cast<double>(Dj[p]);
+      int k = 0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = 0; b <= a; ++b) g[k++] += pw[a] * pw[b];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) g[10 + a] += pw[a] * y;
+    }
+    blockSum(g, s);
+    clusterSum<kGramVals>(cl, s, tot);
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      // Normal equations with the ridge, by FP64 Cholesky: G = L L^T, L y = b, L^T c = y.
+      const int k = d + 1;
+      double A[4][4], L[4][4] = {}, b[4], yv[4];
+      int q = 0;
+      for (int a = 0; a < 4; ++a)
+        for (int bb = 0; bb <= a; ++bb) A[a][bb] = A[bb][a] = tot[q++];
+      const double ridge = 1e-12 * tot[0];
+      for (int a = 0; a < k; ++a) A[a][a] += ridge, b[a] = tot[10 + a];
+      bool ok = true;
+      for (int i = 0; i < k; ++i)
+        for (int j = 0; j <= i; ++j) {
+          double v = A[i][j];
+          for (int m2 = 0; m2 < j; ++m2) v -= L[i][m2] * L[j][m2];
+          if (i == j) {
+            if (!(v > 0.0)) ok = false, v = 1.0;
+            L[i][i] = sqrt(v);
+          } else {
+            L[i][j] = v / L[j][j];
+          }
+        }
+      for (int i = 0; i < k; ++i) {
+        double v = b[i];
+        for (int j = 0; j < i; ++j) v -= L[i][j] * yv[j];
+        yv[i] = v / L[i][i];
+      }
+      for (int i = k - 1; i >= 0; --i) {
+        double v = yv[i];
+        for (int j = i + 1; j < k; ++j) v -= L[j][i] * s.res[3 + j];
+        s.res[3 + i] = v / L[i][i];
+      }
+      if (!ok) atomicExch(err, kDevBadTerm);
+    }
+    cl.sync();
+    if (threadIdx.x < 4) res[3 + threadIdx.x] = cl.map_shared_rank(s.res, 0)[3 + threadIdx.x];
+    __syncthreads();
+  }
+  if (cl.block_rank() == 0 && threadIdx.x == 0) {
+    out[0] = res[0], out[1] = res[1];
+    for (int i = 0; i < 4; ++i) out[2 + i] = res[3 + i];
+  }
+  // No CTA may start the next pass (and overwrite its part) before rank 0 has read every part, nor may
+  // rank 0 overwrite res before every CTA has copied it: the syncs of the next fit order both.
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __restrict__ jobs, const R* __restrict__ x,
+                                                             const R* __restrict__ D, const R* __restrict__ E,
+                                                             const uint32_t* __restrict__ contDates, double* __restrict__ realised,
+                                                             double* __restrict__ out, uint32_t* err) {
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ FitSmem s;
+  __shared__ double res[8];
+  const uint32_t job = blockIdx.x / cl.num_blocks();
+  const AmcFitJob J = jobs[job];
+  const uint32_t nP = J.nP, stride = cl.num_blocks() * kFitThreads, first = cl.block_rank() * kFitThreads + threadIdx.x;
+  double* rz = realised + static_cast<size_t>(job) * nP;
+  for (uint32_t p = first; p < nP; p += stride) rz[p] = 0.0;
+  for (int k = static_cast<int>(J.nE) - 1; k >= 0; --k) {
+    const size_t j = J.exDate[k];
+    const R* Ek = E + static_cast<size_t>(J.eRow + k) * nP;
+    fitOnce<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, nP, static_cast<int>(J.degree), first, stride,
+               out + static_cast<size_t>(J.slotBase + k) * 6, err);
+    // Exercise where the exercise value beats the regression: realised = D e.
+    for (uint32_t p = first; p < nP; p += stride) {
+      const double e = static_cast<double>(Ek[p]);
+      if (e > 0.0 && e > predict(res, static_cast<double>(x[j * nP + p]))) rz[p] = static_cast<double>(D[j * nP + p]) * e;
+    }
+    // Continuation on the dates whose next exercise is k: exDate[k - 1] <= date < exDate[k].
+    const uint32_t lo = k > 0 ? J.exDate[k - 1] : 0u;
+    for (uint32_t i = 0; i < J.contCount; ++i) {
+      const uint32_t jc = contDates[J.contBegin + i];
+      if (jc < lo || jc >= j) continue;
+      fitOnce<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr), rz,
+                 nP, static_cast<int>(J.degree), first, stride, out + static_cast<size_t>(J.slotBase + J.nE + i) * 6, err);
+    }
+  }
+  cl.sync();  // rank 0's shared memory stays alive until every CTA of the cluster is done reading it
+}
+
+}  // namespace
+
+template <typename R>
+cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
+                         double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream) {
+  if (numJobs == 0) return cudaSuccess;
+  if (clusterSize < 1 || clusterSize > 8) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(numJobs * clusterSize);
+  cfg.blockDim = dim3(kFitThreads);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = clusterSize, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, amcFitKernel<R>, jobs, x, D, E, contDates, realised, out, err);
+}
+
+template cudaError_t launchAmcFit<float>(const AmcFitJob*, uint32_t, const float*, const float*, const float*, const uint32_t*,
+                                         double*, double*, uint32_t*, uint32_t, cudaStream_t);
+template cudaError_t launchAmcFit<double>(const AmcFitJob*, uint32_t, const double*, const double*, const double*, const uint32_t*,
+                                          double*, double*, uint32_t*, uint32_t, cudaStream_t);
+
+}  // namespace zk

@@ -425,9 +425,9 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   }
   if (sink) {
     const auto& P = B->plans[0];
-    B->sinkOff[0] = take(static_cast<size_t>(P.nT) * P.nP * 4);
-    B->sinkOff[1] = take(static_cast<size_t>(P.nT) * P.nP * 4);
-    B->sinkOff[2] = take(static_cast<size_t>(std::max<uint32_t>(P.exerciseRows, 1)) * P.nP * 4);
+    B->sinkOff[0] = take(static_cast<size_t>(P.nT) * P.nP * sizeof(R));
+    B->sinkOff[1] = take(static_cast<size_t>(P.nT) * P.nP * sizeof(R));
+    B->sinkOff[2] = take(static_cast<size_t>(std::max<uint32_t>(P.exerciseRows, 1)) * P.nP * sizeof(R));
   }
   B->outBegin = off;
   for (size_t i = 0; i < nPlans; ++i) {
@@ -478,9 +478,9 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
       A.offCall = P.offCall, A.offRep = P.offRep, A.nSlots = P.nSlots, A.ring = P.ring;
       A.usesAssets = P.usesAssets ? 1u : 0u;
       if (B.sink) {
-        A.sinkX = static_cast<float*>(dptr(B.sinkOff[0]));
-        A.sinkD = static_cast<float*>(dptr(B.sinkOff[1]));
-        A.sinkEx = static_cast<float*>(dptr(B.sinkOff[2]));
+        A.sinkX = static_cast<R*>(dptr(B.sinkOff[0]));
+        A.sinkD = static_cast<R*>(dptr(B.sinkOff[1]));
+        A.sinkEx = static_cast<R*>(dptr(B.sinkOff[2]));
         A.sinkRowOfBermudan = static_cast<const uint32_t*>(dptr(B.bermRowOff));
       }
     }
@@ -673,6 +673,104 @@ zk_status runInjected(zk_context* ctx, const ViewT* plan, const double* normals,
     return record(ctx, f);
   }
 }
+
+// The Longstaff-Schwartz fit of a plan's Bermudans (fitAmc, src/gpu/fused_exposure.cpp:103-156): the AMC
+// state pass of the fused kernel (x, deflator, exercise values on the device), then one thread-block
+// cluster per Bermudan fits the policy of every exercise and the continuation of every date, and the
+// fitted records are written into a copy of the plan's term table.
+template <typename R, typename ViewT>
+zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size_t streams, const uint32_t* degrees,
+                 size_t numBermudans, R* termsOut, size_t termsLen) {
+  void* dmem = nullptr;
+  try {
+    requireCtx(ctx);
+    if (!plan || !termsOut || (numBermudans && !degrees)) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (termsLen != plan->terms_len) throw fail(ZK_ERR_INVALID_ARGUMENT, "terms_out holds %zu values, the plan %zu", termsLen, plan->terms_len);
+    auto B = build<R>(ctx, {viewOf(*plan)}, true, normals, streams);
+    const auto& P = B->plans[0];
+    const View<R> v = viewOf(*plan);
+    if (numBermudans != P.nBerm)
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "the plan has %u Bermudans, not %zu", P.nBerm, numBermudans);
+    // Layout of the regressions: policy term and date of each exercise, continuation term of each date.
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> decide(numBermudans), cont(numBermudans);
+    for (uint32_t j = 0; j < P.nT; ++j)
+      for (uint32_t t = v.indices[j]; t < v.indices[j + 1]; ++t) {
+        const auto code = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]);
+        const uint32_t kind = code & 15u, b = (code >> 8u) & 15u, e = code >> 12u;
+        if (kind != 6u && kind != 7u) continue;
+        if (b >= numBermudans) throw fail(ZK_ERR_INVALID_PLAN, "an AMC term of Bermudan %u", b);
+        if (kind == 6u) {
+          if (e >= static_cast<uint32_t>(kMaxExercises)) throw fail(ZK_ERR_INVALID_PLAN, "exercise index %u", e);
+          if (decide[b].size() <= e) decide[b].resize(e + 1, {0xFFFFFFFFu, 0u});
+          decide[b][e] = {t, j};
+        } else {
+          cont[b].push_back({j, t});
+        }
+      }
+    std::vector<AmcFitJob> jobs(numBermudans);
+    std::vector<uint32_t> contDates;
+    uint32_t slots = 0, eRow = 0;
+    for (size_t b = 0; b < numBermudans; ++b) {
+      if (degrees[b] > 3) throw fail(ZK_ERR_INVALID_ARGUMENT, "AMC regression degree %u above 3", degrees[b]);
+      AmcFitJob& J = jobs[b];
+      J = AmcFitJob{};
+      J.nP = P.nP, J.nT = P.nT, J.nE = static_cast<uint32_t>(decide[b].size()), J.degree = degrees[b];
+      if (J.nE != P.bermRows[b]) throw fail(ZK_ERR_INVALID_PLAN, "Bermudan %zu: inconsistent exercise terms", b);
+      J.eRow = eRow, eRow += J.nE;
+      J.slotBase = slots, slots += J.nE + static_cast<uint32_t>(cont[b].size());
+      for (uint32_t e = 0; e < J.nE; ++e) {
+        if (decide[b][e].first == 0xFFFFFFFFu || (e > 0 && decide[b][e].second <= decide[b][e - 1].second))
+          throw fail(ZK_ERR_INVALID_PLAN, "Bermudan %zu: exercise %u missing or out of order", b, e);
+        J.exDate[e] = decide[b][e].second;
+      }
+      J.contBegin = static_cast<uint32_t>(contDates.size()), J.contCount = static_cast<uint32_t>(cont[b].size());
+      for (const auto& c : cont[b]) contDates.push_back(c.first);
+    }
+    std::copy(v.terms, v.terms + termsLen, termsOut);
+    if (numBermudans == 0) return ZK_OK;
+    upload(*B, ctx, true, normals, streams);
+    execute(*B);
+    // Device scratch: jobs, continuation dates, realised values per Bermudan, fitted records.
+    const size_t jobsBytes = jobs.size() * sizeof(AmcFitJob), datesBytes = std::max<size_t>(contDates.size(), 1) * 4;
+    const size_t realisedBytes = numBermudans * static_cast<size_t>(P.nP) * 8, outBytes = static_cast<size_t>(slots) * 6 * 8;
+    const size_t o1 = (jobsBytes + 255) / 256 * 256, o2 = o1 + (datesBytes + 255) / 256 * 256, o3 = o2 + (realisedBytes + 255) / 256 * 256;
+    ZK_CUDA(cudaMalloc(&dmem, o3 + outBytes));
+    unsigned char* d = static_cast<unsigned char*>(dmem);
+    ZK_CUDA(cudaMemcpyAsync(d, jobs.data(), jobsBytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (!contDates.empty()) ZK_CUDA(cudaMemcpyAsync(d + o1, contDates.data(), contDates.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    const uint32_t cluster = P.nP >= 65536 ? 8u : P.nP >= 16384 ? 4u : P.nP >= 4096 ? 2u : 1u;
+    const R* sx = reinterpret_cast<const R*>(B->base + B->sinkOff[0]);
+    const R* sd = reinterpret_cast<const R*>(B->base + B->sinkOff[1]);
+    const R* se = reinterpret_cast<const R*>(B->base + B->sinkOff[2]);
+    ZK_CUDA(launchAmcFit<R>(reinterpret_cast<const AmcFitJob*>(d), static_cast<uint32_t>(numBermudans), sx, sd, se,
+                            reinterpret_cast<const uint32_t*>(d + o1), reinterpret_cast<double*>(d + o2),
+                            reinterpret_cast<double*>(d + o3), ctx->dErr, cluster, ctx->stream));
+    std::vector<double> fitted(static_cast<size_t>(slots) * 6);
+    uint32_t devErr = 0;
+    ZK_CUDA(cudaMemcpyAsync(fitted.data(), d + o3, outBytes, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(&devErr, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    ZK_CUDA(cudaFree(dmem));
+    dmem = nullptr;
+    if (devErr != 0) throw fail(ZK_ERR_CUDA, "the AMC fit reported error %u (normal equations not positive definite)", devErr);
+    // The records as the reference writes them: center, 1 / scale, c0..c3 (fused_exposure.cpp:118-123).
+    auto write = [&](uint32_t term, const double* f) {
+      R* r = termsOut + static_cast<size_t>(term) * kTermStride;
+      r[2] = static_cast<R>(f[0]);
+      r[3] = static_cast<R>(1.0 / f[1]);
+      for (int i = 0; i < 4; ++i) r[4 + i] = static_cast<R>(f[2 + i]);
+    };
+    for (size_t b = 0; b < numBermudans; ++b) {
+      const AmcFitJob& J = jobs[b];
+      for (uint32_t e = 0; e < J.nE; ++e) write(decide[b][e].first, &fitted[(J.slotBase + e) * 6]);
+      for (uint32_t i = 0; i < J.contCount; ++i) write(cont[b][i].second, &fitted[(J.slotBase + J.nE + i) * 6]);
+    }
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (dmem) cudaFree(dmem);
+    return record(ctx, f);
+  }
+}
 }  // namespace
 
 // ================================================================================================
@@ -772,6 +870,21 @@ zk_status zk_amc_states(zk_context* ctx, const zk_plan_view* plan, float* x, flo
   }
 }
 
+
+zk_status zk_run_plan_rows(zk_context* ctx, const zk_plan_view* plan, zk_output* out, float* rows) {
+  if (!rows) return record(ctx, fail(ZK_ERR_INVALID_ARGUMENT, "null rows buffer"));
+  return runInjected<float>(ctx, plan, nullptr, 0, out, rows);
+}
+
+zk_status zk_fit_amc(zk_context* ctx, const zk_plan_view* plan, const uint32_t* degrees, size_t num_bermudans, float* terms_out,
+                     size_t terms_len) {
+  return fitAmc<float>(ctx, plan, nullptr, 0, degrees, num_bermudans, terms_out, terms_len);
+}
+
+zk_status zk_fit_amc_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams,
+                         const uint32_t* degrees, size_t num_bermudans, double* terms_out, size_t terms_len) {
+  return fitAmc<double>(ctx, plan, normals, streams, degrees, num_bermudans, terms_out, terms_len);
+}
 
 zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams, zk_output_f64* out,
                           double* rows) {

@@ -340,8 +340,8 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
 #pragma unroll
       for (int i = 0; i < PPT; ++i)
         if (act[i]) {
-          A.sinkX[static_cast<size_t>(j) * nP + pth[i]] = static_cast<float>(x[i]);
-          A.sinkD[static_cast<size_t>(j) * nP + pth[i]] = static_cast<float>(D[i]);
+          A.sinkX[static_cast<size_t>(j) * nP + pth[i]] = x[i];
+          A.sinkD[static_cast<size_t>(j) * nP + pth[i]] = D[i];
         }
 
     R value[PPT], ev[4][PPT];
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
           for (int i = 0; i < PPT; ++i) {
             const R e = pick4<R, PPT>(ev, bm, i);
             if (kSink) {
-              if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = static_cast<float>(e);
+              if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
             } else if (pick4<R, PPT>(ex, bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
               const R v = static_cast<R>(extra);
               if (bm == 0) ex[0][i] = v;

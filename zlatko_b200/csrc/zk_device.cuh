@@ -85,10 +85,10 @@ struct NsArgs {
   uint32_t offCall, offRep, nSlots, ring;
   uint32_t usesAssets;     // some term reads an asset level
   uint32_t pad0;
-  // AMC state pass (zk_amc_states): x / deflator [date][path] and exercise values [row][path].
-  float* sinkX;
-  float* sinkD;
-  float* sinkEx;
+  // AMC state pass (zk_amc_states, zk_fit_amc): x / deflator [date][path] and exercise values [row][path].
+  R* sinkX;
+  R* sinkD;
+  R* sinkEx;
   const uint32_t* sinkRowOfBermudan;  // first exercise row of each Bermudan
 };
 

@@ -41,4 +41,17 @@ struct RowJob {
 template <typename R>
 cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream);
 
+// One Bermudan of the AMC fit (zk_fit_amc): its exercise dates (grid indices, ascending), its first row of
+// exercise values in the AMC pass, the slots of its fitted records (slotBase + k: policy of exercise k;
+// slotBase + nE + i: continuation on date contDates[contBegin + i]) and its regression degree.
+constexpr int kMaxExercises = 64;
+struct AmcFitJob {
+  uint32_t nP, nT, nE, degree, eRow, slotBase, contBegin, contCount;
+  uint32_t exDate[kMaxExercises];
+};
+// One thread-block cluster of clusterSize CTAs per job; out[slot][6] = center, scale, c0..c3.
+template <typename R>
+cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
+                         double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream);
+
 }  // namespace zk

@@ -15,6 +15,7 @@ itself run unchanged.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence
 
@@ -48,6 +49,7 @@ class Plan:
     market_survival: Optional[np.ndarray] = None
     tables64: Optional[Dict[str, np.ndarray]] = None  # double-precision params/steps/terms/requests (zk_compile)
     exercise_rows: int = 0
+    amc_degrees: List[int] = field(default_factory=list)  # regression degree of each Bermudan (zk_fit_amc)
 
     def __post_init__(self):
         self.header = np.ascontiguousarray(self.header, np.uint32)
@@ -107,15 +109,20 @@ class Plan:
                            self.rows_total, self.num_outputs)
 
 
-def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Options] = None) -> Plan:
+def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Options] = None,
+            fit: Optional["Context"] = None) -> Plan:
     """zk_compile: the host plan compiler (a restatement of gpu::compile, src/gpu/fused_exposure.cpp:214).
-    Raises ValueError where the reference throws std::invalid_argument."""
+    Raises ValueError where the reference throws std::invalid_argument.  The reference's compile also fits
+    the Longstaff-Schwartz regressions of the Bermudans; here that is zk_fit_amc on the GPU: pass a Context
+    as `fit` (or call Context.fit_amc on the plan)."""
     options = options or S.Options()
     plan = compile_arrays(S.encode_model(model), S.encode_netting_set(netting_set), S.encode_options(options))
     if model.credits:
         from .summary import hazard_survival
         c = model.credits[options.counterparty]
         plan.market_survival = np.array([hazard_survival(c.pillars, c.hazards, t) for t in plan.times])
+    if fit is not None and plan.amc_degrees:
+        plan = fit.fit_amc(plan)
     return plan
 
 
@@ -152,6 +159,7 @@ def compile_arrays(m: np.ndarray, n: np.ndarray, o: np.ndarray) -> Plan:
                          "requests": arr(v64.requests, v64.requests_len, np.float64)}
         plan.exercise_rows = int(sizes[5])
         plan.market_survival = np.ones(nT)
+        plan.amc_degrees = S.bermudan_degrees(n)
         return plan
     finally:
         L.zk_plan_destroy(h)
@@ -232,9 +240,17 @@ class Context:
         outs = (T * len(plans))(*[T(_ptr(s, ct), s.size, _ptr(v, ct), v.size) for s, v in bufs])
         return outs, bufs
 
-    def run(self, plan: Plan):
-        """zk_run_plan: the drop-in for gpu::runFusedReference.  Returns (sums, values) as float32."""
-        return self.run_many([plan])[0]
+    def run(self, plan: Plan, rows: bool = False):
+        """zk_run_plan: the drop-in for gpu::runFusedReference.  Returns (sums, values) as float32, and with
+        rows=True also the per-path rows [row][path] the fused kernel wrote (zk_run_plan_rows)."""
+        if not rows:
+            return self.run_many([plan])[0]
+        v = plan.view()
+        outs, bufs = self._outputs([plan])
+        r = np.zeros(max(plan.rows_total, 1) * plan.num_paths, np.float32)
+        check(lib().zk_run_plan_rows(self.handle, C.byref(v), outs, r.ctypes.data), self.handle)
+        sums, values = bufs[0]
+        return sums, values, r[: plan.rows_total * plan.num_paths].reshape(plan.rows_total, plan.num_paths)
 
     def run_many(self, plans: Sequence[Plan]):
         views = (PlanView * len(plans))(*[p.view() for p in plans])
@@ -250,6 +266,28 @@ class Context:
         v = plan.view()
         check(lib().zk_amc_states(self.handle, C.byref(v), x.ctypes.data, d.ctypes.data, ex.ctypes.data, exercise_rows), self.handle)
         return x.reshape(nT, nP), d.reshape(nT, nP), ex[: exercise_rows * nP].reshape(exercise_rows, nP)
+
+    def fit_amc(self, plan: Plan) -> Plan:
+        """zk_fit_amc: the plan with its Bermudans' policy and continuation regressions fitted on the GPU
+        (the fit gpu::compile runs; fused_exposure.cpp:103-156)."""
+        out = plan.terms.copy()
+        deg = np.ascontiguousarray(plan.amc_degrees, np.uint32)
+        v = plan.view()
+        check(lib().zk_fit_amc(self.handle, C.byref(v), deg.ctypes.data, deg.size, out.ctypes.data, out.size), self.handle)
+        return dataclasses.replace(plan, terms=out)
+
+    def fit_amc_f64(self, plan: Plan, normals: Optional[np.ndarray] = None, streams: int = 0) -> Plan:
+        """zk_fit_amc_f64: the fit in the FP64 mode on the FP64 state pass (optionally on injected normals);
+        returns the plan with fitted double-precision terms."""
+        v = plan.view64()
+        out = plan.tables64["terms"].copy()
+        deg = np.ascontiguousarray(plan.amc_degrees, np.uint32)
+        z = None if normals is None else np.ascontiguousarray(normals, np.float64)
+        check(lib().zk_fit_amc_f64(self.handle, C.byref(v), None if z is None else z.ctypes.data, streams, deg.ctypes.data,
+                                   deg.size, out.ctypes.data, out.size), self.handle)
+        t64 = dict(plan.tables64)
+        t64["terms"] = out
+        return dataclasses.replace(plan, tables64=t64)
 
     def run_f64(self, plan: Plan, normals: Optional[np.ndarray] = None, streams: int = 0, rows: bool = False):
         """FP64 mode (zk_run_plan_f64), optionally on injected normals [step][normal][stream]."""

@@ -268,6 +268,34 @@ def encode_netting_set(ns: NettingSet) -> np.ndarray:
     return np.asarray(out, dtype=np.float64)
 
 
+def bermudan_degrees(ns_array: np.ndarray) -> List[int]:
+    """The regression degree of each Bermudan of an encoded netting set, in trade order."""
+    a = np.asarray(ns_array, np.float64)
+    i, out = 2, []
+    for _ in range(int(a[1])):
+        kind = int(a[i])
+        if kind == 0:
+            i += 4
+            i += 1 + int(a[i])
+        elif kind == 1:
+            i += 5
+        elif kind == 2:
+            i += 6
+        elif kind == 3:
+            i += 4
+            i += 1 + int(a[i])
+            i += 1 + int(a[i])
+            out.append(int(a[i + 2]))
+            i += 3
+        elif kind == 4:
+            i += 4
+            i += 1 + int(a[i])
+            i += 1 + int(a[i])
+        else:
+            raise ValueError(f"netting set: unknown trade type {kind}")
+    return out
+
+
 def encode_options(o: Options) -> np.ndarray:
     out = [OPTIONS_MAGIC, o.pfe_quantile, o.counterparty, float(o.per_trade), o.im_quantile, o.im_inner_paths,
            o.im_margin_period, o.im_audit_paths, o.im_audit_inner_paths, o.samples, o.histogram_time,
