@@ -169,6 +169,13 @@ zk_status zk_batch_read(zk_batch* b, zk_output* outs);
 zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info);
 void zk_batch_destroy(zk_batch* b);
 
+/* ---- the surrogate's tensor-core GEMM (no counterpart in the reference) --------------------------------- */
+/* C[M][N] = A[M][K] B[N][K]^T (+ bias[N], SiLU if act == 1): bf16 operands (raw bit patterns), FP32 result,
+ * on the fifth-generation tensor cores (tcgen05.mma, FP32 accumulation in TMEM).  M % 128 == 0, N % 16 == 0,
+ * K % 16 == 0.  Host buffers; bias nullable. */
+zk_status zk_gemm_bf16(zk_context* ctx, const uint16_t* A, const uint16_t* B, uint32_t M, uint32_t N, uint32_t K,
+                       const float* bias, uint32_t act, float* C);
+
 /* Measured rate of the special-function unit's ex2 (billions per second on the whole GPU), the ceiling
  * of the fused kernel's bond exponentials (a roofline denominator; not part of the reference). */
 zk_status zk_peak_ex2(int device, double* giga_per_s);

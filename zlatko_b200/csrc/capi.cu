@@ -886,6 +886,41 @@ zk_status zk_fit_amc_f64(zk_context* ctx, const zk_plan_view_f64* plan, const do
   return fitAmc<double>(ctx, plan, normals, streams, degrees, num_bermudans, terms_out, terms_len);
 }
 
+zk_status zk_gemm_bf16(zk_context* ctx, const uint16_t* A, const uint16_t* B, uint32_t M, uint32_t N, uint32_t K,
+                       const float* bias, uint32_t act, float* C) {
+  void* d = nullptr;
+  try {
+    requireCtx(ctx);
+    if (!A || !B || !C) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (M % 128 || N % 16 || K % 16 || M == 0 || N == 0 || K == 0)
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "M must be a multiple of 128, N and K of 16 (got %u, %u, %u)", M, N, K);
+    const size_t a = static_cast<size_t>(M) * K * 2, b = static_cast<size_t>(N) * K * 2, c = static_cast<size_t>(M) * N * 4;
+    const size_t ob = (a + 255) / 256 * 256, oc = ob + (b + 255) / 256 * 256, obias = oc + (c + 255) / 256 * 256;
+    ZK_CUDA(cudaMalloc(&d, obias + N * 4));
+    unsigned char* p = static_cast<unsigned char*>(d);
+    ZK_CUDA(cudaMemcpyAsync(p, A, a, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(p + ob, B, b, cudaMemcpyHostToDevice, ctx->stream));
+    if (bias) ZK_CUDA(cudaMemcpyAsync(p + obias, bias, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    GemmArgs g{};
+    g.A = reinterpret_cast<const __nv_bfloat16*>(p), g.B = reinterpret_cast<const __nv_bfloat16*>(p + ob);
+    g.M = M, g.N = N, g.K = K, g.bias = bias ? reinterpret_cast<const float*>(p + obias) : nullptr;
+    g.C = reinterpret_cast<float*>(p + oc), g.act = act, g.err = ctx->dErr;
+    ZK_CUDA(launchGemm(g, ctx->stream));
+    uint32_t devErr = 0;
+    ZK_CUDA(cudaMemcpyAsync(C, p + oc, c, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(&devErr, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    ZK_CUDA(cudaFree(d));
+    d = nullptr;
+    if (devErr) throw fail(ZK_ERR_DEVICE_TIMEOUT, "the GEMM's wait for its tensor-core operations gave up");
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (d) cudaFree(d);
+    return record(ctx, f);
+  }
+}
+
 zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams, zk_output_f64* out,
                           double* rows) {
   return runInjected<double>(ctx, plan, normals, streams, out, rows);

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "zk_device.cuh"
@@ -53,5 +54,23 @@ struct AmcFitJob {
 template <typename R>
 cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
                          double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream);
+
+// C = A B^T with A [M][K], B [N][K] bf16 row-major (K contiguous) and FP32 accumulation on the tensor cores
+// (mlp.cu); M % 128 == 0, N % 16 == 0, K % 16 == 0.  Epilogue: z = acc + bias[n]; C (fp32, or C += z when
+// accumulate), Z = bf16(z), H = bf16(act(z)) row-major, HT = bf16(act(z)) transposed [N][M]; any may be null.
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  const __nv_bfloat16* B;
+  uint32_t M, N, K;
+  const float* bias;
+  float* C;
+  __nv_bfloat16* Z;
+  __nv_bfloat16* H;
+  __nv_bfloat16* HT;
+  uint32_t act;         // 0 identity, 1 SiLU
+  uint32_t accumulate;
+  uint32_t* err;
+};
+cudaError_t launchGemm(const GemmArgs& g, cudaStream_t stream);
 
 }  // namespace zk

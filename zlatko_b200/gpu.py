@@ -109,6 +109,16 @@ class Plan:
                            self.rows_total, self.num_outputs)
 
 
+def to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    """Round to the nearest bf16 (ties to even) and return the raw 16-bit patterns."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def from_bf16_bits(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
 def compile(model: S.Model, netting_set: S.NettingSet, options: Optional[S.Options] = None,
             fit: Optional["Context"] = None) -> Plan:
     """zk_compile: the host plan compiler (a restatement of gpu::compile, src/gpu/fused_exposure.cpp:214).
@@ -266,6 +276,17 @@ class Context:
         v = plan.view()
         check(lib().zk_amc_states(self.handle, C.byref(v), x.ctypes.data, d.ctypes.data, ex.ctypes.data, exercise_rows), self.handle)
         return x.reshape(nT, nP), d.reshape(nT, nP), ex[: exercise_rows * nP].reshape(exercise_rows, nP)
+
+    def gemm_bf16(self, a: np.ndarray, b: np.ndarray, bias: Optional[np.ndarray] = None, act: int = 0) -> np.ndarray:
+        """zk_gemm_bf16: a @ b.T on the tensor cores, a [M][K] and b [N][K] rounded to bf16, FP32 result."""
+        A, B = to_bf16_bits(a), to_bf16_bits(b)
+        M, K = A.shape
+        N = B.shape[0]
+        out = np.zeros((M, N), np.float32)
+        bs = None if bias is None else np.ascontiguousarray(bias, np.float32)
+        check(lib().zk_gemm_bf16(self.handle, A.ctypes.data, B.ctypes.data, M, N, K, None if bs is None else bs.ctypes.data,
+                                 act, out.ctypes.data), self.handle)
+        return out
 
     def fit_amc(self, plan: Plan) -> Plan:
         """zk_fit_amc: the plan with its Bermudans' policy and continuation regressions fitted on the GPU
