@@ -176,6 +176,25 @@ void zk_batch_destroy(zk_batch* b);
 zk_status zk_gemm_bf16(zk_context* ctx, const uint16_t* A, const uint16_t* B, uint32_t M, uint32_t N, uint32_t K,
                        const float* bias, uint32_t act, float* C);
 
+/* ---- the learned revaluation surrogate (no counterpart in the reference) -------------------------------- */
+/* A 16 -> 128 -> 128 -> 128 -> 1 perceptron (SiLU), BF16 weights and activations, FP32 accumulation, trained
+ * and evaluated on the tensor cores by this library's kernels.  Inputs x are [n][16] floats, targets and
+ * predictions [n] floats, all host buffers; inputs and targets are standardised with the moments of the first
+ * training (or gradient) set.  Parameters flatten as W1[128][16] b1[128] W2[128][128] b2 W3[128][128] b3
+ * w4[128] b4 (ZK_SURROGATE_PARAMS floats); the scaling as mean[16], 1/sd[16], target mean, target sd. */
+#define ZK_SURROGATE_PARAMS 35329u
+typedef struct zk_surrogate zk_surrogate;
+zk_status zk_surrogate_create(zk_context* ctx, uint32_t seed, zk_surrogate** out);
+void zk_surrogate_destroy(zk_surrogate* s);
+/* Adam over `epochs` passes in batches of `batch` rows (mean squared error in standardised units). */
+zk_status zk_surrogate_train(zk_surrogate* s, const float* x, const float* y, size_t n, uint32_t epochs, uint32_t batch, float lr,
+                             float weight_decay, float* loss_per_epoch);
+zk_status zk_surrogate_predict(zk_surrogate* s, const float* x, size_t n, float* y);
+/* Loss and gradient of the mean squared error over n rows (one batch, n <= 2^20) at the current parameters. */
+zk_status zk_surrogate_gradients(zk_surrogate* s, const float* x, const float* y, size_t n, float* loss, float* grads);
+/* Reads (get, scaling_get[34]) and / or replaces (set, scaling_set[34]) the FP32 parameters and the scaling. */
+zk_status zk_surrogate_params(zk_surrogate* s, float* get, const float* set, float* scaling_get, const float* scaling_set);
+
 /* Measured rate of the special-function unit's ex2 (billions per second on the whole GPU), the ceiling
  * of the fused kernel's bond exponentials (a roofline denominator; not part of the reference). */
 zk_status zk_peak_ex2(int device, double* giga_per_s);

@@ -31,3 +31,71 @@ def test_gemm_rejects_bad_shapes(ctx):
 
     with pytest.raises(ZkError, match="INVALID_ARGUMENT"):
         ctx.gemm_bf16(np.zeros((100, 16)), np.zeros((16, 16)))
+
+
+# ---------------------------------------------------------------- the surrogate perceptron
+def data(n, seed):
+    rng = np.random.default_rng(seed)
+    sd = np.array([0.02, 0.1, 0.1, 0.01, 1.0, 3.0, 0.5, 1, 1, 1, 0.03, 5.0, 0.2, 1.0, 0.1, 1.0], np.float32)
+    x = (rng.standard_normal((n, 16)) * sd + np.arange(16) * 0.1).astype(np.float32)
+    z = (x - np.arange(16) * 0.1) / sd
+    y = (np.sin(z[:, 0]) + 0.5 * z[:, 1] * z[:, 2] + np.tanh(z[:, 4] - z[:, 5]) + 0.1 * z[:, 11] ** 2).astype(np.float32)
+    return x, y
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_surrogate_gradients_match_the_fp64_oracle(ctx):
+    """Per parameter block: within 5e-3 (relative L2) of the oracle at the GPU's bf16 rounding points (what is
+    left is FP32 against FP64 accumulation and the odd bf16 tie), within 5e-2 of the exact FP64 network."""
+    from oracle import mlp_oracle as O
+    from zlatko_b200.surrogate import LAYOUT, Surrogate
+
+    with Surrogate(ctx, seed=3) as s:
+        x, y = data(1000, 1)  # 1000 rows: a padded last tile of 128
+        loss, g = s.gradients(x, y)
+        p, sc = s.params()
+        lo, go = O.loss_and_grads(p, sc, x, y, emulate=True)
+        l64, g64 = O.loss_and_grads(p, sc, x, y, emulate=False)
+        assert abs(loss - lo) <= 1e-4 * lo
+        assert abs(loss - l64) <= 2e-2 * l64
+        o = 0
+        for name, shape in LAYOUT:
+            k = int(np.prod(shape))
+            assert rel(g[o:o + k], go[o:o + k]) <= 5e-3, name
+            assert rel(g[o:o + k], g64[o:o + k]) <= 5e-2, name
+            o += k
+
+
+def test_surrogate_forward_matches_the_oracle(ctx):
+    """A bf16 activation that rounds the other way on a tie moves one output by ~1e-3 of its scale; all others
+    agree to ~1e-7."""
+    from oracle import mlp_oracle as O
+    from zlatko_b200.surrogate import Surrogate
+
+    with Surrogate(ctx, seed=5) as s:
+        x, y = data(3000, 2)
+        s.gradients(x, y)  # fixes the scaling from this set
+        p, sc = s.params()
+        got = s.predict(x)
+        ref = O.predict(p, sc, x, emulate=True)
+        err = np.abs(got - ref) / np.abs(ref).max()
+        assert err.max() <= 1e-2 and np.quantile(err, 0.99) <= 1e-5
+
+
+def test_surrogate_training_learns_a_smooth_function(ctx):
+    from oracle import mlp_oracle as O
+    from zlatko_b200.surrogate import Surrogate
+
+    with Surrogate(ctx, seed=7) as s:
+        x, y = data(65536, 3)
+        losses = s.train(x, y, epochs=30, batch=4096, lr=2e-3)
+        assert losses[-1] < 0.05 * losses[0], losses
+        xt, yt = data(8192, 4)  # held-out rows
+        pred = s.predict(xt)
+        assert np.sqrt(np.mean((pred - yt) ** 2)) <= 0.15 * np.std(yt)
+        p, sc = s.params()
+        err = np.abs(pred - O.predict(p, sc, xt, emulate=True)) / np.abs(yt).max()
+        assert err.max() <= 1e-2 and np.quantile(err, 0.99) <= 1e-4

@@ -66,7 +66,8 @@ class BatchInfo(C.Structure):
 EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream",
            "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc",
            "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
-           "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
+           "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
+           "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
            "zk_plan_destroy"]
 
 _lib: Optional[C.CDLL] = None
@@ -95,6 +96,12 @@ def lib() -> C.CDLL:
         "zk_fit_amc": (st, [vp, P(PlanView), vp, sz, vp, sz]),
         "zk_run_plan_rows": (st, [vp, P(PlanView), P(Output), vp]),
         "zk_gemm_bf16": (st, [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint32, vp]),
+        "zk_surrogate_create": (st, [vp, C.c_uint32, vp]),
+        "zk_surrogate_destroy": (None, [vp]),
+        "zk_surrogate_train": (st, [vp, vp, vp, sz, C.c_uint32, C.c_uint32, C.c_float, C.c_float, vp]),
+        "zk_surrogate_predict": (st, [vp, vp, sz, vp]),
+        "zk_surrogate_gradients": (st, [vp, vp, vp, sz, vp, vp]),
+        "zk_surrogate_params": (st, [vp, vp, vp, vp, vp]),
         "zk_fit_amc_f64": (st, [vp, P(PlanViewF64), vp, sz, vp, sz, vp, sz]),
         "zk_run_plan_f64": (st, [vp, P(PlanViewF64), vp, sz, P(OutputF64), vp]),
         "zk_run_plan_injected": (st, [vp, P(PlanView), vp, sz, P(Output), vp]),

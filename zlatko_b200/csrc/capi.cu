@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/zlatko_b200.h"
+#include "surrogate.cuh"
 #include "zk_kernels.h"
 
 using namespace zk;
@@ -917,6 +918,169 @@ zk_status zk_gemm_bf16(zk_context* ctx, const uint16_t* A, const uint16_t* B, ui
     return ZK_OK;
   } catch (const Failure& f) {
     if (d) cudaFree(d);
+    return record(ctx, f);
+  }
+}
+
+}  // extern "C"
+
+// ---- the learned revaluation surrogate ----
+struct zk_surrogate {
+  zk_context* ctx = nullptr;
+  zk::SurrogateState S;
+};
+
+namespace {
+zk_context* ctxOf(zk_surrogate* s) {
+  if (!s || !s->ctx) throw fail(ZK_ERR_INVALID_ARGUMENT, "null surrogate");
+  requireCtx(s->ctx);
+  return s->ctx;
+}
+// A device copy of n host values; the caller frees it.
+template <typename T>
+T* toDevice(const T* h, size_t n, cudaStream_t st) {
+  void* d = nullptr;
+  ZK_CUDA(cudaMalloc(&d, std::max<size_t>(n, 1) * sizeof(T)));
+  const cudaError_t e = cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    ZK_CUDA(e);
+  }
+  return static_cast<T*>(d);
+}
+void checkErrWord(zk_context* ctx) {
+  uint32_t devErr = 0;
+  ZK_CUDA(cudaMemcpyAsync(&devErr, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (devErr) throw fail(ZK_ERR_DEVICE_TIMEOUT, "a tensor-core wait gave up (error %u)", devErr);
+}
+void scaleFromHost(zk_surrogate* s, const float* x, const float* y, size_t n) {
+  float sc[32];
+  zk::surrogateScaleFrom(s->S, x, y, n, sc);
+  ZK_CUDA(cudaMemcpyAsync(s->S.scale, sc, sizeof sc, cudaMemcpyHostToDevice, s->ctx->stream));
+  ZK_CUDA(cudaStreamSynchronize(s->ctx->stream));
+}
+}  // namespace
+
+extern "C" {
+
+zk_status zk_surrogate_create(zk_context* ctx, uint32_t seed, zk_surrogate** out) {
+  try {
+    requireCtx(ctx);
+    if (!out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    auto s = std::make_unique<zk_surrogate>();
+    s->ctx = ctx;
+    const cudaError_t e = zk::surrogateCreate(s->S, ctx->stream, ctx->dErr, seed);
+    if (e != cudaSuccess) {
+      zk::surrogateFree(s->S);
+      ZK_CUDA(e);
+    }
+    *out = s.release();
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
+void zk_surrogate_destroy(zk_surrogate* s) {
+  if (!s) return;
+  if (s->ctx) cudaSetDevice(s->ctx->device);
+  zk::surrogateFree(s->S);
+  delete s;
+}
+
+zk_status zk_surrogate_train(zk_surrogate* s, const float* x, const float* y, size_t n, uint32_t epochs, uint32_t batch, float lr,
+                             float weight_decay, float* loss_per_epoch) {
+  zk_context* ctx = s ? s->ctx : nullptr;
+  float *dx = nullptr, *dy = nullptr;
+  try {
+    ctx = ctxOf(s);
+    if (!x || !y || n == 0 || batch == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "empty training set or batch");
+    if (!s->S.scaled) scaleFromHost(s, x, y, n);
+    dx = toDevice(x, n * zk::kIn, ctx->stream);
+    dy = toDevice(y, n, ctx->stream);
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    for (uint32_t e = 0; e < epochs; ++e) {
+      double loss = 0.0;
+      ZK_CUDA(zk::surrogateEpoch(s->S, dx, dy, n, batch, lr, weight_decay, true, &loss));
+      if (loss_per_epoch) loss_per_epoch[e] = static_cast<float>(loss);
+    }
+    checkErrWord(ctx);
+    cudaFree(dx), cudaFree(dy);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_surrogate_predict(zk_surrogate* s, const float* x, size_t n, float* y) {
+  zk_context* ctx = s ? s->ctx : nullptr;
+  float *dx = nullptr, *dy = nullptr;
+  try {
+    ctx = ctxOf(s);
+    if (!x || !y) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return ZK_OK;
+    dx = toDevice(x, n * zk::kIn, ctx->stream);
+    ZK_CUDA(cudaMalloc(&dy, n * 4));
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    ZK_CUDA(zk::surrogatePredict(s->S, dx, n, dy));
+    ZK_CUDA(cudaMemcpyAsync(y, dy, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    checkErrWord(ctx);
+    cudaFree(dx), cudaFree(dy);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_surrogate_gradients(zk_surrogate* s, const float* x, const float* y, size_t n, float* loss, float* grads) {
+  zk_context* ctx = s ? s->ctx : nullptr;
+  float *dx = nullptr, *dy = nullptr;
+  try {
+    ctx = ctxOf(s);
+    if (!x || !y || !grads || n == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument or empty set");
+    if (n > (1u << 20)) throw fail(ZK_ERR_INVALID_ARGUMENT, "gradients of at most 2^20 rows (one batch)");
+    if (!s->S.scaled) scaleFromHost(s, x, y, n);
+    dx = toDevice(x, n * zk::kIn, ctx->stream);
+    dy = toDevice(y, n, ctx->stream);
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    double l = 0.0;
+    ZK_CUDA(zk::surrogateEpoch(s->S, dx, dy, n, static_cast<uint32_t>(n), 0.0f, 0.0f, false, &l));
+    ZK_CUDA(cudaMemcpyAsync(grads, s->S.grad, zk::SurrogateState::kParams * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    checkErrWord(ctx);
+    if (loss) *loss = static_cast<float>(l);
+    cudaFree(dx), cudaFree(dy);
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_surrogate_params(zk_surrogate* s, float* get, const float* set, float* scaling_get, const float* scaling_set) {
+  zk_context* ctx = s ? s->ctx : nullptr;
+  try {
+    ctx = ctxOf(s);
+    const size_t P = zk::SurrogateState::kParams;
+    if (set) {
+      ZK_CUDA(cudaMemcpyAsync(s->S.p, set, P * 4, cudaMemcpyHostToDevice, ctx->stream));
+      ZK_CUDA(zk::surrogateSync(s->S));
+    }
+    if (scaling_set) {
+      ZK_CUDA(cudaMemcpyAsync(s->S.scale, scaling_set, 32 * 4, cudaMemcpyHostToDevice, ctx->stream));
+      s->S.yMean = scaling_set[32], s->S.yScale = scaling_set[33], s->S.scaled = true;
+    }
+    if (get) ZK_CUDA(cudaMemcpyAsync(get, s->S.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (scaling_get) ZK_CUDA(cudaMemcpyAsync(scaling_get, s->S.scale, 32 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (scaling_get) scaling_get[32] = s->S.yMean, scaling_get[33] = s->S.yScale;
+    return ZK_OK;
+  } catch (const Failure& f) {
     return record(ctx, f);
   }
 }

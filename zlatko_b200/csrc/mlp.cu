@@ -85,7 +85,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
       for (int j = 0; j < 16; ++j) {
         const uint32_t n = n0 + c + j;
         const size_t at = static_cast<size_t>(row) * g.N + n;
-        const float z = v[j] + (g.bias ? g.bias[n] : 0.0f);
+        float z = v[j] + (g.bias ? g.bias[n] : 0.0f);
+        if (g.gradOf) z *= umma::siluGrad(__bfloat162float(g.gradOf[at]));
         if (g.C) g.C[at] = g.accumulate ? g.C[at] + z : z;
         const float h = g.act ? umma::silu(z) : z;
         if (g.Z) g.Z[at] = __float2bfloat16_rn(z);

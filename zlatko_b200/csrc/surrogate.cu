@@ -1,0 +1,345 @@
+// The learned revaluation surrogate: a 16 -> 128 -> 128 -> 128 -> 1 multilayer perceptron with SiLU
+// activations, BF16 weights and activations and FP32 accumulation, trained and evaluated on the GPU by this
+// library's own kernels (no counterpart in the reference: its AI chapter fits a small FP64 tanh network to
+// XVA adjustments on the CPU, src/ai/surrogate.cpp).
+//
+// Every product of the forward and backward passes is one tensor-core GEMM of mlp.cu (tcgen05, FP32 in TMEM)
+// whose epilogue applies the bias, the SiLU or the SiLU derivative and writes the BF16 activations in the
+// layouts the next product reads.  The scalar head (128 -> 1), the loss, the bias gradients and Adam are
+// CUDA-core kernels here.  Inputs and targets are standardised with the training set's moments.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "surrogate.cuh"
+#include "umma.cuh"
+
+namespace zk {
+
+namespace {
+
+// Row pass of the head: pred = h3 . w4 + b4 (standardised units); with targets, dOut = 2 (pred - y) / n and the
+// block's sum of squared errors.  Rows >= n are padding and contribute nothing.
+__global__ void headKernel(const bf16* __restrict__ H3, const float* __restrict__ w4, const float* __restrict__ b4,
+                           const float* __restrict__ y, uint32_t n, float* __restrict__ pred, float* __restrict__ dOut,
+                           float* __restrict__ lossPart) {
+  __shared__ float red[128];
+  const uint32_t r = blockIdx.x * 128 + threadIdx.x;
+  const bf16* h = H3 + static_cast<size_t>(r) * kHid;
+  float p = 0.0f, l = 0.0f;
+  for (uint32_t j = 0; j < kHid; ++j) p += __bfloat162float(h[j]) * w4[j];
+  p += b4[0];
+  if (pred) pred[r] = p;
+  if (dOut) {
+    const float d = r < n ? p - y[r] : 0.0f;
+    dOut[r] = 2.0f * d / static_cast<float>(n);
+    l = d * d;
+  }
+  if (lossPart) {
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (uint32_t s = 64; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) lossPart[blockIdx.x] = red[0];
+  }
+}
+
+// Column pass of the head on a block of 128 rows: the block's partial dw4 and db4, and
+// dZ3 = dOut w4 silu'(Z3) row-major and transposed.
+__global__ void headBackKernel(const bf16* __restrict__ H3, const bf16* __restrict__ Z3, const float* __restrict__ w4,
+                               const float* __restrict__ dOut, uint32_t rows, float* __restrict__ part,
+                               bf16* __restrict__ dZ3, bf16* __restrict__ dZ3T) {
+  __shared__ float d[128];
+  const uint32_t r0 = blockIdx.x * 128, j = threadIdx.x;
+  d[j] = dOut[r0 + j];
+  __syncthreads();
+  float gw = 0.0f, gb = 0.0f;
+  for (uint32_t i = 0; i < 128; ++i) {
+    const size_t at = static_cast<size_t>(r0 + i) * kHid + j;
+    gw += d[i] * __bfloat162float(H3[at]);
+    gb += d[i];
+    const bf16 v = __float2bfloat16_rn(d[i] * w4[j] * umma::siluGrad(__bfloat162float(Z3[at])));
+    dZ3[at] = v;
+    dZ3T[static_cast<size_t>(j) * rows + r0 + i] = v;
+  }
+  part[static_cast<size_t>(blockIdx.x) * (kHid + 1) + j] = gw;
+  if (j == 0) part[static_cast<size_t>(blockIdx.x) * (kHid + 1) + kHid] = gb;
+}
+
+// out[c] = sum over blocks b of part[b][c], in block order (deterministic).
+__global__ void sumRowsKernel(const float* __restrict__ part, uint32_t blocks, uint32_t w, float* __restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= w) return;
+  float s = 0.0f;
+  for (uint32_t b = 0; b < blocks; ++b) s += part[static_cast<size_t>(b) * w + c];
+  out[c] = s;
+}
+
+// Column sums of a bf16 [rows][128] matrix (the bias gradients), in row order.
+__global__ void colSumKernel(const bf16* __restrict__ M, uint32_t rows, float* __restrict__ out) {
+  const uint32_t j = threadIdx.x;
+  float s = 0.0f;
+  for (uint32_t r = 0; r < rows; ++r) s += __bfloat162float(M[static_cast<size_t>(r) * kHid + j]);
+  out[j] = s;
+}
+
+// Adam on one parameter block [outDim][inDim] (or a vector); refreshes the bf16 copies of matrices.
+__global__ void adamKernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ g,
+                           uint32_t n, uint32_t outDim, uint32_t inDim, float lr, float b1, float b2, float c1, float c2,
+                           float eps, float decay, bf16* __restrict__ wb, bf16* __restrict__ wbT) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i] + decay * w[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi, v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+  if (wbT) wbT[static_cast<size_t>(i % inDim) * outDim + i / inDim] = __float2bfloat16_rn(wi);
+}
+
+__global__ void castKernel(const float* __restrict__ w, uint32_t n, uint32_t outDim, uint32_t inDim, bf16* __restrict__ wb,
+                           bf16* __restrict__ wbT) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  wb[i] = __float2bfloat16_rn(w[i]);
+  wbT[static_cast<size_t>(i % inDim) * outDim + i / inDim] = __float2bfloat16_rn(w[i]);
+}
+
+// Standardised bf16 inputs X [rows][16] (and XT [16][rows]), zero rows past n; standardised targets.
+__global__ void prepareKernel(const float* __restrict__ x, const float* __restrict__ y, uint32_t n, uint32_t rows,
+                              const float* __restrict__ mean, const float* __restrict__ inv, float yMean, float yInv,
+                              bf16* __restrict__ X, bf16* __restrict__ XT, float* __restrict__ ys) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  for (uint32_t k = 0; k < kIn; ++k) {
+    const float v = r < n ? (x[static_cast<size_t>(r) * kIn + k] - mean[k]) * inv[k] : 0.0f;
+    const bf16 b = __float2bfloat16_rn(v);
+    X[static_cast<size_t>(r) * kIn + k] = b;
+    if (XT) XT[static_cast<size_t>(k) * rows + r] = b;
+  }
+  if (ys) ys[r] = r < n ? (y[r] - yMean) * yInv : 0.0f;
+}
+
+__global__ void unscaleKernel(const float* __restrict__ pred, uint32_t n, float yMean, float yScale, float* __restrict__ out) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) out[r] = pred[r] * yScale + yMean;
+}
+
+uint32_t blocksOf(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
+
+#define SG_CUDA(x)                    \
+  do {                                \
+    cudaError_t e_ = (x);             \
+    if (e_ != cudaSuccess) return e_; \
+  } while (0)
+
+cudaError_t ensureWorkspace(SurrogateState& S, uint32_t rows) {
+  if (rows <= S.cap) return cudaSuccess;
+  if (S.ws) cudaFree(S.ws);
+  S.ws = nullptr;
+  S.cap = 0;
+  const size_t r = rows, bh = r * kHid * 2, bi = r * kIn * 2;
+  const size_t sizes[] = {bi, bi, bh, bh, bh, bh, bh, bh, bh, bh, bh, bh, bh, bh, bh, bh,
+                          r * 4, r * 4, r * 4, (r / 128 + 1) * (kHid + 1) * 4, (r / 128 + 1) * 4};
+  constexpr size_t nb = sizeof(sizes) / sizeof(sizes[0]);
+  size_t off[nb], total = 0;
+  for (size_t i = 0; i < nb; ++i) off[i] = total, total += (sizes[i] + 255) / 256 * 256;
+  SG_CUDA(cudaMalloc(&S.ws, total));
+  bf16** bp[] = {&S.X, &S.XT, &S.Z1, &S.H1, &S.H1T, &S.Z2, &S.H2, &S.H2T, &S.Z3, &S.H3, &S.dZ3, &S.dZ3T, &S.dZ2, &S.dZ2T, &S.dZ1, &S.dZ1T};
+  for (size_t i = 0; i < 16; ++i) *bp[i] = reinterpret_cast<bf16*>(S.ws + off[i]);
+  float** fp[] = {&S.ys, &S.pred, &S.dOut, &S.part, &S.lossPart};
+  for (size_t i = 0; i < 5; ++i) *fp[i] = reinterpret_cast<float*>(S.ws + off[16 + i]);
+  S.cap = rows;
+  return cudaSuccess;
+}
+
+GemmArgs gemm(const bf16* A, const bf16* B, uint32_t M, uint32_t N, uint32_t K, uint32_t* err) {
+  GemmArgs g{};
+  g.A = A, g.B = B, g.M = M, g.N = N, g.K = K, g.err = err;
+  return g;
+}
+
+// Forward pass of `rows` (a multiple of 128) standardised rows in S.X: Z and H of the three hidden layers
+// (and the transposed H1, H2 that the weight gradients read, when training).
+cudaError_t forward(SurrogateState& S, uint32_t rows, bool training) {
+  const cudaStream_t s = S.stream;
+  GemmArgs g = gemm(S.X, S.wb, rows, kHid, kIn, S.err);
+  g.bias = S.b1(), g.act = 1, g.Z = S.Z1, g.H = S.H1, g.HT = training ? S.H1T : nullptr;
+  SG_CUDA(launchGemm(g, s));
+  g = gemm(S.H1, S.wb + SurrogateState::kW1, rows, kHid, kHid, S.err);
+  g.bias = S.b2(), g.act = 1, g.Z = S.Z2, g.H = S.H2, g.HT = training ? S.H2T : nullptr;
+  SG_CUDA(launchGemm(g, s));
+  g = gemm(S.H2, S.wb + SurrogateState::kW1 + SurrogateState::kW2, rows, kHid, kHid, S.err);
+  g.bias = S.b3(), g.act = 1, g.Z = S.Z3, g.H = S.H3;
+  SG_CUDA(launchGemm(g, s));
+  return cudaSuccess;
+}
+
+// Loss and gradient of the batch (n real rows of `rows`) into S.grad; the squared errors into S.lossPart.
+cudaError_t backward(SurrogateState& S, uint32_t n, uint32_t rows) {
+  const cudaStream_t s = S.stream;
+  const uint32_t blocks = rows / 128;
+  headKernel<<<blocks, 128, 0, s>>>(S.H3, S.w4(), S.b4(), S.ys, n, S.pred, S.dOut, S.lossPart);
+  headBackKernel<<<blocks, 128, 0, s>>>(S.H3, S.Z3, S.w4(), S.dOut, rows, S.part, S.dZ3, S.dZ3T);
+  sumRowsKernel<<<2, 128, 0, s>>>(S.part, blocks, kHid + 1, S.grad + S.offOf(S.w4()));
+  // dW3 = dZ3^T H2, db3, dZ2 = (dZ3 W3) silu'(Z2)
+  GemmArgs g = gemm(S.dZ3T, S.H2T, kHid, kHid, rows, S.err);
+  g.C = S.grad + S.offOf(S.W3());
+  SG_CUDA(launchGemm(g, s));
+  colSumKernel<<<1, kHid, 0, s>>>(S.dZ3, rows, S.grad + S.offOf(S.b3()));
+  g = gemm(S.dZ3, S.wbT + SurrogateState::kW1 + SurrogateState::kW2, rows, kHid, kHid, S.err);
+  g.gradOf = S.Z2, g.H = S.dZ2, g.HT = S.dZ2T;
+  SG_CUDA(launchGemm(g, s));
+  // dW2 = dZ2^T H1, db2, dZ1 = (dZ2 W2) silu'(Z1)
+  g = gemm(S.dZ2T, S.H1T, kHid, kHid, rows, S.err);
+  g.C = S.grad + S.offOf(S.W2());
+  SG_CUDA(launchGemm(g, s));
+  colSumKernel<<<1, kHid, 0, s>>>(S.dZ2, rows, S.grad + S.offOf(S.b2()));
+  g = gemm(S.dZ2, S.wbT + SurrogateState::kW1, rows, kHid, kHid, S.err);
+  g.gradOf = S.Z1, g.H = S.dZ1, g.HT = S.dZ1T;
+  SG_CUDA(launchGemm(g, s));
+  // dW1 = dZ1^T X, db1
+  g = gemm(S.dZ1T, S.XT, kHid, kIn, rows, S.err);
+  g.C = S.grad + S.offOf(S.W1());
+  SG_CUDA(launchGemm(g, s));
+  colSumKernel<<<1, kHid, 0, s>>>(S.dZ1, rows, S.grad + S.offOf(S.b1()));
+  return cudaGetLastError();
+}
+
+cudaError_t adam(SurrogateState& S, float lr, float decay) {
+  ++S.step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, static_cast<float>(S.step)), c2 = 1.0f - std::pow(b2, static_cast<float>(S.step));
+  struct Blk {
+    float* w;
+    uint32_t n, out, in;
+    size_t wb;
+    bool mat;
+  } blks[] = {{S.W1(), SurrogateState::kW1, kHid, kIn, 0, true},
+              {S.b1(), kHid, 1, 1, 0, false},
+              {S.W2(), SurrogateState::kW2, kHid, kHid, SurrogateState::kW1, true},
+              {S.b2(), kHid, 1, 1, 0, false},
+              {S.W3(), SurrogateState::kW3, kHid, kHid, SurrogateState::kW1 + SurrogateState::kW2, true},
+              {S.b3(), kHid, 1, 1, 0, false},
+              {S.w4(), kHid + 1, 1, 1, 0, false}};  // w4 and b4
+  for (const auto& b : blks) {
+    const size_t o = S.offOf(b.w);
+    adamKernel<<<blocksOf(b.n, 256), 256, 0, S.stream>>>(b.w, S.m + o, S.v + o, S.grad + o, b.n, b.out, b.in, lr, b1, b2, c1,
+                                                         c2, 1e-8f, b.mat ? decay : 0.0f, b.mat ? S.wb + b.wb : nullptr,
+                                                         b.mat ? S.wbT + b.wb : nullptr);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t surrogateSync(SurrogateState& S) {
+  const size_t o2 = SurrogateState::kW1, o3 = SurrogateState::kW1 + SurrogateState::kW2;
+  castKernel<<<blocksOf(SurrogateState::kW1, 256), 256, 0, S.stream>>>(S.W1(), SurrogateState::kW1, kHid, kIn, S.wb, S.wbT);
+  castKernel<<<blocksOf(SurrogateState::kW2, 256), 256, 0, S.stream>>>(S.W2(), SurrogateState::kW2, kHid, kHid, S.wb + o2,
+                                                                        S.wbT + o2);
+  castKernel<<<blocksOf(SurrogateState::kW3, 256), 256, 0, S.stream>>>(S.W3(), SurrogateState::kW3, kHid, kHid, S.wb + o3,
+                                                                        S.wbT + o3);
+  return cudaGetLastError();
+}
+
+cudaError_t surrogateCreate(SurrogateState& S, cudaStream_t stream, uint32_t* err, uint32_t seed) {
+  S.stream = stream, S.err = err;
+  const size_t P = SurrogateState::kParams;
+  const size_t wbN = SurrogateState::kW1 + SurrogateState::kW2 + SurrogateState::kW3;
+  void* mem = nullptr;
+  SG_CUDA(cudaMalloc(&mem, P * 4 * 4 + wbN * 2 * 2 + 32 * 4));
+  S.p = static_cast<float*>(mem);
+  S.grad = S.p + P, S.m = S.grad + P, S.v = S.m + P;
+  S.wb = reinterpret_cast<bf16*>(S.v + P);
+  S.wbT = S.wb + wbN;
+  S.scale = reinterpret_cast<float*>(S.wbT + wbN);
+  // He-uniform initialisation (fan-in) from a seeded 64-bit LCG on the host; zero biases.
+  std::vector<float> h(P, 0.0f), sc(32);
+  uint64_t st = 0x9E3779B97F4A7C15ull ^ seed;
+  auto uni = [&] {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return static_cast<float>((st >> 40) & 0xFFFFFF) / 16777216.0f * 2.0f - 1.0f;
+  };
+  auto fill = [&](size_t off, size_t n, uint32_t fanIn) {
+    const float a = std::sqrt(6.0f / static_cast<float>(fanIn));
+    for (size_t i = 0; i < n; ++i) h[off + i] = a * uni();
+  };
+  fill(0, SurrogateState::kW1, kIn);
+  fill(SurrogateState::kW1 + kHid, SurrogateState::kW2, kHid);
+  fill(SurrogateState::kW1 + kHid + SurrogateState::kW2 + kHid, SurrogateState::kW3, kHid);
+  fill(SurrogateState::kW1 + kHid + SurrogateState::kW2 + kHid + SurrogateState::kW3 + kHid, kHid, kHid);
+  for (uint32_t k = 0; k < 16; ++k) sc[k] = 0.0f, sc[16 + k] = 1.0f;
+  SG_CUDA(cudaMemcpyAsync(S.p, h.data(), P * 4, cudaMemcpyHostToDevice, stream));
+  SG_CUDA(cudaMemsetAsync(S.grad, 0, P * 4 * 3, stream));
+  SG_CUDA(cudaMemcpyAsync(S.scale, sc.data(), 32 * 4, cudaMemcpyHostToDevice, stream));
+  SG_CUDA(surrogateSync(S));
+  return cudaStreamSynchronize(stream);  // the host vectors above go out of scope
+}
+
+void surrogateFree(SurrogateState& S) {
+  if (S.p) cudaFree(S.p);
+  if (S.ws) cudaFree(S.ws);
+  S.p = nullptr, S.ws = nullptr, S.cap = 0;
+}
+
+void surrogateScaleFrom(SurrogateState& S, const float* x, const float* y, size_t n, float* hostScale) {
+  double mu[kIn] = {}, m2[kIn] = {}, ym = 0.0, y2 = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    for (uint32_t k = 0; k < kIn; ++k) {
+      const double v = x[i * kIn + k];
+      mu[k] += v, m2[k] += v * v;
+    }
+    ym += y[i], y2 += static_cast<double>(y[i]) * y[i];
+  }
+  const double dn = static_cast<double>(n > 0 ? n : 1);
+  for (uint32_t k = 0; k < kIn; ++k) {
+    const double mean = mu[k] / dn, var = m2[k] / dn - mean * mean;
+    hostScale[k] = static_cast<float>(mean);
+    hostScale[16 + k] = var > 1e-24 ? static_cast<float>(1.0 / std::sqrt(var)) : 1.0f;
+  }
+  S.yMean = static_cast<float>(ym / dn);
+  const double yv = y2 / dn - (ym / dn) * (ym / dn);
+  S.yScale = yv > 1e-24 ? static_cast<float>(std::sqrt(yv)) : 1.0f;
+  S.scaled = true;
+}
+
+cudaError_t surrogateEpoch(SurrogateState& S, const float* dx, const float* dy, size_t n, uint32_t batch, float lr, float decay,
+                           bool train, double* loss) {
+  const uint32_t rowsCap = (batch + 127) / 128 * 128;
+  SG_CUDA(ensureWorkspace(S, rowsCap));
+  double total = 0.0;
+  std::vector<float> lp(rowsCap / 128);
+  for (size_t b0 = 0; b0 < n; b0 += batch) {
+    const uint32_t nb = static_cast<uint32_t>(std::min<size_t>(batch, n - b0)), rows = (nb + 127) / 128 * 128;
+    prepareKernel<<<blocksOf(rows, 128), 128, 0, S.stream>>>(dx + b0 * kIn, dy + b0, nb, rows, S.scale, S.scale + 16, S.yMean,
+                                                              1.0f / S.yScale, S.X, S.XT, S.ys);
+    SG_CUDA(forward(S, rows, true));
+    SG_CUDA(backward(S, nb, rows));
+    if (train) SG_CUDA(adam(S, lr, decay));
+    SG_CUDA(cudaMemcpyAsync(lp.data(), S.lossPart, rows / 128 * 4, cudaMemcpyDeviceToHost, S.stream));
+    SG_CUDA(cudaStreamSynchronize(S.stream));
+    for (uint32_t i = 0; i < rows / 128; ++i) total += lp[i];
+  }
+  if (loss) *loss = total / static_cast<double>(n > 0 ? n : 1);
+  return cudaSuccess;
+}
+
+cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float* dout) {
+  const uint32_t chunk = 1u << 16;
+  SG_CUDA(ensureWorkspace(S, chunk));
+  for (size_t b0 = 0; b0 < n; b0 += chunk) {
+    const uint32_t nb = static_cast<uint32_t>(std::min<size_t>(chunk, n - b0)), rows = (nb + 127) / 128 * 128;
+    prepareKernel<<<blocksOf(rows, 128), 128, 0, S.stream>>>(dx + b0 * kIn, nullptr, nb, rows, S.scale, S.scale + 16, 0.0f, 1.0f,
+                                                              S.X, nullptr, nullptr);
+    SG_CUDA(forward(S, rows, false));
+    headKernel<<<rows / 128, 128, 0, S.stream>>>(S.H3, S.w4(), S.b4(), nullptr, nb, S.pred, nullptr, nullptr);
+    unscaleKernel<<<blocksOf(nb, 256), 256, 0, S.stream>>>(S.pred, nb, S.yMean, S.yScale, dout + b0);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace zk

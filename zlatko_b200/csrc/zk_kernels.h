@@ -56,8 +56,9 @@ cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, co
                          double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream);
 
 // C = A B^T with A [M][K], B [N][K] bf16 row-major (K contiguous) and FP32 accumulation on the tensor cores
-// (mlp.cu); M % 128 == 0, N % 16 == 0, K % 16 == 0.  Epilogue: z = acc + bias[n]; C (fp32, or C += z when
-// accumulate), Z = bf16(z), H = bf16(act(z)) row-major, HT = bf16(act(z)) transposed [N][M]; any may be null.
+// (mlp.cu); M % 128 == 0, N % 16 == 0, K % 16 == 0.  Epilogue: z = acc + bias[n], times silu'(gradOf[m][n])
+// when gradOf is given (back-propagation through a SiLU); C (fp32, or C += z when accumulate), Z = bf16(z),
+// H = bf16(act(z)) row-major, HT = bf16(act(z)) transposed [N][M]; any may be null.
 struct GemmArgs {
   const __nv_bfloat16* A;
   const __nv_bfloat16* B;
@@ -67,6 +68,7 @@ struct GemmArgs {
   __nv_bfloat16* Z;
   __nv_bfloat16* H;
   __nv_bfloat16* HT;
+  const __nv_bfloat16* gradOf;  // [M][N] pre-activations of the SiLU being back-propagated, or null
   uint32_t act;         // 0 identity, 1 SiLU
   uint32_t accumulate;
   uint32_t* err;
