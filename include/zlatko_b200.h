@@ -195,6 +195,28 @@ zk_status zk_surrogate_gradients(zk_surrogate* s, const float* x, const float* y
 /* Reads (get, scaling_get[34]) and / or replaces (set, scaling_set[34]) the FP32 parameters and the scaling. */
 zk_status zk_surrogate_params(zk_surrogate* s, float* get, const float* set, float* scaling_get, const float* scaling_set);
 
+/* A trade of a book the surrogate revalues: kind 0 interest-rate swap (sign +1 pay fixed, -1 receive; strike
+ * = fixed rate), 1 FX forward (sign +1), 2 FX option (sign +1 call, -1 put); asset = FX factor (forward,
+ * option); maturity in years; the surrogate predicts the value per unit notional. */
+typedef struct zk_surrogate_trade {
+  uint32_t netting_set, kind, asset;
+  int32_t sign;
+  float notional, strike, maturity, pad;
+} zk_surrogate_trade;
+/* Features of every (trade, reporting date, path): X[nTr][nR][nP][16] (the training inputs).  factors is
+ * [2 + nA][nR][nP] on the reporting dates: the deflator, the Hull-White state x, then ln S of each FX factor;
+ * resets[nTr][nR] is the reporting-date index of the reset of the swap period running on each date (-1: none),
+ * periods[nTr][nR][2] that period's start and end. */
+zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* X);
+/* Revaluation of a book by the surrogate on the GPU: features, tensor-core inference and netting per netting
+ * set, then exposure[num_netting_sets][nR][2] = (EE, EE*) on the reporting dates; netted_out (nullable,
+ * [num_netting_sets][nR][paths_out]) receives the netted values of the first paths_out paths; ms[2] (nullable) the
+ * device time of the revaluation and of the exposure reduction. */
+zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                            const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
+                            uint32_t num_netting_sets, double* exposure, float* netted_out, uint32_t paths_out, float* ms);
+
 /* Measured rate of the special-function unit's ex2 (billions per second on the whole GPU), the ceiling
  * of the fused kernel's bond exponentials (a roofline denominator; not part of the reference). */
 zk_status zk_peak_ex2(int device, double* giga_per_s);

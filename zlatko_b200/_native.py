@@ -67,7 +67,8 @@ EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last
            "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc",
            "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
            "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
-           "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
+           "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params",
+           "zk_surrogate_features", "zk_surrogate_book", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
            "zk_plan_destroy"]
 
 _lib: Optional[C.CDLL] = None
@@ -102,6 +103,9 @@ def lib() -> C.CDLL:
         "zk_surrogate_predict": (st, [vp, vp, sz, vp]),
         "zk_surrogate_gradients": (st, [vp, vp, vp, sz, vp, vp]),
         "zk_surrogate_params": (st, [vp, vp, vp, vp, vp]),
+        "zk_surrogate_features": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp]),
+        "zk_surrogate_book": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp,
+                                   C.c_uint32, vp]),
         "zk_fit_amc_f64": (st, [vp, P(PlanViewF64), vp, sz, vp, sz, vp, sz]),
         "zk_run_plan_f64": (st, [vp, P(PlanViewF64), vp, sz, P(OutputF64), vp]),
         "zk_run_plan_injected": (st, [vp, P(PlanView), vp, sz, P(Output), vp]),

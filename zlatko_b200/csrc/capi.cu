@@ -1062,6 +1062,102 @@ zk_status zk_surrogate_gradients(zk_surrogate* s, const float* x, const float* y
   }
 }
 
+zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* X) {
+  void* d = nullptr;
+  try {
+    requireCtx(ctx);
+    if (!factors || !times || !trades || !resets || !periods || !X) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t plane = static_cast<size_t>(nR) * nP, nf = (2 + nA) * plane, rows = plane * nTr;
+    for (uint32_t t = 0; t < nTr; ++t)
+      if (trades[t].kind > 2) throw fail(ZK_ERR_INVALID_ARGUMENT, "trade %u: kind %u", t, trades[t].kind);
+    for (size_t i = 0; i < static_cast<size_t>(nTr) * nR; ++i)
+      if (resets[i] >= static_cast<int32_t>(nR)) throw fail(ZK_ERR_INVALID_ARGUMENT, "reset index beyond the reporting dates");
+    const size_t o1 = (nf * 4 + 255) / 256 * 256, o2 = o1 + (nR * 4 + 255) / 256 * 256, o3 = o2 + (nTr * 32 + 255) / 256 * 256;
+    const size_t o4 = o3 + (nTr * nR * 4 + 255) / 256 * 256, o5 = o4 + (nTr * nR * 8 + 255) / 256 * 256;
+    ZK_CUDA(cudaMalloc(&d, o5 + std::max<size_t>(rows, 1) * 64));
+    unsigned char* b = static_cast<unsigned char*>(d);
+    ZK_CUDA(cudaMemcpyAsync(b, factors, nf * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + o1, times, nR * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + o2, trades, nTr * 32, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + o3, resets, nTr * nR * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + o4, periods, nTr * nR * 8, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(zk::surrogateFeatures(reinterpret_cast<const float*>(b), nA, nR, nP, reinterpret_cast<const float*>(b + o1),
+                                  reinterpret_cast<const zk::SurrogateTrade*>(b + o2), reinterpret_cast<const int32_t*>(b + o3),
+                                  reinterpret_cast<const float*>(b + o4), 0, rows, reinterpret_cast<float*>(b + o5), ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(X, b + o5, rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    ZK_CUDA(cudaFree(d));
+    return ZK_OK;
+  } catch (const Failure& f) {
+    if (d) cudaFree(d);
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                            const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
+                            uint32_t num_netting_sets, double* exposure, float* netted_out, uint32_t paths_out, float* ms) {
+  zk_context* ctx = s ? s->ctx : nullptr;
+  void* d = nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  try {
+    ctx = ctxOf(s);
+    if (!factors || !times || !trades || !resets || !periods || !exposure) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (paths_out > nP || (paths_out && !netted_out)) throw fail(ZK_ERR_INVALID_ARGUMENT, "paths_out beyond the paths");
+    for (uint32_t t = 0; t < nTr; ++t) {
+      if (trades[t].kind > 2) throw fail(ZK_ERR_INVALID_ARGUMENT, "trade %u: kind %u", t, trades[t].kind);
+      if (trades[t].netting_set >= num_netting_sets) throw fail(ZK_ERR_INVALID_ARGUMENT, "trade %u: netting set beyond the count", t);
+    }
+    for (size_t i = 0; i < static_cast<size_t>(nTr) * nR; ++i)
+      if (resets[i] >= static_cast<int32_t>(nR)) throw fail(ZK_ERR_INVALID_ARGUMENT, "reset index beyond the reporting dates");
+    const size_t plane = static_cast<size_t>(nR) * nP, nf = (2 + nA) * plane;
+    const uint32_t chunk = static_cast<uint32_t>(std::max<size_t>(1, (size_t(1) << 23) / std::max<size_t>(plane, 1)));
+    const size_t chunkRows = plane * std::min(chunk, std::max(nTr, 1u));
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t oF = take(nf * 4), oT = take(nR * 4), oTr = take(nTr * 32), oR = take(nTr * nR * 4), oP = take(nTr * nR * 8);
+    const size_t oN = take(static_cast<size_t>(num_netting_sets) * plane * 4), oE = take(num_netting_sets * nR * 16);
+    const size_t oX = take(chunkRows * 64), oY = take(chunkRows * 4);
+    ZK_CUDA(cudaMalloc(&d, off));
+    unsigned char* b = static_cast<unsigned char*>(d);
+    ZK_CUDA(cudaMemcpyAsync(b + oF, factors, nf * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + oT, times, nR * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + oTr, trades, nTr * 32, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + oR, resets, nTr * nR * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(b + oP, periods, nTr * nR * 8, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemsetAsync(b + oN, 0, static_cast<size_t>(num_netting_sets) * plane * 4, ctx->stream));
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    for (auto& e : ev) ZK_CUDA(cudaEventCreate(&e));
+    ZK_CUDA(cudaEventRecord(ev[0], ctx->stream));
+    ZK_CUDA(zk::surrogateBook(s->S, reinterpret_cast<const float*>(b + oF), nA, nR, nP, reinterpret_cast<const float*>(b + oT),
+                              reinterpret_cast<const zk::SurrogateTrade*>(b + oTr), nTr, reinterpret_cast<const int32_t*>(b + oR),
+                              reinterpret_cast<const float*>(b + oP), reinterpret_cast<float*>(b + oN), reinterpret_cast<float*>(b + oX),
+                              reinterpret_cast<float*>(b + oY), chunk));
+    ZK_CUDA(cudaEventRecord(ev[1], ctx->stream));
+    ZK_CUDA(zk::surrogateExposure(reinterpret_cast<const float*>(b + oN), reinterpret_cast<const float*>(b + oF), num_netting_sets, nR,
+                                  nP, reinterpret_cast<double*>(b + oE), ctx->stream));
+    ZK_CUDA(cudaEventRecord(ev[2], ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(exposure, b + oE, num_netting_sets * nR * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    if (paths_out)
+      ZK_CUDA(cudaMemcpy2DAsync(netted_out, paths_out * 4, b + oN, nP * 4, paths_out * 4, static_cast<size_t>(num_netting_sets) * nR,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    checkErrWord(ctx);
+    if (ms) {
+      ZK_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+      ZK_CUDA(cudaEventElapsedTime(&ms[1], ev[1], ev[2]));
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    ZK_CUDA(cudaFree(d));
+    return ZK_OK;
+  } catch (const Failure& f) {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (d) cudaFree(d);
+    return record(ctx, f);
+  }
+}
+
 zk_status zk_surrogate_params(zk_surrogate* s, float* get, const float* set, float* scaling_get, const float* scaling_set) {
   zk_context* ctx = s ? s->ctx : nullptr;
   try {

@@ -342,4 +342,115 @@ cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float
   return cudaGetLastError();
 }
 
+
+// ---- revaluation of a book by the surrogate -------------------------------------------------------------
+namespace {
+
+// Features of row (trade, reporting date r, path p), rows in [row0, row0 + n) of the trade-major order
+// ((trade * nR + r) * nP + p).  factors = [D | x | ln S_0 .. ln S_{nA-1}][nR][nP].
+__global__ void featureKernel(const float* __restrict__ factors, uint32_t nA, uint32_t nR, uint32_t nP,
+                              const float* __restrict__ times, const SurrogateTrade* __restrict__ trades,
+                              const int32_t* __restrict__ resets, const float* __restrict__ periods, uint64_t row0, uint64_t n,
+                              float* __restrict__ X) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t row = row0 + i;
+  const uint32_t p = static_cast<uint32_t>(row % nP), r = static_cast<uint32_t>((row / nP) % nR);
+  const uint32_t tr = static_cast<uint32_t>(row / (static_cast<uint64_t>(nP) * nR));
+  const SurrogateTrade T = trades[tr];
+  const size_t plane = static_cast<size_t>(nR) * nP, at = static_cast<size_t>(r) * nP + p;
+  const float t = times[r];
+  float f[16];
+  f[0] = factors[plane + at];                                                   // x
+  f[1] = T.kind != 0 && T.asset < nA ? factors[(2 + T.asset) * plane + at] : 0.0f;  // ln S of the trade's factor
+  f[2] = t;
+  f[3] = fmaxf(T.maturity - t, 0.0f);
+  f[4] = T.kind == 0 ? 1.0f : 0.0f, f[5] = T.kind == 1 ? 1.0f : 0.0f, f[6] = T.kind == 2 ? 1.0f : 0.0f;
+  f[7] = T.strike;
+  f[8] = static_cast<float>(T.sign);
+  const size_t tr_r = static_cast<size_t>(tr) * nR + r;
+  const int32_t k = resets[tr_r];
+  f[9] = k >= 0 ? factors[plane + static_cast<size_t>(k) * nP + p] : 0.0f;  // x at the current period's reset
+  const float ts = periods[2 * tr_r], te = periods[2 * tr_r + 1];
+  f[10] = k >= 0 ? t - ts : 0.0f;
+  f[11] = k >= 0 ? te - t : 0.0f;
+  f[12] = te - ts;
+  f[13] = static_cast<float>(T.asset);
+  f[14] = 0.0f, f[15] = 0.0f;
+  float4* dst = reinterpret_cast<float4*>(X + i * kIn);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) dst[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+}
+
+// netted[ns][r][p] += notional * pred for the trades [tr0, tr1) in trade order (one thread per (r, p)), zero
+// past maturity.
+__global__ void netKernel(const float* __restrict__ pred, const SurrogateTrade* __restrict__ trades, uint32_t tr0, uint32_t tr1,
+                          const float* __restrict__ times, uint32_t nR, uint32_t nP, float* __restrict__ netted) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t plane = static_cast<uint64_t>(nR) * nP;
+  if (i >= plane) return;
+  const uint32_t r = static_cast<uint32_t>(i / nP);
+  for (uint32_t tr = tr0; tr < tr1; ++tr) {
+    const SurrogateTrade T = trades[tr];
+    if (times[r] >= T.maturity - 1e-6f) continue;
+    netted[T.nettingSet * plane + i] += T.notional * pred[static_cast<size_t>(tr - tr0) * plane + i];
+  }
+}
+
+// Per (netting set, date): EE = mean max(V, 0) and EE* = mean D max(V, 0), each thread summing a strided
+// share of the paths in double, then a fixed tree.
+__global__ void exposureKernel(const float* __restrict__ netted, const float* __restrict__ D, uint32_t nR, uint32_t nP,
+                               double* __restrict__ out) {
+  __shared__ double a[256], b[256];
+  const uint32_t ns = blockIdx.y, r = blockIdx.x;
+  const float* v = netted + (static_cast<size_t>(ns) * nR + r) * nP;
+  const float* d = D + static_cast<size_t>(r) * nP;
+  double ee = 0.0, dee = 0.0;
+  for (uint32_t p = threadIdx.x; p < nP; p += 256) {
+    const double e = fmax(static_cast<double>(v[p]), 0.0);
+    ee += e, dee += static_cast<double>(d[p]) * e;
+  }
+  a[threadIdx.x] = ee, b[threadIdx.x] = dee;
+  __syncthreads();
+  for (uint32_t s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) a[threadIdx.x] += a[threadIdx.x + s], b[threadIdx.x] += b[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[(static_cast<size_t>(ns) * nR + r) * 2] = a[0] / nP;
+    out[(static_cast<size_t>(ns) * nR + r) * 2 + 1] = b[0] / nP;
+  }
+}
+
+}  // namespace
+
+cudaError_t surrogateFeatures(const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, uint64_t row0, uint64_t n,
+                              float* X, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  featureKernel<<<static_cast<uint32_t>((n + 255) / 256), 256, 0, s>>>(factors, nA, nR, nP, times, trades, resets, periods, row0, n, X);
+  return cudaGetLastError();
+}
+
+cudaError_t surrogateBook(SurrogateState& S, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* netted,
+                          float* X, float* pred, uint32_t chunkTrades) {
+  const uint64_t plane = static_cast<uint64_t>(nR) * nP;
+  for (uint32_t t0 = 0; t0 < nTr; t0 += chunkTrades) {
+    const uint32_t t1 = std::min(nTr, t0 + chunkTrades);
+    const uint64_t rows = plane * (t1 - t0);
+    SG_CUDA(surrogateFeatures(factors, nA, nR, nP, times, trades, resets, periods, plane * t0, rows, X, S.stream));
+    SG_CUDA(surrogatePredict(S, X, rows, pred));
+    netKernel<<<static_cast<uint32_t>((plane + 255) / 256), 256, 0, S.stream>>>(pred, trades, t0, t1, times, nR, nP, netted);
+    SG_CUDA(cudaGetLastError());
+  }
+  return cudaSuccess;
+}
+
+cudaError_t surrogateExposure(const float* netted, const float* D, uint32_t numNs, uint32_t nR, uint32_t nP, double* out,
+                              cudaStream_t s) {
+  exposureKernel<<<dim3(nR, numNs), 256, 0, s>>>(netted, D, nR, nP, out);
+  return cudaGetLastError();
+}
+
 }  // namespace zk

@@ -49,6 +49,13 @@ struct SurrogateState {
   size_t offOf(const float* q) const { return static_cast<size_t>(q - p); }
 };
 
+// A trade of a book revalued by the surrogate (mirrors zk_surrogate_trade of the C ABI).
+struct SurrogateTrade {
+  uint32_t nettingSet, kind, asset;
+  int32_t sign;
+  float notional, strike, maturity, pad;
+};
+
 cudaError_t surrogateCreate(SurrogateState& S, cudaStream_t stream, uint32_t* err, uint32_t seed);
 void surrogateFree(SurrogateState& S);
 // bf16 copies (row-major and transposed) of the matrices from the fp32 masters.
@@ -61,5 +68,18 @@ cudaError_t surrogateEpoch(SurrogateState& S, const float* dx, const float* dy, 
                            bool train, double* loss);
 // Predictions in original units for n device rows.
 cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float* dout);
+
+// Features of rows [row0, row0 + n) in (trade, reporting date, path) order into X [n][16].
+cudaError_t surrogateFeatures(const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, uint64_t row0, uint64_t n,
+                              float* X, cudaStream_t s);
+// Netted values [numNs][nR][nP] (accumulated into `netted`, zeroed by the caller) of a book, chunkTrades trades
+// at a time through features, prediction and netting; X and pred hold chunkTrades * nR * nP rows.
+cudaError_t surrogateBook(SurrogateState& S, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
+                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* netted,
+                          float* X, float* pred, uint32_t chunkTrades);
+// out[ns][r] = (EE, EE*) of the netted values with the deflator D [nR][nP].
+cudaError_t surrogateExposure(const float* netted, const float* D, uint32_t numNs, uint32_t nR, uint32_t nP, double* out,
+                              cudaStream_t s);
 
 }  // namespace zk

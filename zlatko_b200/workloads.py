@@ -82,8 +82,10 @@ def swap_portfolio(paths: int = 10_000) -> Tuple[S.Model, S.NettingSet, S.Option
     return m, ns, S.Options(pfe_quantile=0.975)
 
 
-def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
-    """Returns (model, netting sets, options, number of trades)."""
+def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100,
+                        num_trades: int = 1000) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
+    """Returns (model, netting sets, options, number of trades).  num_trades keeps the 60/30/10 mix of swaps,
+    FX forwards and FX options."""
     rng = np.random.default_rng(PORTFOLIO_SEED + 1)
     a, sigma = rng.uniform(0.01, 0.1), rng.uniform(0.005, 0.015)
     fx = [S.Asset(spot, rng.uniform(0.08, 0.15), S.Curve.flat(rng.uniform(0.0, 0.04))) for spot in (1.1, 0.9)]
@@ -97,13 +99,15 @@ def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100) -> Tuple[
     corr = c6[np.ix_(keep, keep)]
     m = S.Model(curve=S.Curve.flat(0.02), hw_a=a, hw_sigma=sigma, assets=fx, credits=[credit], correlation=corr,
                 num_paths=paths, seed=SIM_SEED, antithetic=True, base_grid=[k / 12.0 for k in range(1, 121)])
-    trades: list = [random_swap(rng, 120) for _ in range(600)]
-    for _ in range(300):
+    n_swaps, n_fwds = round(0.6 * num_trades), round(0.3 * num_trades)
+    n_opts = num_trades - n_swaps - n_fwds
+    trades: list = [random_swap(rng, 120) for _ in range(n_swaps)]
+    for _ in range(n_fwds):
         asset = int(rng.integers(0, 2))
         months = int(rng.integers(3, 61))
         spot = fx[asset].spot
         trades.append(S.Forward(asset, rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 1e7), spot * rng.uniform(0.9, 1.1), months / 12.0))
-    for _ in range(100):
+    for _ in range(n_opts):
         asset = int(rng.integers(0, 2))
         months = int(rng.integers(3, 37))
         spot = fx[asset].spot
