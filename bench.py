@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate leg")
+    ap.add_argument("--surrogate-paths", type=int, default=2048)
+    ap.add_argument("--no-amc", action="store_true", help="skip the Bermudan (AMC) leg")
+    ap.add_argument("--amc-paths", type=int, default=200_000)
     return ap.parse_args()
 
 
@@ -171,6 +175,73 @@ def cpu_reference(plans, trades: int, target_s: float, steps: int = 1):
     return paths * nT * trades / dt, paths, threads, dt, times, kind
 
 
+def guarded(fn, *args):
+    try:
+        return fn(*args)
+    except Exception as exc:  # pragma: no cover - reported in the JSON line instead of failing the bench
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+
+
+def surrogate_leg(ctx, a):
+    """CVA of the book (uncollateralised) by the surrogate with its plain-pricer audit against the plain GPU
+    pricer, on the same paths: device time of each and the CVA difference.  Training (on 64 paths of every trade)
+    is reported apart; it runs once per book."""
+    from zlatko_b200 import surrogate_book as SB
+    from zlatko_b200 import workloads
+    from zlatko_b200.surrogate import Surrogate
+
+    m, books, _, trades = workloads.correlated_csa_book(a.surrogate_paths)
+    book = SB.make_book(m, books)
+    t0 = time.perf_counter()
+    X, y = SB.training_set(ctx, book, 64)
+    with Surrogate(ctx, seed=1) as s:
+        for lr, ep in ((2e-3, 3), (5e-4, 2), (1e-4, 1)):
+            losses = s.train(X, y, epochs=ep, batch=8192, lr=lr)
+        train_s = time.perf_counter() - t0
+        _, dee_p, ms_plain = SB.plain_exposure(ctx, book, a.surrogate_paths)
+        run = SB.audited_exposure(ctx, s, book, a.surrogate_paths)
+    plain = float(SB.cva(book, dee_p).sum())
+    ms_sur = run.ms_surrogate + run.ms_audit + run.ms_fallback
+    revals = float(a.surrogate_paths) * len(book.times) * trades
+    return {"workload": f"correlated book, {trades} trades in 100 netting sets without CSA, {a.surrogate_paths} paths, "
+                        f"{len(book.times)} reporting dates",
+            "cva_plain": plain, "cva_surrogate_audited": float(run.cva.sum()),
+            "delta_cva_rel": float(run.cva.sum() / plain - 1.0),
+            "ms_plain": ms_plain, "ms_surrogate": run.ms_surrogate, "ms_audit": run.ms_audit, "ms_fallback": run.ms_fallback,
+            "speedup_vs_plain": ms_plain / ms_sur if ms_sur > 0 else None,
+            "surrogate_revals_per_s": revals / (run.ms_surrogate / 1e3),
+            "fallback_netting_sets": len(run.fallback), "train_rows": int(len(y)), "train_s": train_s,
+            "train_loss": float(losses[-1])}
+
+
+def amc_leg(ctx, a):
+    """Bermudan swaption book: the Longstaff-Schwartz fit on the GPU (zk_fit_amc, with its AMC state pass) and the
+    fused revaluation of the fitted plans."""
+    from zlatko_b200 import gpu, workloads
+    from zlatko_b200 import spec as S
+
+    m, books, n = workloads.bermudan_book(a.amc_paths)
+    plans = [gpu.compile(m, b, S.Options()) for b in books]
+    ctx.fit_amc(plans[0])  # warm-up
+    t0 = time.perf_counter()
+    fitted = [ctx.fit_amc(p) for p in plans]
+    fit_s = time.perf_counter() - t0
+    b = ctx.batch(fitted)
+    try:
+        for _ in range(3):
+            b.execute()
+        b.execute()
+        ms = float(np.sum(b.timings()))
+    finally:
+        b.close()
+    nT = plans[0].num_dates
+    revals = float(a.amc_paths) * nT * n
+    return {"workload": f"{n} Bermudan swaptions (10y, annual exercise 1y-9y, degree 3) in {len(books)} netting sets, "
+                        f"{a.amc_paths} paths, {nT} dates",
+            "fit_s": fit_s, "revalue_ms": ms, "revals_per_s": revals / (fit_s + ms / 1e3),
+            "revalue_revals_per_s": revals / (ms / 1e3)}
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -261,8 +332,8 @@ def main():
     fused_s = float(np.mean(fused_ms)) / 1e3
     nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
     cube_bytes = (2 + nA + nC) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
-    tiles = (nP + int(info.tile_paths) - 1) // int(info.tile_paths)
-    alg_bytes = sum(p.rows_total * nP * 4 + tiles * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
+    groups = (nP + 127) // 128  # statistics partials per 128-path group
+    alg_bytes = sum(p.rows_total * nP * 4 + groups * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
     ex2 = C_ex2 = None
     try:
         import ctypes as C
@@ -303,7 +374,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": alg_bytes / fused_s / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg_bytes / fused_s / 1e9 / peak, "traffic": traffic_per_launch(nP),
                          "note": f"revalue kernel (the dominant one); peak of {peak_kind}; algorithmic bytes = factor cube read "
-                                 "once + PFE rows written + per-tile partials + plan tables"},
+                                 "once + PFE rows written + per-group partials + plan tables"},
             "roofline_mufu": {"bound": "sfu", "achieved": exp_per_launch / fused_s / 1e9 if C_ex2 else None,
                               "peak": C_ex2 / 1e9 if C_ex2 else None, "unit": "G ex2/s",
                               "frac": exp_per_launch / fused_s / C_ex2 if C_ex2 else None},
@@ -311,6 +382,10 @@ def main():
             "plan_compile_s": compile_s,
             "cpu_baseline": cpu,
         }
+        if not a.no_surrogate:
+            line["surrogate"] = guarded(surrogate_leg, ctx, a)
+        if not a.no_amc:
+            line["amc"] = guarded(amc_leg, ctx, a)
         print(json.dumps(line))
     batch.close()
     ctx.close()
