@@ -91,6 +91,7 @@ struct Plan {
   size_t nTerms, nReq, nIdx;
   uint32_t nSlots = 0, ring = 1, ctype = 0, stateWords = 0;
   bool usesAssets = false, probes = false;
+  bool amcOrProbe = false;  // some term is an AMC or probe term (the lean revalue variant cannot run the plan)
   // The term table lowered for the revalue kernel (lowerTerms).
   std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, assetBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot
   std::vector<R> table;         // records of 4 values
@@ -166,6 +167,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
     if (kind != kBermContinue && (!(rec[1] >= R(0)) || rec[1] >= R(4294967296.0))) throw bad("invalid term slot");
     const uint32_t slot = kind == kBermContinue ? 0u : static_cast<uint32_t>(rec[1]);
     if (kind == kAsset || kind == kOption) p.usesAssets = true;
+    if (kind > kOption) p.amcOrProbe = true;
     if (kind == kProbe) {
       const uint32_t what = slot & 15u;
       if (what == 2 || what == 6) p.usesAssets = true;
@@ -310,7 +312,7 @@ struct Batch {
     std::vector<uint32_t> planIdx;
     uint32_t numFields = 0;
     size_t stateWordsMax = 0;
-    bool perTrade = false, probes = false;
+    bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
   };
   std::vector<Launch> launches;
@@ -368,6 +370,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
       L.perTrade = L.perTrade || P.nTr > 0;
       L.probes = L.probes || P.probes;
+      L.lean = L.lean && !P.amcOrProbe;
     }
     const Plan<R>& P0 = B->plans[L.planIdx.front()];
     ScenarioArgs<R>& sc = L.sc;
@@ -555,7 +558,7 @@ void execute(Batch<R>& B) {
   ZK_CUDA(cudaEventRecord(B.ev[1], s));
   for (auto& L : B.launches)
     ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                             numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, B.ppt, s));
+                             numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
   ZK_CUDA(cudaEventRecord(B.ev[2], s));
   if (!B.sink) {
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
@@ -1362,7 +1365,7 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     const auto& L = B->launches.front();
     ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
     ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                                 numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, B->ppt, s));
+                                 numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, false, B->ppt, s));
     ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, s));
     ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
     std::vector<unsigned char> host(B->outBytes);

@@ -239,8 +239,14 @@ __device__ __forceinline__ R pick4(const R (&a)[4][PPT], uint32_t k, int i) {
 
 // Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
 // statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
-template <typename R, int PPT, bool kPerTrade, bool kSink>
-__global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
+// Resident CTAs per SM the lean variants are compiled for (register budget 65536 / (128 x blocks)).
+template <int PPT, bool kLean>
+constexpr int revalueMinBlocks() {
+  return !kLean ? 1 : PPT == 1 ? 8 : PPT == 2 ? 6 : 3;
+}
+
+template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean>
+__global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
   __shared__ NsArgs<R> sA;
@@ -411,67 +417,70 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
           }
           break;
         }
-        case kBermExercise:
-#pragma unroll
-          for (int i = 0; i < PPT; ++i) {
-            const R v = c * (rec[3] * fastExp(nB * x[i]));
-            if (bm == 0) ev[0][i] += v;
-            else if (bm == 1) ev[1][i] += v;
-            else if (bm == 2) ev[2][i] += v;
-            else ev[3][i] += v;
-          }
-          break;
-        case kBermDecide:
-#pragma unroll
-          for (int i = 0; i < PPT; ++i) {
-            const R e = pick4<R, PPT>(ev, bm, i);
-            if (kSink) {
-              if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
-            } else if (pick4<R, PPT>(ex, bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
-              const R v = static_cast<R>(extra);
-              if (bm == 0) ex[0][i] = v;
-              else if (bm == 1) ex[1][i] = v;
-              else if (bm == 2) ex[2][i] = v;
-              else ex[3][i] = v;
+        default:
+          if constexpr (!kLean) switch (kind) {  // the AMC and probe terms (absent from lean launches)
+          case kBermExercise:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const R v = c * (rec[3] * fastExp(nB * x[i]));
+              if (bm == 0) ev[0][i] += v;
+              else if (bm == 1) ev[1][i] += v;
+              else if (bm == 2) ev[2][i] += v;
+              else ev[3][i] += v;
             }
-          }
-          break;
-        case kBermContinue:
-#pragma unroll
-          for (int i = 0; i < PPT; ++i)
-            if (pick4<R, PPT>(ex, bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
-          break;
-        case kBermBond:
-#pragma unroll
-          for (int i = 0; i < PPT; ++i) {
-            const R e = pick4<R, PPT>(ex, bm, i);
-            if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = c * (rec[3] * fastExp(nB * x[i]));
-          }
-          break;
-        case kProbe: {
-          const uint32_t what = slot & 15u, ix = min(slot >> 4u, 3u), ic = min(ix, 1u);
-#pragma unroll
-          for (int i = 0; i < PPT; ++i) {
-            R q;
-            switch (what) {
-              case 0: q = x[i]; break;
-              case 1: q = D[i]; break;
-              case 2: q = pick4<R, PPT>(S, ix, i); break;
-              case 3: q = ix < cb.nA ? cube(cb.fLnS + ix, j, i) : R(0); break;
-              case 4: q = ic < cb.nC ? cube(cb.fY + ic, j, i) : R(0); break;
-              case 5: q = ic < cb.nC ? cube(cb.fQ + ic, j, i) : R(1); break;
-              case 6: q = D[i] * pick4<R, PPT>(S, ix, i); break;
-              default: q = D[i] * (rec[3] * fastExp(nB * x[i]));
+            break;
+          case kBermDecide:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const R e = pick4<R, PPT>(ev, bm, i);
+              if (kSink) {
+                if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
+              } else if (pick4<R, PPT>(ex, bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
+                const R v = static_cast<R>(extra);
+                if (bm == 0) ex[0][i] = v;
+                else if (bm == 1) ex[1][i] = v;
+                else if (bm == 2) ex[2][i] = v;
+                else ex[3][i] = v;
+              }
             }
-            if (!kSink && act[i]) expo[static_cast<size_t>(static_cast<uint32_t>(rec[5])) * nP + pth[i]] = q + c;
+            break;
+          case kBermContinue:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i)
+              if (pick4<R, PPT>(ex, bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
+            break;
+          case kBermBond:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const R e = pick4<R, PPT>(ex, bm, i);
+              if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = c * (rec[3] * fastExp(nB * x[i]));
+            }
+            break;
+          case kProbe: {
+            const uint32_t what = slot & 15u, ix = min(slot >> 4u, 3u), ic = min(ix, 1u);
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              R q;
+              switch (what) {
+                case 0: q = x[i]; break;
+                case 1: q = D[i]; break;
+                case 2: q = pick4<R, PPT>(S, ix, i); break;
+                case 3: q = ix < cb.nA ? cube(cb.fLnS + ix, j, i) : R(0); break;
+                case 4: q = ic < cb.nC ? cube(cb.fY + ic, j, i) : R(0); break;
+                case 5: q = ic < cb.nC ? cube(cb.fQ + ic, j, i) : R(1); break;
+                case 6: q = D[i] * pick4<R, PPT>(S, ix, i); break;
+                default: q = D[i] * (rec[3] * fastExp(nB * x[i]));
+              }
+              if (!kSink && act[i]) expo[static_cast<size_t>(static_cast<uint32_t>(rec[5])) * nP + pth[i]] = q + c;
+            }
+            break;
           }
-          break;
-        }
-        default:  // kBermFloat
-#pragma unroll
-          for (int i = 0; i < PPT; ++i) {
-            const R e = pick4<R, PPT>(ex, bm, i);
-            if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = (c * fix(slot, i) + rec[5]) * (rec[3] * fastExp(nB * x[i]));
+          default:  // kBermFloat
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const R e = pick4<R, PPT>(ex, bm, i);
+              if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = (c * fix(slot, i) + rec[5]) * (rec[3] * fastExp(nB * x[i]));
+            }
           }
       }
       if (kPerTrade && A.nTr > 0) {
@@ -547,7 +556,7 @@ __global__ void __launch_bounds__(kTile) revalueKernel(const CubeArgs<R> cb, con
         if (A.rowTrades != kNoRow)
           for (uint32_t g = 0; g < nTr; ++g) expo[(A.rowTrades + g * A.nR + k) * nP + pi] = vt(g, i);
       }
-      if (act[i] && A.rowEx != kNoRow)
+      if (!kLean && act[i] && A.rowEx != kNoRow)
         for (uint32_t b = 0; b < min(A.nBerm, 4u); ++b) {
           const R v = pick4<R, PPT>(ex, b, i);
           expo[(A.rowEx + b) * static_cast<size_t>(nP) + pth[i]] = v < R(0) ? R(-1) : v;
@@ -623,7 +632,7 @@ size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) 
 namespace {
 template <typename R, int PPT>
 cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                             bool perTrade, bool sink, cudaStream_t stream) {
+                             bool perTrade, bool sink, bool lean, cudaStream_t stream) {
   const size_t smem = revalueSmemBytes(stateWordsMax, perTrade, sizeof(R) == 8, PPT);
   const uint64_t blocks = static_cast<uint64_t>(numTiles) * numNs;
   if (blocks == 0) return cudaSuccess;
@@ -634,20 +643,21 @@ cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uin
     kernel<<<static_cast<uint32_t>(blocks), kTile, smem, stream>>>(cb, nsArgs, numNs);
     return cudaGetLastError();
   };
-  if (sink) return go(revalueKernel<R, PPT, false, true>);
-  if (perTrade) return go(revalueKernel<R, PPT, true, false>);
-  return go(revalueKernel<R, PPT, false, false>);
+  if (sink) return go(revalueKernel<R, PPT, false, true, false>);
+  if (perTrade) return go(revalueKernel<R, PPT, true, false, false>);
+  if (lean) return go(revalueKernel<R, PPT, false, false, true>);
+  return go(revalueKernel<R, PPT, false, false, false>);
 }
 }  // namespace
 
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, int ppt, cudaStream_t stream) {
+                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream) {
   switch (ppt) {
-    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
-    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
+    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
+    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
     case 4:
-      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, stream);
+      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
@@ -655,9 +665,9 @@ cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32
 
 template cudaError_t launchSimulate<float>(const ScenarioArgs<float>&, const CubeArgs<float>&, cudaStream_t);
 template cudaError_t launchSimulate<double>(const ScenarioArgs<double>&, const CubeArgs<double>&, cudaStream_t);
-template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, int,
-                                          cudaStream_t);
-template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool, int,
-                                           cudaStream_t);
+template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, bool,
+                                          int, cudaStream_t);
+template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool, bool,
+                                           int, cudaStream_t);
 
 }  // namespace zk

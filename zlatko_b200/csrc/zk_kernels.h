@@ -15,10 +15,11 @@ template <typename R>
 cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream);
 
 // Revalue / net / collateralise / reduce: one CTA per (path tile, netting set); each thread owns `ppt`
-// paths (1, 2 or 4 in single precision, 1 or 2 in double), so a tile holds kTile * ppt paths.
+// paths (1, 2 or 4 in single precision, 1 or 2 in double), so a tile holds kTile * ppt paths.  `lean`: no
+// netting set of the launch has AMC or probe terms (a variant without their state).
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, int ppt, cudaStream_t stream);
+                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream);
 size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt);
 
 // One reduce job per plan: sums[i] = (sum over tiles of partials[tile][i]) / nP for i < n.
