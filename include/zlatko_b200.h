@@ -153,11 +153,14 @@ typedef struct zk_batch_info {
   uint64_t row_bytes;            /* bytes of per-path rows (PFE inputs) written per execute        */
   uint64_t kernels_per_execute;  /* kernel launches of one zk_batch_execute                         */
   uint64_t tile_paths;           /* paths per revalue CTA, chosen by the autotuner at creation     */
+  uint64_t graph_replay;         /* 1 once executes replay a captured CUDA graph, 0 while eager    */
 } zk_batch_info;
 
 /* Uploads the plans.  The first zk_batch_execute autotunes the tile shape (paths per revalue CTA) on
  * them, a few timed runs, unless zk_batch_set_tile_paths pinned one. */
 zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out);
+/* After the tile shape is settled, the execute sequence is captured once in a CUDA graph and replayed (the
+ * context's stream must be capturable; otherwise executes stay eager). */
 zk_status zk_batch_execute(zk_batch* b);
 /* Pins the tile shape: paths per revalue CTA, 128 x (1, 2 or 4) in single precision. */
 zk_status zk_batch_set_tile_paths(zk_batch* b, uint64_t tile_paths);

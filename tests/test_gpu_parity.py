@@ -218,6 +218,29 @@ def test_results_do_not_depend_on_the_tile_shape(ctx):
             assert np.array_equal(s0, s1) and np.array_equal(v0, v1)
 
 
+def test_batch_replays_a_cuda_graph_with_the_same_bits(ctx):
+    """After the tile shape settles, a batch's executes replay one captured CUDA graph: same results as the
+    eager first execute and as single-plan runs."""
+    m = gpu_model(3000)
+    m.base_grid = [k / 12 for k in range(1, 61)]
+    plans = [gpu.compile(m, swap_book(n, seed=s, csa=S.Csa(1e5, 1e5, 1e4)), S.Options()) for n, s in ((5, 1), (9, 2))]
+    b = ctx.batch(plans)
+    try:
+        b.execute()  # autotunes, then captures
+        first = b.read()
+        assert b.info().graph_replay == 1
+        for _ in range(3):
+            b.execute()
+        again = b.read()
+        assert np.all(b.timings() > 0)
+    finally:
+        b.close()
+    for (s0, v0), (s1, v1), p in zip(first, again, plans):
+        s2, v2 = ctx.run(p)
+        assert np.array_equal(s0, s1) and np.array_equal(v0, v1)
+        assert np.array_equal(s0, s2) and np.array_equal(v0, v2)
+
+
 def test_pfe_is_the_exact_interpolated_quantile(ctx):
     """The row-statistics kernel returns ccr::quantile of the rows the fused kernel wrote (exactly, up to
     the final rounding to float)."""

@@ -545,29 +545,35 @@ void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normal
   ZK_CUDA(cudaMemcpyAsync(B.base, B.image.data(), B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));
 }
 
+cudaError_t recordEvent(cudaEvent_t e, cudaStream_t s, bool capturing) {
+  return cudaEventRecordWithFlags(e, s, capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
+
+// Inside a stream capture the timing events must be recorded as graph nodes (cudaEventRecordExternal); an
+// ordinary record there only orders the capture.
 template <typename R>
-void execute(Batch<R>& B) {
+void execute(Batch<R>& B, bool capturing = false) {
   zk_context* ctx = B.ctx;
   cudaStream_t s = ctx->stream;
   if (!B.ev[0])
     for (auto& e : B.ev) ZK_CUDA(cudaEventCreate(&e));
   ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, s));
-  ZK_CUDA(cudaEventRecord(B.ev[0], s));
+  ZK_CUDA(recordEvent(B.ev[0], s, capturing));
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
   for (auto& L : B.launches) ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
-  ZK_CUDA(cudaEventRecord(B.ev[1], s));
+  ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   for (auto& L : B.launches)
     ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
                              numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
-  ZK_CUDA(cudaEventRecord(B.ev[2], s));
+  ZK_CUDA(recordEvent(B.ev[2], s, capturing));
   if (!B.sink) {
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
-    ZK_CUDA(cudaEventRecord(B.ev[3], s));
+    ZK_CUDA(recordEvent(B.ev[3], s, capturing));
     ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff), B.numRowJobs, ctx->dErr, s));
   } else {
-    ZK_CUDA(cudaEventRecord(B.ev[3], s));
+    ZK_CUDA(recordEvent(B.ev[3], s, capturing));
   }
-  ZK_CUDA(cudaEventRecord(B.ev[4], s));
+  ZK_CUDA(recordEvent(B.ev[4], s, capturing));
   B.timed = true;
 }
 
@@ -781,7 +787,48 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
 struct zk_batch {
   std::unique_ptr<Batch<float>> b;
   bool tuned = false;  // the tile shape was autotuned or pinned
+  // The execute sequence (simulate, revalue, reduce, row statistics and their timing events) captured once per
+  // tile shape in a CUDA graph and replayed; an execute that cannot be captured runs eagerly instead.
+  cudaGraphExec_t graph = nullptr;
+  int graphPpt = 0;
+  bool eager = false;
+  ~zk_batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
 };
+
+namespace {
+// Captures the batch's execute sequence into b->graph; returns false (and leaves no capture open) if the
+// stream cannot be captured.
+bool captureExecute(zk_batch* b) {
+  Batch<float>& B = *b->b;
+  const cudaStream_t s = B.ctx->stream;
+  if (!B.ev[0])
+    for (auto& e : B.ev) ZK_CUDA(cudaEventCreate(&e));
+  if (b->graph) cudaGraphExecDestroy(b->graph), b->graph = nullptr;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  bool ok = true;
+  try {
+    execute(B, true);
+  } catch (const Failure&) {
+    ok = false;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (!ok || e != cudaSuccess || !g || cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    b->graph = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  cudaGraphDestroy(g);
+  b->graphPpt = B.ppt;
+  return true;
+}
+}  // namespace
 
 extern "C" {
 
@@ -1220,7 +1267,13 @@ zk_status zk_batch_execute(zk_batch* b) {
       autotune(*b->b);  // first execute: time the tile shapes on this batch, keep the fastest
       b->tuned = true;
     }
-    execute(*b->b);
+    if (!b->eager && (!b->graph || b->graphPpt != b->b->ppt) && !captureExecute(b)) b->eager = true;
+    if (b->eager) {
+      execute(*b->b);
+    } else {
+      ZK_CUDA(cudaGraphLaunch(b->graph, b->b->ctx->stream));
+      b->b->timed = true;
+    }
     return ZK_OK;
   } catch (const Failure& f) {
     return record(b->b->ctx, f);
@@ -1286,6 +1339,7 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
   }
   info->kernels_per_execute = 2 * B.launches.size() + 2;
   info->tile_paths = static_cast<uint64_t>(kTile) * B.ppt;
+  info->graph_replay = b->graph && !b->eager && b->graphPpt == B.ppt ? 1u : 0u;
   return ZK_OK;
 }
 
