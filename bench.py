@@ -175,6 +175,19 @@ def cpu_reference(plans, trades: int, target_s: float, steps: int = 1):
     return paths * nT * trades / dt, paths, threads, dt, times, kind
 
 
+def replica_throughput(units: float, t_device: float, t_e2e: float, world: int, dist=None, device: str = "cpu"):
+    """Whole-job throughput of `world` replicas: every rank processed `units`; the job takes the slowest rank's
+    time (max over ranks of the device time and of the end-to-end time).  Returns (value, e2e, t_device, t_e2e)."""
+    if dist is not None and world > 1:
+        import torch
+
+        t = torch.tensor([t_device, t_e2e], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_device, t_e2e = float(t[0]), float(t[1])
+    total = units * world
+    return total / t_device, total / t_e2e, t_device, t_e2e
+
+
 def guarded(fn, *args):
     try:
         return fn(*args)
@@ -318,15 +331,8 @@ def main():
             t0 = time.perf_counter()
             ctx.run_many(plans)
             e2e_s.append(time.perf_counter() - t0)
-    t_step = float(np.sum(step_ms)) / 1e3
-    t_e2e = float(np.sum(e2e_s))
-    if dist:
-        t = torch.tensor([t_step, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_step, t_e2e = float(t[0]), float(t[1])
-    total = revals * world * a.steps
-    value = total / t_step
-    e2e = total / t_e2e
+    value, e2e, t_step, t_e2e = replica_throughput(revals * a.steps, float(np.sum(step_ms)) / 1e3, float(np.sum(e2e_s)), world,
+                                                   dist, "cuda")
 
     peak, peak_kind = peaks()
     fused_s = float(np.mean(fused_ms)) / 1e3
