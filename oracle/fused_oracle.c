@@ -12,7 +12,7 @@
 
 #include "oracle.h"
 
-enum { WG = 64, STATS = 8, TRADE_STATS = 5, MAX_ASSETS = 4, MAX_CREDITS = 2, MAX_SLOTS = 32, MAX_NORMALS = 64,
+enum { INNER_TOP = 16, WG = 64, STATS = 8, TRADE_STATS = 5, MAX_ASSETS = 4, MAX_CREDITS = 2, MAX_SLOTS = 32, MAX_NORMALS = 64,
        MAX_TRADES = 16, MAX_BERM = 4, CHOL = 8, STEP = 24, TERM = 8, REQ = 8 };
 #define NO_ROW 0xFFFFFFFFu
 #define NOT_EXERCISED 0xFFFFFFFFu
@@ -74,12 +74,24 @@ static float amc_poly(const float* rec, float x) {
   return ((rec[7] * z + rec[6]) * z + rec[5]) * z + rec[4];
 }
 
-typedef struct {
+typedef struct PlanS {
   const uint32_t *H, *I;
   const float *FP, *ST, *T;
   uint32_t nP, nT, nA, nC, sub, nNormals, seed, anti, hasCsa, cpty, nCorr, offCall, offRep, nS, nR, nTr;
   uint32_t rowDV, rowE, rowV, rowC, rowGross, rowTrades, rowEx, nBerm, rowEP;
+  uint32_t rowIm, nInner;
+  float imLevel;
 } Plan;
+
+/* Nested Monte Carlo for the conditional initial margin (fused_reference.cpp:108-196): one inner path's state
+ * and its exact step from date j - 1 to j on its own stream (the outer step with the inner normals). */
+typedef struct {
+  float x, lnD, lnS[MAX_ASSETS], S[MAX_ASSETS], y[MAX_CREDITS], Y[MAX_CREDITS];
+} InnerPath;
+
+struct PlanS;
+static void inner_step(const struct PlanS* v, InnerPath* st, uint32_t j, uint32_t stream, float sign);
+static float inner_value(const struct PlanS* v, const InnerPath* st, float* fix, uint32_t* ex, uint32_t j);
 
 /* The AMC regression pass records x and the deflator on every date and each exercise value instead of
  * deciding exercise (fused_reference.cpp:89-97, 275-281). */
@@ -261,6 +273,48 @@ static void simulate_path(const Plan* v, uint32_t p, float* stats, float* expo, 
         for (uint32_t i = 0; i < nTr; ++i) PUT(v->rowTrades, (size_t)i * v->nR + k, vt[i]);
 #undef PUT
     }
+    /* Nested Monte Carlo: the conditional initial margin of this path on this reporting date, the imLevel
+     * quantile of |V_inner(t + MPR) - V(t)| over nInner inner paths from the grid's kInnerTop largest samples
+     * (fused_reference.cpp:356-393). */
+    if (rs > 0 && v->nInner > 0) {
+      const uint32_t target = v->I[v->offRep + v->nT + j];
+      float im = 0.0f;
+      if (target != NO_ROW) {
+        float top[INNER_TOP];
+        memset(top, 0, sizeof top);
+        InnerPath start;
+        memset(&start, 0, sizeof start);
+        start.x = x, start.lnD = lnD;
+        for (int a = 0; a < MAX_ASSETS; ++a) start.lnS[a] = lnS[a], start.S[a] = S[a];
+        for (int c = 0; c < MAX_CREDITS; ++c) start.y[c] = y[c], start.Y[c] = Y[c];
+        for (uint32_t i = 0; i < v->nInner; ++i) {
+          InnerPath st = start;
+          float f2[MAX_SLOTS];
+          uint32_t e2[MAX_BERM];
+          memcpy(f2, fix, sizeof f2);
+          memcpy(e2, exercised, sizeof e2);
+          const uint32_t istream = pcg_hash(stream ^ pcg_hash(0x85EBCA6Bu + (i >> 1u) * 0x9E3779B9u + j));
+          const float isign = (i & 1u) == 1u ? -1.0f : 1.0f;
+          float vi = value;
+          for (uint32_t jj = j + 1; jj <= target; ++jj) {
+            inner_step(v, &st, jj, istream, isign);
+            vi = inner_value(v, &st, f2, e2, jj);
+          }
+          float cur = fabsf(vi - value);
+          for (uint32_t k = 0; k < INNER_TOP; ++k)
+            if (cur > top[k]) {
+              const float t = top[k];
+              top[k] = cur, cur = t;
+            }
+        }
+        const float rank = v->imLevel * (float)(v->nInner - 1);
+        const uint32_t k = (uint32_t)floorf(rank);
+        const uint32_t hiIdx = v->nInner - 1 - k < INNER_TOP - 1 ? v->nInner - 1 - k : INNER_TOP - 1;
+        const float ok = top[hiIdx], ok1 = hiIdx > 0 ? top[hiIdx - 1] : ok;
+        im = ok + (rank - (float)k) * (ok1 - ok);
+      }
+      if (v->rowIm != NO_ROW) expo[((size_t)v->rowIm + rs - 1) * stride] = im;
+    }
     if (v->rowEx != NO_ROW)
       for (uint32_t i = 0; i < v->nBerm && i < MAX_BERM; ++i)
         expo[((size_t)v->rowEx + i) * stride] = exercised[i] == NOT_EXERCISED ? -1.0f : (float)exercised[i];
@@ -279,6 +333,91 @@ static void simulate_path(const Plan* v, uint32_t p, float* stats, float* expo, 
       st[k] = i < nTr ? trade_stat((k - STATS) % TRADE_STATS, vt[i], value, D) : 0.0f;
     }
   }
+}
+
+static void inner_step(const Plan* v, InnerPath* st, uint32_t j, uint32_t stream, float sign) {
+  const float* FP = v->FP;
+  const float* step = v->ST + (size_t)j * STEP;
+  float z[MAX_NORMALS], w[CHOL];
+  memset(z, 0, sizeof z);
+  const uint32_t nZ = 4 * ((v->nNormals + 3) / 4);
+  for (uint32_t k = 0; k < nZ; k += 2) normal_pair(stream, j, k / 2, &z[k]);
+  for (uint32_t k = 0; k < nZ; ++k) z[k] *= sign;
+  for (int i = 0; i < CHOL; ++i) {
+    const float* row = &FP[16 + i * CHOL];
+    const float d0 = row[0] * z[0] + row[1] * z[1] + row[2] * z[2] + row[3] * z[3];
+    const float d1 = row[4] * z[4] + row[5] * z[5] + row[6] * z[6] + row[7] * z[7];
+    w[i] = d0 + d1;
+  }
+  const float integrated = st->x * step[5] + step[2] * w[0] + step[3] * z[v->nCorr] + step[4];
+  st->x = st->x * step[0] + step[1] * w[0];
+  st->lnD = st->lnD - integrated;
+  for (int a = 0; a < MAX_ASSETS; ++a) {
+    st->lnS[a] = st->lnS[a] + (integrated - step[8 + a] - step[16 + a] + step[12 + a] * w[1 + a]);
+    st->S[a] = FP[12 + a] * expf(st->lnS[a]);
+  }
+  const float dt = step[6];
+  uint32_t off = v->nCorr + 1;
+  for (uint32_t c = 0; c < v->nC; ++c) {
+    const float kappa = FP[4 * c], theta = FP[4 * c + 1], xi = FP[4 * c + 2];
+    const float h = dt / (float)v->sub;
+    float rem = sqrtf(dt) * w[1 + v->nA + c], remT = dt, yy = st->y[c], YY = st->Y[c];
+    for (uint32_t s = 0; s < v->sub; ++s) {
+      float dW = rem;
+      if (s + 1 < v->sub) dW = h / remT * rem + sqrtf(maxf(h * (remT - h) / remT, 0.0f)) * z[off + s];
+      rem -= dW;
+      remT -= h;
+      const float yp = maxf(yy, 0.0f);
+      const float yn = yy + kappa * (theta - yp) * h + xi * sqrtf(yp) * dW;
+      YY += 0.5f * (yp + maxf(yn, 0.0f)) * h;
+      yy = yn;
+    }
+    st->y[c] = yy;
+    st->Y[c] = YY;
+    off += v->sub - 1;
+  }
+}
+
+/* The netting set's value on an inner path (no trade groups, no probes). */
+static float inner_value(const Plan* v, const InnerPath* st, float* fix, uint32_t* ex, uint32_t j) {
+  float value = 0.0f, ev[MAX_BERM] = {0, 0, 0, 0};
+  const float x = st->x;
+  for (uint32_t t = v->I[j]; t < v->I[j + 1]; ++t) {
+    const float* rec = v->T + (size_t)t * TERM;
+    const uint32_t code = (uint32_t)rec[0];
+    const uint32_t kind = code & 15u, extra = code >> 12u;
+    uint32_t bm = (code >> 8u) & 15u;
+    if (bm > MAX_BERM - 1) bm = MAX_BERM - 1;
+    const uint32_t slot = (uint32_t)rec[1];
+    const float c = rec[2];
+    const float bond = rec[3] * expf(-rec[4] * x);
+    switch (kind) {
+      case 0: value += c * bond; break;
+      case 1: value += (fix[slot] * c + rec[5]) * bond; break;
+      case 2: value += c * st->S[slot] * rec[3]; break;
+      case 3: fix[slot] = (bond - 1.0f) / c; break;
+      case 4: {
+        const float p3 = rec[7];
+        value += c * black76(st->S[slot] * rec[5] / bond, rec[6], fabsf(p3), bond, p3 > 0.0f);
+        break;
+      }
+      case 5: ev[bm] += c * bond; break;
+      case 6:
+        if (ex[bm] == NOT_EXERCISED && ev[bm] > 0.0f && ev[bm] > amc_poly(rec, x)) ex[bm] = extra;
+        break;
+      case 7:
+        if (ex[bm] == NOT_EXERCISED) value += rec[1] * maxf(amc_poly(rec, x), 0.0f);
+        break;
+      case 8:
+        if (ex[bm] != NOT_EXERCISED && ex[bm] <= extra) value += c * bond;
+        break;
+      case 9:
+        if (ex[bm] != NOT_EXERCISED && ex[bm] <= extra) value += (fix[slot] * c + rec[5]) * bond;
+        break;
+      default: break;
+    }
+  }
+  return value;
 }
 
 static int cmp_double(const void* a, const void* b) {
@@ -309,9 +448,10 @@ static int read_plan(Plan* v, const uint32_t* header, const uint32_t* indices, c
   v->cpty = header[9], v->nCorr = header[11], v->offCall = header[12], v->offRep = header[13], v->nS = header[16];
   v->nR = header[17], v->nTr = header[18], v->rowDV = header[19], v->rowE = header[20], v->rowV = header[21];
   v->rowC = header[22], v->rowGross = header[23], v->rowTrades = header[24], v->rowEx = header[25];
-  v->nBerm = header[27], v->rowEP = header[28];
-  if (v->nP == 0 || v->nT == 0 || header[30] != 0) {
-    if (err && errLen) snprintf(err, errLen, "empty plan or nested initial margin");
+  v->nBerm = header[27], v->rowEP = header[28], v->rowIm = header[29], v->nInner = header[30];
+  memcpy(&v->imLevel, &header[31], sizeof(float));
+  if (v->nP == 0 || v->nT == 0) {
+    if (err && errLen) snprintf(err, errLen, "empty plan");
     return 1;
   }
   return 0;

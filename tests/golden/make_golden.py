@@ -1,7 +1,7 @@
 """Generates the golden fixtures of the exposure path from the reference itself.
 
 Run in a container that has the reference's sources (``make -C oracle ref`` builds oracle/_ref/libccr_ref.so
-from them): ``python tests/golden/make_golden.py``.  Each fixture holds the flat model / netting-set / options
+from them): ``python tests/golden/make_golden.py [name ...]``.  Each fixture holds the flat model / netting-set / options
 arrays, the tables the reference's gpu::compile produced for them, and what the reference computed:
 
   fused_*.npz   gpu::runFusedReference (the reference's FP32 CPU kernels): sums and values; plus, for every
@@ -47,6 +47,9 @@ def fused_cases():
     m = gpu_model(300, seed=11)
     m.base_grid = [k / 12 for k in range(1, 61)]
     yield "fused_swap_book", m, swap_book(6, seed=5, csa=S.Csa(1e5, 1e5, 1e4)), S.Options(pfe_quantile=0.9)
+    m, ns = gpu_setup(256, True)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0), degree=2))
+    yield "fused_nested_im", m, ns, S.Options(im_quantile=0.99, im_inner_paths=64, samples=2)
 
 
 def engine_cases():
@@ -56,9 +59,12 @@ def engine_cases():
 
 
 def main() -> None:
+    only = set(sys.argv[1:])  # fixture names to (re)generate; all when none are given
     if not ref.available():
         raise SystemExit("oracle/_ref/libccr_ref.so is not built: run `make -C oracle ref` where the reference is")
     for name, m, ns, o in fused_cases():
+        if only and name not in only:
+            continue
         em, en, eo = S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o)
         r = ref.compile_plan(em, en, eo)
         sums, values = ref.run_fused(r)
@@ -75,6 +81,8 @@ def main() -> None:
                             reporting=r.reporting.astype(np.int64), sums=sums, values=values, exact_quantiles=exact)
         print(name, r.num_dates, "dates", r.stats_per_date, "stats", len(r.requests) // 8, "requests")
     for name, m, ns, seed in engine_cases():
+        if only and name not in only:
+            continue
         em, en = S.encode_model(m), S.encode_netting_set(ns)
         from zlatko_b200 import gpu
 

@@ -11,7 +11,9 @@ pytestmark = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not bui
 
 OPTIONS = [S.Options(), S.Options(per_trade=True, im_quantile=0.99),
            S.Options(samples=12, histogram_time=2.0, gross=True, collateral_bands=True, trade_views=True),
-           S.Options(factor_views=True, samples=5, bond_maturity=8.0), S.Options(pfe_quantile=0.975)]
+           S.Options(factor_views=True, samples=5, bond_maturity=8.0), S.Options(pfe_quantile=0.975),
+           S.Options(im_quantile=0.99, im_inner_paths=64, samples=2), S.Options(per_trade=True, im_quantile=0.95, im_inner_paths=40),
+           S.Options(im_quantile=0.99, im_inner_paths=128, im_audit_paths=32, im_audit_inner_paths=512, im_margin_period=20 / 250)]
 
 
 def _ref_plan(m, ns, o):
@@ -102,6 +104,15 @@ def test_invalid_inputs_raise_like_the_reference():
         gpu.compile(m, ns, S.Options(counterparty=3))
     with pytest.raises(ValueError):
         gpu.compile(m, ns, S.Options(im_quantile=1.5))
+    # Nested initial margin (fused_exposure.cpp:233-247): 2 to 1024 inner paths, the quantile's order statistic
+    # among the 16 largest samples, an audit with more inner paths than the kernel.
+    for o in (S.Options(im_quantile=0.99, im_inner_paths=1), S.Options(im_quantile=0.99, im_inner_paths=2048),
+              S.Options(im_quantile=0.5, im_inner_paths=64),
+              S.Options(im_quantile=0.99, im_inner_paths=64, im_audit_paths=8, im_audit_inner_paths=64)):
+        with pytest.raises(ValueError):
+            gpu.compile(m, ns, o)
+        with pytest.raises(ValueError):
+            ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o))
     m.assets, m.correlation = m.assets * 5, None
     with pytest.raises(ValueError):
         gpu.compile(m, ns, S.Options())

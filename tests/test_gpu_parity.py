@@ -139,7 +139,7 @@ def test_two_schedule_swap_book(ctx):
 
 
 @pytest.mark.parametrize("name", ["fused_plain", "fused_csa_views", "fused_bond_collateral", "fused_asset_collateral",
-                                  "fused_bermudan", "fused_swap_book"])
+                                  "fused_bermudan", "fused_swap_book", "fused_nested_im"])
 def test_golden_fixtures(ctx, name):
     """The reference's own tables run on the GPU reproduce the reference's own outputs.  These fixtures have a
     few hundred paths, so one margin call that CUDA's and glibc's single-precision exponentials decide
@@ -147,13 +147,73 @@ def test_golden_fixtures(ctx, name):
     with securities collateral); the collateralised and Bermudan fixtures allow 1e-3."""
     f, p = fixture(name)
     sg, vg = ctx.run(p)
-    loose = name in ("fused_bermudan", "fused_bond_collateral", "fused_asset_collateral")
+    loose = name in ("fused_bermudan", "fused_bond_collateral", "fused_asset_collateral", "fused_nested_im")
     check_sums(p, sg, f["sums"], rtol=1e-3 if loose else RTOL)
     exact = f["values"].copy()
     for q in p.requests.reshape(-1, 8):  # quantiles: the exact ccr::quantile of the reference's rows
         if int(q[0]) in (0, 7):
             exact[int(q[7])] = f["exact_quantiles"][int(q[7])]
     check_values(p, vg, exact, rtol=1e-3 if loose else RTOL)
+
+
+# ---------------------------------------------------------------- nested initial margin
+IM_OPTIONS = [S.Options(im_quantile=0.99, im_inner_paths=64, samples=2),
+              S.Options(per_trade=True, im_quantile=0.95, im_inner_paths=40),  # lanes 8..31 run one inner path
+              S.Options(im_quantile=1.0, im_inner_paths=33)]                   # the largest sample: order statistic 0
+
+
+def check_im_rows(p, rg, rr, tol):
+    """The margin rows [nR][paths]: each path's margin is an order statistic of |V_inner - V| over its inner paths,
+    a continuous function of the values, so it moves with their rounding (CUDA's against glibc's single-precision
+    exponentials); an inner Bermudan exercise decided differently at its boundary moves one sample, so the bound
+    on single paths is on 99.9% of them, the mean of every date holds on all."""
+    im, nR = int(p.header[29]), p.num_reporting
+    a, b = rg[im:im + nR].astype(np.float64), rr[im:im + nR].astype(np.float64)
+    scale = np.abs(b).max()
+    assert scale > 0 and np.isfinite(a).all()
+    err = np.abs(a - b)
+    assert np.quantile(err, 0.999) <= tol * scale, np.quantile(err, 0.999) / scale
+    assert np.abs(a.mean(1) - b.mean(1)).max() <= tol * scale
+
+
+@pytest.mark.parametrize("csa", [False, True])
+@pytest.mark.parametrize("oi", range(len(IM_OPTIONS)))
+def test_nested_initial_margin(ctx, csa, oi):
+    m, ns = gpu_setup(1500, csa)
+    p = gpu.compile(m, ns, IM_OPTIONS[oi])
+    sg, vg, rg = ctx.run(p, rows=True)
+    sr, vr, rr = restated.run_plan(p, rows=True)
+    check_sums(p, sg, sr)
+    check_values(p, vg, vr, rtol=1e-3 if csa else RTOL)
+    check_im_rows(p, rg, rr, 1e-3 if csa else RTOL)
+
+
+def test_nested_initial_margin_with_bermudans_and_1024_inner_paths(ctx):
+    m, ns = gpu_setup(256, True)
+    ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=True, degree=2))
+    ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=False, position=-0.5, degree=3))
+    p = gpu.compile(m, ns, S.Options(im_quantile=0.99, im_inner_paths=1024), fit=ctx)
+    sg, vg, rg = ctx.run(p, rows=True)
+    sr, vr, rr = restated.run_plan(p, rows=True)
+    check_sums(p, sg, sr, rtol=1e-3)
+    check_im_rows(p, rg, rr, 1e-3)
+
+
+def test_nested_initial_margin_in_a_batch_and_a_graph(ctx):
+    """Batched with plans without the margin (one shared scenario), replayed from the captured graph: the same
+    bits as the single run."""
+    m, ns = gpu_setup(2000, True)
+    p_im = gpu.compile(m, ns, S.Options(im_quantile=0.99, im_inner_paths=64))
+    p_plain = gpu.compile(m, ns, S.Options())
+    s1, v1 = ctx.run(p_im)
+    b = ctx.batch([p_plain, p_im, p_plain])
+    try:
+        for _ in range(3):
+            b.execute()
+            out = b.read()
+            assert np.array_equal(out[1][0], s1) and np.array_equal(out[1][1][: p_im.num_outputs], v1[: p_im.num_outputs])
+    finally:
+        b.close()
 
 
 @pytest.mark.parametrize("physical", [True, False])
@@ -283,11 +343,19 @@ def test_invalid_plans_are_rejected(ctx):
                                 p.num_outputs, p.times, p.reporting)
     with pytest.raises(ZkError, match="INVALID_PLAN"):
         ctx.run(bad2)
-    h = p.header.copy()
-    h[30] = 64  # nested initial margin: not run by this build
-    with pytest.raises(ZkError, match="UNSUPPORTED"):
-        ctx.run(gpu.Plan.from_arrays(h, p.indices, p.params, p.steps, p.terms, p.requests, p.rows_total, p.num_outputs,
-                                     p.times, p.reporting))
+    pim = gpu.compile(m, ns, S.Options(im_quantile=0.99, im_inner_paths=64))
+    h = pim.header.copy()
+    h[30] = 2048  # nested initial margin: more inner paths than the reference's 1024
+    with pytest.raises(ZkError, match="INVALID_PLAN"):
+        ctx.run(gpu.Plan.from_arrays(h, pim.indices, pim.params, pim.steps, pim.terms, pim.requests, pim.rows_total,
+                                     pim.num_outputs, pim.times, pim.reporting))
+    idx = pim.indices.copy()
+    nT = pim.num_dates
+    rep = np.nonzero(idx[2 * nT + 1:3 * nT + 1])[0]
+    idx[3 * nT + 1 + rep[1]] = rep[1]  # an initial-margin target on its own date
+    with pytest.raises(ZkError, match="INVALID_PLAN"):
+        ctx.run(gpu.Plan.from_arrays(pim.header, idx, pim.params, pim.steps, pim.terms, pim.requests, pim.rows_total,
+                                     pim.num_outputs, pim.times, pim.reporting))
     # The context stays usable after errors.
     s, v = ctx.run(p)
     assert np.isfinite(s).all()

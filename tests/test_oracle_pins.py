@@ -23,7 +23,7 @@ from zlatko_b200 import spec as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FUSED = ["fused_plain", "fused_csa_views", "fused_bond_collateral", "fused_asset_collateral", "fused_bermudan",
-         "fused_swap_book"]
+         "fused_swap_book", "fused_nested_im"]
 needs_ref = pytest.mark.skipif(not ref.available(), reason="the reference is not built in this container")
 
 
@@ -181,7 +181,9 @@ def test_workgroup_order_matters_only_through_rounding():
 # ------------------------------------------------------------------ 3. the reference itself
 OPTIONS = [S.Options(), S.Options(per_trade=True, im_quantile=0.99),
            S.Options(samples=12, histogram_time=2.0, gross=True, collateral_bands=True, trade_views=True),
-           S.Options(factor_views=True, samples=5, bond_maturity=8.0), S.Options(pfe_quantile=0.975)]
+           S.Options(factor_views=True, samples=5, bond_maturity=8.0), S.Options(pfe_quantile=0.975),
+           S.Options(im_quantile=0.99, im_inner_paths=64, samples=2),
+           S.Options(per_trade=True, im_quantile=0.95, im_inner_paths=40)]
 
 
 @needs_ref

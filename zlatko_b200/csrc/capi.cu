@@ -90,6 +90,12 @@ struct Plan {
   uint32_t rowDV, rowE, rowV, rowC, rowGross, rowTrades, rowEx, rowEP;
   size_t nTerms, nReq, nIdx;
   uint32_t nSlots = 0, ring = 1, ctype = 0, stateWords = 0;
+  // Nested initial margin: inner paths per outer path and date, the quantile level, the row block; `im` when
+  // the plan asks for the margin rows, with the (date, target date) of each reporting slot.
+  uint32_t nInner = 0, rowIm = kNoRow;
+  float imLevel = 0.0f;
+  bool im = false;
+  std::vector<uint32_t> imSlots;  // [nR][2]
   bool usesAssets = false, probes = false;
   bool amcOrProbe = false;  // some term is an AMC or probe term (the lean revalue variant cannot run the plan)
   // The term table lowered for the revalue kernel (lowerTerms).
@@ -114,7 +120,8 @@ Plan<R> parse(const View<R>& v, size_t index) {
   p.rowDV = H[hRowDV], p.rowE = H[hRowE], p.rowV = H[hRowV], p.rowC = H[hRowC], p.rowGross = H[hRowGross];
   p.rowTrades = H[hRowTrades], p.rowEx = H[hRowEx], p.rowEP = H[hRowEP];
   if (p.nP == 0 || p.nT == 0) throw bad("empty plan");
-  if (H[hInner] != 0) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the nested initial margin (imInnerPaths > 0) is not run by this build", index);
+  p.nInner = H[hInner], p.rowIm = H[hRowIm];
+  std::memcpy(&p.imLevel, &H[hImLevel], sizeof(float));
   if (!v.params || v.params_len != static_cast<size_t>(kParamCount)) throw bad("params must hold 84 values");
   if (!v.steps || v.steps_len != static_cast<size_t>(p.nT) * kStepStride) throw bad("steps must hold nT * 24 values");
   if (p.nA > kMaxAssets) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: at most 4 assets", index);
@@ -137,6 +144,17 @@ Plan<R> parse(const View<R>& v, size_t index) {
   for (uint32_t j = 0; j < p.nT; ++j)
     if (I[j] > I[j + 1]) throw bad("term starts must not decrease");
   if (I[p.nT] > p.nTerms) throw bad("term starts beyond the term table");
+  if (p.nInner > 0) {
+    // The reference's inner Monte Carlo (fused_reference.cpp:356-393): targets after their date, at most
+    // kMaxInnerPaths inner paths, a quantile level in [0, 1].
+    if (p.nInner > static_cast<uint32_t>(kMaxInnerPaths)) throw bad("more than 1024 inner paths");
+    if (!(p.imLevel >= 0.0f && p.imLevel <= 1.0f)) throw bad("initial-margin quantile level outside [0, 1]");
+    if (v.indices_len < 4 * static_cast<size_t>(p.nT) + 1) throw bad("index table too short for the initial-margin targets");
+    for (uint32_t j = 0; j < p.nT; ++j) {
+      const uint32_t t = I[p.offRep + p.nT + j];
+      if (t != kNoRow && (t <= j || t >= p.nT)) throw bad("initial-margin target date not after its date");
+    }
+  }
   const uint32_t rows = v.rows_total;
   uint32_t maxLag = 0, maxSlot = 0;
   bool anySlot = false;
@@ -157,6 +175,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
   rowBlock(p.rowGross, p.nR, "gross rows beyond rows_total");
   rowBlock(p.rowTrades, static_cast<uint64_t>(std::min<uint32_t>(p.nTr, kMaxTradeGroups)) * p.nR, "trade rows beyond rows_total");
   rowBlock(p.rowEx, std::min<uint32_t>(p.nBerm, kMaxBermudans), "exercise rows beyond rows_total");
+  if (p.nInner > 0) rowBlock(p.rowIm, p.nR, "initial-margin rows beyond rows_total");
   if (p.rowEP == kNoRow) throw bad("the exposure rows are required");
   for (size_t t = 0; t < p.nTerms; ++t) {
     const R* rec = v.terms + t * kTermStride;
@@ -213,6 +232,18 @@ Plan<R> parse(const View<R>& v, size_t index) {
     throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the margin-call look-back spans %u dates (at most %d)", index, maxLag, kMaxRing - 1);
   if (p.ctype == 2) p.usesAssets = true;
   p.stateWords = p.nSlots + (p.hasCsa ? p.ring * (p.ctype != 0 ? 2 : 1) : 0);
+  p.im = p.nInner > 0 && p.rowIm != kNoRow;
+  if (p.im) {
+    // The full revalue variant records the outer state on the reporting dates; the inner paths start from it
+    // and from ln S in the factor cube.
+    p.probes = true;
+    p.amcOrProbe = true;
+    p.imSlots.assign(2 * static_cast<size_t>(p.nR), kNoRow);
+    for (uint32_t j = 0; j < p.nT; ++j) {
+      const uint32_t rs = I[p.offRep + j];
+      if (rs > 0) p.imSlots[2 * (rs - 1)] = j, p.imSlots[2 * (rs - 1) + 1] = I[p.offRep + p.nT + j];
+    }
+  }
   lowerTerms(p);
   return p;
 }
@@ -319,6 +350,7 @@ struct Batch {
   // device offsets per plan
   struct Dev {
     size_t dates, table, steps, req, expo, partials, sums, values;
+    size_t imSlots = 0, imModel = 0, imState = 0;  // nested initial margin: slots [nR][2], spots + Cholesky, outer state
   };
   std::vector<Dev> dev;
   size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
@@ -326,6 +358,7 @@ struct Batch {
   uint32_t numRowJobs = 0, maxReduceN = 0;
   int ppt = 2;                        // paths per revalue thread: the tile shape (autotuned by zk_batch_create)
   std::vector<ReduceJob<R>> reduceJobs;  // host copy; numTiles follows ppt
+  std::vector<ImArgs<R>> im;             // nested initial margin launches, after the revalue launches
   std::vector<unsigned char> image;  // host image of the input region
   unsigned char* base = nullptr;     // device arena
   bool ownsArena = false;
@@ -404,6 +437,10 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     D.table = take(P.table.size() * sizeof(R));
     D.steps = take(static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
     D.req = take(P.nReq * kRequestStride * sizeof(R));
+    if (P.im) {
+      D.imSlots = take(P.imSlots.size() * 4);
+      D.imModel = take((4 + kChol * kChol) * sizeof(R));
+    }
   }
   for (auto& L : B->launches) L.nsOff = take(L.planIdx.size() * sizeof(NsArgs<R>));
   B->reduceOff = take(nPlans * sizeof(ReduceJob<R>));
@@ -426,6 +463,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     const uint32_t tiles = (P.nP + kTile - 1) / kTile;  // the most tiles any tile shape uses
     B->dev[i].expo = take(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
     B->dev[i].partials = take(static_cast<size_t>(tiles) * P.nT * P.nS * sizeof(R));
+    if (P.im && !sink) B->dev[i].imState = take(static_cast<size_t>(P.nR) * (5 + P.nSlots) * P.nP * sizeof(R));
   }
   if (sink) {
     const auto& P = B->plans[0];
@@ -448,6 +486,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
 template <typename R>
 void fillImage(Batch<R>& B, const double* normals, size_t streams) {
   B.image.assign(B.inputBytes, 0);
+  B.im.clear();
   unsigned char* img = B.image.data();
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
   auto dptr = [&](size_t o) { return reinterpret_cast<void*>(base + o); };
@@ -458,6 +497,10 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
     std::memcpy(img + D.table, P.table.data(), P.table.size() * sizeof(R));
     std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
     if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
+    if (P.im) {
+      std::memcpy(img + D.imSlots, P.imSlots.data(), P.imSlots.size() * 4);
+      std::memcpy(img + D.imModel, P.v.params + 12, (4 + kChol * kChol) * sizeof(R));
+    }
   }
   for (auto& L : B.launches) {
     std::vector<NsArgs<R>> args(L.planIdx.size());
@@ -481,6 +524,19 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
       A.rowTrades = P.rowTrades, A.rowEx = P.rowEx;
       A.offCall = P.offCall, A.offRep = P.offRep, A.nSlots = P.nSlots, A.ring = P.ring;
       A.usesAssets = P.usesAssets ? 1u : 0u;
+      if (P.im && !B.sink) {
+        A.imState = static_cast<R*>(dptr(D.imState));
+        A.imWords = 5 + P.nSlots;
+        ImArgs<R> M{};
+        M.cube = static_cast<const R*>(dptr(L.cubeOff));
+        M.dates = A.dates, M.table = A.table, M.steps = A.steps;
+        M.model = static_cast<const R*>(dptr(D.imModel));
+        M.slots = static_cast<const uint32_t*>(dptr(D.imSlots));
+        M.state = A.imState, M.expo = A.expo;
+        M.nP = P.nP, M.nT = P.nT, M.nA = P.nA, M.fLnS = L.cb.fLnS, M.nR = P.nR, M.nSlots = P.nSlots, M.nInner = P.nInner;
+        M.rowIm = P.rowIm, M.seed = P.seed, M.anti = P.anti, M.nCorr = P.nCorr, M.level = static_cast<R>(P.imLevel);
+        B.im.push_back(M);
+      }
       if (B.sink) {
         A.sinkX = static_cast<R*>(dptr(B.sinkOff[0]));
         A.sinkD = static_cast<R*>(dptr(B.sinkOff[1]));
@@ -565,6 +621,7 @@ void execute(Batch<R>& B, bool capturing = false) {
   for (auto& L : B.launches)
     ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
                              numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
+  for (const auto& M : B.im) ZK_CUDA(launchNestedIm<R>(M, s));
   ZK_CUDA(recordEvent(B.ev[2], s, capturing));
   if (!B.sink) {
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
@@ -1420,6 +1477,7 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
     ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
                                  numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, false, B->ppt, s));
+    for (const auto& M : B->im) ZK_CUDA(launchNestedIm<float>(M, s));
     ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, s));
     ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
     std::vector<unsigned char> host(B->outBytes);

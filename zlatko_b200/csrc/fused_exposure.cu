@@ -237,14 +237,14 @@ __device__ __forceinline__ R pick4(const R (&a)[4][PPT], uint32_t k, int i) {
   return k == 0 ? a[0][i] : k == 1 ? a[1][i] : k == 2 ? a[2][i] : a[3][i];
 }
 
-// Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
-// statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
 // Resident CTAs per SM the lean variants are compiled for (register budget 65536 / (128 x blocks)).
 template <int PPT, bool kLean>
 constexpr int revalueMinBlocks() {
   return !kLean ? 1 : PPT == 1 ? 8 : PPT == 2 ? 6 : 3;
 }
 
+// Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
+// statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
 template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean>
 __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
@@ -556,6 +556,13 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
         if (A.rowTrades != kNoRow)
           for (uint32_t g = 0; g < nTr; ++g) expo[(A.rowTrades + g * A.nR + k) * nP + pi] = vt(g, i);
       }
+      if (!kLean && !kSink && rs > 0 && A.imState && act[i]) {  // the start of this path's inner paths
+        R* st = A.imState + static_cast<size_t>(rs - 1) * A.imWords * nP + pth[i];
+        st[0] = value[i];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) st[static_cast<size_t>(1 + b) * nP] = pick4<R, PPT>(ex, b, i);
+        for (uint32_t q = 0; q < nSlots; ++q) st[static_cast<size_t>(5 + q) * nP] = fix(q, i);
+      }
       if (!kLean && act[i] && A.rowEx != kNoRow)
         for (uint32_t b = 0; b < min(A.nBerm, 4u); ++b) {
           const R v = pick4<R, PPT>(ex, b, i);
@@ -617,6 +624,212 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
 }
 
 // ---------------------------------------------------------------------------------------------
+// Nested Monte Carlo for the conditional initial margin (the reference's innerStep / innerValue and the
+// inner loop of simulatePath: fused_reference.cpp:108-196, 356-393).  The reference runs the nInner inner
+// paths of an outer path one after the other inside the path's thread; here one warp takes one
+// (reporting slot, outer path) and its lanes run inner paths lane, lane + 32, ... side by side: every lane of
+// the warp steps the same dates, so the date's records are warp-uniform broadcasts, and the grid holds
+// nR x nP warps instead of nP threads.
+
+// One inner path's exact step to date jj on its own stream: the outer step's short rate and asset levels
+// with the inner normals (the intensity enters no value and is not stepped).  Pairs past the normals the
+// Cholesky rows and the integrated rate read stay zero; the Cholesky factor is zero there.
+template <typename R>
+__device__ __forceinline__ void innerStep(const ImArgs<R>& M, uint32_t jj, uint32_t stream, R sign, R& x, R (&lnS)[4],
+                                          R (&S)[4]) {
+  R z[8];
+  const uint32_t pairs = M.nCorr / 2 + 1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    z[2 * k] = z[2 * k + 1] = R(0);
+    if (static_cast<uint32_t>(k) < pairs) {
+      gauss2(stream, jj, static_cast<uint32_t>(k), z[2 * k], z[2 * k + 1]);
+      z[2 * k] *= sign, z[2 * k + 1] *= sign;
+    }
+  }
+  R w[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const R* row = M.model + 4 + i * kChol;
+    const R d0 = __ldg(row) * z[0] + __ldg(row + 1) * z[1] + __ldg(row + 2) * z[2] + __ldg(row + 3) * z[3];
+    const R d1 = __ldg(row + 4) * z[4] + __ldg(row + 5) * z[5] + __ldg(row + 6) * z[6] + __ldg(row + 7) * z[7];
+    w[i] = d0 + d1;
+  }
+  R zc = R(0);  // the independent normal of the integrated rate, z[nCorr]
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (static_cast<uint32_t>(k) == M.nCorr) zc = z[k];
+  const R* st = M.steps + static_cast<size_t>(jj) * kStepStride;
+  const R integrated = x * __ldg(st + 5) + __ldg(st + 2) * w[0] + __ldg(st + 3) * zc + __ldg(st + 4);
+  x = x * __ldg(st) + __ldg(st + 1) * w[0];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+    if (static_cast<uint32_t>(a) < M.nA) {
+      lnS[a] = lnS[a] + (integrated - __ldg(st + 8 + a) - __ldg(st + 16 + a) + __ldg(st + 12 + a) * w[1 + a]);
+      S[a] = __ldg(M.model + a) * rexp(lnS[a]);
+    }
+}
+
+// The netting set's value on date jj of one inner path, from the date's lowered runs (the outer kernel's
+// order: floating coupons, bonds, asset forwards, generic records, fixings); no trade groups, no probes.
+// fix points at the lane's fixings, fixing s at fix[s * 32].
+template <typename R>
+__device__ R innerDateValue(const ImArgs<R>& M, uint32_t jj, R x, const R (&S)[4], R* fix, R (&ex)[4]) {
+  using R4 = typename Vec4<R>::T;
+  const uint4* dates = reinterpret_cast<const uint4*>(M.dates);
+  const uint4 d0 = __ldg(dates + 2 * jj), d1 = __ldg(dates + 2 * jj + 1);
+  const R* table = M.table;
+  R value = R(0), ev[4] = {R(0), R(0), R(0), R(0)};
+  for (uint32_t u = d0.x; u < d0.y; ++u) {
+    const R4 r = ld4(table + 4 * u);
+    value += (r.x * fix[static_cast<uint32_t>(r.w) * 32u] + r.y) * termExp(r.z, x);
+  }
+  for (uint32_t u = d0.y; u < d0.z; ++u) {
+    const R4 r = ld4(table + 4 * u);
+    value += r.x * termExp(r.y, x) + r.z * termExp(r.w, x);
+  }
+  for (uint32_t u = d0.z; u < d0.w; ++u) {
+    const R4 r = ld4(table + 4 * u);
+    value += r.x * sel4(S, static_cast<uint32_t>(r.z) & 3u) * r.y;
+  }
+  for (uint32_t u = d0.w; u < d1.x; u += 2) {
+    R rec[8];
+    loadTerm(table + 4 * u, rec);
+    const uint32_t code = static_cast<uint32_t>(rec[0]);
+    const uint32_t kind = code & 15u, bm = min((code >> 8u) & 15u, 3u), extra = code >> 12u;
+    const uint32_t slot = static_cast<uint32_t>(rec[1]);
+    const R c = rec[2];
+    switch (kind) {
+      case kBond: value += c * (rec[3] * fastExp(-rec[4] * x)); break;
+      case kFixedFloat: value += (c * fix[slot * 32u] + rec[5]) * (rec[3] * fastExp(-rec[4] * x)); break;
+      case kAsset: value += c * sel4(S, slot & 3u) * rec[3]; break;
+      case kSetFixing: fix[slot * 32u] = (rec[3] * fastExp(-rec[4] * x) - R(1)) / c; break;
+      case kOption: {
+        const R b0 = rec[3] * fastExp(-rec[4] * x);
+        value += c * black(sel4(S, slot & 3u) * rec[5] / b0, rec[6], fabs(rec[7]), b0, rec[7] > R(0));
+        break;
+      }
+      case kBermExercise: add4(ev, bm, c * (rec[3] * fastExp(-rec[4] * x))); break;
+      case kBermDecide:
+        if (sel4(ex, bm) < R(0) && sel4(ev, bm) > R(0) && sel4(ev, bm) > amcPoly(rec, x)) set4(ex, bm, static_cast<R>(extra));
+        break;
+      case kBermContinue:
+        if (sel4(ex, bm) < R(0)) value += rec[1] * fmax(amcPoly(rec, x), R(0));
+        break;
+      case kBermBond: {
+        const R e = sel4(ex, bm);
+        if (e >= R(0) && e <= static_cast<R>(extra)) value += c * (rec[3] * fastExp(-rec[4] * x));
+        break;
+      }
+      case kBermFloat: {
+        const R e = sel4(ex, bm);
+        if (e >= R(0) && e <= static_cast<R>(extra)) value += (c * fix[slot * 32u] + rec[5]) * (rec[3] * fastExp(-rec[4] * x));
+        break;
+      }
+      default: break;  // probes write rows of the outer path only
+    }
+  }
+  for (uint32_t u = d1.x; u < d1.y; ++u) {
+    const R4 r = ld4(table + 4 * u);
+    fix[static_cast<uint32_t>(r.w) * 32u] = (r.x * termExp(r.y, x) - R(1)) * r.z;
+  }
+  return value;
+}
+
+constexpr int kImWarps = 4;
+
+// One warp per (reporting slot r, outer path p), item r * nP + p.  Each lane keeps the 16 largest of its
+// samples |V_inner(target) - V| in descending order (the reference's insertion, which never admits a NaN);
+// 16 rounds of a warp maximum over the lanes' heads then give the 16 largest of all nInner samples, the
+// same multiset as the reference's single list, and the quantile interpolates between two of them.
+template <typename R>
+__global__ void __launch_bounds__(kImWarps * 32) nestedImKernel(const ImArgs<R> M) {
+  extern __shared__ __align__(16) unsigned char smemRaw[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  R* fixIn = reinterpret_cast<R*>(smemRaw) + static_cast<size_t>(warp) * M.nSlots * 33u;  // [nSlots][32] inner
+  R* fixOut = fixIn + M.nSlots * 32u;                                                     // [nSlots] outer
+  const uint64_t item = static_cast<uint64_t>(blockIdx.x) * kImWarps + warp;
+  if (item >= static_cast<uint64_t>(M.nR) * M.nP) return;  // warp-uniform; no block barrier below
+  const uint32_t r = static_cast<uint32_t>(item / M.nP), p = static_cast<uint32_t>(item % M.nP);
+  const uint32_t j = __ldg(M.slots + 2 * r), target = __ldg(M.slots + 2 * r + 1);
+  if (j == kNoRow) return;  // a reporting slot on no date: the outer kernel writes no row for it either
+  R* out = M.expo + static_cast<size_t>(M.rowIm + r) * M.nP + p;
+  if (target == kNoRow) {
+    if (lane == 0) *out = R(0);
+    return;
+  }
+  const size_t nP = M.nP, fs = static_cast<size_t>(M.nT) * nP;
+  const R* os = M.state + static_cast<size_t>(r) * (5 + M.nSlots) * nP + p;
+  const R value = os[0];
+  R ex0[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) ex0[b] = os[(1 + b) * nP];
+  for (uint32_t q = lane; q < M.nSlots; q += 32) fixOut[q] = os[(5 + q) * nP];
+  __syncwarp();
+  const R x0 = M.cube[static_cast<size_t>(j) * nP + p];
+  R lnS0[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+    lnS0[a] = static_cast<uint32_t>(a) < M.nA ? M.cube[(M.fLnS + a) * fs + static_cast<size_t>(j) * nP + p] : R(0);
+  const uint32_t pathStream = M.anti ? p >> 1u : p;
+  const uint32_t stream = pcg(pcg(M.seed) ^ pcg(pathStream + 0x9E3779B9u));
+
+  R top[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) top[k] = R(0);
+  for (uint32_t i = lane; i < M.nInner; i += 32) {
+    R x = x0, lnS[4], S[4], ex[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) lnS[a] = lnS0[a], S[a] = R(0), ex[a] = ex0[a];
+    for (uint32_t q = 0; q < M.nSlots; ++q) fixIn[q * 32u + lane] = fixOut[q];
+    const uint32_t istream = pcg(stream ^ pcg(0x85EBCA6Bu + (i >> 1u) * 0x9E3779B9u + j));
+    const R isign = (i & 1u) ? R(-1) : R(1);
+    R vi = value;
+    for (uint32_t jj = j + 1; jj <= target; ++jj) {
+      innerStep(M, jj, istream, isign, x, lnS, S);
+      vi = innerDateValue(M, jj, x, S, fixIn + lane, ex);
+    }
+    R cur = fabs(vi - value);
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (cur > top[k]) {
+        const R t = top[k];
+        top[k] = cur, cur = t;
+      }
+  }
+  const R rank = M.level * static_cast<R>(M.nInner - 1);
+  const uint32_t k = static_cast<uint32_t>(floor(rank));
+  const uint32_t hi = min(M.nInner - 1 - k, 15u);
+  R ok = R(0), ok1 = R(0);
+  for (uint32_t round = 0; round <= hi; ++round) {
+    R m = top[0];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, d));
+    if (round + 1 == hi) ok1 = m;
+    if (round == hi) ok = m;
+    const uint32_t owner = __ffs(__ballot_sync(0xFFFFFFFFu, top[0] == m)) - 1;
+    if (lane == owner) {
+#pragma unroll
+      for (int q = 0; q < 15; ++q) top[q] = top[q + 1];
+      top[15] = R(0);
+    }
+  }
+  if (hi == 0) ok1 = ok;
+  if (lane == 0) *out = ok + (rank - static_cast<R>(k)) * (ok1 - ok);
+}
+
+template <typename R>
+cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream) {
+  const uint64_t items = static_cast<uint64_t>(M.nR) * M.nP;
+  if (items == 0 || M.nInner == 0) return cudaSuccess;
+  const uint64_t blocks = (items + kImWarps - 1) / kImWarps;
+  if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  const size_t smem = static_cast<size_t>(kImWarps) * M.nSlots * 33u * sizeof(R);
+  nestedImKernel<R><<<static_cast<uint32_t>(blocks), kImWarps * 32, smem, stream>>>(M);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
 template <typename R>
 cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream) {
   const uint32_t blocks = (sc.nP + 255) / 256;
@@ -663,6 +876,8 @@ cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32
   }
 }
 
+template cudaError_t launchNestedIm<float>(const ImArgs<float>&, cudaStream_t);
+template cudaError_t launchNestedIm<double>(const ImArgs<double>&, cudaStream_t);
 template cudaError_t launchSimulate<float>(const ScenarioArgs<float>&, const CubeArgs<float>&, cudaStream_t);
 template cudaError_t launchSimulate<double>(const ScenarioArgs<double>&, const CubeArgs<double>&, cudaStream_t);
 template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, bool,

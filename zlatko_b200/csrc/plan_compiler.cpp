@@ -23,6 +23,7 @@ namespace zk::host {
 namespace {
 constexpr std::size_t kMaxAssets = 4, kMaxCredits = 2, kMaxSlots = 32, kMaxNormals = 64, kMaxTradeGroups = 16;
 constexpr std::size_t kMaxBermudans = 4, kMaxExercises = 64, kMaxAmcDegree = 3, kStepStride = 24, kTermStride = 8;
+constexpr std::size_t kMaxInnerPaths = 1024, kInnerTop = 16;  // nested initial margin (fused_exposure.hpp:57-58)
 constexpr std::size_t kParamCount = 84, kMaxSamples = 64, kPfeBins = 3072, kStatsPerDate = 8, kTradeStats = 5;
 constexpr std::uint32_t kNoRow = 0xFFFFFFFFu;
 enum Kind { kBond = 0, kFixedFloat = 1, kAsset = 2, kSetFixing = 3, kOption = 4, kBermExercise = 5, kBermDecide = 6,
@@ -396,7 +397,22 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   if (o.gross || o.tradeViews) eff.perTrade = true;
   if (eff.perTrade && ns.trades.size() > kMaxTradeGroups) throw std::invalid_argument("per-trade statistics on the GPU support at most 16 trades");
   if (o.imQuantile < 0.0 || o.imQuantile > 1.0) throw std::invalid_argument("imQuantile must be in [0, 1]");
-  if (o.imInnerPaths > 0) throw std::invalid_argument("the nested initial margin (imInnerPaths > 0) is not compiled by this build");
+  if (o.imInnerPaths > 0) {
+    // The kernel keeps the kInnerTop largest inner samples: the quantile's order statistic must be among them
+    // (gpu::compile, fused_exposure.cpp:233-247).
+    auto checkInner = [&](std::size_t n) {
+      if (n > kMaxInnerPaths || n < 2) throw std::invalid_argument("nested initial margin: 2 to 1024 inner paths");
+      const double rank = o.imQuantile * static_cast<double>(n - 1);
+      if (static_cast<double>(n - 1) - std::floor(rank) >= static_cast<double>(kInnerTop - 1))
+        throw std::invalid_argument("nested initial margin: the quantile needs more inner paths (keeps the 16 largest)");
+    };
+    checkInner(o.imInnerPaths);
+    if (o.imAuditPaths > 0) {
+      checkInner(o.imAuditInnerPaths);
+      if (o.imAuditInnerPaths <= o.imInnerPaths)
+        throw std::invalid_argument("nested initial margin: the audit needs more inner paths than the kernel");
+    }
+  }
   if (m.assets.size() > kMaxAssets) throw std::invalid_argument("GPU kernel supports at most 4 assets");
   if (m.credits.size() > kMaxCredits) throw std::invalid_argument("GPU kernel supports at most 2 credits");
   for (const auto& c : m.credits)
@@ -417,6 +433,12 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   if (ns.csa && ns.csa->mpr > 0.0)
     for (double x : reporting.t)
       if (x > ns.csa->mpr) sim.push_back(x - ns.csa->mpr);
+  // Nested initial margin: inner paths run from every reporting date t to t + MPR, so t + MPR joins the grid.
+  if (o.imInnerPaths > 0) {
+    const double horizon = reporting.t.back();
+    for (double x : reporting.t)
+      if (x + o.imMarginPeriod <= horizon + 1e-10) sim.push_back(x + o.imMarginPeriod);
+  }
   sim.insert(sim.end(), o.extraDates.begin(), o.extraDates.end());
   const Grid grid(sim);
   const std::size_t nT = grid.t.size();
@@ -672,11 +694,12 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   if (o.gross) L.gross = block(nR);
   if (o.tradeViews) L.trades = block(static_cast<std::uint32_t>(nTr * nR));
   if (o.exerciseViews && !amc.empty()) L.exercise = block(static_cast<std::uint32_t>(amc.size()));
+  if (o.imInnerPaths > 0) L.conditionalIm = block(nR);
   auto probe = [&](std::size_t j, std::uint32_t row, int what, std::size_t index, double offset = 0.0, double A = 0.0, double B = 0.0) {
     at[j].push_back(Term{kProbe, static_cast<double>(what + 16 * static_cast<int>(index)), offset, A, B, static_cast<double>(row), 0.0, 0.0, 0, 0, 0});
   };
   std::uint32_t deflatorRows = kNoRow;
-  if (o.gross || o.tradeViews || o.factorViews) {
+  if (o.gross || o.tradeViews || o.factorViews || o.imInnerPaths > 0) {
     deflatorRows = block(nR);
     for (std::uint32_t r = 0; r < nR; ++r) probe(repDates[r], deflatorRows + r, 1, 0);
   }
@@ -731,6 +754,11 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
     perDate(kRowSamples, L.netted, static_cast<std::uint32_t>(S));
     if (L.collateral != kNoRow) perDate(kRowSamples, L.collateral, static_cast<std::uint32_t>(S));
   }
+  if (L.conditionalIm != kNoRow) {
+    perDate(kRowMeanProduct, L.conditionalIm, 1, 0.0, deflatorRows);
+    perDate(kRowMean, L.conditionalIm);
+    for (double q : {0.05, 0.5, 0.95}) perDate(kRowQuantile, L.conditionalIm, 1, q);
+  }
   if (o.collateralBands && L.collateral != kNoRow)
     for (double q : o.bandLevels) perDate(kRowQuantile, L.collateral, 1, q);
   if (o.gross) profileOf(L.gross);
@@ -782,6 +810,10 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   const std::size_t offCall = nT + 1, offRep = offCall + nT, offIm = offRep + nT;
   P.indices.assign(offIm + nT, kNoRow);
   for (std::size_t j = 0; j < offIm; ++j) P.indices[j] = 0u;
+  if (o.imInnerPaths > 0)
+    for (std::size_t r = 0; r < nR; ++r)
+      if (const auto target = grid.find(grid.t[repDates[r]] + o.imMarginPeriod, 1e-8))
+        P.indices[offIm + repDates[r]] = static_cast<std::uint32_t>(*target);
   for (std::size_t j = 0; j < nT; ++j) {
     P.indices[j] = static_cast<std::uint32_t>(P.terms.size() / kTermStride);
     auto emit = [&](const std::vector<Term>& recs, std::size_t group) {
@@ -865,7 +897,8 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
               floatBits(static_cast<float>(o.pfeQuantile)), static_cast<std::uint32_t>(numWG), static_cast<std::uint32_t>(P.statsPerDate),
               nR, static_cast<std::uint32_t>(perTradeGroups), L.valueChange, L.exposureValue, L.netted, L.collateral, L.gross,
               L.trades, L.exercise, static_cast<std::uint32_t>(P.requests.size() / 8), static_cast<std::uint32_t>(amc.size()),
-              L.exposure, L.conditionalIm, 0u, floatBits(static_cast<float>(o.imQuantile))};
+              L.exposure, L.conditionalIm, static_cast<std::uint32_t>(o.imInnerPaths),
+              floatBits(static_cast<float>(o.imQuantile))};
   auto toF = [](const std::vector<double>& v) {
     std::vector<float> f(v.size());
     for (std::size_t k = 0; k < v.size(); ++k) f[k] = static_cast<float>(v[k]);

@@ -26,6 +26,7 @@ constexpr int kMaxNormals = 64;
 constexpr int kMaxBermudans = 4;
 constexpr int kMaxTradeGroups = 16;
 constexpr int kMaxRing = 32;           // look-back depth (dates) of the CSA margin call kept on chip
+constexpr int kMaxInnerPaths = 1024;    // inner paths of the nested initial margin per outer path and date
 constexpr int kTermChunk = 128;        // terms staged in shared memory at a time
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 
@@ -90,6 +91,11 @@ struct NsArgs {
   R* sinkD;
   R* sinkEx;
   const uint32_t* sinkRowOfBermudan;  // first exercise row of each Bermudan
+  // Nested initial margin: on each reporting date the outer state the inner paths start from, written to
+  // imState[(slot * imWords + w) * nP + path] with w = 0 the netted value, 1..4 the Bermudans' exercise
+  // indices, 5.. the fixings (imWords = 5 + nSlots; imState null without the nested margin).
+  R* imState;
+  uint32_t imWords, pad1;
 };
 
 // ---- counter-based normals: PCG hash + Box-Muller, keyed by (seed, path stream, date, pair) ----

@@ -22,6 +22,24 @@ cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32
                           bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream);
 size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt);
 
+// The nested initial margin of one plan (fused_reference.cpp:356-393), after its revalue launch: one warp
+// per (reporting slot, outer path), the lanes running the inner paths; the margin into rows rowIm + r.
+template <typename R>
+struct ImArgs {
+  const R* cube;          // the launch's factor cube: x in field 0, ln S of asset a in field fLnS + a
+  const uint32_t* dates;  // the plan's lowered date descriptors [nT][8] and records
+  const R* table;
+  const R* steps;         // [nT][24]
+  const R* model;         // spots [4] | padded Cholesky factor [8][8]
+  const uint32_t* slots;  // [nR][2]: the date of reporting slot r (kNoRow: none), its target date (kNoRow: none)
+  const R* state;         // the outer state on the reporting dates (NsArgs::imState)
+  R* expo;                // the plan's rows
+  uint32_t nP, nT, nA, fLnS, nR, nSlots, nInner, rowIm, seed, anti, nCorr, pad;
+  R level;                // the margin's quantile level
+};
+template <typename R>
+cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream);
+
 // One reduce job per plan: sums[i] = (sum over tiles of partials[tile][i]) / nP for i < n.
 template <typename R>
 struct ReduceJob {
