@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--surrogate-paths", type=int, default=2048)
     ap.add_argument("--no-amc", action="store_true", help="skip the Bermudan (AMC) leg")
     ap.add_argument("--amc-paths", type=int, default=200_000)
+    ap.add_argument("--no-im", action="store_true", help="skip the nested initial-margin leg")
+    ap.add_argument("--im-paths", type=int, default=20_000)
     return ap.parse_args()
 
 
@@ -255,6 +257,83 @@ def amc_leg(ctx, a):
             "revalue_revals_per_s": revals / (ms / 1e3)}
 
 
+def inner_revaluations(plan, trades: int) -> float:
+    """Inner path-date-trade revaluations of one run of a plan with the nested margin: every path, on every
+    reporting date with a target, steps its inner paths to the target date and revalues the netting set there."""
+    nT, nP, nInner = plan.num_dates, plan.num_paths, int(plan.header[30])
+    I = plan.indices
+    rep, tgt = I[2 * nT + 1:3 * nT + 1], I[3 * nT + 1:4 * nT + 1]
+    dates = sum(int(tgt[j]) - j for j in range(nT) if rep[j] > 0 and tgt[j] != 0xFFFFFFFF)
+    return float(nP) * nInner * dates * trades
+
+
+def im_leg(ctx, a):
+    """Nested conditional initial margin with the reference's XVA defaults (128 inner paths, the 99% quantile,
+    a 10-day margin period) on the book's largest netting set: inner revaluations per second of the whole plan
+    on the GPU and on the reference's CPU kernels (a path sample, all host threads), and the device time of the
+    inner Monte Carlo (the plan's revalue phase with the margin minus without)."""
+    from oracle import ref
+    from zlatko_b200 import gpu, workloads
+    from zlatko_b200 import spec as S
+
+    m, books, _, _ = workloads.correlated_csa_book(a.im_paths)
+    ns = max(books, key=lambda b: len(b.trades))
+    p_im, p0 = gpu.compile(m, ns, S.Options(im_quantile=0.99, im_inner_paths=128)), gpu.compile(m, ns, S.Options(im_quantile=0.99))
+
+    def device_ms(p):
+        b = ctx.batch([p])
+        try:
+            for _ in range(3):
+                b.execute()
+            t = []
+            for _ in range(5):
+                b.execute()
+                t.append(b.timings())
+            return np.median(np.array(t), axis=0)
+        finally:
+            b.close()
+
+    ms_im, ms0 = device_ms(p_im), device_ms(p0)
+    trades = len(ns.trades)
+    inner = inner_revaluations(p_im, trades)
+    line = {"workload": f"largest CSA netting set of the correlated book ({trades} trades), {a.im_paths} paths, 128 inner paths, "
+                        f"99% quantile, 10-day margin period, {p_im.num_dates} dates",
+            "inner_revals_per_s": inner / (float(ms_im.sum()) / 1e3), "plan_ms": float(ms_im.sum()),
+            "inner_mc_ms": float(ms_im[1] - ms0[1]), "plan_without_margin_ms": float(ms0.sum())}
+    if not a.no_cpu:
+        if ref.available():
+            kind, threads = "reference", os.cpu_count() or 1
+
+            def run(n):
+                rp = ref.plan_from_buffers(p_im.header, p_im.indices, p_im.params, p_im.steps, p_im.terms, p_im.requests,
+                                           p_im.rows_total, p_im.num_outputs, p_im.times, p_im.reporting, num_paths=n)
+                t0 = time.perf_counter()
+                ref.run_fused(rp, threads)
+                return time.perf_counter() - t0
+        else:
+            from oracle import restated
+
+            kind, threads = "port", 1
+
+            def run(n):
+                h = p_im.header.copy()
+                h[0], h[15] = n, (n + 63) // 64
+                t0 = time.perf_counter()
+                restated.run_fused(h, p_im.indices, p_im.params, p_im.steps, p_im.terms, p_im.requests, p_im.rows_total,
+                                   p_im.num_outputs)
+                return time.perf_counter() - t0
+
+        sample = 64
+        dt = run(sample)
+        sample = int(min(a.im_paths, max(64, sample * 5.0 / max(dt, 1e-3))) // 64 * 64)  # about 5 s of CPU work
+        dt = run(sample)
+        cpu = inner * sample / a.im_paths / dt
+        line["cpu_baseline"] = {"value": cpu, "unit": "inner revaluations/s", "cores": threads, "kind": kind,
+                                "sample": f"{sample} of {a.im_paths} paths of the same plan"}
+        line["speedup_vs_cpu"] = line["inner_revals_per_s"] / cpu
+    return line
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,6 +471,8 @@ def main():
             line["surrogate"] = guarded(surrogate_leg, ctx, a)
         if not a.no_amc:
             line["amc"] = guarded(amc_leg, ctx, a)
+        if not a.no_im:
+            line["nested_im"] = guarded(im_leg, ctx, a)
         print(json.dumps(line))
     batch.close()
     ctx.close()

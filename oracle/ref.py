@@ -54,6 +54,8 @@ def lib() -> C.CDLL:
         L.ref_amc_rows.argtypes = [C.c_void_p]
         L.ref_summarise.restype = C.c_int
         L.ref_summarise.argtypes = [C.c_void_p, _fp, _fp, _dp, C.c_char_p, sz]
+        L.ref_summarise_views.restype = C.c_int
+        L.ref_summarise_views.argtypes = [C.c_void_p, _fp, _fp, _dp, sz, C.c_char_p, sz]
         L.ref_engine_run.restype = C.c_void_p
         L.ref_engine_run.argtypes = [_dp, sz, _dp, sz, C.c_double, C.c_void_p, sz, C.c_char_p, sz]
         L.ref_engine_free.argtypes = [C.c_void_p]
@@ -216,6 +218,26 @@ def summarise(plan: RefPlan, sums: np.ndarray, values: np.ndarray) -> dict:
     r = {k: out[i * nR:(i + 1) * nR] for i, k in enumerate(SUMMARY_FIELDS)}
     r["times"] = plan.times[plan.reporting.astype(np.int64)]
     r["pathwise_cva_04"] = out[9 * nR]
+    return r
+
+
+VIEW_FIELDS = ("value_change_quantile", "conditional_im_discounted", "conditional_im_mean", "conditional_im_band_05",
+               "conditional_im_band_50", "conditional_im_band_95", "conditional_discounted_ee",
+               "conditional_im_audit_ratio", "conditional_im_discounted_uncorrected")
+TRADE_FIELDS = ("marginal_discounted", "marginal", "incremental_discounted", "standalone_discounted", "standalone")
+
+
+def summarise_views(plan: RefPlan, sums: np.ndarray, values: np.ndarray) -> dict:
+    """The rest of gpu::summarise's FusedResult per reporting date (NaN rows where the result has none), with
+    the nested-IM audit the reference runs inside summarise; "trades" holds one dict per trade group."""
+    nR, nTr = len(plan.reporting), int(plan.header[18])
+    out = np.zeros((9 + 5 * nTr) * nR)
+    e = _err()
+    if lib().ref_summarise_views(plan.handle, np.ascontiguousarray(sums, np.float32), np.ascontiguousarray(values, np.float32),
+                                 out, out.size, e, 512):
+        raise ValueError(e.value.decode())
+    r = {k: out[i * nR:(i + 1) * nR] for i, k in enumerate(VIEW_FIELDS)}
+    r["trades"] = [{k: out[(9 + 5 * t + i) * nR:(10 + 5 * t + i) * nR] for i, k in enumerate(TRADE_FIELDS)} for t in range(nTr)]
     return r
 
 

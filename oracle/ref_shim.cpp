@@ -20,6 +20,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <limits>
 #include <vector>
 
 #include "ccr/core/math.hpp"
@@ -447,6 +448,39 @@ int ref_summarise(const void* h, const float* sums, const float* values, double*
     for (std::size_t c = 0; c < cols.size(); ++c)
       for (std::size_t k = 0; k < nR; ++k) out[c * nR + k] = (*cols[c])[k];
     out[9 * nR] = r.pathwiseCva(0.4);
+    return 0;
+  } catch (const std::exception& e) {
+    setError(err, errlen, e);
+    return 1;
+  }
+}
+
+// The rest of gpu::summarise's result per reporting date, in blocks of nR doubles (NaN where the result has
+// no such series): valueChangeQuantile, conditionalImDiscounted, conditionalImMean, the three
+// conditionalImBands, conditionalDiscountedEe, conditionalImAuditRatio, conditionalImDiscountedUncorrected,
+// then for each trade group its marginalDiscounted, marginal, incrementalDiscounted, standaloneDiscounted,
+// standalone.  out holds (9 + 5 * numTradeGroups) * nR doubles.
+int ref_summarise_views(const void* h, const float* sums, const float* values, double* out, std::size_t nOut, char* err,
+                        std::size_t errlen) {
+  try {
+    const auto& p = *static_cast<const gpu::FusedPlan*>(h);
+    gpu::FusedOutput o;
+    o.sums.assign(sums, sums + p.numDates() * p.statsPerDate);
+    o.values.assign(values, values + std::max<std::size_t>(1, p.numOutputs));
+    const auto r = gpu::summarise(p, o);
+    const std::size_t nR = p.reporting.size();
+    if (nOut != (9 + 5 * r.trades.size()) * nR) throw std::invalid_argument("ref_summarise_views: output size");
+    std::vector<const std::vector<double>*> cols = {&r.valueChangeQuantile, &r.conditionalImDiscounted, &r.conditionalImMean};
+    for (std::size_t b = 0; b < 3; ++b) cols.push_back(b < r.conditionalImBands.size() ? &r.conditionalImBands[b] : nullptr);
+    cols.push_back(&r.conditionalDiscountedEe);
+    cols.push_back(&r.conditionalImAuditRatio);
+    cols.push_back(&r.conditionalImDiscountedUncorrected);
+    for (const auto& t : r.trades)
+      for (const auto* c : {&t.marginalDiscounted, &t.marginal, &t.incrementalDiscounted, &t.standaloneDiscounted, &t.standalone})
+        cols.push_back(c);
+    for (std::size_t c = 0; c < cols.size(); ++c)
+      for (std::size_t k = 0; k < nR; ++k)
+        out[c * nR + k] = cols[c] && cols[c]->size() == nR ? (*cols[c])[k] : std::numeric_limits<double>::quiet_NaN();
     return 0;
   } catch (const std::exception& e) {
     setError(err, errlen, e);

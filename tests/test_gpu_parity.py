@@ -199,6 +199,23 @@ def test_nested_initial_margin_with_bermudans_and_1024_inner_paths(ctx):
     check_im_rows(p, rg, rr, 1e-3)
 
 
+def test_nested_initial_margin_audit_on_the_gpu(ctx):
+    """gpu::summarise's audit of the margin (two more runs on the first paths, with the kernel's and with more
+    inner paths) with the GPU as its backend, against the same audit on the oracle."""
+    m, ns = gpu_setup(1200, True)
+    p = gpu.compile(m, ns, S.Options(per_trade=True, im_quantile=0.99, im_inner_paths=64, im_audit_paths=256,
+                                     im_audit_inner_paths=512))
+    sg, vg = ctx.run(p)
+    sr, vr = restated.run_plan(p)
+    from zlatko_b200.summary import summarise
+
+    a, b = ctx.summarise(p, sg, vg), summarise(p, sr, vr, run=restated.run_plan)
+    assert np.any(b["conditional_im_audit_ratio"] != 1.0)
+    assert np.abs(a["conditional_im_audit_ratio"] - b["conditional_im_audit_ratio"]).max() <= 1e-3
+    for k in ("conditional_im_discounted", "conditional_im_mean", "conditional_im_discounted_uncorrected"):
+        assert np.abs(a[k] - b[k]).max() <= 1e-3 * np.abs(b[k]).max(), k
+
+
 def test_nested_initial_margin_in_a_batch_and_a_graph(ctx):
     """Batched with plans without the margin (one shared scenario), replayed from the captured graph: the same
     bits as the single run."""

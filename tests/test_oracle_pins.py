@@ -210,6 +210,48 @@ def test_restatement_is_bitwise_the_reference(csa, oi):
             assert np.array_equal(_bits(v1[out:out + width]), _bits(v2[out:out + width]))
 
 
+SUMMARY_OPTIONS = [S.Options(), S.Options(per_trade=True, im_quantile=0.99),
+                   S.Options(per_trade=True, im_quantile=0.99, im_inner_paths=64, im_audit_paths=64, im_audit_inner_paths=256),
+                   S.Options(im_quantile=0.975, im_inner_paths=128, samples=2)]
+
+
+@needs_ref
+@pytest.mark.parametrize("csa", [False, True])
+@pytest.mark.parametrize("oi", range(len(SUMMARY_OPTIONS)))
+def test_summarise_is_the_reference_summarise(csa, oi):
+    """summary.summarise on the reference's own read-back gives gpu::summarise's FusedResult bit for bit: the
+    profile, the CVA inputs, the per-trade statistics, the margin proxy, the nested margin's views and its
+    audit (run on the restated kernels, which are the reference's bits)."""
+    from zlatko_b200.summary import summarise
+
+    m, ns = gpu_setup(300, csa)
+    o = SUMMARY_OPTIONS[oi]
+    r = ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o))
+    p = gpu.compile(m, ns, o)
+    sums, values = ref.run_fused(r)
+    want, views = ref.summarise(r, sums, values), ref.summarise_views(r, sums, values)
+    got = summarise(p, sums, values, run=restated.run_plan)
+    same = lambda a, b: np.array_equal(np.asarray(a, np.float64), np.asarray(b, np.float64), equal_nan=True)  # noqa: E731
+    for k in ("ev", "ee", "ene", "pfe", "dee", "dene", "cva_inc", "mean_survival", "mean_deflator"):
+        assert same(got[k], want[k]), k
+    assert same(got["conditional_discounted_ee"], views["conditional_discounted_ee"])
+    nR = len(p.reporting)
+    absent = np.full(nR, np.nan)
+    assert same(got.get("value_change_quantile", absent), views["value_change_quantile"])
+    assert same(got.get("conditional_im_discounted", absent), views["conditional_im_discounted"])
+    assert same(got.get("conditional_im_mean", absent), views["conditional_im_mean"])
+    for b, name in enumerate(("conditional_im_band_05", "conditional_im_band_50", "conditional_im_band_95")):
+        assert same(got["conditional_im_bands"][b] if "conditional_im_bands" in got else absent, views[name]), name
+    for k in ("conditional_im_audit_ratio", "conditional_im_discounted_uncorrected"):
+        assert same(got.get(k, absent), views[k]), k
+    if o.im_audit_paths:
+        assert np.any(got["conditional_im_audit_ratio"] != 1.0)
+    assert len(got["trades"]) == len(views["trades"])
+    for a, b in zip(got["trades"], views["trades"]):
+        for k in b:
+            assert same(a[k], b[k]), k
+
+
 @needs_ref
 def test_amc_states_are_bitwise_the_reference():
     m, ns = gpu_setup(900, False)

@@ -50,6 +50,8 @@ class Plan:
     tables64: Optional[Dict[str, np.ndarray]] = None  # double-precision params/steps/terms/requests (zk_compile)
     exercise_rows: int = 0
     amc_degrees: List[int] = field(default_factory=list)  # regression degree of each Bermudan (zk_fit_amc)
+    im_audit_paths: int = 0          # the nested-IM audit (FusedPlan::imAuditPaths, imAuditInnerPaths); 0: off
+    im_audit_inner_paths: int = 0
 
     def __post_init__(self):
         self.header = np.ascontiguousarray(self.header, np.uint32)
@@ -170,6 +172,8 @@ def compile_arrays(m: np.ndarray, n: np.ndarray, o: np.ndarray) -> Plan:
         plan.exercise_rows = int(sizes[5])
         plan.market_survival = np.ones(nT)
         plan.amc_degrees = S.bermudan_degrees(n)
+        if o[5] > 0 and o[7] > 0:  # options: im_inner_paths, im_audit_paths, im_audit_inner_paths (spec.encode_options)
+            plan.im_audit_paths, plan.im_audit_inner_paths = int(o[7]), int(o[8])
         return plan
     finally:
         L.zk_plan_destroy(h)
@@ -261,6 +265,12 @@ class Context:
         check(lib().zk_run_plan_rows(self.handle, C.byref(v), outs, r.ctypes.data), self.handle)
         sums, values = bufs[0]
         return sums, values, r[: plan.rows_total * plan.num_paths].reshape(plan.rows_total, plan.num_paths)
+
+    def summarise(self, plan: Plan, sums: np.ndarray, values: np.ndarray):
+        """summary.summarise with this context as the backend of the nested-IM audit (gpu::summarise runs the
+        audit on the reference's CPU kernels; here it runs on the GPU)."""
+        from .summary import summarise
+        return summarise(plan, sums, values, run=self.run)
 
     def run_many(self, plans: Sequence[Plan]):
         views = (PlanView * len(plans))(*[p.view() for p in plans])

@@ -7,6 +7,7 @@ src/exposure/exposure_profile.cpp:51-60.  The integrals are summed with Kahan co
 from __future__ import annotations
 
 import math
+from dataclasses import replace
 from typing import Dict, Sequence
 
 import numpy as np
@@ -36,22 +37,99 @@ def _kahan(values) -> float:
     return s
 
 
-def summarise(plan, sums: np.ndarray, values: np.ndarray) -> Dict[str, np.ndarray]:
-    """Per reporting date: EV, EE, ENE, PFE, EE*, ENE*, pathwise-CVA increments, E[Q], E[D]."""
+NO_ROW = 0xFFFFFFFF
+ROW_QUANTILE, ROW_MEAN, ROW_MEAN_PRODUCT = 0, 1, 6  # row-statistics operations (fused_exposure.hpp:64-75)
+TRADE_FIELDS = ("marginal_discounted", "marginal", "incremental_discounted", "standalone_discounted", "standalone")
+IM_BAND_LEVELS = (0.05, 0.5, 0.95)
+
+
+def _outputs(plan):
+    """(op, row, level) -> output offset of every row-statistics request of the plan."""
+    out = {}
+    for q in np.asarray(plan.requests, np.float32).reshape(-1, 8):
+        out.setdefault((int(q[0]), int(q[1]), float(q[4])), int(q[7]))
+    return out
+
+
+def _per_date(plan, values, index, op, base, level=0.0):
+    """The outputs of one view: request (op, base + r, level) for every reporting date r."""
+    nR = len(plan.reporting)
+    lv = float(np.float32(level))
+    return np.array([float(values[index[(op, base + r, lv)]]) for r in range(nR)], np.float64)
+
+
+def summarise(plan, sums: np.ndarray, values: np.ndarray, run=None) -> Dict[str, np.ndarray]:
+    """gpu::summarise (src/gpu/fused_exposure.cpp:816-867) on a read-back, per reporting date: EV, EE, ENE, PFE,
+    EE*, ENE*, the pathwise-CVA increments, E[Q], E[D], the conditional EE* per default period, and where the
+    plan has them: the per-trade statistics ("trades", one dict per trade group), the initial-margin proxy
+    (the value-change quantile, 0 on the first date) and the nested conditional initial margin (E[D IM],
+    E[IM], its 5 / 50 / 95% bands).  With the plan's IM audit (im_audit_paths > 0) and a backend `run`
+    (plan -> (sums, values)), the margin series are scaled by the audit ratio (audit_conditional_im)."""
     nS = plan.stats_per_date
     if sums.size != plan.num_dates * nS or values.size < plan.num_outputs:
         raise ValueError("summarise: read-back does not match the plan")
     st = np.asarray(sums, np.float64).reshape(plan.num_dates, nS)
     rep = np.asarray(plan.reporting, np.int64)
+    nR = len(rep)
+    H = plan.header
     r = {"times": np.asarray(plan.times)[rep]}
     for k, name in enumerate(("ev", "ee", "ene", "dee", "dene", "cva_inc", "mean_survival", "mean_deflator")):
         r[name] = st[rep, k].copy()
-    r["pfe"] = np.asarray(values[: len(rep)], np.float64).copy()  # the PFE requests come first
+    r["pfe"] = np.asarray(values[:nR], np.float64).copy()  # the PFE requests come first
     if plan.market_survival is not None:
         r["market_survival"] = np.asarray(plan.market_survival)[rep]
-    if int(plan.header[3]) == 0:
+    index = _outputs(plan)
+    if int(H[19]) != NO_ROW:  # the value-change rows of the initial-margin proxy, at the margin's quantile level
+        lv = next(l for (op, row, l) in index if op == ROW_QUANTILE and row == int(H[19]))
+        v = _per_date(plan, values, index, ROW_QUANTILE, int(H[19]), lv)
+        v[0] = 0.0
+        r["value_change_quantile"] = v
+    r["trades"] = [{f: st[rep, 8 + 5 * i + k].copy() for k, f in enumerate(TRADE_FIELDS)} for i in range(int(H[18]))]
+    im = int(H[29])
+    if im != NO_ROW:
+        r["conditional_im_discounted"] = _per_date(plan, values, index, ROW_MEAN_PRODUCT, im)
+        r["conditional_im_mean"] = _per_date(plan, values, index, ROW_MEAN, im)
+        r["conditional_im_bands"] = [_per_date(plan, values, index, ROW_QUANTILE, im, q) for q in IM_BAND_LEVELS]
+    cdee = np.full(nR, np.nan)
+    for k in range(1, nR):
+        pd = r["mean_survival"][k - 1] - r["mean_survival"][k]
+        if pd > 0:
+            cdee[k] = r["cva_inc"][k] / pd
+    r["conditional_discounted_ee"] = cdee
+    if int(H[3]) == 0:
         r["cva_inc"][:] = np.nan
+    if getattr(plan, "im_audit_paths", 0) > 0 and "conditional_im_discounted" in r and run is not None:
+        ratio = audit_conditional_im(plan, run)
+        r["conditional_im_audit_ratio"] = ratio
+        r["conditional_im_discounted_uncorrected"] = r["conditional_im_discounted"].copy()
+        r["conditional_im_discounted"] = r["conditional_im_discounted"] * ratio
+        r["conditional_im_mean"] = r["conditional_im_mean"] * ratio
+        r["conditional_im_bands"] = [b * ratio for b in r["conditional_im_bands"]]
     return r
+
+
+def audit_conditional_im(plan, run) -> np.ndarray:
+    """auditConditionalIm (src/gpu/fused_exposure.cpp:869-886): per reporting date, E[D IM] with the plan's
+    im_audit_inner_paths inner paths over E[D IM] with its own inner paths, both on the plan's first
+    im_audit_paths paths (the normals are keyed by path, date and inner index, so these are the same outer
+    paths, and the first inner samples are the kernel's own); 1 where either is 0.  `run` is the backend."""
+    if getattr(plan, "im_audit_paths", 0) == 0 or int(plan.header[30]) == 0 or int(plan.header[29]) == NO_ROW:
+        return np.zeros(0)
+    n = min(plan.num_paths, int(plan.im_audit_paths))
+    h = plan.header.copy()
+    h[0], h[15] = n, (n + 63) // 64
+
+    def sub(header):
+        p = replace(plan, header=header.copy(), im_audit_paths=0)
+        return summarise(p, *run(p))["conditional_im_discounted"]
+
+    base = sub(h)
+    h[30] = int(plan.im_audit_inner_paths)
+    audited = sub(h)
+    ratio = np.ones(len(base))
+    ok = (base > 0.0) & (audited > 0.0)
+    ratio[ok] = audited[ok] / base[ok]
+    return ratio
 
 
 def pathwise_cva(result: Dict[str, np.ndarray], recovery: float) -> float:
