@@ -284,7 +284,7 @@ def im_leg(ctx, a):
         b = ctx.batch([p])
         try:
             for _ in range(3):
-                b.execute()
+                b.execute()  # the first execute autotunes the tile shape
             t = []
             for _ in range(5):
                 b.execute()
