@@ -56,6 +56,8 @@ def lib() -> C.CDLL:
         L.ref_summarise.argtypes = [C.c_void_p, _fp, _fp, _dp, C.c_char_p, sz]
         L.ref_summarise_views.restype = C.c_int
         L.ref_summarise_views.argtypes = [C.c_void_p, _fp, _fp, _dp, sz, C.c_char_p, sz]
+        L.ref_summarise_full.restype = C.c_int64
+        L.ref_summarise_full.argtypes = [C.c_void_p, _fp, _fp, C.c_void_p, sz, C.c_char_p, sz]
         L.ref_engine_run.restype = C.c_void_p
         L.ref_engine_run.argtypes = [_dp, sz, _dp, sz, C.c_double, C.c_void_p, sz, C.c_char_p, sz]
         L.ref_engine_free.argtypes = [C.c_void_p]
@@ -238,6 +240,68 @@ def summarise_views(plan: RefPlan, sums: np.ndarray, values: np.ndarray) -> dict
         raise ValueError(e.value.decode())
     r = {k: out[i * nR:(i + 1) * nR] for i, k in enumerate(VIEW_FIELDS)}
     r["trades"] = [{k: out[(9 + 5 * t + i) * nR:(10 + 5 * t + i) * nR] for i, k in enumerate(TRADE_FIELDS)} for t in range(nTr)]
+    return r
+
+
+PROFILE_FIELDS = ("times", "ev", "ee", "ene", "pfe", "dee", "dene")
+
+
+def summarise_full(plan: RefPlan, sums: np.ndarray, values: np.ndarray) -> dict:
+    """The whole FusedResult of gpu::summarise (with the reference's own nested-margin audit) as nested dicts
+    and arrays, under the key names of zlatko_b200.summary.summarise."""
+    s, v = np.ascontiguousarray(sums, np.float32), np.ascontiguousarray(values, np.float32)
+    e = _err()
+    n = lib().ref_summarise_full(plan.handle, s, v, None, 0, e, 512)
+    if n < 0:
+        raise ValueError(e.value.decode())
+    flat = np.zeros(n)
+    lib().ref_summarise_full(plan.handle, s, v, flat.ctypes.data, n, e, 512)
+    pos = 0
+
+    def scalar():
+        nonlocal pos
+        pos += 1
+        return float(flat[pos - 1])
+
+    def vec():
+        k = int(scalar())
+        nonlocal pos
+        pos += k
+        return flat[pos - k:pos].copy()
+
+    def mat():
+        return [vec() for _ in range(int(scalar()))]
+
+    def profile():
+        return {k: vec() for k in PROFILE_FIELDS}
+
+    r = profile()
+    for k in ("mean_survival", "market_survival", "cva_inc", "conditional_discounted_ee", "mean_deflator",
+              "value_change_quantile", "conditional_im_discounted", "conditional_im_mean"):
+        r[k] = vec()
+    r["conditional_im_bands"] = mat()
+    r["conditional_im_audit_ratio"] = vec()
+    r["conditional_im_discounted_uncorrected"] = vec()
+    r["trades"] = [{k: vec() for k in TRADE_FIELDS} for _ in range(int(scalar()))]
+    for k in ("exposure_samples", "netted_samples", "collateral_samples", "collateral_bands"):
+        r[k] = mat()
+    r["gross_profile"] = profile() if scalar() else None
+    r["histogram_time"] = scalar()
+    r["histogram_edges"], r["histogram_counts"] = vec(), vec()
+    r["trade_views"] = [{"profile": profile(), "samples": mat(), "bands": mat(), "mean_deflated": vec()}
+                        for _ in range(int(scalar()))]
+    r["exercise"] = [{"distribution": vec(), "sample_index": vec()} for _ in range(int(scalar()))]
+    r["factors"] = None
+    if scalar():
+        f = {"rate_samples": mat(), "rate_bands": mat(), "rate_mean": vec(), "deflator_mean": vec(), "bond_mean": vec()}
+        f["assets"] = [{"samples": mat(), "bands": mat(), "mean": vec(), "deflated_mean": vec()} for _ in range(int(scalar()))]
+        f["credits"] = [{"intensity_samples": mat(), "intensity_bands": mat(), "survival_samples": mat(), "survival_mean": vec()}
+                        for _ in range(int(scalar()))]
+        k = int(scalar())
+        f["increment_correlation"] = flat[pos:pos + k * k].reshape(k, k).copy()
+        pos += k * k
+        r["factors"] = f
+    assert pos == n
     return r
 
 

@@ -488,6 +488,104 @@ int ref_summarise_views(const void* h, const float* sums, const float* values, d
   }
 }
 
+namespace {
+// Flattens a FusedResult into length-prefixed arrays (oracle/ref.py: summarise_full reads them in this order).
+struct Flat {
+  std::vector<double> d;
+  void vec(const std::vector<double>& v) {
+    d.push_back(static_cast<double>(v.size()));
+    d.insert(d.end(), v.begin(), v.end());
+  }
+  void mat(const std::vector<std::vector<double>>& m) {
+    d.push_back(static_cast<double>(m.size()));
+    for (const auto& v : m) vec(v);
+  }
+  void profile(const ExposureProfile& p) {
+    for (const auto* v : {&p.times, &p.expectedValue, &p.expectedExposure, &p.expectedNegativeExposure,
+                          &p.potentialFutureExposure, &p.discountedExpectedExposure, &p.discountedExpectedNegativeExposure})
+      vec(*v);
+  }
+};
+}  // namespace
+
+// The whole gpu::summarise result (audit included), flattened; returns the number of doubles, writing at most
+// cap of them into out (a first call with cap 0 sizes the buffer).
+std::int64_t ref_summarise_full(const void* h, const float* sums, const float* values, double* out, std::size_t cap, char* err,
+                                std::size_t errlen) {
+  try {
+    const auto& p = *static_cast<const gpu::FusedPlan*>(h);
+    gpu::FusedOutput o;
+    o.sums.assign(sums, sums + p.numDates() * p.statsPerDate);
+    o.values.assign(values, values + std::max<std::size_t>(1, p.numOutputs));
+    const auto r = gpu::summarise(p, o);
+    Flat f;
+    f.profile(r.profile);
+    for (const auto* v : {&r.meanSurvival, &r.marketSurvival, &r.cvaIncrements, &r.conditionalDiscountedEe, &r.meanDeflator,
+                          &r.valueChangeQuantile, &r.conditionalImDiscounted, &r.conditionalImMean})
+      f.vec(*v);
+    f.mat(r.conditionalImBands);
+    f.vec(r.conditionalImAuditRatio);
+    f.vec(r.conditionalImDiscountedUncorrected);
+    f.d.push_back(static_cast<double>(r.trades.size()));
+    for (const auto& t : r.trades)
+      for (const auto* v : {&t.marginalDiscounted, &t.marginal, &t.incrementalDiscounted, &t.standaloneDiscounted, &t.standalone})
+        f.vec(*v);
+    f.mat(r.exposureSamples);
+    f.mat(r.nettedSamples);
+    f.mat(r.collateralSamples);
+    f.mat(r.collateralBands);
+    f.d.push_back(r.grossProfile ? 1.0 : 0.0);
+    if (r.grossProfile) f.profile(*r.grossProfile);
+    f.d.push_back(r.histogramTime);
+    f.vec(r.histogramEdges);
+    f.vec(r.histogramCounts);
+    f.d.push_back(static_cast<double>(r.tradeViews.size()));
+    for (const auto& t : r.tradeViews) {
+      f.profile(t.profile);
+      f.mat(t.samples);
+      f.mat(t.bands);
+      f.vec(t.meanDeflated);
+    }
+    f.d.push_back(static_cast<double>(r.exercise.size()));
+    for (const auto& e : r.exercise) {
+      f.vec(e.distribution);
+      f.vec(e.sampleIndex);
+    }
+    f.d.push_back(r.factors ? 1.0 : 0.0);
+    if (r.factors) {
+      const auto& F = *r.factors;
+      f.mat(F.rateSamples);
+      f.mat(F.rateBands);
+      f.vec(F.rateMean);
+      f.vec(F.deflatorMean);
+      f.vec(F.bondMean);
+      f.d.push_back(static_cast<double>(F.assets.size()));
+      for (const auto& a : F.assets) {
+        f.mat(a.samples);
+        f.mat(a.bands);
+        f.vec(a.mean);
+        f.vec(a.deflatedMean);
+      }
+      f.d.push_back(static_cast<double>(F.credits.size()));
+      for (const auto& c : F.credits) {
+        f.mat(c.intensitySamples);
+        f.mat(c.intensityBands);
+        f.mat(c.survivalSamples);
+        f.vec(c.survivalMean);
+      }
+      const std::size_t n = F.incrementCorrelation.rows();
+      f.d.push_back(static_cast<double>(n));
+      for (std::size_t i = 0; i < n; ++i)
+        for (std::size_t k = 0; k < n; ++k) f.d.push_back(F.incrementCorrelation(i, k));
+    }
+    for (std::size_t k = 0; k < f.d.size() && k < cap; ++k) out[k] = f.d[k];
+    return static_cast<std::int64_t>(f.d.size());
+  } catch (const std::exception& e) {
+    setError(err, errlen, e);
+    return -1;
+  }
+}
+
 // ------------------------------------------------------------------ FP64 engine
 // ExposureEngine::run (exposure_engine.cpp:50-81) on the reference's own normals (normals == nullptr) or
 // on injected normals (see generateInjected).  Returns a handle; ref_engine_get copies its matrices.

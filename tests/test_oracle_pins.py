@@ -252,6 +252,60 @@ def test_summarise_is_the_reference_summarise(csa, oi):
             assert same(a[k], b[k]), k
 
 
+VIEW_OPTIONS = [S.Options(samples=12, histogram_time=2.0, gross=True, collateral_bands=True, trade_views=True,
+                          pfe_quantile=0.975, per_trade=True, im_quantile=0.99),
+                S.Options(factor_views=True, samples=5, bond_maturity=8.0, histogram_time=0.0, histogram_bins=7),
+                S.Options(factor_views=True, band_levels=(0.1, 0.9), factor_band_levels=(0.5,), gross=True, histogram_time=30.0),
+                S.Options(exercise_views=True, samples=4, trade_views=True, im_quantile=0.99, im_inner_paths=64)]
+
+
+def _same_tree(got, want, path="result"):
+    """Every array of the reference's FusedResult bit for bit (NaN included); an absent key stands for the
+    reference's empty series."""
+    if isinstance(want, dict):
+        for k, w in want.items():
+            _same_tree(got.get(k) if got is not None else None, w, f"{path}.{k}")
+    elif isinstance(want, list):
+        got = [] if got is None else got
+        assert len(got) == len(want), (path, len(got), len(want))
+        for i, (a, b) in enumerate(zip(got, want)):
+            _same_tree(a, b, f"{path}[{i}]")
+    elif want is None:
+        assert got is None, path
+    else:
+        w = np.asarray(want, np.float64)
+        g = np.zeros(0) if got is None else np.asarray(got, np.float64)
+        if w.size == 0 and g.size == 0:
+            return
+        assert g.shape == w.shape, (path, g.shape, w.shape)
+        assert np.array_equal(g, w, equal_nan=True), (path, np.abs(g - w).max())
+
+
+@needs_ref
+@pytest.mark.parametrize("oi", range(len(VIEW_OPTIONS)))
+def test_summarise_views_are_the_reference_views(oi):
+    """Every view of gpu::summarise's FusedResult (samples, bands, gross profile, histogram, per-trade views,
+    exercise distributions, factor views, the margin series) from summary.summarise on the reference's
+    read-back, bit for bit."""
+    from zlatko_b200.summary import summarise
+
+    m, ns = gpu_setup(320, oi != 1)
+    if oi == 3:
+        ns.trades.append(bermudan(exercise=(1.0, 2.0, 3.0, 4.0), physical=True, degree=2))
+        ns.trades.append(bermudan(exercise=(2.0, 3.0), physical=False, position=-0.5, degree=3))
+    o = VIEW_OPTIONS[oi]
+    r = ref.compile_plan(S.encode_model(m), S.encode_netting_set(ns), S.encode_options(o))
+    p = gpu.compile(m, ns, o)
+    sums, values = ref.run_fused(r)
+    want = ref.summarise_full(r, sums, values)
+    got = summarise(p, sums, values, run=restated.run_plan)
+    ms = want.pop("market_survival")  # the plan's curve: the reference's compile against this package's
+    assert np.abs(got.pop("market_survival") - ms).max() <= 1e-15
+    if o.trade_views or o.exercise_views or o.factor_views or o.gross or o.samples:
+        assert any(want.get(k) for k in ("trade_views", "exercise", "exposure_samples")) or want["factors"] or want["gross_profile"]
+    _same_tree(got, want)
+
+
 @needs_ref
 def test_amc_states_are_bitwise_the_reference():
     m, ns = gpu_setup(900, False)

@@ -52,6 +52,7 @@ class Plan:
     amc_degrees: List[int] = field(default_factory=list)  # regression degree of each Bermudan (zk_fit_amc)
     im_audit_paths: int = 0          # the nested-IM audit (FusedPlan::imAuditPaths, imAuditInnerPaths); 0: off
     im_audit_inner_paths: int = 0
+    options: Optional[S.Options] = None  # the options compiled (summarise decodes the views with them)
 
     def __post_init__(self):
         self.header = np.ascontiguousarray(self.header, np.uint32)
@@ -172,8 +173,9 @@ def compile_arrays(m: np.ndarray, n: np.ndarray, o: np.ndarray) -> Plan:
         plan.exercise_rows = int(sizes[5])
         plan.market_survival = np.ones(nT)
         plan.amc_degrees = S.bermudan_degrees(n)
-        if o[5] > 0 and o[7] > 0:  # options: im_inner_paths, im_audit_paths, im_audit_inner_paths (spec.encode_options)
-            plan.im_audit_paths, plan.im_audit_inner_paths = int(o[7]), int(o[8])
+        plan.options = S.decode_options(o)
+        if plan.options.im_inner_paths > 0 and plan.options.im_audit_paths > 0:
+            plan.im_audit_paths, plan.im_audit_inner_paths = plan.options.im_audit_paths, plan.options.im_audit_inner_paths
         return plan
     finally:
         L.zk_plan_destroy(h)

@@ -307,6 +307,25 @@ def encode_options(o: Options) -> np.ndarray:
     return np.asarray(out, dtype=np.float64)
 
 
+def decode_options(a) -> Options:
+    """The inverse of encode_options."""
+    a = [float(v) for v in a]
+    if not a or a[0] != OPTIONS_MAGIC:
+        raise ValueError("options: bad magic")
+    o = Options(pfe_quantile=a[1], counterparty=int(a[2]), per_trade=bool(a[3]), im_quantile=a[4], im_inner_paths=int(a[5]),
+                im_margin_period=a[6], im_audit_paths=int(a[7]), im_audit_inner_paths=int(a[8]), samples=int(a[9]),
+                histogram_time=a[10], histogram_bins=int(a[11]), gross=bool(a[12]), collateral_bands=bool(a[13]),
+                trade_views=bool(a[14]), exercise_views=bool(a[15]), factor_views=bool(a[16]), bond_maturity=a[17])
+    i = 18
+    seqs = []
+    for _ in range(3):
+        n = int(a[i])
+        seqs.append(tuple(a[i + 1:i + 1 + n]))
+        i += 1 + n
+    o.extra_dates, o.band_levels, o.factor_band_levels = seqs
+    return o
+
+
 def expand_swap2(t: Swap2) -> List[Swap]:
     """The three one-schedule swaps whose sum is a two-schedule swap (linear in the legs)."""
     return [Swap(t.notional, 0.0, t.pay_fixed, t.float_schedule),

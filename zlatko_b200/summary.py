@@ -58,13 +58,139 @@ def _per_date(plan, values, index, op, base, level=0.0):
     return np.array([float(values[index[(op, base + r, lv)]]) for r in range(nR)], np.float64)
 
 
-def summarise(plan, sums: np.ndarray, values: np.ndarray, run=None) -> Dict[str, np.ndarray]:
+PROFILE_FIELDS = ("times", "ev", "ee", "ene", "pfe", "dee", "dene")
+
+
+class _Requests:
+    """The plan's row-statistics requests in the order gpu::compile emits them (fused_exposure.cpp:505-609):
+    each view takes the next requests and reads its outputs at their offsets."""
+
+    def __init__(self, plan, values):
+        self.q = np.asarray(plan.requests, np.float32).reshape(-1, 8)
+        self.i = 0
+        self.v = np.asarray(values, np.float64)
+        self.nR = len(plan.reporting)
+
+    def take(self, n: int = 1) -> np.ndarray:
+        if self.i + n > len(self.q):
+            raise ValueError("summarise: the plan's requests do not match its options")
+        self.i += n
+        return self.q[self.i - n:self.i]
+
+    def per_date(self) -> int:
+        return int(self.take(self.nR)[0, 7])
+
+    def series(self, o: int) -> np.ndarray:
+        return self.v[o:o + self.nR].copy()
+
+    def samples(self, o: int, S: int) -> list:
+        """Outputs [date][path] to [path][date]."""
+        return list(self.v[o:o + self.nR * S].reshape(self.nR, S).T.copy())
+
+    def profile(self, times) -> dict:
+        o = [self.per_date() for _ in range(6)]  # mean, positive, negative, PFE, positive / negative deflated
+        return {"times": np.asarray(times, np.float64), "ev": self.series(o[0]), "ee": self.series(o[1]),
+                "ene": self.series(o[2]), "pfe": self.series(o[3]), "dee": self.series(o[4]), "dene": self.series(o[5])}
+
+
+def _views(plan, values, o, times) -> dict:
+    """addViews (src/gpu/fused_exposure.cpp:715-812): every view the options asked for, from the plan's
+    requests in emission order."""
+    H = plan.header
+    Q = _Requests(plan, values)
+    S, nR, nP = int(o.samples), len(times), plan.num_paths
+    r: Dict = {"histogram_time": 0.0}
+    Q.per_date()  # PFE (read by summarise directly)
+    if o.im_quantile > 0.0:
+        vc = Q.series(Q.per_date())
+        vc[0] = 0.0
+        r["value_change_quantile"] = vc
+    collateral = int(H[22]) != NO_ROW
+    if S > 0:
+        r["exposure_samples"] = Q.samples(Q.per_date(), S)
+        r["netted_samples"] = Q.samples(Q.per_date(), S)
+        if collateral:
+            r["collateral_samples"] = Q.samples(Q.per_date(), S)
+    if int(H[29]) != NO_ROW:
+        r["conditional_im_discounted"] = Q.series(Q.per_date())
+        r["conditional_im_mean"] = Q.series(Q.per_date())
+        r["conditional_im_bands"] = [Q.series(Q.per_date()) for _ in IM_BAND_LEVELS]
+    if o.collateral_bands and collateral:
+        r["collateral_bands"] = [Q.series(Q.per_date()) for _ in o.band_levels]
+    if o.gross:
+        r["gross_profile"] = Q.profile(times)
+    if o.histogram_time >= 0.0:
+        rank = 0
+        for k in range(nR):
+            if times[k] <= o.histogram_time + 1e-10:
+                rank = k
+        q = Q.take(1)[0]
+        h, nB = int(q[7]), int(q[3])
+        lo, hi = Q.v[h + nB], Q.v[h + nB + 1]
+        r["histogram_time"] = float(times[rank])
+        r["histogram_edges"] = np.array([lo + (hi - lo) * b / nB for b in range(nB + 1)])
+        r["histogram_counts"] = Q.v[h:h + nB] / nP
+    if o.trade_views:
+        r["trade_views"] = []
+        for _ in range(int(H[18])):
+            t = {"profile": Q.profile(times)}
+            t["samples"] = Q.samples(Q.per_date(), S) if S > 0 else []
+            t["bands"] = [Q.series(Q.per_date()) for _ in o.band_levels]
+            t["mean_deflated"] = Q.series(Q.per_date())
+            r["trade_views"].append(t)
+    if int(H[25]) != NO_ROW:
+        r["exercise"] = []
+        for _ in range(int(H[27])):
+            q = Q.take(1)[0]
+            h, nE = int(q[7]), int(q[3]) - 1
+            e = {"distribution": np.append(Q.v[h + 1:h + 1 + nE], Q.v[h]) / nP}
+            e["sample_index"] = Q.v[int(Q.take(1)[0, 7]):][:S].copy() if S > 0 else np.zeros(0)
+            r["exercise"].append(e)
+    if o.factor_views:
+        nA, nC = int(H[2]), int(H[3])
+        f = {"rate_samples": Q.samples(Q.per_date(), S) if S > 0 else []}
+        f["rate_bands"] = [Q.series(Q.per_date()) for _ in o.factor_band_levels]
+        f["rate_mean"], f["deflator_mean"], f["bond_mean"] = (Q.series(Q.per_date()) for _ in range(3))
+        f["assets"] = []
+        for _ in range(nA):
+            a = {"samples": Q.samples(Q.per_date(), S) if S > 0 else []}
+            a["bands"] = [Q.series(Q.per_date()) for _ in o.factor_band_levels]
+            a["mean"], a["deflated_mean"] = Q.series(Q.per_date()), Q.series(Q.per_date())
+            f["assets"].append(a)
+        f["credits"] = []
+        for _ in range(nC):
+            c = {"intensity_samples": [], "survival_samples": []}
+            if S > 0:
+                c["intensity_samples"] = Q.samples(Q.per_date(), S)
+                c["survival_samples"] = Q.samples(Q.per_date(), S)
+            c["intensity_bands"] = [Q.series(Q.per_date()) for _ in o.factor_band_levels]
+            c["survival_mean"] = Q.series(Q.per_date())
+            f["credits"].append(c)
+        n = 1 + nA + nC if plan.num_dates > 1 else 0  # first-step increments of x, ln S and y
+        means = [float(np.float32(Q.v[int(q[7])])) for q in Q.take(n)]
+        prods = np.array([Q.v[int(q[7])] for q in Q.take(n * n)]).reshape(n, n)
+        corr = np.zeros((n, n))
+        for i in range(n):
+            for k in range(n):
+                cov = prods[i, k] - means[i] * means[k]
+                vi, vk = prods[i, i] - means[i] * means[i], prods[k, k] - means[k] * means[k]
+                corr[i, k] = cov / np.sqrt(vi * vk) if vi > 0 and vk > 0 else (1.0 if i == k else 0.0)
+        f["increment_correlation"] = corr
+        r["factors"] = f
+    if Q.i != len(Q.q):
+        raise ValueError("summarise: the plan's requests do not match its options")
+    return r
+
+
+def summarise(plan, sums: np.ndarray, values: np.ndarray, run=None) -> Dict:
     """gpu::summarise (src/gpu/fused_exposure.cpp:816-867) on a read-back, per reporting date: EV, EE, ENE, PFE,
-    EE*, ENE*, the pathwise-CVA increments, E[Q], E[D], the conditional EE* per default period, and where the
-    plan has them: the per-trade statistics ("trades", one dict per trade group), the initial-margin proxy
-    (the value-change quantile, 0 on the first date) and the nested conditional initial margin (E[D IM],
-    E[IM], its 5 / 50 / 95% bands).  With the plan's IM audit (im_audit_paths > 0) and a backend `run`
-    (plan -> (sums, values)), the margin series are scaled by the audit ratio (audit_conditional_im)."""
+    EE*, ENE*, the pathwise-CVA increments, E[Q], E[D], the conditional EE* per default period and the
+    per-trade statistics ("trades", one dict per trade group).  For a plan compiled here (plan.options) also
+    every view its options asked for (addViews: path samples [path][date], bands, the gross profile, the
+    histogram, per-trade views, Bermudan exercise distributions, factor views), under the names of
+    FusedResult in snake case; for other plans the margin views the header locates.  The nested conditional
+    initial margin: E[D IM], E[IM] and its 5 / 50 / 95% bands; with the plan's audit (im_audit_paths > 0) and a
+    backend `run` (plan -> (sums, values)), scaled by the audit ratio (audit_conditional_im)."""
     nS = plan.stats_per_date
     if sums.size != plan.num_dates * nS or values.size < plan.num_outputs:
         raise ValueError("summarise: read-back does not match the plan")
@@ -78,18 +204,21 @@ def summarise(plan, sums: np.ndarray, values: np.ndarray, run=None) -> Dict[str,
     r["pfe"] = np.asarray(values[:nR], np.float64).copy()  # the PFE requests come first
     if plan.market_survival is not None:
         r["market_survival"] = np.asarray(plan.market_survival)[rep]
-    index = _outputs(plan)
-    if int(H[19]) != NO_ROW:  # the value-change rows of the initial-margin proxy, at the margin's quantile level
-        lv = next(l for (op, row, l) in index if op == ROW_QUANTILE and row == int(H[19]))
-        v = _per_date(plan, values, index, ROW_QUANTILE, int(H[19]), lv)
-        v[0] = 0.0
-        r["value_change_quantile"] = v
     r["trades"] = [{f: st[rep, 8 + 5 * i + k].copy() for k, f in enumerate(TRADE_FIELDS)} for i in range(int(H[18]))]
-    im = int(H[29])
-    if im != NO_ROW:
-        r["conditional_im_discounted"] = _per_date(plan, values, index, ROW_MEAN_PRODUCT, im)
-        r["conditional_im_mean"] = _per_date(plan, values, index, ROW_MEAN, im)
-        r["conditional_im_bands"] = [_per_date(plan, values, index, ROW_QUANTILE, im, q) for q in IM_BAND_LEVELS]
+    if getattr(plan, "options", None) is not None:
+        r.update(_views(plan, values, plan.options, r["times"]))
+    else:
+        index = _outputs(plan)
+        if int(H[19]) != NO_ROW:  # the value-change rows of the initial-margin proxy, at the margin's quantile level
+            lv = next(l for (op, row, l) in index if op == ROW_QUANTILE and row == int(H[19]))
+            v = _per_date(plan, values, index, ROW_QUANTILE, int(H[19]), lv)
+            v[0] = 0.0
+            r["value_change_quantile"] = v
+        im = int(H[29])
+        if im != NO_ROW:
+            r["conditional_im_discounted"] = _per_date(plan, values, index, ROW_MEAN_PRODUCT, im)
+            r["conditional_im_mean"] = _per_date(plan, values, index, ROW_MEAN, im)
+            r["conditional_im_bands"] = [_per_date(plan, values, index, ROW_QUANTILE, im, q) for q in IM_BAND_LEVELS]
     cdee = np.full(nR, np.nan)
     for k in range(1, nR):
         pd = r["mean_survival"][k - 1] - r["mean_survival"][k]
