@@ -22,10 +22,10 @@ namespace zk {
 
 namespace {
 
-constexpr int kRowThreads = 512;
+constexpr int kRowThreads = 256;
 constexpr int kRowWarps = kRowThreads / 32;
 constexpr int kBins = 4096;
-constexpr int kCap = 8192;
+constexpr int kCap = 4096;
 constexpr int kMaxRounds = 16;
 constexpr int kHistBins = 3072;  // the reference's histogram-request limit (kPfeBins)
 
@@ -82,6 +82,37 @@ __device__ __forceinline__ bool passes(const RowSmem<R>& s, int rounds, double v
   return true;
 }
 
+// Calls f(v, valid) for every value of the row, through max(x, 0) when pos, in warp-uniform steps (every lane
+// calls f the same number of times, so f may vote).  Rows that start on a 16-byte boundary with a length a
+// multiple of 16 bytes are read 16 bytes per load.
+template <typename R, typename F>
+__device__ __forceinline__ void forEachValue(const R* X, uint32_t nP, bool pos, F&& f) {
+  const uint32_t tid = threadIdx.x;
+  auto fix = [&](R x) { return pos ? fmax(x, R(0)) : x; };
+  constexpr uint32_t kVec = 16 / sizeof(R);
+  if ((nP % kVec) == 0 && (reinterpret_cast<uintptr_t>(X) & 15u) == 0) {
+    const uint32_t nv = nP / kVec;
+#pragma unroll 2
+    for (uint32_t base = 0; base < nv; base += kRowThreads) {
+      const uint32_t i = base + tid;
+      const bool ok = i < nv;
+      if constexpr (sizeof(R) == 4) {
+        const float4 q = ok ? __ldg(reinterpret_cast<const float4*>(X) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+        f(fix(q.x), ok), f(fix(q.y), ok), f(fix(q.z), ok), f(fix(q.w), ok);
+      } else {
+        const double2 q = ok ? __ldg(reinterpret_cast<const double2*>(X) + i) : make_double2(0.0, 0.0);
+        f(fix(q.x), ok), f(fix(q.y), ok);
+      }
+    }
+  } else {
+    for (uint32_t base = 0; base < nP; base += kRowThreads) {
+      const uint32_t i = base + tid;
+      const bool ok = i < nP;
+      f(fix(ok ? X[i] : R(0)), ok);
+    }
+  }
+}
+
 // Bitonic sort of n (<= kCap) values in shared memory, padded with +inf to a power of two.
 template <typename R>
 __device__ void bitonicSort(R* a, uint32_t n) {
@@ -104,7 +135,7 @@ __device__ void bitonicSort(R* a, uint32_t n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char raw[];
   RowSmem<R>& s = *reinterpret_cast<RowSmem<R>*>(raw);
   const RowJob<R> J = jobs[blockIdx.x];
@@ -123,18 +154,23 @@ __global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* _
   if (op != 0 && op != 5 && op != 7) {  // means, in double precision
     const R* Y = J.expo + static_cast<size_t>(row2) * nP;
     double acc = 0.0;
-    for (uint32_t i = tid; i < nP; i += kRowThreads) {
-      const R x = X[i];
-      R f = x;
-      switch (op) {
-        case 2: f = fmax(x, R(0)); break;
-        case 3: f = fmin(x, R(0)); break;
-        case 6: f = x * Y[i]; break;
-        case 8: f = fmax(x, R(0)) * Y[i]; break;
-        case 9: f = fmin(x, R(0)) * Y[i]; break;
-        default: break;
+    if (op == 1 || op == 2 || op == 3) {
+      forEachValue(X, nP, false, [&](R x, bool ok) {
+        const R f = op == 2 ? fmax(x, R(0)) : op == 3 ? fmin(x, R(0)) : x;
+        if (ok) acc += static_cast<double>(f);
+      });
+    } else {
+      for (uint32_t i = tid; i < nP; i += kRowThreads) {
+        const R x = X[i];
+        R f = x;
+        switch (op) {
+          case 6: f = x * Y[i]; break;
+          case 8: f = fmax(x, R(0)) * Y[i]; break;
+          case 9: f = fmin(x, R(0)) * Y[i]; break;
+          default: break;
+        }
+        acc += static_cast<double>(f);
       }
-      acc += static_cast<double>(f);
     }
     const double total = blockSum(acc, s.dsum);
     if (tid == 0) out[0] = static_cast<R>(total / static_cast<double>(nP));
@@ -142,12 +178,10 @@ __global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* _
   }
 
   const bool pos = op == 7;
-  auto val = [&](uint32_t i) -> R { const R x = X[i]; return pos ? fmax(x, R(0)) : x; };
   R lo = R(INFINITY), hi = R(-INFINITY);
-  for (uint32_t i = tid; i < nP; i += kRowThreads) {
-    const R v = val(i);
-    lo = fmin(lo, v), hi = fmax(hi, v);
-  }
+  forEachValue(X, nP, pos, [&](R v, bool ok) {
+    if (ok) lo = fmin(lo, v), hi = fmax(hi, v);
+  });
   blockMinMax(lo, hi, s.rmin, s.rmax);
 
   if (op == 5) {  // histogram of `count` bins on [lo, hi] (the request's range unless lo == hi there)
@@ -187,10 +221,9 @@ __global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* _
     // Range of the current candidates (round 0: the whole row, already known).
     if (rounds > 0) {
       lo = R(INFINITY), hi = R(-INFINITY);
-      for (uint32_t i = tid; i < nP; i += kRowThreads) {
-        const R v = val(i);
-        if (passes(s, rounds, static_cast<double>(v))) lo = fmin(lo, v), hi = fmax(hi, v);
-      }
+      forEachValue(X, nP, pos, [&](R v, bool ok) {
+        if (ok && passes(s, rounds, static_cast<double>(v))) lo = fmin(lo, v), hi = fmax(hi, v);
+      });
       blockMinMax(lo, hi, s.rmin, s.rmax);
       if (!(lo < hi)) {  // every candidate has the same value
         vk = lo, vk1 = lo;
@@ -200,10 +233,17 @@ __global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* _
     const double dlo = static_cast<double>(lo), invw = static_cast<double>(kBins) / (static_cast<double>(hi) - dlo);
     for (uint32_t b = tid; b < kBins; b += kRowThreads) s.hist[b] = 0;
     __syncthreads();
-    for (uint32_t i = tid; i < nP; i += kRowThreads) {
-      const double v = static_cast<double>(val(i));
-      if (passes(s, rounds, v)) atomicAdd(&s.hist[binOf(v, dlo, invw)], 1u);
-    }
+    // Bin 0 holds the row's minimum, the dominant duplicate of exposure rows (exact zeros): its lanes are
+    // counted with one vote per warp instead of contended shared-memory atomics.
+    uint32_t zeroBin = 0;
+    forEachValue(X, nP, pos, [&](R x, bool ok) {
+      const double v = static_cast<double>(x);
+      const bool in = ok && passes(s, rounds, v);
+      const uint32_t b = binOf(v, dlo, invw);
+      zeroBin += __popc(__ballot_sync(0xFFFFFFFFu, in && b == 0));
+      if (in && b != 0) atomicAdd(&s.hist[b], 1u);
+    });
+    if ((tid & 31u) == 0 && zeroBin) atomicAdd(&s.hist[0], zeroBin);
     __syncthreads();
     if (tid == 0) {
       uint32_t cum = below, b0 = kBins - 1, b1 = kBins - 1, below0 = below;
@@ -224,25 +264,23 @@ __global__ void __launch_bounds__(kRowThreads) rowStatsKernel(const RowJob<R>* _
     if (b0 != b1) {
       // k is the largest value of bin b0, k + 1 the smallest of bin b1.
       R mx = R(-INFINITY), mn = R(INFINITY);
-      for (uint32_t i = tid; i < nP; i += kRowThreads) {
-        const R v = val(i);
+      forEachValue(X, nP, pos, [&](R v, bool ok) {
         const double dv = static_cast<double>(v);
-        if (!passes(s, rounds, dv)) continue;
+        if (!ok || !passes(s, rounds, dv)) return;
         const uint32_t b = binOf(dv, dlo, invw);
         if (b == b0) mx = fmax(mx, v);
         if (b == b1) mn = fmin(mn, v);
-      }
+      });
       blockMinMax(mn, mx, s.rmin, s.rmax);  // block minimum of mn, block maximum of mx
       vk = mx, vk1 = mn;
       done = true;
     } else if (c0 <= static_cast<uint32_t>(kCap)) {
       if (tid == 0) s.candCount = 0;
       __syncthreads();
-      for (uint32_t i = tid; i < nP; i += kRowThreads) {
-        const R v = val(i);
+      forEachValue(X, nP, pos, [&](R v, bool ok) {
         const double dv = static_cast<double>(v);
-        if (passes(s, rounds, dv) && binOf(dv, dlo, invw) == b0) s.cand[atomicAdd(&s.candCount, 1u)] = v;
-      }
+        if (ok && passes(s, rounds, dv) && binOf(dv, dlo, invw) == b0) s.cand[atomicAdd(&s.candCount, 1u)] = v;
+      });
       __syncthreads();
       const uint32_t n = s.candCount;
       bitonicSort(s.cand, n);
