@@ -334,10 +334,9 @@ def test_pfe_is_the_exact_interpolated_quantile(ctx):
 
 
 @pytest.mark.parametrize("paths", [8192, 30001])
-def test_one_pass_quantile_window(ctx, paths):
-    """Rows of at least 8,192 paths take the one-pass window search (a sorted sample of 2,048 paths brackets the
-    ranks); levels in the zero mass of the exposure rows, the median, the tails and both ends, on a row length
-    read 16 bytes per load (8,192) and one that is not (30,001): the exact interpolated quantile."""
+def test_exact_quantile_on_long_rows(ctx, paths):
+    """Levels in the zero mass of the exposure rows, the median, the tails and both ends, on a row length read 16
+    bytes per load (8,192) and one that is not (30,001): the exact interpolated quantile."""
     m, ns = gpu_setup(paths, True)
     for level in (0.0, 0.3, 0.5, 0.9, 0.975, 0.999, 1.0):
         p = gpu.compile(m, ns, S.Options(pfe_quantile=level))
