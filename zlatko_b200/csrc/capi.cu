@@ -5,8 +5,10 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <exception>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/zlatko_b200.h"
@@ -23,6 +25,12 @@ struct zk_context {
   uint32_t* dErr = nullptr;
   void* arena = nullptr;  // reusable device memory of zk_run_plan*
   size_t arenaBytes = 0;
+  // Reusable page-locked staging of zk_run_plan*: the host image of a call's inputs and its read-back.  A call
+  // ends with the stream synchronised, so the next call may overwrite them.
+  unsigned char* stageIn = nullptr;
+  size_t stageInBytes = 0;
+  unsigned char* stageOut = nullptr;
+  size_t stageOutBytes = 0;
 };
 
 namespace {
@@ -376,12 +384,41 @@ struct Batch {
 };
 
 
+// Validates and lowers the plans, on several host threads for a book of many plans; the first failure in plan
+// order is the one reported.
+template <typename R>
+void parseAll(const std::vector<View<R>>& views, std::vector<Plan<R>>& plans) {
+  const size_t n = views.size();
+  plans.assign(n, Plan<R>());
+  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+  const size_t workers = n >= 8 ? std::min<size_t>({hw, 16, n / 4}) : 1;
+  std::vector<std::exception_ptr> errs(n);
+  auto work = [&](size_t w) {
+    for (size_t i = w; i < n; i += workers) {
+      try {
+        plans[i] = parse(views[i], i);
+      } catch (...) {
+        errs[i] = std::current_exception();
+      }
+    }
+  };
+  if (workers == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (size_t w = 0; w < workers; ++w) pool.emplace_back(work, w);
+    for (auto& t : pool) t.join();
+  }
+  for (const auto& e : errs)
+    if (e) std::rethrow_exception(e);
+}
+
 template <typename R>
 std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams) {
   auto B = std::make_unique<Batch<R>>();
   B->ctx = ctx;
   B->sink = sink;
-  for (size_t i = 0; i < views.size(); ++i) B->plans.push_back(parse(views[i], i));
+  parseAll(views, B->plans);
   const size_t nPlans = B->plans.size();
   // ---- launch groups: plans sharing the scenario ----
   std::vector<int> launchOf(nPlans, -1);
@@ -483,11 +520,16 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
 }
 
 // Fills the host image of the input region, once the arena base is known.
+// img: the host image to fill (B.inputBytes), B.image when null.
 template <typename R>
-void fillImage(Batch<R>& B, const double* normals, size_t streams) {
-  B.image.assign(B.inputBytes, 0);
+void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char* img = nullptr) {
   B.im.clear();
-  unsigned char* img = B.image.data();
+  if (img) {
+    std::memset(img, 0, B.inputBytes);
+  } else {
+    B.image.assign(B.inputBytes, 0);
+    img = B.image.data();
+  }
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
   auto dptr = [&](size_t o) { return reinterpret_cast<void*>(base + o); };
   for (size_t i = 0; i < B.plans.size(); ++i) {
@@ -580,6 +622,14 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams) {
   }
 }
 
+void growStage(unsigned char*& stage, size_t& bytes, size_t need) {
+  if (bytes >= need) return;
+  if (stage) cudaFreeHost(stage);
+  stage = nullptr, bytes = 0;
+  ZK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&stage), std::max<size_t>(need, 1)));
+  bytes = need;
+}
+
 template <typename R>
 void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normals, size_t streams) {
   if (useCtxArena) {
@@ -597,8 +647,17 @@ void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normal
     B.base = static_cast<unsigned char*>(p);
     B.ownsArena = true;
   }
-  fillImage(B, normals, streams);
-  ZK_CUDA(cudaMemcpyAsync(B.base, B.image.data(), B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (useCtxArena) {
+    // Calls on the context arena synchronise before they return, so the context's page-locked staging is free;
+    // the wait below covers a previous call that failed with its copy in flight.
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    growStage(ctx->stageIn, ctx->stageInBytes, B.inputBytes);
+    fillImage(B, normals, streams, ctx->stageIn);
+    ZK_CUDA(cudaMemcpyAsync(B.base, ctx->stageIn, B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    fillImage(B, normals, streams);
+    ZK_CUDA(cudaMemcpyAsync(B.base, B.image.data(), B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));
+  }
 }
 
 cudaError_t recordEvent(cudaEvent_t e, cudaStream_t s, bool capturing) {
@@ -649,14 +708,16 @@ void finish(Batch<R>& B) {
 
 template <typename R, typename Out>
 void readOutputs(Batch<R>& B, Out* outs) {
-  std::vector<unsigned char> host(B.outBytes);
-  ZK_CUDA(cudaMemcpyAsync(host.data(), B.base + B.outBegin, B.outBytes, cudaMemcpyDeviceToHost, B.ctx->stream));
+  zk_context* ctx = B.ctx;
+  growStage(ctx->stageOut, ctx->stageOutBytes, B.outBytes);
+  unsigned char* host = ctx->stageOut;
+  ZK_CUDA(cudaMemcpyAsync(host, B.base + B.outBegin, B.outBytes, cudaMemcpyDeviceToHost, ctx->stream));
   finish(B);
   for (size_t i = 0; i < B.plans.size(); ++i) {
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    const R* sums = reinterpret_cast<const R*>(host.data() + (D.sums - B.outBegin));
-    const R* vals = reinterpret_cast<const R*>(host.data() + (D.values - B.outBegin));
+    const R* sums = reinterpret_cast<const R*>(host + (D.sums - B.outBegin));
+    const R* vals = reinterpret_cast<const R*>(host + (D.values - B.outBegin));
     const size_t nS = static_cast<size_t>(P.nT) * P.nS, nV = std::max<uint32_t>(P.v.num_outputs, 1);
     for (size_t k = 0; k < nS; ++k) outs[i].sums[k] = sums[k];
     for (size_t k = 0; k < nV; ++k) outs[i].values[k] = vals[k];
@@ -917,6 +978,8 @@ void zk_context_destroy(zk_context* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->arena) cudaFree(ctx->arena);
+  if (ctx->stageIn) cudaFreeHost(ctx->stageIn);
+  if (ctx->stageOut) cudaFreeHost(ctx->stageOut);
   if (ctx->dErr) cudaFree(ctx->dErr);
   if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
