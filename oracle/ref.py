@@ -68,6 +68,17 @@ def lib() -> C.CDLL:
         L.ref_unilateral_cva.restype = C.c_double
         L.ref_unilateral_cva.argtypes = [_dp, _dp, sz, _dp, _dp, sz, C.c_double]
         L.ref_bilateral_cva.argtypes = [_dp, _dp, _dp, sz, _dp, _dp, sz, _dp, _dp, sz, C.c_double, C.c_double, _dp]
+        vp = C.c_void_p
+        L.ref_xva.restype = None
+        L.ref_xva.argtypes = [_dp, _dp, _dp, sz, vp, _dp, _dp, sz, C.c_double, _dp, _dp, sz, C.c_double, _dp, _dp]
+        L.ref_allocate_exposure_xva.restype = None
+        L.ref_allocate_exposure_xva.argtypes = [_dp, sz, _dp, sz, _dp, _dp, sz, C.c_double, _dp, _dp, sz, _dp, _dp]
+        L.ref_initial_margin_profile.restype = None
+        L.ref_initial_margin_profile.argtypes = [_dp, _dp, sz, _dp, sz, C.c_double, C.c_double, _dp]
+        L.ref_marginal_contributions.restype = None
+        L.ref_marginal_contributions.argtypes = [_dp, sz, _dp, vp, sz, sz, _dp]
+        L.ref_incremental_exposure.restype = None
+        L.ref_incremental_exposure.argtypes = [_dp, _dp, vp, sz, sz, _dp]
         L.ref_quantile.restype = C.c_double
         L.ref_quantile.argtypes = [_dp, sz, C.c_double]
         L.ref_profile.argtypes = [_dp, _dp, sz, _dp, sz, C.c_double, C.c_double, _dp]
@@ -364,6 +375,56 @@ def bilateral_cva(times, dee, dene, cpty, own, rc: float, ro: float):
     lib().ref_bilateral_cva(f(times), f(dee), f(dene), len(times), f(cpty[0]), f(cpty[1]), len(cpty[0]), f(own[0]),
                             f(own[1]), len(own[0]), rc, ro, out)
     return float(out[0]), float(out[1])
+
+
+XVA_PARAM_ORDER = ("funding_spread_borrow", "funding_spread_lend", "margin_funding_spread", "hurdle_rate", "capital_ratio",
+                   "risk_weight", "alpha")
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
+def xva(times, dee, dene, dim, cpty, rc: float, own, ro: float, params: dict) -> dict:
+    """ccr::xva on a profile; cpty / own are (pillars, hazards); dim the discounted initial margin or None."""
+    out = np.zeros(6)
+    pr = _f64([params[k] for k in XVA_PARAM_ORDER])
+    d = _f64(dim) if dim is not None else None
+    lib().ref_xva(_f64(times), _f64(dee), _f64(dene), len(times), None if d is None else d.ctypes.data, _f64(cpty[0]),
+                  _f64(cpty[1]), len(cpty[0]), rc, _f64(own[0]), _f64(own[1]), len(own[0]), ro, pr, out)
+    return dict(zip(("cva", "dva", "fca", "fba", "mva", "kva"), out.tolist()))
+
+
+def allocate_exposure_xva(times, contributions, cpty, rc: float, own, params: dict) -> np.ndarray:
+    c = _f64(contributions)
+    out = np.zeros((c.shape[0], 3))
+    pr = _f64([params[k] for k in XVA_PARAM_ORDER])
+    lib().ref_allocate_exposure_xva(_f64(times), len(times), c, c.shape[0], _f64(cpty[0]), _f64(cpty[1]), len(cpty[0]), rc,
+                                    _f64(own[0]), _f64(own[1]), len(own[0]), pr, out)
+    return out
+
+
+def initial_margin_profile(values, deflator, times, q: float, mpr: float) -> np.ndarray:
+    v, d = _f64(values), _f64(deflator)
+    out = np.zeros(v.shape[1])
+    lib().ref_initial_margin_profile(v, d, v.shape[0], _f64(times), v.shape[1], q, mpr, out)
+    return out
+
+
+def marginal_contributions(trade_values, netted, deflator=None) -> np.ndarray:
+    tv, nv = _f64(trade_values), _f64(netted)
+    d = _f64(deflator) if deflator is not None else None
+    out = np.zeros((tv.shape[0], nv.shape[1]))
+    lib().ref_marginal_contributions(tv, tv.shape[0], nv, None if d is None else d.ctypes.data, nv.shape[0], nv.shape[1], out)
+    return out
+
+
+def incremental_exposure(netted, new_trade, deflator=None) -> np.ndarray:
+    nv, nt = _f64(netted), _f64(new_trade)
+    d = _f64(deflator) if deflator is not None else None
+    out = np.zeros(nv.shape[1])
+    lib().ref_incremental_exposure(nv, nt, None if d is None else d.ctypes.data, nv.shape[0], nv.shape[1], out)
+    return out
 
 
 def quantile(values, p: float) -> float:

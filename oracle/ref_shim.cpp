@@ -26,6 +26,8 @@
 #include "ccr/core/math.hpp"
 #include "ccr/core/parallel.hpp"
 #include "ccr/cva/cva.hpp"
+#include "ccr/exposure/allocation.hpp"
+#include "ccr/xva/xva.hpp"
 #include "ccr/exposure/collateral.hpp"
 #include "ccr/exposure/exposure_engine.hpp"
 #include "ccr/exposure/exposure_profile.hpp"
@@ -697,6 +699,78 @@ void ref_bilateral_cva(const double* times, const double* dee, const double* den
   const BilateralCva b = bilateralCva(p, c, rc, o, ro);
   out[0] = b.cva;
   out[1] = b.dva;
+}
+
+// ---- xVA and allocation (src/xva/xva.cpp, src/exposure/allocation.cpp) ----
+namespace {
+XvaParameters xvaParams(const double* p) {
+  XvaParameters x;
+  x.fundingSpreadBorrow = p[0], x.fundingSpreadLend = p[1], x.marginFundingSpread = p[2], x.hurdleRate = p[3];
+  x.capitalRatio = p[4], x.riskWeight = p[5], x.alpha = p[6];
+  return x;
+}
+CreditCurve curveOf(const double* pillars, const double* hazards, std::size_t n) {
+  return CreditCurve(std::vector<double>(pillars, pillars + n), std::vector<double>(hazards, hazards + n));
+}
+Matrix matrixOf(const double* a, std::size_t rows, std::size_t cols) {
+  Matrix m(rows, cols);
+  for (std::size_t i = 0; i < rows; ++i)
+    for (std::size_t j = 0; j < cols; ++j) m(i, j) = a[i * cols + j];
+  return m;
+}
+}  // namespace
+
+// xva(): out = cva, dva, fca, fba, mva, kva.  dim may be null (no initial margin).
+void ref_xva(const double* times, const double* dee, const double* dene, std::size_t n, const double* dim, const double* cp,
+             const double* ch, std::size_t nc, double rc, const double* op, const double* oh, std::size_t no, double ro,
+             const double* params, double* out) {
+  ExposureProfile p;
+  p.times.assign(times, times + n);
+  p.discountedExpectedExposure.assign(dee, dee + n);
+  p.discountedExpectedNegativeExposure.assign(dene, dene + n);
+  const std::vector<double> im = dim ? std::vector<double>(dim, dim + n) : std::vector<double>();
+  const Xva x = xva(p, im, curveOf(cp, ch, nc), rc, curveOf(op, oh, no), ro, xvaParams(params));
+  out[0] = x.cva, out[1] = x.dva, out[2] = x.fca, out[3] = x.fba, out[4] = x.mva, out[5] = x.kva;
+}
+
+// allocateExposureXva over `trades` contribution profiles [trade][n]: out[trade][3] = cva, fca, kva.
+void ref_allocate_exposure_xva(const double* times, std::size_t n, const double* contributions, std::size_t trades,
+                               const double* cp, const double* ch, std::size_t nc, double rc, const double* op, const double* oh,
+                               std::size_t no, const double* params, double* out) {
+  std::vector<std::vector<double>> c(trades);
+  for (std::size_t i = 0; i < trades; ++i) c[i].assign(contributions + i * n, contributions + (i + 1) * n);
+  const auto r = allocateExposureXva(std::vector<double>(times, times + n), c, curveOf(cp, ch, nc), rc, curveOf(op, oh, no),
+                                     xvaParams(params));
+  for (std::size_t i = 0; i < trades; ++i) out[3 * i] = r[i].cva, out[3 * i + 1] = r[i].fca, out[3 * i + 2] = r[i].kva;
+}
+
+// initialMarginProfile on values and deflator [paths][dates] and the grid's times: out[dates].
+void ref_initial_margin_profile(const double* values, const double* deflator, std::size_t paths, const double* times,
+                                std::size_t dates, double q, double mpr, double* out) {
+  const auto m = initialMarginProfile(matrixOf(values, paths, dates), TimeGrid(std::vector<double>(times, times + dates)),
+                                      matrixOf(deflator, paths, dates), q, mpr);
+  for (std::size_t j = 0; j < dates; ++j) out[j] = m[j];
+}
+
+// marginalExposureContributions: trade values [trade][paths][dates], netted [paths][dates], deflator (nullable):
+// out[trade][dates].
+void ref_marginal_contributions(const double* tradeValues, std::size_t trades, const double* netted, const double* deflator,
+                                std::size_t paths, std::size_t dates, double* out) {
+  std::vector<Matrix> tv;
+  for (std::size_t i = 0; i < trades; ++i) tv.push_back(matrixOf(tradeValues + i * paths * dates, paths, dates));
+  const Matrix nv = matrixOf(netted, paths, dates);
+  const Matrix d = deflator ? matrixOf(deflator, paths, dates) : Matrix();
+  const auto c = marginalExposureContributions(tv, nv, deflator ? &d : nullptr);
+  for (std::size_t i = 0; i < trades; ++i)
+    for (std::size_t j = 0; j < dates; ++j) out[i * dates + j] = c[i][j];
+}
+
+// incrementalExposure: out[dates].
+void ref_incremental_exposure(const double* netted, const double* newTrade, const double* deflator, std::size_t paths,
+                              std::size_t dates, double* out) {
+  const Matrix d = deflator ? matrixOf(deflator, paths, dates) : Matrix();
+  const auto r = incrementalExposure(matrixOf(netted, paths, dates), matrixOf(newTrade, paths, dates), deflator ? &d : nullptr);
+  for (std::size_t j = 0; j < dates; ++j) out[j] = r[j];
 }
 
 double ref_quantile(const double* v, std::size_t n, double p) { return quantile(std::vector<double>(v, v + n), p); }

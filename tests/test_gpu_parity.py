@@ -446,3 +446,24 @@ def test_fp64_matches_golden_engine(ctx, csa):
     scale = np.abs(f["netted"]).max()
     assert np.abs(rows[H[21]:H[21] + nR].T - f["netted"]).max() <= 1e-9 * scale
     assert abs(0.6 * np.nansum(res["cva_inc"]) - float(f["pathwise_cva_04"])) <= 1e-9 * abs(float(f["pathwise_cva_04"]))
+
+
+# ---------------------------------------------------------------- a book on common scenarios
+def test_book_on_the_gpu_matches_the_oracle(ctx):
+    """A book of four netting sets of two counterparties (zlatko_b200.book): one zk_run_plans call on the GPU, the
+    combined profile, the xVA per netting set and the per-trade allocation against the same book on the oracle."""
+    from test_book import OWN, small_book
+    from zlatko_b200 import book as B
+
+    m, nets, cps = small_book()
+    m.num_paths = 4000
+    plans = B.compile_book(m, nets, cps, S.Options(per_trade=True))
+    g = B.run_book(plans, m, cps, OWN, ctx=ctx)
+    r = B.run_book(plans, m, cps, OWN, run=restated.run_plan)
+    for k in B.ADDITIVE:
+        assert np.abs(g.total[k] - r.total[k]).max() <= RTOL * np.abs(r.total[k]).max(), k
+    for k in ("cva", "dva", "fca", "fba", "kva"):
+        assert abs(g.xva_total[k] - r.xva_total[k]) <= 1e-3 * abs(r.xva_total[k]), k
+    for ag, ar in zip(g.allocation, r.allocation):
+        scale = max(abs(t["cva"]) for t in ar)
+        assert max(abs(a["cva"] - b["cva"]) for a, b in zip(ag, ar)) <= 1e-3 * scale

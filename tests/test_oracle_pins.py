@@ -417,3 +417,58 @@ def test_engine_bermudans_are_the_reference_engine(csa):
     assert np.array_equal(e1.netted, e2.netted) and np.array_equal(e1.collateral, e2.collateral)
     for k in e1.profile:
         assert np.array_equal(e1.profile[k], e2.profile[k]), k
+
+
+# ------------------------------------------------------------------ xVA and allocation against the reference
+def _xva_inputs(seed=3, n=41):
+    rng = np.random.default_rng(seed)
+    t = np.concatenate([[0.0], np.cumsum(rng.uniform(0.05, 0.3, n - 1))])
+    dee = np.abs(rng.normal(1e6, 3e5, n)) * np.exp(-0.02 * t)
+    dene = -np.abs(rng.normal(8e5, 2e5, n)) * np.exp(-0.02 * t)
+    dim = np.abs(rng.normal(4e5, 1e5, n)) * np.exp(-0.02 * t)
+    cpty = ([1.0, 3.0, 7.0], [0.01, 0.015, 0.02])
+    own = ([2.0, 5.0], [0.005, 0.008])
+    return t, dee, dene, dim, cpty, own
+
+
+@needs_ref
+@pytest.mark.parametrize("with_im", [False, True])
+def test_xva_is_the_reference_xva(with_im):
+    from zlatko_b200 import xva as X
+
+    t, dee, dene, dim, cpty, own = _xva_inputs()
+    p = X.XvaParameters(funding_spread_borrow=0.012, funding_spread_lend=0.004, margin_funding_spread=0.009)
+    got = X.xva({"times": t, "dee": dee, "dene": dene}, dim if with_im else None, cpty, 0.4, own, 0.35, p)
+    want = ref.xva(t, dee, dene, dim if with_im else None, cpty, 0.4, own, 0.35, p.as_dict())
+    for k, w in want.items():
+        assert abs(got[k] - w) <= 1e-12 * max(abs(w), 1e-300), (k, got[k], w)
+    assert (got["mva"] > 0) == with_im
+    alloc = X.allocate_exposure_xva(t, [dee * 0.3, dee * 0.7], cpty, 0.4, own, p)
+    wa = ref.allocate_exposure_xva(t, [dee * 0.3, dee * 0.7], cpty, 0.4, own, p.as_dict())
+    for a, w in zip(alloc, wa):
+        for j, k in enumerate(("cva", "fca", "kva")):
+            assert abs(a[k] - w[j]) <= 1e-12 * abs(w[j])
+    assert abs(sum(a["cva"] for a in alloc) - got["cva"]) <= 1e-12 * got["cva"]  # the allocation adds up
+
+
+@needs_ref
+def test_allocation_and_margin_proxy_are_the_reference():
+    from zlatko_b200 import xva as X
+
+    rng = np.random.default_rng(9)
+    P, T, N = 500, 13, 4
+    times = np.linspace(0.0, 3.0, T)
+    tv = rng.normal(0.0, 1e5, (N, P, T))
+    tv[:, :, 0] = 0.0
+    netted = tv.sum(axis=0)
+    defl = np.exp(-0.02 * times)[None, :] * rng.uniform(0.9, 1.1, (P, T))
+    for d in (None, defl):
+        got = X.marginal_exposure_contributions(tv, netted, d)
+        want = ref.marginal_contributions(tv, netted, d)
+        assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
+        assert np.abs(got.sum(axis=0) - (np.maximum(netted, 0) * (1 if d is None else d)).mean(axis=0)).max() <= 1e-6
+        gi, wi = X.incremental_exposure(netted, tv[0], d), ref.incremental_exposure(netted, tv[0], d)
+        assert np.abs(gi - wi).max() <= 1e-9 * np.abs(wi).max()
+    gm = X.initial_margin_profile(netted, times, defl, 0.99, 10 / 250)
+    wm = ref.initial_margin_profile(netted, defl, times, 0.99, 10 / 250)
+    assert gm[0] == 0.0 and np.abs(gm - wm).max() <= 1e-12 * np.abs(wm).max()

@@ -27,6 +27,19 @@ def hazard_survival(pillars: Sequence[float], hazards: Sequence[float], t: float
     return math.exp(-integral)
 
 
+def exact_quantile(values, p: float) -> float:
+    """ccr::quantile (include/ccr/core/math.hpp:39-47): the sorted values interpolated between the order
+    statistics floor(h) and floor(h) + 1, h = p (n - 1)."""
+    s = np.sort(np.asarray(values, np.float64))
+    n = len(s)
+    if n == 0:
+        return math.nan
+    h = p * (n - 1)
+    lo = int(math.floor(h))
+    hi = min(lo + 1, n - 1)
+    return float(s[lo] + (h - lo) * (s[hi] - s[lo]))
+
+
 def _kahan(values) -> float:
     s, c = 0.0, 0.0
     for v in values:
