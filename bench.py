@@ -417,8 +417,8 @@ def main():
     fused_s = float(np.mean(fused_ms)) / 1e3
     nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
     cube_bytes = (2 + nA + nC) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
-    groups = (nP + 127) // 128  # statistics partials per 128-path group
-    alg_bytes = sum(p.rows_total * nP * 4 + groups * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
+    warps = -(-nP // (32 * (int(info.tile_paths) // 128)))  # statistics partials: one per revalue warp
+    alg_bytes = sum(p.rows_total * nP * 4 + warps * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
     ex2 = C_ex2 = None
     try:
         import ctypes as C

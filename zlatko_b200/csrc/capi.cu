@@ -497,9 +497,9 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
   for (size_t i = 0; i < nPlans; ++i) {
     const auto& P = B->plans[i];
-    const uint32_t tiles = (P.nP + kTile - 1) / kTile;  // the most tiles any tile shape uses
+    const uint32_t warps = (P.nP + 31) / 32;  // the most revalue warps any tile shape uses: one partial each
     B->dev[i].expo = take(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
-    B->dev[i].partials = take(static_cast<size_t>(tiles) * P.nT * P.nS * sizeof(R));
+    B->dev[i].partials = take(static_cast<size_t>(warps) * P.nT * P.nS * sizeof(R));
     if (P.im && !sink) B->dev[i].imState = take(static_cast<size_t>(P.nR) * (5 + P.nSlots) * P.nP * sizeof(R));
   }
   if (sink) {
@@ -683,7 +683,8 @@ void execute(Batch<R>& B, bool capturing = false) {
   for (const auto& M : B.im) ZK_CUDA(launchNestedIm<R>(M, s));
   ZK_CUDA(recordEvent(B.ev[2], s, capturing));
   if (!B.sink) {
-    ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN, s));
+    ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN,
+                            B.ppt, s));
     ZK_CUDA(recordEvent(B.ev[3], s, capturing));
     ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff), B.numRowJobs, ctx->dErr, s));
   } else {
@@ -741,8 +742,8 @@ void checkOutputs(const Batch<R>& B, const void* outs, bool f64) {
   }
 }
 
-// The tile shape: paths per revalue thread (kTile * ppt paths per CTA).  The partials are per 128-path
-// group whatever the shape, so the reduce jobs and the results do not change with it.
+// The tile shape: paths per revalue thread (kTile * ppt paths per CTA).  The reduce kernel completes the
+// 128-path groups' sums from the warp partials of the shape, so the results do not change with it.
 template <typename R>
 void setTileShape(Batch<R>& B, int ppt) {
   B.ppt = ppt;
@@ -1541,7 +1542,7 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
                                  numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, false, B->ppt, s));
     for (const auto& M : B->im) ZK_CUDA(launchNestedIm<float>(M, s));
-    ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, s));
+    ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, B->ppt, s));
     ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
     std::vector<unsigned char> host(B->outBytes);
     uint32_t devErr = 0;

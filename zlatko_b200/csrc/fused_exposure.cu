@@ -25,32 +25,35 @@ namespace zk {
 
 namespace {
 
-// lane l ends with the warp sum of statistic statSlotOfLane(l).
+// Lane l ends with the warp sum of statistic statSlotOfLane(l).  The lanes are combined as a binary tree over
+// neighbours (xor 1, then 2, 4, 8, 16: the first three halve the 8 values, the last two complete the sums), so
+// a statistic's sum over the warp's paths has the same tree whether a lane holds one path or the in-thread sum
+// of 2 or 4 adjacent paths: the partials do not depend on the tile shape.
 template <typename R>
 __device__ __forceinline__ R warpReduceScatter8(const R (&v)[8], uint32_t lane) {
-  const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u;
+  const bool b0 = lane & 1u, b1 = lane & 2u, b2 = lane & 4u;
   R a[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const R send = b4 ? v[i] : v[i + 4];
-    const R keep = b4 ? v[i + 4] : v[i];
-    a[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 16);
+    const R send = b0 ? v[i] : v[i + 4];
+    const R keep = b0 ? v[i + 4] : v[i];
+    a[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 1);
   }
   R b[2];
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
-    const R send = b3 ? a[i] : a[i + 2];
-    const R keep = b3 ? a[i + 2] : a[i];
-    b[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 8);
+    const R send = b1 ? a[i] : a[i + 2];
+    const R keep = b1 ? a[i + 2] : a[i];
+    b[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 2);
   }
   R c = (b2 ? b[1] : b[0]) + __shfl_xor_sync(0xFFFFFFFFu, b2 ? b[0] : b[1], 4);
-  c += __shfl_xor_sync(0xFFFFFFFFu, c, 2);
-  c += __shfl_xor_sync(0xFFFFFFFFu, c, 1);
+  c += __shfl_xor_sync(0xFFFFFFFFu, c, 8);
+  c += __shfl_xor_sync(0xFFFFFFFFu, c, 16);
   return c;
 }
 
 __device__ __forceinline__ uint32_t statSlotOfLane(uint32_t lane) {
-  return ((lane >> 4) & 1u) * 4u + ((lane >> 3) & 1u) * 2u + ((lane >> 2) & 1u);
+  return (lane & 1u) * 4u + ((lane >> 1) & 1u) * 2u + ((lane >> 2) & 1u);
 }
 
 template <typename R>
@@ -250,8 +253,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
   __shared__ NsArgs<R> sA;
-  R* red = reinterpret_cast<R*>(smemRaw);                          // [2][PPT][kWarps][8]
-  R* vtBuf = red + 2 * PPT * kWarps * 8;                           // [16][PPT][kTile] per-trade values
+  R* vtBuf = reinterpret_cast<R*>(smemRaw);                        // [16][PPT][kTile] per-trade values
   R* state = vtBuf + (kPerTrade ? kMaxTradeGroups * PPT * kTile : 0);  // fixings [nSlots][PPT][kTile] | ring
 
   const uint32_t n = blockIdx.x % numNs, tile = blockIdx.x / numNs;
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
   bool act[PPT];
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
-    pth[i] = tile * (kTile * PPT) + i * kTile + tid;
+    pth[i] = tile * (kTile * PPT) + tid * PPT + i;  // a thread's paths are adjacent
     act[i] = pth[i] < nP;
     pp[i] = act[i] ? pth[i] : nP - 1;  // threads past the last path read a valid path and contribute nothing
   }
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
 #pragma unroll
     for (int b = 0; b < 4; ++b) ex[b][i] = R(-1);  // exercise index of each Bermudan, -1 if not exercised
   }
-  uint32_t redBuf = 0, ringPos = 0;
+  uint32_t ringPos = 0;
 
   // Software pipeline: the factors and the date descriptor of date j + 1 load while date j computes.
   R nx[PPT], nD[PPT], nQ[PPT], nS4[4][PPT];
@@ -582,42 +584,41 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
       }
     }
 
-    // ---- statistics of this date: the netting set's 8, then kTradeStats per trade, reduced per 128-path
-    // group (slot i of the tile), so the partials and their bits do not depend on the tile shape ----
-    const uint32_t group0 = tile * PPT;
+    // ---- statistics of this date: the netting set's 8, then kTradeStats per trade, summed per warp over its
+    // 32 PPT adjacent paths as a binary tree (a thread's adjacent paths first, then the lanes) into one partial
+    // per warp: no block barrier.  The reduce kernel completes each 128-path group's tree from 4, 2 or 1 warp
+    // partials, so the group sums and their bits do not depend on the tile shape ----
+    const uint32_t unit = tile * kWarps + warp;
+    const bool unitLive = unit * (32u * PPT) < nP;
     for (uint32_t q = 0; q < nS; q += 8) {
-      R* rb = red + redBuf * (PPT * kWarps * 8);
+      R w8[PPT][8];
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
-        R v8[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) v8[c] = R(0);
+        for (int c = 0; c < 8; ++c) w8[i][c] = R(0);
         if (act[i]) {
           if (q == 0) {
-            v8[0] = e[i], v8[1] = ep[i], v8[2] = en[i], v8[3] = D[i] * ep[i], v8[4] = D[i] * en[i];
-            v8[5] = cvaInc[i], v8[6] = Q[i], v8[7] = D[i];
+            w8[i][0] = e[i], w8[i][1] = ep[i], w8[i][2] = en[i], w8[i][3] = D[i] * ep[i], w8[i][4] = D[i] * en[i];
+            w8[i][5] = cvaInc[i], w8[i][6] = Q[i], w8[i][7] = D[i];
           } else {
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
               const uint32_t k = q + c - kStatsPerDate, g = k / kTradeStats;
-              if (q + c < nS && g < nTr) v8[c] = tradeStat<R>(k % kTradeStats, vt(g, i), value[i], D[i]);
+              if (q + c < nS && g < nTr) w8[i][c] = tradeStat<R>(k % kTradeStats, vt(g, i), value[i], D[i]);
             }
           }
         }
-        const R s = warpReduceScatter8(v8, lane);
-        if ((lane & 3u) == 0) rb[(i * kWarps + warp) * 8 + statSlotOfLane(lane)] = s;
       }
-      __syncthreads();
-      if (tid < 8 * PPT) {
-        const uint32_t i = tid >> 3, c = tid & 7u;
-        if (q + c < nS && (group0 + i) * kTile < nP) {
-          R sum = R(0);
+      R v8[8];
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) sum += rb[(i * kWarps + w) * 8 + c];
-          A.partials[(static_cast<size_t>(group0 + i) * nT + j) * nS + q + c] = sum;
-        }
+      for (int c = 0; c < 8; ++c) {
+        if constexpr (PPT == 1) v8[c] = w8[0][c];
+        else if constexpr (PPT == 2) v8[c] = w8[0][c] + w8[1][c];
+        else v8[c] = (w8[0][c] + w8[1][c]) + (w8[2][c] + w8[3][c]);
       }
-      redBuf ^= 1u;  // the other buffer next time: one barrier per block of statistics
+      const R s = warpReduceScatter8(v8, lane);
+      const uint32_t c = statSlotOfLane(lane);
+      if (lane < 8u && unitLive && q + c < nS) A.partials[(static_cast<size_t>(unit) * nT + j) * nS + q + c] = s;
     }
     ringPos = ringPos + 1 == ringLen ? 0u : ringPos + 1;
   }
@@ -839,7 +840,7 @@ cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cud
 
 size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) {
   const size_t r = f64 ? 8 : 4;
-  return (2 * ppt * kWarps * 8 + (perTrade ? kMaxTradeGroups * ppt * kTile : 0) + stateWordsMax * ppt * kTile) * r;
+  return ((perTrade ? kMaxTradeGroups * ppt * kTile : 0) + stateWordsMax * ppt * kTile) * r;
 }
 
 namespace {

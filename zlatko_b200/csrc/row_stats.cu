@@ -300,14 +300,25 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
   }
 }
 
-template <typename R>
+// Partials come one per warp of the revalue kernel: the sum over its 32 ppt adjacent paths.  A 128-path group's
+// sum completes the binary tree of the warp sums ((w0 + w1) + (w2 + w3) for one path per thread, w0 + w1 for
+// two, w0 for four), absent warps past the last path counting as 0, so it has the same bits for every tile
+// shape; the groups are then summed in path order with a compensated double sum.
+template <typename R, int PPT>
 __global__ void reduceKernel(const ReduceJob<R>* __restrict__ jobs) {
   const ReduceJob<R> J = jobs[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= J.n) return;
+  constexpr uint32_t kUnits = 4 / PPT, kUnitPaths = 32 * PPT;
+  auto unit = [&](uint32_t u) { return u * kUnitPaths < J.nP ? J.partials[static_cast<size_t>(u) * J.n + i] : R(0); };
   double sum = 0.0, comp = 0.0;
   for (uint32_t t = 0; t < J.numTiles; ++t) {
-    const double yv = static_cast<double>(J.partials[static_cast<size_t>(t) * J.n + i]) - comp;
+    const uint32_t u0 = t * kUnits;
+    R g;
+    if constexpr (PPT == 1) g = (unit(u0) + unit(u0 + 1)) + (unit(u0 + 2) + unit(u0 + 3));
+    else if constexpr (PPT == 2) g = unit(u0) + unit(u0 + 1);
+    else g = unit(u0);
+    const double yv = static_cast<double>(g) - comp;
     const double tv = sum + yv;
     comp = (tv - sum) - yv;
     sum = tv;
@@ -318,10 +329,15 @@ __global__ void reduceKernel(const ReduceJob<R>* __restrict__ jobs) {
 }  // namespace
 
 template <typename R>
-cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, cudaStream_t stream) {
+cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, int ppt, cudaStream_t stream) {
   if (numJobs == 0 || maxN == 0) return cudaSuccess;
   const dim3 grid((maxN + 255) / 256, numJobs);
-  reduceKernel<R><<<grid, 256, 0, stream>>>(jobs);
+  switch (ppt) {
+    case 1: reduceKernel<R, 1><<<grid, 256, 0, stream>>>(jobs); break;
+    case 2: reduceKernel<R, 2><<<grid, 256, 0, stream>>>(jobs); break;
+    case 4: reduceKernel<R, 4><<<grid, 256, 0, stream>>>(jobs); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -335,8 +351,8 @@ cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* er
   return cudaGetLastError();
 }
 
-template cudaError_t launchReduce<float>(const ReduceJob<float>*, uint32_t, uint32_t, cudaStream_t);
-template cudaError_t launchReduce<double>(const ReduceJob<double>*, uint32_t, uint32_t, cudaStream_t);
+template cudaError_t launchReduce<float>(const ReduceJob<float>*, uint32_t, uint32_t, int, cudaStream_t);
+template cudaError_t launchReduce<double>(const ReduceJob<double>*, uint32_t, uint32_t, int, cudaStream_t);
 template cudaError_t launchRowStats<float>(const RowJob<float>*, uint32_t, uint32_t*, cudaStream_t);
 template cudaError_t launchRowStats<double>(const RowJob<double>*, uint32_t, uint32_t*, cudaStream_t);
 

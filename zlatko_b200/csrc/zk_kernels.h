@@ -40,7 +40,8 @@ struct ImArgs {
 template <typename R>
 cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream);
 
-// One reduce job per plan: sums[i] = (sum over tiles of partials[tile][i]) / nP for i < n.
+// One reduce job per plan: sums[i] = (sum over the 128-path groups of the group's partials) / nP for i < n, the
+// partials [warp][i] being one per revalue warp of the tile shape ppt (32 ppt paths); numTiles counts the groups.
 template <typename R>
 struct ReduceJob {
   const R* partials;
@@ -48,7 +49,7 @@ struct ReduceJob {
   uint32_t n, numTiles, nP, pad;
 };
 template <typename R>
-cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, cudaStream_t stream);
+cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, int ppt, cudaStream_t stream);
 
 // One row-statistics job per request (fused_kernels.cpp:565-771): the request record, its plan's rows.
 template <typename R>
