@@ -235,6 +235,39 @@ __device__ __forceinline__ void prefetchDate(uint32_t begin, uint32_t end, const
   if (tid < lines) prefetchL1(reinterpret_cast<const char*>(table) + (b / 128 + tid) * 128);
 }
 
+// A thread's PPT adjacent paths in one 8- or 16-byte access (p aligned to PPT values).
+template <typename R, int PPT>
+__device__ __forceinline__ void ldPaths(const R* p, R (&v)[PPT]) {
+  if constexpr (PPT == 1) {
+    v[0] = __ldg(p);
+  } else if constexpr (sizeof(R) == 4 && PPT == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = t.x, v[1] = t.y;
+  } else if constexpr (sizeof(R) == 4 && PPT == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < PPT; q += 2) {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(p) + q / 2);
+      v[q] = t.x, v[q + 1] = t.y;
+    }
+  }
+}
+template <typename R, int PPT>
+__device__ __forceinline__ void stPaths(R* p, const R (&v)[PPT]) {
+  if constexpr (PPT == 1) {
+    p[0] = v[0];
+  } else if constexpr (sizeof(R) == 4 && PPT == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else if constexpr (sizeof(R) == 4 && PPT == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < PPT; q += 2) reinterpret_cast<double2*>(p)[q / 2] = make_double2(v[q], v[q + 1]);
+  }
+}
+
 template <typename R, int PPT>
 __device__ __forceinline__ R pick4(const R (&a)[4][PPT], uint32_t k, int i) {
   return k == 0 ? a[0][i] : k == 1 ? a[1][i] : k == 2 ? a[2][i] : a[3][i];
@@ -275,7 +308,9 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
   for (int i = 0; i < PPT; ++i) {
     pth[i] = tile * (kTile * PPT) + tid * PPT + i;  // a thread's paths are adjacent
     act[i] = pth[i] < nP;
-    pp[i] = act[i] ? pth[i] : nP - 1;  // threads past the last path read a valid path and contribute nothing
+    // Threads past the last path read valid paths and contribute nothing: the last PPT paths when nP is a
+    // multiple of PPT (an aligned group, read as one vector), else the last path.
+    pp[i] = act[i] ? pth[i] : nP % PPT == 0 ? nP - PPT + i : nP - 1;
   }
   auto fix = [&](uint32_t slot, int i) -> R& { return state[(slot * PPT + i) * kTile + tid]; };
   auto ring = [&](uint32_t r, int i) -> R& { return state[((nSlots + r) * PPT + i) * kTile + tid]; };
@@ -310,8 +345,32 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
   // Software pipeline: the factors and the date descriptor of date j + 1 load while date j computes.
   R nx[PPT], nD[PPT], nQ[PPT], nS4[4][PPT];
   const size_t qOff = fQ != 0xFFFFFFFFu ? fQ * fieldStride : 0, sOff = static_cast<size_t>(cb.fS) * fieldStride;
+  // With nP a multiple of PPT a thread's paths are all live or all past the end, and their factors are one
+  // vector access per field (past the end: the last PPT paths).
+  const bool vecPaths = PPT > 1 && nP % PPT == 0;
   auto loadFactors = [&](uint32_t j) {
     const size_t off = static_cast<size_t>(j) * nP;
+    if (vecPaths) {
+      const R* c = cubeP[0] + off;
+      ldPaths<R, PPT>(c, nx);
+      ldPaths<R, PPT>(c + fieldStride, nD);
+      if (fQ != 0xFFFFFFFFu) {
+        ldPaths<R, PPT>(c + qOff, nQ);
+      } else {
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) nQ[i] = R(1);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (usesAssets && static_cast<uint32_t>(a) < cb.nA) {
+          ldPaths<R, PPT>(c + sOff + a * fieldStride, nS4[a]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) nS4[a][i] = R(0);
+        }
+      }
+      return;
+    }
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
       const R* c = cubeP[i] + off;
@@ -543,7 +602,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
       e[i] = value[i] - collateral, ep[i] = fmax(e[i], R(0)), en[i] = fmin(e[i], R(0));
       if (act[i] && rs > 0) {
         const size_t k = rs - 1, pi = pth[i], at = k * nP + pi;
-        rowEP[at] = ep[i];
+        if (!vecPaths) rowEP[at] = ep[i];
         if (moreRows) {
           if (A.rowDV != kNoRow) expo[(A.rowDV + k) * nP + pi] = rs == 1 ? R(0) : fabs(value[i] - prevRV[i]);
           if (A.rowE != kNoRow) expo[(A.rowE + k) * nP + pi] = e[i];
@@ -571,6 +630,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) reval
           expo[(A.rowEx + b) * static_cast<size_t>(nP) + pth[i]] = v < R(0) ? R(-1) : v;
         }
     }
+    if (vecPaths && act[0] && rs > 0) stPaths<R, PPT>(rowEP + static_cast<size_t>(rs - 1) * nP + pth[0], ep);
     R cvaInc[PPT];
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
