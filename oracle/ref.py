@@ -18,6 +18,7 @@ _LIB_PATH = os.path.join(_HERE, "_ref", "libccr_ref.so")
 _lib: Optional[C.CDLL] = None
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+INNER_FN = C.CFUNCTYPE(None, C.c_size_t, C.c_uint64, C.POINTER(C.c_double), C.c_size_t, C.c_void_p)
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
@@ -79,6 +80,16 @@ def lib() -> C.CDLL:
         L.ref_marginal_contributions.argtypes = [_dp, sz, _dp, vp, sz, sz, _dp]
         L.ref_incremental_exposure.restype = None
         L.ref_incremental_exposure.argtypes = [_dp, _dp, vp, sz, sz, _dp]
+        L.ref_estimate_adaptive.restype = C.c_int64
+        L.ref_estimate_adaptive.argtypes = [_dp, sz, sz, _dp, vp, INNER_FN, vp, C.c_double, C.c_double, C.c_double, _dp, sz,
+                                            C.c_uint64, vp, sz, C.c_char_p, sz]
+        L.ref_estimate_uniform.restype = C.c_int
+        L.ref_estimate_uniform.argtypes = [vp, sz, INNER_FN, vp, vp, sz, sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp,
+                                           C.c_char_p, sz]
+        L.ref_counter_normal.restype = C.c_double
+        L.ref_counter_normal.argtypes = [C.c_uint64, sz]
+        L.ref_derive_seed.restype = C.c_uint64
+        L.ref_derive_seed.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
         L.ref_quantile.restype = C.c_double
         L.ref_quantile.argtypes = [_dp, sz, C.c_double]
         L.ref_profile.argtypes = [_dp, _dp, sz, _dp, sz, C.c_double, C.c_double, _dp]
@@ -425,6 +436,75 @@ def incremental_exposure(netted, new_trade, deflator=None) -> np.ndarray:
     out = np.zeros(nv.shape[1])
     lib().ref_incremental_exposure(nv, nt, None if d is None else d.ctypes.data, nv.shape[0], nv.shape[1], out)
     return out
+
+
+def _adaptive_opts(o) -> np.ndarray:
+    return np.array([o.training_fraction, o.hermite_degree, o.inner_batch, o.min_inner_for_variance, o.max_inner_per_scenario,
+                     o.inner_budget, o.max_scenarios_per_round, o.max_rounds, o.audit_per_bin, o.min_per_bin_for_misspecification,
+                     float(o.refine_outside_training_range), 0.0] + list(o.bin_probabilities), np.float64)
+
+
+def _inner_callback(simulate):
+    def cb(scenario, seed, out, n, user):
+        buf = np.ctypeslib.as_array(out, shape=(n,))
+        simulate(int(scenario), int(seed), buf)
+    return INNER_FN(cb)
+
+
+def estimate_adaptive(features, payoff, weight, simulate, ee_rel: float, ee_abs: float, q: float, options) -> dict:
+    """nested::estimateAdaptive with PositivePart(ee_rel, ee_abs) and Quantile(q, positive part); simulate(scenario,
+    seed, out) fills out with inner payoffs."""
+    F = np.ascontiguousarray(features, np.float64)
+    y = np.ascontiguousarray(payoff, np.float64)
+    w = None if weight is None else np.ascontiguousarray(weight, np.float64)
+    opts = _adaptive_opts(options)
+    cb = _inner_callback(simulate)
+    e = _err()
+    args = (F, F.shape[0], F.shape[1], y, None if w is None else w.ctypes.data, cb, None, ee_rel, ee_abs, q, opts, opts.size,
+            int(options.seed))
+    n = lib().ref_estimate_adaptive(*args, None, 0, e, 512)
+    if n < 0:
+        raise ValueError(e.value.decode())
+    flat = np.zeros(n)
+    lib().ref_estimate_adaptive(*args, flat.ctypes.data, n, e, 512)
+    pos = 0
+
+    def take(k):
+        nonlocal pos
+        pos += k
+        return flat[pos - k:pos].copy()
+
+    def vec():
+        return take(int(take(1)[0]))
+
+    r = {"estimate": take(2), "baseline": take(2), "regression": take(2), "training": vec(), "evaluation": vec(),
+         "proxy": vec(), "value": vec(), "inner": vec()}
+    for k in ("inner_paths", "audit_inner_paths", "refined_scenarios", "audited_scenarios", "rounds", "unresolved",
+              "proxy_degree", "proxy_basis"):
+        r[k] = int(take(1)[0])
+    r["stop"] = ("converged", "scenario caps", "budget", "max rounds")[int(take(1)[0])]
+    r["bins"] = [take(7) for _ in range(int(take(1)[0]))]
+    return r
+
+
+def estimate_uniform(weight, n: int, simulate, scenarios, per_scenario: int, ee_rel: float, ee_abs: float, q: float,
+                     seed: int) -> np.ndarray:
+    w = None if weight is None else np.ascontiguousarray(weight, np.float64)
+    sc = np.ascontiguousarray(scenarios, np.uint64)
+    out = np.zeros(2 + len(sc))
+    e = _err()
+    if lib().ref_estimate_uniform(None if w is None else w.ctypes.data, n, _inner_callback(simulate), None, sc.ctypes.data, len(sc),
+                                  per_scenario, ee_rel, ee_abs, q, int(seed), out, e, 512):
+        raise ValueError(e.value.decode())
+    return out
+
+
+def counter_normal(seed: int, m: int) -> float:
+    return lib().ref_counter_normal(seed, m)
+
+
+def derive_seed(seed: int, a: int, b: int = 0, c: int = 0) -> int:
+    return lib().ref_derive_seed(seed, a, b, c)
 
 
 def quantile(values, p: float) -> float:

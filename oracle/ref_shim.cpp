@@ -28,6 +28,8 @@
 #include "ccr/cva/cva.hpp"
 #include "ccr/exposure/allocation.hpp"
 #include "ccr/xva/xva.hpp"
+#include "ccr/nested/adaptive_nested.hpp"
+#include "ccr/nested/nested_exposure.hpp"
 #include "ccr/exposure/collateral.hpp"
 #include "ccr/exposure/exposure_engine.hpp"
 #include "ccr/exposure/exposure_profile.hpp"
@@ -587,6 +589,103 @@ std::int64_t ref_summarise_full(const void* h, const float* sums, const float* v
     return -1;
   }
 }
+
+// ---- adaptive nested Monte Carlo (src/nested/adaptive_nested.cpp) ----
+// The inner simulator as a C callback: payoffs of `n` inner paths of `scenario` from `seed` into out.
+typedef void (*ref_inner_fn)(std::size_t scenario, std::uint64_t seed, double* out, std::size_t n, void* user);
+
+namespace {
+nested::AdaptiveOptions adaptiveOptions(const double* o, std::size_t no) {
+  nested::AdaptiveOptions a;
+  a.trainingFraction = o[0], a.hermiteDegree = static_cast<std::size_t>(o[1]), a.innerBatch = static_cast<std::size_t>(o[2]);
+  a.minInnerForVariance = static_cast<std::size_t>(o[3]), a.maxInnerPerScenario = static_cast<std::size_t>(o[4]);
+  a.innerBudget = static_cast<std::size_t>(o[5]), a.maxScenariosPerRound = static_cast<std::size_t>(o[6]);
+  a.maxRounds = static_cast<std::size_t>(o[7]), a.auditPerBin = static_cast<std::size_t>(o[8]);
+  a.minPerBinForMisspecification = static_cast<std::size_t>(o[9]), a.refineOutsideTrainingRange = o[10] != 0.0;
+  a.seed = static_cast<std::uint64_t>(o[11]);
+  a.binProbabilities.assign(o + 12, o + no);
+  return a;
+}
+}  // namespace
+
+// estimateAdaptive with statistics PositivePart(eeRel, eeAbs) and Quantile(q, positive part, 2.0), flattened:
+// estimate[2], baseline[2], regression[2], then length-prefixed training, evaluation, proxy, value, inner, then
+// innerPaths, auditInnerPaths, refinedScenarios, auditedScenarios, rounds, unresolved, proxyDegree, proxyBasis,
+// stop, then the bins (count, 7 numbers each).  seedHi/seedLo carry the 64-bit seed.  Returns the length.
+std::int64_t ref_estimate_adaptive(const double* features, std::size_t n, std::size_t dims, const double* payoff, const double* weight,
+                                   ref_inner_fn fn, void* user, double eeRel, double eeAbs, double q, const double* opts,
+                                   std::size_t nOpts, std::uint64_t seed, double* out, std::size_t cap, char* err, std::size_t errlen) {
+  try {
+    nested::OuterSample outer;
+    outer.features = Matrix(n, dims);
+    for (std::size_t i = 0; i < n; ++i)
+      for (std::size_t j = 0; j < dims; ++j) outer.features(i, j) = features[i * dims + j];
+    outer.payoff.assign(payoff, payoff + n);
+    if (weight) outer.weight.assign(weight, weight + n);
+    nested::AdaptiveOptions o = adaptiveOptions(opts, nOpts);
+    o.seed = seed;
+    const nested::PositivePart ee(eeRel, eeAbs, "EE*");
+    const nested::Quantile pfe(q, true, 2.0, "PFE");
+    const nested::InnerSimulator inner = [&](std::size_t sc, std::uint64_t sd, double* o2, std::size_t m) { fn(sc, sd, o2, m, user); };
+    SpinPool pool(1);
+    const auto r = nested::estimateAdaptive(outer, inner, {&ee, &pfe}, o, pool);
+    std::vector<double> d;
+    auto vec = [&](const auto& v) {
+      d.push_back(static_cast<double>(v.size()));
+      for (const auto& x : v) d.push_back(static_cast<double>(x));
+    };
+    for (const auto* v : {&r.estimate, &r.baseline, &r.regression})
+      for (double x : *v) d.push_back(x);
+    vec(r.training), vec(r.evaluation), vec(r.proxy), vec(r.value), vec(r.inner);
+    for (std::size_t x : {r.innerPaths, r.auditInnerPaths, r.refinedScenarios, r.auditedScenarios, r.rounds, r.unresolved,
+                          r.proxyDegree, r.proxyBasis})
+      d.push_back(static_cast<double>(x));
+    d.push_back(static_cast<double>(static_cast<int>(r.stop)));
+    d.push_back(static_cast<double>(r.bins.size()));
+    for (const auto& b : r.bins)
+      for (double x : {b.lowerProbability, b.upperProbability, static_cast<double>(b.scenarios), static_cast<double>(b.refined),
+                       b.residualStdDev, b.biasShift, b.biasRms})
+        d.push_back(x);
+    for (std::size_t k = 0; k < d.size() && k < cap; ++k) out[k] = d[k];
+    return static_cast<std::int64_t>(d.size());
+  } catch (const std::exception& e) {
+    setError(err, errlen, e);
+    return -1;
+  }
+}
+
+// estimateUniform with the same two statistics: out = estimate[2], then the value of every scenario.
+int ref_estimate_uniform(const double* weight, std::size_t n, ref_inner_fn fn, void* user, const std::uint64_t* scenarios,
+                         std::size_t ns, std::size_t perScenario, double eeRel, double eeAbs, double q, std::uint64_t seed, double* out,
+                         char* err, std::size_t errlen) {
+  try {
+    nested::OuterSample outer;
+    outer.features = Matrix(n, 1);
+    outer.payoff.assign(n, 0.0);
+    if (weight) outer.weight.assign(weight, weight + n);
+    const nested::PositivePart ee(eeRel, eeAbs, "EE*");
+    const nested::Quantile pfe(q, true, 2.0, "PFE");
+    const nested::InnerSimulator inner = [&](std::size_t sc, std::uint64_t sd, double* o2, std::size_t m) { fn(sc, sd, o2, m, user); };
+    SpinPool pool(1);
+    const std::vector<std::size_t> sc(scenarios, scenarios + ns);
+    const auto u = nested::estimateUniform(outer, inner, sc, perScenario, {&ee, &pfe}, seed, pool);
+    out[0] = u.estimate[0], out[1] = u.estimate[1];
+    for (std::size_t k = 0; k < ns; ++k) out[2 + k] = u.value[k];
+    return 0;
+  } catch (const std::exception& e) {
+    setError(err, errlen, e);
+    return 1;
+  }
+}
+
+// The reference's counter-based normals and seed mixing, for known answers.
+double ref_counter_normal(std::uint64_t seed, std::size_t m) {
+  nested::CounterNormals c(seed);
+  double v = 0.0;
+  for (std::size_t k = 0; k <= m; ++k) v = c.next();
+  return v;
+}
+std::uint64_t ref_derive_seed(std::uint64_t seed, std::uint64_t a, std::uint64_t b, std::uint64_t c) { return nested::deriveSeed(seed, a, b, c); }
 
 // ------------------------------------------------------------------ FP64 engine
 // ExposureEngine::run (exposure_engine.cpp:50-81) on the reference's own normals (normals == nullptr) or

@@ -1,0 +1,797 @@
+"""Adaptive nested Monte Carlo: a least-squares proxy on the outer paths, a stratified audit of its bias, and inner
+simulations only where a statistic needs them.
+
+Restates src/nested/adaptive_nested.cpp (the estimator: HermiteProxy, ScenarioEstimates, the PositivePart and
+Quantile statistics, estimateAdaptive, estimateUniform) in the reference's arithmetic order, so that on the same
+outer sample and the same inner payoffs it reaches the same decisions and estimates.  The estimator is host
+control logic; its inner simulations are the expensive part and run as batches: every round hands all its jobs
+(scenario, seed, paths) to the inner simulator at once, so a GPU simulator (nested_gpu.InnerPaths) runs a round
+in one kernel launch where the reference calls a per-scenario callback on a thread pool.
+"""
+from __future__ import annotations
+
+import bisect
+import math
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .summary import exact_quantile
+
+M64 = 0xFFFFFFFFFFFFFFFF
+GOLDEN = 0x9E3779B97F4A7C15
+MIN_GAIN = 0.05                 # refining a scenario that removes less of its error variance is skipped
+ADAPTIVE_TAG = 0x6164617074697665
+UNIFORM_TAG = 0x756E69666F726D00
+SPLIT_TAG = 0x73706C6974000000
+
+# An inner simulator takes a round's jobs [(scenario, seed, paths)] and returns one payoff array per job.
+InnerBatches = Callable[[List[Tuple[int, int, int]]], List[np.ndarray]]
+
+
+def split_mix(z: int) -> int:
+    """SplitMix64 finaliser (adaptive_nested.cpp:23-28)."""
+    z = (z + GOLDEN) & M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+    return z ^ (z >> 31)
+
+
+def derive_seed(seed: int, a: int, b: int = 0, c: int = 0) -> int:
+    """deriveSeed (adaptive_nested.cpp:120-125)."""
+    x = split_mix((seed + GOLDEN) & M64)
+    x = split_mix(x ^ (a & M64))
+    x = split_mix(x ^ ((b * 0xD1B54A32D192ED03) & M64))
+    return split_mix(x ^ ((c * 0x8CB92BA72F3D8DD7) & M64))
+
+
+def shuffle(v: List[int], seed: int) -> None:
+    """Deterministic Fisher-Yates shuffle (adaptive_nested.cpp:31-38)."""
+    s = seed
+    for i in range(len(v), 1, -1):
+        s = split_mix(s)
+        j = s % i
+        v[i - 1], v[j] = v[j], v[i - 1]
+
+
+def counter_normal(seed: int, m: int) -> float:
+    """Normal m (0-based) of CounterNormals(seed) (adaptive_nested.cpp:127-141): pair m // 2 of the SplitMix64
+    stream, the cosine half first.  Counter-based, so any normal is reached directly."""
+    state = (seed + (m // 2 + 1) * GOLDEN) & M64
+    h1 = split_mix(state)
+    h2 = split_mix(h1 ^ 0x68E31DA4B5297A4D)
+    u1 = (float(h1 >> 11) + 0.5) * 2.0 ** -53
+    u2 = float(h2 >> 11) * 2.0 ** -53
+    r, a = math.sqrt(-2.0 * math.log(u1)), 6.283185307179586 * u2
+    return r * math.cos(a) if m % 2 == 0 else r * math.sin(a)
+
+
+def normal_cdf(x: float) -> float:
+    """ccr::normalCdf (include/ccr/core/math.hpp:15)."""
+    return 0.5 * math.erfc(-x / math.sqrt(2.0))
+
+
+def _seq_sum(a) -> float:
+    """A left-to-right sum (the reference's loops), not numpy's pairwise one."""
+    s = 0.0
+    for v in a:
+        s += v
+    return s
+
+
+def _cholesky(a: np.ndarray) -> np.ndarray:
+    """ccr::cholesky (src/core/matrix.cpp:49-68); raises ValueError where the reference throws."""
+    n = a.shape[0]
+    lo = np.zeros((n, n))
+    for i in range(n):
+        for j in range(i + 1):
+            if abs(a[i, j] - a[j, i]) > 1e-10:
+                raise ValueError("cholesky: matrix must be symmetric")
+            s = float(a[i, j])
+            for k in range(j):
+                s -= lo[i, k] * lo[j, k]
+            if i == j:
+                if s <= 0.0:
+                    raise ValueError("cholesky: matrix is not positive definite")
+                lo[i, i] = math.sqrt(s)
+            else:
+                lo[i, j] = s / lo[j, j]
+    return lo
+
+
+def _cholesky_solve(lo: np.ndarray, b) -> np.ndarray:
+    """Forward and back substitution with a lower-triangular factor (adaptive_nested.cpp:41-54)."""
+    n = lo.shape[0]
+    x = [float(v) for v in b]
+    for i in range(n):
+        s = x[i]
+        for k in range(i):
+            s -= lo[i, k] * x[k]
+        x[i] = s / lo[i, i]
+    for i in range(n - 1, -1, -1):
+        s = x[i]
+        for k in range(i + 1, n):
+            s -= lo[k, i] * x[k]
+        x[i] = s / lo[i, i]
+    return np.array(x)
+
+
+def total_degree_terms(dims: int, degree: int) -> List[List[int]]:
+    """Exponent vectors of total degree <= degree in graded order (adaptive_nested.cpp:57-75)."""
+    out: List[List[int]] = []
+    cur = [0] * dims
+
+    def rec(pos: int, remaining: int) -> None:
+        if pos == dims:
+            out.append(list(cur))
+            return
+        for k in range(remaining + 1):
+            cur[pos] = k
+            rec(pos + 1, remaining - k)
+        cur[pos] = 0
+
+    rec(0, degree)
+    return sorted(out, key=sum)  # stable, as std::stable_sort
+
+
+class HermiteProxy:
+    """Least-squares proxy of V in probabilists' Hermite polynomials of the standardised features, all products
+    up to a total degree, with the HC0 sandwich variance of every prediction (adaptive_nested.cpp:145-277)."""
+
+    def __init__(self, degree: int = 3, ridge: float = 1e-10):
+        self.degree_, self.ridge = degree, ridge
+        self.fitted_degree = 0
+        self.terms: List[List[int]] = []
+        self.beta: Optional[np.ndarray] = None
+
+    def basis_rows(self, x: np.ndarray) -> np.ndarray:
+        """phi for every row of x [n][dims] (the reference's basis(), row by row in its operation order)."""
+        x = np.atleast_2d(np.asarray(x, np.float64))
+        d, m = self.fitted_degree, len(self.active)
+        h = np.zeros((x.shape[0], m, d + 1))
+        for f, j in enumerate(self.active):
+            z = (x[:, j] - self.mean[j]) / self.scale[j]
+            h[:, f, 0] = 1.0
+            if d >= 1:
+                h[:, f, 1] = z
+            for k in range(1, d):
+                h[:, f, k + 1] = z * h[:, f, k] - float(k) * h[:, f, k - 1]
+        phi = np.ones((x.shape[0], len(self.terms)))
+        for t, powers in enumerate(self.terms):
+            v = np.ones(x.shape[0])
+            for f in range(m):
+                if powers[f] > 0:
+                    v = v * h[:, f, powers[f]]
+            phi[:, t] = v
+        return phi
+
+    def fit(self, features: np.ndarray, y: Sequence[float], rows: Sequence[int]) -> None:
+        n = len(rows)
+        if n < 2:
+            raise ValueError("HermiteProxy: needs at least two training rows")
+        F = np.asarray(features, np.float64)
+        if F.shape[0] != len(y):
+            raise ValueError("HermiteProxy: features and targets differ in length")
+        dim = F.shape[1]
+        mean = np.zeros(dim)
+        for r in rows:
+            mean = mean + F[r]
+        mean = mean / float(n)
+        ss = np.zeros(dim)
+        for r in rows:
+            ss = ss + (F[r] - mean) * (F[r] - mean)
+        self.mean, self.scale, self.active = mean, np.ones(dim), []
+        for j in range(dim):
+            sd = math.sqrt(ss[j] / float(n - 1))
+            if sd > 1e-12 * max(1.0, abs(mean[j])):
+                self.scale[j] = sd
+                self.active.append(j)
+        d = self.degree_
+        while True:
+            self.terms = total_degree_terms(len(self.active), d)
+            self.fitted_degree = d
+            if 2 * len(self.terms) <= n or d == 0:
+                break
+            d -= 1
+        if len(self.terms) > 2000:
+            raise ValueError("HermiteProxy: more than 2000 basis functions")
+        p = len(self.terms)
+        phis = self.basis_rows(F[list(rows)])
+        yy = np.asarray(y, np.float64)
+        gram, rhs = np.zeros((p, p)), np.zeros(p)
+        for k, r in enumerate(rows):
+            phi = phis[k]
+            rhs = rhs + phi * yy[r]
+            gram = gram + np.outer(phi, phi)
+        trace = 0.0
+        for a in range(p):
+            trace += gram[a, a]
+        gram = np.tril(gram) + np.tril(gram, -1).T
+        ridge = self.ridge
+        while True:
+            g = gram.copy()
+            lam = ridge * max(trace / float(p), 1e-300)
+            for a in range(p):
+                g[a, a] += lam
+            try:
+                lo = _cholesky(g)
+                break
+            except ValueError:
+                if ridge > 1e-2:
+                    raise ValueError("HermiteProxy: normal equations are singular")
+                ridge *= 1e3
+        self.beta = _cholesky_solve(lo, rhs)
+        meat = np.zeros((p, p))
+        for k, r in enumerate(rows):
+            phi = phis[k]
+            fitted = _seq_sum(phi * self.beta)
+            e2 = (yy[r] - fitted) * (yy[r] - fitted)
+            meat = meat + np.outer(e2 * phi, phi)
+        meat = np.tril(meat) + np.tril(meat, -1).T
+        inverse = np.zeros((p, p))
+        for c in range(p):
+            unit = np.zeros(p)
+            unit[c] = 1.0
+            inverse[:, c] = _cholesky_solve(lo, unit)
+        tmp = np.zeros((p, p))
+        for a in range(p):
+            for k in range(p):
+                v = inverse[a, k]
+                if v != 0.0:
+                    tmp[a] = tmp[a] + v * meat[k]
+        cov = np.zeros((p, p))
+        for a in range(p):
+            for k in range(p):
+                v = tmp[a, k]
+                if v != 0.0:
+                    cov[a] = cov[a] + v * inverse[k]
+        self.cov = cov
+
+    def predict_rows(self, x: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """(value, estimation variance) of every row of x, each summed in the reference's order."""
+        if self.beta is None:
+            raise RuntimeError("HermiteProxy: predict before fit")
+        phi = self.basis_rows(x)
+        value = np.add.accumulate(phi * self.beta[None, :], axis=1)[:, -1]
+        acc = np.stack([np.add.accumulate(self.cov[a][None, :] * phi, axis=1)[:, -1] for a in range(len(self.terms))], axis=1)
+        var = np.add.accumulate(phi * acc, axis=1)[:, -1]
+        return value, np.maximum(var, 0.0)
+
+    def degree(self) -> int:
+        return self.fitted_degree
+
+    def num_basis(self) -> int:
+        return len(self.terms)
+
+
+def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int, float, float]:
+    """Chan et al. merge of a batch into a running (count, mean, M2) (adaptive_nested.cpp:371-384)."""
+    n = len(payoffs)
+    if n == 0:
+        return count, mean, m2
+    batch_mean = _seq_sum(payoffs) / float(n)
+    batch_m2 = _seq_sum((payoffs - batch_mean) * (payoffs - batch_mean))
+    na, nb = float(count), float(n)
+    total = na + nb
+    delta = batch_mean - mean
+    mean += delta * nb / total
+    m2 += batch_m2 + delta * delta * (na * nb / total)
+    return count + n, mean, m2
+
+
+class ScenarioEstimates:
+    """What is known about every evaluation scenario: proxy value and uncertainty, bin, and inner samples in two
+    folds (adaptive_nested.cpp:279-437)."""
+
+    def __init__(self, outer_payoff, weight, proxy_mean, proxy_variance, bins, residual_variance_by_bin,
+                 min_inner_for_variance: int, max_inner_per_scenario: int):
+        n = len(proxy_mean)
+        if not (len(outer_payoff) == len(weight) == len(proxy_variance) == len(bins) == n):
+            raise ValueError("ScenarioEstimates: inconsistent sizes")
+        self.w = [float(v) for v in weight]
+        self.mu = [float(v) for v in proxy_mean]
+        self.pv = [float(v) for v in proxy_variance]
+        self.bin = [int(b) for b in bins]
+        self.residual = [float(v) for v in residual_variance_by_bin]
+        nb = len(self.residual)
+        self.misspec, self.shift = [0.0] * nb, [0.0] * nb
+        self.min_inner, self.max_inner = min_inner_for_variance, max_inner_per_scenario
+        self.count0, self.count1, self.batches = [1] * n, [0] * n, [0] * n
+        self.mean0, self.mean1 = [float(v) for v in outer_payoff], [0.0] * n
+        self.m20, self.m21 = [0.0] * n, [0.0] * n
+
+    def size(self) -> int:
+        return len(self.mu)
+
+    def num_bins(self) -> int:
+        return len(self.residual)
+
+    def proxy_mean(self, i: int) -> float:
+        return self.mu[i] + self.shift[self.bin[i]]
+
+    def proxy_variance(self, i: int) -> float:
+        return self.pv[i] + self.misspec[self.bin[i]]
+
+    def inner_paths(self, i: int) -> int:
+        return self.count0[i] + self.count1[i] - 1
+
+    def pooled(self, i: int) -> Tuple[float, float, float]:
+        n0, n1 = float(self.count0[i]), float(self.count1[i])
+        n = n0 + n1
+        if self.count1[i] == 0:
+            return n, self.mean0[i], self.m20[i]
+        d = self.mean1[i] - self.mean0[i]
+        return n, self.mean0[i] + d * n1 / n, self.m20[i] + self.m21[i] + d * d * (n0 * n1 / n)
+
+    def blend(self, i: int, sample_mean: float, sample_variance: float) -> Tuple[float, float]:
+        pvar, proxy = self.proxy_variance(i), self.proxy_mean(i)
+        den = pvar + sample_variance
+        if den <= 0.0:
+            return proxy, 0.0
+        return proxy + pvar / den * (sample_mean - proxy), pvar * sample_variance / den
+
+    def within_variance(self, i: int) -> float:
+        n, _, m2 = self.pooled(i)
+        return m2 / (n - 1.0) if n >= 1.0 + float(self.min_inner) else self.residual[self.bin[i]]
+
+    def estimate(self, i: int) -> float:
+        n, mean, _ = self.pooled(i)
+        return self.blend(i, mean, self.within_variance(i) / n)[0]
+
+    def std_error(self, i: int) -> float:
+        n, mean, _ = self.pooled(i)
+        return math.sqrt(self.blend(i, mean, self.within_variance(i) / n)[1])
+
+    def refinement_gain(self, i: int) -> float:
+        n, mean, _ = self.pooled(i)
+        within = self.within_variance(i)
+        current = self.blend(i, mean, within / n)[1]
+        if current <= 0.0:
+            return 0.0
+        used = float(self.inner_paths(i))
+        remaining = max(0.0, float(self.max_inner) - used)
+        best = self.blend(i, mean, within / (n + remaining))[1]
+        return 1.0 - best / current
+
+    def selection_estimate(self, i: int) -> float:
+        if self.count1[i] == 0:
+            return self.proxy_mean(i)
+        return self.blend(i, self.mean0[i], self.within_variance(i) / float(self.count0[i]))[0]
+
+    def value_estimate(self, i: int) -> float:
+        return self.mean1[i] if self.count1[i] > 0 else self.mean0[i]
+
+    def value_variance(self, i: int) -> float:
+        return self.within_variance(i) / float(self.count1[i] if self.count1[i] > 0 else self.count0[i])
+
+    def add_inner_batch(self, i: int, payoffs: np.ndarray) -> None:
+        n = len(payoffs)
+        if n == 0:
+            return
+        if not np.all(np.isfinite(payoffs)):
+            raise RuntimeError("nested Monte Carlo: inner simulation returned a non-finite payoff")
+        half = n // 2
+        self.count0[i], self.mean0[i], self.m20[i] = _merge(self.count0[i], self.mean0[i], self.m20[i], payoffs[:half])
+        self.count1[i], self.mean1[i], self.m21[i] = _merge(self.count1[i], self.mean1[i], self.m21[i], payoffs[half:])
+        self.batches[i] += 1
+
+    def update_misspecification(self, min_scenarios_per_bin: int) -> None:
+        nb = self.num_bins()
+        s, sq, noise, cnt = [0.0] * nb, [0.0] * nb, [0.0] * nb, [0] * nb
+        gsq = gnoise = 0.0
+        gcount = 0
+        for i in range(self.size()):
+            n, mean, m2 = self.pooled(i)
+            if n < 1.0 + float(self.min_inner):
+                continue
+            d = mean - self.mu[i]
+            sampling = m2 / (n - 1.0) / n + self.pv[i]
+            b = self.bin[i]
+            s[b] += d
+            sq[b] += d * d
+            noise[b] += sampling
+            cnt[b] += 1
+            gsq += d * d
+            gnoise += sampling
+            gcount += 1
+        glob = max(0.0, (gsq - gnoise) / float(gcount)) if gcount > 0 else 0.0
+        for b in range(nb):
+            if cnt[b] >= min_scenarios_per_bin:
+                c = float(cnt[b])
+                self.shift[b] = s[b] / c
+                self.misspec[b] = max(0.0, (sq[b] - c * self.shift[b] * self.shift[b] - noise[b]) / c)
+            else:
+                self.shift[b] = 0.0
+                self.misspec[b] = glob
+
+
+def _misclassification_probability(gap: float, se: float) -> float:
+    return normal_cdf(-gap / se) if se > 0.0 else 0.0
+
+
+def _mark_largest(contribution: List[float], s: ScenarioEstimates, excess: float, urgency: List[float]) -> None:
+    """The error-budget rule (adaptive_nested.cpp:85-106)."""
+    n = len(contribution)
+    gain = [s.refinement_gain(i) for i in range(n)]
+    reducible = [contribution[i] * gain[i] for i in range(n)]
+    order = sorted(range(n), key=lambda i: -reducible[i])  # stable, descending
+    covered = 0.0
+    for i in order:
+        if covered >= excess or reducible[i] <= 0.0:
+            break
+        if gain[i] < MIN_GAIN:
+            continue
+        urgency[i] = max(urgency[i], 2.0)
+        covered += reducible[i]
+
+
+class PositivePart:
+    """E[w max(V, 0)]: EE with w = 1, EE* with w = D(0, t) (adaptive_nested.cpp:439-488)."""
+
+    def __init__(self, relative_tolerance: float = 0.01, absolute_tolerance: float = 0.0, label: str = "EE"):
+        if not (relative_tolerance >= 0.0) or not (absolute_tolerance >= 0.0) or relative_tolerance + absolute_tolerance == 0.0:
+            raise ValueError("PositivePart: tolerances must be non-negative and not both zero")
+        self.rel, self.abs, self.label = relative_tolerance, absolute_tolerance, label
+
+    def name(self) -> str:
+        return self.label
+
+    def evaluate(self, s: ScenarioEstimates) -> float:
+        total = 0.0
+        for i in range(s.size()):
+            if s.selection_estimate(i) > 0.0:
+                total += s.w[i] * s.value_estimate(i)
+        return total / float(s.size()) if s.size() else 0.0
+
+    def plug_in(self, values, weights) -> float:
+        total = 0.0
+        for i, v in enumerate(values):
+            total += (1.0 if weights is None or len(weights) == 0 else weights[i]) * max(v, 0.0)
+        return total / float(len(values)) if len(values) else 0.0
+
+    def urgency(self, s: ScenarioEstimates, urgency: List[float]) -> None:
+        n = s.size()
+        if n == 0:
+            return
+        half = 0.5 * max(self.abs, self.rel * abs(self.evaluate(s)))
+        if not (half > 0.0):
+            return
+        nn = float(n)
+        noise, counted = 0.0, 0
+        sel = [s.selection_estimate(i) for i in range(n)]
+        for i in range(n):
+            if sel[i] > 0.0:
+                noise += s.w[i] * s.w[i] * s.value_variance(i)
+                counted += 1
+        if counted > 0 and math.sqrt(noise) / nn > half:
+            share = half * half * nn * nn / float(counted)
+            for i in range(n):
+                if sel[i] > 0.0:
+                    urgency[i] = max(urgency[i], s.w[i] * s.w[i] * s.value_variance(i) / share)
+        contribution = [0.0] * n
+        total = 0.0
+        for i in range(n):
+            est, se = s.estimate(i), s.std_error(i)
+            gap = abs(est)
+            contribution[i] = s.w[i] * (gap * _misclassification_probability(gap, se)) / nn
+            total += contribution[i]
+        if total > half:
+            _mark_largest(contribution, s, total - half, urgency)
+
+
+class Quantile:
+    """The `level` quantile of V across scenarios, of max(V, 0) with positive_part (PFE) (adaptive_nested.cpp:490-523)."""
+
+    def __init__(self, level: float, positive_part: bool = False, z_critical: float = 2.0, label: str = "quantile"):
+        if not (0.0 < level < 1.0):
+            raise ValueError("Quantile: level must be in (0, 1)")
+        if not (z_critical > 0.0):
+            raise ValueError("Quantile: zCritical must be positive")
+        self.level, self.pos, self.z, self.label = level, positive_part, z_critical, label
+
+    def name(self) -> str:
+        return self.label
+
+    def plug_in(self, values, weights=None) -> float:
+        if len(values) == 0:
+            return 0.0
+        q = exact_quantile(values, self.level)
+        return max(q, 0.0) if self.pos else q
+
+    def evaluate(self, s: ScenarioEstimates) -> float:
+        return self.plug_in([s.estimate(i) for i in range(s.size())])
+
+    def urgency(self, s: ScenarioEstimates, urgency: List[float]) -> None:
+        n = s.size()
+        if n == 0:
+            return
+        v = [s.estimate(i) for i in range(n)]
+        q = exact_quantile(v, self.level)
+        if self.pos and q < 0.0:
+            return
+        threshold = normal_cdf(-self.z)
+        for i in range(n):
+            p = _misclassification_probability(abs(v[i] - q), s.std_error(i))
+            urgency[i] = max(urgency[i], s.refinement_gain(i) * p / threshold)
+
+
+@dataclass
+class AdaptiveOptions:
+    """AdaptiveOptions (include/ccr/nested/adaptive_nested.hpp:205-227)."""
+
+    training_fraction: float = 0.5
+    hermite_degree: int = 3
+    inner_batch: int = 64
+    min_inner_for_variance: int = 32
+    max_inner_per_scenario: int = 4096
+    inner_budget: int = 2_000_000
+    max_scenarios_per_round: int = 2000
+    max_rounds: int = 50
+    audit_per_bin: int = 16
+    min_per_bin_for_misspecification: int = 8
+    bin_probabilities: Sequence[float] = (0.005, 0.01, 0.025, 0.05, 0.1, 0.25, 0.5, 0.75, 0.9, 0.95, 0.975, 0.99, 0.995)
+    refine_outside_training_range: bool = True
+    seed: int = 20261122
+
+    def validate(self) -> None:
+        if not (0.0 < self.training_fraction < 1.0):
+            raise ValueError("AdaptiveOptions: trainingFraction must be in (0, 1)")
+        if self.inner_batch < 1:
+            raise ValueError("AdaptiveOptions: innerBatch must be at least 1")
+        if self.min_inner_for_variance < 2:
+            raise ValueError("AdaptiveOptions: minInnerForVariance must be at least 2")
+        if self.max_inner_per_scenario < max(self.inner_batch, self.min_inner_for_variance):
+            raise ValueError("AdaptiveOptions: maxInnerPerScenario must be at least innerBatch and minInnerForVariance")
+        if self.max_scenarios_per_round < 1:
+            raise ValueError("AdaptiveOptions: maxScenariosPerRound must be at least 1")
+        if self.min_per_bin_for_misspecification < 1:
+            raise ValueError("AdaptiveOptions: minPerBinForMisspecification must be at least 1")
+        for k, p in enumerate(self.bin_probabilities):
+            if not (0.0 < p < 1.0) or (k > 0 and not p > self.bin_probabilities[k - 1]):
+                raise ValueError("AdaptiveOptions: binProbabilities must be strictly increasing in (0, 1)")
+
+
+STOP_REASONS = ("converged", "scenario caps", "budget", "max rounds")
+
+
+@dataclass
+class AdaptiveResult:
+    names: List[str] = field(default_factory=list)
+    estimate: List[float] = field(default_factory=list)
+    baseline: List[float] = field(default_factory=list)
+    regression: List[float] = field(default_factory=list)
+    training: List[int] = field(default_factory=list)
+    evaluation: List[int] = field(default_factory=list)
+    proxy: List[float] = field(default_factory=list)
+    value: List[float] = field(default_factory=list)
+    inner: List[int] = field(default_factory=list)
+    inner_paths: int = 0
+    audit_inner_paths: int = 0
+    refined_scenarios: int = 0
+    audited_scenarios: int = 0
+    rounds: int = 0
+    unresolved: int = 0
+    proxy_degree: int = 0
+    proxy_basis: int = 0
+    stop: str = "converged"
+    bins: List[dict] = field(default_factory=list)
+
+
+def _quantile_index(n: int, p: float) -> int:
+    k = math.ceil(float(n) * p - 1e-9) - 1.0
+    return int(min(max(k, 0.0), float(n - 1)))
+
+
+def _run_batch(s: ScenarioEstimates, evaluation: List[int], chosen: List[int], batch: int, max_inner: int, budget: int,
+               seed: int, inner: InnerBatches) -> int:
+    """One inner batch for each chosen scenario that fits in the budget (adaptive_nested.cpp:541-573), all of the
+    round's jobs handed to the simulator at once."""
+    jobs, total = [], 0
+    for i in chosen:
+        used = s.inner_paths(i)
+        m = 0 if used >= max_inner else min(batch, max_inner - used)
+        if m == 0:
+            continue
+        if total + m > budget:
+            break
+        jobs.append((i, m, derive_seed(seed, evaluation[i], s.batches[i], ADAPTIVE_TAG)))
+        total += m
+    if jobs:
+        outs = inner([(evaluation[i], sd, m) for i, m, sd in jobs])
+        for (i, m, _), out in zip(jobs, outs):
+            s.add_inner_batch(i, np.asarray(out, np.float64)[:m])
+    return total
+
+
+def _candidates(s: ScenarioEstimates, statistics, outside: List[bool], o: AdaptiveOptions) -> Tuple[List[int], int]:
+    """The scenarios to refine this round (adaptive_nested.cpp:578-625)."""
+    n = s.size()
+    queues, wanted, capped = [], [False] * n, 0
+    for st in statistics:
+        urgency = [0.0] * n
+        st.urgency(s, urgency)
+        keyed = []
+        for i in range(n):
+            if not (urgency[i] > 1.0):
+                continue
+            if s.inner_paths(i) >= o.max_inner_per_scenario:
+                if not wanted[i]:
+                    capped += 1
+                wanted[i] = True
+                continue
+            keyed.append((urgency[i], i))
+        keyed = sorted(keyed, key=lambda k: -k[0])  # stable, descending
+        queues.append([k[1] for k in keyed])
+    out, taken = [], [False] * n
+    if o.refine_outside_training_range:
+        for i in range(n):
+            if len(out) >= o.max_scenarios_per_round:
+                break
+            if outside[i] and s.inner_paths(i) < o.min_inner_for_variance:
+                out.append(i)
+                taken[i] = True
+    depth = 0
+    while len(out) < o.max_scenarios_per_round:
+        anyq = False
+        for q in queues:
+            if depth >= len(q):
+                continue
+            anyq = True
+            i = q[depth]
+            if not taken[i] and len(out) < o.max_scenarios_per_round:
+                out.append(i)
+                taken[i] = True
+        if not anyq:
+            break
+        depth += 1
+    return out, capped
+
+
+def estimate_adaptive(features: np.ndarray, payoff: Sequence[float], weight: Optional[Sequence[float]], inner: InnerBatches,
+                      statistics: Sequence, o: AdaptiveOptions) -> AdaptiveResult:
+    """estimateAdaptive (adaptive_nested.cpp:629-767): features [n][dims] of the outer scenarios' states, their own
+    discounted payoffs, optional weights, the inner simulator and the statistics refined jointly."""
+    o.validate()
+    F = np.asarray(features, np.float64)
+    n = len(payoff)
+    if F.shape[0] != n:
+        raise ValueError("estimateAdaptive: features and payoffs differ in length")
+    if weight is not None and len(weight) and len(weight) != n:
+        raise ValueError("estimateAdaptive: weights differ in length")
+    if not statistics:
+        raise ValueError("estimateAdaptive: no statistic")
+    n_train = int(math.floor(float(n) * o.training_fraction + 0.5))
+    if n_train < 2 or n - n_train < 1:
+        raise ValueError("estimateAdaptive: too few outer scenarios for the split")
+    order = list(range(n))
+    shuffle(order, derive_seed(o.seed, SPLIT_TAG))
+    r = AdaptiveResult()
+    r.training = sorted(order[:n_train])
+    r.evaluation = sorted(order[n_train:])
+    n_eval = len(r.evaluation)
+
+    proxy = HermiteProxy(o.hermite_degree)
+    proxy.fit(F, payoff, r.training)
+    r.proxy_degree, r.proxy_basis = proxy.degree(), proxy.num_basis()
+    mu_a, var_a = proxy.predict_rows(F[r.evaluation])
+    mu, est_var = [float(v) for v in mu_a], [float(v) for v in var_a]
+    w_all = None if weight is None or len(weight) == 0 else [float(v) for v in weight]
+    wts = [1.0 if w_all is None else w_all[i] for i in r.evaluation]
+    pay = [float(payoff[i]) for i in r.evaluation]
+
+    srt = sorted(mu)
+    thresholds = [srt[_quantile_index(n_eval, p)] for p in o.bin_probabilities]
+    nb = len(thresholds) + 1
+    bins = [bisect.bisect_left(thresholds, v) for v in mu]
+    rsum, rcount, rtotal = [0.0] * nb, [0] * nb, 0.0
+    fitted_t, _ = proxy.predict_rows(F[r.training])
+    for k, i in enumerate(r.training):
+        fitted = float(fitted_t[k])
+        e2 = (float(payoff[i]) - fitted) * (float(payoff[i]) - fitted)
+        b = bisect.bisect_left(thresholds, fitted)
+        rsum[b] += e2
+        rcount[b] += 1
+        rtotal += e2
+    rglobal = rtotal / float(n_train)
+    rvar = [rsum[b] / float(rcount[b]) if rcount[b] >= 2 else rglobal for b in range(nb)]
+
+    s = ScenarioEstimates(pay, wts, mu, est_var, bins, rvar, o.min_inner_for_variance, o.max_inner_per_scenario)
+    for st in statistics:
+        r.names.append(st.name())
+        r.baseline.append(st.evaluate(s))
+        r.regression.append(st.plug_in(mu, wts))
+    r.proxy = mu
+
+    dims = F.shape[1]
+    lo = [math.inf] * dims
+    hi = [-math.inf] * dims
+    for i in r.training:
+        for j in range(dims):
+            lo[j] = min(lo[j], F[i, j])
+            hi[j] = max(hi[j], F[i, j])
+    outside = [any(F[i, j] < lo[j] or F[i, j] > hi[j] for j in range(dims)) for i in r.evaluation]
+
+    audit_batch = max(o.inner_batch, o.min_inner_for_variance)
+    audit_per_bin = min(o.audit_per_bin, max(2, o.inner_budget // 5 // (nb * audit_batch)))
+    audit: List[int] = []
+    if o.audit_per_bin > 0:
+        members: List[List[int]] = [[] for _ in range(nb)]
+        for k in range(n_eval):
+            members[bins[k]].append(k)
+        for b in range(nb):
+            shuffle(members[b], derive_seed(o.seed, SPLIT_TAG, b + 1))
+            audit += members[b][:min(audit_per_bin, len(members[b]))]
+    used = _run_batch(s, r.evaluation, audit, audit_batch, o.max_inner_per_scenario, o.inner_budget, o.seed, inner)
+    r.audit_inner_paths = used
+    s.update_misspecification(o.min_per_bin_for_misspecification)
+
+    while True:
+        if r.rounds >= o.max_rounds:
+            r.stop = "max rounds"
+            break
+        chosen, capped = _candidates(s, statistics, outside, o)
+        if not chosen:
+            r.stop = "scenario caps" if capped > 0 else "converged"
+            break
+        spent = _run_batch(s, r.evaluation, chosen, o.inner_batch, o.max_inner_per_scenario, o.inner_budget - used, o.seed, inner)
+        if spent == 0:
+            r.stop = "budget"
+            break
+        used += spent
+        r.rounds += 1
+        s.update_misspecification(o.min_per_bin_for_misspecification)
+    chosen, capped = _candidates(s, statistics, outside, o)
+    r.unresolved = len(chosen) + capped
+
+    for st in statistics:
+        r.estimate.append(st.evaluate(s))
+    r.inner_paths = used
+    per_bin, refined_bin = [0] * nb, [0] * nb
+    for k in range(n_eval):
+        r.value.append(s.estimate(k))
+        r.inner.append(s.inner_paths(k))
+        per_bin[bins[k]] += 1
+        if r.inner[k] > 0:
+            r.refined_scenarios += 1
+            refined_bin[bins[k]] += 1
+    r.audited_scenarios = sum(1 for k in audit if s.inner_paths(k) > 0)
+    for b in range(nb):
+        r.bins.append({"lower_probability": 0.0 if b == 0 else o.bin_probabilities[b - 1],
+                       "upper_probability": 1.0 if b + 1 == nb else o.bin_probabilities[b],
+                       "scenarios": per_bin[b], "refined": refined_bin[b], "residual_std_dev": math.sqrt(s.residual[b]),
+                       "bias_shift": s.shift[b], "bias_rms": math.sqrt(s.misspec[b])})
+    return r
+
+
+@dataclass
+class UniformResult:
+    estimate: List[float]
+    value: List[float]
+    inner_paths: int
+
+
+def estimate_uniform(weight: Optional[Sequence[float]], inner: InnerBatches, scenarios: Sequence[int], inner_per_scenario: int,
+                     statistics: Sequence, seed: int) -> UniformResult:
+    """estimateUniform (adaptive_nested.cpp:769-790): the classical nest with the same inner paths per scenario."""
+    if inner_per_scenario < 1:
+        raise ValueError("estimateUniform: at least one inner path per scenario")
+    outs = inner([(int(sc), derive_seed(seed, int(sc), 0, UNIFORM_TAG), inner_per_scenario) for sc in scenarios])
+    value = [_seq_sum(np.asarray(o, np.float64)[:inner_per_scenario]) / float(inner_per_scenario) for o in outs]
+    w = [1.0] * len(scenarios)
+    if weight is not None and len(weight):
+        w = [float(weight[sc]) for sc in scenarios]
+    return UniformResult([st.plug_in(value, w) for st in statistics], value, len(scenarios) * inner_per_scenario)
+
+
+def per_scenario(simulate: Callable[[int, int, np.ndarray], None]) -> InnerBatches:
+    """Adapts a per-scenario simulator simulate(scenario, seed, out) -- the reference's InnerSimulator shape -- to
+    the batch interface."""
+    def run(jobs):
+        outs = []
+        for sc, seed, m in jobs:
+            out = np.zeros(m)
+            simulate(sc, seed, out)
+            outs.append(out)
+        return outs
+    return run
