@@ -128,6 +128,34 @@ zk_status zk_run_plan_f64(zk_context* ctx, const zk_plan_view_f64* plan, const d
 zk_status zk_run_plan_injected(zk_context* ctx, const zk_plan_view* plan, const double* normals, size_t streams,
                                zk_output* out, float* rows);
 
+/* The simulated risk factors of a plan in the FP64 mode (normals as in zk_run_plan_f64; nullable): out
+ * [2 + nA][nT][nP] = the Hull-White state x, the deflator D and every asset level S_a on every date and path. */
+zk_status zk_factor_paths_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams, double* out,
+                              size_t out_len);
+
+/* ---- nested exposure: the inner simulations (src/nested/nested_exposure.cpp:211-244 runs them on the CPU) ---- */
+/* The inner paths of one reporting date t of a netting set, on the GPU: from the outer scenarios' states at t,
+ * exact Hull-White and lognormal steps (FP64) to every later event date, coupons and terminal flows
+ * discounted to t, the normals of the reference's CounterNormals.  model: the flat model of zk_compile;
+ * periods [n_periods][6] (ts, te, tau, amount = +-notional, fixed rate, slot: the swap whose running coupon
+ * the period uses, < 64); terminals [n_terminals][6] (asset, option, call, notional, strike, maturity);
+ * x [n_scenarios], spot [n_scenarios][nA] and known [n_scenarios][n_slots] (the fixing of each slot's
+ * coupon running at t, 0 where none) the outer states at t. */
+typedef struct zk_nest zk_nest;
+zk_status zk_nest_create(zk_context* ctx, const double* model, size_t model_len, const double* periods, size_t n_periods,
+                         const double* terminals, size_t n_terminals, double t, const double* x, const double* spot,
+                         const double* known, size_t n_slots, size_t n_scenarios, zk_nest** out);
+/* One round of jobs: job k runs paths[k] inner paths of scenario[k] on the normal stream seed[k] (inner path q
+ * from normal q x events x (nA + 2)); out receives the payoffs job after job (sum of paths values). */
+zk_status zk_nest_run(zk_nest* nest, const uint64_t* scenario, const uint64_t* seed, const uint64_t* paths, size_t num_jobs,
+                      double* out);
+/* The zero-bond coefficients of the model's Hull-White curve: P(ts, te | x) = ratio exp(c - B x) for each pair
+ * (ts, te) of ts_te [n][2]; out [n][3] = ratio, c, B (hull_white.cpp:27-31). */
+zk_status zk_zero_bond_coefficients(const double* model, size_t model_len, const double* ts_te, size_t n, double* out);
+/* The number of event dates after t (0: nothing is paid after t). */
+zk_status zk_nest_events(const zk_nest* nest, uint64_t* events);
+void zk_nest_destroy(zk_nest* nest);
+
 /* ---- without device allocation (no counterpart in the reference) ----------------------------------- */
 /* For callers that cannot call cudaMalloc: a host that hands all device memory to its own pooling
  * allocator up front (a serving process, a framework's caching allocator), or a plug-in that runs

@@ -86,6 +86,11 @@ def lib() -> C.CDLL:
         L.ref_estimate_uniform.restype = C.c_int
         L.ref_estimate_uniform.argtypes = [vp, sz, INNER_FN, vp, vp, sz, sz, C.c_double, C.c_double, C.c_double, C.c_uint64, _dp,
                                            C.c_char_p, sz]
+        L.ref_normal_stream.restype = None
+        L.ref_normal_stream.argtypes = [C.c_uint64, sz, _dp]
+        L.ref_nested_exposure.restype = C.c_int64
+        L.ref_nested_exposure.argtypes = [_dp, sz, _dp, sz, _dp, sz, C.c_double, _dp, sz, C.c_uint64, C.c_int, vp, sz,
+                                          C.c_char_p, sz]
         L.ref_counter_normal.restype = C.c_double
         L.ref_counter_normal.argtypes = [C.c_uint64, sz]
         L.ref_derive_seed.restype = C.c_uint64
@@ -497,6 +502,31 @@ def estimate_uniform(weight, n: int, simulate, scenarios, per_scenario: int, ee_
                                   per_scenario, ee_rel, ee_abs, q, int(seed), out, e, 512):
         raise ValueError(e.value.decode())
     return out
+
+
+def normal_stream(seed: int, n: int) -> np.ndarray:
+    """The first n normals of the reference's NormalGenerator(seed) (mt19937_64, normal_distribution)."""
+    out = np.zeros(n)
+    lib().ref_normal_stream(seed, n, out)
+    return out
+
+
+NESTED_POINT_FIELDS = ("time", "ee_exact", "pfe_exact", "ee_regression", "pfe_regression", "ee_uniform", "pfe_uniform",
+                       "ee_adaptive", "pfe_adaptive", "evaluated", "inner_paths", "audit_inner_paths", "refined", "rounds",
+                       "uniform_inner_per_scenario", "live")
+
+
+def nested_exposure(model: np.ndarray, ns: np.ndarray, reporting, pfe_quantile: float, adaptive, uniform: bool = True):
+    """nested::nestedExposure on the reference's own outer simulation: one dict per reporting point."""
+    m, n, t = (np.ascontiguousarray(a, np.float64) for a in (model, ns, reporting))
+    opts = _adaptive_opts(adaptive)
+    e = _err()
+    out = np.zeros(16 * (len(t) + 1))
+    k = lib().ref_nested_exposure(m, m.size, n, n.size, t, t.size, pfe_quantile, opts, opts.size, int(adaptive.seed),
+                                  int(uniform), out.ctypes.data, out.size, e, 512)
+    if k < 0:
+        raise ValueError(e.value.decode())
+    return [dict(zip(NESTED_POINT_FIELDS, out[16 * i:16 * (i + 1)].tolist())) for i in range(k)]
 
 
 def counter_normal(seed: int, m: int) -> float:

@@ -25,6 +25,7 @@
 
 #include "ccr/core/math.hpp"
 #include "ccr/core/parallel.hpp"
+#include "ccr/core/random.hpp"
 #include "ccr/cva/cva.hpp"
 #include "ccr/exposure/allocation.hpp"
 #include "ccr/xva/xva.hpp"
@@ -686,6 +687,47 @@ double ref_counter_normal(std::uint64_t seed, std::size_t m) {
   return v;
 }
 std::uint64_t ref_derive_seed(std::uint64_t seed, std::uint64_t a, std::uint64_t b, std::uint64_t c) { return nested::deriveSeed(seed, a, b, c); }
+
+// ---- nested exposure (src/nested/nested_exposure.cpp) ----
+// The reference's own outer normals: the first n of NormalGenerator(seed), in the order generate() reads them.
+void ref_normal_stream(std::uint64_t seed, std::size_t n, double* out) {
+  NormalGenerator g(seed);
+  g.fill(out, n);
+}
+
+// nestedExposure on the model's generator and simulation (paths, seed, antithetic) and the reporting dates;
+// adaptive options as in ref_estimate_adaptive, seed passed apart.  out [nR][16]: time, EE* and PFE of the exact,
+// regression, uniform and adaptive estimates, evaluated, inner paths, audit inner paths, refined, rounds, uniform
+// inner paths per scenario, live.  Returns the number of points.
+std::int64_t ref_nested_exposure(const double* model, std::size_t nm, const double* ns, std::size_t nn, const double* reporting,
+                                 std::size_t nr, double pfeQuantile, const double* opts, std::size_t nOpts, std::uint64_t seed,
+                                 int uniform, double* out, std::size_t cap, char* err, std::size_t errlen) {
+  try {
+    const ModelSpec m = readModel(model, nm);
+    const NettingSet n = readNettingSet(ns, nn);
+    const ScenarioGenerator gen(m.hw, m.assets, m.credits, m.correlation);
+    nested::NestedExposureOptions o;
+    o.pfeQuantile = pfeQuantile;
+    o.adaptive = adaptiveOptions(opts, nOpts);
+    o.adaptive.seed = seed;
+    o.uniform = uniform != 0;
+    SpinPool pool(1);
+    const auto r = nested::nestedExposure(gen, n, TimeGrid(std::vector<double>(reporting, reporting + nr)), m.sim, o, pool);
+    std::size_t k = 0;
+    for (const auto& p : r.points)
+      for (double v : {p.time, p.eeExact, p.pfeExact, p.eeRegression, p.pfeRegression, p.eeUniform, p.pfeUniform, p.eeAdaptive,
+                       p.pfeAdaptive, static_cast<double>(p.evaluated), static_cast<double>(p.innerPaths),
+                       static_cast<double>(p.auditInnerPaths), static_cast<double>(p.refined), static_cast<double>(p.rounds),
+                       static_cast<double>(p.uniformInnerPerScenario), p.live ? 1.0 : 0.0}) {
+        if (k < cap) out[k] = v;
+        ++k;
+      }
+    return static_cast<std::int64_t>(r.points.size());
+  } catch (const std::exception& e) {
+    setError(err, errlen, e);
+    return -1;
+  }
+}
 
 // ------------------------------------------------------------------ FP64 engine
 // ExposureEngine::run (exposure_engine.cpp:50-81) on the reference's own normals (normals == nullptr) or

@@ -8,6 +8,7 @@ present.  Only tests/, the smoke check and bench.py's CPU-baseline leg may impor
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -239,3 +240,55 @@ def bilateral_cva(times, dee, dene, cpty, own, rc: float, ro: float):
     lib().orc_bilateral_cva(f(times), f(dee), f(dene), len(times), f(cpty[0]), f(cpty[1]), len(cpty[0]), f(own[0]),
                             f(own[1]), len(own[0]), rc, ro, out)
     return float(out[0]), float(out[1])
+
+
+# ---- the reference's outer normals (src/models/scenario_generator.cpp:89 reads ccr::NormalGenerator) ----
+class Mt19937_64:
+    """std::mt19937_64 (the C++ standard's parameters)."""
+
+    def __init__(self, seed: int):
+        M = (1 << 64) - 1
+        self.mt = [seed & M]
+        for i in range(1, 312):
+            prev = self.mt[-1]
+            self.mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & M)
+        self.i = 312
+
+    def __call__(self) -> int:
+        M = (1 << 64) - 1
+        if self.i >= 312:
+            mt = self.mt
+            for k in range(312):
+                y = (mt[k] & 0xFFFFFFFF80000000) | (mt[(k + 1) % 312] & 0x7FFFFFFF)
+                mt[k] = mt[(k + 156) % 312] ^ (y >> 1) ^ (0xB5026F5AA96619E9 if y & 1 else 0)
+            self.i = 0
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & M
+
+
+def normal_stream(seed: int, n: int) -> np.ndarray:
+    """The first n draws of ccr::NormalGenerator(seed) (include/ccr/core/random.hpp): std::normal_distribution on
+    std::mt19937_64 as GCC's libstdc++ implements it (the image's compiler): the Marsaglia polar method on
+    generate_canonical<double, 53> (one 64-bit draw scaled by 2^-64), the y half returned first and the x half
+    kept for the next call."""
+    g = Mt19937_64(seed)
+    out = np.zeros(n)
+    k = 0
+    while k < n:
+        while True:
+            x = 2.0 * (float(g()) * 2.0 ** -64) - 1.0
+            y = 2.0 * (float(g()) * 2.0 ** -64) - 1.0
+            r2 = x * x + y * y
+            if not (r2 > 1.0 or r2 == 0.0):
+                break
+        mult = math.sqrt(-2.0 * math.log(r2) / r2)
+        out[k] = y * mult
+        if k + 1 < n:
+            out[k + 1] = x * mult
+        k += 2
+    return out

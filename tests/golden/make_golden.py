@@ -8,7 +8,10 @@ arrays, the tables the reference's gpu::compile produced for them, and what the 
                 quantile request, ccr::quantile of the reference's own exposure row at the plan's level
                 (the exact value the fused pipeline approximates);
   engine_*.npz  ExposureEngine::run (FP64) on injected normals drawn from numpy's PCG64 with a stored seed:
-                the exposure profile, pathwise CVA, and netted / collateral values on the reporting dates.
+                the exposure profile, pathwise CVA, and netted / collateral values on the reporting dates;
+  nested_*.npz  nested::nestedExposure on the reference's own outer normals (NormalGenerator, restated by
+                oracle/restated.py:normal_stream): per reporting date the exact, regression, uniform and adaptive
+                EE* and PFE with the inner-path counts.
 
 The tests read these files on machines without the reference (tests/test_oracle_pins.py).
 """
@@ -58,6 +61,15 @@ def engine_cases():
         yield f"engine_{'csa' if csa else 'plain'}", m, ns, 5 if csa else 6
 
 
+def nested_cases():
+    """nestedExposure of the reference (the adaptive nest, src/nested/) on its own outer simulation."""
+    from zlatko_b200 import nested as N
+
+    m, ns = gpu_setup(400, False)
+    o = N.AdaptiveOptions(inner_budget=150_000, max_rounds=20)
+    yield "nested_exposure", m, ns, [0.5, 1.0, 2.0, 3.5], 0.95, o
+
+
 def main() -> None:
     only = set(sys.argv[1:])  # fixture names to (re)generate; all when none are given
     if not ref.available():
@@ -80,6 +92,15 @@ def main() -> None:
                             rows_total=r.rows_total, num_outputs=r.num_outputs, times=r.times,
                             reporting=r.reporting.astype(np.int64), sums=sums, values=values, exact_quantiles=exact)
         print(name, r.num_dates, "dates", r.stats_per_date, "stats", len(r.requests) // 8, "requests")
+    for name, m, ns, reporting, q, o in nested_cases():
+        if only and name not in only:
+            continue
+        em, en = S.encode_model(m), S.encode_netting_set(ns)
+        pts = ref.nested_exposure(em, en, reporting, q, o, True)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), model=em, netting_set=en, reporting=np.array(reporting),
+                            pfe_quantile=q, adaptive=ref._adaptive_opts(o), seed=o.seed,
+                            points=np.array([[p[k] for k in ref.NESTED_POINT_FIELDS] for p in pts]))
+        print(name, len(pts), "points")
     for name, m, ns, seed in engine_cases():
         if only and name not in only:
             continue

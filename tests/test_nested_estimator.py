@@ -84,3 +84,11 @@ def test_options_are_validated_like_the_reference():
         N.PositivePart(0.0, 0.0)
     with pytest.raises(ValueError):
         N.Quantile(1.0)
+
+
+@needs_ref
+def test_outer_normals_are_the_reference_normal_generator():
+    from oracle import restated
+
+    for seed in (42, 7, 20261203):
+        assert np.array_equal(restated.normal_stream(seed, 3001), ref.normal_stream(seed, 3001))

@@ -69,7 +69,8 @@ EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last
            "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
            "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params",
            "zk_surrogate_features", "zk_surrogate_book", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
-           "zk_plan_destroy"]
+           "zk_plan_destroy", "zk_factor_paths_f64", "zk_nest_create", "zk_nest_run", "zk_nest_events", "zk_nest_destroy",
+           "zk_zero_bond_coefficients"]
 
 _lib: Optional[C.CDLL] = None
 
@@ -113,6 +114,12 @@ def lib() -> C.CDLL:
         "zk_batch_create": (st, [vp, P(PlanView), sz, P(vp)]),
         "zk_batch_execute": (st, [vp]),
         "zk_batch_set_tile_paths": (st, [vp, C.c_uint64]),
+        "zk_factor_paths_f64": (st, [vp, P(PlanViewF64), vp, sz, vp, sz]),
+        "zk_nest_create": (st, [vp, vp, sz, vp, sz, vp, sz, C.c_double, vp, vp, vp, sz, sz, P(vp)]),
+        "zk_nest_run": (st, [vp, vp, vp, vp, sz, vp]),
+        "zk_nest_events": (st, [vp, P(C.c_uint64)]),
+        "zk_nest_destroy": (None, [vp]),
+        "zk_zero_bond_coefficients": (st, [vp, sz, vp, sz, vp]),
         "zk_batch_timings": (st, [vp, P(C.c_float)]),
         "zk_batch_read": (st, [vp, P(Output)]),
         "zk_batch_info_get": (st, [vp, P(BatchInfo)]),

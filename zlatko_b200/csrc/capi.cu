@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/zlatko_b200.h"
+#include "plan_compiler.h"
 #include "surrogate.cuh"
 #include "zk_kernels.h"
 
@@ -1362,6 +1363,26 @@ zk_status zk_run_plan_injected(zk_context* ctx, const zk_plan_view* plan, const 
   return runInjected<float>(ctx, plan, normals, streams, out, rows);
 }
 
+zk_status zk_factor_paths_f64(zk_context* ctx, const zk_plan_view_f64* plan, const double* normals, size_t streams, double* out,
+                              size_t out_len) {
+  try {
+    requireCtx(ctx);
+    if (!plan || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    auto B = build<double>(ctx, {viewOf(*plan)}, false, normals, streams);
+    const auto& L = B->launches.front();
+    const size_t n = static_cast<size_t>(2 + L.sc.nA) * L.sc.nT * L.sc.nP;
+    if (out_len != n) throw fail(ZK_ERR_INVALID_ARGUMENT, "out must hold (2 + nA) nT nP = %zu values", n);
+    upload(*B, ctx, true, normals, streams);
+    ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
+    ZK_CUDA(launchSimulate<double>(L.sc, L.cb, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(out, B->base + L.cubeOff, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
 // ---- device-resident batches ----
 zk_status zk_batch_create(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_batch** out) {
   try {
@@ -1562,4 +1583,149 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
   } catch (const std::exception& e) {
     return report(fail(ZK_ERR_CUDA, "%s", e.what()));
   }
+}
+
+// ---- nested exposure: inner paths on the GPU ----
+struct zk_nest {
+  zk_context* ctx = nullptr;
+  unsigned char* dmem = nullptr;  // the program and the outer states
+  NestArgs args{};
+  size_t numScenarios = 0;
+  unsigned char* djobs = nullptr;  // a round's jobs and payoffs, grown on demand
+  size_t jobsBytes = 0;
+  ~zk_nest() {
+    if (dmem) cudaFree(dmem);
+    if (djobs) cudaFree(djobs);
+  }
+};
+
+zk_status zk_nest_create(zk_context* ctx, const double* model, size_t model_len, const double* periods, size_t n_periods,
+                         const double* terminals, size_t n_terminals, double t, const double* x, const double* spot,
+                         const double* known, size_t n_slots, size_t n_scenarios, zk_nest** out) {
+  try {
+    requireCtx(ctx);
+    if (!model || !x || !out || (n_periods && !periods) || (n_terminals && !terminals)) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (n_scenarios == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "no scenarios");
+    if (n_slots > kMaxNestSlots) throw fail(ZK_ERR_UNSUPPORTED, "at most %u swaps with a running coupon", kMaxNestSlots);
+    zk::host::Model m;
+    zk::host::NestProgram P;
+    try {
+      m = zk::host::decodeModel(model, model_len);
+      P = zk::host::nestProgram(m, periods, n_periods, terminals, n_terminals, t);
+    } catch (const std::exception& e) {
+      throw fail(ZK_ERR_INVALID_ARGUMENT, "%s", e.what());
+    }
+    const uint32_t nA = static_cast<uint32_t>(P.nA);
+    if (nA > 0 && !spot) throw fail(ZK_ERR_INVALID_ARGUMENT, "null spot");
+    if (n_slots > 0 && !known) throw fail(ZK_ERR_INVALID_ARGUMENT, "null known fixings");
+    for (size_t i = 0; i < n_periods; ++i)
+      if (!(periods[6 * i + 5] >= 0.0) || periods[6 * i + 5] >= static_cast<double>(n_slots) || !(periods[6 * i + 2] > 0.0))
+        throw fail(ZK_ERR_INVALID_ARGUMENT, "period %zu: slot beyond n_slots or non-positive accrual", i);
+    for (size_t f = 0; f < n_terminals; ++f)
+      if (!(terminals[6 * f] >= 0.0) || terminals[6 * f] >= static_cast<double>(nA))
+        throw fail(ZK_ERR_INVALID_ARGUMENT, "terminal flow %zu: asset beyond the model's assets", f);
+    auto N = std::make_unique<zk_nest>();
+    N->ctx = ctx, N->numScenarios = n_scenarios;
+    // One device block: coef | opBegin | ops | periods | terminals | chol | fixToday | x0 | spot0 | fix0.
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off = alignUp(off + std::max<size_t>(bytes, 16)); return o; };
+    const size_t oCoef = take(P.coef.size() * 8), oBegin = take(P.begin.size() * 4), oOps = take(P.ops.size() * 4);
+    const size_t oPer = take(P.periods.size() * 8), oTerm = take(P.terminals.size() * 8), oChol = take(P.chol.size() * 8);
+    const size_t oToday = take(P.fixToday.size() * 4), oX = take(n_scenarios * 8), oSpot = take(n_scenarios * nA * 8);
+    const size_t oFix = take(n_scenarios * n_slots * 8);
+    std::vector<unsigned char> img(off, 0);
+    auto put = [&](size_t o, const void* src, size_t bytes) { if (bytes) std::memcpy(img.data() + o, src, bytes); };
+    put(oCoef, P.coef.data(), P.coef.size() * 8), put(oBegin, P.begin.data(), P.begin.size() * 4);
+    put(oOps, P.ops.data(), P.ops.size() * 4), put(oPer, P.periods.data(), P.periods.size() * 8);
+    put(oTerm, P.terminals.data(), P.terminals.size() * 8), put(oChol, P.chol.data(), P.chol.size() * 8);
+    put(oToday, P.fixToday.data(), P.fixToday.size() * 4), put(oX, x, n_scenarios * 8);
+    put(oSpot, spot, n_scenarios * nA * 8), put(oFix, known, n_scenarios * n_slots * 8);
+    ZK_CUDA(cudaMalloc(reinterpret_cast<void**>(&N->dmem), off));
+    ZK_CUDA(cudaMemcpyAsync(N->dmem, img.data(), off, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    unsigned char* b = N->dmem;
+    NestArgs& A = N->args;
+    A.coef = reinterpret_cast<const double*>(b + oCoef), A.opBegin = reinterpret_cast<const uint32_t*>(b + oBegin);
+    A.ops = reinterpret_cast<const uint32_t*>(b + oOps), A.periods = reinterpret_cast<const double*>(b + oPer);
+    A.terminals = reinterpret_cast<const double*>(b + oTerm), A.chol = reinterpret_cast<const double*>(b + oChol);
+    A.fixToday = reinterpret_cast<const uint32_t*>(b + oToday), A.x0 = reinterpret_cast<const double*>(b + oX);
+    A.spot0 = reinterpret_cast<const double*>(b + oSpot), A.fix0 = reinterpret_cast<const double*>(b + oFix);
+    A.numEvents = static_cast<uint32_t>(P.times.size()), A.nA = nA, A.numSlots = static_cast<uint32_t>(n_slots);
+    A.numFixToday = static_cast<uint32_t>(P.fixToday.size());
+    *out = N.release();
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_nest_run(zk_nest* nest, const uint64_t* scenario, const uint64_t* seed, const uint64_t* paths, size_t num_jobs, double* out) {
+  if (!nest) return ZK_ERR_INVALID_ARGUMENT;
+  zk_context* ctx = nest->ctx;
+  try {
+    requireCtx(ctx);
+    if (num_jobs == 0) return ZK_OK;
+    if (!scenario || !seed || !paths || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    if (num_jobs > 0xFFFFFFFFull) throw fail(ZK_ERR_INVALID_ARGUMENT, "too many jobs");
+    std::vector<unsigned long long> start(num_jobs);
+    unsigned long long total = 0;
+    for (size_t k = 0; k < num_jobs; ++k) {
+      if (scenario[k] >= nest->numScenarios) throw fail(ZK_ERR_INVALID_ARGUMENT, "job %zu: scenario beyond the outer sample", k);
+      start[k] = total;
+      total += paths[k];
+    }
+    if (total == 0) return ZK_OK;
+    const size_t jobBytes = alignUp(num_jobs * 8);
+    const size_t need = 3 * jobBytes + total * 8;
+    if (nest->jobsBytes < need) {
+      if (nest->djobs) cudaFree(nest->djobs);
+      nest->djobs = nullptr, nest->jobsBytes = 0;
+      ZK_CUDA(cudaMalloc(reinterpret_cast<void**>(&nest->djobs), need));
+      nest->jobsBytes = need;
+    }
+    unsigned char* d = nest->djobs;
+    ZK_CUDA(cudaMemcpyAsync(d, scenario, num_jobs * 8, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(d + jobBytes, seed, num_jobs * 8, cudaMemcpyHostToDevice, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(d + 2 * jobBytes, start.data(), num_jobs * 8, cudaMemcpyHostToDevice, ctx->stream));
+    NestArgs A = nest->args;
+    A.jobScenario = reinterpret_cast<const unsigned long long*>(d);
+    A.jobSeed = reinterpret_cast<const unsigned long long*>(d + jobBytes);
+    A.jobStart = reinterpret_cast<const unsigned long long*>(d + 2 * jobBytes);
+    A.out = reinterpret_cast<double*>(d + 3 * jobBytes);
+    A.totalPaths = total, A.numJobs = static_cast<uint32_t>(num_jobs);
+    ZK_CUDA(launchNestInner(A, ctx->stream));
+    ZK_CUDA(cudaMemcpyAsync(out, A.out, total * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ZK_OK;
+  } catch (const Failure& f) {
+    return record(ctx, f);
+  }
+}
+
+zk_status zk_zero_bond_coefficients(const double* model, size_t model_len, const double* ts_te, size_t n, double* out) {
+  if (!model || (n && (!ts_te || !out))) return ZK_ERR_INVALID_ARGUMENT;
+  try {
+    const auto m = zk::host::decodeModel(model, model_len);
+    for (size_t i = 0; i < n; ++i) {
+      const double ts = ts_te[2 * i], te = ts_te[2 * i + 1];
+      out[3 * i] = m.hw.curve.discount(te) / m.hw.curve.discount(ts);
+      out[3 * i + 1] = 0.5 * (m.hw.V(ts, te) - m.hw.V(0.0, te) + m.hw.V(0.0, ts));
+      out[3 * i + 2] = m.hw.B(ts, te);
+    }
+    return ZK_OK;
+  } catch (const std::exception&) {
+    return ZK_ERR_INVALID_ARGUMENT;
+  }
+}
+
+zk_status zk_nest_events(const zk_nest* nest, uint64_t* events) {
+  if (!nest || !events) return ZK_ERR_INVALID_ARGUMENT;
+  *events = nest->args.numEvents;
+  return ZK_OK;
+}
+
+void zk_nest_destroy(zk_nest* nest) {
+  if (!nest) return;
+  cudaSetDevice(nest->ctx->device);
+  delete nest;
 }

@@ -392,6 +392,108 @@ std::uint32_t floatBits(float f) {
 
 }  // namespace
 
+// The exact step from t0 to t1 of the Hull-White state and its integral (hull_white.cpp:40-68) and of every
+// lognormal asset (lognormal_asset.cpp:17-22), as one row of the step table: [0] e^{-a dt}, [1] sd of x,
+// [2] [3] the integral's loadings on the x and independent normals, [4] the integral of the shift, [5]
+// (1 - e^{-a dt}) / a, [6] dt, [8 + k] the log carry ratio, [12 + k] vol sqrt(dt), [16 + k] vol^2 dt / 2, [20 + c]
+// the CIR++ shift integrated to t1.
+void stepRow(const Model& m, double t0, double t1, double* row) {
+  const HullWhite& hw = m.hw;
+  const double a = hw.a, sigma = hw.sigma;
+  const double dt = t1 - t0, e = std::exp(-a * dt), s2 = sigma * sigma;
+  const double varX = s2 * (1 - e * e) / (2 * a);
+  const double varI = s2 / (a * a) * (dt - 2 * (1 - e) / a + (1 - e * e) / (2 * a));
+  const double cov = s2 / (2 * a * a) * (1 - e) * (1 - e);
+  const double sdX = std::sqrt(varX), c1 = sdX > 0 ? cov / sdX : 0.0, c2 = std::sqrt(std::max(varI - c1 * c1, 0.0));
+  const double g2 = dt - 2 / a * (std::exp(-a * t0) - std::exp(-a * t1)) + 0.5 / a * (std::exp(-2 * a * t0) - std::exp(-2 * a * t1));
+  row[0] = e, row[1] = sdX, row[2] = c1, row[3] = c2;
+  row[4] = std::log(hw.curve.discount(t0) / hw.curve.discount(t1)) + s2 / (2 * a * a) * g2;
+  row[5] = (1 - e) / a, row[6] = dt;
+  for (std::size_t k = 0; k < m.assets.size(); ++k) {
+    const Asset& s = m.assets[k];
+    row[8 + k] = std::log(s.carry.discount(t0) / s.carry.discount(t1));
+    row[12 + k] = s.vol * std::sqrt(dt);
+    row[16 + k] = 0.5 * s.vol * s.vol * dt;
+  }
+  for (std::size_t c = 0; c < m.credits.size(); ++c) row[20 + c] = m.credits[c].integratedShift(t1);
+}
+
+NestProgram nestProgram(const Model& m, const double* periods, std::size_t nPer, const double* terminals, std::size_t nTerm, double t) {
+  constexpr double kEps = 1e-10;  // the trades' tolerance for "on or before t" (nested_exposure.cpp:19)
+  NestProgram P;
+  P.nA = m.assets.size();
+  // Event dates after t (nested_exposure.cpp:87-117): fixings after t, payments and terminal flows after t.
+  std::vector<double> times;
+  for (std::size_t i = 0; i < nPer; ++i) {
+    const double* q = periods + 6 * i;
+    if (q[1] <= t + kEps) continue;
+    if (q[0] > t + kEps) times.push_back(q[0]);
+    times.push_back(q[1]);
+  }
+  for (std::size_t f = 0; f < nTerm; ++f)
+    if (terminals[6 * f + 5] > t + kEps) times.push_back(terminals[6 * f + 5]);
+  std::sort(times.begin(), times.end());
+  for (double u : times)
+    if (P.times.empty() || u > P.times.back() + 1e-9) P.times.push_back(u);
+  const std::size_t E = P.times.size();
+  auto at = [&](double u) {
+    for (std::size_t e = 0; e < E; ++e)
+      if (std::fabs(P.times[e] - u) <= 1e-9) return e;
+    throw std::logic_error("nested exposure: event date not in the program");
+  };
+  std::vector<std::vector<std::uint32_t>> pay(E), fix(E), term(E);
+  for (std::size_t i = 0; i < nPer; ++i) {
+    const double* q = periods + 6 * i;
+    if (q[1] <= t + kEps) continue;
+    if (q[0] > t + kEps) fix[at(q[0])].push_back(static_cast<std::uint32_t>(i));
+    else if (q[0] >= t - kEps) P.fixToday.push_back(static_cast<std::uint32_t>(i));  // fixed today, from x at t
+    pay[at(q[1])].push_back(static_cast<std::uint32_t>(i));
+  }
+  for (std::size_t f = 0; f < nTerm; ++f)
+    if (terminals[6 * f + 5] > t + kEps) term[at(terminals[6 * f + 5])].push_back(static_cast<std::uint32_t>(f));
+  // The step of every event from the previous one (t first), and the event's operations in the reference's
+  // order: payments, then fixings, then terminal flows.
+  P.coef.assign(E * kStepStride, 0.0);
+  P.begin.push_back(0);
+  double prev = t;
+  for (std::size_t e = 0; e < E; ++e) {
+    stepRow(m, prev, P.times[e], &P.coef[e * kStepStride]);
+    P.coef[e * kStepStride + 7] = m.hw.a;  // the inner step forms x (1 - e^{-a dt}) / a as the reference does
+    prev = P.times[e];
+    for (auto i : pay[e]) P.ops.push_back(i);
+    for (auto i : fix[e]) P.ops.push_back((1u << 28) | i);
+    for (auto f : term[e]) P.ops.push_back((2u << 28) | f);
+    P.begin.push_back(static_cast<std::uint32_t>(P.ops.size()));
+  }
+  // Periods: tau, amount, fixed rate, slot, and the zero bond P(ts, te | x) = ratio exp(c - B x) of the fixing
+  // (hull_white.cpp:27-31); terminal flows: asset, option, call, notional, strike.
+  P.periods.assign(nPer * 8, 0.0);
+  for (std::size_t i = 0; i < nPer; ++i) {
+    const double* q = periods + 6 * i;
+    double* r = &P.periods[8 * i];
+    const double ts = q[0], te = q[1];
+    r[0] = q[2], r[1] = q[3], r[2] = q[4], r[3] = q[5];
+    if (te > ts) {
+      r[4] = m.hw.curve.discount(te) / m.hw.curve.discount(ts);
+      r[5] = 0.5 * (m.hw.V(ts, te) - m.hw.V(0.0, te) + m.hw.V(0.0, ts));
+      r[6] = m.hw.B(ts, te);
+    }
+  }
+  P.terminals.assign(nTerm * 8, 0.0);
+  for (std::size_t f = 0; f < nTerm; ++f)
+    for (int k = 0; k < 5; ++k) P.terminals[8 * f + k] = terminals[6 * f + k];
+  // The first 1 + nA rows of the correlation's Cholesky factor (nested_exposure.cpp:136, 215-222).
+  const std::size_t F = m.numFactors(), r = 1 + P.nA;
+  std::vector<double> corr(F * F, 0.0);
+  for (std::size_t i = 0; i < F; ++i) corr[i * F + i] = 1.0;
+  if (!m.correlation.empty()) corr = m.correlation;
+  const std::vector<double> chol = cholesky(corr, F);
+  P.chol.assign(r * r, 0.0);
+  for (std::size_t i = 0; i < r; ++i)
+    for (std::size_t k = 0; k <= i; ++k) P.chol[i * r + k] = chol[i * F + k];
+  return P;
+}
+
 CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   Options eff = o;
   if (o.gross || o.tradeViews) eff.perTrade = true;
@@ -443,7 +545,6 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   const Grid grid(sim);
   const std::size_t nT = grid.t.size();
   const HullWhite& hw = m.hw;
-  const double a = hw.a, sigma = hw.sigma;
 
   CompiledPlan P;
   P.times = grid.t;
@@ -453,25 +554,7 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
 
   // ---- step coefficients (the exact transitions of hull_white.cpp:40-68 and lognormal_asset.cpp:17-22)
   P.steps.assign(nT * kStepStride, 0.0);
-  for (std::size_t j = 1; j < nT; ++j) {
-    const double t0 = grid.t[j - 1], t1 = grid.t[j], dt = t1 - t0, e = std::exp(-a * dt), s2 = sigma * sigma;
-    const double varX = s2 * (1 - e * e) / (2 * a);
-    const double varI = s2 / (a * a) * (dt - 2 * (1 - e) / a + (1 - e * e) / (2 * a));
-    const double cov = s2 / (2 * a * a) * (1 - e) * (1 - e);
-    const double sdX = std::sqrt(varX), c1 = sdX > 0 ? cov / sdX : 0.0, c2 = std::sqrt(std::max(varI - c1 * c1, 0.0));
-    const double g2 = dt - 2 / a * (std::exp(-a * t0) - std::exp(-a * t1)) + 0.5 / a * (std::exp(-2 * a * t0) - std::exp(-2 * a * t1));
-    double* row = &P.steps[j * kStepStride];
-    row[0] = e, row[1] = sdX, row[2] = c1, row[3] = c2;
-    row[4] = std::log(hw.curve.discount(t0) / hw.curve.discount(t1)) + s2 / (2 * a * a) * g2;
-    row[5] = (1 - e) / a, row[6] = dt;
-    for (std::size_t k = 0; k < m.assets.size(); ++k) {
-      const Asset& s = m.assets[k];
-      row[8 + k] = std::log(s.carry.discount(t0) / s.carry.discount(t1));
-      row[12 + k] = s.vol * std::sqrt(dt);
-      row[16 + k] = 0.5 * s.vol * s.vol * dt;
-    }
-    for (std::size_t c = 0; c < m.credits.size(); ++c) row[20 + c] = m.credits[c].integratedShift(t1);
-  }
+  for (std::size_t j = 1; j < nT; ++j) stepRow(m, grid.t[j - 1], grid.t[j], &P.steps[j * kStepStride]);
 
   // ---- valuation terms per date
   std::vector<std::vector<Term>> at(nT);

@@ -132,4 +132,26 @@ struct CompiledPlan {
 
 CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o);
 
+// One row of the step table: the exact transitions of the rate state, its integral and the assets from t0 to t1.
+void stepRow(const Model& m, double t0, double t1, double* row);
+
+// The inner paths of the nested exposure from date t (src/nested/nested_exposure.cpp:87-117, 211-244): the event
+// dates after t with each one's step from the previous date and its operations, the periods' and terminal flows'
+// constants, and the correlation rows of the rate and the assets.  periods are [nPer][6] (ts, te, tau, amount =
+// sign x notional, fixed rate, slot: the swap whose fixing the period uses), terminals [nTerm][6] (asset, option,
+// call, notional, strike, maturity).
+struct NestProgram {
+  std::size_t nA = 0;
+  std::vector<double> times;           // [E]
+  std::vector<double> coef;            // [E][24] step rows
+  std::vector<std::uint32_t> begin;    // [E + 1] into ops
+  std::vector<std::uint32_t> ops;      // kind << 28 | index: 0 payment, 1 fixing, 2 terminal flow
+  std::vector<std::uint32_t> fixToday; // periods that fix at t itself
+  std::vector<double> periods;         // [nPer][8]: tau, amount, fixed rate, slot, bond ratio, bond c, bond B, 0
+  std::vector<double> terminals;       // [nTerm][8]: asset, option, call, notional, strike
+  std::vector<double> chol;            // [(1 + nA)^2] lower
+};
+NestProgram nestProgram(const Model& m, const double* periods, std::size_t nPer, const double* terminals, std::size_t nTerm,
+                        double t);
+
 }  // namespace zk::host

@@ -40,6 +40,29 @@ struct ImArgs {
 template <typename R>
 cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream);
 
+// Inner paths of the nested exposure (nested_inner.cu) for one reporting date: the program of events after the
+// date (nestProgram in plan_compiler.cpp) and a round's jobs (scenario, seed, paths), one thread per inner path.
+constexpr uint32_t kMaxNestSlots = 64;  // swaps whose running coupon an inner path tracks
+struct NestArgs {
+  const double* coef;                 // [events][24] step rows, column 7 = a
+  const uint32_t* opBegin;            // [events + 1]
+  const uint32_t* ops;                // kind << 28 | index
+  const double* periods;              // [nPer][8]
+  const double* terminals;            // [nTerm][8]
+  const double* chol;                 // [(1 + nA)^2]
+  const uint32_t* fixToday;           // periods fixing at the date itself
+  const double* x0;                   // [scenarios] rate state at the date
+  const double* spot0;                // [scenarios][nA]
+  const double* fix0;                 // [scenarios][numSlots] fixings known at the date
+  const unsigned long long* jobScenario;
+  const unsigned long long* jobSeed;
+  const unsigned long long* jobStart;  // first inner path of each job (ascending)
+  double* out;                         // [totalPaths], job after job
+  unsigned long long totalPaths;
+  uint32_t numJobs, numEvents, nA, numSlots, numFixToday, pad;
+};
+cudaError_t launchNestInner(const NestArgs& M, cudaStream_t stream);
+
 // One reduce job per plan: sums[i] = (sum over the 128-path groups of the group's partials) / nP for i < n, the
 // partials [warp][i] being one per revalue warp of the tile shape ppt (32 ppt paths); numTiles counts the groups.
 template <typename R>

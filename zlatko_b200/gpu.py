@@ -333,6 +333,16 @@ class Context:
         sums, values = bufs[0]
         return (sums, values, r.reshape(plan.rows_total, plan.num_paths)) if rows else (sums, values)
 
+    def factor_paths_f64(self, plan: Plan, normals: Optional[np.ndarray] = None, streams: int = 0) -> np.ndarray:
+        """zk_factor_paths_f64: [2 + nA][nT][nP] = x, D and every asset level on every date and path (FP64)."""
+        v = plan.view64()
+        nA = int(plan.header[2])
+        out = np.zeros((2 + nA) * plan.num_dates * plan.num_paths)
+        z = None if normals is None else np.ascontiguousarray(normals, np.float64)
+        check(lib().zk_factor_paths_f64(self.handle, C.byref(v), None if z is None else z.ctypes.data, streams,
+                                        out.ctypes.data, out.size), self.handle)
+        return out.reshape(2 + nA, plan.num_dates, plan.num_paths)
+
     def run_injected(self, plan: Plan, normals: np.ndarray, streams: int, rows: bool = False):
         """FP32 kernels on injected normals (zk_run_plan_injected)."""
         v = plan.view()
