@@ -21,6 +21,7 @@ N > 1: replicas (the path runs on one GPU by design); every rank runs the worklo
 from __future__ import annotations
 
 import argparse
+from dataclasses import replace
 import json
 import os
 import subprocess
@@ -52,6 +53,8 @@ def parse():
     ap.add_argument("--no-amc", action="store_true", help="skip the Bermudan (AMC) leg")
     ap.add_argument("--amc-paths", type=int, default=200_000)
     ap.add_argument("--no-im", action="store_true", help="skip the nested initial-margin leg")
+    ap.add_argument("--no-nest", action="store_true", help="skip the adaptive nested-exposure leg")
+    ap.add_argument("--nest-paths", type=int, default=4000)
     ap.add_argument("--im-paths", type=int, default=20_000)
     return ap.parse_args()
 
@@ -334,6 +337,40 @@ def im_leg(ctx, a):
     return line
 
 
+def nest_leg(ctx, a):
+    """Exposure by the adaptive nest (the reference's defaults: 2M inner paths per date, 50 rounds) of 32 trades on
+    the correlated book's model, quarterly to 5y: the inner simulations on the GPU (one launch per round) and the
+    reference's nestedExposure on all host threads.  The two arms draw their own outer scenarios (the GPU's
+    counter-based normals, the reference's Mersenne twister), so they are compared by inner paths per second."""
+    from oracle import ref
+    from zlatko_b200 import nested_exposure as E
+    from zlatko_b200 import spec as S
+    from zlatko_b200 import workloads
+
+    m, _, _, _ = workloads.correlated_csa_book(a.nest_paths)
+    ns = workloads.nested_netting_set()
+    reporting = [q / 4.0 for q in range(1, 21)]
+    o = E.NestedExposureOptions()
+    E.nested_exposure(ctx, replace(m, num_paths=512), ns, reporting[:2], o)  # warm-up
+    t0 = time.perf_counter()
+    res = E.nested_exposure(ctx, m, ns, reporting, o)
+    gpu_s = time.perf_counter() - t0
+    line = {"workload": f"{len(ns.trades)} trades (20 swaps, 8 FX forwards, 4 FX options), {a.nest_paths} outer paths, "
+                        f"{len(reporting)} quarterly dates, adaptive nest with the reference's defaults",
+            "wall_s": gpu_s, "inner_paths": res.inner_paths, "inner_launches": res.inner_launches,
+            "inner_paths_per_s": res.inner_paths / gpu_s}
+    if not a.no_cpu and ref.available():
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        pts = ref.nested_exposure(S.encode_model(m), S.encode_netting_set(ns), reporting, o.pfe_quantile, o.adaptive, True, threads)
+        cpu_s = time.perf_counter() - t0
+        inner = sum(p["inner_paths"] for p in pts)
+        line["cpu_baseline"] = {"value": inner / cpu_s, "unit": "inner paths/s", "cores": threads, "kind": "reference",
+                                "sample": f"the whole workload (nestedExposure, {threads} threads): {cpu_s:.2f} s, {int(inner)} inner paths"}
+        line["speedup_vs_cpu"] = line["inner_paths_per_s"] / line["cpu_baseline"]["value"]
+    return line
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -473,6 +510,8 @@ def main():
             line["amc"] = guarded(amc_leg, ctx, a)
         if not a.no_im:
             line["nested_im"] = guarded(im_leg, ctx, a)
+        if not a.no_nest:
+            line["adaptive_nest"] = guarded(nest_leg, ctx, a)
         print(json.dumps(line))
     batch.close()
     ctx.close()

@@ -89,7 +89,7 @@ def lib() -> C.CDLL:
         L.ref_normal_stream.restype = None
         L.ref_normal_stream.argtypes = [C.c_uint64, sz, _dp]
         L.ref_nested_exposure.restype = C.c_int64
-        L.ref_nested_exposure.argtypes = [_dp, sz, _dp, sz, _dp, sz, C.c_double, _dp, sz, C.c_uint64, C.c_int, vp, sz,
+        L.ref_nested_exposure.argtypes = [_dp, sz, _dp, sz, _dp, sz, C.c_double, _dp, sz, C.c_uint64, C.c_int, sz, vp, sz,
                                           C.c_char_p, sz]
         L.ref_counter_normal.restype = C.c_double
         L.ref_counter_normal.argtypes = [C.c_uint64, sz]
@@ -516,14 +516,16 @@ NESTED_POINT_FIELDS = ("time", "ee_exact", "pfe_exact", "ee_regression", "pfe_re
                        "uniform_inner_per_scenario", "live")
 
 
-def nested_exposure(model: np.ndarray, ns: np.ndarray, reporting, pfe_quantile: float, adaptive, uniform: bool = True):
-    """nested::nestedExposure on the reference's own outer simulation: one dict per reporting point."""
+def nested_exposure(model: np.ndarray, ns: np.ndarray, reporting, pfe_quantile: float, adaptive, uniform: bool = True,
+                    threads: int = 1):
+    """nested::nestedExposure on the reference's own outer simulation (on `threads` threads): one dict per
+    reporting point."""
     m, n, t = (np.ascontiguousarray(a, np.float64) for a in (model, ns, reporting))
     opts = _adaptive_opts(adaptive)
     e = _err()
     out = np.zeros(16 * (len(t) + 1))
     k = lib().ref_nested_exposure(m, m.size, n, n.size, t, t.size, pfe_quantile, opts, opts.size, int(adaptive.seed),
-                                  int(uniform), out.ctypes.data, out.size, e, 512)
+                                  int(uniform), threads, out.ctypes.data, out.size, e, 512)
     if k < 0:
         raise ValueError(e.value.decode())
     return [dict(zip(NESTED_POINT_FIELDS, out[16 * i:16 * (i + 1)].tolist())) for i in range(k)]

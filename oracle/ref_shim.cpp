@@ -695,13 +695,13 @@ void ref_normal_stream(std::uint64_t seed, std::size_t n, double* out) {
   g.fill(out, n);
 }
 
-// nestedExposure on the model's generator and simulation (paths, seed, antithetic) and the reporting dates;
-// adaptive options as in ref_estimate_adaptive, seed passed apart.  out [nR][16]: time, EE* and PFE of the exact,
+// nestedExposure on the model's generator and simulation (paths, seed, antithetic) and the reporting dates, on
+// `threads` pool threads; adaptive options as in ref_estimate_adaptive, seed passed apart.  out [nR][16]: time, EE* and PFE of the exact,
 // regression, uniform and adaptive estimates, evaluated, inner paths, audit inner paths, refined, rounds, uniform
 // inner paths per scenario, live.  Returns the number of points.
 std::int64_t ref_nested_exposure(const double* model, std::size_t nm, const double* ns, std::size_t nn, const double* reporting,
                                  std::size_t nr, double pfeQuantile, const double* opts, std::size_t nOpts, std::uint64_t seed,
-                                 int uniform, double* out, std::size_t cap, char* err, std::size_t errlen) {
+                                 int uniform, std::size_t threads, double* out, std::size_t cap, char* err, std::size_t errlen) {
   try {
     const ModelSpec m = readModel(model, nm);
     const NettingSet n = readNettingSet(ns, nn);
@@ -711,7 +711,7 @@ std::int64_t ref_nested_exposure(const double* model, std::size_t nm, const doub
     o.adaptive = adaptiveOptions(opts, nOpts);
     o.adaptive.seed = seed;
     o.uniform = uniform != 0;
-    SpinPool pool(1);
+    SpinPool pool(std::max<std::size_t>(threads, 1));
     const auto r = nested::nestedExposure(gen, n, TimeGrid(std::vector<double>(reporting, reporting + nr)), m.sim, o, pool);
     std::size_t k = 0;
     for (const auto& p : r.points)

@@ -5,7 +5,7 @@ Restates src/nested/adaptive_nested.cpp (the estimator: HermiteProxy, ScenarioEs
 Quantile statistics, estimateAdaptive, estimateUniform) in the reference's arithmetic order, so that on the same
 outer sample and the same inner payoffs it reaches the same decisions and estimates.  The estimator is host
 control logic; its inner simulations are the expensive part and run as batches: every round hands all its jobs
-(scenario, seed, paths) to the inner simulator at once, so a GPU simulator (nested_gpu.InnerPaths) runs a round
+(scenario, seed, paths) to the inner simulator at once, so a GPU simulator (nested_exposure.GpuInner) runs a round
 in one kernel launch where the reference calls a per-scenario callback on a thread pool.
 """
 from __future__ import annotations
@@ -280,26 +280,36 @@ def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int
     return count + n, mean, m2
 
 
+def _acc_sum(a) -> float:
+    """A left-to-right sum of an array (np.add.accumulate is sequential), the reference's loop order."""
+    a = np.asarray(a, np.float64)
+    return float(np.add.accumulate(a)[-1]) if a.size else 0.0
+
+
+def _erfc(a: np.ndarray) -> np.ndarray:
+    return np.array([math.erfc(v) for v in a.tolist()], np.float64)
+
+
 class ScenarioEstimates:
     """What is known about every evaluation scenario: proxy value and uncertainty, bin, and inner samples in two
-    folds (adaptive_nested.cpp:279-437)."""
+    folds (adaptive_nested.cpp:279-437).  The per-scenario quantities are computed for all scenarios at once with
+    element-wise IEEE operations in the reference's order, so they carry the reference's bits."""
 
     def __init__(self, outer_payoff, weight, proxy_mean, proxy_variance, bins, residual_variance_by_bin,
                  min_inner_for_variance: int, max_inner_per_scenario: int):
         n = len(proxy_mean)
         if not (len(outer_payoff) == len(weight) == len(proxy_variance) == len(bins) == n):
             raise ValueError("ScenarioEstimates: inconsistent sizes")
-        self.w = [float(v) for v in weight]
-        self.mu = [float(v) for v in proxy_mean]
-        self.pv = [float(v) for v in proxy_variance]
-        self.bin = [int(b) for b in bins]
-        self.residual = [float(v) for v in residual_variance_by_bin]
+        f = lambda v: np.array(v, np.float64)  # noqa: E731
+        self.w, self.mu, self.pv = f(weight), f(proxy_mean), f(proxy_variance)
+        self.bin = np.array(bins, np.int64)
+        self.residual = f(residual_variance_by_bin)
         nb = len(self.residual)
-        self.misspec, self.shift = [0.0] * nb, [0.0] * nb
+        self.misspec, self.shift = np.zeros(nb), np.zeros(nb)
         self.min_inner, self.max_inner = min_inner_for_variance, max_inner_per_scenario
-        self.count0, self.count1, self.batches = [1] * n, [0] * n, [0] * n
-        self.mean0, self.mean1 = [float(v) for v in outer_payoff], [0.0] * n
-        self.m20, self.m21 = [0.0] * n, [0.0] * n
+        self.count0, self.count1, self.batches = np.ones(n, np.int64), np.zeros(n, np.int64), np.zeros(n, np.int64)
+        self.mean0, self.mean1 = f(outer_payoff), np.zeros(n)
+        self.m20, self.m21 = np.zeros(n), np.zeros(n)
 
     def size(self) -> int:
         return len(self.mu)
@@ -307,63 +317,66 @@ class ScenarioEstimates:
     def num_bins(self) -> int:
         return len(self.residual)
 
-    def proxy_mean(self, i: int) -> float:
-        return self.mu[i] + self.shift[self.bin[i]]
+    def proxy_mean(self) -> np.ndarray:
+        return self.mu + self.shift[self.bin]
 
-    def proxy_variance(self, i: int) -> float:
-        return self.pv[i] + self.misspec[self.bin[i]]
+    def proxy_variance(self) -> np.ndarray:
+        return self.pv + self.misspec[self.bin]
 
-    def inner_paths(self, i: int) -> int:
-        return self.count0[i] + self.count1[i] - 1
+    def inner_paths(self) -> np.ndarray:
+        return self.count0 + self.count1 - 1
 
-    def pooled(self, i: int) -> Tuple[float, float, float]:
-        n0, n1 = float(self.count0[i]), float(self.count1[i])
+    def pooled(self):
+        n0, n1 = self.count0.astype(np.float64), self.count1.astype(np.float64)
         n = n0 + n1
-        if self.count1[i] == 0:
-            return n, self.mean0[i], self.m20[i]
-        d = self.mean1[i] - self.mean0[i]
-        return n, self.mean0[i] + d * n1 / n, self.m20[i] + self.m21[i] + d * d * (n0 * n1 / n)
+        d = self.mean1 - self.mean0
+        one = self.count1 == 0
+        with np.errstate(invalid="ignore", divide="ignore"):
+            mean = np.where(one, self.mean0, self.mean0 + d * n1 / n)
+            m2 = np.where(one, self.m20, self.m20 + self.m21 + d * d * (n0 * n1 / n))
+        return n, mean, m2
 
-    def blend(self, i: int, sample_mean: float, sample_variance: float) -> Tuple[float, float]:
-        pvar, proxy = self.proxy_variance(i), self.proxy_mean(i)
+    def blend(self, sample_mean: np.ndarray, sample_variance: np.ndarray):
+        pvar, proxy = self.proxy_variance(), self.proxy_mean()
         den = pvar + sample_variance
-        if den <= 0.0:
-            return proxy, 0.0
-        return proxy + pvar / den * (sample_mean - proxy), pvar * sample_variance / den
+        pos = den > 0.0
+        with np.errstate(invalid="ignore", divide="ignore"):
+            value = np.where(pos, proxy + pvar / den * (sample_mean - proxy), proxy)
+            var = np.where(pos, pvar * sample_variance / den, 0.0)
+        return value, var
 
-    def within_variance(self, i: int) -> float:
-        n, _, m2 = self.pooled(i)
-        return m2 / (n - 1.0) if n >= 1.0 + float(self.min_inner) else self.residual[self.bin[i]]
+    def within_variance(self) -> np.ndarray:
+        n, _, m2 = self.pooled()
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.where(n >= 1.0 + float(self.min_inner), m2 / (n - 1.0), self.residual[self.bin])
 
-    def estimate(self, i: int) -> float:
-        n, mean, _ = self.pooled(i)
-        return self.blend(i, mean, self.within_variance(i) / n)[0]
+    def estimate(self) -> np.ndarray:
+        n, mean, _ = self.pooled()
+        return self.blend(mean, self.within_variance() / n)[0]
 
-    def std_error(self, i: int) -> float:
-        n, mean, _ = self.pooled(i)
-        return math.sqrt(self.blend(i, mean, self.within_variance(i) / n)[1])
+    def std_error(self) -> np.ndarray:
+        n, mean, _ = self.pooled()
+        return np.sqrt(self.blend(mean, self.within_variance() / n)[1])
 
-    def refinement_gain(self, i: int) -> float:
-        n, mean, _ = self.pooled(i)
-        within = self.within_variance(i)
-        current = self.blend(i, mean, within / n)[1]
-        if current <= 0.0:
-            return 0.0
-        used = float(self.inner_paths(i))
-        remaining = max(0.0, float(self.max_inner) - used)
-        best = self.blend(i, mean, within / (n + remaining))[1]
-        return 1.0 - best / current
+    def refinement_gain(self) -> np.ndarray:
+        n, mean, _ = self.pooled()
+        within = self.within_variance()
+        current = self.blend(mean, within / n)[1]
+        used = self.inner_paths().astype(np.float64)
+        remaining = np.maximum(0.0, float(self.max_inner) - used)
+        best = self.blend(mean, within / (n + remaining))[1]
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.where(current <= 0.0, 0.0, 1.0 - best / current)
 
-    def selection_estimate(self, i: int) -> float:
-        if self.count1[i] == 0:
-            return self.proxy_mean(i)
-        return self.blend(i, self.mean0[i], self.within_variance(i) / float(self.count0[i]))[0]
+    def selection_estimate(self) -> np.ndarray:
+        value = self.blend(self.mean0, self.within_variance() / self.count0.astype(np.float64))[0]
+        return np.where(self.count1 == 0, self.proxy_mean(), value)
 
-    def value_estimate(self, i: int) -> float:
-        return self.mean1[i] if self.count1[i] > 0 else self.mean0[i]
+    def value_estimate(self) -> np.ndarray:
+        return np.where(self.count1 > 0, self.mean1, self.mean0)
 
-    def value_variance(self, i: int) -> float:
-        return self.within_variance(i) / float(self.count1[i] if self.count1[i] > 0 else self.count0[i])
+    def value_variance(self) -> np.ndarray:
+        return self.within_variance() / np.where(self.count1 > 0, self.count1, self.count0).astype(np.float64)
 
     def add_inner_batch(self, i: int, payoffs: np.ndarray) -> None:
         n = len(payoffs)
@@ -372,29 +385,30 @@ class ScenarioEstimates:
         if not np.all(np.isfinite(payoffs)):
             raise RuntimeError("nested Monte Carlo: inner simulation returned a non-finite payoff")
         half = n // 2
-        self.count0[i], self.mean0[i], self.m20[i] = _merge(self.count0[i], self.mean0[i], self.m20[i], payoffs[:half])
-        self.count1[i], self.mean1[i], self.m21[i] = _merge(self.count1[i], self.mean1[i], self.m21[i], payoffs[half:])
+        c, m, q = _merge(int(self.count0[i]), float(self.mean0[i]), float(self.m20[i]), payoffs[:half])
+        self.count0[i], self.mean0[i], self.m20[i] = c, m, q
+        c, m, q = _merge(int(self.count1[i]), float(self.mean1[i]), float(self.m21[i]), payoffs[half:])
+        self.count1[i], self.mean1[i], self.m21[i] = c, m, q
         self.batches[i] += 1
 
     def update_misspecification(self, min_scenarios_per_bin: int) -> None:
         nb = self.num_bins()
+        n, mean, m2 = self.pooled()
+        ok = np.nonzero(~(n < 1.0 + float(self.min_inner)))[0]
         s, sq, noise, cnt = [0.0] * nb, [0.0] * nb, [0.0] * nb, [0] * nb
         gsq = gnoise = 0.0
-        gcount = 0
-        for i in range(self.size()):
-            n, mean, m2 = self.pooled(i)
-            if n < 1.0 + float(self.min_inner):
-                continue
-            d = mean - self.mu[i]
-            sampling = m2 / (n - 1.0) / n + self.pv[i]
-            b = self.bin[i]
-            s[b] += d
-            sq[b] += d * d
-            noise[b] += sampling
-            cnt[b] += 1
-            gsq += d * d
-            gnoise += sampling
-            gcount += 1
+        if ok.size:
+            d = mean[ok] - self.mu[ok]
+            sampling = m2[ok] / (n[ok] - 1.0) / n[ok] + self.pv[ok]
+            for k, i in enumerate(ok.tolist()):
+                b = int(self.bin[i])
+                s[b] += d[k]
+                sq[b] += d[k] * d[k]
+                noise[b] += sampling[k]
+                cnt[b] += 1
+                gsq += d[k] * d[k]
+                gnoise += sampling[k]
+        gcount = int(ok.size)
         glob = max(0.0, (gsq - gnoise) / float(gcount)) if gcount > 0 else 0.0
         for b in range(nb):
             if cnt[b] >= min_scenarios_per_bin:
@@ -406,18 +420,20 @@ class ScenarioEstimates:
                 self.misspec[b] = glob
 
 
-def _misclassification_probability(gap: float, se: float) -> float:
-    return normal_cdf(-gap / se) if se > 0.0 else 0.0
+def _misclassification_probability(gap: np.ndarray, se: np.ndarray) -> np.ndarray:
+    with np.errstate(invalid="ignore", divide="ignore"):
+        x = -gap / se
+    p = 0.5 * _erfc(-x / math.sqrt(2.0))
+    return np.where(se > 0.0, p, 0.0)
 
 
-def _mark_largest(contribution: List[float], s: ScenarioEstimates, excess: float, urgency: List[float]) -> None:
+def _mark_largest(contribution: np.ndarray, s: ScenarioEstimates, excess: float, urgency: np.ndarray) -> None:
     """The error-budget rule (adaptive_nested.cpp:85-106)."""
-    n = len(contribution)
-    gain = [s.refinement_gain(i) for i in range(n)]
-    reducible = [contribution[i] * gain[i] for i in range(n)]
-    order = sorted(range(n), key=lambda i: -reducible[i])  # stable, descending
+    gain = s.refinement_gain()
+    reducible = contribution * gain
+    order = np.argsort(-reducible, kind="stable")
     covered = 0.0
-    for i in order:
+    for i in order.tolist():
         if covered >= excess or reducible[i] <= 0.0:
             break
         if gain[i] < MIN_GAIN:
@@ -438,19 +454,19 @@ class PositivePart:
         return self.label
 
     def evaluate(self, s: ScenarioEstimates) -> float:
-        total = 0.0
-        for i in range(s.size()):
-            if s.selection_estimate(i) > 0.0:
-                total += s.w[i] * s.value_estimate(i)
-        return total / float(s.size()) if s.size() else 0.0
+        if not s.size():
+            return 0.0
+        sel = s.selection_estimate() > 0.0
+        return _acc_sum((s.w * s.value_estimate())[sel]) / float(s.size())
 
     def plug_in(self, values, weights) -> float:
-        total = 0.0
-        for i, v in enumerate(values):
-            total += (1.0 if weights is None or len(weights) == 0 else weights[i]) * max(v, 0.0)
-        return total / float(len(values)) if len(values) else 0.0
+        v = np.asarray(values, np.float64)
+        if not v.size:
+            return 0.0
+        w = np.ones_like(v) if weights is None or len(weights) == 0 else np.asarray(weights, np.float64)
+        return _acc_sum(w * np.maximum(v, 0.0)) / float(v.size)
 
-    def urgency(self, s: ScenarioEstimates, urgency: List[float]) -> None:
+    def urgency(self, s: ScenarioEstimates, urgency: np.ndarray) -> None:
         n = s.size()
         if n == 0:
             return
@@ -458,24 +474,17 @@ class PositivePart:
         if not (half > 0.0):
             return
         nn = float(n)
-        noise, counted = 0.0, 0
-        sel = [s.selection_estimate(i) for i in range(n)]
-        for i in range(n):
-            if sel[i] > 0.0:
-                noise += s.w[i] * s.w[i] * s.value_variance(i)
-                counted += 1
+        sel = s.selection_estimate() > 0.0
+        vv = s.value_variance()
+        noise = _acc_sum((s.w * s.w * vv)[sel])
+        counted = int(np.count_nonzero(sel))
         if counted > 0 and math.sqrt(noise) / nn > half:
             share = half * half * nn * nn / float(counted)
-            for i in range(n):
-                if sel[i] > 0.0:
-                    urgency[i] = max(urgency[i], s.w[i] * s.w[i] * s.value_variance(i) / share)
-        contribution = [0.0] * n
-        total = 0.0
-        for i in range(n):
-            est, se = s.estimate(i), s.std_error(i)
-            gap = abs(est)
-            contribution[i] = s.w[i] * (gap * _misclassification_probability(gap, se)) / nn
-            total += contribution[i]
+            cand = s.w * s.w * vv / share
+            np.maximum(urgency, np.where(sel, cand, urgency), out=urgency)
+        gap = np.abs(s.estimate())
+        contribution = s.w * (gap * _misclassification_probability(gap, s.std_error())) / nn
+        total = _acc_sum(contribution)
         if total > half:
             _mark_largest(contribution, s, total - half, urgency)
 
@@ -500,20 +509,18 @@ class Quantile:
         return max(q, 0.0) if self.pos else q
 
     def evaluate(self, s: ScenarioEstimates) -> float:
-        return self.plug_in([s.estimate(i) for i in range(s.size())])
+        return self.plug_in(s.estimate())
 
-    def urgency(self, s: ScenarioEstimates, urgency: List[float]) -> None:
-        n = s.size()
-        if n == 0:
+    def urgency(self, s: ScenarioEstimates, urgency: np.ndarray) -> None:
+        if s.size() == 0:
             return
-        v = [s.estimate(i) for i in range(n)]
+        v = s.estimate()
         q = exact_quantile(v, self.level)
         if self.pos and q < 0.0:
             return
         threshold = normal_cdf(-self.z)
-        for i in range(n):
-            p = _misclassification_probability(abs(v[i] - q), s.std_error(i))
-            urgency[i] = max(urgency[i], s.refinement_gain(i) * p / threshold)
+        p = _misclassification_probability(np.abs(v - q), s.std_error())
+        np.maximum(urgency, s.refinement_gain() * p / threshold, out=urgency)
 
 
 @dataclass
@@ -588,14 +595,15 @@ def _run_batch(s: ScenarioEstimates, evaluation: List[int], chosen: List[int], b
     """One inner batch for each chosen scenario that fits in the budget (adaptive_nested.cpp:541-573), all of the
     round's jobs handed to the simulator at once."""
     jobs, total = [], 0
+    inner_paths = s.inner_paths()
     for i in chosen:
-        used = s.inner_paths(i)
+        used = int(inner_paths[i])
         m = 0 if used >= max_inner else min(batch, max_inner - used)
         if m == 0:
             continue
         if total + m > budget:
             break
-        jobs.append((i, m, derive_seed(seed, evaluation[i], s.batches[i], ADAPTIVE_TAG)))
+        jobs.append((i, m, derive_seed(seed, evaluation[i], int(s.batches[i]), ADAPTIVE_TAG)))
         total += m
     if jobs:
         outs = inner([(evaluation[i], sd, m) for i, m, sd in jobs])
@@ -607,28 +615,24 @@ def _run_batch(s: ScenarioEstimates, evaluation: List[int], chosen: List[int], b
 def _candidates(s: ScenarioEstimates, statistics, outside: List[bool], o: AdaptiveOptions) -> Tuple[List[int], int]:
     """The scenarios to refine this round (adaptive_nested.cpp:578-625)."""
     n = s.size()
-    queues, wanted, capped = [], [False] * n, 0
+    queues, wanted, capped = [], np.zeros(n, bool), 0
+    inner_paths = s.inner_paths()
+    at_cap = inner_paths >= o.max_inner_per_scenario
     for st in statistics:
-        urgency = [0.0] * n
+        urgency = np.zeros(n)
         st.urgency(s, urgency)
-        keyed = []
-        for i in range(n):
-            if not (urgency[i] > 1.0):
-                continue
-            if s.inner_paths(i) >= o.max_inner_per_scenario:
-                if not wanted[i]:
-                    capped += 1
-                wanted[i] = True
-                continue
-            keyed.append((urgency[i], i))
-        keyed = sorted(keyed, key=lambda k: -k[0])  # stable, descending
-        queues.append([k[1] for k in keyed])
+        asked = urgency > 1.0  # also skips NaN
+        capped += int(np.count_nonzero(asked & at_cap & ~wanted))
+        wanted |= asked & at_cap
+        idx = np.nonzero(asked & ~at_cap)[0]
+        order = np.argsort(-urgency[idx], kind="stable")  # stable, descending
+        queues.append(idx[order].tolist())
     out, taken = [], [False] * n
     if o.refine_outside_training_range:
         for i in range(n):
             if len(out) >= o.max_scenarios_per_round:
                 break
-            if outside[i] and s.inner_paths(i) < o.min_inner_for_variance:
+            if outside[i] and inner_paths[i] < o.min_inner_for_variance:
                 out.append(i)
                 taken[i] = True
     depth = 0
@@ -748,19 +752,19 @@ def estimate_adaptive(features: np.ndarray, payoff: Sequence[float], weight: Opt
         r.estimate.append(st.evaluate(s))
     r.inner_paths = used
     per_bin, refined_bin = [0] * nb, [0] * nb
+    r.value = s.estimate().tolist()
+    r.inner = [int(v) for v in s.inner_paths()]
     for k in range(n_eval):
-        r.value.append(s.estimate(k))
-        r.inner.append(s.inner_paths(k))
         per_bin[bins[k]] += 1
         if r.inner[k] > 0:
             r.refined_scenarios += 1
             refined_bin[bins[k]] += 1
-    r.audited_scenarios = sum(1 for k in audit if s.inner_paths(k) > 0)
+    r.audited_scenarios = sum(1 for k in audit if r.inner[k] > 0)
     for b in range(nb):
         r.bins.append({"lower_probability": 0.0 if b == 0 else o.bin_probabilities[b - 1],
                        "upper_probability": 1.0 if b + 1 == nb else o.bin_probabilities[b],
-                       "scenarios": per_bin[b], "refined": refined_bin[b], "residual_std_dev": math.sqrt(s.residual[b]),
-                       "bias_shift": s.shift[b], "bias_rms": math.sqrt(s.misspec[b])})
+                       "scenarios": per_bin[b], "refined": refined_bin[b], "residual_std_dev": math.sqrt(float(s.residual[b])),
+                       "bias_shift": float(s.shift[b]), "bias_rms": math.sqrt(float(s.misspec[b]))})
     return r
 
 

@@ -141,3 +141,23 @@ def bermudan_book(paths: int = 200_000, bermudans: int = 200) -> Tuple[S.Model, 
                                  physical=True, position=1.0, degree=3))
     books = [S.NettingSet(trades[i:i + 4], None) for i in range(0, bermudans, 4)]
     return m, books, bermudans
+
+
+def nested_netting_set(seed: int = PORTFOLIO_SEED + 7, swaps: int = 20, forwards: int = 8, options: int = 4) -> S.NettingSet:
+    """A netting set of the trades the nested exposure supports (src/nested/nested_exposure.cpp:59-82): one-schedule
+    swaps (semiannual, 1-5y), FX forwards (3m-5y) and FX options (3m-3y) on the correlated book's two FX factors."""
+    rng = np.random.default_rng(seed)
+    trades: list = []
+    for _ in range(swaps):
+        months = int(rng.integers(12, 61)) // 6 * 6
+        sched = [k / 12.0 for k in range(0, months + 1, 6)]
+        trades.append(S.Swap(rng.uniform(1e6, 1e7), rng.uniform(0.01, 0.04), bool(rng.random() < 0.5), sched))
+    for _ in range(forwards):
+        asset = int(rng.integers(0, 2))
+        trades.append(S.Forward(asset, rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 5e6), (1.1, 0.9)[asset] * rng.uniform(0.9, 1.1),
+                                int(rng.integers(3, 61)) / 12.0))
+    for _ in range(options):
+        asset = int(rng.integers(0, 2))
+        trades.append(S.Option(asset, bool(rng.random() < 0.5), rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 3e6),
+                               (1.1, 0.9)[asset] * rng.uniform(0.9, 1.1), int(rng.integers(3, 37)) / 12.0))
+    return S.NettingSet(trades, None)
