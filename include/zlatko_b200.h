@@ -156,6 +156,22 @@ zk_status zk_zero_bond_coefficients(const double* model, size_t model_len, const
 zk_status zk_nest_events(const zk_nest* nest, uint64_t* events);
 void zk_nest_destroy(zk_nest* nest);
 
+/* ---- the adaptive nest's proxy (HermiteProxy, src/nested/adaptive_nested.cpp:145-277; host code) ---- */
+/* Least squares of y on the Hermite products of the standardised features up to total degree `degree`
+ * (lowered until every basis function has two training rows), ridge relative to the mean diagonal, HC0
+ * sandwich covariance; the reference's arithmetic order, so its bits.  features [n_rows][dims] row-major,
+ * y [n_rows]; rows [n_train] the training rows (HermiteProxy::fit).  Errors (fewer than two rows, more than
+ * 2000 basis functions, singular equations) return ZK_ERR_INVALID_ARGUMENT with the message in err. */
+typedef struct zk_hermite zk_hermite;
+zk_status zk_hermite_fit(const double* features, size_t n_rows, size_t dims, const double* y, const uint64_t* rows, size_t n_train,
+                         uint32_t degree, double ridge, zk_hermite** out, char* err, size_t err_len);
+/* value[k] and variance[k] (>= 0) of feature row rows[k] (HermiteProxy::predict), row-parallel on the host. */
+zk_status zk_hermite_predict(const zk_hermite* proxy, const double* features, size_t dims, const uint64_t* rows, size_t n,
+                             double* value, double* variance);
+/* degree_and_basis[0] = the fitted degree, [1] = the number of basis functions. */
+zk_status zk_hermite_info(const zk_hermite* proxy, uint64_t* degree_and_basis);
+void zk_hermite_destroy(zk_hermite* proxy);
+
 /* ---- without device allocation (no counterpart in the reference) ----------------------------------- */
 /* For callers that cannot call cudaMalloc: a host that hands all device memory to its own pooling
  * allocator up front (a serving process, a framework's caching allocator), or a plug-in that runs

@@ -66,6 +66,36 @@ def test_estimate_adaptive_is_the_reference(case):
 
 
 @needs_ref
+def test_estimate_adaptive_with_many_features_is_the_reference():
+    """Ten features, one of them constant (dropped from the basis): 220 basis functions at degree 3, so the
+    proxy's Gram, sandwich and predictions run on several host threads and must keep the reference's bits."""
+    F, y, w, v, simulate = toy(n=2400, dims=10, seed=11)
+    F[:, 7] = 0.25
+    o = N.AdaptiveOptions(inner_budget=30_000, max_rounds=6, seed=7, hermite_degree=3)
+    size = float(np.mean(w * np.abs(y)))
+    stats = [N.PositivePart(0.01, 1e-3 * size, "EE*"), N.Quantile(0.95, True, 2.0, "PFE")]
+    got = N.estimate_adaptive(F, y, w, N.per_scenario(simulate), stats, o)
+    want = ref.estimate_adaptive(F, y, w, simulate, 0.01, 1e-3 * size, 0.95, o)
+    assert got.proxy_basis == want["proxy_basis"] == 220 and got.proxy_degree == 3
+    for k in ("estimate", "baseline", "regression", "proxy", "value"):
+        assert np.array_equal(np.asarray(getattr(got, k)), want[k]), k
+    assert got.inner_paths == want["inner_paths"]
+
+
+def test_proxy_errors_are_the_reference_messages():
+    F = np.random.default_rng(0).normal(size=(10, 2))
+    with pytest.raises(ValueError, match="at least two training rows"):
+        N.HermiteProxy(3).fit(F, F[:, 0], [3])
+    with pytest.raises(RuntimeError, match="predict before fit"):
+        N.HermiteProxy(3).predict(F, [0])
+    p = N.HermiteProxy(3)
+    p.fit(F, F[:, 0] + F[:, 1] ** 2, range(10))
+    assert (p.degree(), p.num_basis()) == (1, 3)  # degree 2 has 6 terms > 10 / 2
+    with pytest.raises(ValueError, match="do not match"):
+        p.predict(F[:, :1], [0])
+
+
+@needs_ref
 def test_estimate_uniform_is_the_reference():
     F, y, w, v, simulate = toy()
     sc = list(range(0, 1200, 7))

@@ -20,7 +20,7 @@ LIB = os.path.join(OUT_DIR, "libzlatko_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["fused_exposure.cu", "row_stats.cu", "nested_inner.cu", "amc_fit.cu", "mlp.cu", "surrogate.cu", "capi.cu", "peaks.cu"]
-CPP_SOURCES = ["plan_compiler.cpp"]
+CPP_SOURCES = ["plan_compiler.cpp", "hermite_proxy.cpp"]
 HEADERS = ["zk_device.cuh", "zk_kernels.h", "plan_compiler.h"]
 
 

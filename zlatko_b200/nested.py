@@ -11,12 +11,14 @@ in one kernel launch where the reference calls a per-scenario callback on a thre
 from __future__ import annotations
 
 import bisect
+import ctypes as C
 import math
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
+from . import _native
 from .summary import exact_quantile
 
 M64 = 0xFFFFFFFFFFFFFFFF
@@ -80,189 +82,65 @@ def _seq_sum(a) -> float:
     return s
 
 
-def _cholesky(a: np.ndarray) -> np.ndarray:
-    """ccr::cholesky (src/core/matrix.cpp:49-68); raises ValueError where the reference throws."""
-    n = a.shape[0]
-    lo = np.zeros((n, n))
-    for i in range(n):
-        for j in range(i + 1):
-            if abs(a[i, j] - a[j, i]) > 1e-10:
-                raise ValueError("cholesky: matrix must be symmetric")
-            s = float(a[i, j])
-            for k in range(j):
-                s -= lo[i, k] * lo[j, k]
-            if i == j:
-                if s <= 0.0:
-                    raise ValueError("cholesky: matrix is not positive definite")
-                lo[i, i] = math.sqrt(s)
-            else:
-                lo[i, j] = s / lo[j, j]
-    return lo
-
-
-def _cholesky_solve(lo: np.ndarray, b) -> np.ndarray:
-    """Forward and back substitution with a lower-triangular factor (adaptive_nested.cpp:41-54)."""
-    n = lo.shape[0]
-    x = [float(v) for v in b]
-    for i in range(n):
-        s = x[i]
-        for k in range(i):
-            s -= lo[i, k] * x[k]
-        x[i] = s / lo[i, i]
-    for i in range(n - 1, -1, -1):
-        s = x[i]
-        for k in range(i + 1, n):
-            s -= lo[k, i] * x[k]
-        x[i] = s / lo[i, i]
-    return np.array(x)
-
-
-def total_degree_terms(dims: int, degree: int) -> List[List[int]]:
-    """Exponent vectors of total degree <= degree in graded order (adaptive_nested.cpp:57-75)."""
-    out: List[List[int]] = []
-    cur = [0] * dims
-
-    def rec(pos: int, remaining: int) -> None:
-        if pos == dims:
-            out.append(list(cur))
-            return
-        for k in range(remaining + 1):
-            cur[pos] = k
-            rec(pos + 1, remaining - k)
-        cur[pos] = 0
-
-    rec(0, degree)
-    return sorted(out, key=sum)  # stable, as std::stable_sort
-
-
 class HermiteProxy:
     """Least-squares proxy of V in probabilists' Hermite polynomials of the standardised features, all products
-    up to a total degree, with the HC0 sandwich variance of every prediction (adaptive_nested.cpp:145-277)."""
+    up to a total degree, with the HC0 sandwich variance of every prediction (adaptive_nested.cpp:145-277).
+    Fit and prediction are native host code (zk_hermite_fit / zk_hermite_predict) in the reference's arithmetic
+    order, threaded over independent entries and rows; there is no Python fallback."""
 
     def __init__(self, degree: int = 3, ridge: float = 1e-10):
         self.degree_, self.ridge = degree, ridge
-        self.fitted_degree = 0
-        self.terms: List[List[int]] = []
-        self.beta: Optional[np.ndarray] = None
+        self._h = None
+        self._info = (0, 0)
 
-    def basis_rows(self, x: np.ndarray) -> np.ndarray:
-        """phi for every row of x [n][dims] (the reference's basis(), row by row in its operation order)."""
-        x = np.atleast_2d(np.asarray(x, np.float64))
-        d, m = self.fitted_degree, len(self.active)
-        h = np.zeros((x.shape[0], m, d + 1))
-        for f, j in enumerate(self.active):
-            z = (x[:, j] - self.mean[j]) / self.scale[j]
-            h[:, f, 0] = 1.0
-            if d >= 1:
-                h[:, f, 1] = z
-            for k in range(1, d):
-                h[:, f, k + 1] = z * h[:, f, k] - float(k) * h[:, f, k - 1]
-        phi = np.ones((x.shape[0], len(self.terms)))
-        for t, powers in enumerate(self.terms):
-            v = np.ones(x.shape[0])
-            for f in range(m):
-                if powers[f] > 0:
-                    v = v * h[:, f, powers[f]]
-            phi[:, t] = v
-        return phi
+    def __del__(self):
+        if getattr(self, "_h", None) is not None:
+            _native.lib().zk_hermite_destroy(self._h)
+            self._h = None
 
     def fit(self, features: np.ndarray, y: Sequence[float], rows: Sequence[int]) -> None:
-        n = len(rows)
-        if n < 2:
-            raise ValueError("HermiteProxy: needs at least two training rows")
-        F = np.asarray(features, np.float64)
-        if F.shape[0] != len(y):
+        F = np.ascontiguousarray(features, np.float64)
+        if F.ndim != 2:
+            raise ValueError("HermiteProxy: features must be [rows][dims]")
+        yy = np.ascontiguousarray(y, np.float64)
+        if F.shape[0] != yy.shape[0]:
             raise ValueError("HermiteProxy: features and targets differ in length")
-        dim = F.shape[1]
-        mean = np.zeros(dim)
-        for r in rows:
-            mean = mean + F[r]
-        mean = mean / float(n)
-        ss = np.zeros(dim)
-        for r in rows:
-            ss = ss + (F[r] - mean) * (F[r] - mean)
-        self.mean, self.scale, self.active = mean, np.ones(dim), []
-        for j in range(dim):
-            sd = math.sqrt(ss[j] / float(n - 1))
-            if sd > 1e-12 * max(1.0, abs(mean[j])):
-                self.scale[j] = sd
-                self.active.append(j)
-        d = self.degree_
-        while True:
-            self.terms = total_degree_terms(len(self.active), d)
-            self.fitted_degree = d
-            if 2 * len(self.terms) <= n or d == 0:
-                break
-            d -= 1
-        if len(self.terms) > 2000:
-            raise ValueError("HermiteProxy: more than 2000 basis functions")
-        p = len(self.terms)
-        phis = self.basis_rows(F[list(rows)])
-        yy = np.asarray(y, np.float64)
-        gram, rhs = np.zeros((p, p)), np.zeros(p)
-        for k, r in enumerate(rows):
-            phi = phis[k]
-            rhs = rhs + phi * yy[r]
-            gram = gram + np.outer(phi, phi)
-        trace = 0.0
-        for a in range(p):
-            trace += gram[a, a]
-        gram = np.tril(gram) + np.tril(gram, -1).T
-        ridge = self.ridge
-        while True:
-            g = gram.copy()
-            lam = ridge * max(trace / float(p), 1e-300)
-            for a in range(p):
-                g[a, a] += lam
-            try:
-                lo = _cholesky(g)
-                break
-            except ValueError:
-                if ridge > 1e-2:
-                    raise ValueError("HermiteProxy: normal equations are singular")
-                ridge *= 1e3
-        self.beta = _cholesky_solve(lo, rhs)
-        meat = np.zeros((p, p))
-        for k, r in enumerate(rows):
-            phi = phis[k]
-            fitted = _seq_sum(phi * self.beta)
-            e2 = (yy[r] - fitted) * (yy[r] - fitted)
-            meat = meat + np.outer(e2 * phi, phi)
-        meat = np.tril(meat) + np.tril(meat, -1).T
-        inverse = np.zeros((p, p))
-        for c in range(p):
-            unit = np.zeros(p)
-            unit[c] = 1.0
-            inverse[:, c] = _cholesky_solve(lo, unit)
-        tmp = np.zeros((p, p))
-        for a in range(p):
-            for k in range(p):
-                v = inverse[a, k]
-                if v != 0.0:
-                    tmp[a] = tmp[a] + v * meat[k]
-        cov = np.zeros((p, p))
-        for a in range(p):
-            for k in range(p):
-                v = tmp[a, k]
-                if v != 0.0:
-                    cov[a] = cov[a] + v * inverse[k]
-        self.cov = cov
+        rr = np.ascontiguousarray(rows, np.uint64)
+        L = _native.lib()
+        h, err = C.c_void_p(), C.create_string_buffer(256)
+        st = L.zk_hermite_fit(F.ctypes.data, F.shape[0], F.shape[1], yy.ctypes.data, rr.ctypes.data, rr.size,
+                              int(self.degree_), float(self.ridge), C.byref(h), err, len(err))
+        if st != 0:
+            raise ValueError(err.value.decode() or f"HermiteProxy: fit failed ({st})")
+        if self._h is not None:
+            L.zk_hermite_destroy(self._h)
+        self._h, self._dims = h, F.shape[1]
+        info = (C.c_uint64 * 2)()
+        L.zk_hermite_info(h, info)
+        self._info = (int(info[0]), int(info[1]))
 
-    def predict_rows(self, x: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
-        """(value, estimation variance) of every row of x, each summed in the reference's order."""
-        if self.beta is None:
+    def predict(self, features: np.ndarray, rows: Sequence[int]) -> Tuple[np.ndarray, np.ndarray]:
+        """(value, estimation variance) of the feature rows `rows`."""
+        if self._h is None:
             raise RuntimeError("HermiteProxy: predict before fit")
-        phi = self.basis_rows(x)
-        value = np.add.accumulate(phi * self.beta[None, :], axis=1)[:, -1]
-        acc = np.stack([np.add.accumulate(self.cov[a][None, :] * phi, axis=1)[:, -1] for a in range(len(self.terms))], axis=1)
-        var = np.add.accumulate(phi * acc, axis=1)[:, -1]
-        return value, np.maximum(var, 0.0)
+        F = np.ascontiguousarray(features, np.float64)
+        if F.ndim != 2 or F.shape[1] != self._dims:
+            raise ValueError("HermiteProxy: features do not match the fit")
+        rr = np.ascontiguousarray(rows, np.uint64)
+        if rr.size and int(rr.max()) >= F.shape[0]:
+            raise ValueError("HermiteProxy: row beyond the features")
+        value, var = np.empty(rr.size), np.empty(rr.size)
+        st = _native.lib().zk_hermite_predict(self._h, F.ctypes.data, F.shape[1], rr.ctypes.data, rr.size,
+                                              value.ctypes.data, var.ctypes.data)
+        if st != 0:
+            raise RuntimeError(f"HermiteProxy: predict failed ({st})")
+        return value, var
 
     def degree(self) -> int:
-        return self.fitted_degree
+        return self._info[0]
 
     def num_basis(self) -> int:
-        return len(self.terms)
+        return self._info[1]
 
 
 def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int, float, float]:
@@ -678,7 +556,7 @@ def estimate_adaptive(features: np.ndarray, payoff: Sequence[float], weight: Opt
     proxy = HermiteProxy(o.hermite_degree)
     proxy.fit(F, payoff, r.training)
     r.proxy_degree, r.proxy_basis = proxy.degree(), proxy.num_basis()
-    mu_a, var_a = proxy.predict_rows(F[r.evaluation])
+    mu_a, var_a = proxy.predict(F, r.evaluation)
     mu, est_var = [float(v) for v in mu_a], [float(v) for v in var_a]
     w_all = None if weight is None or len(weight) == 0 else [float(v) for v in weight]
     wts = [1.0 if w_all is None else w_all[i] for i in r.evaluation]
@@ -689,7 +567,7 @@ def estimate_adaptive(features: np.ndarray, payoff: Sequence[float], weight: Opt
     nb = len(thresholds) + 1
     bins = [bisect.bisect_left(thresholds, v) for v in mu]
     rsum, rcount, rtotal = [0.0] * nb, [0] * nb, 0.0
-    fitted_t, _ = proxy.predict_rows(F[r.training])
+    fitted_t, _ = proxy.predict(F, r.training)
     for k, i in enumerate(r.training):
         fitted = float(fitted_t[k])
         e2 = (float(payoff[i]) - fitted) * (float(payoff[i]) - fitted)
