@@ -165,9 +165,10 @@ void zk_nest_destroy(zk_nest* nest);
 typedef struct zk_hermite zk_hermite;
 zk_status zk_hermite_fit(const double* features, size_t n_rows, size_t dims, const double* y, const uint64_t* rows, size_t n_train,
                          uint32_t degree, double ridge, zk_hermite** out, char* err, size_t err_len);
-/* value[k] and variance[k] (>= 0) of feature row rows[k] (HermiteProxy::predict), row-parallel on the host. */
-zk_status zk_hermite_predict(const zk_hermite* proxy, const double* features, size_t dims, const uint64_t* rows, size_t n,
-                             double* value, double* variance);
+/* value[k] and variance[k] (>= 0) of feature row rows[k] of features [n_rows][dims] (HermiteProxy::predict),
+ * row-parallel on the host; a row index >= n_rows or a dims other than the fit's is ZK_ERR_INVALID_ARGUMENT. */
+zk_status zk_hermite_predict(const zk_hermite* proxy, const double* features, size_t n_rows, size_t dims, const uint64_t* rows,
+                             size_t n, double* value, double* variance);
 /* degree_and_basis[0] = the fitted degree, [1] = the number of basis functions. */
 zk_status zk_hermite_info(const zk_hermite* proxy, uint64_t* degree_and_basis);
 void zk_hermite_destroy(zk_hermite* proxy);

@@ -93,6 +93,10 @@ def test_proxy_errors_are_the_reference_messages():
     assert (p.degree(), p.num_basis()) == (1, 3)  # degree 2 has 6 terms > 10 / 2
     with pytest.raises(ValueError, match="do not match"):
         p.predict(F[:, :1], [0])
+    with pytest.raises(ValueError, match="beyond the features"):
+        p.predict(F, [0, 10])
+    v, s = p.predict(F, [])
+    assert v.size == s.size == 0
 
 
 @needs_ref

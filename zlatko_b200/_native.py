@@ -121,7 +121,7 @@ def lib() -> C.CDLL:
         "zk_nest_destroy": (None, [vp]),
         "zk_zero_bond_coefficients": (st, [vp, sz, vp, sz, vp]),
         "zk_hermite_fit": (st, [vp, sz, sz, vp, vp, sz, C.c_uint32, C.c_double, P(vp), C.c_char_p, sz]),
-        "zk_hermite_predict": (st, [vp, vp, sz, vp, sz, vp, vp]),
+        "zk_hermite_predict": (st, [vp, vp, sz, sz, vp, sz, vp, vp]),
         "zk_hermite_info": (st, [vp, P(C.c_uint64)]),
         "zk_hermite_destroy": (None, [vp]),
         "zk_batch_timings": (st, [vp, P(C.c_float)]),

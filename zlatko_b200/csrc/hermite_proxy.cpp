@@ -305,9 +305,11 @@ zk_status zk_hermite_fit(const double* features, size_t n_rows, size_t dims, con
   }
 }
 
-zk_status zk_hermite_predict(const zk_hermite* h, const double* features, size_t dims, const uint64_t* rows, size_t n, double* value,
-                             double* variance) {
-  if (!h || !features || !rows || !value || !variance || dims != h->dims) return ZK_ERR_INVALID_ARGUMENT;
+zk_status zk_hermite_predict(const zk_hermite* h, const double* features, size_t n_rows, size_t dims, const uint64_t* rows, size_t n,
+                             double* value, double* variance) {
+  if (!h || (n > 0 && (!features || !rows || !value || !variance)) || dims != h->dims) return ZK_ERR_INVALID_ARGUMENT;
+  for (std::size_t k = 0; k < n; ++k)
+    if (rows[k] >= n_rows) return ZK_ERR_INVALID_ARGUMENT;
   const std::size_t p = h->basisSize();
   parallelFor(n, std::max<std::size_t>(1, 1000000 / std::max<std::size_t>(p * p, 1)), [&](std::size_t b, std::size_t e) {
     std::vector<double> phi(p), he(h->active.size() * (h->degree + 1));

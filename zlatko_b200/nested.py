@@ -127,13 +127,11 @@ class HermiteProxy:
         if F.ndim != 2 or F.shape[1] != self._dims:
             raise ValueError("HermiteProxy: features do not match the fit")
         rr = np.ascontiguousarray(rows, np.uint64)
-        if rr.size and int(rr.max()) >= F.shape[0]:
-            raise ValueError("HermiteProxy: row beyond the features")
         value, var = np.empty(rr.size), np.empty(rr.size)
-        st = _native.lib().zk_hermite_predict(self._h, F.ctypes.data, F.shape[1], rr.ctypes.data, rr.size,
+        st = _native.lib().zk_hermite_predict(self._h, F.ctypes.data, F.shape[0], F.shape[1], rr.ctypes.data, rr.size,
                                               value.ctypes.data, var.ctypes.data)
         if st != 0:
-            raise RuntimeError(f"HermiteProxy: predict failed ({st})")
+            raise ValueError("HermiteProxy: a row beyond the features")
         return value, var
 
     def degree(self) -> int:
