@@ -172,6 +172,9 @@ zk_status zk_hermite_predict(const zk_hermite* proxy, const double* features, si
 /* degree_and_basis[0] = the fitted degree, [1] = the number of basis functions. */
 zk_status zk_hermite_info(const zk_hermite* proxy, uint64_t* degree_and_basis);
 void zk_hermite_destroy(zk_hermite* proxy);
+/* out[k] = erfc(x[k]) of the C library (the reference's normalCdf, include/ccr/core/math.hpp:15, is
+ * 0.5 erfc(-x / sqrt 2)): the estimator's misclassification probabilities of all scenarios in one call. */
+zk_status zk_erfc_array(const double* x, size_t n, double* out);
 
 /* ---- without device allocation (no counterpart in the reference) ----------------------------------- */
 /* For callers that cannot call cudaMalloc: a host that hands all device memory to its own pooling

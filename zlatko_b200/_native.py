@@ -70,7 +70,7 @@ EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last
            "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params",
            "zk_surrogate_features", "zk_surrogate_book", "zk_compile", "zk_plan_view_of", "zk_plan_view_f64_of", "zk_plan_dates", "zk_plan_sizes",
            "zk_plan_destroy", "zk_factor_paths_f64", "zk_nest_create", "zk_nest_run", "zk_nest_events", "zk_nest_destroy",
-           "zk_zero_bond_coefficients", "zk_hermite_fit", "zk_hermite_predict", "zk_hermite_info", "zk_hermite_destroy"]
+           "zk_zero_bond_coefficients", "zk_hermite_fit", "zk_hermite_predict", "zk_hermite_info", "zk_hermite_destroy", "zk_erfc_array"]
 
 _lib: Optional[C.CDLL] = None
 
@@ -124,6 +124,7 @@ def lib() -> C.CDLL:
         "zk_hermite_predict": (st, [vp, vp, sz, sz, vp, sz, vp, vp]),
         "zk_hermite_info": (st, [vp, P(C.c_uint64)]),
         "zk_hermite_destroy": (None, [vp]),
+        "zk_erfc_array": (st, [vp, sz, vp]),
         "zk_batch_timings": (st, [vp, P(C.c_float)]),
         "zk_batch_read": (st, [vp, P(Output)]),
         "zk_batch_info_get": (st, [vp, P(BatchInfo)]),

@@ -311,20 +311,28 @@ zk_status zk_hermite_predict(const zk_hermite* h, const double* features, size_t
   for (std::size_t k = 0; k < n; ++k)
     if (rows[k] >= n_rows) return ZK_ERR_INVALID_ARGUMENT;
   const std::size_t p = h->basisSize();
-  parallelFor(n, std::max<std::size_t>(1, 1000000 / std::max<std::size_t>(p * p, 1)), [&](std::size_t b, std::size_t e) {
-    std::vector<double> phi(p), he(h->active.size() * (h->degree + 1));
-    for (std::size_t k = b; k < e; ++k) {
-      h->basis(features + rows[k] * dims, phi.data(), he.data());
-      double v = 0.0, var = 0.0;
+  // Four rows at a time: each row's sums keep their own order, and the four independent chains hide the
+  // latency of the in-order additions.
+  constexpr std::size_t kRows = 4;
+  const std::size_t groups = (n + kRows - 1) / kRows;
+  parallelFor(groups, std::max<std::size_t>(1, 250000 / std::max<std::size_t>(p * p, 1)), [&](std::size_t b, std::size_t e) {
+    std::vector<double> phi(kRows * p), he(h->active.size() * (h->degree + 1));
+    for (std::size_t g = b; g < e; ++g) {
+      const std::size_t k0 = g * kRows, m = std::min(kRows, n - k0);
+      for (std::size_t r = 0; r < kRows; ++r)  // short groups repeat their last row
+        h->basis(features + rows[k0 + std::min(r, m - 1)] * dims, &phi[r * p], he.data());
+      double v[kRows] = {}, var[kRows] = {};
       for (std::size_t a = 0; a < p; ++a) {
-        v += phi[a] * h->beta[a];
         const double* ca = &h->cov[a * p];
-        double u = 0.0;
-        for (std::size_t c = 0; c < p; ++c) u += ca[c] * phi[c];
-        var += phi[a] * u;
+        double u[kRows] = {};
+        for (std::size_t c = 0; c < p; ++c)
+          for (std::size_t r = 0; r < kRows; ++r) u[r] += ca[c] * phi[r * p + c];
+        for (std::size_t r = 0; r < kRows; ++r) {
+          v[r] += phi[r * p + a] * h->beta[a];
+          var[r] += phi[r * p + a] * u[r];
+        }
       }
-      value[k] = v;
-      variance[k] = std::max(var, 0.0);
+      for (std::size_t r = 0; r < m; ++r) value[k0 + r] = v[r], variance[k0 + r] = std::max(var[r], 0.0);
     }
   });
   return ZK_OK;
@@ -338,5 +346,11 @@ zk_status zk_hermite_info(const zk_hermite* h, uint64_t* degree_and_basis) {
 }
 
 void zk_hermite_destroy(zk_hermite* h) { delete h; }
+
+zk_status zk_erfc_array(const double* x, size_t n, double* out) {
+  if (n > 0 && (!x || !out)) return ZK_ERR_INVALID_ARGUMENT;
+  for (std::size_t k = 0; k < n; ++k) out[k] = std::erfc(x[k]);
+  return ZK_OK;
+}
 
 }  // extern "C"

@@ -75,11 +75,10 @@ def normal_cdf(x: float) -> float:
 
 
 def _seq_sum(a) -> float:
-    """A left-to-right sum (the reference's loops), not numpy's pairwise one."""
-    s = 0.0
-    for v in a:
-        s += v
-    return s
+    """A left-to-right sum from 0.0 (the reference's loops), not numpy's pairwise one: np.add.accumulate adds in
+    order; the final + 0.0 turns the -0.0 of an all-negative-zero input into the loop's +0.0."""
+    a = np.asarray(a, np.float64).ravel()
+    return float(np.add.accumulate(a)[-1]) + 0.0 if a.size else 0.0
 
 
 class HermiteProxy:
@@ -156,14 +155,16 @@ def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int
     return count + n, mean, m2
 
 
-def _acc_sum(a) -> float:
-    """A left-to-right sum of an array (np.add.accumulate is sequential), the reference's loop order."""
-    a = np.asarray(a, np.float64)
-    return float(np.add.accumulate(a)[-1]) if a.size else 0.0
+_acc_sum = _seq_sum
 
 
 def _erfc(a: np.ndarray) -> np.ndarray:
-    return np.array([math.erfc(v) for v in a.tolist()], np.float64)
+    """erfc of every element by the C library's erfc (the one math.erfc calls), in one native call."""
+    x = np.ascontiguousarray(a, np.float64)
+    out = np.empty_like(x)
+    if x.size and _native.lib().zk_erfc_array(x.ctypes.data, x.size, out.ctypes.data) != 0:
+        raise RuntimeError("erfc failed")
+    return out
 
 
 class ScenarioEstimates:
@@ -274,16 +275,17 @@ class ScenarioEstimates:
         s, sq, noise, cnt = [0.0] * nb, [0.0] * nb, [0.0] * nb, [0] * nb
         gsq = gnoise = 0.0
         if ok.size:
+            # Per bin and overall, each sum runs over the scenarios in ascending order, as the reference's loop.
             d = mean[ok] - self.mu[ok]
+            d2 = d * d
             sampling = m2[ok] / (n[ok] - 1.0) / n[ok] + self.pv[ok]
-            for k, i in enumerate(ok.tolist()):
-                b = int(self.bin[i])
-                s[b] += d[k]
-                sq[b] += d[k] * d[k]
-                noise[b] += sampling[k]
-                cnt[b] += 1
-                gsq += d[k] * d[k]
-                gnoise += sampling[k]
+            bins = self.bin[ok]
+            for b in range(nb):
+                sel = bins == b
+                cnt[b] = int(np.count_nonzero(sel))
+                if cnt[b]:
+                    s[b], sq[b], noise[b] = _seq_sum(d[sel]), _seq_sum(d2[sel]), _seq_sum(sampling[sel])
+            gsq, gnoise = _seq_sum(d2), _seq_sum(sampling)
         gcount = int(ok.size)
         glob = max(0.0, (gsq - gnoise) / float(gcount)) if gcount > 0 else 0.0
         for b in range(nb):
@@ -583,14 +585,11 @@ def estimate_adaptive(features: np.ndarray, payoff: Sequence[float], weight: Opt
         r.regression.append(st.plug_in(mu, wts))
     r.proxy = mu
 
-    dims = F.shape[1]
-    lo = [math.inf] * dims
-    hi = [-math.inf] * dims
-    for i in r.training:
-        for j in range(dims):
-            lo[j] = min(lo[j], F[i, j])
-            hi[j] = max(hi[j], F[i, j])
-    outside = [any(F[i, j] < lo[j] or F[i, j] > hi[j] for j in range(dims)) for i in r.evaluation]
+    # The training range of every feature (min and max are exact in any order); a scenario is outside it when
+    # any of its features is.
+    lo, hi = F[r.training].min(axis=0), F[r.training].max(axis=0)
+    E = F[r.evaluation]
+    outside = np.any((E < lo) | (E > hi), axis=1).tolist()
 
     audit_batch = max(o.inner_batch, o.min_inner_for_variance)
     audit_per_bin = min(o.audit_per_bin, max(2, o.inner_budget // 5 // (nb * audit_batch)))
