@@ -48,6 +48,22 @@ def derive_seed(seed: int, a: int, b: int = 0, c: int = 0) -> int:
     return split_mix(x ^ ((c * 0x8CB92BA72F3D8DD7) & M64))
 
 
+def _split_mix_u64(z: np.ndarray) -> np.ndarray:
+    """split_mix of every element of a uint64 array (numpy's uint64 arithmetic wraps modulo 2^64)."""
+    z = z + np.uint64(GOLDEN)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def derive_seeds(seed: int, a: np.ndarray, b: np.ndarray, c: int) -> np.ndarray:
+    """derive_seed(seed, a[k], b[k], c) for every k at once."""
+    x = np.full(len(a), split_mix((seed + GOLDEN) & M64), np.uint64)
+    x = _split_mix_u64(x ^ np.asarray(a, np.uint64))
+    x = _split_mix_u64(x ^ (np.asarray(b, np.uint64) * np.uint64(0xD1B54A32D192ED03)))
+    return _split_mix_u64(x ^ np.uint64((c * 0x8CB92BA72F3D8DD7) & M64))
+
+
 def shuffle(v: List[int], seed: int) -> None:
     """Deterministic Fisher-Yates shuffle (adaptive_nested.cpp:31-38)."""
     s = seed
@@ -156,6 +172,25 @@ def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int
 
 
 _acc_sum = _seq_sum
+
+
+def _row_sums(a: np.ndarray) -> np.ndarray:
+    """_seq_sum of every row of a 2-D array."""
+    return np.add.accumulate(a, axis=1)[:, -1] + 0.0
+
+
+def _merge_rows(count: np.ndarray, mean: np.ndarray, m2: np.ndarray, payoffs: np.ndarray):
+    """_merge of row k of payoffs into (count[k], mean[k], m2[k]) for every k, element by element."""
+    n = payoffs.shape[1]
+    if n == 0:
+        return count, mean, m2
+    batch_mean = _row_sums(payoffs) / float(n)
+    dev = payoffs - batch_mean[:, None]
+    batch_m2 = _row_sums(dev * dev)
+    na, nb = count.astype(np.float64), float(n)
+    total = na + nb
+    delta = batch_mean - mean
+    return count + n, mean + delta * nb / total, m2 + (batch_m2 + delta * delta * (na * nb / total))
 
 
 def _erfc(a: np.ndarray) -> np.ndarray:
@@ -267,6 +302,20 @@ class ScenarioEstimates:
         c, m, q = _merge(int(self.count1[i]), float(self.mean1[i]), float(self.m21[i]), payoffs[half:])
         self.count1[i], self.mean1[i], self.m21[i] = c, m, q
         self.batches[i] += 1
+
+    def add_inner_batches(self, idx: np.ndarray, payoffs: np.ndarray) -> None:
+        """add_inner_batch of scenario idx[k] with payoffs[k] for every k at once: distinct scenarios, batches
+        of one length.  Every row's sums run in order, so the result is that of the one-by-one calls."""
+        if payoffs.shape[1] == 0:
+            return
+        if not np.all(np.isfinite(payoffs)):
+            raise RuntimeError("nested Monte Carlo: inner simulation returned a non-finite payoff")
+        half = payoffs.shape[1] // 2
+        for count, mean, m2, part in ((self.count0, self.mean0, self.m20, payoffs[:, :half]),
+                                      (self.count1, self.mean1, self.m21, payoffs[:, half:])):
+            c, m, q = _merge_rows(count[idx], mean[idx], m2[idx], part)
+            count[idx], mean[idx], m2[idx] = c, m, q
+        self.batches[idx] += 1
 
     def update_misspecification(self, min_scenarios_per_bin: int) -> None:
         nb = self.num_bins()
@@ -472,7 +521,7 @@ def _run_batch(s: ScenarioEstimates, evaluation: List[int], chosen: List[int], b
                seed: int, inner: InnerBatches) -> int:
     """One inner batch for each chosen scenario that fits in the budget (adaptive_nested.cpp:541-573), all of the
     round's jobs handed to the simulator at once."""
-    jobs, total = [], 0
+    picked, sizes, total = [], [], 0
     inner_paths = s.inner_paths()
     for i in chosen:
         used = int(inner_paths[i])
@@ -481,12 +530,20 @@ def _run_batch(s: ScenarioEstimates, evaluation: List[int], chosen: List[int], b
             continue
         if total + m > budget:
             break
-        jobs.append((i, m, derive_seed(seed, evaluation[i], int(s.batches[i]), ADAPTIVE_TAG)))
+        picked.append(i)
+        sizes.append(m)
         total += m
-    if jobs:
-        outs = inner([(evaluation[i], sd, m) for i, m, sd in jobs])
-        for (i, m, _), out in zip(jobs, outs):
-            s.add_inner_batch(i, np.asarray(out, np.float64)[:m])
+    if picked:
+        idx = np.asarray(picked, np.int64)
+        ev = np.asarray(evaluation, np.int64)[idx]
+        seeds = derive_seeds(seed, ev, s.batches[idx], ADAPTIVE_TAG)
+        outs = inner([(int(e), int(sd), m) for e, sd, m in zip(ev.tolist(), seeds.tolist(), sizes)])
+        # The batches of one length go in together (a scenario appears once per round).
+        sz = np.asarray(sizes, np.int64)
+        for m in np.unique(sz).tolist():
+            ks = np.nonzero(sz == m)[0]
+            rows = np.stack([np.asarray(outs[k], np.float64)[:m] for k in ks.tolist()])
+            s.add_inner_batches(idx[ks], rows)
     return total
 
 
@@ -504,29 +561,26 @@ def _candidates(s: ScenarioEstimates, statistics, outside: List[bool], o: Adapti
         wanted |= asked & at_cap
         idx = np.nonzero(asked & ~at_cap)[0]
         order = np.argsort(-urgency[idx], kind="stable")  # stable, descending
-        queues.append(idx[order].tolist())
-    out, taken = [], [False] * n
-    if o.refine_outside_training_range:
-        for i in range(n):
-            if len(out) >= o.max_scenarios_per_round:
-                break
-            if outside[i] and inner_paths[i] < o.min_inner_for_variance:
-                out.append(i)
-                taken[i] = True
-    depth = 0
-    while len(out) < o.max_scenarios_per_round:
-        anyq = False
-        for q in queues:
-            if depth >= len(q):
-                continue
-            anyq = True
-            i = q[depth]
-            if not taken[i] and len(out) < o.max_scenarios_per_round:
-                out.append(i)
-                taken[i] = True
-        if not anyq:
-            break
-        depth += 1
+        queues.append(idx[order])
+    out: List[int] = []
+    taken = np.zeros(n, bool)
+    if o.refine_outside_training_range and o.max_scenarios_per_round > 0:
+        first = np.nonzero(np.asarray(outside, bool) & (inner_paths < o.min_inner_for_variance))[0]
+        first = first[:o.max_scenarios_per_round]
+        out = first.tolist()
+        taken[first] = True
+    # Round robin over the queues (depth by depth, queue by queue), each scenario once, until the round is full.
+    room = o.max_scenarios_per_round - len(out)
+    if room > 0 and any(len(q) for q in queues):
+        depth = max(len(q) for q in queues)
+        grid = np.full((depth, len(queues)), -1, np.int64)
+        for k, q in enumerate(queues):
+            grid[:len(q), k] = q
+        flat = grid.ravel()
+        flat = flat[flat >= 0]
+        flat = flat[~taken[flat]]
+        _, first = np.unique(flat, return_index=True)
+        out += flat[np.sort(first)][:room].tolist()
     return out, capped
 
 
