@@ -156,21 +156,6 @@ class HermiteProxy:
         return self._info[1]
 
 
-def _merge(count: int, mean: float, m2: float, payoffs: np.ndarray) -> Tuple[int, float, float]:
-    """Chan et al. merge of a batch into a running (count, mean, M2) (adaptive_nested.cpp:371-384)."""
-    n = len(payoffs)
-    if n == 0:
-        return count, mean, m2
-    batch_mean = _seq_sum(payoffs) / float(n)
-    batch_m2 = _seq_sum((payoffs - batch_mean) * (payoffs - batch_mean))
-    na, nb = float(count), float(n)
-    total = na + nb
-    delta = batch_mean - mean
-    mean += delta * nb / total
-    m2 += batch_m2 + delta * delta * (na * nb / total)
-    return count + n, mean, m2
-
-
 _acc_sum = _seq_sum
 
 
@@ -180,7 +165,8 @@ def _row_sums(a: np.ndarray) -> np.ndarray:
 
 
 def _merge_rows(count: np.ndarray, mean: np.ndarray, m2: np.ndarray, payoffs: np.ndarray):
-    """_merge of row k of payoffs into (count[k], mean[k], m2[k]) for every k, element by element."""
+    """Chan et al. merge of row k of payoffs into the running (count[k], mean[k], M2[k]) for every k, element by
+    element in the reference's order (adaptive_nested.cpp:373-385)."""
     n = payoffs.shape[1]
     if n == 0:
         return count, mean, m2
@@ -291,17 +277,9 @@ class ScenarioEstimates:
         return self.within_variance() / np.where(self.count1 > 0, self.count1, self.count0).astype(np.float64)
 
     def add_inner_batch(self, i: int, payoffs: np.ndarray) -> None:
-        n = len(payoffs)
-        if n == 0:
-            return
-        if not np.all(np.isfinite(payoffs)):
-            raise RuntimeError("nested Monte Carlo: inner simulation returned a non-finite payoff")
-        half = n // 2
-        c, m, q = _merge(int(self.count0[i]), float(self.mean0[i]), float(self.m20[i]), payoffs[:half])
-        self.count0[i], self.mean0[i], self.m20[i] = c, m, q
-        c, m, q = _merge(int(self.count1[i]), float(self.mean1[i]), float(self.m21[i]), payoffs[half:])
-        self.count1[i], self.mean1[i], self.m21[i] = c, m, q
-        self.batches[i] += 1
+        """ScenarioEstimates::addInnerBatch (adaptive_nested.cpp:390-400): the first half of the batch goes to the
+        selection fold, the rest to the value fold, each merged as Chan et al."""
+        self.add_inner_batches(np.array([i], np.int64), np.asarray(payoffs, np.float64)[None, :])
 
     def add_inner_batches(self, idx: np.ndarray, payoffs: np.ndarray) -> None:
         """add_inner_batch of scenario idx[k] with payoffs[k] for every k at once: distinct scenarios, batches
