@@ -208,6 +208,15 @@ class ScenarioEstimates:
         self.count0, self.count1, self.batches = np.ones(n, np.int64), np.zeros(n, np.int64), np.zeros(n, np.int64)
         self.mean0, self.mean1 = f(outer_payoff), np.zeros(n)
         self.m20, self.m21 = np.zeros(n), np.zeros(n)
+        # Derived arrays of the current state (pooled moments, blended estimates), dropped on every change: a
+        # round asks for them many times between two changes.  Callers treat them as read-only.
+        self._memo: dict = {}
+
+    def _cached(self, key: str, make):
+        v = self._memo.get(key)
+        if v is None:
+            v = self._memo[key] = make()
+        return v
 
     def size(self) -> int:
         return len(self.mu)
@@ -216,15 +225,18 @@ class ScenarioEstimates:
         return len(self.residual)
 
     def proxy_mean(self) -> np.ndarray:
-        return self.mu + self.shift[self.bin]
+        return self._cached("proxy_mean", lambda: self.mu + self.shift[self.bin])
 
     def proxy_variance(self) -> np.ndarray:
-        return self.pv + self.misspec[self.bin]
+        return self._cached("proxy_variance", lambda: self.pv + self.misspec[self.bin])
 
     def inner_paths(self) -> np.ndarray:
         return self.count0 + self.count1 - 1
 
     def pooled(self):
+        return self._cached("pooled", self._pooled)
+
+    def _pooled(self):
         n0, n1 = self.count0.astype(np.float64), self.count1.astype(np.float64)
         n = n0 + n1
         d = self.mean1 - self.mean0
@@ -244,22 +256,27 @@ class ScenarioEstimates:
         return value, var
 
     def within_variance(self) -> np.ndarray:
+        return self._cached("within", self._within_variance)
+
+    def _within_variance(self) -> np.ndarray:
         n, _, m2 = self.pooled()
         with np.errstate(invalid="ignore", divide="ignore"):
             return np.where(n >= 1.0 + float(self.min_inner), m2 / (n - 1.0), self.residual[self.bin])
 
-    def estimate(self) -> np.ndarray:
+    def _current(self):
         n, mean, _ = self.pooled()
-        return self.blend(mean, self.within_variance() / n)[0]
+        return self._cached("current", lambda: self.blend(mean, self.within_variance() / n))
+
+    def estimate(self) -> np.ndarray:
+        return self._current()[0]
 
     def std_error(self) -> np.ndarray:
-        n, mean, _ = self.pooled()
-        return np.sqrt(self.blend(mean, self.within_variance() / n)[1])
+        return self._cached("std_error", lambda: np.sqrt(self._current()[1]))
 
     def refinement_gain(self) -> np.ndarray:
         n, mean, _ = self.pooled()
         within = self.within_variance()
-        current = self.blend(mean, within / n)[1]
+        current = self._current()[1]
         used = self.inner_paths().astype(np.float64)
         remaining = np.maximum(0.0, float(self.max_inner) - used)
         best = self.blend(mean, within / (n + remaining))[1]
@@ -288,6 +305,7 @@ class ScenarioEstimates:
             return
         if not np.all(np.isfinite(payoffs)):
             raise RuntimeError("nested Monte Carlo: inner simulation returned a non-finite payoff")
+        self._memo.clear()
         half = payoffs.shape[1] // 2
         for count, mean, m2, part in ((self.count0, self.mean0, self.m20, payoffs[:, :half]),
                                       (self.count1, self.mean1, self.m21, payoffs[:, half:])):
@@ -323,6 +341,7 @@ class ScenarioEstimates:
             else:
                 self.shift[b] = 0.0
                 self.misspec[b] = glob
+        self._memo.clear()  # the proxy's shift and variance changed
 
 
 def _misclassification_probability(gap: np.ndarray, se: np.ndarray) -> np.ndarray:
