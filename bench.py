@@ -62,9 +62,27 @@ def parse():
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            with open(path) as f:
+                d = json.load(f)
+        except (OSError, ValueError):
+            d = {}
+
+        def find(node):  # "hbm_gbs" at the top, else the first numeric HBM GB/s entry anywhere
+            if isinstance(node, dict):
+                for k, v in node.items():
+                    if "hbm" in str(k).lower() and "gb" in str(k).lower() and isinstance(v, (int, float)) and v > 0:
+                        return float(v)
+                for v in node.values():
+                    r = find(v)
+                    if r:
+                        return r
+            return None
+
+        v = d.get("hbm_gbs") if isinstance(d, dict) else None
+        v = float(v) if isinstance(v, (int, float)) and v > 0 else find(d)
+        if v:
+            return v, "measured"
     return 6650.0, "fallback"
 
 
