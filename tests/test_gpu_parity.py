@@ -295,6 +295,35 @@ def test_results_do_not_depend_on_the_tile_shape(ctx):
             assert np.array_equal(s0, s1) and np.array_equal(v0, v1)
 
 
+def test_large_and_small_state_netting_sets_share_a_batch(ctx):
+    """A netting set with 30 running-coupon slots (more shared-memory state than the variant with more resident
+    CTAs allows) and two small ones: with 2 or 4 paths per thread the batch revalues them in two launches, the
+    small ones on the kernel compiled for more resident CTAs.  Every tile shape gives the same bits, and so does
+    each plan run alone."""
+    m = gpu_model(3000)
+    m.base_grid = [k / 12 for k in range(1, 61)]
+    csa = S.Csa(1e5, 1e5, 1e4)  # every plan on the same dates (margin-call dates included): one launch group
+    books = [swap_book(3, seed=1, csa=csa), swap_book(30, seed=5, csa=csa), swap_book(9, seed=2, csa=csa)]
+    plans = [gpu.compile(m, b, S.Options(pfe_quantile=0.975)) for b in books]
+    out = []
+    for tile in (128, 256, 512):
+        b = ctx.batch(plans)
+        try:
+            b.set_tile_paths(tile)
+            b.execute()
+            out.append(b.read())
+            if tile > 128:
+                assert b.info().kernels_per_execute == 5  # simulate, two revalue launches, reduce, row statistics
+        finally:
+            b.close()
+    for r in out[1:]:
+        for (s0, v0), (s1, v1) in zip(out[0], r):
+            assert np.array_equal(s0, s1) and np.array_equal(v0, v1)
+    for p, (s, v) in zip(plans, out[1]):
+        s1, v1 = ctx.run(p)
+        assert np.array_equal(s, s1) and np.array_equal(v, v1)
+
+
 def test_batch_replays_a_cuda_graph_with_the_same_bits(ctx):
     """After the tile shape settles, a batch's executes replay one captured CUDA graph: same results as the
     eager first execute and as single-plan runs."""

@@ -32,6 +32,10 @@ struct zk_context {
   size_t stageInBytes = 0;
   unsigned char* stageOut = nullptr;
   size_t stageOutBytes = 0;
+  // A second stream for the large-state revalue launch of a split batch, beside the small-state launch on the
+  // context's stream (fork and join events order the two); created by the first eager execute that splits.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -352,6 +356,9 @@ struct Batch {
     std::vector<uint32_t> planIdx;
     uint32_t numFields = 0;
     size_t stateWordsMax = 0;
+    // Netting sets in decreasing order of shared-memory state: [splitAt, n) keep at most kSmallStateWords words
+    // per path (at most smallStateMax) and may run as a second launch with more resident CTAs.
+    size_t splitAt = 0, smallStateMax = 0;
     bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
   };
@@ -436,6 +443,11 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   if (normals && B->launches.size() != 1) throw fail(ZK_ERR_INVALID_ARGUMENT, "injected normals need plans of one scenario");
   // ---- per launch: the factor cube shared by its netting sets, one CTA column per netting set ----
   for (auto& L : B->launches) {
+    std::stable_sort(L.planIdx.begin(), L.planIdx.end(),
+                     [&](uint32_t a, uint32_t b) { return B->plans[a].stateWords > B->plans[b].stateWords; });
+    L.splitAt = L.planIdx.size();
+    while (L.splitAt > 0 && B->plans[L.planIdx[L.splitAt - 1]].stateWords <= static_cast<uint32_t>(kSmallStateWords)) --L.splitAt;
+    if (L.splitAt < L.planIdx.size()) L.smallStateMax = B->plans[L.planIdx[L.splitAt]].stateWords;
     for (uint32_t k : L.planIdx) {
       const auto& P = B->plans[k];
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
@@ -678,9 +690,38 @@ void execute(Batch<R>& B, bool capturing = false) {
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
   for (auto& L : B.launches) ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
   ZK_CUDA(recordEvent(B.ev[1], s, capturing));
-  for (auto& L : B.launches)
-    ZK_CUDA(launchRevalue<R>(L.cb, reinterpret_cast<const NsArgs<R>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                             numTilesOf(L.sc.nP, B.ppt), L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
+  for (auto& L : B.launches) {
+    const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff);
+    const uint32_t n = static_cast<uint32_t>(L.planIdx.size()), tiles = numTilesOf(L.sc.nP, B.ppt);
+    // Lean single-precision launches of 2 or 4 paths per thread: the netting sets with little state run as
+    // their own launch, compiled for more resident CTAs than the shared memory of the largest allows.
+    const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < n;
+    if (!split) {
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
+      continue;
+    }
+    const uint32_t big = static_cast<uint32_t>(L.splitAt);
+    if (big > 0 && !ctx->side && !capturing) {
+      ZK_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      ZK_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+      ZK_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
+    }
+    // The few large-state netting sets fill less than a wave of long CTAs: they run on the side stream while
+    // the small-state launch fills the rest of the GPU.
+    const bool fork = big > 0 && ctx->side;
+    if (fork) {
+      ZK_CUDA(cudaEventRecord(ctx->fork, s));
+      ZK_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, ctx->side));
+    } else if (big > 0) {
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, s));
+    }
+    ZK_CUDA(launchRevalue<R>(L.cb, ns + big, n - big, tiles, L.smallStateMax, false, false, true, B.ppt, s, true));
+    if (fork) {
+      ZK_CUDA(cudaEventRecord(ctx->join, ctx->side));
+      ZK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
+    }
+  }
   for (const auto& M : B.im) ZK_CUDA(launchNestedIm<R>(M, s));
   ZK_CUDA(recordEvent(B.ev[2], s, capturing));
   if (!B.sink) {
@@ -983,6 +1024,12 @@ void zk_context_destroy(zk_context* ctx) {
   if (ctx->stageIn) cudaFreeHost(ctx->stageIn);
   if (ctx->stageOut) cudaFreeHost(ctx->stageOut);
   if (ctx->dErr) cudaFree(ctx->dErr);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->fork) cudaEventDestroy(ctx->fork);
+  if (ctx->join) cudaEventDestroy(ctx->join);
   if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1479,7 +1526,12 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
     info->table_bytes += P.nIdx * 4 + P.nTerms * 32 + static_cast<uint64_t>(P.nT) * 96 + P.nReq * 32;
     info->row_bytes += static_cast<uint64_t>(P.nR) * P.nP * 4;
   }
-  info->kernels_per_execute = 2 * B.launches.size() + 2;
+  uint64_t kernels = 2 + B.im.size();  // reduce, row statistics, one nested-margin launch per margin plan
+  for (const auto& L : B.launches) {
+    const bool split = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && L.splitAt < L.planIdx.size();
+    kernels += 1 + (split && L.splitAt > 0 ? 2 : 1);  // simulate, then one or two revalue launches
+  }
+  info->kernels_per_execute = kernels;
   info->tile_paths = static_cast<uint64_t>(kTile) * B.ppt;
   info->graph_replay = b->graph && !b->eager && b->graphPpt == B.ppt ? 1u : 0u;
   return ZK_OK;

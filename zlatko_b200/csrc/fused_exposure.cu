@@ -273,16 +273,19 @@ __device__ __forceinline__ R pick4(const R (&a)[4][PPT], uint32_t k, int i) {
   return k == 0 ? a[0][i] : k == 1 ? a[1][i] : k == 2 ? a[2][i] : a[3][i];
 }
 
-// Resident CTAs per SM the lean variants are compiled for (register budget 65536 / (128 x blocks)).
-template <int PPT, bool kLean>
+// Resident CTAs per SM the lean variants are compiled for (register budget 65536 / (128 x blocks)).  The
+// shared-memory state of a netting set with many swap slots allows 6 CTAs of 2-path threads; netting sets
+// with little state (kSmallState: at most kSmallStateWords words per path) fit 8, and their variant is
+// compiled for 8 (64 registers).
+template <int PPT, bool kLean, bool kSmallState = false>
 constexpr int revalueMinBlocks() {
-  return !kLean ? 1 : PPT == 1 ? 8 : PPT == 2 ? 6 : 3;
+  return !kLean ? 1 : PPT == 1 ? 8 : PPT == 2 ? (kSmallState ? 8 : 6) : (kSmallState ? 4 : 3);
 }
 
 // Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
 // statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
-template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean>
-__global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
+template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean, bool kSmallState = false>
+__global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallState>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
   __shared__ NsArgs<R> sA;
@@ -906,7 +909,7 @@ size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) 
 namespace {
 template <typename R, int PPT>
 cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                             bool perTrade, bool sink, bool lean, cudaStream_t stream) {
+                             bool perTrade, bool sink, bool lean, bool smallState, cudaStream_t stream) {
   const size_t smem = revalueSmemBytes(stateWordsMax, perTrade, sizeof(R) == 8, PPT);
   const uint64_t blocks = static_cast<uint64_t>(numTiles) * numNs;
   if (blocks == 0) return cudaSuccess;
@@ -919,6 +922,8 @@ cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uin
   };
   if (sink) return go(revalueKernel<R, PPT, false, true, false>);
   if (perTrade) return go(revalueKernel<R, PPT, true, false, false>);
+  if (lean && smallState && stateWordsMax <= static_cast<size_t>(kSmallStateWords) && sizeof(R) == 4 && PPT > 1)
+    return go(revalueKernel<R, PPT, false, false, true, true>);
   if (lean) return go(revalueKernel<R, PPT, false, false, true>);
   return go(revalueKernel<R, PPT, false, false, false>);
 }
@@ -926,12 +931,12 @@ cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uin
 
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream) {
+                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream, bool smallState) {
   switch (ppt) {
-    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
-    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
+    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
+    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
     case 4:
-      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, stream);
+      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
@@ -942,8 +947,8 @@ template cudaError_t launchNestedIm<double>(const ImArgs<double>&, cudaStream_t)
 template cudaError_t launchSimulate<float>(const ScenarioArgs<float>&, const CubeArgs<float>&, cudaStream_t);
 template cudaError_t launchSimulate<double>(const ScenarioArgs<double>&, const CubeArgs<double>&, cudaStream_t);
 template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, bool,
-                                          int, cudaStream_t);
+                                          int, cudaStream_t, bool);
 template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool, bool,
-                                           int, cudaStream_t);
+                                           int, cudaStream_t, bool);
 
 }  // namespace zk
