@@ -534,29 +534,48 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
 
 // Fills the host image of the input region, once the arena base is known.
 // img: the host image to fill (B.inputBytes), B.image when null.
+// fn(w) for w in [0, workers) on that many host threads (the calling thread alone when workers is 1).
+template <class F>
+void onThreads(size_t workers, F&& fn) {
+  if (workers <= 1) {
+    fn(size_t{0});
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t w = 0; w < workers; ++w) pool.emplace_back([&, w] { fn(w); });
+  for (auto& t : pool) t.join();
+}
+
 template <typename R>
 void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char* img = nullptr) {
   B.im.clear();
-  if (img) {
-    std::memset(img, 0, B.inputBytes);
-  } else {
-    B.image.assign(B.inputBytes, 0);
+  if (!img) {
+    B.image.resize(B.inputBytes);
     img = B.image.data();
   }
+  // A book's tables are megabytes: the image is cleared and filled on up to 16 host threads.
+  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+  const size_t workers = std::min<size_t>({hw, 16, std::max<size_t>(1, B.inputBytes >> 19)});
+  onThreads(workers, [&](size_t w) {
+    const size_t a = B.inputBytes * w / workers, b = B.inputBytes * (w + 1) / workers;
+    std::memset(img + a, 0, b - a);
+  });
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
   auto dptr = [&](size_t o) { return reinterpret_cast<void*>(base + o); };
-  for (size_t i = 0; i < B.plans.size(); ++i) {
-    const auto& P = B.plans[i];
-    const auto& D = B.dev[i];
-    std::memcpy(img + D.dates, P.dates.data(), P.dates.size() * 4);
-    std::memcpy(img + D.table, P.table.data(), P.table.size() * sizeof(R));
-    std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
-    if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
-    if (P.im) {
-      std::memcpy(img + D.imSlots, P.imSlots.data(), P.imSlots.size() * 4);
-      std::memcpy(img + D.imModel, P.v.params + 12, (4 + kChol * kChol) * sizeof(R));
+  onThreads(std::min(workers, B.plans.size()), [&](size_t w) {
+    for (size_t i = w; i < B.plans.size(); i += std::min(workers, B.plans.size())) {
+      const auto& P = B.plans[i];
+      const auto& D = B.dev[i];
+      std::memcpy(img + D.dates, P.dates.data(), P.dates.size() * 4);
+      std::memcpy(img + D.table, P.table.data(), P.table.size() * sizeof(R));
+      std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
+      if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
+      if (P.im) {
+        std::memcpy(img + D.imSlots, P.imSlots.data(), P.imSlots.size() * 4);
+        std::memcpy(img + D.imModel, P.v.params + 12, (4 + kChol * kChol) * sizeof(R));
+      }
     }
-  }
+  });
   for (auto& L : B.launches) {
     std::vector<NsArgs<R>> args(L.planIdx.size());
     for (size_t k = 0; k < L.planIdx.size(); ++k) {

@@ -91,13 +91,22 @@ class Plan:
                     np.asarray(times, np.float64), np.asarray(reporting, np.int64), market_survival)
 
     def view(self) -> PlanView:
+        # The view holds pointers into the plan's arrays: kept while they are the same objects (their contents
+        # may change in place), rebuilt when a table is replaced.
+        key = (self.header, self.indices, self.params, self.steps, self.terms, self.requests)
+        cached = getattr(self, "_view", None)
+        if cached is not None and all(a is b for a, b in zip(cached[0], key)) and \
+                (cached[1].rows_total, cached[1].num_outputs) == (self.rows_total, self.num_outputs):
+            return cached[1]
         terms = self.terms if self.terms.size else np.zeros(8, np.float32)
         reqs = self.requests if self.requests.size else np.zeros(8, np.float32)
         self._keep = [terms, reqs]
-        return PlanView(_ptr(self.header, C.c_uint32), self.header.size, _ptr(self.indices, C.c_uint32), self.indices.size,
+        v = PlanView(_ptr(self.header, C.c_uint32), self.header.size, _ptr(self.indices, C.c_uint32), self.indices.size,
                         _ptr(self.params, C.c_float), self.params.size, _ptr(self.steps, C.c_float), self.steps.size,
                         _ptr(terms, C.c_float), self.terms.size, _ptr(reqs, C.c_float), self.requests.size,
                         self.rows_total, self.num_outputs)
+        self._view = (key, v)
+        return v
 
     def view64(self) -> PlanViewF64:
         if self.tables64 is None:
@@ -251,9 +260,21 @@ class Context:
 
     @staticmethod
     def _outputs(plans: Sequence[Plan], f64: bool = False):
-        T, ct, dt = (OutputF64, C.c_double, np.float64) if f64 else (Output, C.c_float, np.float32)
-        bufs = [(np.zeros(p.sums_len(), dt), np.zeros(p.values_len(), dt)) for p in plans]
-        outs = (T * len(plans))(*[T(_ptr(s, ct), s.size, _ptr(v, ct), v.size) for s, v in bufs])
+        """Output records of every plan over two shared buffers (one for the sums, one for the values): the
+        records are written as one array in the C layout {pointer, length, pointer, length}."""
+        T, dt = (OutputF64, np.float64) if f64 else (Output, np.float32)
+        sl = np.array([p.sums_len() for p in plans], np.int64)
+        vl = np.array([p.values_len() for p in plans], np.int64)
+        so, vo = np.cumsum(sl) - sl, np.cumsum(vl) - vl
+        sums, values = np.zeros(max(int(sl.sum()), 1), dt), np.zeros(max(int(vl.sum()), 1), dt)
+        rec = np.zeros((len(plans), 4), np.uint64)
+        rec[:, 0] = sums.ctypes.data + so * sums.itemsize
+        rec[:, 1] = sl
+        rec[:, 2] = values.ctypes.data + vo * values.itemsize
+        rec[:, 3] = vl
+        outs = (T * len(plans)).from_buffer(rec)
+        outs._bufs = (rec, sums, values)  # the records and the buffers they point into live as long as outs
+        bufs = [(sums[a:a + n], values[b:b + m]) for a, n, b, m in zip(so.tolist(), sl.tolist(), vo.tolist(), vl.tolist())]
         return outs, bufs
 
     def run(self, plan: Plan, rows: bool = False):
