@@ -272,10 +272,28 @@ def amc_leg(ctx, a):
         b.close()
     nT = plans[0].num_dates
     revals = float(a.amc_paths) * nT * n
-    return {"workload": f"{n} Bermudan swaptions (10y, annual exercise 1y-9y, degree 3) in {len(books)} netting sets, "
+    line = {"workload": f"{n} Bermudan swaptions (10y, annual exercise 1y-9y, degree 3) in {len(books)} netting sets, "
                         f"{a.amc_paths} paths, {nT} dates",
             "fit_s": fit_s, "revalue_ms": ms, "revals_per_s": revals / (fit_s + ms / 1e3),
-            "revalue_revals_per_s": revals / (ms / 1e3)}
+            "revalue_revals_per_s": revals / (ms / 1e3),
+            "fit_unit": "Bermudan path-dates fitted/s", "fit_rate": revals / fit_s}
+    from oracle import ref
+    if not a.no_cpu and ref.available():
+        # The reference's gpu::compile fits the same book with its CPU kernels (fitAmc on the SpinPool, all host
+        # threads) on a bounded sample of paths: the fit's work is linear in the paths.
+        sample = min(a.amc_paths, 10_000)
+        ms_, bs_, _ = workloads.bermudan_book(sample)
+        mflat, oflat = S.encode_model(ms_), S.encode_options(S.Options())
+        t0 = time.perf_counter()
+        for bk in bs_:
+            ref.compile_plan(mflat, S.encode_netting_set(bk), oflat)
+        cpu_s = time.perf_counter() - t0
+        cpu_rate = float(sample) * nT * n / cpu_s
+        line["cpu_baseline"] = {"value": cpu_rate, "unit": "Bermudan path-dates fitted/s", "cores": os.cpu_count() or 1,
+                                "kind": "reference", "sample": f"all {len(bs_)} netting sets on {sample} paths "
+                                                               f"(gpu::compile with fitAmc): {cpu_s:.2f} s"}
+        line["fit_speedup_vs_cpu"] = line["fit_rate"] / cpu_rate
+    return line
 
 
 def inner_revaluations(plan, trades: int) -> float:
