@@ -362,10 +362,11 @@ def test_pfe_is_the_exact_interpolated_quantile(ctx):
             assert vals[k] == np.float32(exact) or abs(vals[k] - exact) <= 1e-7 * max(abs(exact), 1.0)
 
 
-@pytest.mark.parametrize("paths", [8192, 30001])
+@pytest.mark.parametrize("paths", [8192, 30001, 65536])
 def test_exact_quantile_on_long_rows(ctx, paths):
     """Levels in the zero mass of the exposure rows, the median, the tails and both ends, on a row length read 16
-    bytes per load (8,192) and one that is not (30,001): the exact interpolated quantile."""
+    bytes per load (8,192), one that is not (30,001) and one long enough for the histogram's first range to come
+    from a sample of the row (65,536): the exact interpolated quantile."""
     m, ns = gpu_setup(paths, True)
     for level in (0.0, 0.3, 0.5, 0.9, 0.975, 0.999, 1.0):
         p = gpu.compile(m, ns, S.Options(pfe_quantile=level))

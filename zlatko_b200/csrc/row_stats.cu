@@ -7,7 +7,8 @@
 //
 // row statistics: one CTA per request.  Quantiles are the *exact* empirical quantile interpolated
 // between order statistics k = floor(p (n - 1)) and k + 1, as ccr::quantile does
-// (include/ccr/core/math.hpp:39-47), found without sorting the row: a min/max pass, a 4096-bin
+// (include/ccr/core/math.hpp:39-47), found without sorting the row: a min/max pass (on rows of 64K values or
+// more, over a 1/16 sample: it only sets the first histogram's range), a 4096-bin
 // histogram pass that locates the bins of ranks k and k + 1, then either one pass that reads the
 // maximum of k's bin and the minimum of k+1's bin (different bins) or a gather of k's bin into
 // shared memory and a bitonic sort there (same bin; narrowed again if the bin holds more than
@@ -113,6 +114,38 @@ __device__ __forceinline__ void forEachValue(const R* X, uint32_t nP, bool pos, 
   }
 }
 
+// A quantile's histogram needs a range, not the row's exact extremes: values outside it fall into the end bins,
+// and the ranks are still located exactly.  On long rows the range is the minimum and maximum of a sample,
+// every 16th block of 32 vectors (512 bytes, one 16-byte load per lane of a warp), about 1/16 of the row.
+constexpr uint32_t kSampleStride = 16;
+constexpr uint32_t kSampleMinVectors = 32 * kSampleStride * kRowWarps * 4;
+
+template <typename R>
+__device__ __forceinline__ bool canSample(const R* X, uint32_t nP) {
+  constexpr uint32_t kVec = 16 / sizeof(R);
+  return (nP % kVec) == 0 && (reinterpret_cast<uintptr_t>(X) & 15u) == 0 && nP / kVec >= kSampleMinVectors;
+}
+
+template <typename R>
+__device__ __forceinline__ void sampleMinMax(const R* X, uint32_t nP, bool pos, R& lo, R& hi) {
+  constexpr uint32_t kVec = 16 / sizeof(R);
+  const uint32_t nv = nP / kVec, blocks = nv / 32, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  auto take = [&](R x) {
+    x = pos ? fmax(x, R(0)) : x;
+    lo = fmin(lo, x), hi = fmax(hi, x);
+  };
+  for (uint32_t b = warp * kSampleStride; b < blocks; b += kRowWarps * kSampleStride) {
+    const uint32_t i = b * 32 + lane;
+    if constexpr (sizeof(R) == 4) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(X) + i);
+      take(q.x), take(q.y), take(q.z), take(q.w);
+    } else {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(X) + i);
+      take(q.x), take(q.y);
+    }
+  }
+}
+
 // Bitonic sort of n (<= kCap) values in shared memory, padded with +inf to a power of two.
 template <typename R>
 __device__ void bitonicSort(R* a, uint32_t n) {
@@ -179,10 +212,22 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
 
   const bool pos = op == 7;
   R lo = R(INFINITY), hi = R(-INFINITY);
-  forEachValue(X, nP, pos, [&](R v, bool ok) {
-    if (ok) lo = fmin(lo, v), hi = fmax(hi, v);
-  });
-  blockMinMax(lo, hi, s.rmin, s.rmax);
+  // Quantiles of long rows take their first histogram's range from a sample (the row is then read twice, not
+  // three times); a histogram request reports its range, and a sample without spread proves nothing, so those
+  // read the whole row for its exact minimum and maximum.
+  bool sampled = false;
+  if (op != 5 && canSample(X, nP)) {
+    sampleMinMax(X, nP, pos, lo, hi);
+    blockMinMax(lo, hi, s.rmin, s.rmax);
+    sampled = lo < hi;
+  }
+  if (!sampled) {
+    lo = R(INFINITY), hi = R(-INFINITY);
+    forEachValue(X, nP, pos, [&](R v, bool ok) {
+      if (ok) lo = fmin(lo, v), hi = fmax(hi, v);
+    });
+    blockMinMax(lo, hi, s.rmin, s.rmax);
+  }
 
   if (op == 5) {  // histogram of `count` bins on [lo, hi] (the request's range unless lo == hi there)
     if (rq[5] != rq[6]) lo = rq[5], hi = rq[6];
