@@ -118,7 +118,7 @@ __device__ __forceinline__ void forEachValue(const R* X, uint32_t nP, bool pos, 
 // and the ranks are still located exactly.  On long rows the range is the minimum and maximum of a sample,
 // every 16th block of 32 vectors (512 bytes, one 16-byte load per lane of a warp), about 1/16 of the row.
 constexpr uint32_t kSampleStride = 16;
-constexpr uint32_t kSampleMinVectors = 32 * kSampleStride * kRowWarps * 4;
+constexpr uint32_t kSampleMinVectors = 16384;  // rows of 64K floats or 32K doubles and more
 
 template <typename R>
 __device__ __forceinline__ bool canSample(const R* X, uint32_t nP) {
@@ -143,6 +143,49 @@ __device__ __forceinline__ void sampleMinMax(const R* X, uint32_t nP, bool pos, 
       const double2 q = __ldg(reinterpret_cast<const double2*>(X) + i);
       take(q.x), take(q.y);
     }
+  }
+}
+
+// The bins of ranks k and k1 >= k among the candidates counted in s.hist, `below` values ranking under bin 0:
+// pick = {bin of k, bin of k1, values under k's bin, count of k's bin}, as a walk over the bins in order would
+// find them.  One warp: lane l owns bins [128 l, 128 l + 128) (read skewed by l, free of bank conflicts), a
+// warp scan of the lanes' counts finds the lane holding each rank, and that lane walks its own bins.
+template <typename R>
+__device__ __forceinline__ void locateRanks(RowSmem<R>& s, uint32_t below, uint32_t k, uint32_t k1, uint32_t lane) {
+  constexpr uint32_t kPer = kBins / 32;
+  uint32_t own = 0;
+  for (uint32_t j = 0; j < kPer; ++j) own += s.hist[lane * kPer + ((j + lane) & (kPer - 1))];
+  uint32_t incl = own;
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t start = below + incl - own;  // values under this lane's first bin
+  const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, below + incl > k), m1 = __ballot_sync(0xFFFFFFFFu, below + incl > k1);
+  const uint32_t l0 = m0 ? __ffs(m0) - 1 : 31u, l1 = m1 ? __ffs(m1) - 1 : 31u;
+  auto walk = [&](uint32_t r, uint32_t& bin, uint32_t& under) {
+    uint32_t cum = start;
+    bin = lane * kPer + kPer - 1, under = cum;
+    for (uint32_t b = lane * kPer; b < lane * kPer + kPer; ++b) {
+      const uint32_t c = s.hist[b];
+      if (cum + c > r) {
+        bin = b, under = cum;
+        return;
+      }
+      cum += c;
+    }
+  };
+  if (lane == l0) {
+    uint32_t b0, under0;
+    walk(k, b0, under0);
+    if (!m0) b0 = kBins - 1, under0 = below;  // no rank k among the candidates (cannot happen): the last bin
+    s.pick[0] = b0, s.pick[2] = under0, s.pick[3] = s.hist[b0];
+  }
+  if (lane == l1) {
+    uint32_t b1, under1;
+    walk(k1, b1, under1);
+    if (!m1) b1 = kBins - 1;
+    s.pick[1] = b1;
   }
 }
 
@@ -290,20 +333,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
     });
     if ((tid & 31u) == 0 && zeroBin) atomicAdd(&s.hist[0], zeroBin);
     __syncthreads();
-    if (tid == 0) {
-      uint32_t cum = below, b0 = kBins - 1, b1 = kBins - 1, below0 = below;
-      bool f0 = false;
-      for (uint32_t b = 0; b < kBins; ++b) {
-        const uint32_t c = s.hist[b];
-        if (!f0 && cum + c > k) b0 = b, below0 = cum, f0 = true;
-        if (cum + c > k1) {
-          b1 = b;
-          break;
-        }
-        cum += c;
-      }
-      s.pick[0] = b0, s.pick[1] = b1, s.pick[2] = below0, s.pick[3] = s.hist[b0];
-    }
+    if (tid < 32) locateRanks(s, below, k, k1, tid);
     __syncthreads();
     const uint32_t b0 = s.pick[0], b1 = s.pick[1], below0 = s.pick[2], c0 = s.pick[3];
     if (b0 != b1) {
