@@ -32,8 +32,10 @@ constexpr int kHistBins = 3072;  // the reference's histogram-request limit (kPf
 
 template <typename R>
 struct RowSmem {
-  uint32_t hist[kBins];
-  R cand[kCap];
+  union {  // the histogram is read up to the choice of the bins; the candidates are gathered after it
+    uint32_t hist[kBins];
+    R cand[kCap];
+  };
   double dsum[kRowWarps];
   R rmin[kRowWarps], rmax[kRowWarps];
   uint32_t candCount;
@@ -211,7 +213,7 @@ __device__ void bitonicSort(R* a, uint32_t n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char raw[];
   RowSmem<R>& s = *reinterpret_cast<RowSmem<R>*>(raw);
   const RowJob<R> J = jobs[blockIdx.x];
