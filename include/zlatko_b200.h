@@ -82,7 +82,10 @@ zk_status zk_context_create(int device, zk_context** out);
 void zk_context_destroy(zk_context* ctx);
 const char* zk_last_error(const zk_context* ctx);
 int zk_abi_version(void);
-/* Runs the context's work on `stream` (a cudaStream_t; NULL: the context's own stream). */
+/* Runs the context's work on `stream` (a cudaStream_t; NULL: the context's own stream).  A book whose netting
+ * sets differ widely in shared-memory state forks its large-state revalue launch onto a second stream the
+ * context owns and joins it back with events, so work on `stream` stays ordered as usual (and a graph
+ * captured from `stream` holds both branches). */
 zk_status zk_context_set_stream(zk_context* ctx, void* stream);
 
 /* ---- the drop-in backend ------------------------------------------------------------------------ */
