@@ -681,8 +681,9 @@ void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normal
   }
   if (useCtxArena) {
     // Calls on the context arena synchronise before they return, so the context's page-locked staging is free;
-    // the wait below covers a previous call that failed with its copy in flight.
+    // the waits below cover a previous call that failed with its copy, or a forked launch, in flight.
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->side) ZK_CUDA(cudaStreamSynchronize(ctx->side));
     growStage(ctx->stageIn, ctx->stageInBytes, B.inputBytes);
     fillImage(B, normals, streams, ctx->stageIn);
     ZK_CUDA(cudaMemcpyAsync(B.base, ctx->stageIn, B.inputBytes, cudaMemcpyHostToDevice, ctx->stream));

@@ -91,23 +91,26 @@ __device__ __forceinline__ void loadTerm(const double* t, double (&r)[8]) {
   }
 }
 
-// Normal m of the current date, drawn on demand from a one-pair cache (normals are consumed in
-// increasing order, so every Box-Muller pair is drawn once).
+constexpr int kSimThreads = 256;  // threads per CTA of the simulate kernel (one path each)
+
+// The normals of one date: every Box-Muller pair drawn up front (independent of one another, so they overlap),
+// or the injected normals, into this thread's column of shared memory, normal m at col[m * kSimThreads].
 template <typename R>
-struct NormalStream {
-  uint32_t stream, j, pair;
-  R z0, z1, sign;
-  const R* injected;
-  uint32_t nStreams, injectedStream, nNormals;
-  __device__ __forceinline__ R get(uint32_t m) {
-    if (injected) return sign * injected[(static_cast<size_t>(j - 1) * nNormals + m) * nStreams + injectedStream];
-    if (m / 2 != pair) {
-      pair = m / 2;
-      gauss2(stream, j, pair, z0, z1);
-    }
-    return sign * ((m & 1u) ? z1 : z0);
+__device__ __forceinline__ void drawDate(uint32_t stream, uint32_t j, R sign, const R* injected, uint32_t nStreams,
+                                         uint32_t injectedStream, uint32_t nNormals, R* col) {
+  if (injected) {
+    for (uint32_t m = 0; m < nNormals; ++m)
+      col[m * kSimThreads] = sign * injected[(static_cast<size_t>(j - 1) * nNormals + m) * nStreams + injectedStream];
+    return;
   }
-};
+#pragma unroll 4
+  for (uint32_t q = 0; 2 * q < nNormals; ++q) {
+    R z0, z1;
+    gauss2(stream, j, q, z0, z1);
+    col[2 * q * kSimThreads] = sign * z0;
+    if (2 * q + 1 < nNormals) col[(2 * q + 1) * kSimThreads] = sign * z1;
+  }
+}
 
 }  // namespace
 
@@ -116,7 +119,9 @@ struct NormalStream {
 // hull_white.cpp:40-68, lognormal_asset.cpp:17-22, cir_intensity.cpp:49-66, in the statement order
 // of the reference kernel).
 template <typename R>
-__global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, CubeArgs<R> cb) {
+__global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs<R> sc, CubeArgs<R> cb) {
+  extern __shared__ __align__(16) unsigned char simRaw[];
+  R* col = reinterpret_cast<R*>(simRaw) + threadIdx.x;  // this thread's normals of the current date
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sc.nP) return;
   const uint32_t nP = sc.nP, nT = sc.nT;
@@ -127,8 +132,8 @@ __global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, 
     if (p & 1u) sign = R(-1);
   }
   const uint32_t injectedStream = sc.nStreams > 0 ? min(pathStream, sc.nStreams - 1) : 0u;
-  NormalStream<R> ns{pcg(pcg(sc.seed) ^ pcg(pathStream + 0x9E3779B9u)), 0, 0xFFFFFFFFu, R(0), R(0), sign, sc.normals,
-                     sc.nStreams, injectedStream, sc.nNormals};
+  const uint32_t stream = pcg(pcg(sc.seed) ^ pcg(pathStream + 0x9E3779B9u));
+  auto normal = [&](uint32_t m) { return col[m * kSimThreads]; };
   R x = R(0), lnD = R(0), D = R(1);
   R S[4], lnS[4] = {R(0), R(0), R(0), R(0)}, y[2], Y[2] = {R(0), R(0)};
 #pragma unroll
@@ -141,12 +146,11 @@ __global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, 
     R Qc[2] = {R(1), R(1)};
     if (j > 0) {
       const R* step = sc.steps + static_cast<size_t>(j) * kStepStride;
-      ns.j = j;
-      ns.pair = 0xFFFFFFFFu;
+      drawDate<R>(stream, j, sign, sc.normals, sc.nStreams, injectedStream, sc.nNormals, col);
       // Correlated drivers: each padded Cholesky row as two 4-term dot products (as the reference).
       R z[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) z[k] = static_cast<uint32_t>(k) < sc.nCorr ? ns.get(k) : R(0);
+      for (int k = 0; k < 8; ++k) z[k] = static_cast<uint32_t>(k) < sc.nCorr ? normal(k) : R(0);
       R w[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, 
         const R d1 = row[4] * z[4] + row[5] * z[5] + row[6] * z[6] + row[7] * z[7];
         w[i] = d0 + d1;
       }
-      const R zI = ns.get(sc.nCorr);
+      const R zI = normal(sc.nCorr);
       const R integratedRate = x * step[5] + step[2] * w[0] + step[3] * zI + step[4];
       x = x * step[0] + step[1] * w[0];
       lnD = lnD - integratedRate;
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(256) simulateKernel(const ScenarioArgs<R> sc, 
           R rem = rsqrt_(dt) * wc, remT = dt, yy = y[c], YY = Y[c];
           for (uint32_t s = 0; s < sc.substeps; ++s) {
             R dW = rem;
-            if (s + 1 < sc.substeps) dW = h / remT * rem + rsqrt_(fmax(h * (remT - h) / remT, R(0))) * ns.get(off + s);
+            if (s + 1 < sc.substeps) dW = h / remT * rem + rsqrt_(fmax(h * (remT - h) / remT, R(0))) * normal(off + s);
             rem -= dW;
             remT -= h;
             const R yp = fmax(yy, R(0));
@@ -896,8 +900,13 @@ cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream) {
 // ---------------------------------------------------------------------------------------------
 template <typename R>
 cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream) {
-  const uint32_t blocks = (sc.nP + 255) / 256;
-  simulateKernel<R><<<blocks, 256, 0, stream>>>(sc, cb);
+  const uint32_t blocks = (sc.nP + kSimThreads - 1) / kSimThreads;
+  const size_t smem = static_cast<size_t>(sc.nNormals) * kSimThreads * sizeof(R);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(simulateKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  simulateKernel<R><<<blocks, kSimThreads, smem, stream>>>(sc, cb);
   return cudaGetLastError();
 }
 
