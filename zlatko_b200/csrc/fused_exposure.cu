@@ -119,9 +119,25 @@ __device__ __forceinline__ void drawDate(uint32_t stream, uint32_t j, R sign, co
 // hull_white.cpp:40-68, lognormal_asset.cpp:17-22, cir_intensity.cpp:49-66, in the statement order
 // of the reference kernel).
 template <typename R>
-__global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs<R> sc, CubeArgs<R> cb) {
+__global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs<R> sc, CubeArgs<R> cb, bool bridgeTable) {
   extern __shared__ __align__(16) unsigned char simRaw[];
   R* col = reinterpret_cast<R*>(simRaw) + threadIdx.x;  // this thread's normals of the current date
+  // The Brownian-bridge coefficients of the CIR sub-steps are the same for every path: with bridgeTable the
+  // CTA computes them once, [date][sub-step][a, b] after the normals, by the very operations of the loop below.
+  const uint32_t nB = sc.substeps - 1;
+  R* bridge = reinterpret_cast<R*>(simRaw) + static_cast<size_t>(sc.nNormals) * kSimThreads;
+  if (bridgeTable) {
+    for (uint32_t jj = threadIdx.x + 1; jj < sc.nT; jj += blockDim.x) {
+      const R dt = sc.steps[static_cast<size_t>(jj) * kStepStride + 6], h = dt / static_cast<R>(sc.substeps);
+      R remT = dt;
+      for (uint32_t q = 0; q < nB; ++q) {
+        bridge[(static_cast<size_t>(jj) * nB + q) * 2] = h / remT;
+        bridge[(static_cast<size_t>(jj) * nB + q) * 2 + 1] = rsqrt_(fmax(h * (remT - h) / remT, R(0)));
+        remT -= h;
+      }
+    }
+    __syncthreads();
+  }
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sc.nP) return;
   const uint32_t nP = sc.nP, nT = sc.nT;
@@ -184,9 +200,14 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
           for (int i = 6; i >= 0; --i)
             if (wi == static_cast<uint32_t>(i)) wc = w[i];
           R rem = rsqrt_(dt) * wc, remT = dt, yy = y[c], YY = Y[c];
+          const R* bj = bridge + static_cast<size_t>(j) * nB * 2;
           for (uint32_t s = 0; s < sc.substeps; ++s) {
             R dW = rem;
-            if (s + 1 < sc.substeps) dW = h / remT * rem + rsqrt_(fmax(h * (remT - h) / remT, R(0))) * normal(off + s);
+            if (s + 1 < sc.substeps) {
+              const R a = bridgeTable ? bj[2 * s] : h / remT;
+              const R b = bridgeTable ? bj[2 * s + 1] : rsqrt_(fmax(h * (remT - h) / remT, R(0)));
+              dW = a * rem + b * normal(off + s);
+            }
             rem -= dW;
             remT -= h;
             const R yp = fmax(yy, R(0));
@@ -901,12 +922,15 @@ cudaError_t launchNestedIm(const ImArgs<R>& M, cudaStream_t stream) {
 template <typename R>
 cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cudaStream_t stream) {
   const uint32_t blocks = (sc.nP + kSimThreads - 1) / kSimThreads;
-  const size_t smem = static_cast<size_t>(sc.nNormals) * kSimThreads * sizeof(R);
+  const size_t normals = static_cast<size_t>(sc.nNormals) * kSimThreads * sizeof(R);
+  const size_t table = static_cast<size_t>(sc.nT) * (sc.substeps - 1) * 2 * sizeof(R);
+  const bool bridgeTable = sc.nC > 0 && sc.substeps > 1 && normals + table <= 64 * 1024;
+  const size_t smem = normals + (bridgeTable ? table : 0);
   if (smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(simulateKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
   }
-  simulateKernel<R><<<blocks, kSimThreads, smem, stream>>>(sc, cb);
+  simulateKernel<R><<<blocks, kSimThreads, smem, stream>>>(sc, cb, bridgeTable);
   return cudaGetLastError();
 }
 
