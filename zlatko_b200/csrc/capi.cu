@@ -6,6 +6,8 @@
 #include <cstring>
 #include <memory>
 #include <exception>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -17,6 +19,82 @@
 #include "zk_kernels.h"
 
 using namespace zk;
+
+namespace zk {
+namespace {
+
+// A fixed set of host threads for the per-call parallel loops (validating and lowering a book's plans, filling
+// its upload image): spawning and joining a dozen threads for each loop of each call costs about as much as
+// the loops.  run(n, fn) calls fn(w) for every w in [0, n) on the pool's threads and the caller's, and returns
+// when all are done.  Idle threads sleep on a condition variable.
+class HostPool {
+ public:
+  explicit HostPool(size_t threads) {
+    for (size_t t = 0; t < threads; ++t) threads_.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    wake_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+  size_t workers() const { return threads_.size() + 1; }
+  void run(size_t n, const std::function<void(size_t)>& fn) {
+    if (n <= 1 || threads_.empty()) {
+      for (size_t w = 0; w < n; ++w) fn(w);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      job_ = &fn, n_ = n, next_ = 0, pending_ = n, ++gen_;
+    }
+    wake_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void work() {
+    for (;;) {
+      const std::function<void(size_t)>* f;
+      size_t w;
+      {
+        std::lock_guard<std::mutex> lk(m_);
+        if (!job_ || next_ >= n_) return;
+        f = job_, w = next_++;
+      }
+      (*f)(w);
+      std::lock_guard<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        wake_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      work();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex m_;
+  std::condition_variable wake_, done_;
+  const std::function<void(size_t)>* job_ = nullptr;
+  size_t n_ = 0, next_ = 0, pending_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
+}  // namespace
+}  // namespace zk
 
 struct zk_context {
   int device = 0;
@@ -36,6 +114,7 @@ struct zk_context {
   // context's stream (fork and join events order the two); created by the first eager execute that splits.
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  std::unique_ptr<zk::HostPool> pool;  // created by the first call that validates more than a few plans
 };
 
 namespace {
@@ -394,12 +473,21 @@ struct Batch {
 
 // Validates and lowers the plans, on several host threads for a book of many plans; the first failure in plan
 // order is the one reported.
+// The context's host threads, created on first need (a call with several plans); null without a context.
+HostPool* hostPool(zk_context* ctx, size_t plans) {
+  if (!ctx || plans < 8) return ctx ? ctx->pool.get() : nullptr;
+  if (!ctx->pool) {
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    ctx->pool = std::make_unique<HostPool>(std::min<size_t>(hw, 16) - 1);
+  }
+  return ctx->pool.get();
+}
+
 template <typename R>
-void parseAll(const std::vector<View<R>>& views, std::vector<Plan<R>>& plans) {
+void parseAll(const std::vector<View<R>>& views, std::vector<Plan<R>>& plans, HostPool* pool) {
   const size_t n = views.size();
   plans.assign(n, Plan<R>());
-  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
-  const size_t workers = n >= 8 ? std::min<size_t>({hw, 16, n / 4}) : 1;
+  const size_t workers = n >= 8 && pool ? std::min<size_t>(pool->workers(), n / 4) : 1;
   std::vector<std::exception_ptr> errs(n);
   auto work = [&](size_t w) {
     for (size_t i = w; i < n; i += workers) {
@@ -413,9 +501,7 @@ void parseAll(const std::vector<View<R>>& views, std::vector<Plan<R>>& plans) {
   if (workers == 1) {
     work(0);
   } else {
-    std::vector<std::thread> pool;
-    for (size_t w = 0; w < workers; ++w) pool.emplace_back(work, w);
-    for (auto& t : pool) t.join();
+    pool->run(workers, work);
   }
   for (const auto& e : errs)
     if (e) std::rethrow_exception(e);
@@ -426,7 +512,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   auto B = std::make_unique<Batch<R>>();
   B->ctx = ctx;
   B->sink = sink;
-  parseAll(views, B->plans);
+  parseAll(views, B->plans, hostPool(ctx, views.size()));
   const size_t nPlans = B->plans.size();
   // ---- launch groups: plans sharing the scenario ----
   std::vector<int> launchOf(nPlans, -1);
@@ -534,18 +620,6 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
 
 // Fills the host image of the input region, once the arena base is known.
 // img: the host image to fill (B.inputBytes), B.image when null.
-// fn(w) for w in [0, workers) on that many host threads (the calling thread alone when workers is 1).
-template <class F>
-void onThreads(size_t workers, F&& fn) {
-  if (workers <= 1) {
-    fn(size_t{0});
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (size_t w = 0; w < workers; ++w) pool.emplace_back([&, w] { fn(w); });
-  for (auto& t : pool) t.join();
-}
-
 template <typename R>
 void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char* img = nullptr) {
   B.im.clear();
@@ -553,9 +627,16 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
     B.image.resize(B.inputBytes);
     img = B.image.data();
   }
-  // A book's tables are megabytes: the image is cleared and filled on up to 16 host threads.
-  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
-  const size_t workers = std::min<size_t>({hw, 16, std::max<size_t>(1, B.inputBytes >> 19)});
+  // A book's tables are megabytes: the image is cleared and filled on the context's host threads.
+  HostPool* pool = B.ctx ? B.ctx->pool.get() : nullptr;
+  const size_t workers = pool ? std::min<size_t>(pool->workers(), std::max<size_t>(1, B.inputBytes >> 19)) : 1;
+  auto onThreads = [&](size_t n, const std::function<void(size_t)>& fn) {
+    if (pool) {
+      pool->run(n, fn);
+    } else {
+      for (size_t w = 0; w < n; ++w) fn(w);
+    }
+  };
   onThreads(workers, [&](size_t w) {
     const size_t a = B.inputBytes * w / workers, b = B.inputBytes * (w + 1) / workers;
     std::memset(img + a, 0, b - a);
