@@ -157,6 +157,8 @@ zk_status zk_nest_run(zk_nest* nest, const uint64_t* scenario, const uint64_t* s
 zk_status zk_zero_bond_coefficients(const double* model, size_t model_len, const double* ts_te, size_t n, double* out);
 /* The number of event dates after t (0: nothing is paid after t). */
 zk_status zk_nest_events(const zk_nest* nest, uint64_t* events);
+/* Returns the nest's device memory to its context, which reuses it for later nests and frees it with the
+ * context: destroy every nest before its context. */
 void zk_nest_destroy(zk_nest* nest);
 
 /* ---- the adaptive nest's proxy (HermiteProxy, src/nested/adaptive_nested.cpp:145-277; host code) ---- */

@@ -115,7 +115,36 @@ struct zk_context {
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   std::unique_ptr<zk::HostPool> pool;  // created by the first call that validates more than a few plans
+  // Device blocks of destroyed nests, reused by later nests and freed with the context: a nest lives for one
+  // reporting date, and freeing its memory synchronises the device (tens of milliseconds a nest).
+  std::vector<std::pair<unsigned char*, size_t>> nestSpares;
 };
+
+namespace {
+
+// The smallest spare block of at least `need` bytes, else a new one; `bytes` receives its size.
+unsigned char* takeNestBlock(zk_context* ctx, size_t need, size_t& bytes) {
+  size_t best = ctx->nestSpares.size();
+  for (size_t i = 0; i < ctx->nestSpares.size(); ++i)
+    if (ctx->nestSpares[i].second >= need && (best == ctx->nestSpares.size() || ctx->nestSpares[i].second < ctx->nestSpares[best].second))
+      best = i;
+  if (best < ctx->nestSpares.size()) {
+    const auto blk = ctx->nestSpares[best];
+    ctx->nestSpares.erase(ctx->nestSpares.begin() + static_cast<std::ptrdiff_t>(best));
+    bytes = blk.second;
+    return blk.first;
+  }
+  unsigned char* p = nullptr;
+  if (cudaMalloc(reinterpret_cast<void**>(&p), need) != cudaSuccess) return nullptr;
+  bytes = need;
+  return p;
+}
+
+void giveNestBlock(zk_context* ctx, unsigned char* p, size_t bytes) {
+  if (p) ctx->nestSpares.emplace_back(p, bytes);
+}
+
+}  // namespace
 
 namespace {
 
@@ -1129,6 +1158,7 @@ void zk_context_destroy(zk_context* ctx) {
     cudaStreamSynchronize(ctx->side);
     cudaStreamDestroy(ctx->side);
   }
+  for (auto& blk : ctx->nestSpares) cudaFree(blk.first);
   if (ctx->fork) cudaEventDestroy(ctx->fork);
   if (ctx->join) cudaEventDestroy(ctx->join);
   if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1746,9 +1776,10 @@ struct zk_nest {
   size_t numScenarios = 0;
   unsigned char* djobs = nullptr;  // a round's jobs and payoffs, grown on demand
   size_t jobsBytes = 0;
-  ~zk_nest() {
-    if (dmem) cudaFree(dmem);
-    if (djobs) cudaFree(djobs);
+  size_t dmemBytes = 0;
+  ~zk_nest() {  // the blocks go back to the context for the next nest
+    giveNestBlock(ctx, dmem, dmemBytes);
+    giveNestBlock(ctx, djobs, jobsBytes);
   }
 };
 
@@ -1793,7 +1824,8 @@ zk_status zk_nest_create(zk_context* ctx, const double* model, size_t model_len,
     put(oTerm, P.terminals.data(), P.terminals.size() * 8), put(oChol, P.chol.data(), P.chol.size() * 8);
     put(oToday, P.fixToday.data(), P.fixToday.size() * 4), put(oX, x, n_scenarios * 8);
     put(oSpot, spot, n_scenarios * nA * 8), put(oFix, known, n_scenarios * n_slots * 8);
-    ZK_CUDA(cudaMalloc(reinterpret_cast<void**>(&N->dmem), off));
+    N->dmem = takeNestBlock(ctx, off, N->dmemBytes);
+    if (!N->dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "nest: %zu bytes of device memory", off);
     ZK_CUDA(cudaMemcpyAsync(N->dmem, img.data(), off, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
     unsigned char* b = N->dmem;
@@ -1831,10 +1863,12 @@ zk_status zk_nest_run(zk_nest* nest, const uint64_t* scenario, const uint64_t* s
     const size_t jobBytes = alignUp(num_jobs * 8);
     const size_t need = 3 * jobBytes + total * 8;
     if (nest->jobsBytes < need) {
-      if (nest->djobs) cudaFree(nest->djobs);
-      nest->djobs = nullptr, nest->jobsBytes = 0;
-      ZK_CUDA(cudaMalloc(reinterpret_cast<void**>(&nest->djobs), need));
-      nest->jobsBytes = need;
+      giveNestBlock(ctx, nest->djobs, nest->jobsBytes);
+      nest->djobs = takeNestBlock(ctx, need, nest->jobsBytes);
+      if (!nest->djobs) {
+        nest->jobsBytes = 0;
+        throw fail(ZK_ERR_OUT_OF_MEMORY, "nest: %zu bytes of device memory for a round", need);
+      }
     }
     unsigned char* d = nest->djobs;
     ZK_CUDA(cudaMemcpyAsync(d, scenario, num_jobs * 8, cudaMemcpyHostToDevice, ctx->stream));
