@@ -159,6 +159,26 @@ class HermiteProxy:
 _acc_sum = _seq_sum
 
 
+def _binned_seq_sums(columns: Sequence[np.ndarray], bins: np.ndarray, nb: int) -> np.ndarray:
+    """[k][b] = _seq_sum of columns[k] over the entries of bin b, in their order: every bin's entries are laid
+    out in one row of a zero-padded matrix (stable by position), and each row is summed in order."""
+    bins = np.asarray(bins, np.int64)
+    out = np.zeros((len(columns), nb))
+    if bins.size == 0:
+        return out
+    order = np.argsort(bins, kind="stable")
+    counts = np.bincount(bins, minlength=nb)
+    starts = np.cumsum(counts) - counts
+    sb = bins[order]
+    pos = np.arange(bins.size) - starts[sb]
+    width = int(counts.max())
+    for k, c in enumerate(columns):
+        m = np.zeros((nb, width))
+        m[sb, pos] = np.asarray(c, np.float64)[order]
+        out[k] = _row_sums(m)
+    return out
+
+
 def _row_sums(a: np.ndarray) -> np.ndarray:
     """_seq_sum of every row of a 2-D array."""
     return np.add.accumulate(a, axis=1)[:, -1] + 0.0
@@ -325,11 +345,8 @@ class ScenarioEstimates:
             d2 = d * d
             sampling = m2[ok] / (n[ok] - 1.0) / n[ok] + self.pv[ok]
             bins = self.bin[ok]
-            for b in range(nb):
-                sel = bins == b
-                cnt[b] = int(np.count_nonzero(sel))
-                if cnt[b]:
-                    s[b], sq[b], noise[b] = _seq_sum(d[sel]), _seq_sum(d2[sel]), _seq_sum(sampling[sel])
+            cnt = np.bincount(bins, minlength=nb).tolist()
+            s, sq, noise = (v.tolist() for v in _binned_seq_sums((d, d2, sampling), bins, nb))
             gsq, gnoise = _seq_sum(d2), _seq_sum(sampling)
         gcount = int(ok.size)
         glob = max(0.0, (gsq - gnoise) / float(gcount)) if gcount > 0 else 0.0
@@ -706,7 +723,9 @@ def estimate_uniform(weight: Optional[Sequence[float]], inner: InnerBatches, sce
     """estimateUniform (adaptive_nested.cpp:769-790): the classical nest with the same inner paths per scenario."""
     if inner_per_scenario < 1:
         raise ValueError("estimateUniform: at least one inner path per scenario")
-    outs = inner([(int(sc), derive_seed(seed, int(sc), 0, UNIFORM_TAG), inner_per_scenario) for sc in scenarios])
+    sc_ = np.asarray(scenarios, np.int64)
+    seeds = derive_seeds(seed, sc_, np.zeros(sc_.size, np.int64), UNIFORM_TAG).tolist()
+    outs = inner([(int(sc), sd, inner_per_scenario) for sc, sd in zip(sc_.tolist(), seeds)])
     value = [_seq_sum(np.asarray(o, np.float64)[:inner_per_scenario]) / float(inner_per_scenario) for o in outs]
     w = [1.0] * len(scenarios)
     if weight is not None and len(weight):
