@@ -115,22 +115,23 @@ struct zk_context {
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   std::unique_ptr<zk::HostPool> pool;  // created by the first call that validates more than a few plans
-  // Device blocks of destroyed nests, reused by later nests and freed with the context: a nest lives for one
-  // reporting date, and freeing its memory synchronises the device (tens of milliseconds a nest).
-  std::vector<std::pair<unsigned char*, size_t>> nestSpares;
+  // Device blocks of short-lived work (a nest lives for one reporting date, an AMC fit for one call), reused by
+  // later work and freed with the context: freeing device memory synchronises the device and took tens of
+  // milliseconds per nest.
+  std::vector<std::pair<unsigned char*, size_t>> spareBlocks;
 };
 
 namespace {
 
 // The smallest spare block of at least `need` bytes, else a new one; `bytes` receives its size.
-unsigned char* takeNestBlock(zk_context* ctx, size_t need, size_t& bytes) {
-  size_t best = ctx->nestSpares.size();
-  for (size_t i = 0; i < ctx->nestSpares.size(); ++i)
-    if (ctx->nestSpares[i].second >= need && (best == ctx->nestSpares.size() || ctx->nestSpares[i].second < ctx->nestSpares[best].second))
+unsigned char* takeBlock(zk_context* ctx, size_t need, size_t& bytes) {
+  size_t best = ctx->spareBlocks.size();
+  for (size_t i = 0; i < ctx->spareBlocks.size(); ++i)
+    if (ctx->spareBlocks[i].second >= need && (best == ctx->spareBlocks.size() || ctx->spareBlocks[i].second < ctx->spareBlocks[best].second))
       best = i;
-  if (best < ctx->nestSpares.size()) {
-    const auto blk = ctx->nestSpares[best];
-    ctx->nestSpares.erase(ctx->nestSpares.begin() + static_cast<std::ptrdiff_t>(best));
+  if (best < ctx->spareBlocks.size()) {
+    const auto blk = ctx->spareBlocks[best];
+    ctx->spareBlocks.erase(ctx->spareBlocks.begin() + static_cast<std::ptrdiff_t>(best));
     bytes = blk.second;
     return blk.first;
   }
@@ -140,8 +141,8 @@ unsigned char* takeNestBlock(zk_context* ctx, size_t need, size_t& bytes) {
   return p;
 }
 
-void giveNestBlock(zk_context* ctx, unsigned char* p, size_t bytes) {
-  if (p) ctx->nestSpares.emplace_back(p, bytes);
+void giveBlock(zk_context* ctx, unsigned char* p, size_t bytes) {
+  if (p) ctx->spareBlocks.emplace_back(p, bytes);
 }
 
 }  // namespace
@@ -983,6 +984,7 @@ template <typename R, typename ViewT>
 zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size_t streams, const uint32_t* degrees,
                  size_t numBermudans, R* termsOut, size_t termsLen) {
   void* dmem = nullptr;
+  size_t dmemBytes = 0;
   try {
     requireCtx(ctx);
     if (!plan || !termsOut || (numBermudans && !degrees)) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
@@ -1035,7 +1037,8 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     const size_t jobsBytes = jobs.size() * sizeof(AmcFitJob), datesBytes = std::max<size_t>(contDates.size(), 1) * 4;
     const size_t realisedBytes = numBermudans * static_cast<size_t>(P.nP) * 8, outBytes = static_cast<size_t>(slots) * 6 * 8;
     const size_t o1 = (jobsBytes + 255) / 256 * 256, o2 = o1 + (datesBytes + 255) / 256 * 256, o3 = o2 + (realisedBytes + 255) / 256 * 256;
-    ZK_CUDA(cudaMalloc(&dmem, o3 + outBytes));
+    dmem = takeBlock(ctx, o3 + outBytes, dmemBytes);
+    if (!dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "AMC fit: %zu bytes of device memory", o3 + outBytes);
     unsigned char* d = static_cast<unsigned char*>(dmem);
     ZK_CUDA(cudaMemcpyAsync(d, jobs.data(), jobsBytes, cudaMemcpyHostToDevice, ctx->stream));
     if (!contDates.empty()) ZK_CUDA(cudaMemcpyAsync(d + o1, contDates.data(), contDates.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -1051,7 +1054,7 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     ZK_CUDA(cudaMemcpyAsync(fitted.data(), d + o3, outBytes, cudaMemcpyDeviceToHost, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(&devErr, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
-    ZK_CUDA(cudaFree(dmem));
+    giveBlock(ctx, static_cast<unsigned char*>(dmem), dmemBytes);
     dmem = nullptr;
     if (devErr != 0) throw fail(ZK_ERR_CUDA, "the AMC fit reported error %u (normal equations not positive definite)", devErr);
     // The records as the reference writes them: center, 1 / scale, c0..c3 (fused_exposure.cpp:118-123).
@@ -1068,7 +1071,10 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     }
     return ZK_OK;
   } catch (const Failure& f) {
-    if (dmem) cudaFree(dmem);
+    if (dmem) {  // the block goes back only once nothing in flight can still use it
+      cudaStreamSynchronize(ctx->stream);
+      giveBlock(ctx, static_cast<unsigned char*>(dmem), dmemBytes);
+    }
     return record(ctx, f);
   }
 }
@@ -1158,7 +1164,7 @@ void zk_context_destroy(zk_context* ctx) {
     cudaStreamSynchronize(ctx->side);
     cudaStreamDestroy(ctx->side);
   }
-  for (auto& blk : ctx->nestSpares) cudaFree(blk.first);
+  for (auto& blk : ctx->spareBlocks) cudaFree(blk.first);
   if (ctx->fork) cudaEventDestroy(ctx->fork);
   if (ctx->join) cudaEventDestroy(ctx->join);
   if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1778,8 +1784,8 @@ struct zk_nest {
   size_t jobsBytes = 0;
   size_t dmemBytes = 0;
   ~zk_nest() {  // the blocks go back to the context for the next nest
-    giveNestBlock(ctx, dmem, dmemBytes);
-    giveNestBlock(ctx, djobs, jobsBytes);
+    giveBlock(ctx, dmem, dmemBytes);
+    giveBlock(ctx, djobs, jobsBytes);
   }
 };
 
@@ -1824,7 +1830,7 @@ zk_status zk_nest_create(zk_context* ctx, const double* model, size_t model_len,
     put(oTerm, P.terminals.data(), P.terminals.size() * 8), put(oChol, P.chol.data(), P.chol.size() * 8);
     put(oToday, P.fixToday.data(), P.fixToday.size() * 4), put(oX, x, n_scenarios * 8);
     put(oSpot, spot, n_scenarios * nA * 8), put(oFix, known, n_scenarios * n_slots * 8);
-    N->dmem = takeNestBlock(ctx, off, N->dmemBytes);
+    N->dmem = takeBlock(ctx, off, N->dmemBytes);
     if (!N->dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "nest: %zu bytes of device memory", off);
     ZK_CUDA(cudaMemcpyAsync(N->dmem, img.data(), off, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1863,8 +1869,8 @@ zk_status zk_nest_run(zk_nest* nest, const uint64_t* scenario, const uint64_t* s
     const size_t jobBytes = alignUp(num_jobs * 8);
     const size_t need = 3 * jobBytes + total * 8;
     if (nest->jobsBytes < need) {
-      giveNestBlock(ctx, nest->djobs, nest->jobsBytes);
-      nest->djobs = takeNestBlock(ctx, need, nest->jobsBytes);
+      giveBlock(ctx, nest->djobs, nest->jobsBytes);
+      nest->djobs = takeBlock(ctx, need, nest->jobsBytes);
       if (!nest->djobs) {
         nest->jobsBytes = 0;
         throw fail(ZK_ERR_OUT_OF_MEMORY, "nest: %zu bytes of device memory for a round", need);
@@ -1914,5 +1920,6 @@ zk_status zk_nest_events(const zk_nest* nest, uint64_t* events) {
 void zk_nest_destroy(zk_nest* nest) {
   if (!nest) return;
   cudaSetDevice(nest->ctx->device);
+  cudaStreamSynchronize(nest->ctx->stream);  // nothing of the nest's may still run when its blocks are reused
   delete nest;
 }
