@@ -81,6 +81,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
     for (uint32_t c = 0; c < BN; c += 16) {
       float v[16];
       umma::ld16(taddr + c, v);
+      // A thread holds 16 adjacent columns of its row: the bf16 outputs leave as two 16-byte stores each.
+      __align__(16) __nv_bfloat16 zb[16], hb[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const uint32_t n = n0 + c + j;
@@ -89,9 +91,18 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
         if (g.gradOf) z *= umma::siluGrad(__bfloat162float(g.gradOf[at]));
         if (g.C) g.C[at] = g.accumulate ? g.C[at] + z : z;
         const float h = g.act ? umma::silu(z) : z;
-        if (g.Z) g.Z[at] = __float2bfloat16_rn(z);
-        if (g.H) g.H[at] = __float2bfloat16_rn(h);
-        if (g.HT) g.HT[static_cast<size_t>(n) * g.M + row] = __float2bfloat16_rn(h);
+        zb[j] = __float2bfloat16_rn(z);
+        hb[j] = __float2bfloat16_rn(h);
+        if (g.HT) g.HT[static_cast<size_t>(n) * g.M + row] = hb[j];
+      }
+      const size_t at0 = static_cast<size_t>(row) * g.N + n0 + c;  // 32-byte aligned: N and n0 + c are multiples of 16
+      if (g.Z) {
+        reinterpret_cast<uint4*>(g.Z + at0)[0] = reinterpret_cast<const uint4*>(zb)[0];
+        reinterpret_cast<uint4*>(g.Z + at0)[1] = reinterpret_cast<const uint4*>(zb)[1];
+      }
+      if (g.H) {
+        reinterpret_cast<uint4*>(g.H + at0)[0] = reinterpret_cast<const uint4*>(hb)[0];
+        reinterpret_cast<uint4*>(g.H + at0)[1] = reinterpret_cast<const uint4*>(hb)[1];
       }
     }
   }

@@ -167,13 +167,13 @@ GemmArgs gemm(const bf16* A, const bf16* B, uint32_t M, uint32_t N, uint32_t K, 
 cudaError_t forward(SurrogateState& S, uint32_t rows, bool training) {
   const cudaStream_t s = S.stream;
   GemmArgs g = gemm(S.X, S.wb, rows, kHid, kIn, S.err);
-  g.bias = S.b1(), g.act = 1, g.Z = S.Z1, g.H = S.H1, g.HT = training ? S.H1T : nullptr;
+  g.bias = S.b1(), g.act = 1, g.Z = training ? S.Z1 : nullptr, g.H = S.H1, g.HT = training ? S.H1T : nullptr;  // Z: backward only
   SG_CUDA(launchGemm(g, s));
   g = gemm(S.H1, S.wb + SurrogateState::kW1, rows, kHid, kHid, S.err);
-  g.bias = S.b2(), g.act = 1, g.Z = S.Z2, g.H = S.H2, g.HT = training ? S.H2T : nullptr;
+  g.bias = S.b2(), g.act = 1, g.Z = training ? S.Z2 : nullptr, g.H = S.H2, g.HT = training ? S.H2T : nullptr;
   SG_CUDA(launchGemm(g, s));
   g = gemm(S.H2, S.wb + SurrogateState::kW1 + SurrogateState::kW2, rows, kHid, kHid, S.err);
-  g.bias = S.b3(), g.act = 1, g.Z = S.Z3, g.H = S.H3;
+  g.bias = S.b3(), g.act = 1, g.Z = training ? S.Z3 : nullptr, g.H = S.H3;
   SG_CUDA(launchGemm(g, s));
   return cudaSuccess;
 }
@@ -329,7 +329,7 @@ cudaError_t surrogateEpoch(SurrogateState& S, const float* dx, const float* dy, 
 }
 
 cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float* dout) {
-  const uint32_t chunk = 1u << 16;
+  const uint32_t chunk = 1u << 18;  // rows per pass: a few hundred passes for a book, a 0.9 GB workspace
   SG_CUDA(ensureWorkspace(S, chunk));
   for (size_t b0 = 0; b0 < n; b0 += chunk) {
     const uint32_t nb = static_cast<uint32_t>(std::min<size_t>(chunk, n - b0)), rows = (nb + 127) / 128 * 128;
