@@ -114,8 +114,9 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
 template <int BN>
 cudaError_t launchGemmBN(const GemmArgs& g, cudaStream_t s) {
   const size_t smemBytes = (128 + BN) * kGemmBK * 2;
-  // At least 57 KB per CTA keeps at most four CTAs (4 x 128 TMEM columns) on an SM.
-  const size_t dyn = smemBytes < 58 * 1024 ? 58 * 1024 : smemBytes;
+  // At least 55 KB per CTA (56 KB with the 1 KB the SM reserves per CTA) keeps at most four CTAs on an SM,
+  // 4 x 128 TMEM columns, so an allocation never waits on another CTA; 58 KB allowed only three.
+  const size_t dyn = smemBytes < 55 * 1024 ? 55 * 1024 : smemBytes;
   cudaError_t e = cudaFuncSetAttribute(gemmKernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn));
   if (e != cudaSuccess) return e;
   gemmKernel<BN><<<dim3(g.M / 128, g.N / BN), kGemmThreads, dyn, s>>>(g);
