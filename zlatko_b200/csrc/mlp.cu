@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
     umma::fenceAfterSync();
     const uint32_t row = m0 + warp * 32 + lane;
     const uint32_t taddr = tmem + ((warp * 32u) << 16);
+    float head = 0.0f;
 #pragma unroll 1
     for (uint32_t c = 0; c < BN; c += 16) {
       float v[16];
@@ -94,6 +95,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
         zb[j] = __float2bfloat16_rn(z);
         hb[j] = __float2bfloat16_rn(h);
         if (g.HT) g.HT[static_cast<size_t>(n) * g.M + row] = hb[j];
+        if (g.headOut) head += __bfloat162float(hb[j]) * g.headW[n];
       }
       const size_t at0 = static_cast<size_t>(row) * g.N + n0 + c;  // 32-byte aligned: N and n0 + c are multiples of 16
       if (g.Z) {
@@ -105,6 +107,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemmKernel(const GemmArgs g) {
         reinterpret_cast<uint4*>(g.H + at0)[1] = reinterpret_cast<const uint4*>(hb)[1];
       }
     }
+    if (g.headOut) g.headOut[row] = head + g.headB[0];
   }
   umma::fenceBeforeSync();
   __syncthreads();
@@ -128,6 +131,7 @@ cudaError_t launchGemmBN(const GemmArgs& g, cudaStream_t s) {
 cudaError_t launchGemm(const GemmArgs& g, cudaStream_t s) {
   if (g.M == 0 || g.N == 0 || g.K == 0) return cudaSuccess;
   if (g.M % 128 || g.N % 16 || g.K % 16) return cudaErrorInvalidValue;
+  if (g.headOut && g.N != 128) return cudaErrorInvalidValue;  // the head needs a row's columns in one tile
   if (g.N % 128 == 0) return launchGemmBN<128>(g, s);
   if (g.N % 64 == 0) return launchGemmBN<64>(g, s);
   if (g.N % 32 == 0) return launchGemmBN<32>(g, s);

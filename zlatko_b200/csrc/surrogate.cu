@@ -114,12 +114,24 @@ __global__ void prepareKernel(const float* __restrict__ x, const float* __restri
                               bf16* __restrict__ X, bf16* __restrict__ XT, float* __restrict__ ys) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  for (uint32_t k = 0; k < kIn; ++k) {
-    const float v = r < n ? (x[static_cast<size_t>(r) * kIn + k] - mean[k]) * inv[k] : 0.0f;
-    const bf16 b = __float2bfloat16_rn(v);
-    X[static_cast<size_t>(r) * kIn + k] = b;
-    if (XT) XT[static_cast<size_t>(k) * rows + r] = b;
+  // A row is 16 floats in (four 16-byte loads) and 16 bf16 out (two 16-byte stores).
+  float xv[kIn];
+  if (r < n) {
+#pragma unroll
+    for (int q = 0; q < kIn / 4; ++q) {
+      const float4 v = reinterpret_cast<const float4*>(x + static_cast<size_t>(r) * kIn)[q];
+      xv[4 * q] = v.x, xv[4 * q + 1] = v.y, xv[4 * q + 2] = v.z, xv[4 * q + 3] = v.w;
+    }
   }
+  __align__(16) bf16 out[kIn];
+#pragma unroll
+  for (uint32_t k = 0; k < kIn; ++k) {
+    const float v = r < n ? (xv[k] - mean[k]) * inv[k] : 0.0f;
+    out[k] = __float2bfloat16_rn(v);
+    if (XT) XT[static_cast<size_t>(k) * rows + r] = out[k];
+  }
+  reinterpret_cast<uint4*>(X + static_cast<size_t>(r) * kIn)[0] = reinterpret_cast<const uint4*>(out)[0];
+  reinterpret_cast<uint4*>(X + static_cast<size_t>(r) * kIn)[1] = reinterpret_cast<const uint4*>(out)[1];
   if (ys) ys[r] = r < n ? (y[r] - yMean) * yInv : 0.0f;
 }
 
@@ -164,7 +176,8 @@ GemmArgs gemm(const bf16* A, const bf16* B, uint32_t M, uint32_t N, uint32_t K, 
 
 // Forward pass of `rows` (a multiple of 128) standardised rows in S.X: Z and H of the three hidden layers
 // (and the transposed H1, H2 that the weight gradients read, when training).
-cudaError_t forward(SurrogateState& S, uint32_t rows, bool training) {
+// headOut (inference): the last layer's epilogue evaluates the linear head into it and H3 is not written.
+cudaError_t forward(SurrogateState& S, uint32_t rows, bool training, float* headOut = nullptr) {
   const cudaStream_t s = S.stream;
   GemmArgs g = gemm(S.X, S.wb, rows, kHid, kIn, S.err);
   g.bias = S.b1(), g.act = 1, g.Z = training ? S.Z1 : nullptr, g.H = S.H1, g.HT = training ? S.H1T : nullptr;  // Z: backward only
@@ -173,7 +186,8 @@ cudaError_t forward(SurrogateState& S, uint32_t rows, bool training) {
   g.bias = S.b2(), g.act = 1, g.Z = training ? S.Z2 : nullptr, g.H = S.H2, g.HT = training ? S.H2T : nullptr;
   SG_CUDA(launchGemm(g, s));
   g = gemm(S.H2, S.wb + SurrogateState::kW1 + SurrogateState::kW2, rows, kHid, kHid, S.err);
-  g.bias = S.b3(), g.act = 1, g.Z = training ? S.Z3 : nullptr, g.H = S.H3;
+  g.bias = S.b3(), g.act = 1, g.Z = training ? S.Z3 : nullptr, g.H = headOut ? nullptr : S.H3;
+  if (headOut) g.headW = S.w4(), g.headB = S.b4(), g.headOut = headOut;
   SG_CUDA(launchGemm(g, s));
   return cudaSuccess;
 }
@@ -335,8 +349,7 @@ cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float
     const uint32_t nb = static_cast<uint32_t>(std::min<size_t>(chunk, n - b0)), rows = (nb + 127) / 128 * 128;
     prepareKernel<<<blocksOf(rows, 128), 128, 0, S.stream>>>(dx + b0 * kIn, nullptr, nb, rows, S.scale, S.scale + 16, 0.0f, 1.0f,
                                                               S.X, nullptr, nullptr);
-    SG_CUDA(forward(S, rows, false));
-    headKernel<<<rows / 128, 128, 0, S.stream>>>(S.H3, S.w4(), S.b4(), nullptr, nb, S.pred, nullptr, nullptr);
+    SG_CUDA(forward(S, rows, false, S.pred));  // the head runs in the last layer's epilogue
     unscaleKernel<<<blocksOf(nb, 256), 256, 0, S.stream>>>(S.pred, nb, S.yMean, S.yScale, dout + b0);
   }
   return cudaGetLastError();

@@ -118,6 +118,11 @@ struct GemmArgs {
   uint32_t act;         // 0 identity, 1 SiLU
   uint32_t accumulate;
   uint32_t* err;
+  // Fused linear head (N = 128, one column tile): headOut[row] = sum_n bf16(h[row][n]) headW[n] + headB[0],
+  // summed over n in order; or null.
+  const float* headW;
+  const float* headB;
+  float* headOut;
 };
 cudaError_t launchGemm(const GemmArgs& g, cudaStream_t stream);
 
