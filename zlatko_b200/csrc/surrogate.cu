@@ -345,65 +345,93 @@ cudaError_t surrogateEpoch(SurrogateState& S, const float* dx, const float* dy, 
 // ---- inference: the whole network per 128-row tile in one kernel ----------------------------------------
 namespace {
 
-constexpr uint32_t kMlpThreads = 128;          // one epilogue row per thread (TMEM lane)
-constexpr uint32_t kMlpWaitLimit = 1u << 26;   // polls of an MMA-completion barrier before the kernel gives up
+constexpr uint32_t kMlpGroups = 4;                    // warpgroups per CTA, each running its own tiles
+constexpr uint32_t kMlpThreads = 128 * kMlpGroups;
+constexpr uint32_t kMlpWaitLimit = 1u << 26;          // polls of an MMA-completion barrier before giving up
 // Shared memory (canonical K-major tiles, no swizzle): W1 [128 x 16], W2 and W3 [128 x 128] as the B operands,
-// the tile's inputs [128 x 16] and its hidden activations [128 x 128] as the A operands.
+// shared by the warpgroups; then per warpgroup its tile's inputs [128 x 16] and hidden activations [128 x 128]
+// as the A operands; then b1 | b2 | b3 | w4 | b4.
 constexpr uint32_t kMlpW1 = 0, kMlpW2 = kMlpW1 + kHid * kIn * 2, kMlpW3 = kMlpW2 + kHid * kHid * 2;
-constexpr uint32_t kMlpX = kMlpW3 + kHid * kHid * 2, kMlpH = kMlpX + 128 * kIn * 2, kMlpSmem = kMlpH + 128 * kHid * 2;
+constexpr uint32_t kMlpTiles = kMlpW3 + kHid * kHid * 2, kMlpTileBytes = 128 * kIn * 2 + 128 * kHid * 2;
+constexpr uint32_t kMlpParams = kMlpTiles + kMlpGroups * kMlpTileBytes;
+constexpr uint32_t kMlpSmem = kMlpParams + (4 * kHid + 4) * 4;
 
-// Copies a row-major [rows][K] bf16 block into the canonical K-major layout, 16 bytes per cp.async.
-__device__ __forceinline__ void stageKMajor(unsigned char* dst, const bf16* src, uint32_t rows, uint32_t K) {
+// Copies a row-major [rows][K] bf16 block into the canonical K-major layout, 16 bytes per cp.async, by the
+// `threads` threads numbered from 0 by t.
+__device__ __forceinline__ void stageKMajor(unsigned char* dst, const bf16* src, uint32_t rows, uint32_t K, uint32_t t,
+                                            uint32_t threads) {
   const uint32_t groups = K / 8;
-  for (uint32_t v = threadIdx.x; v < rows * groups; v += kMlpThreads) {
+  for (uint32_t v = t; v < rows * groups; v += threads) {
     const uint32_t r = v / groups, kg = v % groups;
     umma::cpAsync16(dst + umma::kMajorOffset(r, kg * 8, rows), src + static_cast<size_t>(r) * K + kg * 8);
   }
 }
 
-// pred[row] for `rows` (a multiple of 128) standardised inputs X [rows][16]: each CTA loads the weights once
-// and runs tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Per tile, layer l is one chain of K/16 MMAs into
-// the CTA's 128 TMEM columns (the same products, in the same order, as the layer-by-layer GEMMs), and its
-// epilogue (bias, SiLU, BF16) writes the activations straight into the next layer's A tile in shared memory;
-// the last epilogue evaluates the linear head as gemmKernel's fused head does.  The next tile's inputs load
-// while the tile's layers run.
-__global__ void __launch_bounds__(kMlpThreads) mlpInferKernel(const bf16* __restrict__ X, const bf16* __restrict__ wb,
-                                                              const float* __restrict__ b1, const float* __restrict__ b2,
-                                                              const float* __restrict__ b3, const float* __restrict__ w4,
-                                                              const float* __restrict__ b4, uint32_t rows,
-                                                              float* __restrict__ pred, uint32_t* __restrict__ err) {
+// Barrier of one warpgroup (named barrier 1 + g, 128 threads), optionally and-reducing a predicate.
+__device__ __forceinline__ void groupSync(uint32_t g) { asm volatile("bar.sync %0, 128;" ::"r"(1u + g) : "memory"); }
+__device__ __forceinline__ bool groupAnd(bool v, uint32_t g) {
+  uint32_t r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, %2, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+               : "=r"(r)
+               : "r"(v ? 1u : 0u), "r"(1u + g)
+               : "memory");
+  return r != 0;
+}
+
+// pred[row] for `rows` (a multiple of 128) standardised inputs X [rows][16].  One CTA per SM loads the weights
+// once; each of its warpgroups runs tiles (blockIdx.x * 4 + g), stepping by 4 gridDim.x, with its own 128 TMEM
+// columns, activation tile and mbarrier, so four tiles' epilogues keep the SM busy.  Per tile, layer l is one
+// chain of K/16 MMAs (the same products, in the same order, as the layer-by-layer GEMMs), and its epilogue
+// (bias, SiLU, BF16) writes the activations straight into the next layer's A tile in shared memory; the last
+// epilogue evaluates the linear head as gemmKernel's fused head does.  The next tile's inputs load while the
+// tile's layers run.
+__global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __restrict__ X, const bf16* __restrict__ wb,
+                                                                 const float* __restrict__ b1, const float* __restrict__ b2,
+                                                                 const float* __restrict__ b3, const float* __restrict__ w4,
+                                                                 const float* __restrict__ b4, uint32_t rows,
+                                                                 float* __restrict__ pred, uint32_t* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bars[kMlpGroups];
   __shared__ uint32_t tslot;
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const uint32_t tiles = rows / 128;
-  if (warp == 0) umma::alloc(&tslot, 128);
-  if (tid == 0) mbarInit(&bar, 1);
-  stageKMajor(sm + kMlpW1, wb, kHid, kIn);
-  stageKMajor(sm + kMlpW2, wb + SurrogateState::kW1, kHid, kHid);
-  stageKMajor(sm + kMlpW3, wb + SurrogateState::kW1 + SurrogateState::kW2, kHid, kHid);
-  if (blockIdx.x < tiles) stageKMajor(sm + kMlpX, X + static_cast<size_t>(blockIdx.x) * 128 * kIn, 128, kIn);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, g = warp >> 2, gt = tid & 127u;
+  const uint32_t tiles = rows / 128, stride = gridDim.x * kMlpGroups;
+  unsigned char* xs = sm + kMlpTiles + g * kMlpTileBytes;
+  unsigned char* hs = xs + 128 * kIn * 2;
+  float* par = reinterpret_cast<float*>(sm + kMlpParams);  // b1 | b2 | b3 | w4 | b4
+  uint64_t* bar = &bars[g];
+  if (warp == 0) umma::alloc(&tslot, 128 * kMlpGroups);
+  if (gt == 0) mbarInit(bar, 1);
+  for (uint32_t k = tid; k < kHid; k += kMlpThreads)
+    par[k] = b1[k], par[kHid + k] = b2[k], par[2 * kHid + k] = b3[k], par[3 * kHid + k] = w4[k];
+  if (tid == 0) par[4 * kHid] = b4[0];
+  stageKMajor(sm + kMlpW1, wb, kHid, kIn, tid, kMlpThreads);
+  stageKMajor(sm + kMlpW2, wb + SurrogateState::kW1, kHid, kHid, tid, kMlpThreads);
+  stageKMajor(sm + kMlpW3, wb + SurrogateState::kW1 + SurrogateState::kW2, kHid, kHid, tid, kMlpThreads);
+  uint32_t t = blockIdx.x * kMlpGroups + g;
+  if (t < tiles) stageKMajor(xs, X + static_cast<size_t>(t) * 128 * kIn, 128, kIn, gt, 128);
   umma::cpAsyncCommit();
+  umma::cpAsyncWaitAll();  // the weights are read by every warpgroup: all of them land before anyone starts
+  umma::fenceAsyncShared();
   umma::fenceBeforeSync();
   __syncthreads();
   umma::fenceAfterSync();
-  const uint32_t tmem = tslot, taddr = tmem + ((warp * 32u) << 16);
+  const uint32_t tmem = tslot + g * 128u, taddr = tmem + (((warp & 3u) * 32u) << 16);
   constexpr uint32_t idesc = umma::idescBf16(128, kHid);
   uint32_t phase = 0;
   bool ok = true, pending = false;
-  // One layer: the MMA chain A (at aOff, K wide) x B (at bOff) into TMEM, then the wait for its completion.
-  auto layer = [&](uint32_t aOff, uint32_t bOff, uint32_t K) {
-    if (tid == 0) {
+  // One layer: the MMA chain A (K wide) x B into this warpgroup's TMEM columns, then the wait for it.
+  auto layer = [&](const unsigned char* a, const unsigned char* b, uint32_t K) {
+    if (gt == 0) {
       umma::fenceAfterSync();
       for (uint32_t i = 0; i < K / 16; ++i) {
-        const uint64_t da = umma::desc(umma::smem(sm + aOff) + i * 2 * 128 * 16, 128 * 16, 128);
-        const uint64_t db = umma::desc(umma::smem(sm + bOff) + i * 2 * kHid * 16, kHid * 16, 128);
+        const uint64_t da = umma::desc(umma::smem(a) + i * 2 * 128 * 16, 128 * 16, 128);
+        const uint64_t db = umma::desc(umma::smem(b) + i * 2 * kHid * 16, kHid * 16, 128);
         umma::mma(tmem, da, db, idesc, i > 0);
       }
-      umma::commit(&bar);
+      umma::commit(bar);
     }
-    const bool done = mbarWait(&bar, phase, kMlpWaitLimit);
-    ok = __syncthreads_and(done) != 0;
+    const bool done = mbarWait(bar, phase, kMlpWaitLimit);
+    ok = groupAnd(done, g);
     pending = !ok;
     phase ^= 1u;
     umma::fenceAfterSync();
@@ -420,45 +448,45 @@ __global__ void __launch_bounds__(kMlpThreads) mlpInferKernel(const bf16* __rest
       for (int j = 0; j < 16; ++j) {
         const float z = v[j] + bias[c + j];
         hb[j] = __float2bfloat16_rn(umma::silu(z));
-        if (head) acc += __bfloat162float(hb[j]) * w4[c + j];
+        if (head) acc += __bfloat162float(hb[j]) * par[3 * kHid + c + j];
       }
       if (!head) {
-        *reinterpret_cast<uint4*>(sm + kMlpH + umma::kMajorOffset(tid, c, 128)) = reinterpret_cast<const uint4*>(hb)[0];
-        *reinterpret_cast<uint4*>(sm + kMlpH + umma::kMajorOffset(tid, c + 8, 128)) = reinterpret_cast<const uint4*>(hb)[1];
+        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c, 128)) = reinterpret_cast<const uint4*>(hb)[0];
+        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c + 8, 128)) = reinterpret_cast<const uint4*>(hb)[1];
       }
     }
-    if (head) pred[row] = acc + b4[0];
+    if (head) pred[row] = acc + par[4 * kHid];
     umma::fenceAsyncShared();  // the activations, written through the generic proxy, for the next MMAs
     umma::fenceBeforeSync();
-    __syncthreads();
+    groupSync(g);
   };
-  for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-    umma::cpAsyncWaitAll();  // this tile's inputs (and, on the first tile, the weights)
+  for (; t < tiles && ok; t += stride) {
+    umma::cpAsyncWaitAll();  // this tile's inputs
     umma::fenceAsyncShared();
     umma::fenceBeforeSync();
-    __syncthreads();
-    layer(kMlpX, kMlpW1, kIn);
+    groupSync(g);
+    layer(xs, sm + kMlpW1, kIn);
     if (!ok) break;
     // The inputs were consumed: the next tile's load overlaps this tile's layers.
-    if (t + gridDim.x < tiles) stageKMajor(sm + kMlpX, X + static_cast<size_t>(t + gridDim.x) * 128 * kIn, 128, kIn);
+    if (t + stride < tiles) stageKMajor(xs, X + static_cast<size_t>(t + stride) * 128 * kIn, 128, kIn, gt, 128);
     umma::cpAsyncCommit();
-    const uint32_t row = t * 128 + tid;  // TMEM lane = thread = row of the tile
-    epilogue(b1, false, row);
-    layer(kMlpH, kMlpW2, kHid);
+    const uint32_t row = t * 128 + gt;  // TMEM lane = thread of the warpgroup = row of the tile
+    epilogue(par, false, row);
+    layer(hs, sm + kMlpW2, kHid);
     if (!ok) break;
-    epilogue(b2, false, row);
-    layer(kMlpH, kMlpW3, kHid);
+    epilogue(par + kHid, false, row);
+    layer(hs, sm + kMlpW3, kHid);
     if (!ok) break;
-    epilogue(b3, true, row);
+    epilogue(par + 2 * kHid, true, row);
   }
   umma::cpAsyncWaitAll();
   if (!ok) {
-    if (tid == 0) atomicExch(err, kDevTimeout);
-    if (pending) mbarWait(&bar, phase ^ 1u, kMlpWaitLimit);  // the MMAs in flight, before the TMEM goes away
+    if (gt == 0) atomicExch(err, kDevTimeout);
+    if (pending) mbarWait(bar, phase ^ 1u, kMlpWaitLimit);  // the MMAs in flight, before the TMEM goes away
   }
   umma::fenceBeforeSync();
   __syncthreads();
-  if (warp == 0) umma::dealloc(tmem, 128);
+  if (warp == 0) umma::dealloc(tslot, 128 * kMlpGroups);
 }
 
 }  // namespace
@@ -470,7 +498,7 @@ cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float
     const uint32_t nb = static_cast<uint32_t>(std::min<size_t>(chunk, n - b0)), rows = (nb + 127) / 128 * 128;
     prepareKernel<<<blocksOf(rows, 128), 128, 0, S.stream>>>(dx + b0 * kIn, nullptr, nb, rows, S.scale, S.scale + 16, 0.0f, 1.0f,
                                                               S.X, nullptr, nullptr);
-    const uint32_t tiles = rows / 128, grid = std::min<uint32_t>(tiles, 2 * 148);
+    const uint32_t tiles = rows / 128, grid = std::min<uint32_t>((tiles + kMlpGroups - 1) / kMlpGroups, 148);
     SG_CUDA(cudaFuncSetAttribute(mlpInferKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMlpSmem)));
     mlpInferKernel<<<grid, kMlpThreads, kMlpSmem, S.stream>>>(S.X, S.wb, S.b1(), S.b2(), S.b3(), S.w4(), S.b4(), rows, S.pred, S.err);
     SG_CUDA(cudaGetLastError());
