@@ -445,10 +445,13 @@ __global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __r
       umma::ld16(taddr + c, v);
       __align__(16) bf16 hb[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const float z = v[j] + bias[c + j];
-        hb[j] = __float2bfloat16_rn(umma::silu(z));
-        if (head) acc += __bfloat162float(hb[j]) * par[3 * kHid + c + j];
+      for (int j = 0; j < 16; j += 2) {  // two activations per conversion (each rounded to nearest even)
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(umma::silu(v[j] + bias[c + j]), umma::silu(v[j + 1] + bias[c + j + 1]));
+        hb[j] = h2.x, hb[j + 1] = h2.y;
+        if (head) {
+          acc += __bfloat162float(hb[j]) * par[3 * kHid + c + j];
+          acc += __bfloat162float(hb[j + 1]) * par[3 * kHid + c + j + 1];
+        }
       }
       if (!head) {
         *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c, 128)) = reinterpret_cast<const uint4*>(hb)[0];
