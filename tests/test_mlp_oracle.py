@@ -1,5 +1,5 @@
 """The FP64 surrogate oracle's gradient against central finite differences of its own loss (CPU): the oracle is
-pinned by calculus before it judges the GPU."""
+pinned by calculus before it checks the GPU."""
 import numpy as np
 
 from oracle import mlp_oracle as O
