@@ -569,7 +569,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
       L.perTrade = L.perTrade || P.nTr > 0;
       L.probes = L.probes || P.probes;
-      L.lean = L.lean && !P.amcOrProbe;
+      L.lean = L.lean && !P.amcOrProbe && P.nS == static_cast<uint32_t>(kStatsPerDate);  // lean kernels know nS
     }
     const Plan<R>& P0 = B->plans[L.planIdx.front()];
     ScenarioArgs<R>& sc = L.sc;

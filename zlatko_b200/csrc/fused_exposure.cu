@@ -326,7 +326,8 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   const R* __restrict__ table = A.table;
   R* __restrict__ expo = A.expo;
   const uint32_t nP = cb.nP, nT = cb.nT;
-  const uint32_t nSlots = A.nSlots, ringLen = A.ring, nS = A.nS, ctype = A.ctype;
+  // Lean launches hold only plans with the netting set's 8 statistics per date (no per-trade ones).
+  const uint32_t nSlots = A.nSlots, ringLen = A.ring, nS = kLean ? static_cast<uint32_t>(kStatsPerDate) : A.nS, ctype = A.ctype;
   const bool hasCsa = A.hasCsa != 0, usesAssets = A.usesAssets != 0;
   R* __restrict__ const rowEP = expo + static_cast<size_t>(A.rowEP) * nP;
   const bool moreRows = A.rowDV != kNoRow || A.rowE != kNoRow || A.rowV != kNoRow || A.rowC != kNoRow;
