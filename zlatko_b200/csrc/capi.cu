@@ -569,7 +569,9 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
       L.perTrade = L.perTrade || P.nTr > 0;
       L.probes = L.probes || P.probes;
-      L.lean = L.lean && !P.amcOrProbe && P.nS == static_cast<uint32_t>(kStatsPerDate);  // lean kernels know nS
+      // Lean kernels know nS and write no gross or per-trade rows.
+      L.lean = L.lean && !P.amcOrProbe && P.nS == static_cast<uint32_t>(kStatsPerDate) && P.rowGross == kNoRow &&
+               P.rowTrades == kNoRow;
     }
     const Plan<R>& P0 = B->plans[L.planIdx.front()];
     ScenarioArgs<R>& sc = L.sc;

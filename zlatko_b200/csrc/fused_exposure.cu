@@ -638,12 +638,12 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
           if (A.rowV != kNoRow) expo[(A.rowV + k) * nP + pi] = value[i];
           if (A.rowC != kNoRow) expo[(A.rowC + k) * nP + pi] = collateral;
         }
-        if (A.rowGross != kNoRow) {
+        if (!kLean && A.rowGross != kNoRow) {
           R gross = R(0);
           for (uint32_t g = 0; g < nTr; ++g) gross += fmax(vt(g, i), R(0));
           expo[(A.rowGross + k) * nP + pi] = gross;
         }
-        if (A.rowTrades != kNoRow)
+        if (!kLean && A.rowTrades != kNoRow)
           for (uint32_t g = 0; g < nTr; ++g) expo[(A.rowTrades + g * A.nR + k) * nP + pi] = vt(g, i);
       }
       if (!kLean && !kSink && rs > 0 && A.imState && act[i]) {  // the start of this path's inner paths
