@@ -468,6 +468,9 @@ struct Batch {
     // Netting sets in decreasing order of shared-memory state: [splitAt, n) keep at most kSmallStateWords words
     // per path (at most smallStateMax) and may run as a second launch with more resident CTAs.
     size_t splitAt = 0, smallStateMax = 0;
+    // Every netting set of [0, splitAt) (cashBig), of [splitAt, n) (cashSmall), of the launch (cashAll) has a cash
+    // CSA with a margin-call look-back of at most one date.
+    bool cashBig = true, cashSmall = true, cashAll = true;
     bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
   };
@@ -564,6 +567,12 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     L.splitAt = L.planIdx.size();
     while (L.splitAt > 0 && B->plans[L.planIdx[L.splitAt - 1]].stateWords <= static_cast<uint32_t>(kSmallStateWords)) --L.splitAt;
     if (L.splitAt < L.planIdx.size()) L.smallStateMax = B->plans[L.planIdx[L.splitAt]].stateWords;
+    for (size_t k = 0; k < L.planIdx.size(); ++k) {
+      const auto& P = B->plans[L.planIdx[k]];
+      const bool cash = P.hasCsa && P.ctype == 0 && P.ring <= 2;
+      (k < L.splitAt ? L.cashBig : L.cashSmall) = (k < L.splitAt ? L.cashBig : L.cashSmall) && cash;
+      L.cashAll = L.cashAll && cash;
+    }
     for (uint32_t k : L.planIdx) {
       const auto& P = B->plans[k];
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
@@ -830,7 +839,8 @@ void execute(Batch<R>& B, bool capturing = false) {
     // their own launch, compiled for more resident CTAs than the shared memory of the largest allows.
     const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < n;
     if (!split) {
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s));
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s, false,
+                               L.lean && !L.perTrade && !B.sink && L.cashAll));
       continue;
     }
     const uint32_t big = static_cast<uint32_t>(L.splitAt);
@@ -845,11 +855,11 @@ void execute(Batch<R>& B, bool capturing = false) {
     if (fork) {
       ZK_CUDA(cudaEventRecord(ctx->fork, s));
       ZK_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, ctx->side));
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, ctx->side, false, L.cashBig));
     } else if (big > 0) {
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, s));
+      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, s, false, L.cashBig));
     }
-    ZK_CUDA(launchRevalue<R>(L.cb, ns + big, n - big, tiles, L.smallStateMax, false, false, true, B.ppt, s, true));
+    ZK_CUDA(launchRevalue<R>(L.cb, ns + big, n - big, tiles, L.smallStateMax, false, false, true, B.ppt, s, true, L.cashSmall));
     if (fork) {
       ZK_CUDA(cudaEventRecord(ctx->join, ctx->side));
       ZK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));

@@ -309,7 +309,9 @@ constexpr int revalueMinBlocks() {
 
 // Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
 // statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
-template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean, bool kSmallState = false>
+// kCash: every netting set of the launch has a cash CSA whose margin calls look back at most one date, so the
+// collateral code is that case alone (no securities price, no shared-memory ring).
+template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean, bool kSmallState = false, bool kCash = false>
 __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallState>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -327,8 +329,9 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   R* __restrict__ expo = A.expo;
   const uint32_t nP = cb.nP, nT = cb.nT;
   // Lean launches hold only plans with the netting set's 8 statistics per date (no per-trade ones).
-  const uint32_t nSlots = A.nSlots, ringLen = A.ring, nS = kLean ? static_cast<uint32_t>(kStatsPerDate) : A.nS, ctype = A.ctype;
-  const bool hasCsa = A.hasCsa != 0, usesAssets = A.usesAssets != 0;
+  const uint32_t nSlots = A.nSlots, ringLen = kCash ? 2u : A.ring, nS = kLean ? static_cast<uint32_t>(kStatsPerDate) : A.nS;
+  const uint32_t ctype = kCash ? 0u : A.ctype;
+  const bool hasCsa = kCash || A.hasCsa != 0, usesAssets = A.usesAssets != 0;
   R* __restrict__ const rowEP = expo + static_cast<size_t>(A.rowEP) * nP;
   const bool moreRows = A.rowDV != kNoRow || A.rowE != kNoRow || A.rowV != kNoRow || A.rowC != kNoRow;
   uint32_t pth[PPT], pp[PPT];
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   R held[PPT], prevDE[PPT], prevQ[PPT], prevRV[PPT], ex[4][PPT];
   // Look-back of at most one date (the margin-call dates t - MPR sit on the grid): the previous date's value
   // and collateral price in registers instead of the shared-memory ring.
-  const bool shortLook = ringLen <= 2;
+  const bool shortLook = kCash || ringLen <= 2;
   R vPrev[PPT], pPrev[PPT];
 #pragma unroll
   for (int i = 0; i < PPT; ++i) vPrev[i] = R(0), pPrev[i] = R(1);
@@ -943,7 +946,7 @@ size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt) 
 namespace {
 template <typename R, int PPT>
 cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                             bool perTrade, bool sink, bool lean, bool smallState, cudaStream_t stream) {
+                             bool perTrade, bool sink, bool lean, bool smallState, bool cash, cudaStream_t stream) {
   const size_t smem = revalueSmemBytes(stateWordsMax, perTrade, sizeof(R) == 8, PPT);
   const uint64_t blocks = static_cast<uint64_t>(numTiles) * numNs;
   if (blocks == 0) return cudaSuccess;
@@ -957,20 +960,20 @@ cudaError_t launchRevaluePPT(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uin
   if (sink) return go(revalueKernel<R, PPT, false, true, false>);
   if (perTrade) return go(revalueKernel<R, PPT, true, false, false>);
   if (lean && smallState && stateWordsMax <= static_cast<size_t>(kSmallStateWords) && sizeof(R) == 4 && PPT > 1)
-    return go(revalueKernel<R, PPT, false, false, true, true>);
-  if (lean) return go(revalueKernel<R, PPT, false, false, true>);
+    return cash ? go(revalueKernel<R, PPT, false, false, true, true, true>) : go(revalueKernel<R, PPT, false, false, true, true>);
+  if (lean) return cash ? go(revalueKernel<R, PPT, false, false, true, false, true>) : go(revalueKernel<R, PPT, false, false, true>);
   return go(revalueKernel<R, PPT, false, false, false>);
 }
 }  // namespace
 
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream, bool smallState) {
+                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream, bool smallState, bool cash) {
   switch (ppt) {
-    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
-    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
+    case 1: return launchRevaluePPT<R, 1>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, cash, stream);
+    case 2: return launchRevaluePPT<R, 2>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, cash, stream);
     case 4:
-      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, stream);
+      if (sizeof(R) == 4) return launchRevaluePPT<R, 4>(cb, nsArgs, numNs, numTiles, stateWordsMax, perTrade, sink, lean, smallState, cash, stream);
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
@@ -981,8 +984,8 @@ template cudaError_t launchNestedIm<double>(const ImArgs<double>&, cudaStream_t)
 template cudaError_t launchSimulate<float>(const ScenarioArgs<float>&, const CubeArgs<float>&, cudaStream_t);
 template cudaError_t launchSimulate<double>(const ScenarioArgs<double>&, const CubeArgs<double>&, cudaStream_t);
 template cudaError_t launchRevalue<float>(const CubeArgs<float>&, const NsArgs<float>*, uint32_t, uint32_t, size_t, bool, bool, bool,
-                                          int, cudaStream_t, bool);
+                                          int, cudaStream_t, bool, bool);
 template cudaError_t launchRevalue<double>(const CubeArgs<double>&, const NsArgs<double>*, uint32_t, uint32_t, size_t, bool, bool, bool,
-                                           int, cudaStream_t, bool);
+                                           int, cudaStream_t, bool, bool);
 
 }  // namespace zk

@@ -18,11 +18,13 @@ cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cud
 // paths (1, 2 or 4 in single precision, 1 or 2 in double), so a tile holds kTile * ppt paths.  `lean`: no
 // netting set of the launch has AMC or probe terms (a variant without their state).  `smallState`: every
 // netting set of the launch keeps at most kSmallStateWords shared-memory words per path, so a lean single-
-// precision launch of 2 or 4 paths per thread may use the variant compiled for more resident CTAs.
+// precision launch of 2 or 4 paths per thread may use the variant compiled for more resident CTAs.  `cash`:
+// every netting set of a lean launch has a cash CSA with a margin-call look-back of at most one date.
 constexpr int kSmallStateWords = 26;
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
-                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream, bool smallState = false);
+                          bool perTrade, bool sink, bool lean, int ppt, cudaStream_t stream, bool smallState = false,
+                          bool cash = false);
 size_t revalueSmemBytes(size_t stateWordsMax, bool perTrade, bool f64, int ppt);
 
 // The nested initial margin of one plan (fused_reference.cpp:356-393), after its revalue launch: one warp
