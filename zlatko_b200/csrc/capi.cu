@@ -469,7 +469,7 @@ struct Batch {
     // per path (at most smallStateMax) and may run as a second launch with more resident CTAs.
     size_t splitAt = 0, smallStateMax = 0;
     // Every netting set of [0, splitAt) (cashBig), of [splitAt, n) (cashSmall), of the launch (cashAll) has a cash
-    // CSA with a margin-call look-back of at most one date.
+    // CSA with a margin-call look-back of at most one date and none of the optional value / collateral rows.
     bool cashBig = true, cashSmall = true, cashAll = true;
     bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
@@ -569,7 +569,8 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     if (L.splitAt < L.planIdx.size()) L.smallStateMax = B->plans[L.planIdx[L.splitAt]].stateWords;
     for (size_t k = 0; k < L.planIdx.size(); ++k) {
       const auto& P = B->plans[L.planIdx[k]];
-      const bool cash = P.hasCsa && P.ctype == 0 && P.ring <= 2;
+      const bool cash = P.hasCsa && P.ctype == 0 && P.ring <= 2 && P.rowDV == kNoRow && P.rowE == kNoRow && P.rowV == kNoRow &&
+                        P.rowC == kNoRow;
       (k < L.splitAt ? L.cashBig : L.cashSmall) = (k < L.splitAt ? L.cashBig : L.cashSmall) && cash;
       L.cashAll = L.cashAll && cash;
     }

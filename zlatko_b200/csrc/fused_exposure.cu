@@ -309,8 +309,9 @@ constexpr int revalueMinBlocks() {
 
 // Each thread owns PPT paths (p, p + kTile, ...): every term record, kind decode, date descriptor and
 // statistics reduction is shared by PPT paths, and their independent exponentials keep the SFU busy.
-// kCash: every netting set of the launch has a cash CSA whose margin calls look back at most one date, so the
-// collateral code is that case alone (no securities price, no shared-memory ring).
+// kCash: every netting set of the launch has a cash CSA whose margin calls look back at most one date and writes
+// none of the optional value, exposure, collateral or change rows, so the collateral code is that case alone (no
+// securities price, no shared-memory ring) and the optional rows are compiled out.
 template <typename R, int PPT, bool kPerTrade, bool kSink, bool kLean, bool kSmallState = false, bool kCash = false>
 __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallState>())) revalueKernel(const CubeArgs<R> cb, const NsArgs<R>* __restrict__ nsArgs,
                                                         uint32_t numNs) {
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   const uint32_t ctype = kCash ? 0u : A.ctype;
   const bool hasCsa = kCash || A.hasCsa != 0, usesAssets = A.usesAssets != 0;
   R* __restrict__ const rowEP = expo + static_cast<size_t>(A.rowEP) * nP;
-  const bool moreRows = A.rowDV != kNoRow || A.rowE != kNoRow || A.rowV != kNoRow || A.rowC != kNoRow;
+  const bool moreRows = !kCash && (A.rowDV != kNoRow || A.rowE != kNoRow || A.rowV != kNoRow || A.rowC != kNoRow);
   uint32_t pth[PPT], pp[PPT];
   bool act[PPT];
 #pragma unroll

@@ -19,7 +19,8 @@ cudaError_t launchSimulate(const ScenarioArgs<R>& sc, const CubeArgs<R>& cb, cud
 // netting set of the launch has AMC or probe terms (a variant without their state).  `smallState`: every
 // netting set of the launch keeps at most kSmallStateWords shared-memory words per path, so a lean single-
 // precision launch of 2 or 4 paths per thread may use the variant compiled for more resident CTAs.  `cash`:
-// every netting set of a lean launch has a cash CSA with a margin-call look-back of at most one date.
+// every netting set of a lean launch has a cash CSA with a margin-call look-back of at most one date and none of
+// the optional value, exposure, collateral or change rows.
 constexpr int kSmallStateWords = 26;
 template <typename R>
 cudaError_t launchRevalue(const CubeArgs<R>& cb, const NsArgs<R>* nsArgs, uint32_t numNs, uint32_t numTiles, size_t stateWordsMax,
