@@ -1,20 +1,23 @@
 """Benchmark of the exposure hot path: scenario x trade revaluations per second.
 
-Workload (default): the multi-factor correlated book of zlatko_b200.workloads.correlated_csa_book -- 1,000 trades
-(600 swaps, 300 FX forwards, 100 FX options) in 100 collateralised netting sets of Zipf(1.2) sizes,
-100,000 paths, 120 monthly reporting dates to 10y (241 simulation dates with the margin-call dates),
-synthetic seeded data.  One step = the fused simulate -> revalue -> net -> collateralise -> reduce kernel
-over every netting set, the reduction of the per-tile partials, and the row statistics (PFE 97.5% and
-means) of every netting set and reporting date.
+Workload (default): the correlated CSA book at the size of the surrogate target -- 2,000 trades (1,200 swaps
+with annual fixed and semiannual floating legs, 600 FX forwards, 200 FX options; the 60/30/10 mix of the
+1,000-trade book scaled x2) in 100 collateralised netting sets of Zipf(1.2) sizes, 1,000,000 paths, 120 monthly
+reporting dates to 10y (241 simulation dates with the margin-call dates t - MPR), HW1F + 2 lognormal FX + CIR++,
+synthetic seeded data.  One step = the fused simulate -> revalue -> net -> collateralise -> reduce kernels over
+every netting set, the reduction of the per-warp partials, and the row statistics (PFE 97.5% and means) of every
+netting set and reporting date.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zlatko|reference] [--paths P]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zlatko|reference] [--paths P] [--trades N]
 
 value   revaluations/s = paths x simulation dates x trades / device time of a step (CUDA events on the
-        library's stream; inputs resident in HBM; L2 flushed between steps).
+        library's stream; inputs resident in HBM; L2 flushed between steps).  per_reporting_date counts the
+        120 + 1 reporting dates only.
 e2e     the same metric through the public C ABI (zk_run_plans): plan tables copied host -> device and
         statistics device -> host inside the timed region, wall clock of the blocking call.
---impl reference: the reference's own FP32 CPU kernels (gpu::runFusedReference, compiled from the
-        reference sources into oracle/_ref) on the host cores, on a bounded sample of paths.
+--impl reference: the reference's own FP32 CPU kernels (gpu::runFusedReference, compiled from the reference
+        sources into oracle/_ref) on the host cores, on plans its own gpu::compile builds, on a bounded sample
+        of paths; this process never loads this library.
 N > 1: replicas (the path runs on one GPU by design); every rank runs the workload, value = all ranks'
         revaluations / the slowest rank's time.
 """
@@ -44,7 +47,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="zlatko", choices=["zlatko", "reference"])
-    ap.add_argument("--paths", type=int, default=100_000)
+    ap.add_argument("--paths", type=int, default=1_000_000)
+    ap.add_argument("--trades", type=int, default=2000)
+    ap.add_argument("--netting-sets", type=int, default=100)
+    ap.add_argument("--precision-paths", type=int, default=65_536, help="paths of the FP32-against-FP64 comparison")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32-against-FP64 comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
@@ -146,10 +153,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def workload(paths: int):
+def workload_name(trades: int, netting_sets: int, paths: int) -> str:
+    n_swaps, n_fwds = round(0.6 * trades), round(0.3 * trades)
+    return (f"correlated CSA book: {trades} trades ({n_swaps} IRS / {n_fwds} FX fwd / {trades - n_swaps - n_fwds} FX opt) in "
+            f"{netting_sets} CSA netting sets Zipf(1.2), HW1F + 2 FX + CIR++, {paths} paths, 120 monthly reporting dates "
+            "(241 simulation dates with the margin-call dates)")
+
+
+def workload(paths: int, trades: int = 2000, netting_sets: int = 100):
     from zlatko_b200 import gpu, workloads
 
-    m, books, opts, trades = workloads.correlated_csa_book(paths)
+    m, books, opts, trades = workloads.correlated_csa_book(paths, netting_sets, trades)
     t0 = time.perf_counter()
     plans = [gpu.compile(m, b, opts) for b in books]
     compile_s = time.perf_counter() - t0
@@ -407,6 +421,87 @@ def nest_leg(ctx, a):
     return line
 
 
+def replace_args(a, **kw):
+    b = argparse.Namespace(**vars(a))
+    for k, v in kw.items():
+        setattr(b, k, v)
+    return b
+
+
+def precision_leg(ctx, a):
+    """The error of the FP32 path against the FP64 mode for every output of every netting set (EE, ENE, PFE, EE*,
+    ENE* per reporting date; CVA, first-to-default CVA and DVA with an own hazard of 0.5%, pathwise CVA), beside
+    its Monte Carlo standard error (batch means over 8 independent seeds), on the bench's book at fewer paths."""
+    from zlatko_b200 import precision, workloads
+    from zlatko_b200 import spec as S
+
+    m, books, opts, _ = workloads.correlated_csa_book(a.precision_paths, a.netting_sets, a.trades)
+    own = S.Credit(1e-6, 0.0, 0.0, 0.0, [1.0], [0.005], substeps=1)
+    t0 = time.perf_counter()
+    r = precision.compare(ctx, m, books, opts, own)
+    r["wall_s"] = time.perf_counter() - t0
+    r["all_below_se"] = all(v["max_err_over_se"] < 1.0 for v in r["outputs"].values())
+    return r
+
+
+def reference_arm(a) -> dict:
+    """The reference's own path on the host cores: gpu::compile (src/gpu/fused_exposure.cpp:214) builds the plans
+    and gpu::runFusedReference (src/gpu/fused_reference.cpp:628-630) runs them on all host threads, both from the
+    reference's sources compiled into oracle/_ref.  The book comes from the pure-Python generator; this library's
+    compiler and kernels are never loaded.  The reference's compile caps a netting set at 32 swaps
+    (src/gpu/fused_exposure.cpp:161-189), and a two-schedule swap enters it as three one-schedule swaps, so the
+    largest netting sets are left out: the rate is measured on the netting sets it accepts, per trade, on a sample
+    of the paths of each step, and that is stated on the line."""
+    from oracle import ref
+    from zlatko_b200 import spec as S
+    from zlatko_b200 import workloads
+
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "the reference library oracle/_ref/libccr_ref.so was not built"}
+    m, books, opts, trades = workloads.correlated_csa_book(a.paths, a.netting_sets, a.trades)
+    mflat, oflat = S.encode_model(m), S.encode_options(opts)
+    plans, kept, left_out = [], 0, []
+    for i, b in enumerate(books):
+        try:
+            plans.append(ref.compile_plan(mflat, S.encode_netting_set(b), oflat))
+            kept += len(b.trades)
+        except ValueError as exc:
+            left_out.append({"netting_set": i, "trades": len(b.trades), "why": str(exc)[:120]})
+    if not plans:
+        return {"impl": "reference", "unavailable": "the reference's gpu::compile accepts none of the book's netting sets"}
+    nT = plans[0].num_dates
+    threads = os.cpu_count() or 1
+
+    def run(paths):
+        for p in plans:
+            p.set_paths(paths)
+        t0 = time.perf_counter()
+        for p in plans:
+            ref.run_fused(p, threads)
+        return time.perf_counter() - t0
+
+    per_step = max(2.0, a.cpu_seconds / max(a.steps, 1))
+    probe = 256
+    dt = run(probe)
+    paths = int(max(probe, min(a.paths, probe * per_step / max(dt, 1e-3))) // 64 * 64)
+    for _ in range(min(a.warmup, 1)):
+        run(min(paths, 1024))
+    times = [run(paths) for _ in range(a.steps)]
+    dt = float(np.median(times))
+    value = paths * nT * kept / dt
+    sample = (f"{paths} of {a.paths} paths per step of the {len(plans)} netting sets ({kept} of {trades} trades) that the "
+              f"reference's gpu::compile accepts; {len(left_out)} netting sets above its 32-swap cap left out; "
+              f"gpu::runFusedReference on {threads} threads")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(trades, a.netting_sets, a.paths), "paths_per_step": paths,
+                       "simulation_dates": nT, "trades_timed": kept, "netting_sets_timed": len(plans),
+                       "netting_sets_left_out": left_out},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -416,20 +511,7 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
-        _, _, _, trades, plans, _ = workload(a.paths)
-        per_step = max(2.0, a.cpu_seconds / max(a.steps, 1))
-        for _ in range(min(a.warmup, 1)):
-            cpu_reference(plans, trades, 1.0)
-        value, paths, threads, dt, times, kind = cpu_reference(plans, trades, per_step, steps=a.steps)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "correlated CSA book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
-                                       "HW1F + 2 FX + CIR++, 241 simulation dates", "paths_per_step": paths},
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                                 "sample": f"{paths} paths of each of the 100 netting sets per step (of {a.paths})"},
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(reference_arm(a)))
         return
 
     import torch
@@ -448,8 +530,9 @@ def main():
     from zlatko_b200 import gpu
     from zlatko_b200._native import lib
 
-    m, books, opts, trades, plans, compile_s = workload(a.paths)
+    m, books, opts, trades, plans, compile_s = workload(a.paths, a.trades, a.netting_sets)
     nT, nP = plans[0].num_dates, plans[0].num_paths
+    nR = len(plans[0].reporting)
     revals = float(nP) * nT * trades
     ctx = gpu.Context(device)
     batch = ctx.batch(plans)
@@ -475,6 +558,7 @@ def main():
             sim_ms.append(ms[0]), fused_ms.append(ms[1]), reduce_ms.append(ms[2]), rows_ms.append(ms[3])
             step_ms.append(float(ms.sum()))
         torch.cuda.synchronize()
+        batch.close()  # its device arena goes back before the context allocates its own for the calls below
         # e2e through the public C ABI: host plan tables in, host statistics out.
         for _ in range(a.warmup):
             ctx.run_many(plans)
@@ -510,20 +594,27 @@ def main():
         try:
             if a.no_cpu:
                 raise RuntimeError("skipped (--no-cpu)")
-            cv, cpaths, cthreads, cdt, _, ckind = cpu_reference(plans, trades, a.cpu_seconds / 2)
-            what = "gpu::runFusedReference" if ckind == "reference" else "the plain-C restatement of it"
-            cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": ckind,
-                   "sample": f"{cpaths} of {nP} paths of all 100 netting sets ({what}, {cthreads} threads)"}
+            r = reference_arm(replace_args(a, steps=1, warmup=0, cpu_seconds=a.cpu_seconds / 2))
+            if "unavailable" in r:  # the reference library is absent: the plain-C restatement on this book's plans
+                cv, cpaths, cthreads, cdt, _, ckind = cpu_reference(plans, trades, a.cpu_seconds / 2)
+                cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": ckind,
+                       "sample": f"{cpaths} of {nP} paths of all {len(plans)} netting sets (the plain-C restatement of "
+                                 f"gpu::runFusedReference, {cthreads} threads)"}
+            else:
+                cpu = dict(r["cpu_baseline"])
         except Exception as exc:  # pragma: no cover
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": t_step / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "correlated CSA book: 1000 trades (600 IRS / 300 FX fwd / 100 FX opt), 100 CSA netting sets Zipf(1.2), "
-                                   "HW1F + 2 FX + CIR++, 241 simulation dates", "paths": nP, "simulation_dates": nT,
-                       "trades": trades, "netting_sets": len(plans), "l2": "flushed between steps (256 MB write)",
+            "config": {"workload": workload_name(trades, len(plans), nP), "paths": nP, "simulation_dates": nT,
+                       "reporting_dates": nR, "trades": trades, "netting_sets": len(plans),
+                       "l2": "flushed between steps (256 MB write); the step's rows and partials exceed L2 anyway",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
+            "per_reporting_date": {"value": value * nR / nT, "unit": "scenario x trade revaluations/s on reporting dates",
+                                   "note": "paths x reporting dates x trades / device time; the other simulation dates "
+                                           "are the margin-call dates t - MPR"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(info.kernels_per_execute) * a.steps,
             "tile_paths": int(info.tile_paths),
@@ -540,6 +631,8 @@ def main():
             "plan_compile_s": compile_s,
             "cpu_baseline": cpu,
         }
+        if not a.no_precision:
+            line["fp32_vs_fp64"] = guarded(precision_leg, ctx, a)
         if not a.no_surrogate:
             line["surrogate"] = guarded(surrogate_leg, ctx, a)
         if not a.no_amc:
@@ -549,7 +642,6 @@ def main():
         if not a.no_nest:
             line["adaptive_nest"] = guarded(nest_leg, ctx, a)
         print(json.dumps(line))
-    batch.close()
     ctx.close()
     if dist:
         dist.barrier()

@@ -189,11 +189,25 @@ zk_status zk_erfc_array(const double* x, size_t n, double* out);
  * ZK_NOALLOC_SCRATCH_BYTES that the library reserves on each GPU where it is loaded and holds until the
  * process exits.  A plan that needs more scratch is rejected with ZK_ERR_INVALID_ARGUMENT (use
  * zk_run_plan).  `stream` may be NULL (the legacy default stream).  The first call on a device looks up
- * the array's device address; make that first call before any stream capture.  Every call reuses the
- * same array, so calls that overlap on the GPU (on other streams or from other threads) race: the
- * caller must serialise them.  On failure the message is copied to err (err_len bytes). */
+ * the array's device address; make that first call before any stream capture.  With CUDA's lazy module
+ * loading (the default) that lookup is also what loads the library's kernels on the device and reserves
+ * the array, so a host that hands all free device memory to its own pool must make its first call before
+ * that (or load modules eagerly, CUDA_MODULE_LOADING=EAGER); otherwise the call fails with
+ * ZK_ERR_OUT_OF_MEMORY.  The call makes `device` current while it runs and gives the caller's current
+ * device back before it returns.  Every call reuses the same array, so calls that overlap on the GPU (on
+ * other streams or from other threads) race: the caller must serialise them.  On failure the message is
+ * copied to err (err_len bytes). */
 #define ZK_NOALLOC_SCRATCH_BYTES (32u << 20)
 zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan_view* plan, zk_output* out, char* err, size_t err_len);
+
+/* ---- failure injection for tests (host side; no counterpart in the reference) ---------------------- */
+/* ZK_INJECT_FAIL_LAUNCH: the value-th kernel launch of the context's eager calls from now on fails with
+ * ZK_ERR_CUDA instead of launching (once; 0 clears it), leaving the launches before it in flight and the
+ * context usable.  ZK_INJECT_ROW_ROUNDS: caps the row statistics' quantile search at value narrowing rounds
+ * (16, the default, restores it); a quantile that needs more makes the call fail with ZK_ERR_CUDA. */
+#define ZK_INJECT_FAIL_LAUNCH 1u
+#define ZK_INJECT_ROW_ROUNDS 2u
+zk_status zk_debug_inject(zk_context* ctx, uint32_t what, uint64_t value);
 
 /* ---- device-resident batches (inputs uploaded once; used to time the kernels alone) -------------- */
 typedef struct zk_batch zk_batch;

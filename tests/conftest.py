@@ -20,8 +20,10 @@ def _ensure_built():
     build.build()
     # The plain-C restatement builds anywhere; the reference library only where its sources are (elsewhere the
     # prebuilt copy that travels with the repository, if any, is used).
-    targets = ["restatement"] + (["ref"] if os.path.isdir("/root/reference") else [])
-    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle")] + targets, check=True)
+    # The reference's sources: ZK_REFERENCE_DIR, else where the build container mounts them.
+    reference = os.environ.get("ZK_REFERENCE_DIR", "/root/reference")
+    targets = ["restatement"] + (["ref"] if os.path.isdir(reference) else [])
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), f"REF={reference}"] + targets, check=True)
 
 
 _ensure_built()

@@ -64,7 +64,7 @@ class BatchInfo(C.Structure):
 
 # Every entry point declared in include/zlatko_b200.h.
 EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream",
-           "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc",
+           "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc", "zk_debug_inject",
            "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
            "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
            "zk_surrogate_train", "zk_surrogate_predict", "zk_surrogate_gradients", "zk_surrogate_params",
@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         "zk_run_plan_f64": (st, [vp, P(PlanViewF64), vp, sz, P(OutputF64), vp]),
         "zk_run_plan_injected": (st, [vp, P(PlanView), vp, sz, P(Output), vp]),
         "zk_run_plan_noalloc": (st, [C.c_int, vp, P(PlanView), P(Output), C.c_char_p, sz]),
+        "zk_debug_inject": (st, [vp, C.c_uint32, C.c_uint64]),
         "zk_batch_create": (st, [vp, P(PlanView), sz, P(vp)]),
         "zk_batch_execute": (st, [vp]),
         "zk_batch_set_tile_paths": (st, [vp, C.c_uint64]),

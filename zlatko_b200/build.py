@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["fused_exposure.cu", "row_stats.cu", "nested_inner.cu", "amc_fit.cu", "mlp.cu", "surrogate.cu", "capi.cu", "peaks.cu"]
 CPP_SOURCES = ["plan_compiler.cpp", "hermite_proxy.cpp"]
-HEADERS = ["zk_device.cuh", "zk_kernels.h", "plan_compiler.h"]
+HEADERS = ["zk_device.cuh", "zk_kernels.h", "plan_compiler.h", "umma.cuh", "surrogate.cuh"]
 
 
 def _sources():

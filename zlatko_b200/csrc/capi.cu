@@ -119,6 +119,11 @@ struct zk_context {
   // later work and freed with the context: freeing device memory synchronises the device and took tens of
   // milliseconds per nest.
   std::vector<std::pair<unsigned char*, size_t>> spareBlocks;
+  // Failure injection for tests (zk_debug_inject): the kernel launch, counted from the injection over the
+  // context's eager launches, that fails instead of launching (0: none); the row statistics' cap on the
+  // quantile's narrowing rounds.
+  uint64_t failAtLaunch = 0, launchCount = 0;
+  uint32_t rowRounds = 16;
 };
 
 namespace {
@@ -816,6 +821,49 @@ void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normal
   }
 }
 
+// A point where zk_debug_inject may make a launch fail: the host-side failure of a kernel launch, which leaves
+// the kernels launched before it in flight and the context usable.
+void injectPoint(zk_context* ctx) {
+  if (!ctx || ctx->failAtLaunch == 0) return;
+  if (++ctx->launchCount < ctx->failAtLaunch) return;
+  const unsigned long long k = ctx->launchCount;
+  ctx->failAtLaunch = 0, ctx->launchCount = 0;
+  throw fail(ZK_ERR_CUDA, "injected failure of kernel launch %llu", k);
+}
+
+// The revalue launches of one launch group on stream s.  Lean single-precision launches of 2 or 4 paths per
+// thread run the netting sets with little state as their own launch, compiled for more resident CTAs than the
+// shared memory of the largest allows.  The few large-state netting sets fill less than a wave of long CTAs:
+// with a side stream (and its fork / join events) they run there while the small-state launch fills the rest
+// of the GPU; without one, before it on s.  Either way the kernels and their output bits are the same.
+template <typename R>
+void launchRevalues(const Batch<R>& B, const typename Batch<R>::Launch& L, uintptr_t base, cudaStream_t s, cudaStream_t side,
+                    cudaEvent_t forkEv, cudaEvent_t joinEv) {
+  const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff);
+  const uint32_t n = static_cast<uint32_t>(L.planIdx.size()), tiles = numTilesOf(L.sc.nP, B.ppt);
+  const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < n;
+  if (!split) {
+    injectPoint(B.ctx);
+    ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s, false,
+                             L.lean && !L.perTrade && !B.sink && L.cashAll));
+    return;
+  }
+  const uint32_t big = static_cast<uint32_t>(L.splitAt);
+  const bool fork = big > 0 && side;
+  if (big > 0) injectPoint(B.ctx);
+  if (fork) {
+    ZK_CUDA(cudaEventRecord(forkEv, s));
+    ZK_CUDA(cudaStreamWaitEvent(side, forkEv, 0));
+    ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, side, false, L.cashBig));
+  } else if (big > 0) {
+    ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, s, false, L.cashBig));
+  }
+  if (fork) ZK_CUDA(cudaEventRecord(joinEv, side));  // joined before a failure below can leave the side stream behind
+  injectPoint(B.ctx);
+  ZK_CUDA(launchRevalue<R>(L.cb, ns + big, n - big, tiles, L.smallStateMax, false, false, true, B.ppt, s, true, L.cashSmall));
+  if (fork) ZK_CUDA(cudaStreamWaitEvent(s, joinEv, 0));
+}
+
 cudaError_t recordEvent(cudaEvent_t e, cudaStream_t s, bool capturing) {
   return cudaEventRecordWithFlags(e, s, capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
 }
@@ -831,53 +879,47 @@ void execute(Batch<R>& B, bool capturing = false) {
   ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, s));
   ZK_CUDA(recordEvent(B.ev[0], s, capturing));
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
-  for (auto& L : B.launches) ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
+  for (auto& L : B.launches) {
+    injectPoint(ctx);
+    ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
+  }
   ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   for (auto& L : B.launches) {
-    const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff);
-    const uint32_t n = static_cast<uint32_t>(L.planIdx.size()), tiles = numTilesOf(L.sc.nP, B.ppt);
-    // Lean single-precision launches of 2 or 4 paths per thread: the netting sets with little state run as
-    // their own launch, compiled for more resident CTAs than the shared memory of the largest allows.
-    const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < n;
-    if (!split) {
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s, false,
-                               L.lean && !L.perTrade && !B.sink && L.cashAll));
-      continue;
-    }
-    const uint32_t big = static_cast<uint32_t>(L.splitAt);
-    if (big > 0 && !ctx->side && !capturing) {
+    const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < L.planIdx.size();
+    if (split && L.splitAt > 0 && !ctx->side && !capturing) {
       ZK_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
     }
-    // The few large-state netting sets fill less than a wave of long CTAs: they run on the side stream while
-    // the small-state launch fills the rest of the GPU.
-    const bool fork = big > 0 && ctx->side;
-    if (fork) {
-      ZK_CUDA(cudaEventRecord(ctx->fork, s));
-      ZK_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, ctx->side, false, L.cashBig));
-    } else if (big > 0) {
-      ZK_CUDA(launchRevalue<R>(L.cb, ns, big, tiles, L.stateWordsMax, false, false, true, B.ppt, s, false, L.cashBig));
-    }
-    ZK_CUDA(launchRevalue<R>(L.cb, ns + big, n - big, tiles, L.smallStateMax, false, false, true, B.ppt, s, true, L.cashSmall));
-    if (fork) {
-      ZK_CUDA(cudaEventRecord(ctx->join, ctx->side));
-      ZK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
-    }
+    launchRevalues(B, L, base, s, ctx->side, ctx->fork, ctx->join);
   }
-  for (const auto& M : B.im) ZK_CUDA(launchNestedIm<R>(M, s));
+  for (const auto& M : B.im) {
+    injectPoint(ctx);
+    ZK_CUDA(launchNestedIm<R>(M, s));
+  }
   ZK_CUDA(recordEvent(B.ev[2], s, capturing));
   if (!B.sink) {
+    injectPoint(ctx);
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN,
                             B.ppt, s));
     ZK_CUDA(recordEvent(B.ev[3], s, capturing));
-    ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff), B.numRowJobs, ctx->dErr, s));
+    injectPoint(ctx);
+    ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff), B.numRowJobs, ctx->dErr, s, ctx->rowRounds));
   } else {
     ZK_CUDA(recordEvent(B.ev[3], s, capturing));
   }
   ZK_CUDA(recordEvent(B.ev[4], s, capturing));
   B.timed = true;
+}
+
+// The status of a kernel's error word (DeviceError), the same for every entry point.
+void throwDeviceError(uint32_t err) {
+  if (err == kDevOk) return;
+  if (err == kDevTimeout) throw fail(ZK_ERR_DEVICE_TIMEOUT, "a bounded wait in a kernel gave up");
+  if (err == kDevBadTerm)
+    throw fail(ZK_ERR_CUDA, "a kernel met a case it does not handle (error %u: a quantile search that did not narrow to its ranks "
+                            "within its rounds, or an AMC regression without a solution)", err);
+  throw fail(ZK_ERR_CUDA, "a kernel reported error %u", err);
 }
 
 template <typename R>
@@ -889,8 +931,7 @@ void finish(Batch<R>& B) {
   if (B.timed) {
     for (int k = 0; k < 4; ++k) ZK_CUDA(cudaEventElapsedTime(&B.ms[k], B.ev[k], B.ev[k + 1]));
   }
-  if (err == kDevTimeout) throw fail(ZK_ERR_DEVICE_TIMEOUT, "a bounded wait in the fused kernel gave up");
-  if (err != 0) throw fail(ZK_ERR_CUDA, "a kernel reported error %u", err);
+  throwDeviceError(err);
 }
 
 template <typename R, typename Out>
@@ -1718,17 +1759,35 @@ std::mutex gNoAllocMutex;
 unsigned char* gNoAllocBase[kNoAllocMaxDevices] = {};
 
 // The device address of zkNoAllocScratch on `device` (current), looked up once per device.  In host code
-// the array's name is only a stand-in; the kernels need this address.
+// the array's name is only a stand-in; the kernels need this address.  With lazy module loading (the CUDA
+// default) the lookup is what loads the module on the device and so reserves the array: a host that gives all
+// free device memory to its own pool must make its first call before that.
 unsigned char* noAllocBase(int device) {
   std::lock_guard<std::mutex> lock(gNoAllocMutex);
   if (!gNoAllocBase[device]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, zkNoAllocScratch);
+    if (e == cudaErrorMemoryAllocation)
+      throw fail(ZK_ERR_OUT_OF_MEMORY, "loading the library's kernels and their %u-byte no-alloc array on device %d: out of memory "
+                                       "(make the first call before the host's pool takes the device memory)",
+                 static_cast<unsigned>(ZK_NOALLOC_SCRATCH_BYTES), device);
     if (e != cudaSuccess) throw fail(ZK_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch: %s", cudaGetErrorString(e));
     gNoAllocBase[device] = static_cast<unsigned char*>(p);
   }
   return gNoAllocBase[device];
 }
+
+// Makes `device` current for the lifetime of the guard and gives the caller's current device back on every exit.
+struct DeviceGuard {
+  int saved = -1;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+    ZK_CUDA(cudaSetDevice(device));
+  }
+  ~DeviceGuard() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
 
 }  // namespace
 
@@ -1752,7 +1811,7 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     if (errOff + 256 > static_cast<size_t>(ZK_NOALLOC_SCRATCH_BYTES))
       throw fail(ZK_ERR_INVALID_ARGUMENT, "the plan needs %zu bytes of device scratch; zk_run_plan_noalloc has %zu (use zk_run_plan)",
                  errOff + 256, static_cast<size_t>(ZK_NOALLOC_SCRATCH_BYTES));
-    ZK_CUDA(cudaSetDevice(device));
+    DeviceGuard guard(device);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     B->base = noAllocBase(device);
     uint32_t* dErr = reinterpret_cast<uint32_t*>(B->base + errOff);
@@ -1760,19 +1819,19 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     ZK_CUDA(cudaMemcpyAsync(B->base, B->image.data(), B->inputBytes, cudaMemcpyHostToDevice, s));
     ZK_CUDA(cudaMemsetAsync(dErr, 0, 4, s));  // the array keeps the previous call's contents
     const uintptr_t base = reinterpret_cast<uintptr_t>(B->base);
-    const auto& L = B->launches.front();
-    ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
-    ZK_CUDA(launchRevalue<float>(L.cb, reinterpret_cast<const NsArgs<float>*>(base + L.nsOff), static_cast<uint32_t>(L.planIdx.size()),
-                                 numTilesOf(L.sc.nP, B->ppt), L.stateWordsMax, L.perTrade, false, false, B->ppt, s));
+    // The kernels and variants of zk_run_plan (launchRevalues), all on the caller's stream.
+    for (const auto& L : B->launches) ZK_CUDA(launchSimulate<float>(L.sc, L.cb, s));
+    for (const auto& L : B->launches) launchRevalues(*B, L, base, s, nullptr, nullptr, nullptr);
     for (const auto& M : B->im) ZK_CUDA(launchNestedIm<float>(M, s));
-    ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), 1, B->maxReduceN, B->ppt, s));
+    ZK_CUDA(launchReduce<float>(reinterpret_cast<const ReduceJob<float>*>(base + B->reduceOff), static_cast<uint32_t>(B->plans.size()),
+                                B->maxReduceN, B->ppt, s));
     ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(base + B->rowOff), B->numRowJobs, dErr, s));
     std::vector<unsigned char> host(B->outBytes);
     uint32_t devErr = 0;
     ZK_CUDA(cudaMemcpyAsync(host.data(), B->base + B->outBegin, B->outBytes, cudaMemcpyDeviceToHost, s));
     ZK_CUDA(cudaMemcpyAsync(&devErr, dErr, 4, cudaMemcpyDeviceToHost, s));
     ZK_CUDA(cudaStreamSynchronize(s));
-    if (devErr != 0) throw fail(ZK_ERR_CUDA, "a kernel reported error %u", devErr);
+    throwDeviceError(devErr);
     const auto& P = B->plans[0];
     const auto& D = B->dev[0];
     const float* sums = reinterpret_cast<const float*>(host.data() + (D.sums - B->outBegin));
@@ -1784,6 +1843,23 @@ extern "C" zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan
     return report(f);
   } catch (const std::exception& e) {
     return report(fail(ZK_ERR_CUDA, "%s", e.what()));
+  }
+}
+
+// ---- failure injection for tests ----
+extern "C" zk_status zk_debug_inject(zk_context* ctx, uint32_t what, uint64_t value) {
+  if (!ctx) return ZK_ERR_INVALID_ARGUMENT;
+  switch (what) {
+    case ZK_INJECT_FAIL_LAUNCH:
+      ctx->failAtLaunch = value, ctx->launchCount = 0;
+      return ZK_OK;
+    case ZK_INJECT_ROW_ROUNDS:
+      if (value > 16) return record(ctx, fail(ZK_ERR_INVALID_ARGUMENT, "row-statistics rounds %llu above 16",
+                                              static_cast<unsigned long long>(value)));
+      ctx->rowRounds = static_cast<uint32_t>(value);
+      return ZK_OK;
+    default:
+      return record(ctx, fail(ZK_ERR_INVALID_ARGUMENT, "unknown injection %u", what));
   }
 }
 

@@ -150,7 +150,10 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
   const uint32_t injectedStream = sc.nStreams > 0 ? min(pathStream, sc.nStreams - 1) : 0u;
   const uint32_t stream = pcg(pcg(sc.seed) ^ pcg(pathStream + 0x9E3779B9u));
   auto normal = [&](uint32_t m) { return col[m * kSimThreads]; };
-  R x = R(0), lnD = R(0), D = R(1);
+  // The deflator's exponent -sum of the integrated short rate accumulates in double precision in both modes (the
+  // reference's kernel sums it in single precision, fused_kernels.cpp:250-253); D = exp(lnD) is then taken in R.
+  R x = R(0), D = R(1);
+  double lnD = 0.0;
   R S[4], lnS[4] = {R(0), R(0), R(0), R(0)}, y[2], Y[2] = {R(0), R(0)};
 #pragma unroll
   for (int a = 0; a < 4; ++a) S[a] = sc.spots[a];
@@ -178,8 +181,8 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
       const R zI = normal(sc.nCorr);
       const R integratedRate = x * step[5] + step[2] * w[0] + step[3] * zI + step[4];
       x = x * step[0] + step[1] * w[0];
-      lnD = lnD - integratedRate;
-      D = rexp(lnD);
+      lnD -= static_cast<double>(integratedRate);
+      D = rexp(static_cast<R>(lnD));
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         if (static_cast<uint32_t>(a) < sc.nA) {

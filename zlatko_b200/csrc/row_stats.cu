@@ -213,7 +213,8 @@ __device__ void bitonicSort(R* a, uint32_t n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err,
+                                                                 uint32_t maxRounds) {
   extern __shared__ __align__(16) unsigned char raw[];
   RowSmem<R>& s = *reinterpret_cast<RowSmem<R>*>(raw);
   const RowJob<R> J = jobs[blockIdx.x];
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>
   R vk = lo, vk1 = lo;
   bool done = false;
   while (!done) {
-    if (rounds >= kMaxRounds) {
+    if (rounds >= static_cast<int>(maxRounds)) {
       if (tid == 0) atomicExch(err, kDevBadTerm), out[0] = R(NAN);
       return;
     }
@@ -419,18 +420,19 @@ cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t ma
 }
 
 template <typename R>
-cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream) {
+cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream, uint32_t maxRounds) {
   if (numJobs == 0) return cudaSuccess;
+  maxRounds = maxRounds < static_cast<uint32_t>(kMaxRounds) ? maxRounds : static_cast<uint32_t>(kMaxRounds);
   const size_t smem = sizeof(RowSmem<R>);
   cudaError_t e = cudaFuncSetAttribute(rowStatsKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  rowStatsKernel<R><<<numJobs, kRowThreads, smem, stream>>>(jobs, err);
+  rowStatsKernel<R><<<numJobs, kRowThreads, smem, stream>>>(jobs, err, maxRounds);
   return cudaGetLastError();
 }
 
 template cudaError_t launchReduce<float>(const ReduceJob<float>*, uint32_t, uint32_t, int, cudaStream_t);
 template cudaError_t launchReduce<double>(const ReduceJob<double>*, uint32_t, uint32_t, int, cudaStream_t);
-template cudaError_t launchRowStats<float>(const RowJob<float>*, uint32_t, uint32_t*, cudaStream_t);
-template cudaError_t launchRowStats<double>(const RowJob<double>*, uint32_t, uint32_t*, cudaStream_t);
+template cudaError_t launchRowStats<float>(const RowJob<float>*, uint32_t, uint32_t*, cudaStream_t, uint32_t);
+template cudaError_t launchRowStats<double>(const RowJob<double>*, uint32_t, uint32_t*, cudaStream_t, uint32_t);
 
 }  // namespace zk

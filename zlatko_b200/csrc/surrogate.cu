@@ -401,8 +401,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __r
   uint64_t* bar = &bars[g];
   if (warp == 0) umma::alloc(&tslot, 128 * kMlpGroups);
   if (gt == 0) mbarInit(bar, 1);
+  // The hidden layers' biases halved (exactly): the epilogue forms h = z / 2 = acc / 2 + b / 2 in one FMA.
   for (uint32_t k = tid; k < kHid; k += kMlpThreads)
-    par[k] = b1[k], par[kHid + k] = b2[k], par[2 * kHid + k] = b3[k], par[3 * kHid + k] = w4[k];
+    par[k] = 0.5f * b1[k], par[kHid + k] = 0.5f * b2[k], par[2 * kHid + k] = 0.5f * b3[k], par[3 * kHid + k] = w4[k];
   if (tid == 0) par[4 * kHid] = b4[0];
   stageKMajor(sm + kMlpW1, wb, kHid, kIn, tid, kMlpThreads);
   stageKMajor(sm + kMlpW2, wb + SurrogateState::kW1, kHid, kHid, tid, kMlpThreads);
@@ -443,19 +444,18 @@ __global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __r
     for (uint32_t c = 0; c < kHid; c += 16) {
       float v[16];
       umma::ld16(taddr + c, v);
-      __align__(16) bf16 hb[16];
+      uint32_t hb[8];  // 16 activations as bf16 pairs
 #pragma unroll
-      for (int j = 0; j < 16; j += 2) {  // two activations per conversion (each rounded to nearest even)
-        const __nv_bfloat162 h2 = __floats2bfloat162_rn(umma::silu(v[j] + bias[c + j]), umma::silu(v[j + 1] + bias[c + j + 1]));
-        hb[j] = h2.x, hb[j + 1] = h2.y;
+      for (int j = 0; j < 16; j += 2) {
+        hb[j / 2] = umma::siluHalfBf16x2(fmaf(v[j], 0.5f, bias[c + j]), fmaf(v[j + 1], 0.5f, bias[c + j + 1]));
         if (head) {
-          acc += __bfloat162float(hb[j]) * par[3 * kHid + c + j];
-          acc += __bfloat162float(hb[j + 1]) * par[3 * kHid + c + j + 1];
+          acc += __uint_as_float(hb[j / 2] << 16) * par[3 * kHid + c + j];
+          acc += __uint_as_float(hb[j / 2] & 0xFFFF0000u) * par[3 * kHid + c + j + 1];
         }
       }
       if (!head) {
-        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c, 128)) = reinterpret_cast<const uint4*>(hb)[0];
-        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c + 8, 128)) = reinterpret_cast<const uint4*>(hb)[1];
+        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c, 128)) = make_uint4(hb[0], hb[1], hb[2], hb[3]);
+        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c + 8, 128)) = make_uint4(hb[4], hb[5], hb[6], hb[7]);
       }
     }
     if (head) pred[row] = acc + par[4 * kHid];

@@ -97,6 +97,19 @@ __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+
+// SiLU of two activations for inference, in packed bf16 arithmetic, from h = z / 2 (the caller folds the 1/2
+// into its bias add): sigmoid(z) = (1 + tanh(z / 2)) / 2, so silu(z) = h (1 + tanh h) = fma(h, tanh h, h).  One
+// tanh.approx.bf16x2 (a single special-function op for both) and one bf16x2 FMA; h0 lands in the low half (the
+// first of the two in memory).  Against silu rounded once to bf16 the result carries the rounding of h to bf16
+// and the approximate tanh, about one bf16 unit in the last place more.
+__device__ __forceinline__ uint32_t siluHalfBf16x2(float h0, float h1) {
+  uint32_t p, t, s;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(p) : "f"(h1), "f"(h0));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(p));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(s) : "r"(p), "r"(t));
+  return s;
+}
 // d/dz silu(z) = s (1 + z (1 - s)), s = sigmoid(z)
 __device__ __forceinline__ float siluGrad(float z) {
   const float s = 1.0f / (1.0f + __expf(-z));

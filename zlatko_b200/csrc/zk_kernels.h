@@ -89,7 +89,9 @@ struct RowJob {
   uint32_t nP, pad;
 };
 template <typename R>
-cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream);
+// maxRounds caps the quantile's narrowing rounds (at most 16, the default); a row that needs more sets
+// kDevBadTerm in err and NaN as its value.
+cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream, uint32_t maxRounds = 16);
 
 // One Bermudan of the AMC fit (zk_fit_amc): its exercise dates (grid indices, ascending), its first row of
 // exercise values in the AMC pass, the slots of its fitted records (slotBase + k: policy of exercise k;

@@ -289,6 +289,13 @@ class Context:
         sums, values = bufs[0]
         return sums, values, r[: plan.rows_total * plan.num_paths].reshape(plan.rows_total, plan.num_paths)
 
+    INJECT_FAIL_LAUNCH, INJECT_ROW_ROUNDS = 1, 2
+
+    def inject(self, what: int, value: int) -> None:
+        """zk_debug_inject (tests): INJECT_FAIL_LAUNCH makes the value-th kernel launch from now fail on the host
+        instead of launching; INJECT_ROW_ROUNDS caps the row statistics' quantile search at value rounds."""
+        check(lib().zk_debug_inject(self.handle, what, value), self.handle)
+
     def summarise(self, plan: Plan, sums: np.ndarray, values: np.ndarray):
         """summary.summarise with this context as the backend of the nested-IM audit (gpu::summarise runs the
         audit on the reference's CPU kernels; here it runs on the GPU)."""
