@@ -50,13 +50,14 @@ def parse():
     ap.add_argument("--paths", type=int, default=1_000_000)
     ap.add_argument("--trades", type=int, default=2000)
     ap.add_argument("--netting-sets", type=int, default=100)
-    ap.add_argument("--precision-paths", type=int, default=65_536, help="paths of the FP32-against-FP64 comparison")
+    ap.add_argument("--precision-paths", type=int, default=16_384, help="paths of the FP32-against-FP64 comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-against-FP64 comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate leg")
-    ap.add_argument("--surrogate-paths", type=int, default=2048)
+    ap.add_argument("--surrogate-paths", type=int, default=65_536)
+    ap.add_argument("--surrogate-train-paths", type=int, default=384)
     ap.add_argument("--no-amc", action="store_true", help="skip the Bermudan (AMC) leg")
     ap.add_argument("--amc-paths", type=int, default=200_000)
     ap.add_argument("--no-amc-surrogate", action="store_true", help="skip the AMC continuation surrogate leg")
@@ -98,7 +99,7 @@ def peaks():
 
 def traffic_per_launch(paths: int):
     """DRAM bytes of one fused-kernel launch from the committed ncu summary, scaled by paths."""
-    path = os.path.join(ROOT, "profiles", "revalue_book100.txt")
+    path = os.path.join(ROOT, "profiles", "revalue_book2000.txt")
     if not os.path.exists(path):
         return None
     ref_paths, ref_bytes = None, None
@@ -156,17 +157,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def workload_name(trades: int, netting_sets: int, paths: int) -> str:
+def workload_name(trades: int, netting_sets: int, paths: int, foreign_rates: bool = True) -> str:
     n_swaps, n_fwds = round(0.6 * trades), round(0.3 * trades)
+    model = ("3 Hull-White currencies (stochastic foreign rates) + 2 lognormal FX + CIR++, 6x6 correlation" if foreign_rates else
+             "HW1F + 2 lognormal FX on deterministic foreign curves + CIR++ (the reference's model family)")
     return (f"correlated CSA book: {trades} trades ({n_swaps} IRS / {n_fwds} FX fwd / {trades - n_swaps - n_fwds} FX opt) in "
-            f"{netting_sets} CSA netting sets Zipf(1.2), HW1F + 2 FX + CIR++, {paths} paths, 120 monthly reporting dates "
+            f"{netting_sets} CSA netting sets Zipf(1.2), {model}, {paths} paths, 120 monthly reporting dates "
             "(241 simulation dates with the margin-call dates)")
 
 
-def workload(paths: int, trades: int = 2000, netting_sets: int = 100):
+def workload(paths: int, trades: int = 2000, netting_sets: int = 100, foreign_rates: bool = True):
     from zlatko_b200 import gpu, workloads
 
-    m, books, opts, trades = workloads.correlated_csa_book(paths, netting_sets, trades)
+    m, books, opts, trades = workloads.correlated_csa_book(paths, netting_sets, trades, foreign_rates)
     t0 = time.perf_counter()
     plans = [gpu.compile(m, b, opts) for b in books]
     compile_s = time.perf_counter() - t0
@@ -236,35 +239,42 @@ def guarded(fn, *args):
 
 
 def surrogate_leg(ctx, a):
-    """CVA of the book (uncollateralised) by the surrogate with its plain-pricer audit against the plain GPU
-    pricer, on the same paths: device time of each and the CVA difference.  Training (on 64 paths of every trade)
-    is reported apart; it runs once per book."""
+    """CVA of the bench's book (its netting sets without CSA: the surrogate revalues reporting dates only) by the
+    surrogate with its 1% plain-pricer audit and per-netting-set fallback, against the plain GPU pricer on the same
+    paths: device time of each, the CVA difference and the fallbacks.  The network is trained on the per-trade
+    values the plain pricer itself produces on --surrogate-train-paths paths (every live trade, date and path: about
+    50M revaluations for this book); training is reported apart, it runs once per book."""
     from zlatko_b200 import surrogate_book as SB
     from zlatko_b200 import workloads
     from zlatko_b200.surrogate import Surrogate
 
-    m, books, _, trades = workloads.correlated_csa_book(a.surrogate_paths)
+    # The surrogate's features cover the reference's model family: deterministic foreign curves.
+    m, books, _, trades = workloads.correlated_csa_book(a.surrogate_paths, a.netting_sets, a.trades, foreign_rates=False)
     book = SB.make_book(m, books)
     t0 = time.perf_counter()
-    X, y = SB.training_set(ctx, book, 64)
+    X, y = SB.training_set(ctx, book, a.surrogate_train_paths)
+    rows_s = time.perf_counter() - t0
     with Surrogate(ctx, seed=1) as s:
-        for lr, ep in ((2e-3, 3), (5e-4, 2), (1e-4, 1)):
-            losses = s.train(X, y, epochs=ep, batch=8192, lr=lr)
+        t0 = time.perf_counter()
+        losses = []
+        for lr, ep in ((2e-3, 2), (5e-4, 1), (1e-4, 1)):
+            losses += list(s.train(X, y, epochs=ep, batch=8192, lr=lr))
         train_s = time.perf_counter() - t0
         _, dee_p, ms_plain = SB.plain_exposure(ctx, book, a.surrogate_paths)
         run = SB.audited_exposure(ctx, s, book, a.surrogate_paths)
     plain = float(SB.cva(book, dee_p).sum())
     ms_sur = run.ms_surrogate + run.ms_audit + run.ms_fallback
     revals = float(a.surrogate_paths) * len(book.times) * trades
-    return {"workload": f"correlated book, {trades} trades in 100 netting sets without CSA, {a.surrogate_paths} paths, "
-                        f"{len(book.times)} reporting dates",
+    return {"workload": f"the bench's book without CSA: {trades} trades in {len(books)} netting sets, {a.surrogate_paths} paths, "
+                        f"{len(book.times)} reporting dates; trained on {a.surrogate_train_paths} paths",
             "cva_plain": plain, "cva_surrogate_audited": float(run.cva.sum()),
             "delta_cva_rel": float(run.cva.sum() / plain - 1.0),
             "ms_plain": ms_plain, "ms_surrogate": run.ms_surrogate, "ms_audit": run.ms_audit, "ms_fallback": run.ms_fallback,
             "speedup_vs_plain": ms_plain / ms_sur if ms_sur > 0 else None,
             "surrogate_revals_per_s": revals / (run.ms_surrogate / 1e3),
-            "fallback_netting_sets": len(run.fallback), "train_rows": int(len(y)), "train_s": train_s,
-            "train_loss": float(losses[-1])}
+            "plain_revals_per_s": revals / (ms_plain / 1e3),
+            "fallback_netting_sets": len(run.fallback), "netting_sets": len(books), "train_rows": int(len(y)),
+            "training_rows_s": rows_s, "train_s": train_s, "train_loss": float(losses[-1])}
 
 
 def amc_leg(ctx, a):
@@ -371,7 +381,7 @@ def im_leg(ctx, a):
     from zlatko_b200 import gpu, workloads
     from zlatko_b200 import spec as S
 
-    m, books, _, _ = workloads.correlated_csa_book(a.im_paths)
+    m, books, _, _ = workloads.correlated_csa_book(a.im_paths, foreign_rates=False)  # the reference's nested-margin model
     ns = max(books, key=lambda b: len(b.trades))
     p_im, p0 = gpu.compile(m, ns, S.Options(im_quantile=0.99, im_inner_paths=128)), gpu.compile(m, ns, S.Options(im_quantile=0.99))
 
@@ -439,7 +449,7 @@ def nest_leg(ctx, a):
     from zlatko_b200 import spec as S
     from zlatko_b200 import workloads
 
-    m, _, _, _ = workloads.correlated_csa_book(a.nest_paths)
+    m, _, _, _ = workloads.correlated_csa_book(a.nest_paths, foreign_rates=False)  # the reference's nested model
     ns = workloads.nested_netting_set()
     reporting = [q / 4.0 for q in range(1, 21)]
     o = E.NestedExposureOptions()
@@ -483,6 +493,9 @@ def precision_leg(ctx, a):
     r = precision.compare(ctx, m, books, opts, own)
     r["wall_s"] = time.perf_counter() - t0
     r["all_below_se"] = all(v["max_err_over_se"] < 1.0 for v in r["outputs"].values())
+    r["note"] = ("max_err_over_se: largest |FP32 - FP64| / (Monte Carlo standard error, per path from the FP64 rows) over "
+                 "netting sets and dates; entries without Monte Carlo error (date 0) are compared relative to the output's "
+                 "scale instead")
     return r
 
 
@@ -500,7 +513,8 @@ def reference_arm(a) -> dict:
 
     if not ref.available():
         return {"impl": "reference", "unavailable": "the reference library oracle/_ref/libccr_ref.so was not built"}
-    m, books, opts, trades = workloads.correlated_csa_book(a.paths, a.netting_sets, a.trades)
+    # The reference's own model family: its foreign curves are deterministic (it has no stochastic foreign rates).
+    m, books, opts, trades = workloads.correlated_csa_book(a.paths, a.netting_sets, a.trades, foreign_rates=False)
     mflat, oflat = S.encode_model(m), S.encode_options(opts)
     plans, kept, left_out = [], 0, []
     for i, b in enumerate(books):
@@ -537,7 +551,7 @@ def reference_arm(a) -> dict:
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(trades, a.netting_sets, a.paths), "paths_per_step": paths,
+            "config": {"workload": workload_name(trades, a.netting_sets, a.paths, foreign_rates=False), "paths_per_step": paths,
                        "simulation_dates": nT, "trades_timed": kept, "netting_sets_timed": len(plans),
                        "netting_sets_left_out": left_out},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
@@ -637,8 +651,10 @@ def main():
             if a.no_cpu:
                 raise RuntimeError("skipped (--no-cpu)")
             r = reference_arm(replace_args(a, steps=1, warmup=0, cpu_seconds=a.cpu_seconds / 2))
-            if "unavailable" in r:  # the reference library is absent: the plain-C restatement on this book's plans
-                cv, cpaths, cthreads, cdt, _, ckind = cpu_reference(plans, trades, a.cpu_seconds / 2)
+            if "unavailable" in r:  # the reference library is absent: the plain-C restatement of its kernels, on the
+                # book in the reference's model family (the restatement has no stochastic foreign rates)
+                lplans = workload(a.paths, a.trades, a.netting_sets, foreign_rates=False)[4]
+                cv, cpaths, cthreads, cdt, _, ckind = cpu_reference(lplans, trades, a.cpu_seconds / 2)
                 cpu = {"value": cv, "unit": UNIT, "cores": cthreads, "kind": ckind,
                        "sample": f"{cpaths} of {nP} paths of all {len(plans)} netting sets (the plain-C restatement of "
                                  f"gpu::runFusedReference, {cthreads} threads)"}

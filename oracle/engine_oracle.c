@@ -139,6 +139,16 @@ static double hw_evolve(const HW* m, double t0, double t1, double z1, double z2,
   return intX + intPhi;
 }
 
+/* The foreign rate's step under the domestic measure: hw_evolve with the quanto drift -q of x_f,
+ * q = rho(x_f, S_f) sigma_f sigma_S, added to the state and to its integral (an extension: the reference's
+ * foreign curves are deterministic). */
+static double hw_evolve_drift(const HW* m, double t0, double t1, double z1, double z2, double q, double* x) {
+  const double a = m->a, dt = t1 - t0, e = exp(-a * dt);
+  const double integrated = hw_evolve(m, t0, t1, z1, z2, x);
+  *x -= q * (1.0 - e) / a;
+  return integrated - q / a * (dt - (1.0 - e) / a);
+}
+
 /* ---- CIR++ intensity (cir_intensity.cpp:25-66) */
 static double cir_survival(const Credit* c, double t) {
   if (t <= 0.0) return 1.0;
@@ -221,6 +231,12 @@ typedef struct {
   Credit* credits;
   double *corr, *base;
   int antithetic;
+  /* Stochastic foreign rates (an extension of the reference's model, whose foreign curves are deterministic):
+   * foreign[f] is the Hull-White model of asset f's currency on that asset's carry curve, XF[f] its state
+   * [path][date] once simulated. */
+  size_t nF;
+  HW foreign[2];
+  double* XF[2];
 } Model;
 
 typedef struct {
@@ -263,22 +279,36 @@ static int read_model(const double* a, size_t n, Model* m, char* err, size_t len
     c->market.hazard = (double*)calloc(c->market.n + 1, sizeof(double));
     for (size_t q = 0; q < c->market.n; ++q) c->market.pillar[q] = next(&r), c->market.hazard[q] = next(&r);
   }
-  m->F = 1 + m->nA + m->nC;
   const size_t f = count(&r);
-  m->corr = (double*)calloc(m->F * m->F, sizeof(double));
-  if (f == 0) {
-    for (size_t i = 0; i < m->F; ++i) m->corr[i * m->F + i] = 1.0;
-  } else if (f != m->F) {
-    return fail(err, len, "model: correlation matrix has wrong dimension");
-  } else {
-    for (size_t i = 0; i < f * f; ++i) m->corr[i] = next(&r);
-  }
+  if (f > 8) return fail(err, len, "model: correlation matrix has wrong dimension");
+  double* given = (double*)calloc(f * f + 1, sizeof(double));
+  for (size_t i = 0; i < f * f; ++i) given[i] = next(&r);
   m->nP = count(&r);
   next(&r); /* seed: unused with injected normals */
   m->antithetic = next(&r) != 0.0;
   m->nBase = count(&r);
   m->base = (double*)calloc(m->nBase + 1, sizeof(double));
   for (size_t k = 0; k < m->nBase; ++k) m->base[k] = next(&r);
+  if (r.i < r.n) { /* the foreign-rate block: 7011, nF, (a, sigma) per leading asset */
+    if (next(&r) != 7011.0) return free(given), fail(err, len, "model: unknown trailing block");
+    m->nF = count(&r);
+    if (m->nF > 2 || m->nF > m->nA) return free(given), fail(err, len, "model: at most two foreign rates, one per leading asset");
+    for (size_t q = 0; q < m->nF; ++q) {
+      m->foreign[q].curve = m->assets[q].carry; /* shared with the asset: freed once, with the asset */
+      m->foreign[q].a = next(&r), m->foreign[q].sigma = next(&r);
+    }
+  }
+  m->F = 1 + m->nA + m->nC + m->nF;
+  m->corr = (double*)calloc(m->F * m->F, sizeof(double));
+  if (f == 0) {
+    for (size_t i = 0; i < m->F; ++i) m->corr[i * m->F + i] = 1.0;
+  } else if (f != m->F) {
+    free(given);
+    return fail(err, len, "model: correlation matrix has wrong dimension");
+  } else {
+    for (size_t i = 0; i < f * f; ++i) m->corr[i] = given[i];
+  }
+  free(given);
   if (r.bad) return fail(err, len, "spec: truncated array");
   if (m->hw.curve.n == 0 || m->hw.a <= 1e-8 || m->hw.sigma < 0.0) return fail(err, len, "model: invalid rate model");
   for (size_t k = 0; k < m->nC; ++k)
@@ -427,17 +457,21 @@ static void value_at(const Model* m, const Trade* tr, const Grid* g, size_t j, c
   if (t >= tr->maturity - 1e-10) return;
   const Asset* as = &m->assets[tr->asset];
   const double carry = discount(&as->carry, tr->maturity) / discount(&as->carry, t);
+  /* The foreign discount bond: the deterministic carry, or with a stochastic foreign rate P_f(t, T | x_f). */
+  const int stochastic = tr->asset < m->nF;
+#define FOREIGN_BOND(p) (stochastic ? hw_bond(&m->foreign[tr->asset], t, tr->maturity, m->XF[tr->asset][(p) * nT + j]) : carry)
   if (tr->kind == 1) {
     for (size_t p = 0; p < nP; ++p)
-      out[p] = tr->notional * (S[tr->asset][p * nT + j] * carry - tr->strike * hw_bond(&m->hw, t, tr->maturity, X[p * nT + j]));
+      out[p] = tr->notional * (S[tr->asset][p * nT + j] * FOREIGN_BOND(p) - tr->strike * hw_bond(&m->hw, t, tr->maturity, X[p * nT + j]));
     return;
   }
   const double sd = as->vol * sqrt(tr->maturity - t);
   for (size_t p = 0; p < nP; ++p) {
     const double df = hw_bond(&m->hw, t, tr->maturity, X[p * nT + j]);
-    const double fwd = S[tr->asset][p * nT + j] * carry / df;
+    const double fwd = S[tr->asset][p * nT + j] * FOREIGN_BOND(p) / df;
     out[p] = tr->notional * black(tr->call, fwd, tr->strike, sd, df);
   }
+#undef FOREIGN_BOND
 }
 
 /* A Bermudan swaption on every path and date (bermudan_swaption.cpp:49-146): exercise values of the tail swaps,
@@ -702,7 +736,8 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
 
   /* Scenarios from the injected normals: normal k of step j on stream s at z[((j - 1) nNormals + k) streams + s];
    * path p reads stream p >> 1 with sign (-1)^(p & 1) when antithetic (scenario_generator.cpp:94-141). */
-  size_t nNormals = F + 1;
+  const size_t nF = m.nF;
+  size_t nNormals = F + 1 + nF; /* drivers | rate integral | foreign rate integrals | CIR bridges */
   size_t* cOff = (size_t*)calloc(nC + 1, sizeof(size_t));
   for (size_t c = 0; c < nC; ++c) cOff[c] = nNormals, nNormals += m.credits[c].sub - 1;
   double* L = (double*)malloc(F * F * sizeof(double));
@@ -715,6 +750,8 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
   double** S = (double**)calloc(nA + 1, sizeof(double*));
   for (size_t a = 0; a < nA; ++a) S[a] = (double*)calloc(nP * nT, sizeof(double));
   double* Q0 = (double*)malloc(nP * nT * sizeof(double));
+  for (size_t f = 0; f < nF; ++f) m.XF[f] = (double*)calloc(nP * nT, sizeof(double));
+  double xf[2] = {0.0, 0.0}, intF[2] = {0.0, 0.0};
   double *w = (double*)malloc(F * sizeof(double)), *step = (double*)malloc(nNormals * sizeof(double));
   double *spot = (double*)calloc(nA + 1, sizeof(double)), *y = (double*)calloc(nC + 1, sizeof(double));
   double* iy = (double*)calloc(nC + 1, sizeof(double));
@@ -727,6 +764,7 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
       break;
     }
     double x = 0.0, defl = 1.0;
+    xf[0] = xf[1] = 0.0;
     Dm[p * nT] = 1.0, Q0[p * nT] = 1.0;
     for (size_t a = 0; a < nA; ++a) spot[a] = m.assets[a].spot, S[a][p * nT] = spot[a];
     for (size_t c = 0; c < nC; ++c) y[c] = m.credits[c].y0, iy[c] = 0.0;
@@ -741,9 +779,15 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
       const double integrated = hw_evolve(&m.hw, t0, t1, w[0], step[F], &x);
       defl *= exp(-integrated);
       X[p * nT + j] = x, Dm[p * nT + j] = defl;
+      for (size_t f = 0; f < nF; ++f) {
+        const size_t fi = 1 + nA + nC + f;
+        const double q = m.corr[fi * F + 1 + f] * m.foreign[f].sigma * m.assets[f].vol;
+        intF[f] = hw_evolve_drift(&m.foreign[f], t0, t1, w[fi], step[F + 1 + f], q, &xf[f]);
+        m.XF[f][p * nT + j] = xf[f];
+      }
       for (size_t a = 0; a < nA; ++a) {
         const Asset* as = &m.assets[a];
-        const double dt = t1 - t0, carry = log(discount(&as->carry, t0) / discount(&as->carry, t1));
+        const double dt = t1 - t0, carry = a < nF ? intF[a] : log(discount(&as->carry, t0) / discount(&as->carry, t1));
         const double drift = integrated - carry - 0.5 * as->vol * as->vol * dt;
         spot[a] = spot[a] * exp(drift + as->vol * sqrt(dt) * w[1 + a]);
         S[a][p * nT + j] = spot[a];
@@ -830,6 +874,7 @@ int orc_engine_run(const double* model, size_t nm, const double* ns, size_t nn, 
     free(prof), free(E), free(DR), free(V), free(C);
   }
 done:
+  for (size_t f = 0; f < nF; ++f) free(m.XF[f]);
   for (size_t a = 0; a < nA; ++a) free(S[a]);
   free(S), free(X), free(Dm), free(Q0);
   free(rep.t), free(sim.t);

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def book():
-    m, books, _, _ = W.correlated_csa_book(2048, 10, 100)
+    m, books, _, _ = W.correlated_csa_book(2048, 10, 100, foreign_rates=False)
     return SB.make_book(m, books)
 
 

@@ -69,7 +69,7 @@ def test_swap_portfolio_full_size_fp64_against_the_engine(ctx):
 # ---------------------------------------------------------------- the correlated CSA book
 @pytest.fixture(scope="module")
 def book():
-    m, books, o, trades = workloads.correlated_csa_book(BOOK_PATHS)
+    m, books, o, trades = workloads.correlated_csa_book(BOOK_PATHS, foreign_rates=False)
     return m, books, o, [gpu.compile(m, b, o) for b in books]
 
 
@@ -126,3 +126,4 @@ def test_fp32_error_is_below_the_monte_carlo_error_on_the_book(ctx):
     r = precision.compare(ctx, m, books, o, own)
     for key, v in r["outputs"].items():
         assert v["max_err_over_se"] < 1.0, (key, v)
+        assert v["max_rel_err_without_mc_error"] <= 1e-4, (key, v)  # date 0: single-precision rounding only

@@ -224,6 +224,10 @@ struct Plan {
   bool im = false;
   std::vector<uint32_t> imSlots;  // [nR][2]
   bool usesAssets = false, probes = false;
+  // Stochastic foreign rates (an extension of the reference's plan): nF of them, one per leading asset; the step
+  // rows hold stepStride = 24 + 8 nF values (header word 10 counts them in fours).
+  uint32_t nF = 0, stepStride = kStepStride;
+  bool usesForeign = false;
   bool amcOrProbe = false;  // some term is an AMC or probe term (the lean revalue variant cannot run the plan)
   // The term table lowered for the revalue kernel (lowerTerms).
   std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, assetBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot
@@ -250,12 +254,18 @@ Plan<R> parse(const View<R>& v, size_t index) {
   p.nInner = H[hInner], p.rowIm = H[hRowIm];
   std::memcpy(&p.imLevel, &H[hImLevel], sizeof(float));
   if (!v.params || v.params_len != static_cast<size_t>(kParamCount)) throw bad("params must hold 84 values");
-  if (!v.steps || v.steps_len != static_cast<size_t>(p.nT) * kStepStride) throw bad("steps must hold nT * 24 values");
+  const uint32_t stepVec = H[hStepVec];
+  if (stepVec != 6 && stepVec != 8 && stepVec != 10) throw bad("step rows must hold 24 values (28 or 40 with stochastic foreign rates)");
+  p.nF = (stepVec - 6) / 2, p.stepStride = 4 * stepVec;
+  if (!v.steps || v.steps_len != static_cast<size_t>(p.nT) * p.stepStride) throw bad("steps must hold nT * (step row) values");
   if (p.nA > kMaxAssets) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: at most 4 assets", index);
   if (p.nC > kMaxCredits) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: at most 2 credits", index);
-  if (p.nCorr != 1 + p.nA + p.nC || p.nCorr > kChol) throw bad("number of correlated factors must be 1 + assets + credits");
+  if (p.nF > p.nA) throw bad("more stochastic foreign rates than assets");
+  if (p.nCorr != 1 + p.nA + p.nC + p.nF || p.nCorr > kChol)
+    throw bad("number of correlated factors must be 1 + assets + credits + foreign rates");
   if (p.sub == 0) throw bad("CIR sub-steps must be positive");
-  if (p.nNormals > kMaxNormals || p.nNormals < p.nCorr + 1 + p.nC * (p.sub - 1)) throw bad("inconsistent number of normals per step");
+  if (p.nNormals > kMaxNormals || p.nNormals < p.nCorr + 1 + p.nF + p.nC * (p.sub - 1)) throw bad("inconsistent number of normals per step");
+  if (p.nF > 0 && p.nInner > 0) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the nested initial margin with stochastic foreign rates", index);
   if (p.nC > 0 && p.cpty >= p.nC) throw bad("counterparty index out of range");
   if (p.offCall != p.nT + 1 || p.offRep != 2 * p.nT + 1) throw bad("index table offsets do not match the reference layout");
   if (!v.indices || v.indices_len < 3 * static_cast<size_t>(p.nT) + 1) throw bad("index table too short");
@@ -308,12 +318,19 @@ Plan<R> parse(const View<R>& v, size_t index) {
     const R* rec = v.terms + t * kTermStride;
     if (!(rec[0] >= R(0)) || rec[0] >= R(4294967296.0)) throw bad("invalid term code");
     const uint32_t code = static_cast<uint32_t>(rec[0]), kind = code & 15u;
+    if (kind > kForeignOption) throw bad("unknown term kind");
+    if (kind == kForeignForward || kind == kForeignOption) {  // rec[1] is B_f; the asset sits in the code's extra field
+      if ((code >> 12u) >= p.nF) throw bad("a foreign-rate term on an asset without a stochastic foreign rate");
+      if (!(rec[1] >= R(0))) throw bad("invalid foreign bond coefficient");
+      p.usesAssets = p.usesForeign = true;
+      continue;
+    }
     // rec[1] is an index (swap slot, asset, probe selector) except for continuation terms, where it holds
     // the Bermudan's position.
     if (kind != kBermContinue && (!(rec[1] >= R(0)) || rec[1] >= R(4294967296.0))) throw bad("invalid term slot");
     const uint32_t slot = kind == kBermContinue ? 0u : static_cast<uint32_t>(rec[1]);
     if (kind == kAsset || kind == kOption) p.usesAssets = true;
-    if (kind > kOption) p.amcOrProbe = true;
+    if (kind > kOption && kind <= kProbe) p.amcOrProbe = true;
     if (kind == kProbe) {
       const uint32_t what = slot & 15u;
       if (what == 2 || what == 6) p.usesAssets = true;
@@ -337,7 +354,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
     for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
       const uint32_t kind = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]) & 15u;
       p.termEvals += 1;
-      if (kind != kAsset && kind != kBermDecide && kind != kBermContinue) p.expEvals += 1;
+      if (kind != kAsset && kind != kBermDecide && kind != kBermContinue) p.expEvals += kind == kForeignOption ? 2 : 1;
     }
   }
   for (size_t q = 0; q < p.nReq; ++q) {
@@ -442,13 +459,16 @@ void lowerTerms(Plan<R>& p) {
 template <typename R>
 bool sameScenario(const Plan<R>& a, const Plan<R>& b) {
   if (a.nP != b.nP || a.nT != b.nT || a.nA != b.nA || a.nC != b.nC || a.sub != b.sub || a.nNormals != b.nNormals ||
-      a.seed != b.seed || a.anti != b.anti || a.nCorr != b.nCorr)
+      a.seed != b.seed || a.anti != b.anti || a.nCorr != b.nCorr || a.nF != b.nF)
     return false;
   if (std::memcmp(a.v.params, b.v.params, 8 * sizeof(R)) || std::memcmp(a.v.params + 12, b.v.params + 12, (4 + 64) * sizeof(R)))
     return false;
-  for (uint32_t j = 0; j < a.nT; ++j)
-    if (std::memcmp(a.v.steps + static_cast<size_t>(j) * kStepStride, b.v.steps + static_cast<size_t>(j) * kStepStride, 22 * sizeof(R)))
+  for (uint32_t j = 0; j < a.nT; ++j) {
+    const R* ra = a.v.steps + static_cast<size_t>(j) * a.stepStride;
+    const R* rb = b.v.steps + static_cast<size_t>(j) * b.stepStride;
+    if (std::memcmp(ra, rb, 22 * sizeof(R)) || std::memcmp(ra + kStepStride, rb + kStepStride, (a.stepStride - kStepStride) * sizeof(R)))
       return false;
+  }
   return true;
 }
 
@@ -592,15 +612,17 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     ScenarioArgs<R>& sc = L.sc;
     sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
     sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
+    sc.nF = P0.nF, sc.stepStride = P0.stepStride;
     sc.steps = nullptr, sc.normals = nullptr;
     for (int k = 0; k < 8; ++k) sc.cir[k] = P0.v.params[k];
     for (int k = 0; k < 4; ++k) sc.spots[k] = P0.v.params[12 + k];
     for (int k = 0; k < 64; ++k) sc.chol[k] = P0.v.params[16 + k];
     CubeArgs<R>& cb = L.cb;
     cb.nP = P0.nP, cb.nT = P0.nT, cb.nA = P0.nA, cb.nC = P0.nC;
-    cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fLnS = 2 + P0.nA + P0.nC, cb.fY = 2 + 2 * P0.nA + P0.nC;
+    cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fXf = 2 + P0.nA + P0.nC, cb.nF = P0.nF;
+    cb.fLnS = cb.fXf + P0.nF, cb.fY = cb.fLnS + P0.nA;
     cb.probes = L.probes ? 1u : 0u;
-    L.numFields = L.probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC;
+    L.numFields = (L.probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC) + P0.nF;
     if (revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8, 1) > 200 * 1024)
       throw fail(ZK_ERR_UNSUPPORTED, "a netting set needs more shared memory than a CTA has");
   }
@@ -618,7 +640,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     auto& D = B->dev[i];
     D.dates = take(P.dates.size() * 4);
     D.table = take(P.table.size() * sizeof(R));
-    D.steps = take(static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
+    D.steps = take(static_cast<size_t>(P.nT) * P.stepStride * sizeof(R));
     D.req = take(P.nReq * kRequestStride * sizeof(R));
     if (P.im) {
       D.imSlots = take(P.imSlots.size() * 4);
@@ -696,7 +718,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
       const auto& D = B.dev[i];
       std::memcpy(img + D.dates, P.dates.data(), P.dates.size() * 4);
       std::memcpy(img + D.table, P.table.data(), P.table.size() * sizeof(R));
-      std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * kStepStride * sizeof(R));
+      std::memcpy(img + D.steps, P.v.steps, static_cast<size_t>(P.nT) * P.stepStride * sizeof(R));
       if (P.nReq) std::memcpy(img + D.req, P.v.requests, P.nReq * kRequestStride * sizeof(R));
       if (P.im) {
         std::memcpy(img + D.imSlots, P.imSlots.data(), P.imSlots.size() * 4);
@@ -726,6 +748,8 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
       A.rowTrades = P.rowTrades, A.rowEx = P.rowEx;
       A.offCall = P.offCall, A.offRep = P.offRep, A.nSlots = P.nSlots, A.ring = P.ring;
       A.usesAssets = P.usesAssets ? 1u : 0u;
+      A.usesForeign = P.usesForeign ? 1u : 0u;
+      A.stepStride = P.stepStride;
       if (P.im && !B.sink) {
         A.imState = static_cast<R*>(dptr(D.imState));
         A.imWords = 5 + P.nSlots;

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
   R* bridge = reinterpret_cast<R*>(simRaw) + static_cast<size_t>(sc.nNormals) * kSimThreads;
   if (bridgeTable) {
     for (uint32_t jj = threadIdx.x + 1; jj < sc.nT; jj += blockDim.x) {
-      const R dt = sc.steps[static_cast<size_t>(jj) * kStepStride + 6], h = dt / static_cast<R>(sc.substeps);
+      const R dt = sc.steps[static_cast<size_t>(jj) * sc.stepStride + 6], h = dt / static_cast<R>(sc.substeps);
       R remT = dt;
       for (uint32_t q = 0; q < nB; ++q) {
         bridge[(static_cast<size_t>(jj) * nB + q) * 2] = h / remT;
@@ -155,6 +155,7 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
   R x = R(0), D = R(1);
   double lnD = 0.0;
   R S[4], lnS[4] = {R(0), R(0), R(0), R(0)}, y[2], Y[2] = {R(0), R(0)};
+  R xf[2] = {R(0), R(0)};  // stochastic foreign short-rate states of assets 0 and 1
 #pragma unroll
   for (int a = 0; a < 4; ++a) S[a] = sc.spots[a];
 #pragma unroll
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
   for (uint32_t j = 0; j < nT; ++j) {
     R Qc[2] = {R(1), R(1)};
     if (j > 0) {
-      const R* step = sc.steps + static_cast<size_t>(j) * kStepStride;
+      const R* step = sc.steps + static_cast<size_t>(j) * sc.stepStride;
       drawDate<R>(stream, j, sign, sc.normals, sc.nStreams, injectedStream, sc.nNormals, col);
       // Correlated drivers: each padded Cholesky row as two 4-term dot products (as the reference).
       R z[8];
@@ -183,15 +184,35 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
       x = x * step[0] + step[1] * w[0];
       lnD -= static_cast<double>(integratedRate);
       D = rexp(static_cast<R>(lnD));
+      // Stochastic foreign rates: the exact Hull-White step of x_f (with its quanto drift) and of its integral, on
+      // driver 1 + nA + nC + f and the independent normal nCorr + 1 + f; the asset's carry is then the simulated
+      // integral of r_f instead of the deterministic one.
+      R carry[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) carry[a] = step[8 + a];
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        if (static_cast<uint32_t>(f) < sc.nF) {
+          const R* fs = step + kStepStride + 8 * f;
+          const uint32_t wi = 1 + sc.nA + sc.nC + f;
+          R wf = w[7];
+#pragma unroll
+          for (int i = 6; i >= 0; --i)
+            if (wi == static_cast<uint32_t>(i)) wf = w[i];
+          const R zf = normal(sc.nCorr + 1 + f);
+          carry[f] = xf[f] * fs[5] + fs[2] * wf + fs[3] * zf + fs[4] + fs[7];
+          xf[f] = xf[f] * fs[0] + fs[1] * wf + fs[6];
+        }
+      }
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         if (static_cast<uint32_t>(a) < sc.nA) {
-          lnS[a] = lnS[a] + (integratedRate - step[8 + a] - step[16 + a] + step[12 + a] * w[1 + a]);
+          lnS[a] = lnS[a] + (integratedRate - carry[a] - step[16 + a] + step[12 + a] * w[1 + a]);
           S[a] = sc.spots[a] * rexp(lnS[a]);
         }
       }
       const R dt = step[6];
-      uint32_t off = sc.nCorr + 1;
+      uint32_t off = sc.nCorr + 1 + sc.nF;
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         if (static_cast<uint32_t>(c) < sc.nC) {
@@ -229,6 +250,7 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
     put(1, j, D);
     for (uint32_t a = 0; a < sc.nA; ++a) put(cb.fS + a, j, sel4(S, a));
     for (uint32_t c = 0; c < sc.nC; ++c) put(cb.fQ + c, j, c == 0 ? Qc[0] : Qc[1]);
+    for (uint32_t f = 0; f < sc.nF; ++f) put(cb.fXf + f, j, f == 0 ? xf[0] : xf[1]);
     if (cb.probes) {
       for (uint32_t a = 0; a < sc.nA; ++a) put(cb.fLnS + a, j, sel4(lnS, a));
       for (uint32_t c = 0; c < sc.nC; ++c) put(cb.fY + c, j, c == 0 ? y[0] : y[1]);
@@ -514,6 +536,23 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
           }
           break;
         }
+        case kForeignForward: {  // c S P_f(t, T | x_f), P_f = A_f e^{-B_f x_f}: the foreign bond of the asset's currency
+          const uint32_t a = min(extra, 1u);
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) term[i] = c * pick4<R, PPT>(S, a, i) * (rec[3] * fastExp(-rec[1] * cube(cb.fXf + a, j, i)));
+          break;
+        }
+        case kForeignOption: {  // Black on S P_f(t, T | x_f) / P(t, T | x)
+          const uint32_t a = min(extra, 1u);
+          const R p3 = rec[7];
+#pragma unroll
+          for (int i = 0; i < PPT; ++i) {
+            const R b0 = rec[3] * fastExp(nB * x[i]);
+            const R q = rec[5] * fastExp(-rec[1] * cube(cb.fXf + a, j, i));
+            term[i] = c * black(pick4<R, PPT>(S, a, i) * q / b0, rec[6], fabs(p3), b0, p3 > R(0));
+          }
+          break;
+        }
         default:
           if constexpr (!kLean) switch (kind) {  // the AMC and probe terms (absent from lean launches)
           case kBermExercise:
@@ -610,7 +649,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
       R collateral = R(0);
       if (hasCsa) {
         R price = R(1);
-        if (ctype == 1) price = A.steps[static_cast<size_t>(j) * kStepStride + 22] * rexp(-A.steps[static_cast<size_t>(j) * kStepStride + 23] * x[i]);
+        if (ctype == 1) price = A.steps[static_cast<size_t>(j) * A.stepStride + 22] * rexp(-A.steps[static_cast<size_t>(j) * A.stepStride + 23] * x[i]);
         else if (ctype == 2) price = pick4<R, PPT>(S, min(A.casset, 3u), i);
         R vc, pc = price;
         if (shortLook) {

@@ -27,7 +27,11 @@ constexpr std::size_t kMaxInnerPaths = 1024, kInnerTop = 16;  // nested initial 
 constexpr std::size_t kParamCount = 84, kMaxSamples = 64, kPfeBins = 3072, kStatsPerDate = 8, kTradeStats = 5;
 constexpr std::uint32_t kNoRow = 0xFFFFFFFFu;
 enum Kind { kBond = 0, kFixedFloat = 1, kAsset = 2, kSetFixing = 3, kOption = 4, kBermExercise = 5, kBermDecide = 6,
-            kBermContinue = 7, kBermBond = 8, kBermFloat = 9, kProbe = 10 };
+            kBermContinue = 7, kBermBond = 8, kBermFloat = 9, kProbe = 10,
+            // Terms on an asset whose foreign rate is stochastic (an extension; asset index in the extra field):
+            // kForeignForward (B_f, c, A_f): c S P_f(t, T | x_f); kForeignOption (B_f, N, A, B, A_f, K, +-sd): Black on
+            // S P_f(t, T | x_f) / P(t, T | x) with the reference's volatility.
+            kForeignForward = 11, kForeignOption = 12 };
 enum Op { kRowQuantile = 0, kRowMean = 1, kRowMeanPos = 2, kRowMeanNeg = 3, kRowSamples = 4, kRowHistogram = 5,
           kRowMeanProduct = 6, kRowQuantilePos = 7, kRowMeanPosTimes = 8, kRowMeanNegTimes = 9 };
 
@@ -185,14 +189,25 @@ Model decodeModel(const double* a, std::size_t n) {
     m.credits.push_back(c);
   }
   const std::size_t F = in.u();
-  if (F > 0) {
-    if (F != m.numFactors()) throw std::invalid_argument("correlation matrix has wrong dimension");
-    for (std::size_t k = 0; k < F * F; ++k) m.correlation.push_back(in.d());
-  }
+  if (F > 8) throw std::invalid_argument("correlation matrix has wrong dimension");
+  for (std::size_t k = 0; k < F * F; ++k) m.correlation.push_back(in.d());
   m.numPaths = in.u();
   m.seed = static_cast<std::uint64_t>(in.d());
   m.antithetic = in.d() != 0.0;
   m.base = readSeq(in);
+  if (in.i < in.n) {  // stochastic foreign rates (the spec module's extension block)
+    if (in.d() != 7011.0) throw std::invalid_argument("model: unknown trailing block");
+    const std::size_t nF = in.u();
+    if (nF > nA || nF > 2) throw std::invalid_argument("model: at most two stochastic foreign rates, one per leading asset");
+    for (std::size_t f = 0; f < nF; ++f) {
+      HullWhite h;
+      h.curve = m.assets[f].carry;
+      h.a = in.d(), h.sigma = in.d();
+      if (h.a <= 1e-8 || h.sigma < 0.0) throw std::invalid_argument("foreign HullWhite1F: invalid parameters");
+      m.foreign.push_back(h);
+    }
+  }
+  if (F > 0 && F != m.numFactors()) throw std::invalid_argument("correlation matrix has wrong dimension");
   return m;
 }
 
@@ -311,7 +326,7 @@ bool sameBond(const Term& a, const Term& b) { return a.A == b.A && a.B == b.B; }
 // bonds of one (A, B) summed; a running coupon with the bond of its payment date folded into p1;
 // forwards on one asset summed; options, AMC terms and fixings kept, fixings last.
 std::vector<Term> merge(const std::vector<Term>& in) {
-  std::vector<Term> floating, bonds, assets, options, fixings, exercise, amc;
+  std::vector<Term> floating, bonds, assets, options, fixings, exercise, amc, foreignFwd;
   for (const Term& r : in) {
     switch (r.kind) {
       case kBond: {
@@ -339,6 +354,14 @@ std::vector<Term> merge(const std::vector<Term>& in) {
       }
       case kSetFixing: fixings.push_back(r); break;
       case kOption: options.push_back(r); break;
+      case kForeignForward: {
+        auto it = std::find_if(foreignFwd.begin(), foreignFwd.end(),
+                               [&](const Term& a) { return a.extra == r.extra && a.slot == r.slot && a.A == r.A; });
+        if (it == foreignFwd.end()) foreignFwd.push_back(r);
+        else it->c += r.c;
+        break;
+      }
+      case kForeignOption: options.push_back(r); break;
       case kBermExercise: {
         auto it = std::find_if(exercise.begin(), exercise.end(), [&](const Term& b) { return b.bermudan == r.bermudan && sameBond(b, r); });
         if (it == exercise.end()) exercise.push_back(r);
@@ -359,6 +382,8 @@ std::vector<Term> merge(const std::vector<Term>& in) {
     out.push_back(Term{kBond, 0.0, b.c * b.A, 1.0, b.B, 0.0, 0.0, 0.0, 0, 0, 0, true});
   }
   for (const Term& a : assets)
+    if (a.c != 0.0) out.push_back(a);
+  for (const Term& a : foreignFwd)
     if (a.c != 0.0) out.push_back(a);
   out.insert(out.end(), options.begin(), options.end());
   out.insert(out.end(), exercise.begin(), exercise.end());
@@ -416,10 +441,32 @@ void stepRow(const Model& m, double t0, double t1, double* row) {
     row[16 + k] = 0.5 * s.vol * s.vol * dt;
   }
   for (std::size_t c = 0; c < m.credits.size(); ++c) row[20 + c] = m.credits[c].integratedShift(t1);
+  // Stochastic foreign rate f (an extension): x_f of the foreign Hull-White model under the domestic measure, with
+  // the quanto drift -rho(f, S_f) sigma_f sigma_S of its asset's volatility, and the integral of r_f = x_f + phi_f,
+  // stepped exactly as the domestic rate: [0] e^{-a dt}, [1] sd of x_f, [2] [3] the integral's loadings, [4] the
+  // integral of phi_f, [5] (1 - e^{-a dt}) / a, [6] the drift's contribution to x_f, [7] to its integral.
+  for (std::size_t f = 0; f < m.foreign.size(); ++f) {
+    const HullWhite& h = m.foreign[f];
+    const double af = h.a, sf = h.sigma, ef = std::exp(-af * dt), s2f = sf * sf;
+    const double vX = s2f * (1 - ef * ef) / (2 * af);
+    const double vI = s2f / (af * af) * (dt - 2 * (1 - ef) / af + (1 - ef * ef) / (2 * af));
+    const double cv = s2f / (2 * af * af) * (1 - ef) * (1 - ef);
+    const double sd = std::sqrt(vX), k1 = sd > 0 ? cv / sd : 0.0, k2 = std::sqrt(std::max(vI - k1 * k1, 0.0));
+    const double g = dt - 2 / af * (std::exp(-af * t0) - std::exp(-af * t1)) + 0.5 / af * (std::exp(-2 * af * t0) - std::exp(-2 * af * t1));
+    const std::size_t fi = 1 + m.assets.size() + m.credits.size() + f;
+    const double q = m.correlationOf(fi, 1 + f) * sf * m.assets[f].vol;
+    double* r = row + 24 + 8 * f;
+    r[0] = ef, r[1] = sd, r[2] = k1, r[3] = k2;
+    r[4] = std::log(h.curve.discount(t0) / h.curve.discount(t1)) + s2f / (2 * af * af) * g;
+    r[5] = (1 - ef) / af;
+    r[6] = -q * (1 - ef) / af;
+    r[7] = -q / af * (dt - (1 - ef) / af);
+  }
 }
 
 NestProgram nestProgram(const Model& m, const double* periods, std::size_t nPer, const double* terminals, std::size_t nTerm, double t) {
   constexpr double kEps = 1e-10;  // the trades' tolerance for "on or before t" (nested_exposure.cpp:19)
+  if (!m.foreign.empty()) throw std::invalid_argument("the nested exposure runs the reference's model: no stochastic foreign rates");
   NestProgram P;
   P.nA = m.assets.size();
   // Event dates after t (nested_exposure.cpp:87-117): fixings after t, payments and terminal flows after t.
@@ -553,8 +600,11 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   P.numTrades = ns.trades.size();
 
   // ---- step coefficients (the exact transitions of hull_white.cpp:40-68 and lognormal_asset.cpp:17-22)
-  P.steps.assign(nT * kStepStride, 0.0);
-  for (std::size_t j = 1; j < nT; ++j) stepRow(m, grid.t[j - 1], grid.t[j], &P.steps[j * kStepStride]);
+  const std::size_t stride = m.stepStride();
+  P.steps.assign(nT * stride, 0.0);
+  for (std::size_t j = 1; j < nT; ++j) stepRow(m, grid.t[j - 1], grid.t[j], &P.steps[j * stride]);
+  if (!m.foreign.empty() && o.imInnerPaths > 0)
+    throw std::invalid_argument("the nested initial margin runs the reference's model: no stochastic foreign rates");
 
   // ---- valuation terms per date
   std::vector<std::vector<Term>> at(nT);
@@ -634,7 +684,13 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
       for (std::size_t j = 0; j < nT; ++j) {
         const double t = grid.t[j];
         if (t >= tr.maturity - 1e-10) continue;
-        add(j, kAsset, static_cast<double>(tr.asset), tr.notional, s.carryDiscount(t, tr.maturity), 0.0);
+        if (tr.asset < m.foreign.size()) {
+          const HullWhite& h = m.foreign[tr.asset];
+          at[j].push_back(Term{kForeignForward, h.B(t, tr.maturity), tr.notional, h.bond(t, tr.maturity, 0.0), 0.0, 0.0, 0.0, 0.0,
+                               tradeIndex, 0, tr.asset});
+        } else {
+          add(j, kAsset, static_cast<double>(tr.asset), tr.notional, s.carryDiscount(t, tr.maturity), 0.0);
+        }
         add(j, kBond, 0, -tr.notional * tr.strike, bondA(t, tr.maturity), bondB(t, tr.maturity));
       }
     } else if (tr.kind == Trade::kOption) {
@@ -644,8 +700,14 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
         const double t = grid.t[j];
         if (t >= tr.maturity - 1e-10) continue;
         const double sd = s.vol * std::sqrt(tr.maturity - t);
-        add(j, kOption, static_cast<double>(tr.asset), tr.notional, bondA(t, tr.maturity), bondB(t, tr.maturity),
-            s.carryDiscount(t, tr.maturity), tr.strike, tr.call ? sd : -sd);
+        if (tr.asset < m.foreign.size()) {
+          const HullWhite& h = m.foreign[tr.asset];
+          at[j].push_back(Term{kForeignOption, h.B(t, tr.maturity), tr.notional, bondA(t, tr.maturity), bondB(t, tr.maturity),
+                               h.bond(t, tr.maturity, 0.0), tr.strike, tr.call ? sd : -sd, tradeIndex, 0, tr.asset});
+        } else {
+          add(j, kOption, static_cast<double>(tr.asset), tr.notional, bondA(t, tr.maturity), bondB(t, tr.maturity),
+              s.carryDiscount(t, tr.maturity), tr.strike, tr.call ? sd : -sd);
+        }
       }
     } else {
       if (bermudans >= kMaxBermudans) throw std::invalid_argument("the GPU kernel prices at most 4 Bermudan swaptions");
@@ -929,7 +991,7 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
 
   // ---- parameters: CIR x2 | CSA | spots | Cholesky rows | collateral security
   const std::size_t nCorr = m.numFactors();
-  std::size_t numNormals = nCorr + 1;
+  std::size_t numNormals = nCorr + 1 + m.foreign.size();  // drivers | rate integral | foreign integrals | CIR bridges
   for (const auto& c : m.credits) numNormals += c.substeps - 1;
   if (numNormals > kMaxNormals) throw std::invalid_argument("too many normals per step for the GPU kernel");
   std::vector<double> corr = m.correlation;
@@ -961,8 +1023,8 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
     if (c.type == 1) {
       if (c.bondMaturity < grid.t.back() - 1e-10) throw std::invalid_argument("the collateral bond must mature after the horizon");
       for (std::size_t j = 0; j < nT; ++j) {
-        P.steps[j * kStepStride + 22] = bondA(grid.t[j], c.bondMaturity);
-        P.steps[j * kStepStride + 23] = bondB(grid.t[j], c.bondMaturity);
+        P.steps[j * stride + 22] = bondA(grid.t[j], c.bondMaturity);
+        P.steps[j * stride + 23] = bondB(grid.t[j], c.bondMaturity);
       }
     }
   }
@@ -975,7 +1037,7 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   P.header = {static_cast<std::uint32_t>(m.numPaths), static_cast<std::uint32_t>(nT), static_cast<std::uint32_t>(m.assets.size()),
               static_cast<std::uint32_t>(m.credits.size()), static_cast<std::uint32_t>(m.credits.empty() ? 1 : m.credits.front().substeps),
               static_cast<std::uint32_t>(numNormals), static_cast<std::uint32_t>(m.seed % 4294967296ull), m.antithetic ? 1u : 0u,
-              hasCsa ? 1u : 0u, static_cast<std::uint32_t>(o.counterparty), static_cast<std::uint32_t>(kStepStride / 4),
+              hasCsa ? 1u : 0u, static_cast<std::uint32_t>(o.counterparty), static_cast<std::uint32_t>(stride / 4),
               static_cast<std::uint32_t>(nCorr), static_cast<std::uint32_t>(offCall), static_cast<std::uint32_t>(offRep),
               floatBits(static_cast<float>(o.pfeQuantile)), static_cast<std::uint32_t>(numWG), static_cast<std::uint32_t>(P.statsPerDate),
               nR, static_cast<std::uint32_t>(perTradeGroups), L.valueChange, L.exposureValue, L.netted, L.collateral, L.gross,

@@ -51,12 +51,20 @@ struct Model {
   HullWhite hw;
   std::vector<Asset> assets;
   std::vector<Cir> credits;
-  std::vector<double> correlation;  // F x F, empty: identity
+  // Stochastic foreign short rates (an extension; the reference's foreign curves are deterministic): foreign[f] is
+  // the Hull-White model of asset f's currency, fitted to that asset's carry curve.
+  std::vector<HullWhite> foreign;
+  std::vector<double> correlation;  // F x F over [rate, assets, credits, foreign rates]; empty: identity
   std::size_t numPaths = 0;
   std::uint64_t seed = 42;
   bool antithetic = true;
   std::vector<double> base;
-  std::size_t numFactors() const { return 1 + assets.size() + credits.size(); }
+  std::size_t numFactors() const { return 1 + assets.size() + credits.size() + foreign.size(); }
+  // Columns of a step-table row: the reference's 24, then 8 per foreign rate.
+  std::size_t stepStride() const { return 24 + 8 * foreign.size(); }
+  double correlationOf(std::size_t i, std::size_t j) const {
+    return correlation.empty() ? (i == j ? 1.0 : 0.0) : correlation[i * numFactors() + j];
+  }
 };
 
 struct Swap {
@@ -132,7 +140,8 @@ struct CompiledPlan {
 
 CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o);
 
-// One row of the step table: the exact transitions of the rate state, its integral and the assets from t0 to t1.
+// One row of the step table (m.stepStride() values): the exact transitions of the rate state, its integral, the
+// assets and the foreign rates from t0 to t1.
 void stepRow(const Model& m, double t0, double t1, double* row);
 
 // The inner paths of the nested exposure from date t (src/nested/nested_exposure.cpp:87-117, 211-244): the event

@@ -101,11 +101,14 @@ __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z));
 // SiLU of two activations for inference, in packed bf16 arithmetic, from h = z / 2 (the caller folds the 1/2
 // into its bias add): sigmoid(z) = (1 + tanh(z / 2)) / 2, so silu(z) = h (1 + tanh h) = fma(h, tanh h, h).  One
 // tanh.approx.bf16x2 (a single special-function op for both) and one bf16x2 FMA; h0 lands in the low half (the
-// first of the two in memory).  Against silu rounded once to bf16 the result carries the rounding of h to bf16
-// and the approximate tanh, about one bf16 unit in the last place more.
+// first of the two in memory).  h is rounded to bf16 on the integer pipe -- half a bf16 unit added to the bit
+// pattern, the upper halves of both words kept by one byte permute: round half away from zero, which differs
+// from round-to-nearest-even only on exact ties -- so the special-function pipe only sees the tanh.  Against silu
+// rounded once to bf16 the result carries the rounding of h and the approximate tanh, about one bf16 unit in the
+// last place more.
 __device__ __forceinline__ uint32_t siluHalfBf16x2(float h0, float h1) {
   uint32_t p, t, s;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(p) : "f"(h1), "f"(h0));
+  asm("prmt.b32 %0, %1, %2, 0x7632;" : "=r"(p) : "r"(__float_as_uint(h0) + 0x8000u), "r"(__float_as_uint(h1) + 0x8000u));
   asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(p));
   asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(s) : "r"(p), "r"(t));
   return s;

@@ -33,6 +33,10 @@ constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 enum TermKind : uint32_t {
   kBond = 0, kFixedFloat = 1, kAsset = 2, kSetFixing = 3, kOption = 4,
   kBermExercise = 5, kBermDecide = 6, kBermContinue = 7, kBermBond = 8, kBermFloat = 9, kProbe = 10,
+  // Terms on an asset whose foreign short rate is stochastic (an extension of the reference's kinds; the asset is
+  // the code's extra field, rec[1] the foreign bond's B_f): a forward's c S P_f(t, T | x_f) and a Black option on
+  // the forward S P_f(t, T | x_f) / P(t, T | x).
+  kForeignForward = 11, kForeignOption = 12,
 };
 
 // Header words (fused_kernels.cpp:32-41).
@@ -50,6 +54,7 @@ enum DeviceError : uint32_t { kDevOk = 0, kDevTimeout = 1, kDevBadTerm = 2 };
 template <typename R>
 struct ScenarioArgs {
   uint32_t nP, nT, nA, nC, substeps, nNormals, nCorr, seed, antithetic, nStreams;
+  uint32_t nF, stepStride;  // stochastic foreign rates (of assets 0 .. nF - 1) and the step row length (24 + 8 nF)
   const R* steps;     // [nT][24]; columns 0..21 are shared by every plan of the batch
   const R* normals;   // injected normals [step][normal][stream], or nullptr (counter-based generator)
   R cir[8];           // (kappa, theta, xi, y0) per credit
@@ -66,6 +71,7 @@ struct CubeArgs {
   uint32_t nP, nT, nA, nC;
   uint32_t fS, fQ, fLnS, fY;
   uint32_t probes, pad;
+  uint32_t fXf, nF;  // the foreign short-rate states x_f of assets 0 .. nF - 1 (fields fXf + f)
 };
 
 // ---- one netting set (one plan) inside a launch ----
@@ -85,6 +91,8 @@ struct NsArgs {
   uint32_t rowEP, rowDV, rowE, rowV, rowC, rowGross, rowTrades, rowEx;
   uint32_t offCall, offRep, nSlots, ring;
   uint32_t usesAssets;     // some term reads an asset level
+  uint32_t usesForeign;    // some term reads a foreign short-rate state
+  uint32_t stepStride;     // values per row of `steps`
   uint32_t pad0;
   // AMC state pass (zk_amc_states, zk_fit_amc): x / deflator [date][path] and exercise values [row][path].
   R* sinkX;

@@ -12,7 +12,11 @@ Model block::
     nAssets, per asset (spot, vol, nCarry, (t, r) * nCarry),
     nCredits, per credit (kappa, theta, xi, y0, substeps, nHaz, (pillar, hazard) * nHaz),
     F, F * F correlation (row-major; F = 0 means identity),
-    numPaths, seed, antithetic, nBase, base grid times
+    numPaths, seed, antithetic, nBase, base grid times,
+    [7011, nForeign, (a, sigma) * nForeign]   only when assets carry a stochastic foreign rate (an extension)
+
+    The factors are ordered [domestic rate, assets, credits, foreign rates]; foreign rate f belongs to asset f,
+    so the assets with a stochastic foreign rate come first.
 
 Netting-set block::
 
@@ -41,6 +45,7 @@ from typing import List, Optional, Sequence, Union
 import numpy as np
 
 MODEL_MAGIC = 7001.0
+FOREIGN_MAGIC = 7011.0
 NETTING_MAGIC = 7002.0
 OPTIONS_MAGIC = 7003.0
 
@@ -60,11 +65,20 @@ class Curve:
 
 @dataclass
 class Asset:
-    """Lognormal FX / equity factor (include/ccr/models/lognormal_asset.hpp:17-41)."""
+    """Lognormal FX / equity factor (include/ccr/models/lognormal_asset.hpp:17-41).  The reference's foreign (carry)
+    curve is deterministic; with rate_a > 0 the foreign currency's short rate is a Hull-White factor of its own
+    (mean reversion rate_a, volatility rate_sigma) fitted to the carry curve: an extension with no counterpart in
+    the reference."""
 
     spot: float
     vol: float
     carry: Curve
+    rate_a: float = 0.0
+    rate_sigma: float = 0.0
+
+    @property
+    def stochastic_rate(self) -> bool:
+        return self.rate_a > 0.0
 
 
 @dataclass
@@ -95,8 +109,18 @@ class Model:
     base_grid: Sequence[float] = (0.0,)
 
     @property
+    def num_foreign(self) -> int:
+        """Assets with a stochastic foreign rate (they come first)."""
+        n = 0
+        while n < len(self.assets) and self.assets[n].stochastic_rate:
+            n += 1
+        if any(a.stochastic_rate for a in self.assets[n:]):
+            raise ValueError("the assets with a stochastic foreign rate must come first")
+        return n
+
+    @property
     def num_factors(self) -> int:
-        return 1 + len(self.assets) + len(self.credits)
+        return 1 + len(self.assets) + len(self.credits) + self.num_foreign
 
 
 @dataclass
@@ -228,6 +252,11 @@ def encode_model(m: Model) -> np.ndarray:
         out += [float(v) for v in corr.reshape(-1)]
     out += [float(m.num_paths), float(m.seed), 1.0 if m.antithetic else 0.0, float(len(m.base_grid))]
     out += [float(t) for t in m.base_grid]
+    nf = m.num_foreign
+    if nf:
+        out += [FOREIGN_MAGIC, float(nf)]
+        for a in m.assets[:nf]:
+            out += [float(a.rate_a), float(a.rate_sigma)]
     return np.asarray(out, dtype=np.float64)
 
 

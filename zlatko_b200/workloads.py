@@ -9,9 +9,9 @@ correlated_csa_book: 1,000 trades (600 swaps, 300 FX forwards, 100 FX options) i
     paths on 120 monthly dates to 10y, HW(a, sigma) with a ~ U[0.01, 0.1], sigma ~ U[0.005, 0.015],
     2 lognormal FX rates (vol U[8%, 15%]) and one CIR++ intensity (kappa 0.5, theta 0.02, xi 0.08)
     joined by a correlation with off-diagonals U[-0.3, 0.5] projected to the nearest positive
-    definite matrix.  The reference's model family simulates one Hull-White rate: the two foreign
-    curves are deterministic carry curves (flat, drawn U[0%, 4%]), which the configuration's
-    stochastic foreign rates extend.
+    definite matrix.  The two foreign currencies have Hull-White short rates of their own on flat
+    curves drawn U[0%, 4%] (the configuration's three currencies); with foreign_rates=False they
+    are the reference's deterministic carry curves instead.
 
 Cash-flow and maturity dates are whole months, so every event date falls on the monthly grid.
 Draws use numpy's PCG64 seeded with 20261203 (portfolio) and the simulation seed 42.
@@ -82,10 +82,14 @@ def swap_portfolio(paths: int = 10_000) -> Tuple[S.Model, S.NettingSet, S.Option
     return m, ns, S.Options(pfe_quantile=0.975)
 
 
-def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100,
-                        num_trades: int = 1000) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
+def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100, num_trades: int = 1000,
+                        foreign_rates: bool = True) -> Tuple[S.Model, List[S.NettingSet], S.Options, int]:
     """Returns (model, netting sets, options, number of trades).  num_trades keeps the 60/30/10 mix of swaps,
-    FX forwards and FX options."""
+    FX forwards and FX options.  With foreign_rates the two foreign currencies have Hull-White short rates of
+    their own (a ~ U[0.01, 0.1], sigma ~ U[0.005, 0.015]) on their carry curves, and the full 6 x 6
+    correlation joins domestic rate, foreign rates, FX and the intensity: the configuration's three-currency
+    model.  Without, the reference's model family: deterministic foreign curves, the 4 x 4 block of the
+    simulated factors.  The trades are the same either way."""
     rng = np.random.default_rng(PORTFOLIO_SEED + 1)
     a, sigma = rng.uniform(0.01, 0.1), rng.uniform(0.005, 0.015)
     fx = [S.Asset(spot, rng.uniform(0.08, 0.15), S.Curve.flat(rng.uniform(0.0, 0.04))) for spot in (1.1, 0.9)]
@@ -95,7 +99,9 @@ def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100,
     c6[iu] = rng.uniform(-0.3, 0.5, size=len(iu[0]))
     c6 = np.triu(c6) + np.triu(c6, 1).T
     c6 = nearest_correlation(c6)
-    keep = [0, 3, 4, 5]  # domestic rate, the two FX rates, the counterparty intensity
+    # c6 joins [domestic rate, foreign rate 1, foreign rate 2, FX 1, FX 2, intensity]; the model orders its
+    # factors [rate, assets, credits, foreign rates].
+    keep = [0, 3, 4, 5, 1, 2] if foreign_rates else [0, 3, 4, 5]
     corr = c6[np.ix_(keep, keep)]
     m = S.Model(curve=S.Curve.flat(0.02), hw_a=a, hw_sigma=sigma, assets=fx, credits=[credit], correlation=corr,
                 num_paths=paths, seed=SIM_SEED, antithetic=True, base_grid=[k / 12.0 for k in range(1, 121)])
@@ -120,6 +126,10 @@ def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100,
         t = rng.uniform(0.0, 5e6)
         books.append(S.NettingSet([trades[i] for i in order[at:at + n]], S.Csa(t, t, 1e5, 0.0, 10.0 / 250.0)))
         at += n
+    foreign = [(rng.uniform(0.01, 0.1), rng.uniform(0.005, 0.015)) for _ in fx]  # drawn last: the trades do not move
+    if foreign_rates:
+        for asset, (fa, fs) in zip(fx, foreign):
+            asset.rate_a, asset.rate_sigma = fa, fs
     return m, books, S.Options(pfe_quantile=0.975), len(trades)
 
 
