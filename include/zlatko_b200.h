@@ -87,6 +87,12 @@ int zk_abi_version(void);
  * context owns and joins it back with events, so work on `stream` stays ordered as usual (and a graph
  * captured from `stream` holds both branches). */
 zk_status zk_context_set_stream(zk_context* ctx, void* stream);
+/* Device memory a call or batch of this context may give to per-path rows and warp partials at once (bytes; 0, the
+ * default: all netting sets at once while that takes under 70% of the free device memory, else 60% of it).  A
+ * book whose rows exceed it runs its netting sets in waves that reuse one region: each wave's reduce and row
+ * statistics follow its revalue launch, and the outputs are the same bits as in one wave.  (The reference's
+ * kernels keep every netting set's rows, EXPO[rows][P], at once: fused_exposure.hpp:214-216.) */
+zk_status zk_context_set_row_budget(zk_context* ctx, uint64_t bytes);
 
 /* ---- the drop-in backend ------------------------------------------------------------------------ */
 /* Replaces gpu::runFusedReference(plan) (src/gpu/fused_reference.cpp:628-630): the fused-exposure,
@@ -221,6 +227,7 @@ typedef struct zk_batch_info {
   uint64_t kernels_per_execute;  /* kernel launches of one zk_batch_execute                         */
   uint64_t tile_paths;           /* paths per revalue CTA, chosen by the autotuner at creation     */
   uint64_t graph_replay;         /* 1 once executes replay a captured CUDA graph, 0 while eager    */
+  uint64_t num_waves;            /* waves of netting sets within the row budget (1 per launch group without) */
 } zk_batch_info;
 
 /* Uploads the plans.  The first zk_batch_execute autotunes the tile shape (paths per revalue CTA) on
@@ -233,7 +240,7 @@ zk_status zk_batch_execute(zk_batch* b);
 zk_status zk_batch_set_tile_paths(zk_batch* b, uint64_t tile_paths);
 /* Milliseconds of the last execute by kernel: [0] risk-factor simulation, [1] revalue / net /
  * collateralise / reduce per tile, [2] reduce of the partials, [3] row statistics, measured with CUDA
- * events on the context stream. */
+ * events on the context stream.  A batch that runs in waves counts its waves' reduce and row statistics in [1]. */
 zk_status zk_batch_timings(const zk_batch* b, float* ms4);
 zk_status zk_batch_read(zk_batch* b, zk_output* outs);
 zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info);

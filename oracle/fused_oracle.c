@@ -454,6 +454,10 @@ static int read_plan(Plan* v, const uint32_t* header, const uint32_t* indices, c
     if (err && errLen) snprintf(err, errLen, "empty plan");
     return 1;
   }
+  if (v->nBerm > MAX_BERM) { /* the reference's kernel prices at most 4 Bermudans per netting set */
+    if (err && errLen) snprintf(err, errLen, "the restated kernels run the reference's plans (at most 4 Bermudans)");
+    return 1;
+  }
   if (header[10] != STEP / 4) { /* the reference's plans only: no stochastic foreign rates */
     if (err && errLen) snprintf(err, errLen, "the restated kernels run the reference's plans (24-value step rows)");
     return 1;

@@ -178,7 +178,10 @@ def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarra
     sizes = (C.c_size_t * 2)()
     prof = np.zeros(6 * cap)
     mats = [np.zeros(num_paths * cap) for _ in range(4)]
-    exercise = np.full(4 * num_paths, -1.0)
+    from zlatko_b200.spec import bermudan_degrees
+
+    nb = max(4, len(bermudan_degrees(ns)))
+    exercise = np.full(nb * num_paths, -1.0)
     e = _err()
     z = np.ascontiguousarray(normals, np.float64)
     m, n = np.ascontiguousarray(model, np.float64), np.ascontiguousarray(ns, np.float64)
@@ -195,7 +198,7 @@ def engine_run(model: np.ndarray, ns: np.ndarray, pfe: float, normals: np.ndarra
     pcva = lib().orc_pathwise_cva(expo, np.ascontiguousarray(defl), np.ascontiguousarray(surv), num_paths, nT, reporting,
                                   nR, 0.4)
     return EngineResult(times[:nT].copy(), reporting.astype(np.int64), p, netted, coll, defl, surv, pcva,
-                        exercise.reshape(4, num_paths))
+                        exercise.reshape(nb, num_paths))
 
 
 def quantile(values, p: float) -> float:

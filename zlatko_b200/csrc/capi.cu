@@ -124,6 +124,9 @@ struct zk_context {
   // quantile's narrowing rounds.
   uint64_t failAtLaunch = 0, launchCount = 0;
   uint32_t rowRounds = 16;
+  // Device bytes a batch may give to per-path rows and warp partials at once (zk_context_set_row_budget); 0: all
+  // of its netting sets at once while that takes under 70% of the free device memory, else waves in 60% of it.
+  uint64_t rowBudget = 0;
 };
 
 namespace {
@@ -233,7 +236,8 @@ struct Plan {
   std::vector<uint32_t> dates;  // [nT][8]: floatBegin, bondBegin, assetBegin, genericBegin, fixingBegin, end, callIndex, reportingSlot
   std::vector<R> table;         // records of 4 values
   uint32_t exerciseRows = 0;
-  uint32_t bermRows[kMaxBermudans] = {0, 0, 0, 0};
+  std::vector<uint32_t> bermRows;  // exercise dates of each Bermudan
+  bool manyBerm = false;           // more than 4 Bermudans: exercise state in shared memory (one byte per path)
   uint64_t termEvals = 0, expEvals = 0;
 };
 
@@ -311,7 +315,12 @@ Plan<R> parse(const View<R>& v, size_t index) {
   rowBlock(p.rowC, p.nR, "collateral rows beyond rows_total");
   rowBlock(p.rowGross, p.nR, "gross rows beyond rows_total");
   rowBlock(p.rowTrades, static_cast<uint64_t>(std::min<uint32_t>(p.nTr, kMaxTradeGroups)) * p.nR, "trade rows beyond rows_total");
-  rowBlock(p.rowEx, std::min<uint32_t>(p.nBerm, kMaxBermudans), "exercise rows beyond rows_total");
+  if (p.nBerm > static_cast<uint32_t>(kMaxBermudansPerPlan)) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: more than 256 Bermudans", index);
+  p.manyBerm = p.nBerm > static_cast<uint32_t>(kMaxBermudans);
+  if (p.manyBerm && p.nInner > 0) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the nested initial margin of more than 4 Bermudans", index);
+  if (p.manyBerm && p.nTr > 0 && p.nBerm > 16) throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: per-trade views of more than 16 Bermudans", index);
+  p.bermRows.assign(p.nBerm, 0u);
+  rowBlock(p.rowEx, p.nBerm, "exercise rows beyond rows_total");
   if (p.nInner > 0) rowBlock(p.rowIm, p.nR, "initial-margin rows beyond rows_total");
   if (p.rowEP == kNoRow) throw bad("the exposure rows are required");
   for (size_t t = 0; t < p.nTerms; ++t) {
@@ -344,12 +353,16 @@ Plan<R> parse(const View<R>& v, size_t index) {
     if (kind == kProbe) {
       if (!(rec[5] >= R(0)) || static_cast<double>(rec[5]) >= static_cast<double>(rows)) throw bad("probe row beyond rows_total");
     }
-    if (kind == kBermDecide) {
-      const uint32_t bm = std::min((code >> 8u) & 15u, 3u), extra = code >> 12u;
-      p.bermRows[bm] = std::max(p.bermRows[bm], extra + 1);
+    if (kind >= kBermExercise && kind <= kBermFloat) {
+      const uint32_t bm = bermudanOf(code, p.manyBerm), extra = code >> 12u;
+      if (bm >= p.nBerm) throw bad("an AMC term of a Bermudan beyond the plan's count");
+      if (kind == kBermDecide) {
+        if (extra >= 64u) throw bad("exercise index beyond 64");
+        p.bermRows[bm] = std::max(p.bermRows[bm], extra + 1);
+      }
     }
   }
-  for (uint32_t b = 0; b < kMaxBermudans; ++b) p.exerciseRows += p.bermRows[b];
+  for (uint32_t b = 0; b < p.nBerm; ++b) p.exerciseRows += p.bermRows[b];
   for (uint32_t j = 0; j < p.nT; ++j) {
     for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
       const uint32_t kind = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]) & 15u;
@@ -375,7 +388,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
   if (p.hasCsa && p.ring > static_cast<uint32_t>(kMaxRing))
     throw fail(ZK_ERR_UNSUPPORTED, "plan %zu: the margin-call look-back spans %u dates (at most %d)", index, maxLag, kMaxRing - 1);
   if (p.ctype == 2) p.usesAssets = true;
-  p.stateWords = p.nSlots + (p.hasCsa ? p.ring * (p.ctype != 0 ? 2 : 1) : 0);
+  p.stateWords = p.nSlots + (p.hasCsa ? p.ring * (p.ctype != 0 ? 2 : 1) : 0) + (p.manyBerm ? (p.nBerm + 3) / 4 : 0);
   p.im = p.nInner > 0 && p.rowIm != kNoRow;
   if (p.im) {
     // The full revalue variant records the outer state on the reporting dates; the inner paths start from it
@@ -498,6 +511,13 @@ struct Batch {
     bool cashBig = true, cashSmall = true, cashAll = true;
     bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
+    // Memory-bounded batches: the launch's netting sets [first, first + count) of planIdx run as one wave whose
+    // rows and partials reuse the same device region as every other wave; its reduce and row-statistics jobs are
+    // [reduceFirst, + count) and [rowFirst, + rowCount) of the job arrays.
+    struct Wave {
+      size_t first = 0, count = 0, reduceFirst = 0, rowFirst = 0, rowCount = 0;
+    };
+    std::vector<Wave> waves;
   };
   std::vector<Launch> launches;
   // device offsets per plan
@@ -510,6 +530,8 @@ struct Batch {
   size_t inputBytes = 0, totalBytes = 0, outBegin = 0, outBytes = 0;
   uint32_t numRowJobs = 0, maxReduceN = 0;
   int ppt = 2;                        // paths per revalue thread: the tile shape (autotuned by zk_batch_create)
+  bool waved = false;                 // the netting sets run in waves (Launch::waves) within a row budget
+  std::vector<uint32_t> jobOrder;     // plans in the order of the reduce and row-statistics job arrays
   std::vector<ReduceJob<R>> reduceJobs;  // host copy; numTiles follows ppt
   std::vector<ImArgs<R>> im;             // nested initial margin launches, after the revalue launches
   std::vector<unsigned char> image;  // host image of the input region
@@ -654,7 +676,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   if (sink) {
     const auto& P = B->plans[0];
     B->exerciseRows = P.exerciseRows;
-    B->bermRowOff = take(kMaxBermudans * 4);
+    B->bermRowOff = take(std::max<uint32_t>(P.nBerm, 1) * 4);
   }
   if (normals) {
     const auto& P = B->plans[0];
@@ -663,12 +685,61 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   B->inputBytes = off;
   for (auto& L : B->launches)
     L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
-  for (size_t i = 0; i < nPlans; ++i) {
-    const auto& P = B->plans[i];
+  // Rows and warp partials: one region per plan, or -- when they exceed the row budget -- waves of netting sets
+  // (in each launch's order) that reuse one region, sized by the largest wave.
+  auto rowsBytes = [&](const Plan<R>& P) {
     const uint32_t warps = (P.nP + 31) / 32;  // the most revalue warps any tile shape uses: one partial each
-    B->dev[i].expo = take(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
-    B->dev[i].partials = take(static_cast<size_t>(warps) * P.nT * P.nS * sizeof(R));
-    if (P.im && !sink) B->dev[i].imState = take(static_cast<size_t>(P.nR) * (5 + P.nSlots) * P.nP * sizeof(R));
+    return alignUp(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R)) +
+           alignUp(static_cast<size_t>(warps) * P.nT * P.nS * sizeof(R));
+  };
+  size_t allRows = 0;
+  bool anyIm = false;
+  for (const auto& P : B->plans) allRows += rowsBytes(P), anyIm = anyIm || P.im;
+  uint64_t budget = ctx ? ctx->rowBudget : 0;
+  if (ctx && budget == 0) {
+    size_t freeB = 0, totalB = 0;
+    if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess && allRows > freeB / 10 * 7) budget = freeB / 10 * 6;
+    else cudaGetLastError();
+  }
+  B->waved = budget > 0 && allRows > budget && !sink && !anyIm && !normals;
+  auto placeRows = [&](size_t i, auto&& takeFn) {
+    const auto& P = B->plans[i];
+    const uint32_t warps = (P.nP + 31) / 32;
+    B->dev[i].expo = takeFn(static_cast<size_t>(std::max<uint32_t>(P.v.rows_total, 1)) * P.nP * sizeof(R));
+    B->dev[i].partials = takeFn(static_cast<size_t>(warps) * P.nT * P.nS * sizeof(R));
+  };
+  if (!B->waved) {
+    for (size_t i = 0; i < nPlans; ++i) {
+      const auto& P = B->plans[i];
+      placeRows(i, take);
+      if (P.im && !sink) B->dev[i].imState = take(static_cast<size_t>(P.nR) * (5 + P.nSlots) * P.nP * sizeof(R));
+    }
+    B->jobOrder.resize(nPlans);
+    for (size_t i = 0; i < nPlans; ++i) B->jobOrder[i] = static_cast<uint32_t>(i);
+  } else {
+    const size_t region = off;
+    size_t regionBytes = 0, jobs = 0, rowJobs = 0;
+    for (auto& L : B->launches) {
+      size_t k = 0;
+      while (k < L.planIdx.size()) {
+        typename Batch<R>::Launch::Wave w;
+        w.first = k, w.reduceFirst = jobs, w.rowFirst = rowJobs;
+        size_t used = 0;
+        while (k < L.planIdx.size() && (k == w.first || used + rowsBytes(B->plans[L.planIdx[k]]) <= budget)) {
+          const uint32_t i = L.planIdx[k];
+          size_t at = region + used;
+          placeRows(i, [&](size_t bytes) { const size_t o = at; at = alignUp(at + std::max<size_t>(bytes, 16)); return o; });
+          used += rowsBytes(B->plans[i]);
+          B->jobOrder.push_back(i);
+          w.rowCount += B->plans[i].nReq, ++jobs, ++k;
+        }
+        w.count = k - w.first;
+        rowJobs += w.rowCount;
+        regionBytes = std::max(regionBytes, used);
+        L.waves.push_back(w);
+      }
+    }
+    off = alignUp(region + regionBytes);
   }
   if (sink) {
     const auto& P = B->plans[0];
@@ -750,6 +821,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
       A.usesAssets = P.usesAssets ? 1u : 0u;
       A.usesForeign = P.usesForeign ? 1u : 0u;
       A.stepStride = P.stepStride;
+      A.manyBerm = P.manyBerm ? 1u : 0u;
       if (P.im && !B.sink) {
         A.imState = static_cast<R*>(dptr(D.imState));
         A.imWords = 5 + P.nSlots;
@@ -781,10 +853,11 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
   std::vector<RowJob<R>> rows;
   rows.reserve(B.numRowJobs);
   B.maxReduceN = 0;
-  for (size_t i = 0; i < B.plans.size(); ++i) {
+  for (size_t o = 0; o < B.plans.size(); ++o) {
+    const size_t i = B.jobOrder[o];  // plan order, or wave by wave when the batch runs in waves
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    red[i] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP, 0};
+    red[o] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP, 0};
     B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
     for (size_t q = 0; q < P.nReq; ++q)
       rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),
@@ -794,9 +867,10 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
   B.reduceJobs = red;
   if (!rows.empty()) std::memcpy(img + B.rowOff, rows.data(), rows.size() * sizeof(RowJob<R>));
   if (B.sink) {
-    uint32_t offs[kMaxBermudans], acc = 0;
-    for (int b = 0; b < kMaxBermudans; ++b) offs[b] = acc, acc += B.plans[0].bermRows[b];
-    std::memcpy(img + B.bermRowOff, offs, sizeof offs);
+    std::vector<uint32_t> offs(std::max<uint32_t>(B.plans[0].nBerm, 1), 0u);
+    uint32_t acc = 0;
+    for (uint32_t b = 0; b < B.plans[0].nBerm; ++b) offs[b] = acc, acc += B.plans[0].bermRows[b];
+    std::memcpy(img + B.bermRowOff, offs.data(), offs.size() * 4);
   }
   if (normals) {
     const auto& P = B.plans[0];
@@ -860,19 +934,22 @@ void injectPoint(zk_context* ctx) {
 // shared memory of the largest allows.  The few large-state netting sets fill less than a wave of long CTAs:
 // with a side stream (and its fork / join events) they run there while the small-state launch fills the rest
 // of the GPU; without one, before it on s.  Either way the kernels and their output bits are the same.
+// first / count select a wave of the launch's netting sets (all of them by default).
 template <typename R>
 void launchRevalues(const Batch<R>& B, const typename Batch<R>::Launch& L, uintptr_t base, cudaStream_t s, cudaStream_t side,
-                    cudaEvent_t forkEv, cudaEvent_t joinEv) {
-  const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff);
-  const uint32_t n = static_cast<uint32_t>(L.planIdx.size()), tiles = numTilesOf(L.sc.nP, B.ppt);
-  const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < n;
+                    cudaEvent_t forkEv, cudaEvent_t joinEv, size_t first = 0, size_t count = SIZE_MAX) {
+  count = std::min(count, L.planIdx.size() - first);
+  const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff) + first;
+  const uint32_t n = static_cast<uint32_t>(count), tiles = numTilesOf(L.sc.nP, B.ppt);
+  const size_t splitAt = std::min(count, L.splitAt > first ? L.splitAt - first : 0);
+  const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && splitAt < n;
   if (!split) {
     injectPoint(B.ctx);
     ZK_CUDA(launchRevalue<R>(L.cb, ns, n, tiles, L.stateWordsMax, L.perTrade, B.sink, L.lean, B.ppt, s, false,
                              L.lean && !L.perTrade && !B.sink && L.cashAll));
     return;
   }
-  const uint32_t big = static_cast<uint32_t>(L.splitAt);
+  const uint32_t big = static_cast<uint32_t>(splitAt);
   const bool fork = big > 0 && side;
   if (big > 0) injectPoint(B.ctx);
   if (fork) {
@@ -915,14 +992,29 @@ void execute(Batch<R>& B, bool capturing = false) {
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
     }
-    launchRevalues(B, L, base, s, ctx->side, ctx->fork, ctx->join);
+    if (!B.waved) {
+      launchRevalues(B, L, base, s, ctx->side, ctx->fork, ctx->join);
+      continue;
+    }
+    // Waves: a wave's rows and partials are reduced and read before the next wave overwrites them.  Its timings
+    // count as revalue time ([1]); reduce and row statistics ([2], [3]) stay zero.
+    for (const auto& w : L.waves) {
+      injectPoint(ctx);
+      launchRevalues(B, L, base, s, ctx->side, ctx->fork, ctx->join, w.first, w.count);
+      ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff) + w.reduceFirst, static_cast<uint32_t>(w.count),
+                              B.maxReduceN, B.ppt, s));
+      ZK_CUDA(launchRowStats<R>(reinterpret_cast<const RowJob<R>*>(base + B.rowOff) + w.rowFirst, static_cast<uint32_t>(w.rowCount),
+                                ctx->dErr, s, ctx->rowRounds));
+    }
   }
   for (const auto& M : B.im) {
     injectPoint(ctx);
     ZK_CUDA(launchNestedIm<R>(M, s));
   }
   ZK_CUDA(recordEvent(B.ev[2], s, capturing));
-  if (!B.sink) {
+  if (B.waved) {
+    ZK_CUDA(recordEvent(B.ev[3], s, capturing));
+  } else if (!B.sink) {
     injectPoint(ctx);
     ZK_CUDA(launchReduce<R>(reinterpret_cast<const ReduceJob<R>*>(base + B.reduceOff), static_cast<uint32_t>(B.plans.size()), B.maxReduceN,
                             B.ppt, s));
@@ -1077,7 +1169,7 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     for (uint32_t j = 0; j < P.nT; ++j)
       for (uint32_t t = v.indices[j]; t < v.indices[j + 1]; ++t) {
         const auto code = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]);
-        const uint32_t kind = code & 15u, b = (code >> 8u) & 15u, e = code >> 12u;
+        const uint32_t kind = code & 15u, b = bermudanOf(code, P.manyBerm), e = code >> 12u;
         if (kind != 6u && kind != 7u) continue;
         if (b >= numBermudans) throw fail(ZK_ERR_INVALID_PLAN, "an AMC term of Bermudan %u", b);
         if (kind == 6u) {
@@ -1258,6 +1350,12 @@ zk_status zk_context_set_stream(zk_context* ctx, void* stream) {
     ctx->stream = static_cast<cudaStream_t>(stream);
     ctx->ownStream = false;
   }
+  return ZK_OK;
+}
+
+zk_status zk_context_set_row_budget(zk_context* ctx, uint64_t bytes) {
+  if (!ctx) return ZK_ERR_INVALID_ARGUMENT;
+  ctx->rowBudget = bytes;
   return ZK_OK;
 }
 
@@ -1741,12 +1839,23 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
     info->table_bytes += P.nIdx * 4 + P.nTerms * 32 + static_cast<uint64_t>(P.nT) * 96 + P.nReq * 32;
     info->row_bytes += static_cast<uint64_t>(P.nR) * P.nP * 4;
   }
-  uint64_t kernels = 2 + B.im.size();  // reduce, row statistics, one nested-margin launch per margin plan
+  uint64_t kernels = (B.waved ? 0 : 2) + B.im.size();  // reduce, row statistics, one nested-margin launch per margin plan
   for (const auto& L : B.launches) {
     const bool split = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && L.splitAt < L.planIdx.size();
-    kernels += 1 + (split && L.splitAt > 0 ? 2 : 1);  // simulate, then one or two revalue launches
+    if (!B.waved) {
+      kernels += 1 + (split && L.splitAt > 0 ? 2 : 1);  // simulate, then one or two revalue launches
+      continue;
+    }
+    kernels += 1;  // simulate; per wave one or two revalue launches, a reduce and (with requests) row statistics
+    for (const auto& w : L.waves) {  // as launchRevalues splits a wave
+      const size_t at = std::min(w.count, L.splitAt > w.first ? L.splitAt - w.first : 0);
+      const bool splitW = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && at < w.count;
+      kernels += (splitW && at > 0 ? 2 : 1) + 1 + (w.rowCount ? 1 : 0);
+    }
   }
   info->kernels_per_execute = kernels;
+  info->num_waves = 0;
+  for (const auto& L : B.launches) info->num_waves += B.waved ? L.waves.size() : 1;
   info->tile_paths = static_cast<uint64_t>(kTile) * B.ppt;
   info->graph_replay = b->graph && !b->eager && b->graphPpt == B.ppt ? 1u : 0u;
   return ZK_OK;

@@ -372,6 +372,15 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   }
   auto fix = [&](uint32_t slot, int i) -> R& { return state[(slot * PPT + i) * kTile + tid]; };
   auto ring = [&](uint32_t r, int i) -> R& { return state[((nSlots + r) * PPT + i) * kTile + tid]; };
+  // More than 4 Bermudans (non-lean launches only): each path's exercise index of Bermudan b is a byte of shared
+  // memory after the fixings and the margin ring, [b][PPT][kTile], -1 while not exercised.
+  const bool manyBerm = !kLean && A.manyBerm != 0;
+  signed char* exS = reinterpret_cast<signed char*>(
+      state + static_cast<size_t>(nSlots + (hasCsa ? ringLen * (ctype != 0 ? 2u : 1u) : 0u)) * PPT * kTile);
+  if (manyBerm)
+    for (uint32_t b = 0; b < A.nBerm; ++b)
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) exS[(b * PPT + i) * kTile + tid] = -1;
   auto vt = [&](uint32_t g, int i) -> R& { return vtBuf[(g * PPT + i) * kTile + tid]; };
   for (uint32_t s = 0; s < nSlots; ++s)
 #pragma unroll
@@ -386,6 +395,10 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   auto cube = [&](uint32_t field, uint32_t j, int i) { return cubeP[i][field * fieldStride + static_cast<size_t>(j) * nP]; };
 
   R held[PPT], prevDE[PPT], prevQ[PPT], prevRV[PPT], ex[4][PPT];
+  // The exercise index (-1: not exercised) of Bermudan b on the thread's path i.
+  auto exOf = [&](uint32_t b, int i) -> R {
+    return manyBerm ? static_cast<R>(exS[(b * PPT + i) * kTile + tid]) : pick4<R, PPT>(ex, b, i);
+  };
   // Look-back of at most one date (the margin-call dates t - MPR sit on the grid): the previous date's value
   // and collateral price in registers instead of the shared-memory ring.
   const bool shortLook = kCash || ringLen <= 2;
@@ -503,7 +516,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
       R rec[8];
       loadTerm(table + 4 * u, rec);
       const uint32_t code = static_cast<uint32_t>(rec[0]);
-      const uint32_t kind = code & 15u, bm = min((code >> 8u) & 15u, 3u), extra = code >> 12u;
+      const uint32_t kind = code & 15u, bm = bermudanOf(code, manyBerm), extra = code >> 12u;
       const uint32_t slot = static_cast<uint32_t>(rec[1]);
       const uint32_t grp = min((code >> 4u) & 15u, 15u);
       const R c = rec[2], nB = -rec[4];
@@ -559,7 +572,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {
               const R v = c * (rec[3] * fastExp(nB * x[i]));
-              if (bm == 0) ev[0][i] += v;
+              if (manyBerm || bm == 0) ev[0][i] += v;  // with many Bermudans, one running value: its policy follows
               else if (bm == 1) ev[1][i] += v;
               else if (bm == 2) ev[2][i] += v;
               else ev[3][i] += v;
@@ -568,12 +581,14 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
           case kBermDecide:
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {
-              const R e = pick4<R, PPT>(ev, bm, i);
+              const R e = manyBerm ? ev[0][i] : pick4<R, PPT>(ev, bm, i);
+              if (manyBerm) ev[0][i] = R(0);
               if (kSink) {
                 if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
-              } else if (pick4<R, PPT>(ex, bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
+              } else if (exOf(bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
                 const R v = static_cast<R>(extra);
-                if (bm == 0) ex[0][i] = v;
+                if (manyBerm) exS[(bm * PPT + i) * kTile + tid] = static_cast<signed char>(extra);
+                else if (bm == 0) ex[0][i] = v;
                 else if (bm == 1) ex[1][i] = v;
                 else if (bm == 2) ex[2][i] = v;
                 else ex[3][i] = v;
@@ -583,12 +598,12 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
           case kBermContinue:
   #pragma unroll
             for (int i = 0; i < PPT; ++i)
-              if (pick4<R, PPT>(ex, bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
+              if (exOf(bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
             break;
           case kBermBond:
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {
-              const R e = pick4<R, PPT>(ex, bm, i);
+              const R e = exOf(bm, i);
               if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = c * (rec[3] * fastExp(nB * x[i]));
             }
             break;
@@ -614,7 +629,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
           default:  // kBermFloat
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {
-              const R e = pick4<R, PPT>(ex, bm, i);
+              const R e = exOf(bm, i);
               if (e >= R(0) && e <= static_cast<R>(extra)) term[i] = (c * fix(slot, i) + rec[5]) * (rec[3] * fastExp(nB * x[i]));
             }
           }
@@ -700,8 +715,8 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
         for (uint32_t q = 0; q < nSlots; ++q) st[static_cast<size_t>(5 + q) * nP] = fix(q, i);
       }
       if (!kLean && act[i] && A.rowEx != kNoRow)
-        for (uint32_t b = 0; b < min(A.nBerm, 4u); ++b) {
-          const R v = pick4<R, PPT>(ex, b, i);
+        for (uint32_t b = 0; b < (manyBerm ? A.nBerm : min(A.nBerm, 4u)); ++b) {
+          const R v = exOf(b, i);
           expo[(A.rowEx + b) * static_cast<size_t>(nP) + pth[i]] = v < R(0) ? R(-1) : v;
         }
     }

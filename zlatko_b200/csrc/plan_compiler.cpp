@@ -22,7 +22,12 @@ namespace zk::host {
 
 namespace {
 constexpr std::size_t kMaxAssets = 4, kMaxCredits = 2, kMaxSlots = 32, kMaxNormals = 64, kMaxTradeGroups = 16;
-constexpr std::size_t kMaxBermudans = 4, kMaxExercises = 64, kMaxAmcDegree = 3, kStepStride = 24, kTermStride = 8;
+// Bermudans: the reference's kernel prices at most 4 per netting set (fused_exposure.hpp:127); this compiler takes up
+// to 256.  Plans with at most 4 keep the reference's tables; above 4 a Bermudan's index carries its high bits in the
+// trade-group field of the term code (unused outside per-trade mode) and each Bermudan's exercise terms come
+// directly before its own policy record, so the kernel needs one running exercise value per path.
+constexpr std::size_t kMaxBermudans = 256, kRegisterBermudans = 4, kMaxExercises = 64, kMaxAmcDegree = 3, kStepStride = 24,
+                      kTermStride = 8;
 constexpr std::size_t kMaxInnerPaths = 1024, kInnerTop = 16;  // nested initial margin (fused_exposure.hpp:57-58)
 constexpr std::size_t kParamCount = 84, kMaxSamples = 64, kPfeBins = 3072, kStatsPerDate = 8, kTradeStats = 5;
 constexpr std::uint32_t kNoRow = 0xFFFFFFFFu;
@@ -325,7 +330,7 @@ bool sameBond(const Term& a, const Term& b) { return a.A == b.A && a.B == b.B; }
 // Merges the terms of one date in double precision (the rules of mergeTerms, fused_exposure.cpp:45-100):
 // bonds of one (A, B) summed; a running coupon with the bond of its payment date folded into p1;
 // forwards on one asset summed; options, AMC terms and fixings kept, fixings last.
-std::vector<Term> merge(const std::vector<Term>& in) {
+std::vector<Term> merge(const std::vector<Term>& in, bool manyBermudans = false) {
   std::vector<Term> floating, bonds, assets, options, fixings, exercise, amc, foreignFwd;
   for (const Term& r : in) {
     switch (r.kind) {
@@ -386,8 +391,22 @@ std::vector<Term> merge(const std::vector<Term>& in) {
   for (const Term& a : foreignFwd)
     if (a.c != 0.0) out.push_back(a);
   out.insert(out.end(), options.begin(), options.end());
-  out.insert(out.end(), exercise.begin(), exercise.end());
-  out.insert(out.end(), amc.begin(), amc.end());
+  if (!manyBermudans) {
+    out.insert(out.end(), exercise.begin(), exercise.end());
+    out.insert(out.end(), amc.begin(), amc.end());
+  } else {  // Bermudan by Bermudan: its exercise terms, then its policy, continuation and exercised-tail records
+    std::vector<std::size_t> ids;
+    for (const Term& r : exercise) ids.push_back(r.bermudan);
+    for (const Term& r : amc) ids.push_back(r.bermudan);
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    for (std::size_t b : ids) {
+      for (const Term& r : exercise)
+        if (r.bermudan == b) out.push_back(r);
+      for (const Term& r : amc)
+        if (r.bermudan == b) out.push_back(r);
+    }
+  }
   out.insert(out.end(), fixings.begin(), fixings.end());
   return out;
 }
@@ -710,7 +729,7 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
         }
       }
     } else {
-      if (bermudans >= kMaxBermudans) throw std::invalid_argument("the GPU kernel prices at most 4 Bermudan swaptions");
+      if (bermudans >= kMaxBermudans) throw std::invalid_argument("the GPU kernel prices at most 256 Bermudan swaptions per netting set");
       if (tr.exercise.size() > kMaxExercises) throw std::invalid_argument("too many exercise dates for the GPU kernel");
       if (tr.degree > kMaxAmcDegree) throw std::invalid_argument("AMC regression degree above 3 on the GPU");
       const std::size_t b = bermudans++;
@@ -775,6 +794,9 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
     }
   }
   P.numBermudans = amc.size();
+  const bool manyBermudans = amc.size() > kRegisterBermudans;
+  if (amc.size() > 16 && perTradeGroups > 0) throw std::invalid_argument("per-trade views of more than 16 Bermudans");
+  if (manyBermudans && o.imInnerPaths > 0) throw std::invalid_argument("the nested initial margin of more than 4 Bermudans");
 
   // ---- swap slots.  Up to 32 swaps keep one slot each (the reference's numbering, identical tables).
   // Beyond that a slot is keyed by the floating period (ts, te) instead of the swap: the fixing of a
@@ -962,9 +984,12 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
   for (std::size_t j = 0; j < nT; ++j) {
     P.indices[j] = static_cast<std::uint32_t>(P.terms.size() / kTermStride);
     auto emit = [&](const std::vector<Term>& recs, std::size_t group) {
-      for (const Term& r : merge(recs)) {
-        const double bermudan = r.merged ? 0.0 : static_cast<double>(r.bermudan), extra = r.merged ? 0.0 : static_cast<double>(r.extra);
-        P.terms.push_back(static_cast<double>(r.kind) + 16.0 * static_cast<double>(group) + 256.0 * bermudan + 4096.0 * extra);
+      for (const Term& r : merge(recs, manyBermudans)) {
+        const std::size_t b = r.merged ? 0 : r.bermudan;
+        const double extra = r.merged ? 0.0 : static_cast<double>(r.extra);
+        // Bermudan b: low 4 bits in the reference's field, high bits in the trade-group field (never per-trade here).
+        P.terms.push_back(static_cast<double>(r.kind) + 16.0 * static_cast<double>(group + (b >> 4)) +
+                          256.0 * static_cast<double>(b & 15) + 4096.0 * extra);
         for (double v : {r.slot, r.c, r.A, r.B, r.p1, r.p2, r.p3}) P.terms.push_back(v);
       }
     };

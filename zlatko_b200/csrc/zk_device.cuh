@@ -23,7 +23,8 @@ constexpr int kMaxAssets = 4;
 constexpr int kMaxCredits = 2;
 constexpr int kMaxSwapSlots = 32;
 constexpr int kMaxNormals = 64;
-constexpr int kMaxBermudans = 4;
+constexpr int kMaxBermudans = 4;          // Bermudans of a plan in the reference's layout (exercise state in registers)
+constexpr int kMaxBermudansPerPlan = 256;  // beyond 4: exercise state in shared memory, the index's high bits in the code
 constexpr int kMaxTradeGroups = 16;
 constexpr int kMaxRing = 32;           // look-back depth (dates) of the CSA margin call kept on chip
 constexpr int kMaxInnerPaths = 1024;    // inner paths of the nested initial margin per outer path and date
@@ -92,6 +93,7 @@ struct NsArgs {
   uint32_t offCall, offRep, nSlots, ring;
   uint32_t usesAssets;     // some term reads an asset level
   uint32_t usesForeign;    // some term reads a foreign short-rate state
+  uint32_t manyBerm;       // more than 4 Bermudans: exercise indices in shared memory, bytes [nBerm][PPT][kTile]
   uint32_t stepStride;     // values per row of `steps`
   uint32_t pad0;
   // AMC state pass (zk_amc_states, zk_fit_amc): x / deflator [date][path] and exercise values [row][path].
@@ -207,6 +209,12 @@ template <typename R>
 __device__ __forceinline__ R amcPoly(const R* rec, R x) {
   const R z = (x - rec[2]) * rec[3];
   return ((rec[7] * z + rec[6]) * z + rec[5]) * z + rec[4];
+}
+
+// The Bermudan of an AMC term's code: bits 8-11, and with more than 4 Bermudans in the plan bits 4-7 above them
+// (the trade-group field, which such plans leave to the Bermudan index).
+__host__ __device__ __forceinline__ uint32_t bermudanOf(uint32_t code, bool many) {
+  return many ? (((code >> 8u) & 15u) | (((code >> 4u) & 15u) << 4u)) : ((code >> 8u) & 15u) < 3u ? ((code >> 8u) & 15u) : 3u;
 }
 
 // Order-preserving float <-> uint32 keys (for min / max / radix selection of signed values).

@@ -289,6 +289,11 @@ class Context:
         sums, values = bufs[0]
         return sums, values, r[: plan.rows_total * plan.num_paths].reshape(plan.rows_total, plan.num_paths)
 
+    def set_row_budget(self, nbytes: int) -> None:
+        """zk_context_set_row_budget: device bytes for per-path rows and partials at once (0: automatic); books
+        beyond it run in waves of netting sets with the same results."""
+        check(lib().zk_context_set_row_budget(self.handle, int(nbytes)), self.handle)
+
     INJECT_FAIL_LAUNCH, INJECT_ROW_ROUNDS = 1, 2
 
     def inject(self, what: int, value: int) -> None:

@@ -128,7 +128,7 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
             else:
                 se = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
             err = np.abs(a - b)
-            scale = max(np.abs(b).max(), 1e-30)
+            scale = max(np.abs(b).max(), 1.0)  # one currency unit: some series are exactly zero (no negative exposure)
             live = se > 1e-12 * scale
             if np.any(live):
                 ratio = float(np.max(err[live] / se[live]))
