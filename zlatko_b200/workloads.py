@@ -13,6 +13,11 @@ correlated_csa_book: 1,000 trades (600 swaps, 300 FX forwards, 100 FX options) i
     curves drawn U[0%, 4%] (the configuration's three currencies); with foreign_rates=False they
     are the reference's deterministic carry curves instead.
 
+xva_batch: the large wrong-way-risk XVA batch -- 10,000 trades (60% swaps, 25% FX forwards, 10% FX options, 5%
+    Bermudan swaptions) in 500 netting sets of Zipf(1.1) sizes spread over 8 portfolios, on the correlated book's
+    three-currency model with the intensity correlated 0.3 with the domestic short rate, monthly to 10y; each
+    netting set with and without its CSA.
+
 Cash-flow and maturity dates are whole months, so every event date falls on the monthly grid.
 Draws use numpy's PCG64 seeded with 20261203 (portfolio) and the simulation seed 42.
 """
@@ -171,3 +176,47 @@ def nested_netting_set(seed: int = PORTFOLIO_SEED + 7, swaps: int = 20, forwards
         trades.append(S.Option(asset, bool(rng.random() < 0.5), rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 3e6),
                                (1.1, 0.9)[asset] * rng.uniform(0.9, 1.1), int(rng.integers(3, 37)) / 12.0))
     return S.NettingSet(trades, None)
+
+
+def xva_batch(paths: int = 1_000_000, num_trades: int = 10_000, netting_sets: int = 500, portfolios: int = 8,
+              rate_intensity_correlation: float = 0.3):
+    """Returns (model, collateralised netting sets, uncollateralised netting sets, portfolio of each netting set,
+    number of trades).  The model is the correlated book's (three Hull-White currencies, two FX rates, CIR++)
+    with the correlation of the domestic rate and the intensity set to 0.3 and the matrix projected to the nearest
+    correlation matrix.  Swaps, forwards and options are drawn as in the correlated book, Bermudans as in the AMC
+    book (10y annual swaps, exercise annually from 1y, strike ATM +- 100bp); netting set sizes Zipf(1.1); CSA
+    threshold U[0, 5e6], MTA 1e5, MPR 10 business days; netting set k belongs to portfolio k mod 8."""
+    m, _, _, _ = correlated_csa_book(paths)
+    c = np.asarray(m.correlation, dtype=np.float64).copy()
+    credit = 1 + len(m.assets)  # factor order [rate, assets, credits, foreign rates]
+    c[0, credit] = c[credit, 0] = rate_intensity_correlation
+    m.correlation = nearest_correlation(c)
+    rng = np.random.default_rng(PORTFOLIO_SEED + 4)
+    n_swaps, n_fwds, n_opts = round(0.6 * num_trades), round(0.25 * num_trades), round(0.1 * num_trades)
+    n_berm = num_trades - n_swaps - n_fwds - n_opts
+    fx = m.assets
+    trades: list = [random_swap(rng, 120) for _ in range(n_swaps)]
+    for _ in range(n_fwds):
+        a = int(rng.integers(0, 2))
+        trades.append(S.Forward(a, rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 1e7), fx[a].spot * rng.uniform(0.9, 1.1),
+                                int(rng.integers(3, 61)) / 12.0))
+    for _ in range(n_opts):
+        a = int(rng.integers(0, 2))
+        trades.append(S.Option(a, bool(rng.random() < 0.5), rng.choice([-1.0, 1.0]) * rng.uniform(1e6, 5e6),
+                               fx[a].spot * rng.uniform(0.9, 1.1), int(rng.integers(3, 37)) / 12.0))
+    atm = float(np.expm1(0.02))
+    for _ in range(n_berm):
+        k = atm + rng.uniform(-0.01, 0.01)
+        trades.append(S.Bermudan(S.Swap(1e7, k, bool(rng.random() < 0.5), S.vanilla_schedule(0.0, 10.0, 1)),
+                                 [float(e) for e in range(1, 10)], physical=True, position=1.0, degree=3))
+    order = rng.permutation(len(trades))
+    sizes = zipf_sizes(len(trades), netting_sets, 1.1)
+    csa_books, plain_books, at = [], [], 0
+    for n in sizes:
+        t = rng.uniform(0.0, 5e6)
+        chosen = [trades[i] for i in order[at:at + n]]
+        csa_books.append(S.NettingSet(chosen, S.Csa(t, t, 1e5, 0.0, 10.0 / 250.0)))
+        plain_books.append(S.NettingSet(list(chosen), None))
+        at += n
+    portfolio = [k % portfolios for k in range(netting_sets)]
+    return m, csa_books, plain_books, portfolio, len(trades)
