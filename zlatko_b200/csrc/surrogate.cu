@@ -441,12 +441,12 @@ __global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __r
   auto epilogue = [&](const float* bias, bool head, uint32_t row) {
     float acc = 0.0f;
 #pragma unroll 1
-    for (uint32_t c = 0; c < kHid; c += 16) {
-      float v[16];
-      umma::ld16(taddr + c, v);
-      uint32_t hb[8];  // 16 activations as bf16 pairs
+    for (uint32_t c = 0; c < kHid; c += 32) {  // 32 columns per TMEM load and wait
+      float v[32];
+      umma::ld32(taddr + c, v);
+      uint32_t hb[16];  // 32 activations as bf16 pairs
 #pragma unroll
-      for (int j = 0; j < 16; j += 2) {
+      for (int j = 0; j < 32; j += 2) {
         hb[j / 2] = umma::siluHalfBf16x2(fmaf(v[j], 0.5f, bias[c + j]), fmaf(v[j + 1], 0.5f, bias[c + j + 1]));
         if (head) {
           acc += __uint_as_float(hb[j / 2] << 16) * par[3 * kHid + c + j];
@@ -454,8 +454,10 @@ __global__ void __launch_bounds__(kMlpThreads, 1) mlpInferKernel(const bf16* __r
         }
       }
       if (!head) {
-        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c, 128)) = make_uint4(hb[0], hb[1], hb[2], hb[3]);
-        *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c + 8, 128)) = make_uint4(hb[4], hb[5], hb[6], hb[7]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4*>(hs + umma::kMajorOffset(gt, c + 8 * q, 128)) =
+              make_uint4(hb[4 * q], hb[4 * q + 1], hb[4 * q + 2], hb[4 * q + 3]);
       }
     }
     if (head) pred[row] = acc + par[4 * kHid];

@@ -116,6 +116,9 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
         pk = [gpu.compile(mk, b, options) for b in books]
         est.append([outputs(p, s, v, mk, own) for p, (s, v) in zip(pk, _run32(ctx, pk))])
     scale_paths = np.sqrt(per / model.num_paths)
+    # The scale of a netting set's values, for entries without Monte Carlo error (a series that is exactly zero in
+    # FP64, such as the ENE of a set whose exposure is never negative, has no scale of its own).
+    vscale = [max(np.abs(o["ee"]).max(), np.abs(o["ene"]).max(), 1.0) for o in o64]
     report: Dict[str, Dict] = {}
     for key in SERIES + SCALARS:
         worst, worst_ns, rel, rel_det = 0.0, -1, 0.0, 0.0
@@ -128,7 +131,7 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
             else:
                 se = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
             err = np.abs(a - b)
-            scale = max(np.abs(b).max(), 1.0)  # one currency unit: some series are exactly zero (no negative exposure)
+            scale = max(np.abs(b).max(), vscale[i])
             live = se > 1e-12 * scale
             if np.any(live):
                 ratio = float(np.max(err[live] / se[live]))
