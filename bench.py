@@ -242,20 +242,22 @@ def guarded(fn, *args):
 
 
 def surrogate_leg(ctx, a):
-    """CVA of the bench's book (its netting sets without CSA: the surrogate revalues reporting dates only) by the
-    surrogate with its 1% plain-pricer audit and per-netting-set fallback, against the plain GPU pricer on the same
-    paths: device time of each, the CVA difference and the fallbacks.  The network is trained on the per-trade
-    values the plain pricer itself produces on --surrogate-train-paths paths (every live trade, date and path: about
-    50M revaluations for this book); training is reported apart, it runs once per book."""
+    """CVA of the bench's book, with its cash CSAs, by the surrogate with its 1% plain-pricer audit and
+    per-netting-set fallback, against the plain GPU pricer on the same paths: device time of each, the CVA difference
+    and the fallbacks.  The surrogate revalues every simulation date (the margin-call dates included) and the GPU
+    applies the collateral rule per path.  The network is trained on the per-trade values the plain pricer itself
+    produces on --surrogate-train-paths paths (every live trade and reporting date: about 40M revaluations for this
+    book); training is reported apart, it runs once per book."""
     from zlatko_b200 import surrogate_book as SB
     from zlatko_b200 import workloads
     from zlatko_b200.surrogate import Surrogate
 
     # The surrogate's features cover the reference's model family: deterministic foreign curves.
     m, books, _, trades = workloads.correlated_csa_book(a.surrogate_paths, a.netting_sets, a.trades, foreign_rates=False)
-    book = SB.make_book(m, books)
+    train_book = SB.make_book(m, books)
+    book = SB.make_book(m, books, csa=True)
     t0 = time.perf_counter()
-    X, y = SB.training_set(ctx, book, a.surrogate_train_paths)
+    X, y = SB.training_set(ctx, train_book, a.surrogate_train_paths)
     rows_s = time.perf_counter() - t0
     with Surrogate(ctx, seed=1) as s:
         t0 = time.perf_counter()
@@ -268,15 +270,17 @@ def surrogate_leg(ctx, a):
     plain = float(SB.cva(book, dee_p).sum())
     ms_sur = run.ms_surrogate + run.ms_audit + run.ms_fallback
     revals = float(a.surrogate_paths) * len(book.times) * trades
-    return {"workload": f"the bench's book without CSA: {trades} trades in {len(books)} netting sets, {a.surrogate_paths} paths, "
-                        f"{len(book.times)} reporting dates; trained on {a.surrogate_train_paths} paths",
+    return {"workload": f"the bench's book with its cash CSAs: {trades} trades in {len(books)} netting sets, {a.surrogate_paths} "
+                        f"paths, {len(book.times)} simulation dates (margin-call dates included), reference model family; "
+                        f"trained on {a.surrogate_train_paths} paths",
             "cva_plain": plain, "cva_surrogate_audited": float(run.cva.sum()),
             "delta_cva_rel": float(run.cva.sum() / plain - 1.0),
             "ms_plain": ms_plain, "ms_surrogate": run.ms_surrogate, "ms_audit": run.ms_audit, "ms_fallback": run.ms_fallback,
             "speedup_vs_plain": ms_plain / ms_sur if ms_sur > 0 else None,
             "surrogate_revals_per_s": revals / (run.ms_surrogate / 1e3),
             "plain_revals_per_s": revals / (ms_plain / 1e3),
-            "fallback_netting_sets": len(run.fallback), "netting_sets": len(books), "train_rows": int(len(y)),
+            "fallback_netting_sets": len(run.fallback), "netting_sets": len(books),
+            "audit_error_median": float(np.median(run.audit_error)), "train_rows": int(len(y)),
             "training_rows_s": rows_s, "train_s": train_s, "train_loss": float(losses[-1])}
 
 
@@ -713,6 +717,7 @@ def main():
     except Exception:
         C_ex2 = None
     exp_per_launch = float(info.exp_evaluations) * nP  # one ex2 per bond-like term and path
+    row_bytes = float(sum(p.rows_total for p in plans)) * nP * 4
     h2d = info.table_bytes + sum(p.indices.size * 4 for p in plans)
     d2h = sum((p.sums_len() + p.values_len()) * 4 for p in plans)
 
@@ -753,6 +758,10 @@ def main():
                          "frac": alg_bytes / fused_s / 1e9 / peak, "traffic": traffic_per_launch(nP),
                          "note": f"revalue kernel (the dominant one); peak of {peak_kind}; algorithmic bytes = factor cube read "
                                  "once + PFE rows written + per-group partials + plan tables"},
+            "roofline_row_stats": {"bound": "hbm", "achieved": row_bytes / (float(np.mean(rows_ms)) / 1e3) / 1e9, "peak": peak,
+                                   "unit": "GB/s", "frac": row_bytes / (float(np.mean(rows_ms)) / 1e3) / 1e9 / peak,
+                                   "note": "row-statistics kernel: algorithmic bytes = every exposure row read once; the exact "
+                                           "quantile reads a row up to three times (min/max of a sample, histogram, bracket)"},
             "roofline_mufu": {"bound": "sfu", "achieved": exp_per_launch / fused_s / 1e9 if C_ex2 else None,
                               "peak": C_ex2 / 1e9 if C_ex2 else None, "unit": "G ex2/s",
                               "frac": exp_per_launch / fused_s / C_ex2 if C_ex2 else None},

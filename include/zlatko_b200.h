@@ -283,16 +283,23 @@ typedef struct zk_surrogate_trade {
 /* Features of every (trade, reporting date, path): X[nTr][nR][nP][16] (the training inputs).  factors is
  * [2 + nA][nR][nP] on the reporting dates: the deflator, the Hull-White state x, then ln S of each FX factor;
  * resets[nTr][nR] is the reporting-date index of the reset of the swap period running on each date (-1: none),
- * periods[nTr][nR][2] that period's start and end. */
+ * periods[nTr][nR][2] that period's start and end; bonds (nullable) [nTr][nR][4] = (ln A, B) of the zero bond to
+ * the trade's maturity and of the one to the end of its running period, P(t, T | x) = A exp(-B x): features 14
+ * and 15 (zero without). */
 zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* X);
+                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
+                                const float* bonds, float* X);
 /* Revaluation of a book by the surrogate on the GPU: features, tensor-core inference and netting per netting
- * set, then exposure[num_netting_sets][nR][2] = (EE, EE*) on the reporting dates; netted_out (nullable,
+ * set, then exposure[num_netting_sets][nR][2] = (EE, EE*) on the nR dates given; netted_out (nullable,
  * [num_netting_sets][nR][paths_out]) receives the netted values of the first paths_out paths; ms[2] (nullable) the
- * device time of the revaluation and of the exposure reduction. */
+ * device time of the revaluation and of the exposure reduction.  csa (nullable, [num_netting_sets][4] = hc, ho
+ * (< 0: none), mta (< 0: no CSA), ia) applies each netting set's cash CSA on its netted values before the reduction,
+ * the collateral called on the value at date call_index[j] (at most 31 dates before j; collateral.cpp:10-47):
+ * pass every simulation date, margin-call dates included, and netted_out then holds V - collateral. */
 zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
                             const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
-                            uint32_t num_netting_sets, double* exposure, float* netted_out, uint32_t paths_out, float* ms);
+                            const float* bonds, uint32_t num_netting_sets, const float* csa, const uint32_t* call_index,
+                            double* exposure, float* netted_out, uint32_t paths_out, float* ms);
 
 /* Measured rate of the special-function unit's ex2 (billions per second on the whole GPU), the ceiling
  * of the fused kernel's bond exponentials (a roofline denominator; not part of the reference). */

@@ -105,9 +105,9 @@ def lib() -> C.CDLL:
         "zk_surrogate_predict": (st, [vp, vp, sz, vp]),
         "zk_surrogate_gradients": (st, [vp, vp, vp, sz, vp, vp]),
         "zk_surrogate_params": (st, [vp, vp, vp, vp, vp]),
-        "zk_surrogate_features": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp]),
-        "zk_surrogate_book": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp,
-                                   C.c_uint32, vp]),
+        "zk_surrogate_features": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp, vp]),
+        "zk_surrogate_book": (st, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp, C.c_uint32, vp, vp,
+                                   vp, vp, C.c_uint32, vp]),
         "zk_fit_amc_f64": (st, [vp, P(PlanViewF64), vp, sz, vp, sz, vp, sz]),
         "zk_run_plan_f64": (st, [vp, P(PlanViewF64), vp, sz, P(OutputF64), vp]),
         "zk_run_plan_injected": (st, [vp, P(PlanView), vp, sz, P(Output), vp]),

@@ -1595,7 +1595,8 @@ zk_status zk_surrogate_gradients(zk_surrogate* s, const float* x, const float* y
 }
 
 zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* X) {
+                                const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
+                                const float* bonds, float* X) {
   void* d = nullptr;
   try {
     requireCtx(ctx);
@@ -1606,7 +1607,8 @@ zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t 
     for (size_t i = 0; i < static_cast<size_t>(nTr) * nR; ++i)
       if (resets[i] >= static_cast<int32_t>(nR)) throw fail(ZK_ERR_INVALID_ARGUMENT, "reset index beyond the reporting dates");
     const size_t o1 = (nf * 4 + 255) / 256 * 256, o2 = o1 + (nR * 4 + 255) / 256 * 256, o3 = o2 + (nTr * 32 + 255) / 256 * 256;
-    const size_t o4 = o3 + (nTr * nR * 4 + 255) / 256 * 256, o5 = o4 + (nTr * nR * 8 + 255) / 256 * 256;
+    const size_t o4 = o3 + (nTr * nR * 4 + 255) / 256 * 256, o4b = o4 + (nTr * nR * 8 + 255) / 256 * 256;
+    const size_t o5 = o4b + (bonds ? (nTr * nR * 16 + 255) / 256 * 256 : 0);
     ZK_CUDA(cudaMalloc(&d, o5 + std::max<size_t>(rows, 1) * 64));
     unsigned char* b = static_cast<unsigned char*>(d);
     ZK_CUDA(cudaMemcpyAsync(b, factors, nf * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -1614,9 +1616,11 @@ zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t 
     ZK_CUDA(cudaMemcpyAsync(b + o2, trades, nTr * 32, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(b + o3, resets, nTr * nR * 4, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(b + o4, periods, nTr * nR * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (bonds) ZK_CUDA(cudaMemcpyAsync(b + o4b, bonds, nTr * nR * 16, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(zk::surrogateFeatures(reinterpret_cast<const float*>(b), nA, nR, nP, reinterpret_cast<const float*>(b + o1),
                                   reinterpret_cast<const zk::SurrogateTrade*>(b + o2), reinterpret_cast<const int32_t*>(b + o3),
-                                  reinterpret_cast<const float*>(b + o4), 0, rows, reinterpret_cast<float*>(b + o5), ctx->stream));
+                                  reinterpret_cast<const float*>(b + o4), bonds ? reinterpret_cast<const float*>(b + o4b) : nullptr, 0,
+                                  rows, reinterpret_cast<float*>(b + o5), ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(X, b + o5, rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
     ZK_CUDA(cudaStreamSynchronize(ctx->stream));
     ZK_CUDA(cudaFree(d));
@@ -1629,7 +1633,8 @@ zk_status zk_surrogate_features(zk_context* ctx, const float* factors, uint32_t 
 
 zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
                             const zk_surrogate_trade* trades, uint32_t nTr, const int32_t* resets, const float* periods,
-                            uint32_t num_netting_sets, double* exposure, float* netted_out, uint32_t paths_out, float* ms) {
+                            const float* bonds, uint32_t num_netting_sets, const float* csa, const uint32_t* call_index,
+                            double* exposure, float* netted_out, uint32_t paths_out, float* ms) {
   zk_context* ctx = s ? s->ctx : nullptr;
   void* d = nullptr;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -1637,6 +1642,10 @@ zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, 
     ctx = ctxOf(s);
     if (!factors || !times || !trades || !resets || !periods || !exposure) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
     if (paths_out > nP || (paths_out && !netted_out)) throw fail(ZK_ERR_INVALID_ARGUMENT, "paths_out beyond the paths");
+    if (csa && !call_index) throw fail(ZK_ERR_INVALID_ARGUMENT, "a CSA needs the margin-call index of every date");
+    if (csa)
+      for (uint32_t j = 0; j < nR; ++j)
+        if (call_index[j] > j || j - call_index[j] >= 32u) throw fail(ZK_ERR_INVALID_ARGUMENT, "margin-call date %u of date %u", call_index[j], j);
     for (uint32_t t = 0; t < nTr; ++t) {
       if (trades[t].kind > 2) throw fail(ZK_ERR_INVALID_ARGUMENT, "trade %u: kind %u", t, trades[t].kind);
       if (trades[t].netting_set >= num_netting_sets) throw fail(ZK_ERR_INVALID_ARGUMENT, "trade %u: netting set beyond the count", t);
@@ -1649,6 +1658,8 @@ zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, 
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
     const size_t oF = take(nf * 4), oT = take(nR * 4), oTr = take(nTr * 32), oR = take(nTr * nR * 4), oP = take(nTr * nR * 8);
+    const size_t oB = take(bonds ? nTr * nR * 16 : 16);
+    const size_t oC = take(csa ? num_netting_sets * 16 : 16), oI = take(csa ? nR * 4 : 16);
     const size_t oN = take(static_cast<size_t>(num_netting_sets) * plane * 4), oE = take(num_netting_sets * nR * 16);
     const size_t oX = take(chunkRows * 64), oY = take(chunkRows * 4);
     ZK_CUDA(cudaMalloc(&d, off));
@@ -1658,15 +1669,24 @@ zk_status zk_surrogate_book(zk_surrogate* s, const float* factors, uint32_t nA, 
     ZK_CUDA(cudaMemcpyAsync(b + oTr, trades, nTr * 32, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(b + oR, resets, nTr * nR * 4, cudaMemcpyHostToDevice, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(b + oP, periods, nTr * nR * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (bonds) ZK_CUDA(cudaMemcpyAsync(b + oB, bonds, nTr * nR * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if (csa) {
+      ZK_CUDA(cudaMemcpyAsync(b + oC, csa, num_netting_sets * 16, cudaMemcpyHostToDevice, ctx->stream));
+      ZK_CUDA(cudaMemcpyAsync(b + oI, call_index, nR * 4, cudaMemcpyHostToDevice, ctx->stream));
+    }
     ZK_CUDA(cudaMemsetAsync(b + oN, 0, static_cast<size_t>(num_netting_sets) * plane * 4, ctx->stream));
     ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, ctx->stream));
     for (auto& e : ev) ZK_CUDA(cudaEventCreate(&e));
     ZK_CUDA(cudaEventRecord(ev[0], ctx->stream));
     ZK_CUDA(zk::surrogateBook(s->S, reinterpret_cast<const float*>(b + oF), nA, nR, nP, reinterpret_cast<const float*>(b + oT),
                               reinterpret_cast<const zk::SurrogateTrade*>(b + oTr), nTr, reinterpret_cast<const int32_t*>(b + oR),
-                              reinterpret_cast<const float*>(b + oP), reinterpret_cast<float*>(b + oN), reinterpret_cast<float*>(b + oX),
+                              reinterpret_cast<const float*>(b + oP), bonds ? reinterpret_cast<const float*>(b + oB) : nullptr,
+                              reinterpret_cast<float*>(b + oN), reinterpret_cast<float*>(b + oX),
                               reinterpret_cast<float*>(b + oY), chunk));
     ZK_CUDA(cudaEventRecord(ev[1], ctx->stream));
+    if (csa)
+      ZK_CUDA(zk::surrogateCollateral(reinterpret_cast<float*>(b + oN), reinterpret_cast<const float*>(b + oC),
+                                      reinterpret_cast<const uint32_t*>(b + oI), num_netting_sets, nR, nP, ctx->stream));
     ZK_CUDA(zk::surrogateExposure(reinterpret_cast<const float*>(b + oN), reinterpret_cast<const float*>(b + oF), num_netting_sets, nR,
                                   nP, reinterpret_cast<double*>(b + oE), ctx->stream));
     ZK_CUDA(cudaEventRecord(ev[2], ctx->stream));

@@ -520,8 +520,8 @@ namespace {
 // ((trade * nR + r) * nP + p).  factors = [D | x | ln S_0 .. ln S_{nA-1}][nR][nP].
 __global__ void featureKernel(const float* __restrict__ factors, uint32_t nA, uint32_t nR, uint32_t nP,
                               const float* __restrict__ times, const SurrogateTrade* __restrict__ trades,
-                              const int32_t* __restrict__ resets, const float* __restrict__ periods, uint64_t row0, uint64_t n,
-                              float* __restrict__ X) {
+                              const int32_t* __restrict__ resets, const float* __restrict__ periods,
+                              const float* __restrict__ bonds, uint64_t row0, uint64_t n, float* __restrict__ X) {
   const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint64_t row = row0 + i;
@@ -547,6 +547,11 @@ __global__ void featureKernel(const float* __restrict__ factors, uint32_t nA, ui
   f[12] = te - ts;
   f[13] = static_cast<float>(T.asset);
   f[14] = 0.0f, f[15] = 0.0f;
+  if (bonds) {  // P(t, maturity | x) and P(t, end of the running period | x) = exp(ln A - B x)
+    const float* q = bonds + 4 * tr_r;
+    f[14] = __expf(q[0] - q[1] * f[0]);
+    f[15] = __expf(q[2] - q[3] * f[0]);
+  }
   float4* dst = reinterpret_cast<float4*>(X + i * kIn);
 #pragma unroll
   for (int q = 0; q < 4; ++q) dst[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
@@ -564,6 +569,34 @@ __global__ void netKernel(const float* __restrict__ pred, const SurrogateTrade* 
     const SurrogateTrade T = trades[tr];
     if (times[r] >= T.maturity - 1e-6f) continue;
     netted[T.nettingSet * plane + i] += T.notional * pred[static_cast<size_t>(tr - tr0) * plane + i];
+  }
+}
+
+// The cash CSA of each netting set on its netted values, in place: one thread per (netting set, path) walks the
+// dates in order with the collateral rule of the fused kernel (collateral.cpp:10-47): the value at the margin-call
+// date call[j] (a look-back of at most kSurrogateRing dates, kept in a ring of the thread's past values), two-way
+// thresholds, the minimum transfer amount, the independent amount; netted[ns][j][p] becomes the exposure value
+// V - collateral.  csa[ns] = (hc, ho (< 0: none), mta (< 0: no CSA), ia).
+constexpr int kSurrogateRing = 32;
+__global__ void collateralKernel(float* __restrict__ netted, const float* __restrict__ csa, const uint32_t* __restrict__ call,
+                                 uint32_t numNs, uint32_t nR, uint32_t nP) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<uint64_t>(numNs) * nP) return;
+  const uint32_t ns = static_cast<uint32_t>(i / nP), p = static_cast<uint32_t>(i % nP);
+  const float hc = csa[4 * ns], ho = csa[4 * ns + 1], mta = csa[4 * ns + 2], ia = csa[4 * ns + 3];
+  if (mta < 0.0f) return;
+  float* v = netted + static_cast<size_t>(ns) * nR * nP + p;
+  float ring[kSurrogateRing];
+  float held = 0.0f;
+  for (uint32_t j = 0; j < nR; ++j) {
+    const float value = v[static_cast<size_t>(j) * nP];
+    ring[j % kSurrogateRing] = value;
+    const float vc = ring[call[j] % kSurrogateRing];
+    float required = 0.0f;
+    if (vc > hc) required += vc - hc;
+    if (ho >= 0.0f && -vc > ho) required -= -vc - ho;
+    if (j == 0 || fabsf(required - held) >= mta) held = required;
+    v[static_cast<size_t>(j) * nP] = value - (held + ia);
   }
 }
 
@@ -595,21 +628,22 @@ __global__ void exposureKernel(const float* __restrict__ netted, const float* __
 }  // namespace
 
 cudaError_t surrogateFeatures(const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, uint64_t row0, uint64_t n,
-                              float* X, cudaStream_t s) {
+                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, const float* bonds,
+                              uint64_t row0, uint64_t n, float* X, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  featureKernel<<<static_cast<uint32_t>((n + 255) / 256), 256, 0, s>>>(factors, nA, nR, nP, times, trades, resets, periods, row0, n, X);
+  featureKernel<<<static_cast<uint32_t>((n + 255) / 256), 256, 0, s>>>(factors, nA, nR, nP, times, trades, resets, periods, bonds,
+                                                                      row0, n, X);
   return cudaGetLastError();
 }
 
 cudaError_t surrogateBook(SurrogateState& S, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* netted,
-                          float* X, float* pred, uint32_t chunkTrades) {
+                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, const float* bonds,
+                          float* netted, float* X, float* pred, uint32_t chunkTrades) {
   const uint64_t plane = static_cast<uint64_t>(nR) * nP;
   for (uint32_t t0 = 0; t0 < nTr; t0 += chunkTrades) {
     const uint32_t t1 = std::min(nTr, t0 + chunkTrades);
     const uint64_t rows = plane * (t1 - t0);
-    SG_CUDA(surrogateFeatures(factors, nA, nR, nP, times, trades, resets, periods, plane * t0, rows, X, S.stream));
+    SG_CUDA(surrogateFeatures(factors, nA, nR, nP, times, trades, resets, periods, bonds, plane * t0, rows, X, S.stream));
     SG_CUDA(surrogatePredict(S, X, rows, pred));
     netKernel<<<static_cast<uint32_t>((plane + 255) / 256), 256, 0, S.stream>>>(pred, trades, t0, t1, times, nR, nP, netted);
     SG_CUDA(cudaGetLastError());
@@ -620,6 +654,14 @@ cudaError_t surrogateBook(SurrogateState& S, const float* factors, uint32_t nA, 
 cudaError_t surrogateExposure(const float* netted, const float* D, uint32_t numNs, uint32_t nR, uint32_t nP, double* out,
                               cudaStream_t s) {
   exposureKernel<<<dim3(nR, numNs), 256, 0, s>>>(netted, D, nR, nP, out);
+  return cudaGetLastError();
+}
+
+cudaError_t surrogateCollateral(float* netted, const float* csa, const uint32_t* call, uint32_t numNs, uint32_t nR, uint32_t nP,
+                                cudaStream_t s) {
+  const uint64_t n = static_cast<uint64_t>(numNs) * nP;
+  if (n == 0) return cudaSuccess;
+  collateralKernel<<<static_cast<uint32_t>((n + 255) / 256), 256, 0, s>>>(netted, csa, call, numNs, nR, nP);
   return cudaGetLastError();
 }
 

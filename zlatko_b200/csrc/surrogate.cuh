@@ -71,13 +71,17 @@ cudaError_t surrogatePredict(SurrogateState& S, const float* dx, size_t n, float
 
 // Features of rows [row0, row0 + n) in (trade, reporting date, path) order into X [n][16].
 cudaError_t surrogateFeatures(const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, uint64_t row0, uint64_t n,
-                              float* X, cudaStream_t s);
+                              const SurrogateTrade* trades, const int32_t* resets, const float* periods, const float* bonds,
+                              uint64_t row0, uint64_t n, float* X, cudaStream_t s);
 // Netted values [numNs][nR][nP] (accumulated into `netted`, zeroed by the caller) of a book, chunkTrades trades
 // at a time through features, prediction and netting; X and pred hold chunkTrades * nR * nP rows.
 cudaError_t surrogateBook(SurrogateState& S, const float* factors, uint32_t nA, uint32_t nR, uint32_t nP, const float* times,
-                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, float* netted,
-                          float* X, float* pred, uint32_t chunkTrades);
+                          const SurrogateTrade* trades, uint32_t nTr, const int32_t* resets, const float* periods, const float* bonds,
+                          float* netted, float* X, float* pred, uint32_t chunkTrades);
+// The cash CSA of every netting set applied in place: netted[ns][j][p] becomes V - collateral, the collateral called
+// on the value at date call[j] <= j (at most 31 dates back); csa[ns] = (hc, ho (< 0: none), mta (< 0: no CSA), ia).
+cudaError_t surrogateCollateral(float* netted, const float* csa, const uint32_t* call, uint32_t numNs, uint32_t nR, uint32_t nP,
+                                cudaStream_t s);
 // out[ns][r] = (EE, EE*) of the netted values with the deflator D [nR][nP].
 cudaError_t surrogateExposure(const float* netted, const float* D, uint32_t numNs, uint32_t nR, uint32_t nP, double* out,
                               cudaStream_t s);

@@ -13,10 +13,13 @@ The flow (the learned part of the exposure path; the reference has no counterpar
    paths;
 4. CVA of each netting set from its EE* and the counterparty's market hazard curve (unilateral, LGD 0.6).
 
-The surrogate sees uncollateralised netting sets: a CSA's margin-call look-back needs the values on the
-margin-call dates, which are not reporting dates.  Features: x, ln S of the trade's FX factor, t, time to
+Uncollateralised, the surrogate revalues the reporting dates.  With the netting sets' cash CSAs (make_book with
+csa=True) it revalues every simulation date, the margin-call dates t - MPR included, and zk_surrogate_book applies
+the collateral rule (collateral.cpp:10-47) to each path's netted values before the exposure statistics.  Features: x, ln S of the trade's FX factor, t, time to
 maturity, trade kind (one-hot), strike or fixed rate, call / pay sign, the Hull-White state at the reset of the
-running floating period and that period's position (elapsed, remaining, length), the FX factor index.
+running floating period and that period's position (elapsed, remaining, length), the FX factor index, and the zero
+bonds P(t, maturity | x) and P(t, end of the running period | x) (two exponentials per row, against the network's
+~70 kflop).
 """
 from __future__ import annotations
 
@@ -45,6 +48,15 @@ class Book:
     times: np.ndarray                  # reporting dates
     resets: np.ndarray                 # [nTr][nR] int32
     periods: np.ndarray                # [nTr][nR][2] float32
+    bonds: np.ndarray                  # [nTr][nR][4] float32: (ln A, B) to maturity and to the running period's end
+    report: np.ndarray = None          # indices of the reporting dates in `times` (all of them without a CSA)
+    csa: np.ndarray = None             # [numNs][4] float32 (hc, ho or -1, mta or -1 without CSA, ia), None: no CSA
+    call_index: np.ndarray = None      # [nR] uint32: margin-call date of each date (with csa)
+    factor_model: S.Model = None       # the model whose factor views cover `times`
+
+    @property
+    def report_times(self) -> np.ndarray:
+        return self.times[self.report].astype(np.float64)
 
 
 def uncollateralised(books: Sequence[S.NettingSet]) -> List[S.NettingSet]:
@@ -59,10 +71,34 @@ def _float_schedule(t) -> np.ndarray:
     return np.zeros(0)
 
 
-def make_book(model: S.Model, books: Sequence[S.NettingSet]) -> Book:
-    nets = uncollateralised(books)
-    probe = gpu.compile(model, S.NettingSet([]), S.Options(factor_views=True))
-    times = probe.times[probe.reporting.astype(np.int64)]
+def make_book(model: S.Model, books: Sequence[S.NettingSet], csa: bool = False) -> Book:
+    """The surrogate's view of a book.  Without csa, the netting sets uncollateralised on their reporting dates.  With
+    csa, their cash CSAs kept: the surrogate then revalues every simulation date, the margin-call dates t - MPR
+    included, so that the collateral rule can look back to them."""
+    nets = list(books) if csa else uncollateralised(books)
+    report = call_index = csa_arr = None
+    factor_model = model
+    if csa:
+        plans = [gpu.compile(model, ns, S.Options()) for ns in nets]
+        p0 = plans[0]
+        if any(not np.array_equal(p.times, p0.times) for p in plans):
+            raise ValueError("the surrogate's CSA book needs its netting sets on one simulation grid")
+        times = np.asarray(p0.times)
+        report = p0.reporting.astype(np.int64)
+        call_index = p0.indices[p0.num_dates + 1:2 * p0.num_dates + 1].astype(np.uint32)
+        csa_arr = np.full((len(nets), 4), -1.0, np.float32)
+        for k, ns in enumerate(nets):
+            c = ns.csa
+            if c is None:
+                continue
+            if c.kind != 0:
+                raise ValueError("the surrogate's collateral is cash")
+            csa_arr[k] = (c.threshold_cpty, c.threshold_own if np.isfinite(c.threshold_own) else -1.0, c.mta, c.ia)
+        factor_model = replace(model, base_grid=[float(t) for t in times[1:]])
+    else:
+        probe = gpu.compile(model, S.NettingSet([]), S.Options(factor_views=True))
+        times = probe.times[probe.reporting.astype(np.int64)]
+        report = np.arange(len(times))
     rows, specs = [], []
     for n, ns in enumerate(nets):
         for t in ns.trades:
@@ -90,7 +126,28 @@ def make_book(model: S.Model, books: Sequence[S.NettingSet]) -> Book:
             if live.any() and len(r):
                 resets[i, live] = r[0]
                 periods[i, live] = (ts, te)
-    return Book(model, nets, trades, specs, times.astype(np.float32), resets, periods)
+    return Book(model, nets, trades, specs, times.astype(np.float32), resets, periods, bond_features(model, trades, times, periods),
+                report, csa_arr, call_index, factor_model)
+
+
+def bond_features(model: S.Model, trades: np.ndarray, times: np.ndarray, periods: np.ndarray) -> np.ndarray:
+    """[nTr][nR][4] = (ln A, B) of P(t, maturity | x) and of P(t, end of the running period | x) (the maturity where
+    none runs) on every reporting date, from the Hull-White bond formula (hull_white.cpp:27-31): the network's
+    features 14 and 15.  Past the end (t >= T) the bond is 1."""
+    from .nested_exposure import zero_bonds
+
+    nTr, nR = len(trades), len(times)
+    t = np.broadcast_to(np.asarray(times, np.float64)[None, :], (nTr, nR))
+    mat = np.broadcast_to(trades["maturity"].astype(np.float64)[:, None], (nTr, nR))
+    nxt = np.where(periods[..., 1] > 0, periods[..., 1].astype(np.float64), mat)
+    out = np.zeros((nTr, nR, 4), np.float32)
+    for k, T in ((0, mat), (2, nxt)):
+        live = T > t + 1e-9
+        pairs = np.stack([t[live], T[live]], axis=1)
+        c = zero_bonds(S.encode_model(model), pairs)
+        out[..., k][live] = np.log(c[:, 0]) + c[:, 1]
+        out[..., k + 1][live] = c[:, 2]
+    return out
 
 
 def factor_rows(ctx: gpu.Context, model: S.Model, paths: int) -> np.ndarray:
@@ -134,13 +191,17 @@ def features(ctx: gpu.Context, book: Book, factors: np.ndarray) -> np.ndarray:
     X = np.zeros((nTr, nR, nP, 16), np.float32)
     f = np.ascontiguousarray(factors, np.float32)
     check(lib().zk_surrogate_features(ctx.handle, f.ctypes.data, nA, nR, nP, book.times.ctypes.data, book.trades.ctypes.data,
-                                      nTr, book.resets.ctypes.data, book.periods.ctypes.data, X.ctypes.data), ctx.handle)
+                                      nTr, book.resets.ctypes.data, book.periods.ctypes.data, book.bonds.ctypes.data,
+                                      X.ctypes.data), ctx.handle)
     return X
 
 
 def training_set(ctx: gpu.Context, book: Book, paths: int, seed: int = 1):
     """Inputs and per-unit-notional targets of every (trade, reporting date, path) on `paths` paths, with the
-    rows past each trade's maturity left out (their value is zero by construction)."""
+    rows past each trade's maturity left out (their value is zero by construction).  The book must be the
+    uncollateralised one (a network trained on it revalues the same trades in the CSA book)."""
+    if book.csa is not None:
+        raise ValueError("train on the uncollateralised book (make_book without csa)")
     fac = factor_rows(ctx, book.model, paths)
     X = features(ctx, book, fac)
     V = plain_trade_values(ctx, book, paths) / book.trades["notional"][:, None, None]
@@ -151,19 +212,24 @@ def training_set(ctx: gpu.Context, book: Book, paths: int, seed: int = 1):
     return X[order], y[order]
 
 
-def surrogate_exposure(sur, book: Book, factors: np.ndarray, paths_out: int = 0):
-    """(EE, EE*) [numNs][nR] from zk_surrogate_book, the netted values of the first paths_out paths, and the
-    device milliseconds."""
+def surrogate_exposure(sur, book: Book, factors: np.ndarray, paths_out: int = 0, all_dates: bool = False):
+    """(EE, EE*) [numNs][nR] from zk_surrogate_book on the reporting dates, the netted values (with a CSA: value minus
+    collateral) of the first paths_out paths, and the device milliseconds; all_dates keeps every revalued date."""
     nA, nR, nP = factors.shape[0] - 2, factors.shape[1], factors.shape[2]
     nNs = len(book.netting_sets)
     exp = np.zeros((nNs, nR, 2))
     net = np.zeros((nNs, nR, max(paths_out, 1)), np.float32)
     ms = np.zeros(2, np.float32)
     f = np.ascontiguousarray(factors, np.float32)
+    csa = None if book.csa is None else np.ascontiguousarray(book.csa, np.float32)
+    call = None if book.csa is None else np.ascontiguousarray(book.call_index, np.uint32)
     check(lib().zk_surrogate_book(sur.handle, f.ctypes.data, nA, nR, nP, book.times.ctypes.data, book.trades.ctypes.data,
-                                  len(book.specs), book.resets.ctypes.data, book.periods.ctypes.data, nNs, exp.ctypes.data,
+                                  len(book.specs), book.resets.ctypes.data, book.periods.ctypes.data, book.bonds.ctypes.data,
+                                  nNs, None if csa is None else csa.ctypes.data, None if call is None else call.ctypes.data,
+                                  exp.ctypes.data,
                                   net.ctypes.data if paths_out else None, paths_out, ms.ctypes.data), sur.ctx.handle)
-    return exp[..., 0], exp[..., 1], net[..., :paths_out], ms
+    r = np.arange(nR) if all_dates else book.report  # (EE, EE*) and the audit paths' values on the reporting dates
+    return exp[:, r, 0], exp[:, r, 1], net[:, r, :paths_out], ms
 
 
 def plain_exposure(ctx: gpu.Context, book: Book, paths: int, netting_sets=None):
@@ -186,7 +252,7 @@ def plain_exposure(ctx: gpu.Context, book: Book, paths: int, netting_sets=None):
 
 def cva(book: Book, dee: np.ndarray) -> np.ndarray:
     c = book.model.credits[0]
-    t = book.times.astype(np.float64)
+    t = book.report_times
     return np.array([unilateral_cva(t, d, c.pillars, c.hazards, 1.0 - LGD) for d in dee])
 
 
@@ -205,13 +271,13 @@ class AuditedRun:
 def audited_exposure(ctx: gpu.Context, sur, book: Book, paths: int, audit_fraction: float = 0.01) -> AuditedRun:
     """Surrogate revaluation of the book on `paths` paths, audited by the plain pricer on the first
     audit_fraction of them; netting sets beyond AUDIT_TOLERANCE are revalued by the plain pricer."""
-    fac = factor_rows(ctx, book.model, paths)
+    fac = factor_rows(ctx, book.factor_model or book.model, paths)
     nAudit = max(128, int(round(paths * audit_fraction)))
     ee, dee, net_a, ms = surrogate_exposure(sur, book, fac, paths_out=nAudit)
     # Audit: the plain pricer's EPE on the audit paths against the surrogate's on the same paths.
     pe, _, ms_audit = plain_exposure(ctx, book, nAudit)
     se = np.maximum(net_a, 0.0).mean(axis=2)
-    dt = np.diff(book.times.astype(np.float64), prepend=0.0)
+    dt = np.diff(book.report_times, prepend=0.0)
     epe_p = (pe * dt).sum(1) / max(dt.sum(), 1e-12)
     epe_s = (se * dt).sum(1) / max(dt.sum(), 1e-12)
     err = np.abs(epe_s - epe_p) / np.maximum(epe_p, 1e-12)
