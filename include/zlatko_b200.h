@@ -93,6 +93,18 @@ zk_status zk_context_set_stream(zk_context* ctx, void* stream);
  * statistics follow its revalue launch, and the outputs are the same bits as in one wave.  (The reference's
  * kernels keep every netting set's rows, EXPO[rows][P], at once: fused_exposure.hpp:214-216.) */
 zk_status zk_context_set_row_budget(zk_context* ctx, uint64_t bytes);
+/* Which netting sets of a call or batch run on the tensor-core basis kernel: single-precision plans of bonds,
+ * floating coupons, FX forwards and options, with no CSA or a cash CSA looking back at most one date and no rows
+ * besides the exposure rows, grouped by identical margin-call and reporting dates into groups of at most 128.
+ * On a date every distinct bond, fixing x bond, foreign bond x FX rate, FX rate and option of a group is evaluated
+ * once per path and the netting sets' values are one FP16 hi/lo product on the tensor cores (about 22 bits of
+ * each coefficient and basis value).  ZK_BASIS_AUTO (the default): groups of at least 24 netting sets;
+ * ZK_BASIS_OFF: none (every netting set term by term, as the reference's kernel); ZK_BASIS_ALL: every eligible
+ * netting set.  No counterpart in the reference. */
+#define ZK_BASIS_AUTO 0u
+#define ZK_BASIS_OFF 1u
+#define ZK_BASIS_ALL 2u
+zk_status zk_context_set_basis(zk_context* ctx, uint32_t mode);
 
 /* ---- the drop-in backend ------------------------------------------------------------------------ */
 /* Replaces gpu::runFusedReference(plan) (src/gpu/fused_reference.cpp:628-630): the fused-exposure,
@@ -214,6 +226,13 @@ zk_status zk_run_plan_noalloc(int device, void* stream, const zk_plan_view* plan
 #define ZK_INJECT_FAIL_LAUNCH 1u
 #define ZK_INJECT_ROW_ROUNDS 2u
 zk_status zk_debug_inject(zk_context* ctx, uint32_t what, uint64_t value);
+/* Host check of the basis lowering (no GPU): lowers the n plans as one group and evaluates both the lowered
+ * group and the plans term by term in double along one path of factor values x[nT], S[nT][4], xf[nT][2].
+ * out[0]: the largest difference relative to the netting set's gross basis sum; out[1]: basis columns over all
+ * dates; out[2]: linear terms and options over all dates; out[3]: fixing slots; out[4]: coefficient chunks.
+ * ZK_ERR_UNSUPPORTED (with the reason in err) when the plans do not lower. */
+zk_status zk_debug_basis(const zk_plan_view* plans, size_t n, const double* x, const double* S, const double* xf,
+                         double* out, char* err, size_t err_len);
 
 /* ---- device-resident batches (inputs uploaded once; used to time the kernels alone) -------------- */
 typedef struct zk_batch zk_batch;
@@ -228,6 +247,7 @@ typedef struct zk_batch_info {
   uint64_t tile_paths;           /* paths per revalue CTA, chosen by the autotuner at creation     */
   uint64_t graph_replay;         /* 1 once executes replay a captured CUDA graph, 0 while eager    */
   uint64_t num_waves;            /* waves of netting sets within the row budget (1 per launch group without) */
+  uint64_t num_basis_netting_sets; /* netting sets revalued by the tensor-core basis kernel (zk_context_set_basis) */
 } zk_batch_info;
 
 /* Uploads the plans.  The first zk_batch_execute autotunes the tile shape (paths per revalue CTA) on

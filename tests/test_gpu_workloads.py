@@ -3,8 +3,9 @@
 - The swap portfolio at full size (20 two-schedule swaps, HW(0.03, 0.01), flat 2%, 10,000 paths on 60 monthly
   dates): the FP32 kernels against the restated FP32 kernels of the reference, and the FP64 mode against the
   restated FP64 ExposureEngine on identical normals (1e-9, per path).
-- The correlated CSA book, all 100 netting sets in one zk_run_plans batch (the large- and small-state launches,
-  the cash-CSA variant, the side stream): against the restated FP32 kernels, netting set by netting set; and a
+- The correlated CSA book, all 100 netting sets in one zk_run_plans batch -- on the tensor-core basis kernel, and
+  term by term (the large- and small-state launches, the cash-CSA variant, the side stream) -- against the
+  restated FP32 kernels, netting set by netting set; and a
   few of its netting sets in the FP64 mode against the FP64 engine, every margin call decided the same way.
 - The Bermudan book (10y swaptions, annual exercise, degree 3): the FP64 fit and revaluation against the FP64
   engine's Longstaff-Schwartz on identical normals, every exercise decision the same.
@@ -73,16 +74,23 @@ def book():
     return m, books, o, [gpu.compile(m, b, o) for b in books]
 
 
-def test_correlated_book_in_one_batch_against_the_oracle(ctx, book):
+@pytest.mark.parametrize("basis", [gpu.Context.BASIS_AUTO, gpu.Context.BASIS_OFF])
+def test_correlated_book_in_one_batch_against_the_oracle(ctx, book, basis):
+    """With the basis kernel (the default: the 100 netting sets as one tensor-core group) and term by term."""
     m, books, o, plans = book
     assert len(plans) == 100
-    got = ctx.run_many(plans)
-    b = ctx.batch(plans)
+    ctx.set_basis(basis)
     try:
-        info = b.info()
+        got = ctx.run_many(plans)
+        b = ctx.batch(plans)
+        try:
+            info = b.info()
+        finally:
+            b.close()
     finally:
-        b.close()
+        ctx.set_basis(gpu.Context.BASIS_AUTO)
     assert info.num_launch_groups == 1  # one shared simulation for the 100 netting sets
+    assert info.num_basis_netting_sets == (100 if basis == gpu.Context.BASIS_AUTO else 0)
     for i, (p, (sg, vg)) in enumerate(zip(plans, got)):
         sr, vr = restated.run_plan(p)
         try:

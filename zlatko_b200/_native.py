@@ -59,11 +59,12 @@ class OutputF64(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("num_plans", "num_launch_groups", "num_paths", "num_dates", "num_trades_hint",
                                           "num_terms", "term_evaluations", "exp_evaluations", "table_bytes", "row_bytes",
-                                          "kernels_per_execute", "tile_paths", "graph_replay", "num_waves")]
+                                          "kernels_per_execute", "tile_paths", "graph_replay", "num_waves",
+                                          "num_basis_netting_sets")]
 
 
 # Every entry point declared in include/zlatko_b200.h.
-EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream", "zk_context_set_row_budget",
+EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream", "zk_context_set_row_budget", "zk_context_set_basis", "zk_debug_basis",
            "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc", "zk_debug_inject",
            "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
            "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
@@ -93,6 +94,7 @@ def lib() -> C.CDLL:
         "zk_last_error": (C.c_char_p, [vp]),
         "zk_context_set_stream": (st, [vp, vp]),
         "zk_context_set_row_budget": (st, [vp, C.c_uint64]),
+        "zk_context_set_basis": (st, [vp, C.c_uint32]),
         "zk_run_plan": (st, [vp, P(PlanView), P(Output)]),
         "zk_run_plans": (st, [vp, P(PlanView), sz, P(Output)]),
         "zk_amc_states": (st, [vp, P(PlanView), vp, vp, vp, sz]),
@@ -113,6 +115,7 @@ def lib() -> C.CDLL:
         "zk_run_plan_injected": (st, [vp, P(PlanView), vp, sz, P(Output), vp]),
         "zk_run_plan_noalloc": (st, [C.c_int, vp, P(PlanView), P(Output), C.c_char_p, sz]),
         "zk_debug_inject": (st, [vp, C.c_uint32, C.c_uint64]),
+        "zk_debug_basis": (st, [P(PlanView), sz, vp, vp, vp, vp, C.c_char_p, sz]),
         "zk_batch_create": (st, [vp, P(PlanView), sz, P(vp)]),
         "zk_batch_execute": (st, [vp]),
         "zk_batch_set_tile_paths": (st, [vp, C.c_uint64]),

@@ -19,9 +19,9 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libzlatko_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["fused_exposure.cu", "row_stats.cu", "nested_inner.cu", "amc_fit.cu", "mlp.cu", "surrogate.cu", "capi.cu", "peaks.cu"]
-CPP_SOURCES = ["plan_compiler.cpp", "hermite_proxy.cpp"]
-HEADERS = ["zk_device.cuh", "zk_kernels.h", "plan_compiler.h", "umma.cuh", "surrogate.cuh"]
+CU_SOURCES = ["fused_exposure.cu", "basis_revalue.cu", "row_stats.cu", "nested_inner.cu", "amc_fit.cu", "mlp.cu", "surrogate.cu", "capi.cu", "peaks.cu"]
+CPP_SOURCES = ["plan_compiler.cpp", "hermite_proxy.cpp", "basis_plan.cpp"]
+HEADERS = ["zk_device.cuh", "zk_kernels.h", "plan_compiler.h", "umma.cuh", "surrogate.cuh", "basis.cuh", "basis_plan.h"]
 
 
 def _sources():

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/zlatko_b200.h"
+#include "basis.cuh"
 #include "plan_compiler.h"
 #include "surrogate.cuh"
 #include "zk_kernels.h"
@@ -127,6 +128,9 @@ struct zk_context {
   // Device bytes a batch may give to per-path rows and warp partials at once (zk_context_set_row_budget); 0: all
   // of its netting sets at once while that takes under 70% of the free device memory, else waves in 60% of it.
   uint64_t rowBudget = 0;
+  // Which netting sets run on the tensor-core basis kernel (zk_context_set_basis): 0 groups of at least
+  // kBasisMinNs eligible netting sets, 1 none, 2 every eligible netting set.
+  uint32_t basisMode = 0;
 };
 
 namespace {
@@ -518,6 +522,16 @@ struct Batch {
       size_t first = 0, count = 0, reduceFirst = 0, rowFirst = 0, rowCount = 0;
     };
     std::vector<Wave> waves;
+    // Single precision: planIdx[0, basisCount) run on basisRevalueKernel in groups of at most 128 netting sets
+    // (planIdx[first, first + count) each, its tables and arguments in the input region); the rest on
+    // revalueKernel, in decreasing order of shared-memory state.
+    struct Group {
+      size_t first = 0, count = 0;
+      BasisImage img;
+      size_t dates = 0, kgs = 0, options = 0, fixings = 0, chunks = 0, blob = 0, scale = 0;
+    };
+    size_t basisCount = 0, groupArgs = 0;  // groupArgs: index of the first group's BasisArgs in the batch's array
+    std::vector<Group> groups;
   };
   std::vector<Launch> launches;
   // device offsets per plan
@@ -527,6 +541,8 @@ struct Batch {
   };
   std::vector<Dev> dev;
   size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
+  size_t basisArgsOff = 0, numGroups = 0;  // BasisArgs of every launch's groups
+  std::vector<uint8_t> onBasis;          // per plan: runs on the basis kernel (its partials have one path per lane)
   size_t inputBytes = 0, totalBytes = 0, outBegin = 0, outBytes = 0;
   uint32_t numRowJobs = 0, maxReduceN = 0;
   int ppt = 2;                        // paths per revalue thread: the tile shape (autotuned by zk_batch_create)
@@ -587,6 +603,79 @@ void parseAll(const std::vector<View<R>>& views, std::vector<Plan<R>>& plans, Ho
     if (e) std::rethrow_exception(e);
 }
 
+// Netting sets in a group of fewer run faster term by term (the group's epilogue warps work on 128 lanes).
+constexpr size_t kBasisMinNs = 24;
+
+// A plan the basis kernel runs: single precision, the netting set's 8 statistics, the exposure rows only, no AMC,
+// probes, per-trade views or nested margin, and no CSA or a cash CSA with a look-back of at most one date (term
+// kinds are checked by buildBasis).
+template <typename R>
+bool basisEligible(const Plan<R>& P) {
+  return sizeof(R) == 4 && P.nTr == 0 && !P.amcOrProbe && !P.im && P.nBerm == 0 && P.nS == static_cast<uint32_t>(kStatsPerDate) &&
+         P.rowGross == kNoRow && P.rowTrades == kNoRow && P.rowDV == kNoRow && P.rowE == kNoRow && P.rowV == kNoRow &&
+         P.rowC == kNoRow && (!P.hasCsa || (P.ctype == 0 && P.ring <= 2)) && P.nC <= 2 && P.nF <= 2;
+}
+
+// Reorders a launch's plans into [basis groups | the rest]: eligible netting sets with the same margin-call and
+// reporting dates, in near-equal groups of at most 128 (mode 0: of at least kBasisMinNs), each lowered by
+// buildBasis on the context's host threads; a group that does not lower joins the rest.
+template <typename R>
+void formGroups(Batch<R>& B, typename Batch<R>::Launch& L, uint32_t mode, HostPool* pool) {
+  if constexpr (sizeof(R) == 4) {
+    if (mode == 1 || B.sink) return;
+    std::vector<uint32_t> E, O;
+    for (uint32_t k : L.planIdx) (basisEligible(B.plans[k]) ? E : O).push_back(k);
+    if (E.empty()) return;
+    auto tables = [&](uint32_t k) {
+      const auto& P = B.plans[k];
+      return std::vector<uint32_t>(P.v.indices + P.offCall, P.v.indices + P.offCall + 2 * static_cast<size_t>(P.nT));
+    };
+    std::vector<std::vector<uint32_t>> key(B.plans.size());
+    for (uint32_t k : E) key[k] = tables(k);
+    std::stable_sort(E.begin(), E.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    ParallelFor par = nullptr;
+    if (pool && pool->workers() > 1)
+      par = [pool](size_t n, const std::function<void(size_t)>& fn) {
+        const size_t w = std::min(pool->workers(), n);
+        pool->run(w, [&](size_t t) {
+          for (size_t i = t; i < n; i += w) fn(i);
+        });
+      };
+    std::vector<uint32_t> ordered;
+    for (size_t i = 0; i < E.size();) {
+      size_t e = i + 1;
+      while (e < E.size() && key[E[e]] == key[E[i]]) ++e;
+      const size_t run = e - i, parts = (run + kBasisRows - 1) / kBasisRows;
+      for (size_t q = 0; q < parts; ++q) {
+        const size_t a = i + run * q / parts, b = i + run * (q + 1) / parts;
+        typename Batch<R>::Launch::Group G;
+        std::string why;
+        bool ok = mode == 2 || b - a >= kBasisMinNs;
+        if (ok) {
+          std::vector<BasisPlanIn> in;
+          for (size_t k = a; k < b; ++k) {
+            const auto& P = B.plans[E[k]];
+            in.push_back({P.v.terms, P.v.indices, P.nT, static_cast<uint32_t>(P.nTerms), P.offCall, P.offRep});
+          }
+          ok = buildBasis(in, G.img, why, par);
+        }
+        if (!ok) {
+          O.insert(O.end(), E.begin() + a, E.begin() + b);
+          continue;
+        }
+        G.first = ordered.size(), G.count = b - a;
+        ordered.insert(ordered.end(), E.begin() + a, E.begin() + b);
+        L.groups.push_back(std::move(G));
+      }
+      i = e;
+    }
+    L.basisCount = ordered.size();
+    for (size_t k = 0; k < L.basisCount; ++k) B.onBasis[ordered[k]] = 1;
+    ordered.insert(ordered.end(), O.begin(), O.end());
+    L.planIdx = std::move(ordered);
+  }
+}
+
 template <typename R>
 std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams) {
   auto B = std::make_unique<Batch<R>>();
@@ -608,21 +697,26 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   }
   if (normals && B->launches.size() != 1) throw fail(ZK_ERR_INVALID_ARGUMENT, "injected normals need plans of one scenario");
   // ---- per launch: the factor cube shared by its netting sets, one CTA column per netting set ----
+  B->onBasis.assign(nPlans, 0);
   for (auto& L : B->launches) {
-    std::stable_sort(L.planIdx.begin(), L.planIdx.end(),
+    formGroups(*B, L, ctx ? ctx->basisMode : 1u, hostPool(ctx, views.size()));
+    const size_t nb = L.basisCount;
+    std::stable_sort(L.planIdx.begin() + static_cast<std::ptrdiff_t>(nb), L.planIdx.end(),
                      [&](uint32_t a, uint32_t b) { return B->plans[a].stateWords > B->plans[b].stateWords; });
     L.splitAt = L.planIdx.size();
-    while (L.splitAt > 0 && B->plans[L.planIdx[L.splitAt - 1]].stateWords <= static_cast<uint32_t>(kSmallStateWords)) --L.splitAt;
+    while (L.splitAt > nb && B->plans[L.planIdx[L.splitAt - 1]].stateWords <= static_cast<uint32_t>(kSmallStateWords)) --L.splitAt;
     if (L.splitAt < L.planIdx.size()) L.smallStateMax = B->plans[L.planIdx[L.splitAt]].stateWords;
-    for (size_t k = 0; k < L.planIdx.size(); ++k) {
+    for (size_t k = nb; k < L.planIdx.size(); ++k) {
       const auto& P = B->plans[L.planIdx[k]];
       const bool cash = P.hasCsa && P.ctype == 0 && P.ring <= 2 && P.rowDV == kNoRow && P.rowE == kNoRow && P.rowV == kNoRow &&
                         P.rowC == kNoRow;
       (k < L.splitAt ? L.cashBig : L.cashSmall) = (k < L.splitAt ? L.cashBig : L.cashSmall) && cash;
       L.cashAll = L.cashAll && cash;
     }
-    for (uint32_t k : L.planIdx) {
-      const auto& P = B->plans[k];
+    for (size_t q = 0; q < L.planIdx.size(); ++q) {
+      const auto& P = B->plans[L.planIdx[q]];
+      L.probes = L.probes || P.probes;
+      if (q < nb) continue;  // the rest: the term-by-term kernel's variant and shared memory
       L.stateWordsMax = std::max<size_t>(L.stateWordsMax, P.stateWords);
       L.perTrade = L.perTrade || P.nTr > 0;
       L.probes = L.probes || P.probes;
@@ -670,6 +764,20 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     }
   }
   for (auto& L : B->launches) L.nsOff = take(L.planIdx.size() * sizeof(NsArgs<R>));
+  for (auto& L : B->launches) {
+    L.groupArgs = B->numGroups;
+    B->numGroups += L.groups.size();
+    for (auto& G : L.groups) {
+      G.dates = take(G.img.dates.size() * 4);
+      G.kgs = take(G.img.kgs.size() * sizeof(BasisKg));
+      G.options = take(G.img.options.size() * 4);
+      G.fixings = take(G.img.fixings.size() * 4);
+      G.chunks = take(G.img.chunks.size() * 4);
+      G.blob = take(G.img.blob.size() * 2);
+      G.scale = take(G.img.scale.size() * 4);
+    }
+  }
+  B->basisArgsOff = take(B->numGroups * sizeof(BasisArgs));
   B->reduceOff = take(nPlans * sizeof(ReduceJob<R>));
   for (const auto& P : B->plans) B->numRowJobs += static_cast<uint32_t>(P.nReq);
   B->rowOff = take(B->numRowJobs * sizeof(RowJob<R>));
@@ -721,17 +829,25 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     size_t regionBytes = 0, jobs = 0, rowJobs = 0;
     for (auto& L : B->launches) {
       size_t k = 0;
+      size_t gi = 0;  // the next basis group: a group runs in one wave
       while (k < L.planIdx.size()) {
         typename Batch<R>::Launch::Wave w;
         w.first = k, w.reduceFirst = jobs, w.rowFirst = rowJobs;
         size_t used = 0;
-        while (k < L.planIdx.size() && (k == w.first || used + rowsBytes(B->plans[L.planIdx[k]]) <= budget)) {
-          const uint32_t i = L.planIdx[k];
-          size_t at = region + used;
-          placeRows(i, [&](size_t bytes) { const size_t o = at; at = alignUp(at + std::max<size_t>(bytes, 16)); return o; });
-          used += rowsBytes(B->plans[i]);
-          B->jobOrder.push_back(i);
-          w.rowCount += B->plans[i].nReq, ++jobs, ++k;
+        while (k < L.planIdx.size()) {
+          const size_t end = k < L.basisCount ? L.groups[gi].first + L.groups[gi].count : k + 1;
+          size_t unitBytes = 0;
+          for (size_t q = k; q < end; ++q) unitBytes += rowsBytes(B->plans[L.planIdx[q]]);
+          if (k != w.first && used + unitBytes > budget) break;
+          for (; k < end; ++k) {
+            const uint32_t i = L.planIdx[k];
+            size_t at = region + used;
+            placeRows(i, [&](size_t bytes) { const size_t o = at; at = alignUp(at + std::max<size_t>(bytes, 16)); return o; });
+            used += rowsBytes(B->plans[i]);
+            B->jobOrder.push_back(i);
+            w.rowCount += B->plans[i].nReq, ++jobs;
+          }
+          if (end <= L.basisCount) ++gi;
         }
         w.count = k - w.first;
         rowJobs += w.rowCount;
@@ -843,6 +959,33 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
       }
     }
     std::memcpy(img + L.nsOff, args.data(), args.size() * sizeof(NsArgs<R>));
+    if constexpr (sizeof(R) == 4) {
+      for (size_t q = 0; q < L.groups.size(); ++q) {
+        const auto& G = L.groups[q];
+        const BasisImage& I = G.img;
+        std::memcpy(img + G.dates, I.dates.data(), I.dates.size() * 4);
+        std::memcpy(img + G.kgs, I.kgs.data(), I.kgs.size() * sizeof(BasisKg));
+        if (!I.options.empty()) std::memcpy(img + G.options, I.options.data(), I.options.size() * 4);
+        if (!I.fixings.empty()) std::memcpy(img + G.fixings, I.fixings.data(), I.fixings.size() * 4);
+        if (!I.chunks.empty()) std::memcpy(img + G.chunks, I.chunks.data(), I.chunks.size() * 4);
+        if (!I.blob.empty()) std::memcpy(img + G.blob, I.blob.data(), I.blob.size() * 2);
+        std::memcpy(img + G.scale, I.scale.data(), I.scale.size() * 4);
+        BasisArgs a{};
+        a.cube = static_cast<const float*>(dptr(L.cubeOff));
+        a.nP = L.sc.nP, a.nT = L.sc.nT, a.nA = L.cb.nA, a.nC = L.cb.nC, a.nF = L.cb.nF;
+        a.fS = L.cb.fS, a.fQ = L.cb.fQ, a.fXf = L.cb.fXf;
+        a.dates = static_cast<const uint32_t*>(dptr(G.dates));
+        a.kgs = static_cast<const BasisKg*>(dptr(G.kgs));
+        a.options = static_cast<const float*>(dptr(G.options));
+        a.fixings = static_cast<const float4*>(dptr(G.fixings));
+        a.chunks = static_cast<const uint32_t*>(dptr(G.chunks));
+        a.blob = static_cast<const unsigned char*>(dptr(G.blob));
+        a.scale = static_cast<const float*>(dptr(G.scale));
+        a.ns = reinterpret_cast<const NsArgs<float>*>(dptr(L.nsOff)) + G.first;
+        a.numNs = static_cast<uint32_t>(G.count), a.numFixSlots = I.numFixSlots, a.numChunks = I.numChunks;
+        std::memcpy(img + B.basisArgsOff + (L.groupArgs + q) * sizeof(BasisArgs), &a, sizeof a);
+      }
+    }
     const auto& P0 = B.plans[L.planIdx.front()];
     L.sc.steps = static_cast<const R*>(dptr(B.dev[L.planIdx.front()].steps));
     L.sc.normals = normals ? static_cast<const R*>(dptr(B.normalsOff)) : nullptr;
@@ -857,7 +1000,9 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
     const size_t i = B.jobOrder[o];  // plan order, or wave by wave when the batch runs in waves
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    red[o] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP, 0};
+    // pad: 1 for a basis plan (one path per lane in its partials), 0 for the batch's tile shape
+    red[o] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP,
+              B.onBasis[i] ? 1u : 0u};
     B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
     for (size_t q = 0; q < P.nReq; ++q)
       rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),
@@ -939,6 +1084,21 @@ template <typename R>
 void launchRevalues(const Batch<R>& B, const typename Batch<R>::Launch& L, uintptr_t base, cudaStream_t s, cudaStream_t side,
                     cudaEvent_t forkEv, cudaEvent_t joinEv, size_t first = 0, size_t count = SIZE_MAX) {
   count = std::min(count, L.planIdx.size() - first);
+  if constexpr (sizeof(R) == 4) {
+    // the basis groups of [first, first + count) (whole groups: waves never split one), as one launch
+    if (first < L.basisCount && count > 0) {
+      const size_t last = std::min(first + count, L.basisCount);
+      size_t g0 = 0;
+      while (g0 < L.groups.size() && L.groups[g0].first < first) ++g0;
+      size_t g1 = g0;
+      while (g1 < L.groups.size() && L.groups[g1].first + L.groups[g1].count <= last) ++g1;
+      injectPoint(B.ctx);
+      ZK_CUDA(launchBasisRevalue(reinterpret_cast<const BasisArgs*>(base + B.basisArgsOff) + L.groupArgs + g0,
+                                 static_cast<uint32_t>(g1 - g0), L.sc.nP, B.ctx->dErr, s));
+      count -= last - first, first = last;
+    }
+  }
+  if (count == 0) return;
   const auto* ns = reinterpret_cast<const NsArgs<R>*>(base + L.nsOff) + first;
   const uint32_t n = static_cast<uint32_t>(count), tiles = numTilesOf(L.sc.nP, B.ppt);
   const size_t splitAt = std::min(count, L.splitAt > first ? L.splitAt - first : 0);
@@ -987,7 +1147,7 @@ void execute(Batch<R>& B, bool capturing = false) {
   ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   for (auto& L : B.launches) {
     const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < L.planIdx.size();
-    if (split && L.splitAt > 0 && !ctx->side && !capturing) {
+    if (split && L.splitAt > L.basisCount && !ctx->side && !capturing) {
       ZK_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
       ZK_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
@@ -1357,6 +1517,41 @@ zk_status zk_context_set_row_budget(zk_context* ctx, uint64_t bytes) {
   if (!ctx) return ZK_ERR_INVALID_ARGUMENT;
   ctx->rowBudget = bytes;
   return ZK_OK;
+}
+
+zk_status zk_context_set_basis(zk_context* ctx, uint32_t mode) {
+  if (!ctx || mode > ZK_BASIS_ALL) return ZK_ERR_INVALID_ARGUMENT;
+  ctx->basisMode = mode;
+  return ZK_OK;
+}
+
+zk_status zk_debug_basis(const zk_plan_view* plans, size_t n, const double* x, const double* S, const double* xf,
+                         double* out, char* err, size_t err_len) {
+  auto say = [&](const char* m) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", m);
+  };
+  try {
+    if (!plans || n == 0 || !x || !S || !xf || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<Plan<float>> P(n);
+    std::vector<BasisPlanIn> in;
+    for (size_t i = 0; i < n; ++i) {
+      P[i] = parse(viewOf(plans[i]), i);
+      in.push_back({P[i].v.terms, P[i].v.indices, P[i].nT, static_cast<uint32_t>(P[i].nTerms), P[i].offCall, P[i].offRep});
+    }
+    BasisImage img;
+    std::string why;
+    if (!buildBasis(in, img, why)) throw fail(ZK_ERR_UNSUPPORTED, "%s", why.c_str());
+    out[0] = basisCheck(in, img, x, S, xf);
+    out[1] = static_cast<double>(img.columns), out[2] = static_cast<double>(img.linearTerms);
+    out[3] = img.numFixSlots, out[4] = img.numChunks;
+    return ZK_OK;
+  } catch (const Failure& f) {
+    say(f.message.c_str());
+    return f.status;
+  } catch (const std::exception& e) {
+    say(e.what());
+    return ZK_ERR_INVALID_ARGUMENT;
+  }
 }
 
 zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_output* outs) {
@@ -1786,7 +1981,11 @@ zk_status zk_batch_execute(zk_batch* b) {
   try {
     ZK_CUDA(cudaSetDevice(b->b->ctx->device));
     if (!b->tuned) {
-      autotune(*b->b);  // first execute: time the tile shapes on this batch, keep the fastest
+      // first execute: time the tile shapes on this batch, keep the fastest (they shape the term-by-term launches
+      // only: a batch entirely on the basis kernel keeps the default)
+      bool termByTerm = false;
+      for (const auto& L : b->b->launches) termByTerm = termByTerm || L.basisCount < L.planIdx.size();
+      if (termByTerm) autotune(*b->b);
       b->tuned = true;
     }
     if (!b->eager && (!b->graph || b->graphPpt != b->b->ppt) && !captureExecute(b)) b->eager = true;
@@ -1860,18 +2059,26 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
     info->row_bytes += static_cast<uint64_t>(P.nR) * P.nP * 4;
   }
   uint64_t kernels = (B.waved ? 0 : 2) + B.im.size();  // reduce, row statistics, one nested-margin launch per margin plan
+  auto revalueLaunches = [&](const Batch<float>::Launch& L, size_t first, size_t count) {  // as launchRevalues
+    count = std::min(count, L.planIdx.size() - first);
+    uint64_t k = 0;
+    if (first < L.basisCount && count > 0) {
+      const size_t last = std::min(first + count, L.basisCount);
+      ++k, count -= last - first, first = last;
+    }
+    if (count == 0) return k;
+    const size_t at = std::min(count, L.splitAt > first ? L.splitAt - first : 0);
+    const bool split = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && at < count;
+    return k + (split && at > 0 ? 2 : 1);
+  };
   for (const auto& L : B.launches) {
-    const bool split = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && L.splitAt < L.planIdx.size();
+    info->num_basis_netting_sets += L.basisCount;
     if (!B.waved) {
-      kernels += 1 + (split && L.splitAt > 0 ? 2 : 1);  // simulate, then one or two revalue launches
+      kernels += 1 + revalueLaunches(L, 0, L.planIdx.size());  // simulate, then the revalue launches
       continue;
     }
-    kernels += 1;  // simulate; per wave one or two revalue launches, a reduce and (with requests) row statistics
-    for (const auto& w : L.waves) {  // as launchRevalues splits a wave
-      const size_t at = std::min(w.count, L.splitAt > w.first ? L.splitAt - w.first : 0);
-      const bool splitW = L.lean && !L.perTrade && !B.sink && B.ppt > 1 && at < w.count;
-      kernels += (splitW && at > 0 ? 2 : 1) + 1 + (w.rowCount ? 1 : 0);
-    }
+    kernels += 1;  // simulate; per wave its revalue launches, a reduce and (with requests) row statistics
+    for (const auto& w : L.waves) kernels += revalueLaunches(L, w.first, w.count) + 1 + (w.rowCount ? 1 : 0);
   }
   info->kernels_per_execute = kernels;
   info->num_waves = 0;

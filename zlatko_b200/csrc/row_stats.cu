@@ -387,14 +387,16 @@ __global__ void reduceKernel(const ReduceJob<R>* __restrict__ jobs) {
   const ReduceJob<R> J = jobs[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= J.n) return;
-  constexpr uint32_t kUnits = 4 / PPT, kUnitPaths = 32 * PPT;
+  // A job with pad 1 has one path per lane whatever the batch's shape (the basis kernel's 32-path units).
+  const uint32_t ppt = J.pad == 1u ? 1u : static_cast<uint32_t>(PPT);
+  const uint32_t kUnits = 4 / ppt, kUnitPaths = 32 * ppt;
   auto unit = [&](uint32_t u) { return u * kUnitPaths < J.nP ? J.partials[static_cast<size_t>(u) * J.n + i] : R(0); };
   double sum = 0.0, comp = 0.0;
   for (uint32_t t = 0; t < J.numTiles; ++t) {
     const uint32_t u0 = t * kUnits;
     R g;
-    if constexpr (PPT == 1) g = (unit(u0) + unit(u0 + 1)) + (unit(u0 + 2) + unit(u0 + 3));
-    else if constexpr (PPT == 2) g = unit(u0) + unit(u0 + 1);
+    if (ppt == 1) g = (unit(u0) + unit(u0 + 1)) + (unit(u0 + 2) + unit(u0 + 3));
+    else if (ppt == 2) g = unit(u0) + unit(u0 + 1);
     else g = unit(u0);
     const double yv = static_cast<double>(g) - comp;
     const double tv = sum + yv;

@@ -45,6 +45,13 @@ __host__ __device__ constexpr uint32_t idescBf16(uint32_t M, uint32_t N) {
          | ((M >> 4) << 24);  // M / 16
 }
 
+// Instruction descriptor of kind::f16 with FP16 A and B (both K-major), FP32 accumulator, M x N.
+__host__ __device__ constexpr uint32_t idescF16(uint32_t M, uint32_t N) {
+  return (1u << 4)            // D format F32
+         | ((N >> 3) << 17)   // N / 8; A and B format 0: F16
+         | ((M >> 4) << 24);  // M / 16
+}
+
 // D[tmem] (+)= A[desc] * B[desc]^T, issued by the calling thread.
 __device__ __forceinline__ void mma(uint32_t tmemD, uint64_t da, uint64_t db, uint32_t idesc, bool accumulate) {
   const uint32_t acc = accumulate ? 1u : 0u, z = 0u;
@@ -103,6 +110,36 @@ __device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Four runs of 8 consecutive 32-bit columns of this thread's TMEM lane (at a0..a3) and the wait for them, in one
+// statement, so that no use of the registers can be scheduled before the wait.
+__device__ __forceinline__ void ld8x4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8, %9, %10, %11, %12, %13, %14, %15}, [%33];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16, %17, %18, %19, %20, %21, %22, %23}, [%34];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%24, %25, %26, %27, %28, %29, %30, %31}, [%35];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3)
+      : "memory");
+}
+// Three runs of 8 consecutive 32-bit columns of this thread's TMEM lane (at a0..a2) from registers, and the wait
+// for the stores, in one statement (the registers may be reused as soon as it returns).
+__device__ __forceinline__ void st8x3(uint32_t a0, uint32_t a1, uint32_t a2, const uint32_t (&r)[24]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%3, %4, %5, %6, %7, %8, %9, %10};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%11, %12, %13, %14, %15, %16, %17, %18};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%2], {%19, %20, %21, %22, %23, %24, %25, %26};\n\t"
+      "tcgen05.wait::st.sync.aligned;" ::"r"(a0),
+      "r"(a1), "r"(a2), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+      "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]),
+      "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23])
+      : "memory");
 }
 
 // 16-byte asynchronous global -> shared copy (LDGSTS) and its completion.

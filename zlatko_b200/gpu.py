@@ -294,6 +294,13 @@ class Context:
         beyond it run in waves of netting sets with the same results."""
         check(lib().zk_context_set_row_budget(self.handle, int(nbytes)), self.handle)
 
+    BASIS_AUTO, BASIS_OFF, BASIS_ALL = 0, 1, 2
+
+    def set_basis(self, mode: int) -> None:
+        """zk_context_set_basis: which netting sets run on the tensor-core basis kernel (BASIS_AUTO: groups of at
+        least 24 eligible netting sets; BASIS_OFF: none; BASIS_ALL: every eligible one)."""
+        check(lib().zk_context_set_basis(self.handle, int(mode)), self.handle)
+
     INJECT_FAIL_LAUNCH, INJECT_ROW_ROUNDS = 1, 2
 
     def inject(self, what: int, value: int) -> None:
@@ -392,6 +399,23 @@ class Context:
 
 
 NOALLOC_SCRATCH_BYTES = 32 << 20  # ZK_NOALLOC_SCRATCH_BYTES
+
+
+def basis_check(plans: Sequence[Plan], x: np.ndarray, S: np.ndarray, xf: np.ndarray) -> dict:
+    """zk_debug_basis (host only, no GPU): lowers the plans as one basis group and compares, along one path of
+    factor values x[nT], S[nT][4], xf[nT][2], the group's FP16 hi/lo product with the plans' terms summed one by
+    one (both in double).  Returns the largest difference relative to the gross basis sum, and the counts."""
+    views = (PlanView * len(plans))(*[p.view() for p in plans])
+    x = np.ascontiguousarray(x, np.float64)
+    S = np.ascontiguousarray(S, np.float64)
+    xf = np.ascontiguousarray(xf, np.float64)
+    out = np.zeros(5, np.float64)
+    err = C.create_string_buffer(512)
+    st = lib().zk_debug_basis(views, len(plans), x.ctypes.data, S.ctypes.data, xf.ctypes.data, out.ctypes.data, err, 512)
+    if st != 0:
+        raise RuntimeError(f"zk_debug_basis: status {st}: {err.value.decode()}")
+    return {"rel_err": float(out[0]), "columns": int(out[1]), "linear_terms": int(out[2]), "fixing_slots": int(out[3]),
+            "chunks": int(out[4])}
 
 
 def run_plan_noalloc(plan: Plan, device: int = 0, stream: Optional[int] = None):
