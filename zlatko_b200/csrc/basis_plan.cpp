@@ -379,6 +379,9 @@ bool buildBasis(const std::vector<BasisPlanIn>& plans, BasisImage& out, std::str
     d[bdKgs] = static_cast<uint32_t>(D.kgs.size());
     out.kgs.insert(out.kgs.end(), D.kgs.begin(), D.kgs.end());
     d[bdOpt] = static_cast<uint32_t>(out.options.size() / 8);
+    d[bdOpts] = static_cast<uint32_t>(D.options.size() / 8);
+    if (D.kgs.size() * sizeof(BasisKg) + D.options.size() * 4 > kBasisDescBytes)
+      return why = "a date with more than 16 KB of basis columns and option records", false;
     out.options.insert(out.options.end(), D.options.begin(), D.options.end());
     d[bdChunk] = out.numChunks;
     d[bdChunks] = static_cast<uint32_t>(D.chunkSteps.size());
@@ -390,6 +393,13 @@ bool buildBasis(const std::vector<BasisPlanIn>& plans, BasisImage& out, std::str
     out.blob.insert(out.blob.end(), D.blob.begin(), D.blob.end());
     std::copy(D.scale.begin(), D.scale.end(), out.scale.begin() + static_cast<size_t>(j) * kBasisRows);
     out.linearTerms += D.linearTerms, out.columns += 8ull * D.kgs.size();
+  }
+  uint32_t next = nT;
+  for (uint32_t j = nT; j-- > 0;) {
+    uint32_t* d = &out.dates[static_cast<size_t>(j) * kBasisDateWords];
+    d[bdNextRep] = next;
+    if (d[bdRep] > 0) next = j;
+    d[bdPrevChunks] = j > 0 ? out.dates[static_cast<size_t>(j - 1) * kBasisDateWords + bdChunks] : 0u;
   }
   return true;
 }

@@ -52,10 +52,14 @@ struct BasisKg {
 };
 static_assert(sizeof(BasisKg) == 64, "BasisKg is four 16-byte loads");
 
-// Per date: firstChunk, numChunks, firstKg, numKg, fixBegin, fixEnd, optBegin, callIndex, reportingSlot, 0, 0, 0.
+// Per date: firstChunk, numChunks, firstKg, numKg, fixBegin, fixEnd, optBegin, callIndex, reportingSlot, the next
+// reporting date (nT: none), the previous date's numChunks, the number of option records.
 enum BasisDateWord : int {
   bdChunk = 0, bdChunks = 1, bdKg = 2, bdKgs = 3, bdFixBegin = 4, bdFixEnd = 5, bdOpt = 6, bdCall = 7, bdRep = 8,
+  bdNextRep = 9, bdPrevChunks = 10, bdOpts = 11,
 };
+// A date's k-groups and option records, copied into shared memory a date ahead: at most this many bytes.
+constexpr uint32_t kBasisDescBytes = 16384;
 
 // One netting set of a group: its plan's tables as the reference lays them out.
 struct BasisPlanIn {

@@ -4,24 +4,29 @@
 // The plans' semantics are those of revalueKernel (the reference's fused kernel, src/gpu/fused_kernels.cpp:224-530,
 // for plans whose terms are bonds, floating coupons with their fixings, FX forwards and Black options, under no CSA
 // or a cash CSA whose margin call looks back at most one date).  The work is organised for a B200 instead of term
-// by term:
+// by term, as a pipeline of two warp-specialised halves of the CTA:
 //
-//   1. Basis (CUDA cores).  Four threads per path evaluate the date's basis functions Phi[path][k] (each distinct
-//      bond exponential, fixing x bond, foreign bond x FX rate, FX rate and option price of the group once, however
-//      many netting sets hold it), split each into FP16 hi + lo (lo = the rounding residue of hi), and write them
-//      into shared memory in the K-major layout of the tensor core's B operand, 64 columns per chunk.
-//   2. Product (tensor core).  One thread issues, per chunk, tcgen05.mma kind::f16 C_hi Phi_hi + C_hi Phi_lo +
-//      C_lo Phi_hi into an FP32 accumulator in TMEM: lane = netting set, column = path.  The coefficient chunk
-//      C (128 netting sets x 64 columns, hi and lo) arrives by a bulk copy issued a chunk ahead; the next chunk's
-//      basis is evaluated while the tensor core multiplies this one.
-//   3. Netting set epilogue (CUDA cores).  Thread (netting set r, path block b) takes its 32 paths in order: the
-//      netted value (accumulator x the date's power-of-two scale), the margin call and the collateral, the
-//      exposure row, the CVA increment and the date's 8 statistics summed over the 32 paths -- the partial of the
-//      32-path unit, no shuffles.  The per-(netting set, path) state -- collateral held, the previous value, the
-//      previous discounted positive exposure -- lives in TMEM beside the accumulator (columns 128..511).
+//   Producers (warps 0-7, two threads per path).  Date by date: the path's factors, staged for the consumers
+//   (discount factor, survivals and their CVA differences, and per 32-path unit their sums); the date's basis
+//   functions Phi[path][k] -- each distinct bond exponential, fixing x bond, foreign bond x FX rate, FX rate and
+//   option price of the group once, however many netting sets hold it -- split into FP16 hi + lo (lo = the
+//   rounding residue of hi) in the K-major layout of the tensor core's B operand, 64 columns per chunk.  One
+//   thread issues per chunk tcgen05.mma kind::f16 C_hi Phi_hi + C_hi Phi_lo + C_lo Phi_hi into the date's FP32
+//   accumulator in TMEM (lane = netting set, column = path); the coefficient chunk C (128 netting sets x 64
+//   columns, hi and lo) arrives by a bulk copy issued a chunk ahead.  Then the fixings the date sets.
+//   Consumers (warps 8-15).  Warp (lane quarter q, path half h) takes netting sets 32 q + lane over paths
+//   [64 h, 64 h + 64) in order: the netted value (the accumulator x the date's power-of-two scale), the margin call
+//   on the previous date's value (the previous accumulator, kept: three accumulators rotate) and the collateral
+//   held (TMEM columns 384..511), the exposure row and the date's 8 statistics summed over each 32-path unit --
+//   the unit's partial, no shuffles.  The CVA increment 0.5 (DE' + DE)(Q' - Q) between reporting dates is summed as
+//   0.5 DE (Q - Q_next) on the earlier date (the next survival staged by the producers) plus 0.5 DE (Q' - Q) on
+//   the later one, so no per-path state carries the previous DE.
 //
-// Every wait is bounded: an MMA-completion or bulk-copy barrier that does not complete sets kDevTimeout, every
-// thread leaves at the next barrier, and the TMEM is freed after the work in flight settles.
+// The producers work on date j + 1 while the consumers finish date j.  mbarriers order the halves: a date's
+// staging (stageFull) and products (accFull) before its epilogue; an epilogue (epiDone) before the producers
+// reuse its staging buffer three dates later and its accumulator for the products two dates later.  Every wait
+// is bounded: one that does not complete sets kDevTimeout, the threads leave their loops (each further wait on
+// the other half is bounded too), and the TMEM is freed after the work in flight settles.
 #include <cuda_fp16.h>
 
 #include "basis.cuh"
@@ -30,18 +35,22 @@
 namespace zk {
 namespace {
 
-constexpr uint32_t kThreads = 512;
+constexpr uint32_t kThreads = 512, kProducers = 256;
 constexpr uint32_t kWaitLimit = 1u << 26;               // polls of a barrier before the kernel gives up
 constexpr uint32_t kPhiImage = kBasisPaths * 64 * 2;     // one FP16 image of a basis chunk: 16 KB
 constexpr uint32_t kCoefImage = kBasisRows * 64 * 2;     // one FP16 image of a coefficient chunk: 16 KB
 constexpr uint32_t kOffPhi = 0;                          // [2 buffers][hi, lo]
 constexpr uint32_t kOffCoef = kOffPhi + 4 * kPhiImage;   // [2 buffers][hi, lo]
 constexpr uint32_t kOffFix = kOffCoef + 4 * kCoefImage;  // fixings x 64: [slot][path]
-constexpr uint32_t kOffStage = kOffFix + kBasisMaxFix * kBasisPaths * 4;  // D, Q0, Q1, dQ0, dQ1 per path
-constexpr uint32_t kSmem = kOffStage + 5 * kBasisPaths * 4;
-// TMEM columns: the accumulator [0, 128), then per netting set and path the collateral held, the previous value
-// and the previous discounted positive exposure.
-constexpr uint32_t kColHeld = 128, kColPrev = 256, kColDE = 384;
+// A date's staging: per path D | Q0 Q1 | dQ0 dQ1 (Q' - Q since the previous reporting date) | dQn0 dQn1 (Q - Q at
+// the next reporting date); per 32-path unit the sums of D, Q0, Q1 and the count of live paths.
+constexpr uint32_t kStageFloats = 7 * kBasisPaths + 16;
+constexpr uint32_t kOffStage = kOffFix + kBasisMaxFix * kBasisPaths * 4;  // [3 buffers]
+constexpr uint32_t kOffDesc = kOffStage + 3 * kStageFloats * 4;  // [2 buffers] a date's k-groups, then its options
+constexpr uint32_t kSmem = kOffDesc + 2 * kBasisDescBytes;
+// TMEM columns: the accumulators of three consecutive dates [0, 128), [128, 256), [256, 384); the collateral held
+// per netting set and path [384, 512).
+constexpr uint32_t kColHeld = 384;
 
 struct Factors {
   float x, D, S[4], Q[2], xf[2];
@@ -51,9 +60,9 @@ __device__ __forceinline__ float pick(const float (&a)[4], uint32_t i) {
   return i == 0 ? a[0] : i == 1 ? a[1] : i == 2 ? a[2] : a[3];
 }
 
-// The unscaled Black price of an option record (revalueKernel's kOption / kForeignOption).
+// The unscaled Black price of an option record (revalueKernel's kOption / kForeignOption), read from shared memory.
 __device__ __forceinline__ float optionPrice(const float* rec, bool foreign, const Factors& f) {
-  const float4 r0 = __ldg(reinterpret_cast<const float4*>(rec)), r1 = __ldg(reinterpret_cast<const float4*>(rec) + 1);
+  const float4 r0 = reinterpret_cast<const float4*>(rec)[0], r1 = reinterpret_cast<const float4*>(rec)[1];
   const float b0 = r0.w * fastExp(-r1.x * f.x);
   float F;
   if (!foreign) {
@@ -65,12 +74,13 @@ __device__ __forceinline__ float optionPrice(const float* rec, bool foreign, con
   return black(F, r1.z, fabsf(r1.w), b0, r1.w > 0.0f);
 }
 
-// One k-group of the basis for this thread's path: 8 values of one column type, as FP16 hi and lo.
+// One k-group of the basis for this thread's path: 8 values of one column type, as FP16 hi and lo (the k-group and
+// the option records in shared memory).
 __device__ __forceinline__ void basisGroup(const BasisKg* kg, const float* options, const Factors& f, const float* fixS,
                                            uint32_t row, uint4& hi, uint4& lo) {
-  const float4 b0 = __ldg(reinterpret_cast<const float4*>(kg)), b1 = __ldg(reinterpret_cast<const float4*>(kg) + 1);
-  const uint4 sw = __ldg(reinterpret_cast<const uint4*>(kg) + 2);
-  const uint4 tm = __ldg(reinterpret_cast<const uint4*>(kg) + 3);
+  const float4 b0 = reinterpret_cast<const float4*>(kg)[0], b1 = reinterpret_cast<const float4*>(kg)[1];
+  const uint4 sw = reinterpret_cast<const uint4*>(kg)[2];
+  const uint4 tm = reinterpret_cast<const uint4*>(kg)[3];
   const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
   const uint32_t sel[8] = {sw.x & 0xFFFFu, sw.x >> 16, sw.y & 0xFFFFu, sw.y >> 16,
                            sw.z & 0xFFFFu, sw.z >> 16, sw.w & 0xFFFFu, sw.w >> 16};
@@ -111,229 +121,313 @@ __device__ __forceinline__ void basisGroup(const BasisKg* kg, const float* optio
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Producers' barrier (named barrier 1, the 256 producer threads), and-reducing a predicate.
+__device__ __forceinline__ bool producersAnd(bool v) {
+  uint32_t r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 256, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+               : "=r"(r)
+               : "r"(v ? 1u : 0u)
+               : "memory");
+  return r != 0;
+}
+
 __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArgs* __restrict__ groups, uint32_t* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ BasisArgs G;
-  __shared__ __align__(8) uint64_t mmaBar[2], loadBar[2];
+  __shared__ __align__(8) uint64_t loadBar[2], mmaBar[2], descBar[2], accFull[3], stageFull[3], epiDone[3];
   __shared__ uint32_t tslot;
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, row = tid & 127u;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   if (warp == 0) umma::alloc(&tslot, 512);  // one CTA per SM (its shared memory): the whole TMEM is free
   if (tid == 0) {
     G = groups[blockIdx.y];
-    mbarInit(&mmaBar[0], 1), mbarInit(&mmaBar[1], 1), mbarInit(&loadBar[0], 1), mbarInit(&loadBar[1], 1);
+    for (int b = 0; b < 2; ++b) mbarInit(&loadBar[b], 1), mbarInit(&mmaBar[b], 1), mbarInit(&descBar[b], 1);
+    for (int b = 0; b < 3; ++b) mbarInit(&accFull[b], 1), mbarInit(&stageFull[b], 1), mbarInit(&epiDone[b], 8);
   }
   umma::fenceBeforeSync();
   __syncthreads();
   umma::fenceAfterSync();
   const uint32_t nP = G.nP, nT = G.nT, tile = blockIdx.x;
   float* fixS = reinterpret_cast<float*>(sm + kOffFix);
-  float* stage = reinterpret_cast<float*>(sm + kOffStage);  // [D | Q0 | Q1 | dQ0 | dQ1][128]
-
-  // ---- the basis side: this thread's path (row) ----
-  const uint32_t path = tile * kBasisPaths + row, pp = path < nP ? path : nP - 1;
+  float* stageAll = reinterpret_cast<float*>(sm + kOffStage);
   const size_t fs = static_cast<size_t>(nT) * nP;
-  const float* cubeP = G.cube + pp;
-  auto loadFactors = [&](uint32_t j, Factors& f) {
-    const float* c = cubeP + static_cast<size_t>(j) * nP;
-    f.x = __ldg(c), f.D = __ldg(c + fs);
-#pragma unroll
-    for (uint32_t a = 0; a < 4; ++a) f.S[a] = a < G.nA ? __ldg(c + (G.fS + a) * fs) : 0.0f;
-#pragma unroll
-    for (uint32_t q = 0; q < 2; ++q) f.Q[q] = q < G.nC ? __ldg(c + (G.fQ + q) * fs) : 1.0f;
-#pragma unroll
-    for (uint32_t a = 0; a < 2; ++a) f.xf[a] = a < G.nF ? __ldg(c + (G.fXf + a) * fs) : 0.0f;
-  };
-  float prevQ[2] = {1.0f, 1.0f};
-
-  // ---- the netting-set side: TMEM lane = netting set `row`, paths [32 wg, 32 wg + 32) of the tile ----
-  const uint32_t nsRow = row, pb = wg;
-  const bool nsLive = nsRow < G.numNs;
-  const uint32_t taddr = tslot + ((32u * (warp & 3u)) << 16) + pb * 32u;
-  uint32_t hasCsa = 0, cpty = 0xFFFFFFFFu;
-  float hc = 0.0f, hb = 0.0f, mta = 0.0f, ia = 0.0f;
-  float* rowEP = nullptr;
-  float* partials = nullptr;
-  if (nsLive) {
-    const NsArgs<float>& A = G.ns[nsRow];
-    hasCsa = A.hasCsa, cpty = A.cpty, hc = A.hc, hb = A.hb, mta = A.mta, ia = A.ia;
-    rowEP = A.expo + static_cast<size_t>(A.rowEP) * nP;
-    partials = A.partials;
-  }
-  __syncwarp();  // the TMEM accesses below are warp-collective
-  {
-    uint32_t z[24];
-#pragma unroll
-    for (int i = 0; i < 24; ++i) z[i] = 0u;
-#pragma unroll
-    for (uint32_t q = 0; q < 32; q += 8) umma::st8x3(taddr + kColHeld + q, taddr + kColPrev + q, taddr + kColDE + q, z);
-  }
-  const uint32_t blockFirst = tile * kBasisPaths + pb * 32u;
-  const uint32_t blockPaths = blockFirst < nP ? min(32u, nP - blockFirst) : 0u;
-  const uint32_t unit = tile * 4u + pb;
-  const bool vecRows = nP % 4u == 0u;
-
-  constexpr uint32_t idesc = umma::idescF16(kBasisRows, kBasisPaths);
-  uint32_t g = 0;              // chunks started (all dates)
-  int issued = -1, loaded = -1, consumed = -1;  // thread 0: the last chunk whose MMAs / bulk copy were issued / waited
   bool ok = true;
-  if (tid == 0 && G.numChunks > 0) {
-    const uint32_t bytes = G.chunks[1] * 8192u;
-    mbarExpectTx(&loadBar[0], bytes);
-    bulkLoad(sm + kOffCoef, G.blob + G.chunks[0], bytes, &loadBar[0]);
-    loaded = 0;
-  }
-  Factors nf;
-  loadFactors(0, nf);
-  umma::fenceBeforeSync();
-  __syncthreads();
 
-  for (uint32_t j = 0; j < nT && ok; ++j) {
-    const uint32_t* dj = G.dates + static_cast<size_t>(j) * kBasisDateWords;
-    const uint4 d0 = __ldg(reinterpret_cast<const uint4*>(dj)), d1 = __ldg(reinterpret_cast<const uint4*>(dj) + 1);
-    const uint32_t firstChunk = d0.x, numChunks = d0.y, firstKg = d0.z;
-    const uint32_t fixBegin = d1.x, fixEnd = d1.y, optBegin = d1.z, callJ = d1.w, rs = __ldg(dj + bdRep);
-    const Factors f = nf;
-    if (j + 1 < nT) loadFactors(j + 1, nf);
-    if (wg == 0) {  // the path's discount factor and survivals for the epilogue threads
-      stage[row] = f.D;
+  if (tid < kProducers) {
+    // ================================ producers ================================
+    const uint32_t row = tid & 127u, half = tid >> 7;
+    const uint32_t path = tile * kBasisPaths + row, pp = path < nP ? path : nP - 1;
+    const bool live = path < nP;
+    const float* cubeP = G.cube + pp;
+    // A date's record: (firstChunk, numChunks, firstKg, numKg), (fixBegin, fixEnd, optBegin, callIndex),
+    // (reportingSlot, nextReporting, prevChunks, numOptions).
+    auto loadDate = [&](uint32_t j, uint4 (&d)[3]) {
+      const uint4* dj = reinterpret_cast<const uint4*>(G.dates + static_cast<size_t>(j) * kBasisDateWords);
+      d[0] = __ldg(dj), d[1] = __ldg(dj + 1), d[2] = __ldg(dj + 2);
+    };
+    // The factors of date j, and on a reporting date the survivals at the next reporting date.
+    auto loadFactors = [&](uint32_t j, const uint4 (&d)[3], Factors& f, float (&qn)[2]) {
+      const float* c = cubeP + static_cast<size_t>(j) * nP;
+      f.x = __ldg(c), f.D = __ldg(c + fs);
 #pragma unroll
-      for (uint32_t q = 0; q < 2; ++q) {
-        stage[(1 + q) * kBasisPaths + row] = f.Q[q];
-        stage[(3 + q) * kBasisPaths + row] = j > 0 && rs > 0 ? prevQ[q] - f.Q[q] : 0.0f;
-        if (rs > 0) prevQ[q] = f.Q[q];
+      for (uint32_t a = 0; a < 4; ++a) f.S[a] = a < G.nA ? __ldg(c + (G.fS + a) * fs) : 0.0f;
+#pragma unroll
+      for (uint32_t q = 0; q < 2; ++q) f.Q[q] = q < G.nC ? __ldg(c + (G.fQ + q) * fs) : 1.0f;
+#pragma unroll
+      for (uint32_t a = 0; a < 2; ++a) f.xf[a] = a < G.nF ? __ldg(c + (G.fXf + a) * fs) : 0.0f;
+      const uint32_t rs = d[2].x, nextRep = d[2].y;
+#pragma unroll
+      for (uint32_t q = 0; q < 2; ++q)
+        qn[q] = rs > 0 && nextRep < nT && q < G.nC ? __ldg(cubeP + (G.fQ + q) * fs + static_cast<size_t>(nextRep) * nP)
+                                                   : f.Q[q];
+    };
+    // Thread 0: the k-groups and option records of date j into descriptor buffer j % 2 (issued a date ahead).
+    auto loadDesc = [&](const uint4 (&d)[3], uint32_t j) {
+      const uint32_t kgBytes = d[0].w * static_cast<uint32_t>(sizeof(BasisKg)), optBytes = d[2].w * 32u;
+      unsigned char* dst = sm + kOffDesc + (j & 1u) * kBasisDescBytes;
+      if (kgBytes + optBytes == 0) {
+        mbarArrive(&descBar[j & 1u]);
+        return;
       }
-    }
-    // ---- basis chunks and their products ----
-    for (uint32_t c = 0; c < numChunks; ++c, ++g) {
-      const uint32_t buf = g & 1u;
-      if (g >= 2) ok = mbarWait(&mmaBar[buf], ((g - 2) >> 1) & 1u, kWaitLimit) && ok;  // chunk g - 2 released both buffers
-      const uint32_t kgs = 2u * __ldg(G.chunks + 2 * (firstChunk + c) + 1);
-      unsigned char* phiHi = sm + kOffPhi + buf * 2 * kPhiImage;
+      mbarExpectTx(&descBar[j & 1u], kgBytes + optBytes);
+      if (kgBytes) bulkLoad(dst, G.kgs + d[0].z, kgBytes, &descBar[j & 1u]);
+      if (optBytes) bulkLoad(dst + kgBytes, G.options + 8 * static_cast<size_t>(d[1].z), optBytes, &descBar[j & 1u]);
+    };
+    float prevQ[2] = {1.0f, 1.0f};
+    uint32_t g = 0;                               // chunks started (all dates)
+    int issued = -1, loaded = -1, consumed = -1;  // thread 0: the last chunk whose MMAs / copy were issued / waited
+    int descIssued = -1;                          // thread 0: the last date whose descriptors were requested
+    uint4 nd[3];
+    loadDate(0, nd);
+    Factors nf;
+    float nqn[2];
+    loadFactors(0, nd, nf, nqn);
+    if (tid == 0) loadDesc(nd, 0), descIssued = 0;
+    for (uint32_t j = 0; j < nT; ++j) {
+      const uint4 d0 = nd[0], d1 = nd[1], d2 = nd[2];
+      const uint32_t numChunks = d0.y, numKg = d0.w;
+      const uint32_t fixBegin = d1.x, fixEnd = d1.y, rs = d2.x;
+      const Factors f = nf;
+      const float qn[2] = {nqn[0], nqn[1]};
+      if (j + 1 < nT) {
+        loadDate(j + 1, nd);
+        loadFactors(j + 1, nd, nf, nqn);
+        // descriptor buffer (j + 1) % 2 held date j - 1's, which every producer finished (the last barrier)
+        if (tid == 0) loadDesc(nd, j + 1), descIssued = static_cast<int>(j + 1);
+      }
+      // the staging buffer of date j was last read by the epilogue of date j - 3
+      if (j >= 3) ok = mbarWait(&epiDone[j % 3], ((j - 3) / 3) & 1u, kWaitLimit) && ok;
+      if (half == 0) {
+        float* st = stageAll + (j % 3) * kStageFloats;
+        st[row] = f.D;
 #pragma unroll
-      for (uint32_t q = 0; q < 2; ++q) {
-        const uint32_t kgl = 2u * wg + q;
-        if (kgl < kgs) {
+        for (uint32_t q = 0; q < 2; ++q) {
+          st[(1 + q) * kBasisPaths + row] = f.Q[q];
+          st[(3 + q) * kBasisPaths + row] = j > 0 && rs > 0 ? prevQ[q] - f.Q[q] : 0.0f;
+          st[(5 + q) * kBasisPaths + row] = rs > 0 ? f.Q[q] - qn[q] : 0.0f;
+          if (rs > 0) prevQ[q] = f.Q[q];
+        }
+        float u[4] = {live ? f.D : 0.0f, live ? f.Q[0] : 0.0f, live ? f.Q[1] : 0.0f, live ? 1.0f : 0.0f};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (uint32_t o = 16; o > 0; o >>= 1) u[k] += __shfl_xor_sync(0xFFFFFFFFu, u[k], o);
+        if (lane == 0) {
+          float* us = st + 7 * kBasisPaths + (row >> 5) * 4;
+          us[0] = u[0], us[1] = u[1], us[2] = u[2], us[3] = u[3];
+        }
+      }
+      const unsigned char* desc = sm + kOffDesc + (j & 1u) * kBasisDescBytes;
+      const BasisKg* kgS = reinterpret_cast<const BasisKg*>(desc);
+      const float* optS = reinterpret_cast<const float*>(desc + numKg * sizeof(BasisKg));
+      ok = mbarWait(&descBar[j & 1u], (j >> 1) & 1u, kWaitLimit) && ok;
+      // ---- basis chunks and their products ----
+      for (uint32_t c = 0; c < numChunks; ++c, ++g) {
+        const uint32_t buf = g & 1u;
+        if (g >= 2) ok = mbarWait(&mmaBar[buf], ((g - 2) >> 1) & 1u, kWaitLimit) && ok;  // chunk g - 2 freed both buffers
+        const uint32_t kgs = 2u * __ldg(G.chunks + 2 * g + 1);
+        if (tid == 0 && ok) {  // this chunk's coefficients, landing while the basis below is evaluated
+          const uint32_t bytes = kgs * 4096u;
+          mbarExpectTx(&loadBar[buf], bytes);
+          bulkLoad(sm + kOffCoef + buf * 2 * kCoefImage, G.blob + __ldg(G.chunks + 2 * g), bytes, &loadBar[buf]);
+          loaded = static_cast<int>(g);
+        }
+        unsigned char* phiHi = sm + kOffPhi + buf * 2 * kPhiImage;
+        for (uint32_t kgl = half; kgl < kgs; kgl += 2) {
           uint4 hi, lo;
-          basisGroup(G.kgs + firstKg + c * kBasisChunkKg + kgl, G.options + 8 * static_cast<size_t>(optBegin), f, fixS, row,
-                     hi, lo);
+          basisGroup(kgS + c * kBasisChunkKg + kgl, optS, f, fixS, row, hi, lo);
           const uint32_t off = umma::kMajorOffset(row, kgl * 8u, kBasisPaths);
           *reinterpret_cast<uint4*>(phiHi + off) = hi;
           *reinterpret_cast<uint4*>(phiHi + kPhiImage + off) = lo;
         }
+        umma::fenceAsyncShared();
+        ok = producersAnd(ok);
+        if (!ok) break;
+        if (tid == 0) {
+          bool t0 = mbarWait(&loadBar[buf], (g >> 1) & 1u, kWaitLimit);
+          if (t0) consumed = static_cast<int>(g);
+          // the date's accumulator held date j - 3, read last (as the previous value) by the epilogue of date j - 2
+          if (t0 && c == 0 && j >= 2) t0 = mbarWait(&epiDone[(j - 2) % 3], ((j - 2) / 3) & 1u, kWaitLimit);
+          if (t0) {
+            umma::fenceAfterSync();
+            const uint32_t steps = kgs / 2u, acc = tslot + (j % 3) * 128u;
+            const uint32_t aHi = umma::smem(sm + kOffCoef + buf * 2 * kCoefImage), aLo = aHi + steps * 4096u;
+            const uint32_t bHi = umma::smem(phiHi), bLo = bHi + kPhiImage;
+            constexpr uint32_t idesc = umma::idescF16(kBasisRows, kBasisPaths);
+            for (uint32_t i = 0; i < steps; ++i) {
+              const uint64_t dAh = umma::desc(aHi + i * 4096u, 2048u, 128u), dAl = umma::desc(aLo + i * 4096u, 2048u, 128u);
+              const uint64_t dBh = umma::desc(bHi + i * 4096u, 2048u, 128u), dBl = umma::desc(bLo + i * 4096u, 2048u, 128u);
+              umma::mma(acc, dAh, dBh, idesc, c > 0 || i > 0);
+              umma::mma(acc, dAh, dBl, idesc, true);
+              umma::mma(acc, dAl, dBh, idesc, true);
+            }
+            umma::commit(&mmaBar[buf]);
+            if (c + 1 == numChunks) umma::commit(&accFull[j % 3]);
+            issued = static_cast<int>(g);
+          }
+          ok = t0;
+        }
       }
-      umma::fenceAsyncShared();
-      ok = __syncthreads_and(ok) != 0;
+      ok = producersAnd(ok);  // the staging written, thread 0's last issue known
       if (!ok) break;
       if (tid == 0) {
-        bool t0 = mbarWait(&loadBar[buf], (g >> 1) & 1u, kWaitLimit);
-        if (t0) {
-          consumed = static_cast<int>(g);
-          umma::fenceAfterSync();
-          const uint32_t steps = kgs / 2u;
-          const uint32_t aHi = umma::smem(sm + kOffCoef + buf * 2 * kCoefImage), aLo = aHi + steps * 4096u;
-          const uint32_t bHi = umma::smem(phiHi), bLo = bHi + kPhiImage;
-          for (uint32_t i = 0; i < steps; ++i) {
-            const uint64_t dAh = umma::desc(aHi + i * 4096u, 2048u, 128u), dAl = umma::desc(aLo + i * 4096u, 2048u, 128u);
-            const uint64_t dBh = umma::desc(bHi + i * 4096u, 2048u, 128u), dBl = umma::desc(bLo + i * 4096u, 2048u, 128u);
-            umma::mma(tslot, dAh, dBh, idesc, c > 0 || i > 0);
-            umma::mma(tslot, dAh, dBl, idesc, true);
-            umma::mma(tslot, dAl, dBh, idesc, true);
+        mbarArrive(&stageFull[j % 3]);
+        if (numChunks == 0) mbarArrive(&accFull[j % 3]);  // no products: the epilogue takes the value as 0
+      }
+      // ---- the date's fixings, read from the next date on ----
+      for (uint32_t q = fixBegin + half; q < fixEnd; q += 2) {
+        const float4 r = __ldg(G.fixings + q);
+        fixS[static_cast<uint32_t>(r.w) * kBasisPaths + row] = (r.x * ex2(r.y * f.x) - 1.0f) * r.z * kCouponScale;
+      }
+      ok = producersAnd(ok);
+      if (!ok) break;
+    }
+    if (tid == 0) {
+      if (!ok) atomicExch(err, kDevTimeout);
+      // the work in flight settles before the TMEM and the shared memory go away
+      if (!ok && issued >= 0) mbarWait(&mmaBar[issued & 1], (static_cast<uint32_t>(issued) >> 1) & 1u, kWaitLimit);
+      if (loaded > consumed) mbarWait(&loadBar[loaded & 1], (static_cast<uint32_t>(loaded) >> 1) & 1u, kWaitLimit);
+      // a date's descriptors requested and never waited for (the last date's, or after a failure)
+      for (int d = descIssued; d >= 0 && d + 2 > descIssued; --d)
+        mbarWait(&descBar[d & 1], (static_cast<uint32_t>(d) >> 1) & 1u, kWaitLimit);
+    }
+  } else {
+    // ================================ consumers ================================
+    const uint32_t cw = warp - kProducers / 32, qtr = cw & 3u, half = cw >> 2;
+    const uint32_t nsRow = 32u * qtr + lane;
+    const bool nsLive = nsRow < G.numNs;
+    const uint32_t tl = tslot + ((32u * qtr) << 16);  // this warp's TMEM lanes
+    uint32_t hasCsa = 0, cpty = 0xFFFFFFFFu;
+    float hc = 0.0f, hb = 0.0f, mta = 0.0f, ia = 0.0f;
+    float* rowEP = nullptr;
+    float* partials = nullptr;
+    if (nsLive) {
+      const NsArgs<float>& A = G.ns[nsRow];
+      hasCsa = A.hasCsa, cpty = A.cpty, hc = A.hc, hb = A.hb, mta = A.mta, ia = A.ia;
+      rowEP = A.expo + static_cast<size_t>(A.rowEP) * nP;
+      partials = A.partials;
+    }
+    const bool hasQ = cpty < 2u;
+    const uint32_t qc = hasQ ? cpty : 0u;
+    {
+      const uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (uint32_t q8 = 0; q8 < 64; q8 += 8) umma::st8(tl + kColHeld + half * 64u + q8, z);
+      umma::waitSt();
+    }
+    const bool vecRows = nP % 4u == 0u;
+    float fwd[2] = {0.0f, 0.0f};  // 0.5 sum DE (Q - Q_next) of the last reporting date, per unit
+    // the date's record words and scale, loaded a date ahead
+    auto loadDate = [&](uint32_t j, uint4& w, float& scale) {
+      const uint32_t* dj = G.dates + static_cast<size_t>(j) * kBasisDateWords;
+      w = make_uint4(__ldg(dj + bdChunks), __ldg(dj + bdCall), __ldg(dj + bdRep), __ldg(dj + bdPrevChunks));
+      scale = __ldg(G.scale + static_cast<size_t>(j) * kBasisRows + nsRow);
+    };
+    uint4 nw;
+    float nsc, sc = 0.0f;
+    loadDate(0, nw, nsc);
+    for (uint32_t j = 0; j < nT; ++j) {
+      const uint32_t numChunks = nw.x, callJ = nw.y, rs = nw.z, prevChunks = nw.w;
+      const float scPrev = sc;
+      sc = nsc;
+      if (j + 1 < nT) loadDate(j + 1, nw, nsc);
+      bool w = mbarWait(&stageFull[j % 3], (j / 3) & 1u, kWaitLimit);
+      w = w && mbarWait(&accFull[j % 3], (j / 3) & 1u, kWaitLimit);
+      if (!__all_sync(0xFFFFFFFFu, w)) {
+        ok = false;
+        break;
+      }
+      umma::fenceAfterSync();
+      const float* st = stageAll + (j % 3) * kStageFloats;
+      const uint32_t accCol = (j % 3) * 128u, prevCol = ((j + 2) % 3) * 128u;
+#pragma unroll 1
+      for (uint32_t u = 0; u < 2; ++u) {
+        const uint32_t p00 = half * 64u + u * 32u;  // the unit's first path in the tile
+        const uint32_t first = tile * kBasisPaths + p00;
+        const uint32_t paths = first < nP ? min(32u, nP - first) : 0u;
+        if (paths == 0) continue;
+        float s[7] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // e, ep, en, D ep, D en, CVA, next CVA part
+#pragma unroll 1
+        for (uint32_t q8 = 0; q8 < 32; q8 += 8) {
+          const uint32_t p0 = p00 + q8;
+          uint32_t r[24];
+          umma::ld8x3(tl + accCol + p0, tl + prevCol + p0, tl + kColHeld + p0, r);
+          uint32_t hs[8];
+          float ep8[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const uint32_t p = p0 + i;
+            const float v = numChunks > 0 ? __uint_as_float(r[i]) * sc : 0.0f;
+            const float vPrev = prevChunks > 0 ? __uint_as_float(r[8 + i]) * scPrev : 0.0f;
+            float held = __uint_as_float(r[16 + i]), collateral = 0.0f;
+            if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back (collateral.cpp:10-47)
+              const float vc = callJ != j ? vPrev : v;
+              float required = 0.0f;
+              if (vc > hc) required += vc - hc;
+              if (hb >= 0.0f && -vc > hb) required -= -vc - hb;
+              if (j == 0 || fabsf(required - held) >= mta) held = required;
+              collateral = held + ia;
+            }
+            hs[i] = __float_as_uint(held);
+            const float e = v - collateral, ep = fmaxf(e, 0.0f), en = fminf(e, 0.0f);
+            const float D = st[p], de = D * ep;
+            ep8[i] = ep;
+            if (q8 + i < paths) {
+              s[0] += e, s[1] += ep, s[2] += en, s[3] += de, s[4] += D * en;
+              if (rs > 0 && hasQ) {
+                s[5] += 0.5f * de * st[(3 + qc) * kBasisPaths + p];
+                s[6] += 0.5f * de * st[(5 + qc) * kBasisPaths + p];
+              }
+            }
           }
-          umma::commit(&mmaBar[buf]);
-          issued = static_cast<int>(g);
-          // the next chunk's coefficients into the other buffer, once chunk g - 1's MMAs have read it
-          if (g + 1 < G.numChunks) {
-            if (g >= 1) t0 = mbarWait(&mmaBar[buf ^ 1u], ((g - 1) >> 1) & 1u, kWaitLimit);
-            if (t0) {
-              const uint32_t bytes = __ldg(G.chunks + 2 * (g + 1) + 1) * 8192u;
-              mbarExpectTx(&loadBar[buf ^ 1u], bytes);
-              bulkLoad(sm + kOffCoef + (buf ^ 1u) * 2 * kCoefImage, G.blob + __ldg(G.chunks + 2 * (g + 1)), bytes,
-                       &loadBar[buf ^ 1u]);
-              loaded = static_cast<int>(g + 1);
+          umma::st8(tl + kColHeld + p0, hs);
+          if (rs > 0 && nsLive) {
+            float* dst = rowEP + static_cast<size_t>(rs - 1) * nP + first + q8;
+            if (vecRows && q8 + 8 <= paths) {
+              reinterpret_cast<float4*>(dst)[0] = make_float4(ep8[0], ep8[1], ep8[2], ep8[3]);
+              reinterpret_cast<float4*>(dst)[1] = make_float4(ep8[4], ep8[5], ep8[6], ep8[7]);
+            } else {
+#pragma unroll
+              for (uint32_t i = 0; i < 8; ++i)
+                if (q8 + i < paths) dst[i] = ep8[i];
             }
           }
         }
-        ok = t0;
+        umma::waitSt();  // the unit's collateral held, in TMEM before the next date reads it
+        const float cva = rs > 0 ? s[5] + fwd[u] : 0.0f;
+        if (rs > 0) fwd[u] = s[6];
+        if (nsLive) {
+          const float* us = st + 7 * kBasisPaths + (p00 >> 5) * 4;
+          const uint32_t unit = tile * 4u + (p00 >> 5);
+          float4* pt = reinterpret_cast<float4*>(partials + (static_cast<size_t>(unit) * nT + j) * kStatsPerDate);
+          pt[0] = make_float4(s[0], s[1], s[2], s[3]);
+          pt[1] = make_float4(s[4], cva, hasQ ? us[1 + qc] : us[3], us[0]);
+        }
       }
-    }
-    ok = __syncthreads_and(ok) != 0;  // thread 0's last issue; the staging above, when the date has no chunk
-    if (!ok) break;
-    // ---- the date's fixings (read from the next date on) ----
-    for (uint32_t q = fixBegin + wg; q < fixEnd; q += 4) {
-      const float4 r = __ldg(G.fixings + q);
-      fixS[static_cast<uint32_t>(r.w) * kBasisPaths + row] = (r.x * ex2(r.y * f.x) - 1.0f) * r.z * kCouponScale;
-    }
-    if (numChunks > 0) ok = mbarWait(&mmaBar[(g - 1) & 1u], ((g - 1) >> 1) & 1u, kWaitLimit);
-    umma::fenceAfterSync();
-    // ---- netting-set epilogue (warp-uniform: the TMEM accesses are warp-collective; lanes past the group's netting
-    // sets compute on zeros and store nothing) ----
-    if (blockPaths > 0 && ok) {
       __syncwarp();
-      const float sc = __ldg(G.scale + static_cast<size_t>(j) * kBasisRows + nsRow);
-      const bool hasQ = cpty < 2u;
-      float s8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-      for (uint32_t q8 = 0; q8 < 32; q8 += 8) {
-        uint32_t r[32];
-        umma::ld8x4(taddr + q8, taddr + kColHeld + q8, taddr + kColPrev + q8, taddr + kColDE + q8, r);
-        uint32_t st[24];
-        float ep8[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const uint32_t p = pb * 32u + q8 + i;  // path within the tile
-          const float v = numChunks > 0 ? __uint_as_float(r[i]) * sc : 0.0f;
-          float held = __uint_as_float(r[8 + i]), vPrev = __uint_as_float(r[16 + i]), prevDE = __uint_as_float(r[24 + i]);
-          float collateral = 0.0f;
-          if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back (collateral.cpp:10-47)
-            const float vc = callJ != j ? vPrev : v;
-            float required = 0.0f;
-            if (vc > hc) required += vc - hc;
-            if (hb >= 0.0f && -vc > hb) required -= -vc - hb;
-            if (j == 0 || fabsf(required - held) >= mta) held = required;
-            collateral = held + ia;
-          }
-          vPrev = v;
-          const float e = v - collateral, ep = fmaxf(e, 0.0f), en = fminf(e, 0.0f);
-          const float D = stage[p], Q = hasQ ? stage[(1 + cpty) * kBasisPaths + p] : 1.0f;
-          const float de = D * ep;
-          float cva = 0.0f;
-          if (rs > 0) {
-            if (hasQ) cva = 0.5f * (prevDE + de) * stage[(3 + cpty) * kBasisPaths + p];
-            prevDE = de;
-          }
-          ep8[i] = ep;
-          if (q8 + i < blockPaths) {
-            s8[0] += e, s8[1] += ep, s8[2] += en, s8[3] += de, s8[4] += D * en, s8[5] += cva, s8[6] += Q, s8[7] += D;
-          }
-          st[i] = __float_as_uint(held), st[8 + i] = __float_as_uint(vPrev), st[16 + i] = __float_as_uint(prevDE);
-        }
-        umma::st8x3(taddr + kColHeld + q8, taddr + kColPrev + q8, taddr + kColDE + q8, st);
-        if (rs > 0 && nsLive) {
-          float* dst = rowEP + static_cast<size_t>(rs - 1) * nP + blockFirst + q8;
-          if (vecRows && q8 + 8 <= blockPaths) {
-            reinterpret_cast<float4*>(dst)[0] = make_float4(ep8[0], ep8[1], ep8[2], ep8[3]);
-            reinterpret_cast<float4*>(dst)[1] = make_float4(ep8[4], ep8[5], ep8[6], ep8[7]);
-          } else {
-#pragma unroll
-            for (uint32_t i = 0; i < 8; ++i)
-              if (q8 + i < blockPaths) dst[i] = ep8[i];
-          }
-        }
-      }
-      if (nsLive) {
-        float4* pt = reinterpret_cast<float4*>(partials + (static_cast<size_t>(unit) * nT + j) * kStatsPerDate);
-        pt[0] = make_float4(s8[0], s8[1], s8[2], s8[3]);
-        pt[1] = make_float4(s8[4], s8[5], s8[6], s8[7]);
-      }
+      umma::fenceBeforeSync();
+      if (lane == 0) mbarArrive(&epiDone[j % 3]);
     }
-    umma::fenceBeforeSync();
-    ok = __syncthreads_and(ok) != 0;  // the accumulator is free for the next date's products
-  }
-  if (!ok && tid == 0) {
-    atomicExch(err, kDevTimeout);
-    // the work in flight settles before the TMEM and the shared memory go away
-    if (issued >= 0) mbarWait(&mmaBar[issued & 1], (static_cast<uint32_t>(issued) >> 1) & 1u, kWaitLimit);
-    if (loaded > consumed) mbarWait(&loadBar[loaded & 1], (static_cast<uint32_t>(loaded) >> 1) & 1u, kWaitLimit);
+    if (!ok && lane == 0) atomicExch(err, kDevTimeout);
   }
   umma::fenceBeforeSync();
   __syncthreads();

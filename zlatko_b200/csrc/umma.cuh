@@ -128,6 +128,27 @@ __device__ __forceinline__ void ld8x4(uint32_t a0, uint32_t a1, uint32_t a2, uin
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3)
       : "memory");
 }
+// Three runs of 8 consecutive 32-bit columns of this thread's TMEM lane (at a0..a2) and the wait for them.
+__device__ __forceinline__ void ld8x3(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t (&r)[24]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%24];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8, %9, %10, %11, %12, %13, %14, %15}, [%25];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16, %17, %18, %19, %20, %21, %22, %23}, [%26];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23])
+      : "r"(a0), "r"(a1), "r"(a2)
+      : "memory");
+}
+// 8 consecutive 32-bit columns of this thread's TMEM lane from registers (the registers are read at issue;
+// waitSt completes the stores before the columns are read back or handed to another thread).
+__device__ __forceinline__ void st8(uint32_t a, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(a), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+__device__ __forceinline__ void waitSt() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 // Three runs of 8 consecutive 32-bit columns of this thread's TMEM lane (at a0..a2) from registers, and the wait
 // for the stores, in one statement (the registers may be reused as soon as it returns).
 __device__ __forceinline__ void st8x3(uint32_t a0, uint32_t a1, uint32_t a2, const uint32_t (&r)[24]) {

@@ -256,6 +256,12 @@ __device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// One arrival on `bar` (release semantics: the thread's earlier writes are visible to a waiter that sees the phase
+// complete).
+__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+
 // Waits for phase `parity` of `bar` to complete; gives up after `limit` polls and returns false.
 __device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t parity, uint32_t limit) {
   for (uint32_t i = 0; i < limit; ++i) {

@@ -96,8 +96,10 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
             batches: int = 8) -> Dict:
     """FP32 (zk_run_plans) against FP64 (zk_run_plan_f64) on every netting set of the book, beside each output's
     Monte Carlo standard error (path_standard_errors; batch means over `batches` independent seeds for the pathwise
-    CVA, whose per-path survival the FP64 rows do not carry).  Returns, per output, the largest |FP32 - FP64| / SE
-    over netting sets and dates, the largest relative error |FP32 - FP64| / max|FP64|, the largest relative error on
+    CVA, whose per-path survival the FP64 rows do not carry, and as a floor under the PFE's order-statistic SE, which
+    collapses where a netting set's exposures cluster at the quantile).  Returns, per output, the largest
+    |FP32 - FP64| / SE over netting sets and dates, the largest relative error |FP32 - FP64| / max|FP64|, the largest
+    relative error on
     entries without Monte Carlo error (SE zero: date 0, dates past every trade) and the netting set where the SE
     ratio peaks."""
     plans = [gpu.compile(model, b, options) for b in books]
@@ -128,6 +130,9 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
             a, b = np.atleast_1d(o32[i][key]), np.atleast_1d(o64[i][key])
             if key in ses[i]:
                 se = np.atleast_1d(ses[i][key])
+                if key == "pfe":  # the order-statistic form collapses where exposures cluster: not below batch means
+                    se_b = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
+                    se = np.maximum(se, se_b)
             else:
                 se = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
             err = np.abs(a - b)
