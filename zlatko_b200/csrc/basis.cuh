@@ -25,7 +25,9 @@ struct BasisArgs {
   uint32_t numNs, numFixSlots, numChunks, pad;
 };
 
-// One CTA per (tile of 128 paths, group): grid (tiles, groups), 512 threads, one CTA per SM.
-cudaError_t launchBasisRevalue(const BasisArgs* groups, uint32_t numGroups, uint32_t nP, uint32_t* err, cudaStream_t stream);
+// One CTA per (tile of 128 paths, group): grid (tiles, groups), 512 threads, one CTA per SM; descBytes and fixSlots:
+// the largest over the groups (BasisImage::descBytes, numFixSlots).
+cudaError_t launchBasisRevalue(const BasisArgs* groups, uint32_t numGroups, uint32_t nP, uint32_t descBytes, uint32_t fixSlots,
+                               uint32_t* err, cudaStream_t stream);
 
 }  // namespace zk

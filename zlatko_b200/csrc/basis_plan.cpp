@@ -57,6 +57,14 @@ double optionPrice(const float* r, double x, const double* S, const double* xf) 
   return blackD(S[a] * q / b0, r[6], std::fabs(p3), b0, p3 > 0.0);
 }
 
+// The same price from a basis option record (appendOption).
+double basisOptionPrice(const float* o, bool foreign, double x, const double* S, const double* xf) {
+  const uint32_t flags = static_cast<uint32_t>(o[9]), a = flags & 3u;
+  const double b0 = static_cast<double>(o[0]) * std::exp(-static_cast<double>(o[1]) * x);
+  const double q = foreign ? static_cast<double>(o[2]) * std::exp(-static_cast<double>(o[3]) * xf[std::min(a, 1u)]) : o[2];
+  return blackD(S[a] * q / b0, o[4], o[8], b0, (flags & 4u) != 0);
+}
+
 struct FixKey {
   uint32_t j, A, b, invc;
   bool operator<(const FixKey& o) const { return std::tie(j, A, b, invc) < std::tie(o.j, o.A, o.b, o.invc); }
@@ -84,6 +92,19 @@ uint16_t f2h(float f) {
   }
   const uint32_t y = x - 0x38000000u;  // exponent bias 127 -> 15
   return static_cast<uint16_t>(sign | ((y + 0xFFFu + ((y >> 13) & 1u)) >> 13));
+}
+
+// A Black option term as the basis kernel prices it: A, B, P_f (rec[5]), B_f (foreign options), K, 1 / K,
+// 1 / sd (0 where sd <= 1e-7: the intrinsic value), sd / 2, sd, flags (asset | 4 call), 0, 0 -- the divisions by K
+// and sd of the reference's formula (fused_kernels.cpp:209-215) done once here.
+void appendOption(const float* r, bool foreign, std::vector<float>& out) {
+  const uint32_t code = static_cast<uint32_t>(r[0]);
+  const uint32_t asset = foreign ? std::min<uint32_t>(code >> 12u, 1u) : static_cast<uint32_t>(r[1]) & 3u;
+  const float K = r[6], sd = std::fabs(r[7]);
+  const bool call = r[7] > 0.0f;
+  const float v[kBasisOptWords] = {r[3], r[4], r[5], foreign ? r[1] : 0.0f, K, 1.0f / K, sd <= 1e-7f ? 0.0f : 1.0f / sd,
+                                   0.5f * sd, sd, static_cast<float>(asset | (call ? 4u : 0u)), 0.0f, 0.0f};
+  out.insert(out.end(), v, v + kBasisOptWords);
 }
 
 // One date's part of the image (built independently of the other dates).
@@ -167,21 +188,21 @@ void buildDate(const std::vector<BasisPlanIn>& plans, const std::vector<Fix>& fi
   std::vector<int> colOfSlot;  // column position -> key column, -1 for padding
   size_t c = 0;
   while (c < nCols) {
-    const uint32_t type = ents[colStart[c]].key[0];
+    const uint32_t type = ents[colStart[c]].key[0], asset = ents[colStart[c]].key[1];
+    // a run: the columns of one type (foreign bonds and FX rates: of one asset, so a k-group reads one rate)
+    const bool perAsset = type == kColForeign || type == kColSpot;
     size_t e = c;
-    while (e < nCols && ents[colStart[e]].key[0] == type) ++e;
+    while (e < nCols && ents[colStart[e]].key[0] == type && (!perAsset || ents[colStart[e]].key[1] == asset)) ++e;
     const bool opt = type == kColOption || type == kColForeignOption;
-    const size_t optFirst = D.options.size() / 8;
+    const size_t optFirst = D.options.size() / kBasisOptWords;
     if (opt) {
       for (size_t q = c; q < e; ++q) {
         const auto& k = ents[colStart[q]].key;
-        for (int w = 0; w < 8; ++w) {
-          float v;
-          std::memcpy(&v, &k[3 + w], 4);
-          D.options.push_back(v);
-        }
+        float r[8];
+        for (int w = 0; w < 8; ++w) std::memcpy(&r[w], &k[3 + w], 4);
+        appendOption(r, type == kColForeignOption, D.options);
       }
-      if (D.options.size() / 8 > 0x10000u) {
+      if (D.options.size() / kBasisOptWords > 0x10000u) {
         D.why = "more than 65,536 options on one date";
         return;
       }
@@ -378,10 +399,9 @@ bool buildBasis(const std::vector<BasisPlanIn>& plans, BasisImage& out, std::str
     d[bdKg] = static_cast<uint32_t>(out.kgs.size());
     d[bdKgs] = static_cast<uint32_t>(D.kgs.size());
     out.kgs.insert(out.kgs.end(), D.kgs.begin(), D.kgs.end());
-    d[bdOpt] = static_cast<uint32_t>(out.options.size() / 8);
-    d[bdOpts] = static_cast<uint32_t>(D.options.size() / 8);
-    if (D.kgs.size() * sizeof(BasisKg) + D.options.size() * 4 > kBasisDescBytes)
-      return why = "a date with more than 16 KB of basis columns and option records", false;
+    d[bdOpt] = static_cast<uint32_t>(out.options.size() / kBasisOptWords);
+    d[bdOpts] = static_cast<uint32_t>(D.options.size() / kBasisOptWords);
+    out.descBytes = std::max<uint32_t>(out.descBytes, static_cast<uint32_t>((D.kgs.size() * sizeof(BasisKg) + D.options.size() * 4 + 1023) / 1024 * 1024));
     out.options.insert(out.options.end(), D.options.begin(), D.options.end());
     d[bdChunk] = out.numChunks;
     d[bdChunks] = static_cast<uint32_t>(D.chunkSteps.size());
@@ -394,6 +414,8 @@ bool buildBasis(const std::vector<BasisPlanIn>& plans, BasisImage& out, std::str
     std::copy(D.scale.begin(), D.scale.end(), out.scale.begin() + static_cast<size_t>(j) * kBasisRows);
     out.linearTerms += D.linearTerms, out.columns += 8ull * D.kgs.size();
   }
+  if (basisSmemBytes(out.descBytes, out.numFixSlots) > kBasisMaxSmem)
+    return why = "a date's basis columns, option records and fixings beyond the kernel's shared memory", false;
   uint32_t next = nT;
   for (uint32_t j = nT; j-- > 0;) {
     uint32_t* d = &out.dates[static_cast<size_t>(j) * kBasisDateWords];
@@ -432,7 +454,9 @@ double basisCheck(const std::vector<BasisPlanIn>& plans, const BasisImage& img, 
           case kColCoupon: phi = K.mult * fixImg[K.sel[e]] * std::exp2(static_cast<double>(K.b[e]) * xj); break;
           case kColForeign: phi = Sj[K.sel[e]] * std::exp2(static_cast<double>(K.b[e]) * xfj[K.sel[e]]); break;
           case kColSpot: phi = Sj[K.sel[e]]; break;
-          default: phi = K.mult * optionPrice(&img.options[(static_cast<size_t>(d[bdOpt]) + K.sel[e]) * 8], xj, Sj, xfj);
+          default:
+            phi = K.mult * basisOptionPrice(&img.options[(static_cast<size_t>(d[bdOpt]) + K.sel[e]) * kBasisOptWords],
+                                            K.type == kColForeignOption, xj, Sj, xfj);
         }
         for (size_t n = 0; n < nNs; ++n) {
           const size_t off = static_cast<size_t>(gl) * 1024 + (n & 7) * 8 + (n >> 3) * 64 + e;

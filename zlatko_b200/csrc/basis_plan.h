@@ -32,6 +32,7 @@ constexpr int kBasisMaxFix = 64;      // fixings live at once (shared-memory slo
 constexpr int kBasisDateWords = 12;   // words per date record
 constexpr float kCouponScale = 64.0f; // fixings are kept times 64 (exact): coupon columns of about one
 constexpr float kOptionScale = 16.0f; // option prices times 16
+constexpr int kBasisOptWords = 12;    // floats per option record (appendOption)
 
 enum BasisColumn : uint32_t {
   kColBond = 0,           // 2^(b x)
@@ -45,7 +46,7 @@ enum BasisColumn : uint32_t {
 // One k-group: 8 columns of one type (64 bytes, read with four 16-byte loads).
 struct BasisKg {
   float b[8];        // exponent coefficients, -B log2 e
-  uint16_t sel[8];   // fixing slot, asset, or option record (relative to the date's first)
+  uint16_t sel[8];   // fixing slot, asset (the k-group's one asset), or option record (relative to the date's first)
   uint32_t type;
   float mult;        // the columns' scale (1, 64 or 16): C is divided by it on the host
   uint32_t pad[2];
@@ -58,8 +59,14 @@ enum BasisDateWord : int {
   bdChunk = 0, bdChunks = 1, bdKg = 2, bdKgs = 3, bdFixBegin = 4, bdFixEnd = 5, bdOpt = 6, bdCall = 7, bdRep = 8,
   bdNextRep = 9, bdPrevChunks = 10, bdOpts = 11,
 };
-// A date's k-groups and option records, copied into shared memory a date ahead: at most this many bytes.
-constexpr uint32_t kBasisDescBytes = 16384;
+// The kernel's shared memory: the basis and coefficient chunk buffers (128 KB), three dates' staging, two dates'
+// k-groups and option records (copied a date ahead), and the fixings' slots; at most 227 KB.
+constexpr uint32_t kBasisStageBytes = (7 * kBasisPaths + 16) * 4;
+constexpr uint32_t kBasisFixedSmem = 4 * kBasisPaths * 64 * 2 + 4 * kBasisRows * 64 * 2 + 3 * kBasisStageBytes;
+constexpr uint32_t kBasisMaxSmem = 227 * 1024;
+inline uint32_t basisSmemBytes(uint32_t descBytes, uint32_t fixSlots) {
+  return kBasisFixedSmem + 2 * descBytes + fixSlots * kBasisPaths * 4;
+}
 
 // One netting set of a group: its plan's tables as the reference lays them out.
 struct BasisPlanIn {
@@ -72,13 +79,14 @@ struct BasisImage {
   uint32_t numNs = 0, nT = 0, numFixSlots = 0, numChunks = 0;
   std::vector<uint32_t> dates;      // [nT][kBasisDateWords]
   std::vector<BasisKg> kgs;         // k-groups of every date, in date order
-  std::vector<float> options;       // [*][8]: the option terms' records
+  std::vector<float> options;       // [*][kBasisOptWords]: the option terms, as the kernel prices them
   std::vector<float> fixings;       // [*][4]: A, b, 1 / c, slot
   std::vector<uint32_t> chunks;     // [numChunks][2]: byte offset of the chunk's images in blob, K-steps of 16
   std::vector<uint16_t> blob;       // per chunk: hi image, then lo image (steps * 2 k-groups * 128 rows * 8 halves)
   std::vector<float> scale;         // [nT][kBasisRows]: 2^s
   uint64_t linearTerms = 0;         // the plans' linear terms (bonds, coupons, forwards) and options, all dates
   uint64_t columns = 0;             // basis columns over all dates (padding included)
+  uint32_t descBytes = 0;           // the largest date's k-groups and option records, rounded up to 1 KB
 };
 
 // Runs fn(0) .. fn(n - 1), possibly on several host threads.

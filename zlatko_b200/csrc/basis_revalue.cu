@@ -36,18 +36,17 @@ namespace zk {
 namespace {
 
 constexpr uint32_t kThreads = 512, kProducers = 256;
-constexpr uint32_t kWaitLimit = 1u << 26;               // polls of a barrier before the kernel gives up
 constexpr uint32_t kPhiImage = kBasisPaths * 64 * 2;     // one FP16 image of a basis chunk: 16 KB
 constexpr uint32_t kCoefImage = kBasisRows * 64 * 2;     // one FP16 image of a coefficient chunk: 16 KB
 constexpr uint32_t kOffPhi = 0;                          // [2 buffers][hi, lo]
 constexpr uint32_t kOffCoef = kOffPhi + 4 * kPhiImage;   // [2 buffers][hi, lo]
-constexpr uint32_t kOffFix = kOffCoef + 4 * kCoefImage;  // fixings x 64: [slot][path]
-// A date's staging: per path D | Q0 Q1 | dQ0 dQ1 (Q' - Q since the previous reporting date) | dQn0 dQn1 (Q - Q at
-// the next reporting date); per 32-path unit the sums of D, Q0, Q1 and the count of live paths.
-constexpr uint32_t kStageFloats = 7 * kBasisPaths + 16;
-constexpr uint32_t kOffStage = kOffFix + kBasisMaxFix * kBasisPaths * 4;  // [3 buffers]
-constexpr uint32_t kOffDesc = kOffStage + 3 * kStageFloats * 4;  // [2 buffers] a date's k-groups, then its options
-constexpr uint32_t kSmem = kOffDesc + 2 * kBasisDescBytes;
+// A date's staging: per path D | Q0 Q1 | dQ0 dQ1 ((Q' - Q) / 2 since the previous reporting date) | dQn0 dQn1
+// ((Q - Q at the next reporting date) / 2); per 32-path unit the sums of D, Q0, Q1 and the count of live paths.
+constexpr uint32_t kStageFloats = kBasisStageBytes / 4;
+constexpr uint32_t kOffStage = kOffCoef + 4 * kCoefImage;     // [3 buffers]
+constexpr uint32_t kOffDesc = kOffStage + 3 * kBasisStageBytes;  // [2 buffers of descBytes] k-groups, then options;
+                                                                  // then the fixings x 64, [slot][path]
+static_assert(kOffDesc == kBasisFixedSmem, "the layout of basisSmemBytes");
 // TMEM columns: the accumulators of three consecutive dates [0, 128), [128, 256), [256, 384); the collateral held
 // per netting set and path [384, 512).
 constexpr uint32_t kColHeld = 384;
@@ -60,18 +59,20 @@ __device__ __forceinline__ float pick(const float (&a)[4], uint32_t i) {
   return i == 0 ? a[0] : i == 1 ? a[1] : i == 2 ? a[2] : a[3];
 }
 
-// The unscaled Black price of an option record (revalueKernel's kOption / kForeignOption), read from shared memory.
+// The unscaled Black price of an option (a basis option record in shared memory: A, B, P_f, B_f, K, 1 / K, 1 / sd,
+// sd / 2, sd, flags): revalueKernel's kOption / kForeignOption with the reference's guards and A&S normal CDF
+// (fused_kernels.cpp:201-215), the divisions by K and sd replaced by the record's reciprocals.
 __device__ __forceinline__ float optionPrice(const float* rec, bool foreign, const Factors& f) {
   const float4 r0 = reinterpret_cast<const float4*>(rec)[0], r1 = reinterpret_cast<const float4*>(rec)[1];
-  const float b0 = r0.w * fastExp(-r1.x * f.x);
-  float F;
-  if (!foreign) {
-    F = pick(f.S, static_cast<uint32_t>(r0.y) & 3u) * r1.y / b0;
-  } else {
-    const uint32_t a = min(static_cast<uint32_t>(r0.x) >> 12u, 1u);
-    F = pick(f.S, a) * (r1.y * fastExp(-r0.y * (a == 0 ? f.xf[0] : f.xf[1]))) / b0;
-  }
-  return black(F, r1.z, fabsf(r1.w), b0, r1.w > 0.0f);
+  const float4 r2 = reinterpret_cast<const float4*>(rec)[2];
+  const uint32_t flags = static_cast<uint32_t>(r2.y), a = flags & 3u;
+  const float b0 = r0.x * fastExp(-r0.y * f.x);
+  const float q = foreign ? r0.z * fastExp(-r0.w * (a == 0 ? f.xf[0] : f.xf[1])) : r0.z;
+  const float F = __fdividef(pick(f.S, a) * q, b0), K = r1.x;
+  const float s = (flags & 4u) ? 1.0f : -1.0f;
+  if (r1.z == 0.0f || F <= 0.0f) return b0 * fmaxf(s * (F - K), 0.0f);
+  const float d1 = __logf(F * r1.y) * r1.z + r1.w, d2 = d1 - r2.x;
+  return b0 * s * (F * ncdf(s * d1) - K * ncdf(s * d2));
 }
 
 // One k-group of the basis for this thread's path: 8 values of one column type, as FP16 hi and lo (the k-group and
@@ -96,17 +97,22 @@ __device__ __forceinline__ void basisGroup(const BasisKg* kg, const float* optio
 #pragma unroll
       for (int e = 0; e < 8; ++e) phi[e] = fixS[sel[e] * kBasisPaths + row] * ex2(b[e] * f.x);
       break;
-    case kColForeign:
+    case kColForeign: {  // one asset per k-group
+      const float S = pick(f.S, sel[0]), xf = sel[0] == 0 ? f.xf[0] : f.xf[1];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) phi[e] = pick(f.S, sel[e]) * ex2(b[e] * (sel[e] == 0 ? f.xf[0] : f.xf[1]));
+      for (int e = 0; e < 8; ++e) phi[e] = S * ex2(b[e] * xf);
       break;
-    case kColSpot:
+    }
+    case kColSpot: {
+      const float S = pick(f.S, sel[0]);
 #pragma unroll
-      for (int e = 0; e < 8; ++e) phi[e] = pick(f.S, sel[e]);
+      for (int e = 0; e < 8; ++e) phi[e] = S;
       break;
+    }
     default:  // options, one record per column
 #pragma unroll
-      for (int e = 0; e < 8; ++e) phi[e] = mult * optionPrice(options + 8 * sel[e], type == kColForeignOption, f);
+      for (int e = 0; e < 8; ++e)
+        phi[e] = mult * optionPrice(options + kBasisOptWords * sel[e], type == kColForeignOption, f);
   }
   uint32_t h[4], l[4];
 #pragma unroll
@@ -121,6 +127,22 @@ __device__ __forceinline__ void basisGroup(const BasisKg* kg, const float* optio
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// A bounded mbarrier wait whose polls suspend the warp (up to kSuspendNs each) instead of spinning, so waiting warps
+// leave the issue slots to the working ones.
+constexpr uint32_t kSuspendNs = 1000, kSleepLimit = 1u << 22;  // at most about 4 s
+__device__ __forceinline__ bool waitSleep(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kSleepLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smemAddr(bar)), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Producers' barrier (named barrier 1, the 256 producer threads), and-reducing a predicate.
 __device__ __forceinline__ bool producersAnd(bool v) {
   uint32_t r;
@@ -131,7 +153,8 @@ __device__ __forceinline__ bool producersAnd(bool v) {
   return r != 0;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArgs* __restrict__ groups, uint32_t* err) {
+__global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArgs* __restrict__ groups, uint32_t descBytes,
+                                                                  uint32_t* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ BasisArgs G;
   __shared__ __align__(8) uint64_t loadBar[2], mmaBar[2], descBar[2], accFull[3], stageFull[3], epiDone[3];
@@ -147,7 +170,7 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
   __syncthreads();
   umma::fenceAfterSync();
   const uint32_t nP = G.nP, nT = G.nT, tile = blockIdx.x;
-  float* fixS = reinterpret_cast<float*>(sm + kOffFix);
+  float* fixS = reinterpret_cast<float*>(sm + kOffDesc + 2 * descBytes);
   float* stageAll = reinterpret_cast<float*>(sm + kOffStage);
   const size_t fs = static_cast<size_t>(nT) * nP;
   bool ok = true;
@@ -182,15 +205,15 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
     };
     // Thread 0: the k-groups and option records of date j into descriptor buffer j % 2 (issued a date ahead).
     auto loadDesc = [&](const uint4 (&d)[3], uint32_t j) {
-      const uint32_t kgBytes = d[0].w * static_cast<uint32_t>(sizeof(BasisKg)), optBytes = d[2].w * 32u;
-      unsigned char* dst = sm + kOffDesc + (j & 1u) * kBasisDescBytes;
+      const uint32_t kgBytes = d[0].w * static_cast<uint32_t>(sizeof(BasisKg)), optBytes = d[2].w * 4u * kBasisOptWords;
+      unsigned char* dst = sm + kOffDesc + (j & 1u) * descBytes;
       if (kgBytes + optBytes == 0) {
         mbarArrive(&descBar[j & 1u]);
         return;
       }
       mbarExpectTx(&descBar[j & 1u], kgBytes + optBytes);
       if (kgBytes) bulkLoad(dst, G.kgs + d[0].z, kgBytes, &descBar[j & 1u]);
-      if (optBytes) bulkLoad(dst + kgBytes, G.options + 8 * static_cast<size_t>(d[1].z), optBytes, &descBar[j & 1u]);
+      if (optBytes) bulkLoad(dst + kgBytes, G.options + kBasisOptWords * static_cast<size_t>(d[1].z), optBytes, &descBar[j & 1u]);
     };
     float prevQ[2] = {1.0f, 1.0f};
     uint32_t g = 0;                               // chunks started (all dates)
@@ -215,15 +238,15 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
         if (tid == 0) loadDesc(nd, j + 1), descIssued = static_cast<int>(j + 1);
       }
       // the staging buffer of date j was last read by the epilogue of date j - 3
-      if (j >= 3) ok = mbarWait(&epiDone[j % 3], ((j - 3) / 3) & 1u, kWaitLimit) && ok;
+      if (j >= 3) ok = waitSleep(&epiDone[j % 3], ((j - 3) / 3) & 1u) && ok;
       if (half == 0) {
         float* st = stageAll + (j % 3) * kStageFloats;
         st[row] = f.D;
 #pragma unroll
         for (uint32_t q = 0; q < 2; ++q) {
           st[(1 + q) * kBasisPaths + row] = f.Q[q];
-          st[(3 + q) * kBasisPaths + row] = j > 0 && rs > 0 ? prevQ[q] - f.Q[q] : 0.0f;
-          st[(5 + q) * kBasisPaths + row] = rs > 0 ? f.Q[q] - qn[q] : 0.0f;
+          st[(3 + q) * kBasisPaths + row] = j > 0 && rs > 0 ? 0.5f * (prevQ[q] - f.Q[q]) : 0.0f;
+          st[(5 + q) * kBasisPaths + row] = rs > 0 ? 0.5f * (f.Q[q] - qn[q]) : 0.0f;
           if (rs > 0) prevQ[q] = f.Q[q];
         }
         float u[4] = {live ? f.D : 0.0f, live ? f.Q[0] : 0.0f, live ? f.Q[1] : 0.0f, live ? 1.0f : 0.0f};
@@ -236,14 +259,14 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
           us[0] = u[0], us[1] = u[1], us[2] = u[2], us[3] = u[3];
         }
       }
-      const unsigned char* desc = sm + kOffDesc + (j & 1u) * kBasisDescBytes;
+      const unsigned char* desc = sm + kOffDesc + (j & 1u) * descBytes;
       const BasisKg* kgS = reinterpret_cast<const BasisKg*>(desc);
       const float* optS = reinterpret_cast<const float*>(desc + numKg * sizeof(BasisKg));
-      ok = mbarWait(&descBar[j & 1u], (j >> 1) & 1u, kWaitLimit) && ok;
+      ok = waitSleep(&descBar[j & 1u], (j >> 1) & 1u) && ok;
       // ---- basis chunks and their products ----
       for (uint32_t c = 0; c < numChunks; ++c, ++g) {
         const uint32_t buf = g & 1u;
-        if (g >= 2) ok = mbarWait(&mmaBar[buf], ((g - 2) >> 1) & 1u, kWaitLimit) && ok;  // chunk g - 2 freed both buffers
+        if (g >= 2) ok = waitSleep(&mmaBar[buf], ((g - 2) >> 1) & 1u) && ok;  // chunk g - 2 freed both buffers
         const uint32_t kgs = 2u * __ldg(G.chunks + 2 * g + 1);
         if (tid == 0 && ok) {  // this chunk's coefficients, landing while the basis below is evaluated
           const uint32_t bytes = kgs * 4096u;
@@ -263,10 +286,10 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
         ok = producersAnd(ok);
         if (!ok) break;
         if (tid == 0) {
-          bool t0 = mbarWait(&loadBar[buf], (g >> 1) & 1u, kWaitLimit);
+          bool t0 = waitSleep(&loadBar[buf], (g >> 1) & 1u);
           if (t0) consumed = static_cast<int>(g);
           // the date's accumulator held date j - 3, read last (as the previous value) by the epilogue of date j - 2
-          if (t0 && c == 0 && j >= 2) t0 = mbarWait(&epiDone[(j - 2) % 3], ((j - 2) / 3) & 1u, kWaitLimit);
+          if (t0 && c == 0 && j >= 2) t0 = waitSleep(&epiDone[(j - 2) % 3], ((j - 2) / 3) & 1u);
           if (t0) {
             umma::fenceAfterSync();
             const uint32_t steps = kgs / 2u, acc = tslot + (j % 3) * 128u;
@@ -304,11 +327,11 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
     if (tid == 0) {
       if (!ok) atomicExch(err, kDevTimeout);
       // the work in flight settles before the TMEM and the shared memory go away
-      if (!ok && issued >= 0) mbarWait(&mmaBar[issued & 1], (static_cast<uint32_t>(issued) >> 1) & 1u, kWaitLimit);
-      if (loaded > consumed) mbarWait(&loadBar[loaded & 1], (static_cast<uint32_t>(loaded) >> 1) & 1u, kWaitLimit);
+      if (!ok && issued >= 0) waitSleep(&mmaBar[issued & 1], (static_cast<uint32_t>(issued) >> 1) & 1u);
+      if (loaded > consumed) waitSleep(&loadBar[loaded & 1], (static_cast<uint32_t>(loaded) >> 1) & 1u);
       // a date's descriptors requested and never waited for (the last date's, or after a failure)
       for (int d = descIssued; d >= 0 && d + 2 > descIssued; --d)
-        mbarWait(&descBar[d & 1], (static_cast<uint32_t>(d) >> 1) & 1u, kWaitLimit);
+        waitSleep(&descBar[d & 1], (static_cast<uint32_t>(d) >> 1) & 1u);
     }
   } else {
     // ================================ consumers ================================
@@ -328,6 +351,9 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
     }
     const bool hasQ = cpty < 2u;
     const uint32_t qc = hasQ ? cpty : 0u;
+    // the call rule (collateral.cpp:10-47) branch-free: required = max(vc - hc, 0) + min(vc + hb, 0), the second
+    // term absent for a one-way CSA (hb < 0); one of the two is always zero, so the sum is exact
+    const float hbEff = hb >= 0.0f ? hb : __int_as_float(0x7F800000);
     {
       const uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -350,8 +376,8 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       const float scPrev = sc;
       sc = nsc;
       if (j + 1 < nT) loadDate(j + 1, nw, nsc);
-      bool w = mbarWait(&stageFull[j % 3], (j / 3) & 1u, kWaitLimit);
-      w = w && mbarWait(&accFull[j % 3], (j / 3) & 1u, kWaitLimit);
+      bool w = waitSleep(&stageFull[j % 3], (j / 3) & 1u);
+      w = w && waitSleep(&accFull[j % 3], (j / 3) & 1u);
       if (!__all_sync(0xFFFFFFFFu, w)) {
         ok = false;
         break;
@@ -359,6 +385,8 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       umma::fenceAfterSync();
       const float* st = stageAll + (j % 3) * kStageFloats;
       const uint32_t accCol = (j % 3) * 128u, prevCol = ((j + 2) % 3) * 128u;
+      const float mtaJ = j == 0 ? -1.0f : mta;  // date 0 always calls
+      const bool cvaDate = rs > 0 && hasQ;
 #pragma unroll 1
       for (uint32_t u = 0; u < 2; ++u) {
         const uint32_t p00 = half * 64u + u * 32u;  // the unit's first path in the tile
@@ -379,12 +407,10 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
             const float v = numChunks > 0 ? __uint_as_float(r[i]) * sc : 0.0f;
             const float vPrev = prevChunks > 0 ? __uint_as_float(r[8 + i]) * scPrev : 0.0f;
             float held = __uint_as_float(r[16 + i]), collateral = 0.0f;
-            if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back (collateral.cpp:10-47)
+            if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back
               const float vc = callJ != j ? vPrev : v;
-              float required = 0.0f;
-              if (vc > hc) required += vc - hc;
-              if (hb >= 0.0f && -vc > hb) required -= -vc - hb;
-              if (j == 0 || fabsf(required - held) >= mta) held = required;
+              const float required = fmaxf(vc - hc, 0.0f) + fminf(vc + hbEff, 0.0f);
+              if (fabsf(required - held) >= mtaJ) held = required;
               collateral = held + ia;
             }
             hs[i] = __float_as_uint(held);
@@ -392,10 +418,10 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
             const float D = st[p], de = D * ep;
             ep8[i] = ep;
             if (q8 + i < paths) {
-              s[0] += e, s[1] += ep, s[2] += en, s[3] += de, s[4] += D * en;
-              if (rs > 0 && hasQ) {
-                s[5] += 0.5f * de * st[(3 + qc) * kBasisPaths + p];
-                s[6] += 0.5f * de * st[(5 + qc) * kBasisPaths + p];
+              s[0] += e, s[1] += ep, s[2] += en, s[3] += de, s[4] = fmaf(D, en, s[4]);
+              if (cvaDate) {
+                s[5] = fmaf(de, st[(3 + qc) * kBasisPaths + p], s[5]);
+                s[6] = fmaf(de, st[(5 + qc) * kBasisPaths + p], s[6]);
               }
             }
           }
@@ -437,12 +463,15 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
 
 }  // namespace
 
-cudaError_t launchBasisRevalue(const BasisArgs* groups, uint32_t numGroups, uint32_t nP, uint32_t* err, cudaStream_t stream) {
+cudaError_t launchBasisRevalue(const BasisArgs* groups, uint32_t numGroups, uint32_t nP, uint32_t descBytes, uint32_t fixSlots,
+                               uint32_t* err, cudaStream_t stream) {
   if (numGroups == 0 || nP == 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(basisRevalueKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmem));
+  const uint32_t smem = basisSmemBytes(descBytes, fixSlots);
+  if (smem > kBasisMaxSmem) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(basisRevalueKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   const dim3 grid((nP + kBasisPaths - 1) / kBasisPaths, numGroups);
-  basisRevalueKernel<<<grid, kThreads, kSmem, stream>>>(groups, err);
+  basisRevalueKernel<<<grid, kThreads, smem, stream>>>(groups, descBytes, err);
   return cudaGetLastError();
 }
 

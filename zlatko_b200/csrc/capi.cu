@@ -531,6 +531,7 @@ struct Batch {
       size_t dates = 0, kgs = 0, options = 0, fixings = 0, chunks = 0, blob = 0, scale = 0;
     };
     size_t basisCount = 0, groupArgs = 0;  // groupArgs: index of the first group's BasisArgs in the batch's array
+    uint32_t descBytes = 0, fixSlots = 0;  // the basis kernel's shared memory: the largest over the groups
     std::vector<Group> groups;
   };
   std::vector<Launch> launches;
@@ -670,6 +671,8 @@ void formGroups(Batch<R>& B, typename Batch<R>::Launch& L, uint32_t mode, HostPo
       i = e;
     }
     L.basisCount = ordered.size();
+    for (const auto& G : L.groups)
+      L.descBytes = std::max(L.descBytes, G.img.descBytes), L.fixSlots = std::max(L.fixSlots, G.img.numFixSlots);
     for (size_t k = 0; k < L.basisCount; ++k) B.onBasis[ordered[k]] = 1;
     ordered.insert(ordered.end(), O.begin(), O.end());
     L.planIdx = std::move(ordered);
@@ -1094,7 +1097,7 @@ void launchRevalues(const Batch<R>& B, const typename Batch<R>::Launch& L, uintp
       while (g1 < L.groups.size() && L.groups[g1].first + L.groups[g1].count <= last) ++g1;
       injectPoint(B.ctx);
       ZK_CUDA(launchBasisRevalue(reinterpret_cast<const BasisArgs*>(base + B.basisArgsOff) + L.groupArgs + g0,
-                                 static_cast<uint32_t>(g1 - g0), L.sc.nP, B.ctx->dErr, s));
+                                 static_cast<uint32_t>(g1 - g0), L.sc.nP, L.descBytes, L.fixSlots, B.ctx->dErr, s));
       count -= last - first, first = last;
     }
   }

@@ -24,6 +24,10 @@ from . import spec as S
 from .summary import bilateral_cva, pathwise_cva, summarise, unilateral_cva
 
 SERIES = ("ee", "ene", "pfe", "dee", "dene")
+# Entries whose standard error is below this fraction of the netting set's value scale are below what single
+# precision resolves in a path's value (its rounding is 1e-6 .. 1e-5 of the scale): they count as entries without
+# Monte Carlo error, checked relative to the scale (max_rel_err_without_mc_error).
+RESOLUTION = 1e-5
 SCALARS = ("cva", "cva_bilateral", "dva", "pathwise_cva")
 
 
@@ -99,9 +103,8 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
     CVA, whose per-path survival the FP64 rows do not carry, and as a floor under the PFE's order-statistic SE, which
     collapses where a netting set's exposures cluster at the quantile).  Returns, per output, the largest
     |FP32 - FP64| / SE over netting sets and dates, the largest relative error |FP32 - FP64| / max|FP64|, the largest
-    relative error on
-    entries without Monte Carlo error (SE zero: date 0, dates past every trade) and the netting set where the SE
-    ratio peaks."""
+    relative error on entries without Monte Carlo error (SE below RESOLUTION of the scale: date 0, dates past every
+    trade, quantiles of tightly clustered exposures) and the netting set where the SE ratio peaks."""
     plans = [gpu.compile(model, b, options) for b in books]
     r32 = _run32(ctx, plans)
     o32, o64, ses = [], [], []
@@ -132,12 +135,12 @@ def compare(ctx: gpu.Context, model: S.Model, books: Sequence[S.NettingSet], opt
                 se = np.atleast_1d(ses[i][key])
                 if key == "pfe":  # the order-statistic form collapses where exposures cluster: not below batch means
                     se_b = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
-                    se = np.maximum(se, se_b)
+                    se = np.where(se > 0.0, np.maximum(se, se_b), se)
             else:
                 se = np.std(np.array([np.atleast_1d(e[i][key]) for e in est]), axis=0, ddof=1) * scale_paths
             err = np.abs(a - b)
             scale = max(np.abs(b).max(), vscale[i])
-            live = se > 1e-12 * scale
+            live = se > RESOLUTION * scale
             if np.any(live):
                 ratio = float(np.max(err[live] / se[live]))
                 if ratio > worst:
