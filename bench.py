@@ -100,9 +100,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch(paths: int):
-    """DRAM bytes of one fused-kernel launch from the committed ncu summary, scaled by paths."""
-    path = os.path.join(ROOT, "profiles", "revalue_book2000.txt")
+def tensor_peak():
+    """Dense BF16 / FP16 tensor TFLOP/s: the measured burst figure, else the fallback measured earlier on this pool."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = json.load(f).get("bf16_tflops")
+        if isinstance(v, (int, float)) and v > 0:
+            return float(v), "measured"
+    except (OSError, ValueError, AttributeError):
+        pass
+    return 1590.0, "fallback"
+
+
+def traffic_per_launch(paths: int, basis: bool = True):
+    """DRAM bytes of one revalue launch from the committed ncu summary (the basis kernel's, or the term-by-term
+    kernel's), scaled by paths."""
+    path = os.path.join(ROOT, "profiles", "basis_book2000.txt" if basis else "revalue_book2000.txt")
     if not os.path.exists(path):
         return None
     ref_paths, ref_bytes = None, None
@@ -718,9 +732,16 @@ def main():
     peak, peak_kind = peaks()
     fused_s = float(np.mean(fused_ms)) / 1e3
     nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
-    cube_bytes = (2 + nA + nC) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
-    warps = -(-nP // (32 * (int(info.tile_paths) // 128)))  # statistics partials: one per revalue warp
-    alg_bytes = sum(p.rows_total * nP * 4 + warps * nT * p.stats_per_date * 4 for p in plans) + info.table_bytes + cube_bytes
+    nF = (int(plans[0].header[10]) - 6) // 2
+    cube_bytes = (2 + nA + nC + nF) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
+    # statistics partials: one per 32-path unit on the basis kernel, one per revalue warp term by term
+    nb = int(info.num_basis_netting_sets)
+    units = [-(-nP // 32) if k < nb else -(-nP // (32 * (int(info.tile_paths) // 128))) for k in range(len(plans))]
+    alg_bytes = (sum(p.rows_total * nP * 4 + u * nT * p.stats_per_date * 4 for p, u in zip(plans, units)) + info.table_bytes +
+                 cube_bytes + int(info.basis_bytes))
+    # the basis kernel's products: per 128-path tile and column, C_hi Phi_hi + C_hi Phi_lo + C_lo Phi_hi over 128 rows
+    tensor_flops = 2.0 * 3 * 128 * (-(-nP // 128) * 128) * float(info.basis_columns)
+    tpeak, tpeak_kind = tensor_peak()
     ex2 = C_ex2 = None
     try:
         import ctypes as C
@@ -732,7 +753,7 @@ def main():
         C_ex2 = None
     exp_per_launch = float(info.exp_evaluations) * nP  # one ex2 per bond-like term and path
     row_bytes = float(sum(p.rows_total for p in plans)) * nP * 4
-    h2d = info.table_bytes + sum(p.indices.size * 4 for p in plans)
+    h2d = info.table_bytes + sum(p.indices.size * 4 for p in plans) + int(info.basis_bytes)
     d2h = sum((p.sums_len() + p.values_len()) * 4 for p in plans)
 
     if rank == 0:
@@ -769,16 +790,28 @@ def main():
             "kernel_ms": {"simulate": float(np.mean(sim_ms)), "revalue": float(np.mean(fused_ms)), "reduce": float(np.mean(reduce_ms)),
                           "row_stats": float(np.mean(rows_ms))},
             "roofline": {"bound": "hbm", "achieved": alg_bytes / fused_s / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg_bytes / fused_s / 1e9 / peak, "traffic": traffic_per_launch(nP),
-                         "note": f"revalue kernel (the dominant one); peak of {peak_kind}; algorithmic bytes = factor cube read "
-                                 "once + PFE rows written + per-group partials + plan tables"},
+                         "frac": alg_bytes / fused_s / 1e9 / peak, "traffic": traffic_per_launch(nP, nb > 0),
+                         "note": f"revalue step (the dominant kernel: {'basisRevalueKernel' if nb else 'revalueKernel'}); "
+                                 f"peak of {peak_kind}; algorithmic bytes = factor cube read once + PFE rows written + "
+                                 "per-unit partials + plan and basis tables"},
+            "roofline_tensor": {"bound": "tensor", "achieved": tensor_flops / fused_s / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                                "frac": tensor_flops / fused_s / 1e12 / tpeak,
+                                "note": f"basisRevalueKernel's FP16 hi/lo products (3 MMAs per 16 columns) against the dense "
+                                        f"BF16/FP16 peak of {tpeak_kind}; the kernel is bound by its CUDA-core work (the "
+                                        "basis functions and the netting-set epilogue), not by the tensor pipe"},
+            "basis": {"netting_sets": nb, "columns_per_date": float(info.basis_columns) / nT,
+                      "terms_per_date": float(info.basis_terms) / nT,
+                      "terms_per_column": float(info.basis_terms) / max(float(info.basis_columns), 1.0),
+                      "table_bytes": int(info.basis_bytes)},
             "roofline_row_stats": {"bound": "hbm", "achieved": row_bytes / (float(np.mean(rows_ms)) / 1e3) / 1e9, "peak": peak,
                                    "unit": "GB/s", "frac": row_bytes / (float(np.mean(rows_ms)) / 1e3) / 1e9 / peak,
                                    "note": "row-statistics kernel: algorithmic bytes = every exposure row read once; the exact "
                                            "quantile reads a row up to three times (min/max of a sample, histogram, bracket)"},
-            "roofline_mufu": {"bound": "sfu", "achieved": exp_per_launch / fused_s / 1e9 if C_ex2 else None,
-                              "peak": C_ex2 / 1e9 if C_ex2 else None, "unit": "G ex2/s",
-                              "frac": exp_per_launch / fused_s / C_ex2 if C_ex2 else None},
+            # the term-by-term kernel's SFU rate (one ex2 per bond-like term and path); with the basis kernel the
+            # book's exponentials are the basis columns', far fewer, and this rate does not describe the kernel
+            "roofline_mufu": ({"bound": "sfu", "achieved": exp_per_launch / fused_s / 1e9 if C_ex2 else None,
+                               "peak": C_ex2 / 1e9 if C_ex2 else None, "unit": "G ex2/s",
+                               "frac": exp_per_launch / fused_s / C_ex2 if C_ex2 else None} if nb == 0 else None),
             "clocks": clocks.summary(),
             "plan_compile_s": compile_s,
             "cpu_baseline": cpu,

@@ -248,6 +248,9 @@ typedef struct zk_batch_info {
   uint64_t graph_replay;         /* 1 once executes replay a captured CUDA graph, 0 while eager    */
   uint64_t num_waves;            /* waves of netting sets within the row budget (1 per launch group without) */
   uint64_t num_basis_netting_sets; /* netting sets revalued by the tensor-core basis kernel (zk_context_set_basis) */
+  uint64_t basis_columns;        /* basis functions a path evaluates over all dates, summed over the basis groups */
+  uint64_t basis_terms;          /* the linear terms and options those columns stand for (all dates and groups)   */
+  uint64_t basis_bytes;          /* bytes of the basis groups' tables (coefficient images, columns, options, ...) */
 } zk_batch_info;
 
 /* Uploads the plans.  The first zk_batch_execute autotunes the tile shape (paths per revalue CTA) on

@@ -60,7 +60,8 @@ class BatchInfo(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("num_plans", "num_launch_groups", "num_paths", "num_dates", "num_trades_hint",
                                           "num_terms", "term_evaluations", "exp_evaluations", "table_bytes", "row_bytes",
                                           "kernels_per_execute", "tile_paths", "graph_replay", "num_waves",
-                                          "num_basis_netting_sets")]
+                                          "num_basis_netting_sets", "basis_columns", "basis_terms",
+                                          "basis_bytes")]
 
 
 # Every entry point declared in include/zlatko_b200.h.

@@ -2076,6 +2076,12 @@ zk_status zk_batch_info_get(const zk_batch* b, zk_batch_info* info) {
   };
   for (const auto& L : B.launches) {
     info->num_basis_netting_sets += L.basisCount;
+    for (const auto& G : L.groups) {
+      const BasisImage& I = G.img;
+      info->basis_columns += I.columns, info->basis_terms += I.linearTerms;
+      info->basis_bytes += I.dates.size() * 4 + I.kgs.size() * sizeof(BasisKg) + (I.options.size() + I.fixings.size() + I.scale.size()) * 4 +
+                           I.chunks.size() * 4 + I.blob.size() * 2 + sizeof(BasisArgs);
+    }
     if (!B.waved) {
       kernels += 1 + revalueLaunches(L, 0, L.planIdx.size());  // simulate, then the revalue launches
       continue;
