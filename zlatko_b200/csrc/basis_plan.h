@@ -61,7 +61,7 @@ enum BasisDateWord : int {
 };
 // The kernel's shared memory: the basis and coefficient chunk buffers (128 KB), three dates' staging, two dates'
 // k-groups and option records (copied a date ahead), and the fixings' slots; at most 227 KB.
-constexpr uint32_t kBasisStageBytes = (7 * kBasisPaths + 16) * 4;
+constexpr uint32_t kBasisStageBytes = (3 * 4 * kBasisPaths + 16) * 4;
 constexpr uint32_t kBasisFixedSmem = 4 * kBasisPaths * 64 * 2 + 4 * kBasisRows * 64 * 2 + 3 * kBasisStageBytes;
 constexpr uint32_t kBasisMaxSmem = 227 * 1024;
 inline uint32_t basisSmemBytes(uint32_t descBytes, uint32_t fixSlots) {

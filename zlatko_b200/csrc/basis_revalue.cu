@@ -40,8 +40,9 @@ constexpr uint32_t kPhiImage = kBasisPaths * 64 * 2;     // one FP16 image of a 
 constexpr uint32_t kCoefImage = kBasisRows * 64 * 2;     // one FP16 image of a coefficient chunk: 16 KB
 constexpr uint32_t kOffPhi = 0;                          // [2 buffers][hi, lo]
 constexpr uint32_t kOffCoef = kOffPhi + 4 * kPhiImage;   // [2 buffers][hi, lo]
-// A date's staging: per path D | Q0 Q1 | dQ0 dQ1 ((Q' - Q) / 2 since the previous reporting date) | dQn0 dQn1
-// ((Q - Q at the next reporting date) / 2); per 32-path unit the sums of D, Q0, Q1 and the count of live paths.
+// A date's staging, per credit c (2: none) and path a float4 {D, (Q' - Q) / 2 since the previous reporting date,
+// (Q - Q at the next reporting date) / 2, Q} -- the no-credit record {D, 0, 0, 1} -- then per 32-path unit the sums
+// of D, Q0, Q1 and the count of live paths.
 constexpr uint32_t kStageFloats = kBasisStageBytes / 4;
 constexpr uint32_t kOffStage = kOffCoef + 4 * kCoefImage;     // [3 buffers]
 constexpr uint32_t kOffDesc = kOffStage + 3 * kBasisStageBytes;  // [2 buffers of descBytes] k-groups, then options;
@@ -169,6 +170,18 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
   umma::fenceBeforeSync();
   __syncthreads();
   umma::fenceAfterSync();
+  if (tid >= kProducers) {  // the three accumulators and the collateral held start at zero (finite) for every lane
+    const uint32_t cw = warp - kProducers / 32, base = tslot + ((32u * (cw & 3u)) << 16) + (cw >> 2) * 64u;
+    const uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (uint32_t c = 0; c < 512; c += 128)
+#pragma unroll
+      for (uint32_t q8 = 0; q8 < 64; q8 += 8) umma::st8(base + c + q8, z);
+    umma::waitSt();
+  }
+  umma::fenceBeforeSync();
+  __syncthreads();  // before any product writes an accumulator
+  umma::fenceAfterSync();
   const uint32_t nP = G.nP, nT = G.nT, tile = blockIdx.x;
   float* fixS = reinterpret_cast<float*>(sm + kOffDesc + 2 * descBytes);
   float* stageAll = reinterpret_cast<float*>(sm + kOffStage);
@@ -241,21 +254,21 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       if (j >= 3) ok = waitSleep(&epiDone[j % 3], ((j - 3) / 3) & 1u) && ok;
       if (half == 0) {
         float* st = stageAll + (j % 3) * kStageFloats;
-        st[row] = f.D;
+        float4* cs = reinterpret_cast<float4*>(st);
 #pragma unroll
         for (uint32_t q = 0; q < 2; ++q) {
-          st[(1 + q) * kBasisPaths + row] = f.Q[q];
-          st[(3 + q) * kBasisPaths + row] = j > 0 && rs > 0 ? 0.5f * (prevQ[q] - f.Q[q]) : 0.0f;
-          st[(5 + q) * kBasisPaths + row] = rs > 0 ? 0.5f * (f.Q[q] - qn[q]) : 0.0f;
+          cs[q * kBasisPaths + row] = make_float4(f.D, j > 0 && rs > 0 ? 0.5f * (prevQ[q] - f.Q[q]) : 0.0f,
+                                                  rs > 0 ? 0.5f * (f.Q[q] - qn[q]) : 0.0f, f.Q[q]);
           if (rs > 0) prevQ[q] = f.Q[q];
         }
+        cs[2 * kBasisPaths + row] = make_float4(f.D, 0.0f, 0.0f, 1.0f);
         float u[4] = {live ? f.D : 0.0f, live ? f.Q[0] : 0.0f, live ? f.Q[1] : 0.0f, live ? 1.0f : 0.0f};
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
           for (uint32_t o = 16; o > 0; o >>= 1) u[k] += __shfl_xor_sync(0xFFFFFFFFu, u[k], o);
         if (lane == 0) {
-          float* us = st + 7 * kBasisPaths + (row >> 5) * 4;
+          float* us = st + 12 * kBasisPaths + (row >> 5) * 4;
           us[0] = u[0], us[1] = u[1], us[2] = u[2], us[3] = u[3];
         }
       }
@@ -350,16 +363,10 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       partials = A.partials;
     }
     const bool hasQ = cpty < 2u;
-    const uint32_t qc = hasQ ? cpty : 0u;
+    const uint32_t qc = hasQ ? cpty : 2u;  // the staging record of the counterparty's survival (2: none)
     // the call rule (collateral.cpp:10-47) branch-free: required = max(vc - hc, 0) + min(vc + hb, 0), the second
     // term absent for a one-way CSA (hb < 0); one of the two is always zero, so the sum is exact
     const float hbEff = hb >= 0.0f ? hb : __int_as_float(0x7F800000);
-    {
-      const uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (uint32_t q8 = 0; q8 < 64; q8 += 8) umma::st8(tl + kColHeld + half * 64u + q8, z);
-      umma::waitSt();
-    }
     const bool vecRows = nP % 4u == 0u;
     float fwd[2] = {0.0f, 0.0f};  // 0.5 sum DE (Q - Q_next) of the last reporting date, per unit
     // the date's record words and scale, loaded a date ahead
@@ -384,9 +391,11 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       }
       umma::fenceAfterSync();
       const float* st = stageAll + (j % 3) * kStageFloats;
+      const float4* cs = reinterpret_cast<const float4*>(st) + qc * kBasisPaths;
+      const float scJ = numChunks > 0 ? sc : 0.0f, scP = prevChunks > 0 ? scPrev : 0.0f;  // no products: value 0
       const uint32_t accCol = (j % 3) * 128u, prevCol = ((j + 2) % 3) * 128u;
       const float mtaJ = j == 0 ? -1.0f : mta;  // date 0 always calls
-      const bool cvaDate = rs > 0 && hasQ;
+      float* const rowJ = rs > 0 && nsLive ? rowEP + static_cast<size_t>(rs - 1) * nP + tile * kBasisPaths : nullptr;
 #pragma unroll 1
       for (uint32_t u = 0; u < 2; ++u) {
         const uint32_t p00 = half * 64u + u * 32u;  // the unit's first path in the tile
@@ -404,8 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             const uint32_t p = p0 + i;
-            const float v = numChunks > 0 ? __uint_as_float(r[i]) * sc : 0.0f;
-            const float vPrev = prevChunks > 0 ? __uint_as_float(r[8 + i]) * scPrev : 0.0f;
+            const float v = __uint_as_float(r[i]) * scJ, vPrev = __uint_as_float(r[8 + i]) * scP;
             float held = __uint_as_float(r[16 + i]), collateral = 0.0f;
             if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back
               const float vc = callJ != j ? vPrev : v;
@@ -415,19 +423,17 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
             }
             hs[i] = __float_as_uint(held);
             const float e = v - collateral, ep = fmaxf(e, 0.0f), en = fminf(e, 0.0f);
-            const float D = st[p], de = D * ep;
+            const float4 z = cs[p];  // D, the CVA survival differences (zero without a counterparty), Q
+            const float de = z.x * ep;
             ep8[i] = ep;
             if (q8 + i < paths) {
-              s[0] += e, s[1] += ep, s[2] += en, s[3] += de, s[4] = fmaf(D, en, s[4]);
-              if (cvaDate) {
-                s[5] = fmaf(de, st[(3 + qc) * kBasisPaths + p], s[5]);
-                s[6] = fmaf(de, st[(5 + qc) * kBasisPaths + p], s[6]);
-              }
+              s[0] += e, s[1] += ep, s[2] += en, s[3] += de, s[4] = fmaf(z.x, en, s[4]);
+              if (rs > 0) s[5] = fmaf(de, z.y, s[5]), s[6] = fmaf(de, z.z, s[6]);
             }
           }
           umma::st8(tl + kColHeld + p0, hs);
-          if (rs > 0 && nsLive) {
-            float* dst = rowEP + static_cast<size_t>(rs - 1) * nP + first + q8;
+          if (rowJ) {
+            float* dst = rowJ + p0;
             if (vecRows && q8 + 8 <= paths) {
               reinterpret_cast<float4*>(dst)[0] = make_float4(ep8[0], ep8[1], ep8[2], ep8[3]);
               reinterpret_cast<float4*>(dst)[1] = make_float4(ep8[4], ep8[5], ep8[6], ep8[7]);
@@ -442,11 +448,11 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
         const float cva = rs > 0 ? s[5] + fwd[u] : 0.0f;
         if (rs > 0) fwd[u] = s[6];
         if (nsLive) {
-          const float* us = st + 7 * kBasisPaths + (p00 >> 5) * 4;
+          const float* us = st + 12 * kBasisPaths + (p00 >> 5) * 4;
           const uint32_t unit = tile * 4u + (p00 >> 5);
           float4* pt = reinterpret_cast<float4*>(partials + (static_cast<size_t>(unit) * nT + j) * kStatsPerDate);
           pt[0] = make_float4(s[0], s[1], s[2], s[3]);
-          pt[1] = make_float4(s[4], cva, hasQ ? us[1 + qc] : us[3], us[0]);
+          pt[1] = make_float4(s[4], cva, us[hasQ ? 1 + qc : 3], us[0]);
         }
       }
       __syncwarp();
