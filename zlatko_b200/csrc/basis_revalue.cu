@@ -414,13 +414,12 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
           for (int i = 0; i < 8; ++i) {
             const uint32_t p = p0 + i;
             const float v = __uint_as_float(r[i]) * scJ, vPrev = __uint_as_float(r[8 + i]) * scP;
-            float held = __uint_as_float(r[16 + i]), collateral = 0.0f;
-            if (hasCsa) {  // cash, the margin call at t - MPR, at most one date back
-              const float vc = callJ != j ? vPrev : v;
-              const float required = fmaxf(vc - hc, 0.0f) + fminf(vc + hbEff, 0.0f);
-              if (fabsf(required - held) >= mtaJ) held = required;
-              collateral = held + ia;
-            }
+            // cash, the margin call at t - MPR, at most one date back; without a CSA the state runs and is not used
+            float held = __uint_as_float(r[16 + i]);
+            const float vc = callJ != j ? vPrev : v;
+            const float required = fmaxf(vc - hc, 0.0f) + fminf(vc + hbEff, 0.0f);
+            held = fabsf(required - held) >= mtaJ ? required : held;
+            const float collateral = hasCsa ? held + ia : 0.0f;
             hs[i] = __float_as_uint(held);
             const float e = v - collateral, ep = fmaxf(e, 0.0f), en = fminf(e, 0.0f);
             const float4 z = cs[p];  // D, the CVA survival differences (zero without a counterparty), Q
