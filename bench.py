@@ -734,9 +734,9 @@ def main():
     nA, nC = int(plans[0].header[2]), int(plans[0].header[3])
     nF = (int(plans[0].header[10]) - 6) // 2
     cube_bytes = (2 + nA + nC + nF) * nT * nP * 4  # factor state read once (L2 serves the other netting sets)
-    # statistics partials: one per 32-path unit on the basis kernel, one per revalue warp term by term
+    # statistics partials: one per 64 paths on the basis kernel, one per revalue warp term by term
     nb = int(info.num_basis_netting_sets)
-    units = [-(-nP // 32) if k < nb else -(-nP // (32 * (int(info.tile_paths) // 128))) for k in range(len(plans))]
+    units = [-(-nP // 64) if k < nb else -(-nP // (32 * (int(info.tile_paths) // 128))) for k in range(len(plans))]
     alg_bytes = (sum(p.rows_total * nP * 4 + u * nT * p.stats_per_date * 4 for p, u in zip(plans, units)) + info.table_bytes +
                  cube_bytes + int(info.basis_bytes))
     # the basis kernel's products: per 128-path tile and column, C_hi Phi_hi + C_hi Phi_lo + C_lo Phi_hi over 128 rows

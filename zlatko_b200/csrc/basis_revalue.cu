@@ -17,8 +17,8 @@
 //   Consumers (warps 8-15).  Warp (lane quarter q, path half h) takes netting sets 32 q + lane over paths
 //   [64 h, 64 h + 64) in order: the netted value (the accumulator x the date's power-of-two scale), the margin call
 //   on the previous date's value (the previous accumulator, kept: three accumulators rotate) and the collateral
-//   held (TMEM columns 384..511), the exposure row and the date's 8 statistics summed over each 32-path unit --
-//   the unit's partial, no shuffles.  The CVA increment 0.5 (DE' + DE)(Q' - Q) between reporting dates is summed as
+//   held (TMEM columns 384..511), the exposure row and the date's 8 statistics summed over its 64 paths in order --
+//   the partial of the 64 paths, no shuffles.  The CVA increment 0.5 (DE' + DE)(Q' - Q) between reporting dates is summed as
 //   0.5 DE (Q - Q_next) on the earlier date (the next survival staged by the producers) plus 0.5 DE (Q' - Q) on
 //   the later one, so no per-path state carries the previous DE.
 //
@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
       const float mtaJ = j == 0 ? -1.0f : mta;  // date 0 always calls
       float* const rowJ = rs > 0 && nsLive ? rowEP + static_cast<size_t>(rs - 1) * nP + tile * kBasisPaths : nullptr;
 #pragma unroll 1
+      float h8[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};  // the warp's 64 paths: its two units in order
       for (uint32_t u = 0; u < 2; ++u) {
         const uint32_t p00 = half * 64u + u * 32u;  // the unit's first path in the tile
         const uint32_t first = tile * kBasisPaths + p00;
@@ -446,13 +447,16 @@ __global__ void __launch_bounds__(kThreads, 1) basisRevalueKernel(const BasisArg
         umma::waitSt();  // the unit's collateral held, in TMEM before the next date reads it
         const float cva = rs > 0 ? s[5] + fwd[u] : 0.0f;
         if (rs > 0) fwd[u] = s[6];
-        if (nsLive) {
-          const float* us = st + 12 * kBasisPaths + (p00 >> 5) * 4;
-          const uint32_t unit = tile * 4u + (p00 >> 5);
-          float4* pt = reinterpret_cast<float4*>(partials + (static_cast<size_t>(unit) * nT + j) * kStatsPerDate);
-          pt[0] = make_float4(s[0], s[1], s[2], s[3]);
-          pt[1] = make_float4(s[4], cva, us[hasQ ? 1 + qc : 3], us[0]);
-        }
+        const float* us = st + 12 * kBasisPaths + (p00 >> 5) * 4;
+        h8[0] += s[0], h8[1] += s[1], h8[2] += s[2], h8[3] += s[3], h8[4] += s[4], h8[5] += cva;
+        h8[6] += us[hasQ ? 1 + qc : 3], h8[7] += us[0];
+      }
+      // one partial per 64 paths (the reduce kernel's two-paths-per-lane layout): written when its first path is live
+      if (nsLive && tile * kBasisPaths + half * 64u < nP) {
+        const uint32_t unit = tile * 2u + half;
+        float4* pt = reinterpret_cast<float4*>(partials + (static_cast<size_t>(unit) * nT + j) * kStatsPerDate);
+        pt[0] = make_float4(h8[0], h8[1], h8[2], h8[3]);
+        pt[1] = make_float4(h8[4], h8[5], h8[6], h8[7]);
       }
       __syncwarp();
       umma::fenceBeforeSync();

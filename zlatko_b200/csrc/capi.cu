@@ -543,7 +543,7 @@ struct Batch {
   std::vector<Dev> dev;
   size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
   size_t basisArgsOff = 0, numGroups = 0;  // BasisArgs of every launch's groups
-  std::vector<uint8_t> onBasis;          // per plan: runs on the basis kernel (its partials have one path per lane)
+  std::vector<uint8_t> onBasis;          // per plan: runs on the basis kernel (its partials cover 64 paths each)
   size_t inputBytes = 0, totalBytes = 0, outBegin = 0, outBytes = 0;
   uint32_t numRowJobs = 0, maxReduceN = 0;
   int ppt = 2;                        // paths per revalue thread: the tile shape (autotuned by zk_batch_create)
@@ -1003,9 +1003,9 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
     const size_t i = B.jobOrder[o];  // plan order, or wave by wave when the batch runs in waves
     const auto& P = B.plans[i];
     const auto& D = B.dev[i];
-    // pad: 1 for a basis plan (one path per lane in its partials), 0 for the batch's tile shape
+    // pad: 2 for a basis plan (a partial per 64 paths), 0 for the batch's tile shape
     red[o] = {static_cast<const R*>(dptr(D.partials)), static_cast<R*>(dptr(D.sums)), P.nT * P.nS, numTilesOf(P.nP, 1), P.nP,
-              B.onBasis[i] ? 1u : 0u};
+              B.onBasis[i] ? 2u : 0u};
     B.maxReduceN = std::max(B.maxReduceN, P.nT * P.nS);
     for (size_t q = 0; q < P.nReq; ++q)
       rows.push_back({static_cast<const R*>(dptr(D.expo)), static_cast<const R*>(dptr(D.req + q * kRequestStride * sizeof(R))),

@@ -387,8 +387,8 @@ __global__ void reduceKernel(const ReduceJob<R>* __restrict__ jobs) {
   const ReduceJob<R> J = jobs[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= J.n) return;
-  // A job with pad 1 has one path per lane whatever the batch's shape (the basis kernel's 32-path units).
-  const uint32_t ppt = J.pad == 1u ? 1u : static_cast<uint32_t>(PPT);
+  // A job with pad 1 or 2 has partials of 32 or 64 paths whatever the batch's shape (the basis kernel's: 64).
+  const uint32_t ppt = J.pad == 1u || J.pad == 2u ? J.pad : static_cast<uint32_t>(PPT);
   const uint32_t kUnits = 4 / ppt, kUnitPaths = 32 * ppt;
   auto unit = [&](uint32_t u) { return u * kUnitPaths < J.nP ? J.partials[static_cast<size_t>(u) * J.n + i] : R(0); };
   double sum = 0.0, comp = 0.0;

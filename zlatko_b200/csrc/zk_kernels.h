@@ -76,7 +76,7 @@ struct ReduceJob {
   const R* partials;
   R* sums;
   uint32_t n, numTiles, nP;
-  uint32_t pad;  // 1: partials of one path per lane (the basis kernel's), whatever the launch's tile shape
+  uint32_t pad;  // 1 / 2: partials of 32 / 64 paths (the basis kernel's: 64), whatever the launch's tile shape
 };
 template <typename R>
 cudaError_t launchReduce(const ReduceJob<R>* jobs, uint32_t numJobs, uint32_t maxN, int ppt, cudaStream_t stream);
