@@ -6,7 +6,9 @@
  *   orc_fit_amc                     fitAmc (src/gpu/fused_exposure.cpp:103-156): the policy and continuation
  *                                   coefficients of a plan's Bermudans, fitted in double precision on the
  *                                   single-precision states of the AMC pass (runAmcStates), backwards over the
- *                                   exercise dates.
+ *                                   exercise dates;
+ *   orc_reg2_fit / orc_reg2_predict the two-regressor basis of this library (short rate and co-terminal swap
+ *                                   rate), an extension with no reference code behind it (oracle.h).
  * The sums run in path order, as the reference's, so the fitted coefficients are the reference's bits. */
 #include <math.h>
 #include <stdio.h>
@@ -96,6 +98,84 @@ double orc_reg_predict(const orc_regression* r, double x) {
   const double z = (x - r->center) / r->scale;
   double v = 0.0;
   for (int d = r->ncoef; d-- > 0;) v = v * z + r->coef[d];
+  return v;
+}
+
+int orc_basis2(double z, double w, int degree, double* out) {
+  const double v[10] = {1.0, z, w, z * z, z * w, w * w, z * z * z, z * z * w, z * w * w, w * w * w};
+  const int count = degree <= 0 ? 1 : degree == 1 ? 3 : degree == 2 ? 6 : 10;
+  for (int i = 0; i < 10; ++i) out[i] = i < count ? v[i] : 0.0;
+  return count;
+}
+
+void orc_reg2_fit(orc_regression2* r, int degree, const double* x, const double* s, const double* y, const unsigned char* mask,
+                  size_t n) {
+  size_t count = 0;
+  double sx = 0.0, sxx = 0.0, ss = 0.0, sss = 0.0, sy = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    if (mask && !mask[i]) continue;
+    ++count;
+    sx += x[i], sxx += x[i] * x[i], ss += s[i], sss += s[i] * s[i], sy += y[i];
+  }
+  memset(r, 0, sizeof *r);
+  r->sx = r->ss = 1.0;
+  if (count == 0) {
+    r->degree = -1;
+    return;
+  }
+  const double cnt = (double)count;
+  r->cx = sx / cnt, r->cs = ss / cnt;
+  const double vx = sxx / cnt - r->cx * r->cx, vs = sss / cnt - r->cs * r->cs;
+  r->sx = sqrt(vx > 0.0 ? vx : 0.0), r->ss = sqrt(vs > 0.0 ? vs : 0.0);
+  int deg = degree;
+  if (r->sx < 1e-12 * (fabs(r->cx) > 1.0 ? fabs(r->cx) : 1.0) || r->ss < 1e-12 * (fabs(r->cs) > 1.0 ? fabs(r->cs) : 1.0)) deg = 0;
+  while (deg > 0 && cnt < 2.0 * (deg == 1 ? 3 : deg == 2 ? 6 : 10)) --deg;
+  if (deg == 0) {
+    r->sx = r->ss = 1.0, r->cx = r->cs = 0.0, r->coef[0] = sy / cnt, r->degree = 0;
+    return;
+  }
+  double A[100] = {0}, b[10] = {0}, row[10];
+  const int k = orc_basis2(0.0, 0.0, deg, row);
+  for (size_t i = 0; i < n; ++i) {
+    if (mask && !mask[i]) continue;
+    orc_basis2((x[i] - r->cx) / r->sx, (s[i] - r->cs) / r->ss, deg, row);
+    for (int a = 0; a < k; ++a) {
+      b[a] += row[a] * y[i];
+      for (int c = 0; c <= a; ++c) A[a * 10 + c] += row[a] * row[c];
+    }
+  }
+  /* The two regressors can be nearly collinear (in a one-factor model the swap rate is a smooth function of the short
+   * rate; the graded Gram's condition number then reaches 1e17): a ridge of 1e-6 n on the standardised basis keeps the
+   * solution stable to the summation order (predictions to ~1e-11) at a negligible bias where the data are
+   * well conditioned (eigenvalues O(n)). */
+  const double ridge = 1e-6 * cnt;
+  double L[100] = {0}, z[10];
+  for (int a = 0; a < k; ++a) A[a * 10 + a] += ridge;
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double v = A[i * 10 + j];
+      for (int m = 0; m < j; ++m) v -= L[i * 10 + m] * L[j * 10 + m];
+      L[i * 10 + j] = i == j ? sqrt(v > 0.0 ? v : 1.0) : v / L[j * 10 + j];
+    }
+  for (int i = 0; i < k; ++i) {
+    double v = b[i];
+    for (int j = 0; j < i; ++j) v -= L[i * 10 + j] * z[j];
+    z[i] = v / L[i * 10 + i];
+  }
+  for (int i = k; i-- > 0;) {
+    double v = z[i];
+    for (int j = i + 1; j < k; ++j) v -= L[j * 10 + i] * r->coef[j];
+    r->coef[i] = v / L[i * 10 + i];
+  }
+  r->degree = deg;
+}
+
+double orc_reg2_predict(const orc_regression2* r, double x, double s) {
+  if (r->degree < 0) return 0.0;
+  double row[10];
+  const int k = orc_basis2((x - r->cx) / r->sx, (s - r->cs) / r->ss, r->degree, row);
+  double v = 0.0;
+  for (int i = 0; i < k; ++i) v += r->coef[i] * row[i];
   return v;
 }
 

@@ -474,6 +474,17 @@ static void value_at(const Model* m, const Trade* tr, const Grid* g, size_t j, c
 #undef FOREIGN_BOND
 }
 
+/* The co-terminal swap rate of a tail swap at time t on short-rate state x: (P(t, T_0) - P(t, T_n)) / sum_i tau_i
+ * P(t, T_i) over its schedule T_0 < .. < T_n -- the second regressor of the two-regressor basis (an extension of the
+ * reference, whose regression is on x alone). */
+static double coterminal_rate(const Model* m, const Trade* tail, double t, double x) {
+  double ann = 0.0;
+  for (size_t i = 1; i < tail->nSched; ++i)
+    ann += (tail->sched[i] - tail->sched[i - 1]) * hw_bond(&m->hw, t, tail->sched[i], x);
+  const double flt = hw_bond(&m->hw, t, tail->sched[0], x) - hw_bond(&m->hw, t, tail->sched[tail->nSched - 1], x);
+  return ann > 0.0 ? flt / ann : 0.0;
+}
+
 /* A Bermudan swaption on every path and date (bermudan_swaption.cpp:49-146): exercise values of the tail swaps,
  * backward Longstaff-Schwartz over the exercise dates on the short-rate state, first exercise per path, then
  * on every date the tail swap (exercised, physical), nothing (exercised, cash) or the regressed continuation. */
@@ -496,17 +507,24 @@ static void bermudan_cube(const Model* m, const Trade* tr, const Grid* g, const 
   double* x = (double*)malloc(nP * sizeof(double));
   unsigned char* itm = (unsigned char*)malloc(nP);
   orc_regression reg;
+  orc_regression2 reg2;
+  /* degree >= 10: the two-regressor basis of degree - 10 on (x, co-terminal swap rate) */
+  const int twoD = tr->degree >= 10, deg = twoD ? tr->degree - 10 : tr->degree;
+  double* sw = (double*)malloc(nP * sizeof(double));
   for (size_t k = nE; k-- > 0;) {
     const size_t j = jEx[k];
     for (size_t p = 0; p < nP; ++p) {
       x[p] = X[p * nT + j];
       target[p] = realised[p] / Dm[p * nT + j];
       itm[p] = exValue[k * nP + p] > 0.0;
+      if (twoD) sw[p] = coterminal_rate(m, &tails[k], g->t[j], x[p]);
     }
-    orc_reg_fit(&reg, tr->degree, x, target, itm, nP);
+    if (twoD) orc_reg2_fit(&reg2, deg, x, sw, target, itm, nP);
+    else orc_reg_fit(&reg, deg, x, target, itm, nP);
     for (size_t p = 0; p < nP; ++p) {
       const double e = exValue[k * nP + p];
-      if (e > 0.0 && e > orc_reg_predict(&reg, x[p])) exercise[k * nP + p] = 1, realised[p] = Dm[p * nT + j] * e;
+      const double c = twoD ? orc_reg2_predict(&reg2, x[p], sw[p]) : orc_reg_predict(&reg, x[p]);
+      if (e > 0.0 && e > c) exercise[k * nP + p] = 1, realised[p] = Dm[p * nT + j] * e;
     }
     memcpy(strategy + k * nP, realised, nP * sizeof(double));
   }
@@ -524,10 +542,14 @@ static void bermudan_cube(const Model* m, const Trade* tr, const Grid* g, const 
     size_t nextK = 0;
     while (nextK < nE && tr->ex[nextK] <= t + 1e-10) ++nextK;
     if (nextK < nE) {
-      for (size_t p = 0; p < nP; ++p) x[p] = X[p * nT + j], target[p] = strategy[nextK * nP + p] / Dm[p * nT + j];
-      orc_reg_fit(&reg, tr->degree, x, target, NULL, nP);
       for (size_t p = 0; p < nP; ++p) {
-        const double c = orc_reg_predict(&reg, x[p]);
+        x[p] = X[p * nT + j], target[p] = strategy[nextK * nP + p] / Dm[p * nT + j];
+        if (twoD) sw[p] = coterminal_rate(m, &tails[nextK], t, x[p]);
+      }
+      if (twoD) orc_reg2_fit(&reg2, deg, x, sw, target, NULL, nP);
+      else orc_reg_fit(&reg, deg, x, target, NULL, nP);
+      for (size_t p = 0; p < nP; ++p) {
+        const double c = twoD ? orc_reg2_predict(&reg2, x[p], sw[p]) : orc_reg_predict(&reg, x[p]);
         cont[p] = c > 0.0 ? c : 0.0;
       }
     } else {
@@ -545,7 +567,7 @@ static void bermudan_cube(const Model* m, const Trade* tr, const Grid* g, const 
   }
   for (size_t k = 0; k < nE; ++k) free(tails[k].sched);
   free(tails), free(jEx), free(exValue), free(strategy), free(exercise), free(realised), free(target), free(x);
-  free(itm), free(cont), free(tailv);
+  free(itm), free(cont), free(tailv), free(sw);
 }
 
 static double required_collateral(double v, double hc, double ho) {

@@ -74,6 +74,21 @@ static float amc_poly(const float* rec, float x) {
   return ((rec[7] * z + rec[6]) * z + rec[5]) * z + rec[4];
 }
 
+/* The regression of a policy / continuation record: the polynomial above in x or, when extension records (kind 15)
+ * follow it, the two-regressor basis of this library (an extension with no reference code behind it) in x and the
+ * co-terminal swap rate s = flt / ann summed from the annuity (13) and float-leg (14) records before it: cx, 1 / sx,
+ * cs, 1 / ss, c0, c1 in the record, c2..c8 in the first extension's fields 1..7, c9 in the second's field 1. */
+static float amc_value(const float* rec, int twoD, float x, float ann, float flt) {
+  if (!twoD) return amc_poly(rec, x);
+  const float* e1 = rec + TERM;
+  const float* e2 = rec + 2 * TERM;
+  const float s = ann != 0.0f ? flt / ann : 0.0f;
+  const float z = (x - rec[2]) * rec[3], w = (s - rec[4]) * rec[5];
+  const float zz = z * z, zw = z * w, ww = w * w;
+  return rec[6] + rec[7] * z + e1[1] * w + e1[2] * zz + e1[3] * zw + e1[4] * ww + e1[5] * zz * z + e1[6] * zz * w +
+         e1[7] * zw * w + e2[1] * ww * w;
+}
+
 typedef struct PlanS {
   const uint32_t *H, *I;
   const float *FP, *ST, *T;
@@ -168,7 +183,7 @@ static void simulate_path(const Plan* v, uint32_t p, float* stats, float* expo, 
       if (v->nC > 0) Q = expf(-Y[v->cpty] - step[20 + v->cpty]);
     }
 
-    float value = 0.0f, vt[MAX_TRADES], ev[MAX_BERM] = {0, 0, 0, 0};
+    float value = 0.0f, vt[MAX_TRADES], ev[MAX_BERM] = {0, 0, 0, 0}, ann = 0.0f, flt = 0.0f;
     memset(vt, 0, sizeof vt);
     const uint32_t nTr = v->nTr < MAX_TRADES ? v->nTr : MAX_TRADES;
     if (sink) sink->x[(size_t)j * sink->nP + p] = x, sink->deflator[(size_t)j * sink->nP + p] = D;
@@ -193,15 +208,24 @@ static void simulate_path(const Plan* v, uint32_t p, float* stats, float* expo, 
           break;
         }
         case 5: ev[bm] += c * bond; break;
-        case 6:
+        case 6: {
+          const int twoD = t + 1 < v->I[j + 1] && ((uint32_t)rec[TERM] & 15u) == 15u;
           if (sink)
             sink->exercise[((size_t)sink->offsets[bm] + extra) * sink->nP + p] = ev[bm];
-          else if (exercised[bm] == NOT_EXERCISED && ev[bm] > 0.0f && ev[bm] > amc_poly(rec, x))
+          else if (exercised[bm] == NOT_EXERCISED && ev[bm] > 0.0f && ev[bm] > amc_value(rec, twoD, x, ann, flt))
             exercised[bm] = extra;
+          ann = flt = 0.0f;
           break;
-        case 7:
-          if (exercised[bm] == NOT_EXERCISED) term = rec[1] * maxf(amc_poly(rec, x), 0.0f);
+        }
+        case 7: {
+          const int twoD = t + 1 < v->I[j + 1] && ((uint32_t)rec[TERM] & 15u) == 15u;
+          if (exercised[bm] == NOT_EXERCISED) term = rec[1] * maxf(amc_value(rec, twoD, x, ann, flt), 0.0f);
+          ann = flt = 0.0f;
           break;
+        }
+        case 13: ann += c * bond; break;
+        case 14: flt += c * bond; break;
+        case 15: break;
         case 8:
           if (exercised[bm] != NOT_EXERCISED && exercised[bm] <= extra) term = c * bond;
           break;

@@ -42,6 +42,22 @@ typedef struct orc_regression {
 void orc_reg_fit(orc_regression* r, int degree, const double* x, const double* y, const unsigned char* mask, size_t n);
 double orc_reg_predict(const orc_regression* r, double x);
 
+/* The two-regressor basis (an extension of the reference, whose regression is on the short rate alone; no reference
+ * code pins it): the graded monomials of total degree <= 3 in the standardised short rate z and co-terminal swap
+ * rate w -- 1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3 -- fitted by the normal equations with the ridge 1e-6 n,
+ * solved by Cholesky.  The degree falls to 0 (the mean) when either regressor is degenerate and while the samples
+ * are fewer than twice the basis. */
+typedef struct orc_regression2 {
+  double cx, sx, cs, ss;  /* centers and scales */
+  double coef[10];        /* graded order; zero beyond the degree */
+  int degree;             /* -1: no sample (predicts 0) */
+} orc_regression2;
+void orc_reg2_fit(orc_regression2* r, int degree, const double* x, const double* s, const double* y, const unsigned char* mask,
+                  size_t n);
+double orc_reg2_predict(const orc_regression2* r, double x, double s);
+/* The basis of degree <= 3 at (z, w), graded, into out[10] (zero beyond the degree); the number of functions. */
+int orc_basis2(double z, double w, int degree, double* out);
+
 /* fitAmc (fused_exposure.cpp:103-156): fills the policy and continuation records of terms in place, from the
  * AMC pass of the plan; degrees[b] is the regression degree of Bermudan b. */
 int orc_fit_amc(const uint32_t* header, const uint32_t* indices, const float* params, const float* steps, float* terms,

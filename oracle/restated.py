@@ -49,6 +49,8 @@ def lib() -> C.CDLL:
         L.orc_amc_states.argtypes = [_up, _up, _fp, _fp, _fp, C.c_uint32, _up, _fp, _fp, _fp, C.c_char_p, sz]
         L.orc_reg_fit.restype = None
         L.orc_reg_fit.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_void_p, sz]
+        L.orc_reg2_fit.restype = None
+        L.orc_reg2_fit.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p, sz]
         L.orc_fit_amc.restype = C.c_int
         L.orc_fit_amc.argtypes = [_up, _up, _fp, _fp, _fp, C.c_uint32, _up, sz, C.c_char_p, sz]
         L.orc_engine_run.restype = C.c_int
@@ -142,6 +144,100 @@ def fit_regression(x, y, degree: int, mask=None) -> dict:
     r = _Regression()
     lib().orc_reg_fit(C.byref(r), degree, xs, ys, None if m is None else m.ctypes.data_as(C.c_void_p), xs.size)
     return {"center": r.center, "scale": r.scale, "ncoef": r.ncoef, "coef": list(r.coef)[: r.ncoef]}
+
+
+class _Regression2(C.Structure):
+    _fields_ = [("cx", C.c_double), ("sx", C.c_double), ("cs", C.c_double), ("ss", C.c_double),
+                ("coef", C.c_double * 10), ("degree", C.c_int)]
+
+
+def fit_regression2(x, s, y, degree: int, mask=None) -> dict:
+    """The two-regressor basis (orc_reg2_fit, this library's extension): centers, scales, the 10 graded coefficients
+    in the standardised regressors and the degree used (-1: no sample)."""
+    xs, ss, ys = (np.ascontiguousarray(a, np.float64) for a in (x, s, y))
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    r = _Regression2()
+    lib().orc_reg2_fit(C.byref(r), degree, xs, ss, ys, None if m is None else m.ctypes.data_as(C.c_void_p), xs.size)
+    return {"cx": r.cx, "sx": r.sx, "cs": r.cs, "ss": r.ss, "coef": np.array(list(r.coef)), "degree": r.degree}
+
+
+def predict_regression2(r: dict, x, s) -> np.ndarray:
+    """orc_reg2_predict over arrays: sum_i coef[i] basis_i in graded order (1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2,
+    w^3), the terms beyond the degree zero."""
+    if r["degree"] < 0:
+        return np.zeros(np.shape(x))
+    z, w = (np.asarray(x, np.float64) - r["cx"]) / r["sx"], (np.asarray(s, np.float64) - r["cs"]) / r["ss"]
+    rows = [np.ones_like(z), z, w, z * z, z * w, w * w, z * z * z, z * z * w, z * w * w, w * w * w]
+    count = {0: 1, 1: 3, 2: 6}.get(r["degree"], 10)
+    v = np.zeros_like(z)
+    for i in range(count):
+        v = v + r["coef"][i] * rows[i]
+    return v
+
+
+def fit_amc2(plan, degrees) -> np.ndarray:
+    """fitAmc (src/gpu/fused_exposure.cpp:103-156) extended to the two-regressor basis of this library, on the
+    oracle's AMC pass (amc_states): the Bermudans whose policy / continuation records are followed by extension
+    records (kind 15) regress on the short rate x and the co-terminal swap rate s = sum_14 c A e^{-B x} /
+    sum_13 c A e^{-B x} over the annuity (13) and float-leg (14) records before each record; the others are fitted
+    by fit_amc.  Records: cx, 1 / sx, cs, 1 / ss, c0, c1; c2..c8 in the first extension record's fields 1..7, c9 in
+    the second's field 1.  At most 4 Bermudans (the code's Bermudan field)."""
+    terms = fit_amc(plan, degrees).reshape(-1, 8)
+    x, D, E = amc_states(plan)
+    off = exercise_offsets(plan.terms)
+    nT = plan.num_dates
+    ind = np.asarray(plan.indices, np.int64)[: nT + 1]
+    code = terms[:, 0].astype(np.int64)
+    kind = code & 15
+    date_of = np.repeat(np.arange(nT), np.diff(ind))
+    decide, cont = {}, {}
+    for t in np.flatnonzero((kind == 6) | (kind == 7)):
+        b = min((int(code[t]) >> 8) & 15, 3)
+        if t + 1 >= ind[date_of[t] + 1] or kind[t + 1] != 15:
+            continue
+        if kind[t] == 6:
+            decide.setdefault(b, {})[int(code[t]) >> 12] = (int(t), int(date_of[t]))
+        else:
+            cont.setdefault(b, {})[int(date_of[t])] = int(t)
+
+    def swap_rate(t, xs):
+        u = t
+        while u > ind[date_of[t]] and kind[u - 1] in (13, 14):
+            u -= 1
+        ann, flt = np.zeros_like(xs), np.zeros_like(xs)
+        for q in range(u, t):
+            c, A, B = (float(v) for v in terms[q, 2:5])
+            if kind[q] == 13:
+                ann = ann + c * (A * np.exp(-B * xs))
+            else:
+                flt = flt + c * (A * np.exp(-B * xs))
+        return np.where(ann != 0.0, flt / np.where(ann != 0.0, ann, 1.0), 0.0)
+
+    def write(t, r):
+        rec = terms[t]
+        rec[2], rec[3], rec[4], rec[5] = r["cx"], 1.0 / r["sx"], r["cs"], 1.0 / r["ss"]
+        rec[6], rec[7] = r["coef"][0], r["coef"][1]
+        terms[t + 1, 1:8] = r["coef"][2:9]
+        terms[t + 2, 1] = r["coef"][9]
+
+    for b, dec in decide.items():
+        nE = len(dec)
+        realised = np.zeros(plan.num_paths)
+        for k in range(nE - 1, -1, -1):
+            t, j = dec[k]
+            xs, Dj = x[j].astype(np.float64), D[j].astype(np.float64)
+            e = E[off[b] + k].astype(np.float64)
+            s = swap_rate(t, xs)
+            r = fit_regression2(xs, s, realised / Dj, int(degrees[b]), e > 0.0)
+            write(t, r)
+            go = (e > 0.0) & (e > predict_regression2(r, xs, s))
+            realised[go] = Dj[go] * e[go]
+            lo = dec[k - 1][1] if k > 0 else 0
+            for jc, tc in sorted(cont.get(b, {}).items()):
+                if lo <= jc < j:
+                    xc, Dc = x[jc].astype(np.float64), D[jc].astype(np.float64)
+                    write(tc, fit_regression2(xc, swap_rate(tc, xc), realised / Dc, int(degrees[b])))
+    return terms.reshape(-1)
 
 
 def fit_amc(plan, degrees) -> np.ndarray:

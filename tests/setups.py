@@ -42,8 +42,9 @@ def gpu_setup(paths: int, csa: bool):
 
 
 def bermudan(notional=1e6, fixed=0.03, pay=False, start=1.0, tenor=4.0, exercise=(1.0, 2.0, 3.0), physical=True,
-             position=1.0, degree=3) -> S.Bermudan:
-    return S.Bermudan(S.Swap(notional, fixed, pay, S.vanilla_schedule(start, tenor, 1)), list(exercise), physical, position, degree)
+             position=1.0, degree=3, basis="rate") -> S.Bermudan:
+    return S.Bermudan(S.Swap(notional, fixed, pay, S.vanilla_schedule(start, tenor, 1)), list(exercise), physical, position, degree,
+                      basis)
 
 
 def swap_book(n: int, seed: int = 20261203, horizon_months: int = 60, csa=None) -> S.NettingSet:

@@ -30,11 +30,14 @@ constexpr int kFitThreads = 512;
 constexpr int kFitWarps = kFitThreads / 32;
 constexpr int kMomentVals = 4;   // count, sum x, sum x^2, sum y
 constexpr int kGramVals = 14;    // 10 Gram entries (lower triangle, degree 3) + 4 right-hand sides
+// The two-regressor basis: 55 Gram entries (lower triangle of 10) + 10 right-hand sides, summed in two passes of
+// kHalf2 values each (a thread's sums stay in registers).
+constexpr int kGram2 = 65, kHalf2 = 33;
 
 struct FitSmem {
-  double warpBuf[kFitWarps][kGramVals];
-  double part[kGramVals];   // this CTA's sums
-  double res[8];            // rank 0: center, scale, degree, c0..c3, status
+  double warpBuf[kFitWarps][kHalf2];
+  double part[kHalf2];      // this CTA's sums
+  double res[16];           // rank 0: 1D center, scale, degree, c0..c3, status; 2D cx, sx, cs, ss, c0..c9, degree
 };
 
 // Sums V values over the CTA: a fixed shuffle tree per warp, then the warps in order.
@@ -188,14 +191,172 @@ __device__ void fitOnce(cg::cluster_group& cl, FitSmem& s, double* res, const R*
   // rank 0 overwrite res before every CTA has copied it: the syncs of the next fit order both.
 }
 
+// ---- the two-regressor basis (this library's extension: the reference regresses on x alone) ----
+
+// The co-terminal swap rate of a path from its short rate, over the slot's bonds in plan order (as the fused
+// kernel forms it: annuity and float leg each summed term by term, then their ratio).
+__device__ __forceinline__ double swapRateOf(const double4* __restrict__ b, uint2 range, double x) {
+  double ann = 0.0, flt = 0.0;
+  for (uint32_t i = 0; i < range.y; ++i) {
+    const double4 q = b[range.x + i];
+    const double v = q.y * (q.z * exp(-q.w * x));
+    if (q.x == 13.0) ann += v;
+    else flt += v;
+  }
+  return ann != 0.0 ? flt / ann : 0.0;
+}
+
+// The graded monomials 1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3 (zero beyond `count`).
+__device__ __forceinline__ void basis2(double z, double w, int count, double (&m)[10]) {
+  const double v[10] = {1.0, z, w, z * z, z * w, w * w, z * z * z, z * z * w, z * w * w, w * w * w};
+#pragma unroll
+  for (int i = 0; i < 10; ++i) m[i] = i < count ? v[i] : 0.0;
+}
+
+__device__ __forceinline__ int basisCount2(int d) { return d <= 0 ? 1 : d == 1 ? 3 : d == 2 ? 6 : 10; }
+
+// res: cx, sx, cs, ss, c0..c9, degree (-1: no sample, predicts 0)
+__device__ __forceinline__ double predict2(const double* res, double x, double s) {
+  const int d = static_cast<int>(res[14]);
+  if (d < 0) return 0.0;
+  double m[10];
+  basis2((x - res[0]) / res[1], (s - res[2]) / res[3], basisCount2(d), m);
+  double v = 0.0;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) v += res[4 + i] * m[i];
+  return v;
+}
+
+// One pass of the two-regressor Gram: the sums [LO, LO + N) of the 65 (Gram lower triangle, then X^T y); with the
+// loops unrolled every index is a constant, so the sums stay in registers.
+template <typename R, int LO, int N>
+__device__ __forceinline__ void gram2Pass(double (&g)[kHalf2], const R* __restrict__ X, const R* __restrict__ Dj,
+                                          const R* __restrict__ Ek, const double* __restrict__ realised, const double4* bonds,
+                                          uint2 range, const double* res, int count, uint32_t nP, uint32_t first, uint32_t stride) {
+#pragma unroll
+  for (int i = 0; i < kHalf2; ++i) g[i] = 0.0;
+  for (uint32_t p = first; p < nP; p += stride) {
+    if (Ek && !(Ek[p] > R(0))) continue;
+    const double x = static_cast<double>(X[p]);
+    double m[10];
+    basis2((x - res[0]) / res[1], (swapRateOf(bonds, range, x) - res[2]) / res[3], count, m);
+    const double y = realised[p] / static_cast<double>(Dj[p]);
+    int q = 0;
+#pragma unroll
+    for (int a = 0; a < 10; ++a) {
+#pragma unroll
+      for (int b = 0; b <= a; ++b, ++q)
+        if (q >= LO && q < LO + N) g[q - LO] += m[a] * m[b];
+    }
+#pragma unroll
+    for (int a = 0; a < 10; ++a, ++q)
+      if (q >= LO && q < LO + N) g[q - LO] += m[a] * y;
+  }
+}
+
+// One regression of y = realised / D on (x, s) over the cluster's paths (masked by E > 0 when E is given):
+// standardised regressors, degree 0 when either is degenerate, lower while the samples are fewer than twice the
+// basis, ridge 1e-6 n, FP64 Cholesky.  The ridge is larger than the one-regressor fit's: in a one-factor model the
+// swap rate is a smooth function of the short rate, the graded Gram's condition number reaches 1e17, and 1e-6 n keeps
+// the predictions stable to the summation order (~1e-11) at a negligible bias where the data are well conditioned.
+// Result in every CTA's `res` and, from rank 0, out[0..13] = cx, sx, cs, ss, c0..c9.
 template <typename R>
+__device__ void fitOnce2(cg::cluster_group& cl, FitSmem& s, double* res, const R* __restrict__ X, const R* __restrict__ Dj,
+                         const R* __restrict__ Ek, const double* __restrict__ realised, const double4* bonds, uint2 range,
+                         uint32_t nP, int degree, uint32_t first, uint32_t stride, double* out, uint32_t* err) {
+  __shared__ double tot[kGram2];
+  double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (uint32_t p = first; p < nP; p += stride) {  // count, sum x, sum x^2, sum s, sum s^2, sum y
+    if (Ek && !(Ek[p] > R(0))) continue;
+    const double x = static_cast<double>(X[p]), sw = swapRateOf(bonds, range, x);
+    m[0] += 1.0, m[1] += x, m[2] += x * x, m[3] += sw, m[4] += sw * sw, m[5] += realised[p] / static_cast<double>(Dj[p]);
+  }
+  blockSum<6>(m, s);
+  clusterSum<6>(cl, s, tot);
+  if (cl.block_rank() == 0 && threadIdx.x == 0) {
+    const double n = tot[0];
+    double* r = s.res;
+    for (int i = 0; i < 16; ++i) r[i] = 0.0;
+    r[1] = r[3] = 1.0;
+    if (n == 0.0) {
+      r[14] = -1.0;
+    } else {
+      r[0] = tot[1] / n, r[2] = tot[3] / n;
+      const double vx = tot[2] / n - r[0] * r[0], vs = tot[4] / n - r[2] * r[2];
+      r[1] = sqrt(vx > 0.0 ? vx : 0.0), r[3] = sqrt(vs > 0.0 ? vs : 0.0);
+      int d = degree;
+      if (r[1] < 1e-12 * fmax(1.0, fabs(r[0])) || r[3] < 1e-12 * fmax(1.0, fabs(r[2]))) d = 0;
+      while (d > 0 && n < 2.0 * basisCount2(d)) --d;
+      if (d == 0) r[0] = r[2] = 0.0, r[1] = r[3] = 1.0, r[4] = tot[5] / n;
+      r[14] = static_cast<double>(d);
+    }
+  }
+  cl.sync();
+  const double* r0 = cl.map_shared_rank(s.res, 0);
+  if (threadIdx.x < 16) res[threadIdx.x] = r0[threadIdx.x];
+  __syncthreads();
+  const int d = static_cast<int>(res[14]);
+  if (d > 0) {
+    const int count = basisCount2(d);
+    double g[kHalf2];
+    gram2Pass<R, 0, kHalf2>(g, X, Dj, Ek, realised, bonds, range, res, count, nP, first, stride);
+    blockSum<kHalf2>(g, s);
+    clusterSum<kHalf2>(cl, s, tot);
+    cl.sync();  // rank 0 has read every part before the second pass overwrites them
+    gram2Pass<R, kHalf2, kGram2 - kHalf2>(g, X, Dj, Ek, realised, bonds, range, res, count, nP, first, stride);
+    blockSum<kHalf2>(g, s);
+    clusterSum<kGram2 - kHalf2>(cl, s, tot + kHalf2);
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      double A[10][10], L[10][10] = {}, b[10], z[10], c[10] = {};
+      int q = 0;
+      for (int a = 0; a < 10; ++a)
+        for (int bb = 0; bb <= a; ++bb) A[a][bb] = A[bb][a] = tot[q++];
+      for (int a = 0; a < 10; ++a) b[a] = tot[55 + a];
+      const double n = tot[0];  // the Gram's first entry: sum 1 * 1, the sample count
+      for (int a = 0; a < count; ++a) A[a][a] += 1e-6 * n;
+      bool ok = true;
+      for (int i = 0; i < count; ++i)
+        for (int j = 0; j <= i; ++j) {
+          double v = A[i][j];
+          for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
+          if (i == j) {
+            if (!(v > 0.0)) ok = false, v = 1.0;
+            L[i][i] = sqrt(v);
+          } else {
+            L[i][j] = v / L[j][j];
+          }
+        }
+      for (int i = 0; i < count; ++i) {
+        double v = b[i];
+        for (int j = 0; j < i; ++j) v -= L[i][j] * z[j];
+        z[i] = v / L[i][i];
+      }
+      for (int i = count - 1; i >= 0; --i) {
+        double v = z[i];
+        for (int j = i + 1; j < count; ++j) v -= L[j][i] * c[j];
+        c[i] = v / L[i][i];
+      }
+      for (int i = 0; i < 10; ++i) s.res[4 + i] = c[i];
+      if (!ok) atomicExch(err, kDevBadTerm);
+    }
+    cl.sync();
+    if (threadIdx.x < 10) res[4 + threadIdx.x] = cl.map_shared_rank(s.res, 0)[4 + threadIdx.x];
+    __syncthreads();
+  }
+  if (cl.block_rank() == 0 && threadIdx.x == 0)
+    for (int i = 0; i < 14; ++i) out[i] = res[i];
+}
+
+// TwoD: the launch has two-regressor jobs (its one-regressor jobs run the same code as without).
+template <typename R, bool TwoD>
 __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __restrict__ jobs, const R* __restrict__ x,
                                                              const R* __restrict__ D, const R* __restrict__ E,
-                                                             const uint32_t* __restrict__ contDates, double* __restrict__ realised,
+                                                             const uint32_t* __restrict__ contDates, const double4* __restrict__ bonds,
+                                                             const uint2* __restrict__ bondRange, double* __restrict__ realised,
                                                              double* __restrict__ out, uint32_t* err) {
   cg::cluster_group cl = cg::this_cluster();
   __shared__ FitSmem s;
-  __shared__ double res[8];
+  __shared__ double res[16];
   const uint32_t job = blockIdx.x / cl.num_blocks();
   const AmcFitJob J = jobs[job];
   const uint32_t nP = J.nP, stride = cl.num_blocks() * kFitThreads, first = cl.block_rank() * kFitThreads + threadIdx.x;
@@ -204,20 +365,32 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
   for (int k = static_cast<int>(J.nE) - 1; k >= 0; --k) {
     const size_t j = J.exDate[k];
     const R* Ek = E + static_cast<size_t>(J.eRow + k) * nP;
-    fitOnce<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, nP, static_cast<int>(J.degree), first, stride,
-               out + static_cast<size_t>(J.slotBase + k) * 6, err);
+    const bool twoD = TwoD && J.twoD;
+    const uint2 rk = twoD ? bondRange[J.slotBase + k] : make_uint2(0, 0);
+    if (twoD)
+      fitOnce2<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, bonds, rk, nP, static_cast<int>(J.degree), first, stride,
+                  out + static_cast<size_t>(J.slotBase + k) * kFitOut, err);
+    else
+      fitOnce<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, nP, static_cast<int>(J.degree), first, stride,
+                 out + static_cast<size_t>(J.slotBase + k) * kFitOut, err);
     // Exercise where the exercise value beats the regression: realised = D e.
     for (uint32_t p = first; p < nP; p += stride) {
-      const double e = static_cast<double>(Ek[p]);
-      if (e > 0.0 && e > predict(res, static_cast<double>(x[j * nP + p]))) rz[p] = static_cast<double>(D[j * nP + p]) * e;
+      const double e = static_cast<double>(Ek[p]), xp = static_cast<double>(x[j * nP + p]);
+      const double c = twoD ? predict2(res, xp, swapRateOf(bonds, rk, xp)) : predict(res, xp);
+      if (e > 0.0 && e > c) rz[p] = static_cast<double>(D[j * nP + p]) * e;
     }
     // Continuation on the dates whose next exercise is k: exDate[k - 1] <= date < exDate[k].
     const uint32_t lo = k > 0 ? J.exDate[k - 1] : 0u;
     for (uint32_t i = 0; i < J.contCount; ++i) {
       const uint32_t jc = contDates[J.contBegin + i];
       if (jc < lo || jc >= j) continue;
-      fitOnce<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr), rz,
-                 nP, static_cast<int>(J.degree), first, stride, out + static_cast<size_t>(J.slotBase + J.nE + i) * 6, err);
+      double* oc = out + static_cast<size_t>(J.slotBase + J.nE + i) * kFitOut;
+      if (twoD)
+        fitOnce2<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr),
+                    rz, bonds, bondRange[J.slotBase + J.nE + i], nP, static_cast<int>(J.degree), first, stride, oc, err);
+      else
+        fitOnce<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr),
+                   rz, nP, static_cast<int>(J.degree), first, stride, oc, err);
     }
   }
   cl.sync();  // rank 0's shared memory stays alive until every CTA of the cluster is done reading it
@@ -227,7 +400,8 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
 
 template <typename R>
 cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
-                         double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream) {
+                         const double4* bonds, const uint2* bondRange, double* realised, double* out, uint32_t* err,
+                         uint32_t clusterSize, cudaStream_t stream) {
   if (numJobs == 0) return cudaSuccess;
   if (clusterSize < 1 || clusterSize > 8) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
@@ -239,12 +413,13 @@ cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, co
   attr[0].val.clusterDim.x = clusterSize, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, amcFitKernel<R>, jobs, x, D, E, contDates, realised, out, err);
+  if (bonds) return cudaLaunchKernelEx(&cfg, amcFitKernel<R, true>, jobs, x, D, E, contDates, bonds, bondRange, realised, out, err);
+  return cudaLaunchKernelEx(&cfg, amcFitKernel<R, false>, jobs, x, D, E, contDates, bonds, bondRange, realised, out, err);
 }
 
 template cudaError_t launchAmcFit<float>(const AmcFitJob*, uint32_t, const float*, const float*, const float*, const uint32_t*,
-                                         double*, double*, uint32_t*, uint32_t, cudaStream_t);
+                                         const double4*, const uint2*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
 template cudaError_t launchAmcFit<double>(const AmcFitJob*, uint32_t, const double*, const double*, const double*, const uint32_t*,
-                                          double*, double*, uint32_t*, uint32_t, cudaStream_t);
+                                          const double4*, const uint2*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
 
 }  // namespace zk

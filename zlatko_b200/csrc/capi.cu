@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <exception>
 #include <condition_variable>
@@ -331,7 +332,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
     const R* rec = v.terms + t * kTermStride;
     if (!(rec[0] >= R(0)) || rec[0] >= R(4294967296.0)) throw bad("invalid term code");
     const uint32_t code = static_cast<uint32_t>(rec[0]), kind = code & 15u;
-    if (kind > kForeignOption) throw bad("unknown term kind");
+    if (kind > kBermExt) throw bad("unknown term kind");
     if (kind == kForeignForward || kind == kForeignOption) {  // rec[1] is B_f; the asset sits in the code's extra field
       if ((code >> 12u) >= p.nF) throw bad("a foreign-rate term on an asset without a stochastic foreign rate");
       if (!(rec[1] >= R(0))) throw bad("invalid foreign bond coefficient");
@@ -340,16 +341,16 @@ Plan<R> parse(const View<R>& v, size_t index) {
     }
     // rec[1] is an index (swap slot, asset, probe selector) except for continuation terms, where it holds
     // the Bermudan's position.
-    if (kind != kBermContinue && (!(rec[1] >= R(0)) || rec[1] >= R(4294967296.0))) throw bad("invalid term slot");
+    if (kind != kBermContinue && kind != kBermExt && (!(rec[1] >= R(0)) || rec[1] >= R(4294967296.0))) throw bad("invalid term slot");
     const uint32_t slot = kind == kBermContinue ? 0u : static_cast<uint32_t>(rec[1]);
     if (kind == kAsset || kind == kOption) p.usesAssets = true;
-    if (kind > kOption && kind <= kProbe) p.amcOrProbe = true;
+    if ((kind > kOption && kind <= kProbe) || kind >= kBermAnnuity) p.amcOrProbe = true;
     if (kind == kProbe) {
       const uint32_t what = slot & 15u;
       if (what == 2 || what == 6) p.usesAssets = true;
       if (what == 3 || what == 4) p.probes = true;
     }
-    if (kind == kFixedFloat || kind == kSetFixing || (kind > kProbe) || kind == kBermFloat) {
+    if (kind == kFixedFloat || kind == kSetFixing || (kind > kProbe && kind < kBermAnnuity) || kind == kBermFloat) {
       if (slot >= static_cast<uint32_t>(kMaxSwapSlots)) throw bad("swap slot beyond 32");
       maxSlot = std::max(maxSlot, slot);
       anySlot = true;
@@ -357,7 +358,7 @@ Plan<R> parse(const View<R>& v, size_t index) {
     if (kind == kProbe) {
       if (!(rec[5] >= R(0)) || static_cast<double>(rec[5]) >= static_cast<double>(rows)) throw bad("probe row beyond rows_total");
     }
-    if (kind >= kBermExercise && kind <= kBermFloat) {
+    if ((kind >= kBermExercise && kind <= kBermFloat) || kind >= kBermAnnuity) {
       const uint32_t bm = bermudanOf(code, p.manyBerm), extra = code >> 12u;
       if (bm >= p.nBerm) throw bad("an AMC term of a Bermudan beyond the plan's count");
       if (kind == kBermDecide) {
@@ -367,6 +368,19 @@ Plan<R> parse(const View<R>& v, size_t index) {
     }
   }
   for (uint32_t b = 0; b < p.nBerm; ++b) p.exerciseRows += p.bermRows[b];
+  // The two-regressor basis: a policy or continuation record followed by exactly two extension records of its
+  // date, and extension records nowhere else (the kernel reads them with the record).
+  for (uint32_t j = 0; j < p.nT; ++j)
+    for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
+      const auto kindAt = [&](uint32_t u) { return static_cast<uint32_t>(v.terms[static_cast<size_t>(u) * kTermStride]) & 15u; };
+      const uint32_t kind = kindAt(t);
+      if (kind == kBermExt) throw bad("a regression extension record without its policy or continuation record");
+      if ((kind == kBermDecide || kind == kBermContinue) && t + 1 < I[j + 1] && kindAt(t + 1) == kBermExt) {
+        if (t + 2 >= I[j + 1] || kindAt(t + 2) != kBermExt || (t + 3 < I[j + 1] && kindAt(t + 3) == kBermExt))
+          throw bad("a two-regressor record needs exactly two extension records");
+        t += 2;
+      }
+    }
   for (uint32_t j = 0; j < p.nT; ++j) {
     for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
       const uint32_t kind = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]) & 15u;
@@ -1329,12 +1343,35 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
       throw fail(ZK_ERR_INVALID_ARGUMENT, "the plan has %u Bermudans, not %zu", P.nBerm, numBermudans);
     // Layout of the regressions: policy term and date of each exercise, continuation term of each date.
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> decide(numBermudans), cont(numBermudans);
+    // The two-regressor basis: a policy / continuation record followed by extension records (kind 15) regresses
+    // on (x, s) too; its co-terminal swap's bonds are the annuity / float-leg records (kinds 13, 14) right before it.
+    std::vector<int> twoD(numBermudans, -1);
+    std::map<uint32_t, uint2> coterm;  // term -> range of its bonds in `bonds`
+    std::vector<double4> bonds;
+    const auto kindAt = [&](uint32_t u) { return static_cast<uint32_t>(v.terms[static_cast<size_t>(u) * kTermStride]) & 15u; };
     for (uint32_t j = 0; j < P.nT; ++j)
       for (uint32_t t = v.indices[j]; t < v.indices[j + 1]; ++t) {
         const auto code = static_cast<uint32_t>(v.terms[static_cast<size_t>(t) * kTermStride]);
         const uint32_t kind = code & 15u, b = bermudanOf(code, P.manyBerm), e = code >> 12u;
         if (kind != 6u && kind != 7u) continue;
         if (b >= numBermudans) throw fail(ZK_ERR_INVALID_PLAN, "an AMC term of Bermudan %u", b);
+        const int two = t + 1 < v.indices[j + 1] && kindAt(t + 1) == kBermExt ? 1 : 0;
+        if (twoD[b] >= 0 && twoD[b] != two) throw fail(ZK_ERR_INVALID_PLAN, "Bermudan %u mixes one- and two-regressor records", b);
+        twoD[b] = two;
+        if (two) {
+          uint32_t u = t;
+          while (u > v.indices[j] && (kindAt(u - 1) == kBermAnnuity || kindAt(u - 1) == kBermCoterm)) --u;
+          bool annuity = false;
+          const uint32_t at = static_cast<uint32_t>(bonds.size());
+          for (; u < t; ++u) {
+            const R* r = v.terms + static_cast<size_t>(u) * kTermStride;
+            annuity = annuity || kindAt(u) == kBermAnnuity;
+            bonds.push_back(make_double4(static_cast<double>(kindAt(u)), static_cast<double>(r[2]), static_cast<double>(r[3]),
+                                         static_cast<double>(r[4])));
+          }
+          if (!annuity) throw fail(ZK_ERR_INVALID_PLAN, "Bermudan %u: a two-regressor record without its co-terminal annuity", b);
+          coterm[t] = make_uint2(at, static_cast<uint32_t>(bonds.size()) - at);
+        }
         if (kind == 6u) {
           if (e >= static_cast<uint32_t>(kMaxExercises)) throw fail(ZK_ERR_INVALID_PLAN, "exercise index %u", e);
           if (decide[b].size() <= e) decide[b].resize(e + 1, {0xFFFFFFFFu, 0u});
@@ -1351,6 +1388,7 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
       AmcFitJob& J = jobs[b];
       J = AmcFitJob{};
       J.nP = P.nP, J.nT = P.nT, J.nE = static_cast<uint32_t>(decide[b].size()), J.degree = degrees[b];
+      J.twoD = twoD[b] > 0 ? 1u : 0u;
       if (J.nE != P.bermRows[b]) throw fail(ZK_ERR_INVALID_PLAN, "Bermudan %zu: inconsistent exercise terms", b);
       J.eRow = eRow, eRow += J.nE;
       J.slotBase = slots, slots += J.nE + static_cast<uint32_t>(cont[b].size());
@@ -1362,27 +1400,44 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
       J.contBegin = static_cast<uint32_t>(contDates.size()), J.contCount = static_cast<uint32_t>(cont[b].size());
       for (const auto& c : cont[b]) contDates.push_back(c.first);
     }
+    // Per fit slot, the range of its co-terminal bonds (two-regressor Bermudans only).
+    std::vector<uint2> bondRange(std::max<uint32_t>(slots, 1), make_uint2(0, 0));
+    for (size_t b = 0; b < numBermudans; ++b) {
+      const AmcFitJob& J = jobs[b];
+      if (!J.twoD) continue;
+      for (uint32_t e = 0; e < J.nE; ++e) bondRange[J.slotBase + e] = coterm.at(decide[b][e].first);
+      for (uint32_t i = 0; i < J.contCount; ++i) bondRange[J.slotBase + J.nE + i] = coterm.at(cont[b][i].second);
+    }
     std::copy(v.terms, v.terms + termsLen, termsOut);
     if (numBermudans == 0) return ZK_OK;
     upload(*B, ctx, true, normals, streams);
     execute(*B);
-    // Device scratch: jobs, continuation dates, realised values per Bermudan, fitted records.
+    // Device scratch: jobs, continuation dates, realised values per Bermudan, fitted records, co-terminal bonds and
+    // their ranges.
     const size_t jobsBytes = jobs.size() * sizeof(AmcFitJob), datesBytes = std::max<size_t>(contDates.size(), 1) * 4;
-    const size_t realisedBytes = numBermudans * static_cast<size_t>(P.nP) * 8, outBytes = static_cast<size_t>(slots) * 6 * 8;
-    const size_t o1 = (jobsBytes + 255) / 256 * 256, o2 = o1 + (datesBytes + 255) / 256 * 256, o3 = o2 + (realisedBytes + 255) / 256 * 256;
-    dmem = takeBlock(ctx, o3 + outBytes, dmemBytes);
-    if (!dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "AMC fit: %zu bytes of device memory", o3 + outBytes);
+    const size_t realisedBytes = numBermudans * static_cast<size_t>(P.nP) * 8, outBytes = static_cast<size_t>(slots) * kFitOut * 8;
+    const size_t bondsBytes = std::max<size_t>(bonds.size(), 1) * sizeof(double4), rangeBytes = bondRange.size() * sizeof(uint2);
+    const size_t o1 = alignUp(jobsBytes), o2 = o1 + alignUp(datesBytes), o3 = o2 + alignUp(realisedBytes);
+    const size_t o4 = o3 + alignUp(outBytes), o5 = o4 + alignUp(bondsBytes), total = o5 + rangeBytes;
+    dmem = takeBlock(ctx, total, dmemBytes);
+    if (!dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "AMC fit: %zu bytes of device memory", total);
     unsigned char* d = static_cast<unsigned char*>(dmem);
     ZK_CUDA(cudaMemcpyAsync(d, jobs.data(), jobsBytes, cudaMemcpyHostToDevice, ctx->stream));
     if (!contDates.empty()) ZK_CUDA(cudaMemcpyAsync(d + o1, contDates.data(), contDates.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (!bonds.empty()) {
+      ZK_CUDA(cudaMemcpyAsync(d + o4, bonds.data(), bonds.size() * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+      ZK_CUDA(cudaMemcpyAsync(d + o5, bondRange.data(), rangeBytes, cudaMemcpyHostToDevice, ctx->stream));
+    }
     const uint32_t cluster = P.nP >= 65536 ? 8u : P.nP >= 16384 ? 4u : P.nP >= 4096 ? 2u : 1u;
     const R* sx = reinterpret_cast<const R*>(B->base + B->sinkOff[0]);
     const R* sd = reinterpret_cast<const R*>(B->base + B->sinkOff[1]);
     const R* se = reinterpret_cast<const R*>(B->base + B->sinkOff[2]);
     ZK_CUDA(launchAmcFit<R>(reinterpret_cast<const AmcFitJob*>(d), static_cast<uint32_t>(numBermudans), sx, sd, se,
-                            reinterpret_cast<const uint32_t*>(d + o1), reinterpret_cast<double*>(d + o2),
+                            reinterpret_cast<const uint32_t*>(d + o1),
+                            bonds.empty() ? nullptr : reinterpret_cast<const double4*>(d + o4),
+                            reinterpret_cast<const uint2*>(d + o5), reinterpret_cast<double*>(d + o2),
                             reinterpret_cast<double*>(d + o3), ctx->dErr, cluster, ctx->stream));
-    std::vector<double> fitted(static_cast<size_t>(slots) * 6);
+    std::vector<double> fitted(static_cast<size_t>(slots) * kFitOut);
     uint32_t devErr = 0;
     ZK_CUDA(cudaMemcpyAsync(fitted.data(), d + o3, outBytes, cudaMemcpyDeviceToHost, ctx->stream));
     ZK_CUDA(cudaMemcpyAsync(&devErr, ctx->dErr, 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1391,16 +1446,27 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     dmem = nullptr;
     if (devErr != 0) throw fail(ZK_ERR_CUDA, "the AMC fit reported error %u (normal equations not positive definite)", devErr);
     // The records as the reference writes them: center, 1 / scale, c0..c3 (fused_exposure.cpp:118-123).
-    auto write = [&](uint32_t term, const double* f) {
+    // Two-regressor records: cx, 1 / sx, cs, 1 / ss, c0, c1 in the record, c2..c8 in the first extension record's
+    // fields 1..7 and c9 in the second's field 1 (the kernel's amcPoly2 reads them so).
+    auto write = [&](uint32_t term, const double* f, bool two) {
       R* r = termsOut + static_cast<size_t>(term) * kTermStride;
-      r[2] = static_cast<R>(f[0]);
-      r[3] = static_cast<R>(1.0 / f[1]);
-      for (int i = 0; i < 4; ++i) r[4 + i] = static_cast<R>(f[2 + i]);
+      if (!two) {
+        r[2] = static_cast<R>(f[0]);
+        r[3] = static_cast<R>(1.0 / f[1]);
+        for (int i = 0; i < 4; ++i) r[4 + i] = static_cast<R>(f[2 + i]);
+        return;
+      }
+      r[2] = static_cast<R>(f[0]), r[3] = static_cast<R>(1.0 / f[1]), r[4] = static_cast<R>(f[2]), r[5] = static_cast<R>(1.0 / f[3]);
+      r[6] = static_cast<R>(f[4]), r[7] = static_cast<R>(f[5]);
+      R* e1 = r + kTermStride;
+      R* e2 = r + 2 * kTermStride;
+      for (int i = 0; i < 7; ++i) e1[1 + i] = static_cast<R>(f[6 + i]);
+      e2[1] = static_cast<R>(f[13]);
     };
     for (size_t b = 0; b < numBermudans; ++b) {
       const AmcFitJob& J = jobs[b];
-      for (uint32_t e = 0; e < J.nE; ++e) write(decide[b][e].first, &fitted[(J.slotBase + e) * 6]);
-      for (uint32_t i = 0; i < J.contCount; ++i) write(cont[b][i].second, &fitted[(J.slotBase + J.nE + i) * 6]);
+      for (uint32_t e = 0; e < J.nE; ++e) write(decide[b][e].first, &fitted[(J.slotBase + e) * kFitOut], J.twoD != 0);
+      for (uint32_t i = 0; i < J.contCount; ++i) write(cont[b][i].second, &fitted[(J.slotBase + J.nE + i) * kFitOut], J.twoD != 0);
     }
     return ZK_OK;
   } catch (const Failure& f) {

@@ -91,6 +91,22 @@ __device__ __forceinline__ void loadTerm(const double* t, double (&r)[8]) {
   }
 }
 
+// Whether the record at lowered unit u (of a run ending at `end`) is a two-regressor policy / continuation record:
+// the next record an extension (kBermExt); then its two extension records into e1, e2.
+template <typename R>
+__device__ __forceinline__ bool twoRegressors(const R* table, uint32_t u, uint32_t end, R (&e1)[8], R (&e2)[8]) {
+  if (u + 2 >= end || (static_cast<uint32_t>(table[4 * (u + 2)]) & 15u) != kBermExt) return false;
+  loadTerm(table + 4 * (u + 2), e1);
+  loadTerm(table + 4 * (u + 4), e2);
+  return true;
+}
+
+// The co-terminal swap rate from its float leg and annuity (0 without an annuity).
+template <typename R>
+__device__ __forceinline__ R swapRate(R flt, R ann) {
+  return ann != R(0) ? flt / ann : R(0);
+}
+
 constexpr int kSimThreads = 256;  // threads per CTA of the simulate kernel (one path each)
 
 // The normals of one date: every Box-Muller pair drawn up front (independent of one another, so they overlap),
@@ -483,9 +499,10 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
         }
 
     R value[PPT], ev[4][PPT];
+    R annS[PPT], fltS[PPT];  // the co-terminal swap of the next two-regressor record: annuity, float leg
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
-      value[i] = R(0);
+      value[i] = R(0), annS[i] = R(0), fltS[i] = R(0);
 #pragma unroll
       for (int b = 0; b < 4; ++b) ev[b][i] = R(0);
     }
@@ -578,14 +595,28 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
               else ev[3][i] += v;
             }
             break;
-          case kBermDecide:
+          case kBermAnnuity:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) annS[i] += c * (rec[3] * fastExp(nB * x[i]));
+            break;
+          case kBermCoterm:
+  #pragma unroll
+            for (int i = 0; i < PPT; ++i) fltS[i] += c * (rec[3] * fastExp(nB * x[i]));
+            break;
+          case kBermExt:
+            break;  // read with its policy or continuation record
+          case kBermDecide: {
+            R e1[8], e2[8];
+            const bool twoD = twoRegressors(table, u, d1.x, e1, e2);
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {
               const R e = manyBerm ? ev[0][i] : pick4<R, PPT>(ev, bm, i);
               if (manyBerm) ev[0][i] = R(0);
+              const R cont = twoD ? amcPoly2(rec, e1, e2, x[i], swapRate(fltS[i], annS[i])) : amcPoly(rec, x[i]);
+              annS[i] = R(0), fltS[i] = R(0);
               if (kSink) {
                 if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
-              } else if (exOf(bm, i) < R(0) && e > R(0) && e > amcPoly(rec, x[i])) {
+              } else if (exOf(bm, i) < R(0) && e > R(0) && e > cont) {
                 const R v = static_cast<R>(extra);
                 if (manyBerm) exS[(bm * PPT + i) * kTile + tid] = static_cast<signed char>(extra);
                 else if (bm == 0) ex[0][i] = v;
@@ -595,11 +626,18 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
               }
             }
             break;
-          case kBermContinue:
+          }
+          case kBermContinue: {
+            R e1[8], e2[8];
+            const bool twoD = twoRegressors(table, u, d1.x, e1, e2);
   #pragma unroll
-            for (int i = 0; i < PPT; ++i)
-              if (exOf(bm, i) < R(0)) term[i] = rec[1] * fmax(amcPoly(rec, x[i]), R(0));
+            for (int i = 0; i < PPT; ++i) {
+              const R cont = twoD ? amcPoly2(rec, e1, e2, x[i], swapRate(fltS[i], annS[i])) : amcPoly(rec, x[i]);
+              annS[i] = R(0), fltS[i] = R(0);
+              if (exOf(bm, i) < R(0)) term[i] = rec[1] * fmax(cont, R(0));
+            }
             break;
+          }
           case kBermBond:
   #pragma unroll
             for (int i = 0; i < PPT; ++i) {

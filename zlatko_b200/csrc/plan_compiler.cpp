@@ -36,7 +36,12 @@ enum Kind { kBond = 0, kFixedFloat = 1, kAsset = 2, kSetFixing = 3, kOption = 4,
             // Terms on an asset whose foreign rate is stochastic (an extension; asset index in the extra field):
             // kForeignForward (B_f, c, A_f): c S P_f(t, T | x_f); kForeignOption (B_f, N, A, B, A_f, K, +-sd): Black on
             // S P_f(t, T | x_f) / P(t, T | x) with the reference's volatility.
-            kForeignForward = 11, kForeignOption = 12 };
+            kForeignForward = 11, kForeignOption = 12,
+            // The two-regressor basis of a Bermudan (an extension): before each policy / continuation record, the
+            // co-terminal swap's annuity terms kBermAnnuity (tau, A, B) and float-leg terms kBermCoterm (+-1, A, B)
+            // -- the kernel takes s = float leg / annuity -- and after it two kBermExt records holding the rest of
+            // its coefficients.
+            kBermAnnuity = 13, kBermCoterm = 14, kBermExt = 15 };
 enum Op { kRowQuantile = 0, kRowMean = 1, kRowMeanPos = 2, kRowMeanNeg = 3, kRowSamples = 4, kRowHistogram = 5,
           kRowMeanProduct = 6, kRowQuantilePos = 7, kRowMeanPosTimes = 8, kRowMeanNegTimes = 9 };
 
@@ -252,6 +257,7 @@ NettingSet decodeNettingSet(const double* a, std::size_t n) {
       t.physical = in.d() != 0.0;
       t.position = in.d();
       t.degree = in.u();
+      if (t.degree >= 10) t.twoRegressors = true, t.degree -= 10;  // this library's two-regressor basis
       if (t.exercise.empty()) throw std::invalid_argument("BermudanSwaption: no exercise dates");
     } else if (type == 4) {  // swap with its own fixed and floating schedules
       t.kind = Trade::kSwapLegs;
@@ -737,6 +743,27 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
       const auto& sch = tr.swap.schedule;
       const auto& ex = tr.exercise;
       const std::size_t nE = ex.size();
+      // Two-regressor basis: the co-terminal swap from `start` (its annuity and its float leg at time t), before the
+      // policy or continuation record; after it, the records of its coefficients beyond the second.
+      auto coterminal = [&](std::size_t j, double t, double start) {
+        if (!tr.twoRegressors) return;
+        std::size_t first = sch.size();
+        for (std::size_t i = 1; i < sch.size(); ++i)
+          if (sch[i - 1] >= start - 1e-10) {
+            if (first == sch.size()) first = i;
+            addAmc(j, kBermAnnuity, b, 0, 0.0, sch[i] - sch[i - 1], bondA(t, sch[i]), bondB(t, sch[i]));
+          }
+        if (first == sch.size()) throw std::invalid_argument("Bermudan: an exercise date at or after the last period");
+        addAmc(j, kBermCoterm, b, 0, 0.0, 1.0, bondA(t, sch[first - 1]), bondB(t, sch[first - 1]));
+        addAmc(j, kBermCoterm, b, 0, 0.0, -1.0, bondA(t, sch.back()), bondB(t, sch.back()));
+      };
+      auto extension = [&](std::size_t j) {
+        if (!tr.twoRegressors) return;
+        addAmc(j, kBermExt, b, 0, 0.0, 0.0, 0.0, 0.0);
+        addAmc(j, kBermExt, b, 0, 0.0, 0.0, 0.0, 0.0);
+      };
+      if (tr.twoRegressors && o.imInnerPaths > 0)
+        throw std::invalid_argument("the nested initial margin of a Bermudan with the two-regressor basis");
       for (double e : ex)
         if (!std::any_of(sch.begin(), sch.end() - 1, [e](double x) { return std::fabs(x - e) < 1e-8; }))
           throw std::invalid_argument("BermudanSwaption: exercise dates must be start dates of the underlying periods");
@@ -771,9 +798,15 @@ CompiledPlan compile(const Model& m, const NettingSet& ns, const Options& o) {
             addAmc(j, kBermExercise, b, e, 0.0, sign * n, bondA(t, ts), bondB(t, ts));
             addAmc(j, kBermExercise, b, e, 0.0, -sign * n * (1 + k * tau), bondA(t, te), bondB(t, te));
           }
+          coterminal(j, t, ex[e]);
           addAmc(j, kBermDecide, b, e, 0.0, 0.0, 0.0, 0.0);
+          extension(j);
         }
-        if (next < nE) addAmc(j, kBermContinue, b, 0, pos, 0.0, 0.0, 0.0);
+        if (next < nE) {
+          coterminal(j, t, ex[next]);
+          addAmc(j, kBermContinue, b, 0, pos, 0.0, 0.0, 0.0);
+          extension(j);
+        }
         if (tr.physical)
           for (std::size_t i = 1; i < sch.size(); ++i) {
             if (lastEx[i - 1] < 0) continue;

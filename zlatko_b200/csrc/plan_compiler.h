@@ -84,6 +84,7 @@ struct Trade {
   bool physical = true;
   double position = 1.0;
   std::size_t degree = 3;
+  bool twoRegressors = false;        // Bermudan: the regression on the short rate and the co-terminal swap rate
   std::vector<double> eventTimes() const;
 };
 

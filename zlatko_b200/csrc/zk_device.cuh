@@ -38,6 +38,12 @@ enum TermKind : uint32_t {
   // the code's extra field, rec[1] the foreign bond's B_f): a forward's c S P_f(t, T | x_f) and a Black option on
   // the forward S P_f(t, T | x_f) / P(t, T | x).
   kForeignForward = 11, kForeignOption = 12,
+  // A Bermudan's two-regressor basis (an extension): before its policy or continuation record the co-terminal swap's
+  // annuity terms (tau, A, B) and float-leg terms (+-1, A, B), each c A e^{-B x}; after it two records of its
+  // coefficients.  The record (center_x, 1 / scale_x, center_s, 1 / scale_s, c0, c1) and the extensions (c2..c8),
+  // (c9) give sum_k c_k m_k(z, w) over the graded monomials 1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3 of
+  // z = (x - center_x) / scale_x and w = (s - center_s) / scale_s, s = float leg / annuity.
+  kBermAnnuity = 13, kBermCoterm = 14, kBermExt = 15,
 };
 
 // Header words (fused_kernels.cpp:32-41).
@@ -209,6 +215,16 @@ template <typename R>
 __device__ __forceinline__ R amcPoly(const R* rec, R x) {
   const R z = (x - rec[2]) * rec[3];
   return ((rec[7] * z + rec[6]) * z + rec[5]) * z + rec[4];
+}
+
+// The two-regressor continuation (see kBermAnnuity) at (x, s): rec the policy / continuation record, e1 and e2 its
+// extension records.
+template <typename R>
+__device__ __forceinline__ R amcPoly2(const R* rec, const R* e1, const R* e2, R x, R s) {
+  const R z = (x - rec[2]) * rec[3], w = (s - rec[4]) * rec[5];
+  const R zz = z * z, zw = z * w, ww = w * w;
+  return rec[6] + rec[7] * z + e1[1] * w + e1[2] * zz + e1[3] * zw + e1[4] * ww + e1[5] * zz * z + e1[6] * zz * w +
+         e1[7] * zw * w + e2[1] * ww * w;
 }
 
 // The Bermudan of an AMC term's code: bits 8-11, and with more than 4 Bermudans in the plan bits 4-7 above them

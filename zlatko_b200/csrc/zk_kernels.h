@@ -100,12 +100,18 @@ cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* er
 constexpr int kMaxExercises = 64;
 struct AmcFitJob {
   uint32_t nP, nT, nE, degree, eRow, slotBase, contBegin, contCount;
+  uint32_t twoD, pad;  // twoD: the Bermudan's records use the two-regressor basis
   uint32_t exDate[kMaxExercises];
 };
-// One thread-block cluster of clusterSize CTAs per job; out[slot][6] = center, scale, c0..c3.
+// The two-regressor basis: per fit slot (exercise k at slotBase + k, continuation i at slotBase + nE + i) the range
+// [bondRange.x, + bondRange.y) of its co-terminal swap's bonds {kind (annuity 13 / float leg 14), c, A, B}; the
+// regressor s = sum_float c A e^{-B x} / sum_annuity c A e^{-B x}, as the fused kernel forms it.
+constexpr int kFitOut = 16;  // doubles per fitted slot: 1D center, scale, c0..c3; 2D cx, sx, cs, ss, c0..c9
+// One thread-block cluster of clusterSize CTAs per job; out[slot][kFitOut].
 template <typename R>
 cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
-                         double* realised, double* out, uint32_t* err, uint32_t clusterSize, cudaStream_t stream);
+                         const double4* bonds, const uint2* bondRange, double* realised, double* out, uint32_t* err,
+                         uint32_t clusterSize, cudaStream_t stream);
 
 // C = A B^T with A [M][K], B [N][K] bf16 row-major (K contiguous) and FP32 accumulation on the tensor cores
 // (mlp.cu); M % 128 == 0, N % 16 == 0, K % 16 == 0.  Epilogue: z = acc + bias[n], times silu'(gradOf[m][n])

@@ -166,11 +166,16 @@ class Option:
 
 @dataclass
 class Bermudan:
+    """basis: "rate", the reference's Longstaff-Schwartz regression on the short-rate state; "rate_swap", this
+    library's two-regressor basis -- the graded monomials of total degree <= `degree` in the short rate and the
+    co-terminal swap rate (the swap from the next exercise date to maturity), an extension with no reference
+    counterpart (encoded as degree + 10)."""
     swap: Swap
     exercise: Sequence[float]
     physical: bool = True
     position: float = 1.0
     degree: int = 3
+    basis: str = "rate"
 
 
 Trade = Union[Swap, Swap2, Forward, Option, Bermudan]
@@ -280,7 +285,9 @@ def encode_netting_set(ns: NettingSet) -> np.ndarray:
             out += [3.0, float(s.notional), float(s.fixed_rate), 1.0 if s.pay_fixed else 0.0]
             _schedule(out, s.schedule)
             _schedule(out, t.exercise)
-            out += [1.0 if t.physical else 0.0, float(t.position), float(t.degree)]
+            if t.basis not in ("rate", "rate_swap"):
+                raise ValueError(f"Bermudan basis {t.basis!r}: 'rate' or 'rate_swap'")
+            out += [1.0 if t.physical else 0.0, float(t.position), float(t.degree + (10 if t.basis == "rate_swap" else 0))]
         elif isinstance(t, Swap2):
             out += [4.0, float(t.notional), float(t.fixed_rate), 1.0 if t.pay_fixed else 0.0]
             _schedule(out, t.fixed_schedule)
@@ -298,7 +305,7 @@ def encode_netting_set(ns: NettingSet) -> np.ndarray:
 
 
 def bermudan_degrees(ns_array: np.ndarray) -> List[int]:
-    """The regression degree of each Bermudan of an encoded netting set, in trade order."""
+    """The regression degree of each Bermudan of an encoded netting set, in trade order (for either basis)."""
     a = np.asarray(ns_array, np.float64)
     i, out = 2, []
     for _ in range(int(a[1])):
@@ -314,7 +321,7 @@ def bermudan_degrees(ns_array: np.ndarray) -> List[int]:
             i += 4
             i += 1 + int(a[i])
             i += 1 + int(a[i])
-            out.append(int(a[i + 2]))
+            out.append(int(a[i + 2]) % 10)  # the two-regressor basis adds 10 (the plan's records carry it)
             i += 3
         elif kind == 4:
             i += 4
