@@ -325,6 +325,24 @@ def amc_leg(ctx, a):
             "fit_s": fit_s, "revalue_ms": ms, "revals_per_s": revals / (fit_s + ms / 1e3),
             "revalue_revals_per_s": revals / (ms / 1e3),
             "fit_unit": "Bermudan path-dates fitted/s", "fit_rate": revals / fit_s}
+    # The same book with the two-regressor basis (short rate and co-terminal swap rate, 10 functions of degree <= 3).
+    m2, books2, _ = workloads.bermudan_book(a.amc_paths, basis="rate_swap")
+    plans2 = [gpu.compile(m2, b, S.Options()) for b in books2]
+    ctx.fit_amc(plans2[0])  # warm-up
+    t0 = time.perf_counter()
+    fitted2 = [ctx.fit_amc(p) for p in plans2]
+    fit2_s = time.perf_counter() - t0
+    b2 = ctx.batch(fitted2)
+    try:
+        for _ in range(3):
+            b2.execute()
+        b2.execute()
+        ms2 = float(np.sum(b2.timings()))
+    finally:
+        b2.close()
+    line["two_regressor"] = {"basis": "1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3 (z short rate, w co-terminal swap rate)",
+                             "fit_s": fit2_s, "revalue_ms": ms2, "revals_per_s": revals / (fit2_s + ms2 / 1e3),
+                             "fit_rate": revals / fit2_s}
     from oracle import ref
     if not a.no_cpu and ref.available():
         # The reference's gpu::compile fits the same book with its CPU kernels (fitAmc on the SpinPool, all host

@@ -30,13 +30,13 @@ constexpr int kFitThreads = 512;
 constexpr int kFitWarps = kFitThreads / 32;
 constexpr int kMomentVals = 4;   // count, sum x, sum x^2, sum y
 constexpr int kGramVals = 14;    // 10 Gram entries (lower triangle, degree 3) + 4 right-hand sides
-// The two-regressor basis: 55 Gram entries (lower triangle of 10) + 10 right-hand sides, summed in two passes of
-// kHalf2 values each (a thread's sums stay in registers).
-constexpr int kGram2 = 65, kHalf2 = 33;
+// The two-regressor basis: its Gram entries are the mixed moments sum z^a w^b, a + b <= 6 (28 of them, where the
+// lower triangle of 10 functions has 55 entries), plus the 10 right-hand sides: one pass of 38 sums.
+constexpr int kMom2 = 28, kSums2 = kMom2 + 10;
 
 struct FitSmem {
-  double warpBuf[kFitWarps][kHalf2];
-  double part[kHalf2];      // this CTA's sums
+  double warpBuf[kFitWarps][kSums2];
+  double part[kSums2];      // this CTA's sums
   double res[16];           // rank 0: 1D center, scale, degree, c0..c3, status; 2D cx, sx, cs, ss, c0..c9, degree
 };
 
@@ -206,12 +206,11 @@ __device__ __forceinline__ double swapRateOf(const double4* __restrict__ b, uint
   return ann != 0.0 ? flt / ann : 0.0;
 }
 
-// The graded monomials 1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3 (zero beyond `count`).
-__device__ __forceinline__ void basis2(double z, double w, int count, double (&m)[10]) {
-  const double v[10] = {1.0, z, w, z * z, z * w, w * w, z * z * z, z * z * w, z * w * w, w * w * w};
-#pragma unroll
-  for (int i = 0; i < 10; ++i) m[i] = i < count ? v[i] : 0.0;
-}
+// The graded monomials 1, z, w, z^2, z w, w^2, z^3, z^2 w, z w^2, w^3: the exponents of z and w of function i.
+__host__ __device__ constexpr int powZ(int i) { return i == 1 || i == 4 || i == 8 ? 1 : i == 3 || i == 7 ? 2 : i == 6 ? 3 : 0; }
+__host__ __device__ constexpr int powW(int i) { return i == 2 || i == 4 || i == 7 ? 1 : i == 5 || i == 8 ? 2 : i == 9 ? 3 : 0; }
+// Index of the moment sum z^a w^b (a + b <= 6) among the 28.
+__host__ __device__ constexpr int moment2(int a, int b) { return a * 7 - a * (a - 1) / 2 + b; }
 
 __device__ __forceinline__ int basisCount2(int d) { return d <= 0 ? 1 : d == 1 ? 3 : d == 2 ? 6 : 10; }
 
@@ -219,39 +218,14 @@ __device__ __forceinline__ int basisCount2(int d) { return d <= 0 ? 1 : d == 1 ?
 __device__ __forceinline__ double predict2(const double* res, double x, double s) {
   const int d = static_cast<int>(res[14]);
   if (d < 0) return 0.0;
-  double m[10];
-  basis2((x - res[0]) / res[1], (s - res[2]) / res[3], basisCount2(d), m);
+  const double z = (x - res[0]) / res[1], w = (s - res[2]) / res[3];
+  const double m[10] = {1.0, z, w, z * z, z * w, w * w, z * z * z, z * z * w, z * w * w, w * w * w};
+  const int count = basisCount2(d);
   double v = 0.0;
 #pragma unroll
-  for (int i = 0; i < 10; ++i) v += res[4 + i] * m[i];
+  for (int i = 0; i < 10; ++i)
+    if (i < count) v += res[4 + i] * m[i];
   return v;
-}
-
-// One pass of the two-regressor Gram: the sums [LO, LO + N) of the 65 (Gram lower triangle, then X^T y); with the
-// loops unrolled every index is a constant, so the sums stay in registers.
-template <typename R, int LO, int N>
-__device__ __forceinline__ void gram2Pass(double (&g)[kHalf2], const R* __restrict__ X, const R* __restrict__ Dj,
-                                          const R* __restrict__ Ek, const double* __restrict__ realised, const double4* bonds,
-                                          uint2 range, const double* res, int count, uint32_t nP, uint32_t first, uint32_t stride) {
-#pragma unroll
-  for (int i = 0; i < kHalf2; ++i) g[i] = 0.0;
-  for (uint32_t p = first; p < nP; p += stride) {
-    if (Ek && !(Ek[p] > R(0))) continue;
-    const double x = static_cast<double>(X[p]);
-    double m[10];
-    basis2((x - res[0]) / res[1], (swapRateOf(bonds, range, x) - res[2]) / res[3], count, m);
-    const double y = realised[p] / static_cast<double>(Dj[p]);
-    int q = 0;
-#pragma unroll
-    for (int a = 0; a < 10; ++a) {
-#pragma unroll
-      for (int b = 0; b <= a; ++b, ++q)
-        if (q >= LO && q < LO + N) g[q - LO] += m[a] * m[b];
-    }
-#pragma unroll
-    for (int a = 0; a < 10; ++a, ++q)
-      if (q >= LO && q < LO + N) g[q - LO] += m[a] * y;
-  }
 }
 
 // One regression of y = realised / D on (x, s) over the cluster's paths (masked by E > 0 when E is given):
@@ -259,17 +233,21 @@ __device__ __forceinline__ void gram2Pass(double (&g)[kHalf2], const R* __restri
 // basis, ridge 1e-6 n, FP64 Cholesky.  The ridge is larger than the one-regressor fit's: in a one-factor model the
 // swap rate is a smooth function of the short rate, the graded Gram's condition number reaches 1e17, and 1e-6 n keeps
 // the predictions stable to the summation order (~1e-11) at a negligible bias where the data are well conditioned.
-// Result in every CTA's `res` and, from rank 0, out[0..13] = cx, sx, cs, ss, c0..c9.
+// The first pass forms each included path's swap rate once (its bonds' exponentials) into the CTA's scratch row `sw`,
+// which the Gram pass and the caller's exercise update read.  Result in every CTA's `res` and, from rank 0,
+// out[0..13] = cx, sx, cs, ss, c0..c9.
 template <typename R>
 __device__ void fitOnce2(cg::cluster_group& cl, FitSmem& s, double* res, const R* __restrict__ X, const R* __restrict__ Dj,
                          const R* __restrict__ Ek, const double* __restrict__ realised, const double4* bonds, uint2 range,
-                         uint32_t nP, int degree, uint32_t first, uint32_t stride, double* out, uint32_t* err) {
-  __shared__ double tot[kGram2];
+                         double* __restrict__ sw, uint32_t nP, int degree, uint32_t first, uint32_t stride, double* out,
+                         uint32_t* err) {
+  __shared__ double tot[kSums2];
   double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (uint32_t p = first; p < nP; p += stride) {  // count, sum x, sum x^2, sum s, sum s^2, sum y
     if (Ek && !(Ek[p] > R(0))) continue;
-    const double x = static_cast<double>(X[p]), sw = swapRateOf(bonds, range, x);
-    m[0] += 1.0, m[1] += x, m[2] += x * x, m[3] += sw, m[4] += sw * sw, m[5] += realised[p] / static_cast<double>(Dj[p]);
+    const double x = static_cast<double>(X[p]), r = swapRateOf(bonds, range, x);
+    sw[p] = r;
+    m[0] += 1.0, m[1] += x, m[2] += x * x, m[3] += r, m[4] += r * r, m[5] += realised[p] / static_cast<double>(Dj[p]);
   }
   blockSum<6>(m, s);
   clusterSum<6>(cl, s, tot);
@@ -297,22 +275,35 @@ __device__ void fitOnce2(cg::cluster_group& cl, FitSmem& s, double* res, const R
   __syncthreads();
   const int d = static_cast<int>(res[14]);
   if (d > 0) {
-    const int count = basisCount2(d);
-    double g[kHalf2];
-    gram2Pass<R, 0, kHalf2>(g, X, Dj, Ek, realised, bonds, range, res, count, nP, first, stride);
-    blockSum<kHalf2>(g, s);
-    clusterSum<kHalf2>(cl, s, tot);
-    cl.sync();  // rank 0 has read every part before the second pass overwrites them
-    gram2Pass<R, kHalf2, kGram2 - kHalf2>(g, X, Dj, Ek, realised, bonds, range, res, count, nP, first, stride);
-    blockSum<kHalf2>(g, s);
-    clusterSum<kGram2 - kHalf2>(cl, s, tot + kHalf2);
+    // The moments sum z^a w^b (a + b <= 6) and sum z^a w^b y over the basis' exponents, one pass.
+    double g[kSums2];
+#pragma unroll
+    for (int i = 0; i < kSums2; ++i) g[i] = 0.0;
+    for (uint32_t p = first; p < nP; p += stride) {
+      if (Ek && !(Ek[p] > R(0))) continue;
+      const double z = (static_cast<double>(X[p]) - res[0]) / res[1], w = (sw[p] - res[2]) / res[3];
+      const double y = realised[p] / static_cast<double>(Dj[p]);
+      double zp[7], wp[7];
+      zp[0] = wp[0] = 1.0;
+#pragma unroll
+      for (int i = 1; i < 7; ++i) zp[i] = zp[i - 1] * z, wp[i] = wp[i - 1] * w;
+#pragma unroll
+      for (int a = 0; a <= 6; ++a)
+#pragma unroll
+        for (int b = 0; a + b <= 6; ++b) g[moment2(a, b)] += zp[a] * wp[b];
+#pragma unroll
+      for (int i = 0; i < 10; ++i) g[kMom2 + i] += zp[powZ(i)] * wp[powW(i)] * y;  // the right-hand sides
+    }
+    blockSum<kSums2>(g, s);
+    clusterSum<kSums2>(cl, s, tot);
     if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      const int count = basisCount2(d);
       double A[10][10], L[10][10] = {}, b[10], z[10], c[10] = {};
-      int q = 0;
-      for (int a = 0; a < 10; ++a)
-        for (int bb = 0; bb <= a; ++bb) A[a][bb] = A[bb][a] = tot[q++];
-      for (int a = 0; a < 10; ++a) b[a] = tot[55 + a];
-      const double n = tot[0];  // the Gram's first entry: sum 1 * 1, the sample count
+      for (int i = 0; i < 10; ++i) {
+        for (int j = 0; j < 10; ++j) A[i][j] = tot[moment2(powZ(i) + powZ(j), powW(i) + powW(j))];
+        b[i] = tot[kMom2 + i];
+      }
+      const double n = tot[0];  // sum z^0 w^0: the sample count
       for (int a = 0; a < count; ++a) A[a][a] += 1e-6 * n;
       bool ok = true;
       for (int i = 0; i < count; ++i)
@@ -353,7 +344,8 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
                                                              const R* __restrict__ D, const R* __restrict__ E,
                                                              const uint32_t* __restrict__ contDates, const double4* __restrict__ bonds,
                                                              const uint2* __restrict__ bondRange, double* __restrict__ realised,
-                                                             double* __restrict__ out, uint32_t* err) {
+                                                             double* __restrict__ swapScratch, double* __restrict__ out,
+                                                             uint32_t* err) {
   cg::cluster_group cl = cg::this_cluster();
   __shared__ FitSmem s;
   __shared__ double res[16];
@@ -361,6 +353,7 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
   const AmcFitJob J = jobs[job];
   const uint32_t nP = J.nP, stride = cl.num_blocks() * kFitThreads, first = cl.block_rank() * kFitThreads + threadIdx.x;
   double* rz = realised + static_cast<size_t>(job) * nP;
+  double* sw = TwoD ? swapScratch + static_cast<size_t>(job) * nP : nullptr;
   for (uint32_t p = first; p < nP; p += stride) rz[p] = 0.0;
   for (int k = static_cast<int>(J.nE) - 1; k >= 0; --k) {
     const size_t j = J.exDate[k];
@@ -368,16 +361,19 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
     const bool twoD = TwoD && J.twoD;
     const uint2 rk = twoD ? bondRange[J.slotBase + k] : make_uint2(0, 0);
     if (twoD)
-      fitOnce2<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, bonds, rk, nP, static_cast<int>(J.degree), first, stride,
+      fitOnce2<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, bonds, rk, sw, nP, static_cast<int>(J.degree), first, stride,
                   out + static_cast<size_t>(J.slotBase + k) * kFitOut, err);
     else
       fitOnce<R>(cl, s, res, x + j * nP, D + j * nP, Ek, rz, nP, static_cast<int>(J.degree), first, stride,
                  out + static_cast<size_t>(J.slotBase + k) * kFitOut, err);
-    // Exercise where the exercise value beats the regression: realised = D e.
+    // Exercise where the exercise value is positive and beats the regression: realised = D e (the swap rate of a
+    // path with E > 0 is in its scratch row from the fit).
     for (uint32_t p = first; p < nP; p += stride) {
-      const double e = static_cast<double>(Ek[p]), xp = static_cast<double>(x[j * nP + p]);
-      const double c = twoD ? predict2(res, xp, swapRateOf(bonds, rk, xp)) : predict(res, xp);
-      if (e > 0.0 && e > c) rz[p] = static_cast<double>(D[j * nP + p]) * e;
+      const double e = static_cast<double>(Ek[p]);
+      if (!(e > 0.0)) continue;
+      const double xp = static_cast<double>(x[j * nP + p]);
+      const double c = twoD ? predict2(res, xp, sw[p]) : predict(res, xp);
+      if (e > c) rz[p] = static_cast<double>(D[j * nP + p]) * e;
     }
     // Continuation on the dates whose next exercise is k: exDate[k - 1] <= date < exDate[k].
     const uint32_t lo = k > 0 ? J.exDate[k - 1] : 0u;
@@ -387,7 +383,7 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
       double* oc = out + static_cast<size_t>(J.slotBase + J.nE + i) * kFitOut;
       if (twoD)
         fitOnce2<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr),
-                    rz, bonds, bondRange[J.slotBase + J.nE + i], nP, static_cast<int>(J.degree), first, stride, oc, err);
+                    rz, bonds, bondRange[J.slotBase + J.nE + i], sw, nP, static_cast<int>(J.degree), first, stride, oc, err);
       else
         fitOnce<R>(cl, s, res, x + static_cast<size_t>(jc) * nP, D + static_cast<size_t>(jc) * nP, static_cast<const R*>(nullptr),
                    rz, nP, static_cast<int>(J.degree), first, stride, oc, err);
@@ -400,8 +396,8 @@ __global__ void __launch_bounds__(kFitThreads) amcFitKernel(const AmcFitJob* __r
 
 template <typename R>
 cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
-                         const double4* bonds, const uint2* bondRange, double* realised, double* out, uint32_t* err,
-                         uint32_t clusterSize, cudaStream_t stream) {
+                         const double4* bonds, const uint2* bondRange, double* realised, double* swapScratch, double* out,
+                         uint32_t* err, uint32_t clusterSize, cudaStream_t stream) {
   if (numJobs == 0) return cudaSuccess;
   if (clusterSize < 1 || clusterSize > 8) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
@@ -413,13 +409,16 @@ cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, co
   attr[0].val.clusterDim.x = clusterSize, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (bonds) return cudaLaunchKernelEx(&cfg, amcFitKernel<R, true>, jobs, x, D, E, contDates, bonds, bondRange, realised, out, err);
-  return cudaLaunchKernelEx(&cfg, amcFitKernel<R, false>, jobs, x, D, E, contDates, bonds, bondRange, realised, out, err);
+  if (bonds) {
+    if (!swapScratch) return cudaErrorInvalidValue;
+    return cudaLaunchKernelEx(&cfg, amcFitKernel<R, true>, jobs, x, D, E, contDates, bonds, bondRange, realised, swapScratch, out, err);
+  }
+  return cudaLaunchKernelEx(&cfg, amcFitKernel<R, false>, jobs, x, D, E, contDates, bonds, bondRange, realised, swapScratch, out, err);
 }
 
 template cudaError_t launchAmcFit<float>(const AmcFitJob*, uint32_t, const float*, const float*, const float*, const uint32_t*,
-                                         const double4*, const uint2*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
+                                         const double4*, const uint2*, double*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
 template cudaError_t launchAmcFit<double>(const AmcFitJob*, uint32_t, const double*, const double*, const double*, const uint32_t*,
-                                          const double4*, const uint2*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
+                                          const double4*, const uint2*, double*, double*, double*, uint32_t*, uint32_t, cudaStream_t);
 
 }  // namespace zk

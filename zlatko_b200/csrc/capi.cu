@@ -1418,7 +1418,8 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
     const size_t realisedBytes = numBermudans * static_cast<size_t>(P.nP) * 8, outBytes = static_cast<size_t>(slots) * kFitOut * 8;
     const size_t bondsBytes = std::max<size_t>(bonds.size(), 1) * sizeof(double4), rangeBytes = bondRange.size() * sizeof(uint2);
     const size_t o1 = alignUp(jobsBytes), o2 = o1 + alignUp(datesBytes), o3 = o2 + alignUp(realisedBytes);
-    const size_t o4 = o3 + alignUp(outBytes), o5 = o4 + alignUp(bondsBytes), total = o5 + rangeBytes;
+    const size_t scratchBytes = bonds.empty() ? 0 : realisedBytes;  // the two-regressor fits' swap rates per path
+    const size_t o4 = o3 + alignUp(outBytes), o5 = o4 + alignUp(bondsBytes), o6 = o5 + alignUp(rangeBytes), total = o6 + scratchBytes;
     dmem = takeBlock(ctx, total, dmemBytes);
     if (!dmem) throw fail(ZK_ERR_OUT_OF_MEMORY, "AMC fit: %zu bytes of device memory", total);
     unsigned char* d = static_cast<unsigned char*>(dmem);
@@ -1436,7 +1437,8 @@ zk_status fitAmc(zk_context* ctx, const ViewT* plan, const double* normals, size
                             reinterpret_cast<const uint32_t*>(d + o1),
                             bonds.empty() ? nullptr : reinterpret_cast<const double4*>(d + o4),
                             reinterpret_cast<const uint2*>(d + o5), reinterpret_cast<double*>(d + o2),
-                            reinterpret_cast<double*>(d + o3), ctx->dErr, cluster, ctx->stream));
+                            bonds.empty() ? nullptr : reinterpret_cast<double*>(d + o6), reinterpret_cast<double*>(d + o3),
+                            ctx->dErr, cluster, ctx->stream));
     std::vector<double> fitted(static_cast<size_t>(slots) * kFitOut);
     uint32_t devErr = 0;
     ZK_CUDA(cudaMemcpyAsync(fitted.data(), d + o3, outBytes, cudaMemcpyDeviceToHost, ctx->stream));

@@ -107,11 +107,12 @@ struct AmcFitJob {
 // [bondRange.x, + bondRange.y) of its co-terminal swap's bonds {kind (annuity 13 / float leg 14), c, A, B}; the
 // regressor s = sum_float c A e^{-B x} / sum_annuity c A e^{-B x}, as the fused kernel forms it.
 constexpr int kFitOut = 16;  // doubles per fitted slot: 1D center, scale, c0..c3; 2D cx, sx, cs, ss, c0..c9
-// One thread-block cluster of clusterSize CTAs per job; out[slot][kFitOut].
+// One thread-block cluster of clusterSize CTAs per job; out[slot][kFitOut]; realised and, with bonds, swapScratch:
+// [numJobs][nP] doubles of scratch.
 template <typename R>
 cudaError_t launchAmcFit(const AmcFitJob* jobs, uint32_t numJobs, const R* x, const R* D, const R* E, const uint32_t* contDates,
-                         const double4* bonds, const uint2* bondRange, double* realised, double* out, uint32_t* err,
-                         uint32_t clusterSize, cudaStream_t stream);
+                         const double4* bonds, const uint2* bondRange, double* realised, double* swapScratch, double* out,
+                         uint32_t* err, uint32_t clusterSize, cudaStream_t stream);
 
 // C = A B^T with A [M][K], B [N][K] bf16 row-major (K contiguous) and FP32 accumulation on the tensor cores
 // (mlp.cu); M % 128 == 0, N % 16 == 0, K % 16 == 0.  Epilogue: z = acc + bias[n], times silu'(gradOf[m][n])

@@ -138,12 +138,13 @@ def correlated_csa_book(paths: int = 100_000, netting_sets: int = 100, num_trade
     return m, books, S.Options(pfe_quantile=0.975), len(trades)
 
 
-def bermudan_book(paths: int = 200_000, bermudans: int = 200) -> Tuple[S.Model, List[S.NettingSet], int]:
+def bermudan_book(paths: int = 200_000, bermudans: int = 200, basis: str = "rate") -> Tuple[S.Model, List[S.NettingSet], int]:
     """The AMC workload: `bermudans` Bermudan swaptions under Hull-White (a = 0.03, sigma = 0.01) on a flat 2%
     curve, each on a 10y annual swap with annual exercise from year 1 to year 9, strike at the at-the-money rate
-    +- 100bp (uniform), notional 1e7, payer / receiver 50/50, degree-3 regressions in the short-rate state; four
-    per netting set (the fused kernel's limit), uncollateralised; quarterly dates to 10y (40 exposure dates).
-    Returns (model, netting sets, number of Bermudans)."""
+    +- 100bp (uniform), notional 1e7, payer / receiver 50/50, degree-3 regressions -- in the short-rate state
+    (basis "rate", the reference's) or in the short rate and the co-terminal swap rate (basis "rate_swap", the
+    10-function two-regressor basis); four per netting set, uncollateralised; quarterly dates to 10y (40 exposure
+    dates).  Returns (model, netting sets, number of Bermudans)."""
     rng = np.random.default_rng(PORTFOLIO_SEED + 2)
     m = S.Model(curve=S.Curve.flat(0.02), hw_a=0.03, hw_sigma=0.01, num_paths=paths, seed=SIM_SEED, antithetic=True,
                 base_grid=[k / 4.0 for k in range(1, 41)])
@@ -153,7 +154,7 @@ def bermudan_book(paths: int = 200_000, bermudans: int = 200) -> Tuple[S.Model, 
         k = atm + rng.uniform(-0.01, 0.01)
         pay = bool(rng.random() < 0.5)
         trades.append(S.Bermudan(S.Swap(1e7, k, pay, S.vanilla_schedule(0.0, 10.0, 1)), [float(e) for e in range(1, 10)],
-                                 physical=True, position=1.0, degree=3))
+                                 physical=True, position=1.0, degree=3, basis=basis))
     books = [S.NettingSet(trades[i:i + 4], None) for i in range(0, bermudans, 4)]
     return m, books, bermudans
 
