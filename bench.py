@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--netting-sets", type=int, default=100)
     ap.add_argument("--precision-paths", type=int, default=16_384, help="paths of the FP32-against-FP64 comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-against-FP64 comparison")
+    ap.add_argument("--no-exact", action="store_true", help="skip the exact-decision leg")
+    ap.add_argument("--exact-paths", type=int, default=65_536, help="paths of the exact-decision leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
@@ -246,6 +248,39 @@ def replica_throughput(units: float, t_device: float, t_e2e: float, world: int, 
         t_device, t_e2e = float(t[0]), float(t[1])
     total = units * world
     return total / t_device, total / t_e2e, t_device, t_e2e
+
+
+def exact_leg(ctx, a):
+    """The exact-decision check (zk_context_set_exact_decisions, guard 3e-7) on the bench's book (three-currency
+    model, 2,000 trades in 100 netting sets with cash CSAs): the wall time of one zk_run_plans call (uploads and
+    read-back included) without it (tensor-core basis kernel; term by term) and with it (term by term, then the
+    flagged paths again in FP64 and FP32), and the share of paths it re-ran."""
+    from zlatko_b200 import gpu, workloads
+
+    m, books, opts, _ = workloads.correlated_csa_book(a.exact_paths, num_trades=a.trades, netting_sets=a.netting_sets)
+    plans = [gpu.compile(m, b, opts) for b in books]
+
+    def timed(guard, basis):
+        ctx.set_exact_decisions(guard)
+        ctx.set_basis(basis)
+        ctx.run_many(plans)  # warm-up
+        ctx.exact_stats()
+        t0 = time.perf_counter()
+        ctx.run_many(plans)
+        return time.perf_counter() - t0, ctx.exact_stats()
+
+    try:
+        basis_s, _ = timed(0.0, ctx.BASIS_AUTO)
+        term_s, _ = timed(0.0, ctx.BASIS_OFF)
+        exact_s, (flagged, checked) = timed(3e-7, ctx.BASIS_AUTO)
+    finally:
+        ctx.set_exact_decisions(0.0)
+        ctx.set_basis(ctx.BASIS_AUTO)
+    return {"workload": f"the bench's book on {a.exact_paths} paths, zk_run_plans (host buffers)", "guard": 3e-7,
+            "s_basis_kernel": basis_s, "s_term_kernel": term_s, "s_exact": exact_s,
+            "paths_rerun_fp64": flagged, "paths_checked": checked,
+            "share_rerun": flagged / checked if checked else None,
+            "note": "decisions equal to the FP64 mode's (tests/test_gpu_exact_decisions.py)"}
 
 
 def guarded(fn, *args):
@@ -836,6 +871,8 @@ def main():
         }
         if not a.no_precision:
             line["fp32_vs_fp64"] = guarded(precision_leg, ctx, a)
+        if not a.no_exact:
+            line["exact_decisions"] = guarded(exact_leg, ctx, a)
         if not a.no_surrogate:
             line["surrogate"] = guarded(surrogate_leg, ctx, a)
         if not a.no_amc:

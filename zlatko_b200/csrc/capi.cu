@@ -1,6 +1,7 @@
 // The C ABI of zlatko_b200 (include/zlatko_b200.h): plan validation, batching, device memory and
 // the launch sequence fused-exposure -> reduce -> row statistics.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -116,6 +117,10 @@ struct zk_context {
   // context's stream (fork and join events order the two); created by the first eager execute that splits.
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // Worker streams of a re-run of chosen paths (the exact-decision check), whose plans are separate small launches
+  // that run side by side; created on first need, with one join event each.
+  std::vector<cudaStream_t> workers;
+  std::vector<cudaEvent_t> workerJoin;
   std::unique_ptr<zk::HostPool> pool;  // created by the first call that validates more than a few plans
   // Device blocks of short-lived work (a nest lives for one reporting date, an AMC fit for one call), reused by
   // later work and freed with the context: freeing device memory synchronises the device and took tens of
@@ -132,6 +137,10 @@ struct zk_context {
   // Which netting sets run on the tensor-core basis kernel (zk_context_set_basis): 0 groups of at least
   // kBasisMinNs eligible netting sets, 1 none, 2 every eligible netting set.
   uint32_t basisMode = 0;
+  // Exact decisions (zk_context_set_exact_decisions): the relative guard band (0: off) and the paths the last
+  // calls re-ran in double precision out of the paths they ran.
+  double exactGuard = 0.0;
+  uint64_t exactFlagged = 0, exactPaths = 0;
 };
 
 namespace {
@@ -244,6 +253,10 @@ struct Plan {
   std::vector<uint32_t> bermRows;  // exercise dates of each Bermudan
   bool manyBerm = false;           // more than 4 Bermudans: exercise state in shared memory (one byte per path)
   uint64_t termEvals = 0, expEvals = 0;
+  // The exact-decision check: the guard band of each date's decisions (empty: no check) and, for a re-run of
+  // chosen paths, the plan path of each of its paths (empty: every path in order).
+  std::vector<R> guard;
+  std::vector<uint32_t> pathMap;
 };
 
 template <typename R>
@@ -486,6 +499,51 @@ void lowerTerms(Plan<R>& p) {
   if (p.table.empty()) p.table.assign(4, R(0));
 }
 
+// The guard band of the exact-decision check on each date: rel times a bound on the gross value of the netting
+// set's terms, |value| summed term by term with each term's largest factor taken at its deterministic part (bonds at
+// A, coupons at a fixing of 10%, asset terms at the largest spot, options at their forward's bond, a regression at
+// |z| = 3).  The single-precision value of a path differs from the double-precision one by a few units of rounding
+// of that gross sum (the terms' exponentials, the simulated factors, the sum), so a decision whose margin in single
+// precision lies outside the band is taken the same way in double precision.  A margin call compares the value of
+// the call date with the collateral held, itself set from an earlier call: the band of a date adds the gross sums
+// of the date and of its call date.
+template <typename R>
+std::vector<R> decisionGuard(const Plan<R>& P, double rel) {
+  const uint32_t* I = P.v.indices;
+  double spot = 1.0;
+  for (uint32_t a = 0; a < std::min<uint32_t>(P.nA, 4); ++a) spot = std::max(spot, std::fabs(static_cast<double>(P.v.params[12 + a])));
+  std::vector<double> gross(P.nT, 0.0);
+  for (uint32_t j = 0; j < P.nT; ++j) {
+    double g = 0.0;
+    for (uint32_t t = I[j]; t < I[j + 1]; ++t) {
+      const R* r = P.v.terms + static_cast<size_t>(t) * kTermStride;
+      const uint32_t kind = static_cast<uint32_t>(r[0]) & 15u;
+      const double c = std::fabs(static_cast<double>(r[2])), a = std::fabs(static_cast<double>(r[3]));
+      auto poly = [&](const R* q, int from, int n) {
+        double v = 0.0, w = 1.0;
+        for (int k = 0; k < n; ++k, w *= 3.0) v += std::fabs(static_cast<double>(q[from + k])) * w;
+        return v;
+      };
+      switch (kind) {
+        case kBond: case kBermExercise: case kBermBond: g += c * a; break;
+        case kFixedFloat: case kBermFloat: g += (c * 0.1 + std::fabs(static_cast<double>(r[5]))) * a; break;
+        case kAsset: case kForeignForward: g += c * spot * a; break;
+        case kOption: case kForeignOption: g += c * spot * std::fabs(static_cast<double>(r[5])); break;
+        case kBermDecide: g += poly(r, 4, 4); break;
+        case kBermContinue: g += std::fabs(static_cast<double>(r[1])) * poly(r, 4, 4); break;
+        default: break;
+      }
+    }
+    gross[j] = g;
+  }
+  std::vector<R> out(P.nT);
+  for (uint32_t j = 0; j < P.nT; ++j) {
+    const uint32_t cj = std::min(I[P.offCall + j], P.nT - 1);
+    out[j] = static_cast<R>(rel * (gross[j] + gross[cj]));
+  }
+  return out;
+}
+
 // Plans share a scenario when every input of the risk-factor simulation is identical.
 template <typename R>
 bool sameScenario(const Plan<R>& a, const Plan<R>& b) {
@@ -553,6 +611,7 @@ struct Batch {
   struct Dev {
     size_t dates, table, steps, req, expo, partials, sums, values;
     size_t imSlots = 0, imModel = 0, imState = 0;  // nested initial margin: slots [nR][2], spots + Cholesky, outer state
+    size_t guard = 0, flags = 0, pathMap = 0;      // the exact-decision check; a re-run's path map (0: none)
   };
   std::vector<Dev> dev;
   size_t reduceOff = 0, rowOff = 0, normalsOff = 0, sinkOff[3] = {0, 0, 0}, bermRowOff = 0;
@@ -569,15 +628,23 @@ struct Batch {
   unsigned char* base = nullptr;     // device arena
   bool ownsArena = false;
   bool sink = false;
+  bool exact = false;                // the exact-decision check: guard bands and flags (Dev::guard, Dev::flags)
+  size_t flagsOff = 0, flagsBytes = 0;
   uint32_t exerciseRows = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float ms[4] = {0, 0, 0, 0};
   bool timed = false;
 
+  size_t spareBytes = 0;              // the arena is a spare block of the context (upload with spare), returned here
   ~Batch() {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (ownsArena && base) cudaFree(base);
+    if (spareBytes && base) {  // nothing in flight may still use the block when the next work takes it
+      cudaStreamSynchronize(ctx->stream);
+      for (auto w : ctx->workers) cudaStreamSynchronize(w);
+      ctx->spareBlocks.emplace_back(base, spareBytes);
+    }
   }
 };
 
@@ -693,20 +760,40 @@ void formGroups(Batch<R>& B, typename Batch<R>::Launch& L, uint32_t mode, HostPo
   }
 }
 
+// Options of a batch beyond its plans: the exact-decision check (guard bands and flags; term-by-term revaluation),
+// or the re-run of chosen paths (maps[i]: the paths of plan i, its header's path count their number; every plan its
+// own launch; term by term).
+struct BuildOpts {
+  bool exact = false;
+  const std::vector<std::vector<uint32_t>>* maps = nullptr;
+};
+
 template <typename R>
-std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams) {
+std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams,
+                                const BuildOpts& opts = BuildOpts()) {
   auto B = std::make_unique<Batch<R>>();
   B->ctx = ctx;
   B->sink = sink;
   parseAll(views, B->plans, hostPool(ctx, views.size()));
   const size_t nPlans = B->plans.size();
-  // ---- launch groups: plans sharing the scenario ----
+  if (opts.maps) {
+    for (size_t i = 0; i < nPlans; ++i) {
+      const auto& m = (*opts.maps)[i];
+      if (m.size() != B->plans[i].nP) throw fail(ZK_ERR_INVALID_ARGUMENT, "plan %zu: a path map of %zu paths for %u", i, m.size(), B->plans[i].nP);
+      B->plans[i].pathMap = m;
+    }
+  }
+  B->exact = opts.exact;
+  if (opts.exact)
+    for (auto& P : B->plans)
+      if (!P.im) P.guard = decisionGuard(P, ctx->exactGuard);
+  // ---- launch groups: plans sharing the scenario (a re-run of chosen paths: every plan alone) ----
   std::vector<int> launchOf(nPlans, -1);
   for (size_t i = 0; i < nPlans; ++i) {
     if (launchOf[i] >= 0) continue;
     typename Batch<R>::Launch L;
     for (size_t k = i; k < nPlans; ++k)
-      if (launchOf[k] < 0 && sameScenario(B->plans[i], B->plans[k])) {
+      if (launchOf[k] < 0 && (k == i || (!opts.maps && sameScenario(B->plans[i], B->plans[k])))) {
         launchOf[k] = static_cast<int>(B->launches.size());
         L.planIdx.push_back(static_cast<uint32_t>(k));
       }
@@ -716,7 +803,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   // ---- per launch: the factor cube shared by its netting sets, one CTA column per netting set ----
   B->onBasis.assign(nPlans, 0);
   for (auto& L : B->launches) {
-    formGroups(*B, L, ctx ? ctx->basisMode : 1u, hostPool(ctx, views.size()));
+    formGroups(*B, L, ctx && !opts.exact && !opts.maps ? ctx->basisMode : 1u, hostPool(ctx, views.size()));
     const size_t nb = L.basisCount;
     std::stable_sort(L.planIdx.begin() + static_cast<std::ptrdiff_t>(nb), L.planIdx.end(),
                      [&](uint32_t a, uint32_t b) { return B->plans[a].stateWords > B->plans[b].stateWords; });
@@ -746,7 +833,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
     sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
     sc.nF = P0.nF, sc.stepStride = P0.stepStride;
-    sc.steps = nullptr, sc.normals = nullptr;
+    sc.steps = nullptr, sc.normals = nullptr, sc.pathMap = nullptr;
     for (int k = 0; k < 8; ++k) sc.cir[k] = P0.v.params[k];
     for (int k = 0; k < 4; ++k) sc.spots[k] = P0.v.params[12 + k];
     for (int k = 0; k < 64; ++k) sc.chol[k] = P0.v.params[16 + k];
@@ -779,6 +866,8 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
       D.imSlots = take(P.imSlots.size() * 4);
       D.imModel = take((4 + kChol * kChol) * sizeof(R));
     }
+    if (!P.guard.empty()) D.guard = take(P.guard.size() * sizeof(R));
+    if (!P.pathMap.empty()) D.pathMap = take(P.pathMap.size() * 4);
   }
   for (auto& L : B->launches) L.nsOff = take(L.planIdx.size() * sizeof(NsArgs<R>));
   for (auto& L : B->launches) {
@@ -880,6 +969,13 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
     B->sinkOff[1] = take(static_cast<size_t>(P.nT) * P.nP * sizeof(R));
     B->sinkOff[2] = take(static_cast<size_t>(std::max<uint32_t>(P.exerciseRows, 1)) * P.nP * sizeof(R));
   }
+  // The exact-decision check's flags: a bit per path of every checked plan, cleared by each execute.
+  if (opts.exact) {
+    B->flagsOff = off;
+    for (size_t i = 0; i < nPlans; ++i)
+      if (!B->plans[i].guard.empty()) B->dev[i].flags = take(static_cast<size_t>((B->plans[i].nP + 31) / 32) * 4);
+    B->flagsBytes = off - B->flagsOff;
+  }
   B->outBegin = off;
   for (size_t i = 0; i < nPlans; ++i) {
     const auto& P = B->plans[i];
@@ -928,6 +1024,8 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
         std::memcpy(img + D.imSlots, P.imSlots.data(), P.imSlots.size() * 4);
         std::memcpy(img + D.imModel, P.v.params + 12, (4 + kChol * kChol) * sizeof(R));
       }
+      if (!P.guard.empty()) std::memcpy(img + D.guard, P.guard.data(), P.guard.size() * sizeof(R));
+      if (!P.pathMap.empty()) std::memcpy(img + D.pathMap, P.pathMap.data(), P.pathMap.size() * 4);
     }
   });
   for (auto& L : B.launches) {
@@ -955,6 +1053,10 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
       A.usesForeign = P.usesForeign ? 1u : 0u;
       A.stepStride = P.stepStride;
       A.manyBerm = P.manyBerm ? 1u : 0u;
+      if (!P.guard.empty()) {
+        A.flags = static_cast<uint32_t*>(dptr(D.flags));
+        A.guard = static_cast<const R*>(dptr(D.guard));
+      }
       if (P.im && !B.sink) {
         A.imState = static_cast<R*>(dptr(D.imState));
         A.imWords = 5 + P.nSlots;
@@ -1006,6 +1108,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
     const auto& P0 = B.plans[L.planIdx.front()];
     L.sc.steps = static_cast<const R*>(dptr(B.dev[L.planIdx.front()].steps));
     L.sc.normals = normals ? static_cast<const R*>(dptr(B.normalsOff)) : nullptr;
+    L.sc.pathMap = P0.pathMap.empty() ? nullptr : static_cast<const uint32_t*>(dptr(B.dev[L.planIdx.front()].pathMap));
     L.cb.data = static_cast<R*>(dptr(L.cubeOff));
     (void)P0;
   }
@@ -1050,9 +1153,15 @@ void growStage(unsigned char*& stage, size_t& bytes, size_t need) {
   bytes = need;
 }
 
+// The arena: the context's (useCtxArena), a spare block of the context (spare: short-lived batches), or its own.
 template <typename R>
-void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normals, size_t streams) {
-  if (useCtxArena) {
+void upload(Batch<R>& B, zk_context* ctx, bool useCtxArena, const double* normals, size_t streams, bool spare = false) {
+  if (!useCtxArena && spare) {
+    size_t bytes = 0;
+    B.base = takeBlock(ctx, B.totalBytes, bytes);
+    if (!B.base) throw fail(ZK_ERR_OUT_OF_MEMORY, "%zu bytes of device memory", B.totalBytes);
+    B.spareBytes = bytes;
+  } else if (useCtxArena) {
     if (ctx->arenaBytes < B.totalBytes) {
       if (ctx->arena) cudaFree(ctx->arena);
       ctx->arena = nullptr;
@@ -1155,14 +1264,46 @@ void execute(Batch<R>& B, bool capturing = false) {
   if (!B.ev[0])
     for (auto& e : B.ev) ZK_CUDA(cudaEventCreate(&e));
   ZK_CUDA(cudaMemsetAsync(ctx->dErr, 0, 4, s));
+  if (B.flagsBytes) ZK_CUDA(cudaMemsetAsync(B.base + B.flagsOff, 0, B.flagsBytes, s));
   ZK_CUDA(recordEvent(B.ev[0], s, capturing));
   const uintptr_t base = reinterpret_cast<uintptr_t>(B.base);
-  for (auto& L : B.launches) {
-    injectPoint(ctx);
-    ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
+  // A re-run of chosen paths: every plan is a launch of a few paths; they run side by side on worker streams,
+  // each its simulation then its revaluation, joined before the reduce.
+  const bool fan = !capturing && !B.waved && B.launches.size() > 1 && !B.plans[B.launches[0].planIdx[0]].pathMap.empty();
+  if (fan) {
+    const size_t k = std::min<size_t>(B.launches.size(), 8);
+    while (ctx->workers.size() < k) {
+      cudaStream_t w = nullptr;
+      cudaEvent_t e = nullptr;
+      ZK_CUDA(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
+      ctx->workers.push_back(w);
+      ZK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ctx->workerJoin.push_back(e);
+    }
+    if (!ctx->fork) ZK_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+    ZK_CUDA(cudaEventRecord(ctx->fork, s));
+    for (size_t q = 0; q < k; ++q) ZK_CUDA(cudaStreamWaitEvent(ctx->workers[q], ctx->fork, 0));
+    for (size_t l = 0; l < B.launches.size(); ++l) {
+      const auto& L = B.launches[l];
+      cudaStream_t w = ctx->workers[l % k];
+      injectPoint(ctx);
+      ZK_CUDA(launchSimulate<R>(L.sc, L.cb, w));
+      launchRevalues(B, L, base, w, nullptr, nullptr, nullptr);
+    }
+    for (size_t q = 0; q < k; ++q) {
+      ZK_CUDA(cudaEventRecord(ctx->workerJoin[q], ctx->workers[q]));
+      ZK_CUDA(cudaStreamWaitEvent(s, ctx->workerJoin[q], 0));
+    }
+    ZK_CUDA(recordEvent(B.ev[1], s, capturing));
+  } else {
+    for (auto& L : B.launches) {
+      injectPoint(ctx);
+      ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
+    }
+    ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   }
-  ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   for (auto& L : B.launches) {
+    if (fan) break;  // revalued on the worker streams above
     const bool split = L.lean && !L.perTrade && !B.sink && sizeof(R) == 4 && B.ppt > 1 && L.splitAt < L.planIdx.size();
     if (split && L.splitAt > L.basisCount && !ctx->side && !capturing) {
       ZK_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
@@ -1245,6 +1386,125 @@ void readOutputs(Batch<R>& B, Out* outs) {
   }
 }
 
+// The exact-decision check, after an execute of a single-precision batch built with BuildOpts::exact.  The revalue
+// kernel flagged every path with a margin call or exercise decision inside its guard band (decisionGuard): there the
+// single-precision rule may decide otherwise than double precision would.  Those paths run again, alone, twice: in
+// double precision (their decisions and values as the FP64 mode takes them on the same normals) and in single
+// precision (what the batch summed for them).  Their rows are replaced by the double-precision rows and the plan's
+// row statistics recomputed; the returned patches replace their share of the date statistics after readOutputs.
+// Plans with the nested initial margin are not checked.  A batch in waves has no resident rows to patch.
+struct SumPatch {
+  size_t plan = 0;
+  double share = 0.0;         // re-run paths / the plan's paths (the sums are means)
+  std::vector<float> s32;     // the re-run paths' means in single precision
+  std::vector<double> s64;    // and in double precision
+};
+
+std::vector<SumPatch> exactCheck(Batch<float>& B) {
+  zk_context* ctx = B.ctx;
+  std::vector<SumPatch> patches;
+  if (!B.exact || B.flagsBytes == 0) return patches;
+  if (B.waved)
+    throw fail(ZK_ERR_UNSUPPORTED, "exact decisions: the batch runs in waves (its rows exceed the row budget), so its rows are not resident to patch");
+  std::vector<uint32_t> bits(B.flagsBytes / 4);
+  ZK_CUDA(cudaMemcpyAsync(bits.data(), B.base + B.flagsOff, B.flagsBytes, cudaMemcpyDeviceToHost, ctx->stream));
+  finish(B);
+  std::vector<size_t> which;
+  std::vector<std::vector<uint32_t>> maps;
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    const auto& P = B.plans[i];
+    if (P.guard.empty()) continue;
+    const uint32_t* w = bits.data() + (B.dev[i].flags - B.flagsOff) / 4;
+    std::vector<uint32_t> paths;
+    for (uint32_t p = 0; p < P.nP; ++p)
+      if (w[p >> 5] >> (p & 31u) & 1u) paths.push_back(p);
+    ctx->exactPaths += P.nP;
+    ctx->exactFlagged += paths.size();
+    if (paths.empty()) continue;
+    which.push_back(i);
+    maps.push_back(std::move(paths));
+  }
+  if (which.empty()) return patches;
+  // The flagged paths of each plan as a plan of their own: its header counts them, the tables are the plan's
+  // (converted to double for the double-precision run).
+  const size_t n = which.size();
+  std::vector<std::vector<uint32_t>> headers(n);
+  std::vector<std::vector<double>> d64(4 * n);
+  std::vector<View<float>> v32(n);
+  std::vector<View<double>> v64(n);
+  for (size_t k = 0; k < n; ++k) {
+    const auto& P = B.plans[which[k]];
+    headers[k].assign(P.v.header, P.v.header + P.v.header_len);
+    headers[k][hP] = static_cast<uint32_t>(maps[k].size());
+    v32[k] = P.v;
+    v32[k].header = headers[k].data();
+    auto widen = [&](std::vector<double>& dst, const float* src, size_t len) {
+      dst.assign(src, src + len);
+      return dst.empty() ? nullptr : dst.data();
+    };
+    View<double>& d = v64[k];
+    d.header = headers[k].data(), d.header_len = P.v.header_len;
+    d.indices = P.v.indices, d.indices_len = P.v.indices_len;
+    d.params = widen(d64[4 * k], P.v.params, P.v.params_len), d.params_len = P.v.params_len;
+    d.steps = widen(d64[4 * k + 1], P.v.steps, P.v.steps_len), d.steps_len = P.v.steps_len;
+    d.terms = widen(d64[4 * k + 2], P.v.terms, P.v.terms_len), d.terms_len = P.v.terms_len;
+    d.requests = widen(d64[4 * k + 3], P.v.requests, P.v.requests_len), d.requests_len = P.v.requests_len;
+    d.rows_total = P.v.rows_total, d.num_outputs = P.v.num_outputs;
+  }
+  BuildOpts ro;
+  ro.maps = &maps;
+  auto B32 = build<float>(ctx, v32, false, nullptr, 0, ro);
+  auto B64 = build<double>(ctx, v64, false, nullptr, 0, ro);
+  for (size_t k = 0; k < n; ++k) {
+    SumPatch sp;
+    sp.plan = which[k];
+    sp.share = static_cast<double>(maps[k].size()) / static_cast<double>(B.plans[which[k]].nP);
+    patches.push_back(std::move(sp));
+  }
+  upload(*B32, ctx, false, nullptr, 0, true);
+  execute(*B32);
+  for (size_t k = 0; k < n; ++k) {
+    const auto& P = B32->plans[k];
+    patches[k].s32.resize(static_cast<size_t>(P.nT) * P.nS);
+    ZK_CUDA(cudaMemcpyAsync(patches[k].s32.data(), B32->base + B32->dev[k].sums, patches[k].s32.size() * 4, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  }
+  finish(*B32);
+  upload(*B64, ctx, false, nullptr, 0, true);
+  execute(*B64);
+  for (size_t k = 0; k < n; ++k) {
+    const auto& P = B64->plans[k];
+    patches[k].s64.resize(static_cast<size_t>(P.nT) * P.nS);
+    ZK_CUDA(cudaMemcpyAsync(patches[k].s64.data(), B64->base + B64->dev[k].sums, patches[k].s64.size() * 8, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  }
+  finish(*B64);
+  // The rows of the re-run paths from the double-precision run, then the plan's row statistics on the patched rows
+  // (its jobs sit in plan order in the batch's job array).
+  std::vector<size_t> jobFirst(B.plans.size() + 1, 0);
+  for (size_t i = 0; i < B.plans.size(); ++i) jobFirst[i + 1] = jobFirst[i] + B.plans[i].nReq;
+  for (size_t k = 0; k < n; ++k) {
+    const size_t i = which[k];
+    const auto& P = B.plans[i];
+    ZK_CUDA(launchScatterRows(reinterpret_cast<const double*>(B64->base + B64->dev[k].expo), static_cast<uint32_t>(maps[k].size()),
+                              reinterpret_cast<const uint32_t*>(B64->base + B64->dev[k].pathMap), P.v.rows_total,
+                              reinterpret_cast<float*>(B.base + B.dev[i].expo), P.nP, ctx->stream));
+    ZK_CUDA(launchRowStats<float>(reinterpret_cast<const RowJob<float>*>(B.base + B.rowOff) + jobFirst[i], static_cast<uint32_t>(P.nReq),
+                                  ctx->dErr, ctx->stream, ctx->rowRounds));
+  }
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));  // the sub-batches' arenas are freed with them
+  return patches;
+}
+
+// The date statistics of the re-run paths: their single-precision share replaced by the double-precision one.
+template <typename Out>
+void applyPatches(const std::vector<SumPatch>& patches, Out* outs) {
+  for (const auto& sp : patches)
+    for (size_t k = 0; k < sp.s64.size(); ++k)
+      outs[sp.plan].sums[k] = static_cast<float>(static_cast<double>(outs[sp.plan].sums[k]) +
+                                                 sp.share * (sp.s64[k] - static_cast<double>(sp.s32[k])));
+}
+
 template <typename Out>
 void checkOutput(const Out* o, size_t nSums, size_t nValues, size_t i) {
   if (!o || !o->sums || !o->values) throw fail(ZK_ERR_INVALID_ARGUMENT, "output %zu: null buffer", i);
@@ -1307,16 +1567,21 @@ zk_status runInjected(zk_context* ctx, const ViewT* plan, const double* normals,
   try {
     requireCtx(ctx);
     if (!plan || !out) throw fail(ZK_ERR_INVALID_ARGUMENT, "null argument");
-    auto B = build<R>(ctx, {viewOf(*plan)}, false, normals, streams);
+    BuildOpts bo;
+    bo.exact = sizeof(R) == 4 && !normals && ctx->exactGuard > 0.0;
+    auto B = build<R>(ctx, {viewOf(*plan)}, false, normals, streams, bo);
     checkOutputs(*B, out, sizeof(R) == 8);
     upload(*B, ctx, true, normals, streams);
     execute(*B);
+    std::vector<SumPatch> patches;
+    if constexpr (sizeof(R) == 4) patches = exactCheck(*B);
     if (rows) {
       const auto& P = B->plans[0];
       ZK_CUDA(cudaMemcpyAsync(rows, B->base + B->dev[0].expo, static_cast<size_t>(P.v.rows_total) * P.nP * sizeof(R),
                               cudaMemcpyDeviceToHost, ctx->stream));
     }
     readOutputs(*B, out);
+    if constexpr (sizeof(R) == 4) applyPatches(patches, out);
     return ZK_OK;
   } catch (const Failure& f) {
     return record(ctx, f);
@@ -1566,6 +1831,11 @@ void zk_context_destroy(zk_context* ctx) {
     cudaStreamDestroy(ctx->side);
   }
   for (auto& blk : ctx->spareBlocks) cudaFree(blk.first);
+  for (auto w : ctx->workers) {
+    cudaStreamSynchronize(w);
+    cudaStreamDestroy(w);
+  }
+  for (auto e : ctx->workerJoin) cudaEventDestroy(e);
   if (ctx->fork) cudaEventDestroy(ctx->fork);
   if (ctx->join) cudaEventDestroy(ctx->join);
   if (ctx->ownStream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1593,6 +1863,19 @@ zk_status zk_context_set_row_budget(zk_context* ctx, uint64_t bytes) {
 zk_status zk_context_set_basis(zk_context* ctx, uint32_t mode) {
   if (!ctx || mode > ZK_BASIS_ALL) return ZK_ERR_INVALID_ARGUMENT;
   ctx->basisMode = mode;
+  return ZK_OK;
+}
+
+zk_status zk_context_set_exact_decisions(zk_context* ctx, double guard) {
+  if (!ctx || !(guard >= 0.0) || guard > 1e-2) return ZK_ERR_INVALID_ARGUMENT;
+  ctx->exactGuard = guard;
+  return ZK_OK;
+}
+
+zk_status zk_context_exact_stats(zk_context* ctx, uint64_t* flagged_paths, uint64_t* checked_paths) {
+  if (!ctx || !flagged_paths || !checked_paths) return ZK_ERR_INVALID_ARGUMENT;
+  *flagged_paths = ctx->exactFlagged, *checked_paths = ctx->exactPaths;
+  ctx->exactFlagged = ctx->exactPaths = 0;
   return ZK_OK;
 }
 
@@ -1631,11 +1914,15 @@ zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_
     if (!plans || !outs || n == 0) throw fail(ZK_ERR_INVALID_ARGUMENT, "null or empty plan list");
     std::vector<View<float>> views;
     for (size_t i = 0; i < n; ++i) views.push_back(viewOf(plans[i]));
-    auto B = build<float>(ctx, views, false, nullptr, 0);
+    BuildOpts bo;
+    bo.exact = ctx->exactGuard > 0.0;
+    auto B = build<float>(ctx, views, false, nullptr, 0, bo);
     checkOutputs(*B, outs, false);
     upload(*B, ctx, true, nullptr, 0);
     execute(*B);
+    const auto patches = exactCheck(*B);
     readOutputs(*B, outs);
+    applyPatches(patches, outs);
     return ZK_OK;
   } catch (const Failure& f) {
     return record(ctx, f);

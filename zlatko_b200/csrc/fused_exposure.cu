@@ -157,11 +157,12 @@ __global__ void __launch_bounds__(kSimThreads) simulateKernel(const ScenarioArgs
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sc.nP) return;
   const uint32_t nP = sc.nP, nT = sc.nT;
+  const uint32_t po = sc.pathMap ? sc.pathMap[p] : p;  // the plan's path this thread simulates
   R sign = R(1);
-  uint32_t pathStream = p;
+  uint32_t pathStream = po;
   if (sc.antithetic) {
-    pathStream = p >> 1u;
-    if (p & 1u) sign = R(-1);
+    pathStream = po >> 1u;
+    if (po & 1u) sign = R(-1);
   }
   const uint32_t injectedStream = sc.nStreams > 0 ? min(pathStream, sc.nStreams - 1) : 0u;
   const uint32_t stream = pcg(pcg(sc.seed) ^ pcg(pathStream + 0x9E3779B9u));
@@ -482,6 +483,7 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
       for (int a = 0; a < 4; ++a) S[a][i] = nS4[a][i];
     }
     const uint4 d0 = nd0, d1 = nd1;
+    const R guardJ = A.flags ? A.guard[j] : R(-1);  // < 0: no check
     if (j + 1 < nT) {
       loadFactors(j + 1);
       nd0 = __ldg(dates + 2 * (j + 1)), nd1 = __ldg(dates + 2 * (j + 1) + 1);
@@ -616,13 +618,17 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
               annS[i] = R(0), fltS[i] = R(0);
               if (kSink) {
                 if (act[i]) A.sinkEx[static_cast<size_t>(A.sinkRowOfBermudan[bm] + extra) * nP + pth[i]] = e;
-              } else if (exOf(bm, i) < R(0) && e > R(0) && e > cont) {
-                const R v = static_cast<R>(extra);
-                if (manyBerm) exS[(bm * PPT + i) * kTile + tid] = static_cast<signed char>(extra);
-                else if (bm == 0) ex[0][i] = v;
-                else if (bm == 1) ex[1][i] = v;
-                else if (bm == 2) ex[2][i] = v;
-                else ex[3][i] = v;
+              } else if (exOf(bm, i) < R(0)) {
+                // the exact-decision check: the rule's margins are e (against 0) and e - cont
+                if (act[i] && (fabs(e) <= guardJ || fabs(e - cont) <= guardJ)) flagPath(A.flags, pth[i]);
+                if (e > R(0) && e > cont) {
+                  const R v = static_cast<R>(extra);
+                  if (manyBerm) exS[(bm * PPT + i) * kTile + tid] = static_cast<signed char>(extra);
+                  else if (bm == 0) ex[0][i] = v;
+                  else if (bm == 1) ex[1][i] = v;
+                  else if (bm == 2) ex[2][i] = v;
+                  else ex[3][i] = v;
+                }
               }
             }
             break;
@@ -718,12 +724,18 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
         R required = R(0);
         if (vc > A.hc) required += vc - A.hc;
         if (A.hb >= R(0) && -vc > A.hb) required -= -vc - A.hb;
+        // The call rule |required - held| >= MTA; the exact-decision check flags the path when its margin
+        // | |required - held| - MTA | is within the date's guard.
         if (ctype == 0) {  // cash: one unit is worth one, no division
-          if (j == 0 || fabs(required - held[i]) >= A.mta) held[i] = required;
+          const R gap = fabs(required - held[i]);
+          if (j > 0 && act[i] && fabs(gap - A.mta) <= guardJ) flagPath(A.flags, pth[i]);
+          if (j == 0 || gap >= A.mta) held[i] = required;
           collateral = held[i] + A.ia;
         } else {
           const R keep = A.keepHaircut;
-          if (j == 0 || fabs(required - held[i] * keep * pc) >= A.mta) held[i] = required / (keep * pc);
+          const R gap = fabs(required - held[i] * keep * pc);
+          if (j > 0 && act[i] && fabs(gap - A.mta) <= guardJ) flagPath(A.flags, pth[i]);
+          if (j == 0 || gap >= A.mta) held[i] = required / (keep * pc);
           collateral = held[i] * price + A.ia;
         }
       }

@@ -432,6 +432,24 @@ cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* er
   return cudaGetLastError();
 }
 
+// The exact-decision check's patch: dst[r][map[q]] = src[r][q] (rounded to single precision) for every row r and
+// re-run path q.  One thread per element; map holds distinct paths below nP.
+__global__ void scatterRowsKernel(const double* __restrict__ src, uint32_t m, const uint32_t* __restrict__ map, uint32_t rows,
+                                  float* __restrict__ dst, uint32_t nP) {
+  const uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= static_cast<uint64_t>(rows) * m) return;
+  const uint32_t r = static_cast<uint32_t>(k / m), q = static_cast<uint32_t>(k % m);
+  dst[static_cast<size_t>(r) * nP + map[q]] = static_cast<float>(src[static_cast<size_t>(r) * m + q]);
+}
+
+cudaError_t launchScatterRows(const double* src, uint32_t m, const uint32_t* map, uint32_t rows, float* dst, uint32_t nP,
+                              cudaStream_t stream) {
+  const uint64_t n = static_cast<uint64_t>(rows) * m;
+  if (n == 0) return cudaSuccess;
+  scatterRowsKernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(src, m, map, rows, dst, nP);
+  return cudaGetLastError();
+}
+
 template cudaError_t launchReduce<float>(const ReduceJob<float>*, uint32_t, uint32_t, int, cudaStream_t);
 template cudaError_t launchReduce<double>(const ReduceJob<double>*, uint32_t, uint32_t, int, cudaStream_t);
 template cudaError_t launchRowStats<float>(const RowJob<float>*, uint32_t, uint32_t*, cudaStream_t, uint32_t);

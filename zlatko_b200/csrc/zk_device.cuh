@@ -64,6 +64,9 @@ struct ScenarioArgs {
   uint32_t nF, stepStride;  // stochastic foreign rates (of assets 0 .. nF - 1) and the step row length (24 + 8 nF)
   const R* steps;     // [nT][24]; columns 0..21 are shared by every plan of the batch
   const R* normals;   // injected normals [step][normal][stream], or nullptr (counter-based generator)
+  // Path p of the launch simulates path pathMap[p] of the plan (its normals and antithetic sign; null: p itself):
+  // the re-run of chosen paths by the exact-decision check.
+  const uint32_t* pathMap;
   R cir[8];           // (kappa, theta, xi, y0) per credit
   R spots[4];
   R chol[kChol * kChol];
@@ -112,7 +115,15 @@ struct NsArgs {
   // indices, 5.. the fixings (imWords = 5 + nSlots; imState null without the nested margin).
   R* imState;
   uint32_t imWords, pad1;
+  // Exact decisions (zk_context_set_exact_decisions): a path with a margin call or an exercise decision whose margin
+  // lies within guard[date] of the rule's boundary sets its bit in flags[path / 32]; the host re-runs those paths in
+  // double precision.  flags null: off.
+  uint32_t* flags;
+  const R* guard;
 };
+
+// Marks path p for the double-precision re-check (a rare event: one atomic per flagged decision).
+__device__ __forceinline__ void flagPath(uint32_t* flags, uint32_t p) { atomicOr(flags + (p >> 5), 1u << (p & 31u)); }
 
 // ---- counter-based normals: PCG hash + Box-Muller, keyed by (seed, path stream, date, pair) ----
 // The hash and the key mixing follow the reference kernel (fused_kernels.cpp:185-199,

@@ -93,6 +93,10 @@ template <typename R>
 // maxRounds caps the quantile's narrowing rounds (at most 16, the default); a row that needs more sets
 // kDevBadTerm in err and NaN as its value.
 cudaError_t launchRowStats(const RowJob<R>* jobs, uint32_t numJobs, uint32_t* err, cudaStream_t stream, uint32_t maxRounds = 16);
+// dst[r][map[q]] = float(src[r][q]) for r < rows, q < m (the exact-decision check's patch of re-run paths' rows;
+// the map's paths distinct and below nP).
+cudaError_t launchScatterRows(const double* src, uint32_t m, const uint32_t* map, uint32_t rows, float* dst, uint32_t nP,
+                              cudaStream_t stream);
 
 // One Bermudan of the AMC fit (zk_fit_amc): its exercise dates (grid indices, ascending), its first row of
 // exercise values in the AMC pass, the slots of its fitted records (slotBase + k: policy of exercise k;

@@ -301,6 +301,18 @@ class Context:
         least 24 eligible netting sets; BASIS_OFF: none; BASIS_ALL: every eligible one)."""
         check(lib().zk_context_set_basis(self.handle, int(mode)), self.handle)
 
+    def set_exact_decisions(self, guard: float) -> None:
+        """zk_context_set_exact_decisions: with guard > 0, run / run_plans / run(rows=True) take every margin call
+        and exercise decision as the FP64 mode does on the same normals (paths with a decision inside the guard band
+        re-run in FP64); 0 turns it off."""
+        check(lib().zk_context_set_exact_decisions(self.handle, float(guard)), self.handle)
+
+    def exact_stats(self) -> tuple:
+        """zk_context_exact_stats: (paths re-run in FP64, paths checked) since the last call."""
+        f, n = C.c_uint64(0), C.c_uint64(0)
+        check(lib().zk_context_exact_stats(self.handle, C.byref(f), C.byref(n)), self.handle)
+        return int(f.value), int(n.value)
+
     INJECT_FAIL_LAUNCH, INJECT_ROW_ROUNDS = 1, 2
 
     def inject(self, what: int, value: int) -> None:
