@@ -774,11 +774,12 @@ def main():
         # e2e through the public C ABI: host plan tables in, host statistics out.
         for _ in range(a.warmup):
             ctx.run_many(plans)
-        e2e_s = []
+        e2e_s, phases = [], []
         for _ in range(a.steps):
             t0 = time.perf_counter()
             ctx.run_many(plans)
             e2e_s.append(time.perf_counter() - t0)
+            phases.append(ctx.call_timings())
     value, e2e, t_step, t_e2e = replica_throughput(revals * a.steps, float(np.sum(step_ms)) / 1e3, float(np.sum(e2e_s)), world,
                                                    dist, "cuda")
 
@@ -837,7 +838,8 @@ def main():
             "per_reporting_date": {"value": value * nR / nT, "unit": "scenario x trade revaluations/s on reporting dates",
                                    "note": "paths x reporting dates x trades / device time; the other simulation dates "
                                            "are the margin-call dates t - MPR"},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "host_ms_median": {k: float(np.median([ph[k] for ph in phases])) for k in phases[0]} if phases else None},
             "gpu_launches": int(info.kernels_per_execute) * a.steps,
             "tile_paths": int(info.tile_paths),
             "kernel_ms": {"simulate": float(np.mean(sim_ms)), "revalue": float(np.mean(fused_ms)), "reduce": float(np.mean(reduce_ms)),

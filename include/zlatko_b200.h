@@ -120,6 +120,11 @@ zk_status zk_context_set_basis(zk_context* ctx, uint32_t mode);
 zk_status zk_context_set_exact_decisions(zk_context* ctx, double guard);
 zk_status zk_context_exact_stats(zk_context* ctx, uint64_t* flagged_paths, uint64_t* checked_paths);
 
+/* Host wall time in milliseconds of the last zk_run_plans / zk_run_plan call, by phase: [0] validate and lower the
+ * plans (the basis groups included), [1] fill and send the inputs, [2] the device run, [3] the exact-decision check,
+ * [4] the read-back into the caller's buffers.  No counterpart in the reference. */
+zk_status zk_context_call_timings(const zk_context* ctx, double* ms5);
+
 /* ---- the drop-in backend ------------------------------------------------------------------------ */
 /* Replaces gpu::runFusedReference(plan) (src/gpu/fused_reference.cpp:628-630): the fused-exposure,
  * reduce-partials and row-statistics kernels (src/gpu/fused_kernels.cpp:224-530, :538-563,

@@ -96,3 +96,20 @@ def test_two_regressor_plan_runs_with_one_regressor_bermudans(ctx):
     ex = int(p.header[25])
     for b in range(2):
         assert np.array_equal(rows[ex + b], e.exercise[b]), f"Bermudan {b}: exercise decisions differ"
+
+
+def test_bermudan_book_with_the_two_regressor_basis_in_fp64(ctx):
+    """Two netting sets (8 Bermudans, 10y annual, exercise 1y-9y) of the AMC book with the two-regressor basis at
+    20,000 paths: every exercise decision equal to the FP64 engine's with the same basis."""
+    from zlatko_b200 import workloads
+
+    m, books, _ = workloads.bermudan_book(20_000, basis="rate_swap")
+    for ns in books[:2]:
+        p = gpu.compile(m, ns, S.Options(exercise_views=True, samples=1))
+        z, streams = normals(p, 13)
+        f = ctx.fit_amc_f64(p, z, streams)
+        _, _, rows = ctx.run_f64(f, z, streams, rows=True)
+        e = restated.engine_run(S.encode_model(m), S.encode_netting_set(ns), 0.95, z, streams, m.num_paths)
+        ex = int(p.header[25])
+        for b in range(len(ns.trades)):
+            assert np.array_equal(rows[ex + b], e.exercise[b]), f"Bermudan {b}: exercise decisions differ"

@@ -66,7 +66,7 @@ class BatchInfo(C.Structure):
 
 # Every entry point declared in include/zlatko_b200.h.
 EXPORTS = ["zk_abi_version", "zk_context_create", "zk_context_destroy", "zk_last_error", "zk_context_set_stream", "zk_context_set_row_budget", "zk_context_set_basis", "zk_debug_basis",
-           "zk_context_set_exact_decisions", "zk_context_exact_stats",
+           "zk_context_set_exact_decisions", "zk_context_exact_stats", "zk_context_call_timings",
            "zk_run_plan", "zk_run_plan_rows", "zk_run_plans", "zk_amc_states", "zk_fit_amc", "zk_fit_amc_f64", "zk_run_plan_f64", "zk_run_plan_injected", "zk_run_plan_noalloc", "zk_debug_inject",
            "zk_batch_create", "zk_batch_execute", "zk_batch_set_tile_paths", "zk_batch_timings", "zk_batch_read", "zk_batch_info_get",
            "zk_batch_destroy", "zk_peak_ex2", "zk_gemm_bf16", "zk_surrogate_create", "zk_surrogate_destroy",
@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         "zk_context_set_basis": (st, [vp, C.c_uint32]),
         "zk_context_set_exact_decisions": (st, [vp, C.c_double]),
         "zk_context_exact_stats": (st, [vp, P(C.c_uint64), P(C.c_uint64)]),
+        "zk_context_call_timings": (st, [vp, P(C.c_double)]),
         "zk_run_plan": (st, [vp, P(PlanView), P(Output)]),
         "zk_run_plans": (st, [vp, P(PlanView), sz, P(Output)]),
         "zk_amc_states": (st, [vp, P(PlanView), vp, vp, vp, sz]),

@@ -1,6 +1,7 @@
 // The C ABI of zlatko_b200 (include/zlatko_b200.h): plan validation, batching, device memory and
 // the launch sequence fused-exposure -> reduce -> row statistics.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -141,6 +142,16 @@ struct zk_context {
   // calls re-ran in double precision out of the paths they ran.
   double exactGuard = 0.0;
   uint64_t exactFlagged = 0, exactPaths = 0;
+  // Host wall time of the last zk_run_plans call by phase (zk_context_call_timings): validate and lower the plans
+  // (basis groups included), fill and send the inputs, the device run up to its read-back, the exact-decision check
+  // and the copy into the caller's buffers; milliseconds.
+  double callMs[5] = {0, 0, 0, 0, 0};
+  // zk_run_plans simulates the first plan's scenario before it lowers the plans on the host: the cube and the step
+  // table it reads, grown as needed.
+  void* cube = nullptr;
+  size_t cubeBytes = 0;
+  void* presimSteps = nullptr;
+  size_t presimStepsBytes = 0;
 };
 
 namespace {
@@ -587,6 +598,7 @@ struct Batch {
     bool cashBig = true, cashSmall = true, cashAll = true;
     bool perTrade = false, probes = false, lean = true;
     size_t nsOff = 0, cubeOff = 0;  // device offsets of NsArgs[] and the factor cube
+    R* presim = nullptr;            // the cube, simulated ahead in the context's cube buffer (not in the arena)
     // Memory-bounded batches: the launch's netting sets [first, first + count) of planIdx run as one wave whose
     // rows and partials reuse the same device region as every other wave; its reduce and row-statistics jobs are
     // [reduceFirst, + count) and [rowFirst, + rowCount) of the job arrays.
@@ -760,12 +772,40 @@ void formGroups(Batch<R>& B, typename Batch<R>::Launch& L, uint32_t mode, HostPo
   }
 }
 
+// The simulation arguments of a launch whose first plan is P0 (probes: the launch's plans read ln S and the CIR
+// states); returns the cube's number of fields.
+template <typename R>
+uint32_t scenarioOf(const Plan<R>& P0, bool probes, size_t streams, ScenarioArgs<R>& sc, CubeArgs<R>& cb) {
+  sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
+  sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
+  sc.nF = P0.nF, sc.stepStride = P0.stepStride;
+  sc.steps = nullptr, sc.normals = nullptr, sc.pathMap = nullptr;
+  for (int k = 0; k < 8; ++k) sc.cir[k] = P0.v.params[k];
+  for (int k = 0; k < 4; ++k) sc.spots[k] = P0.v.params[12 + k];
+  for (int k = 0; k < 64; ++k) sc.chol[k] = P0.v.params[16 + k];
+  cb.data = nullptr;
+  cb.nP = P0.nP, cb.nT = P0.nT, cb.nA = P0.nA, cb.nC = P0.nC;
+  cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fXf = 2 + P0.nA + P0.nC, cb.nF = P0.nF;
+  cb.fLnS = cb.fXf + P0.nF, cb.fY = cb.fLnS + P0.nA;
+  cb.probes = probes ? 1u : 0u;
+  cb.pad = 0;
+  return (probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC) + P0.nF;
+}
+
+// A simulation launched ahead of the batch's host work (zk_run_plans): the factor cube of the first plan's scenario,
+// in the context's cube buffer, with or without the probe fields.
+struct Presim {
+  float* cube = nullptr;
+  bool probes = false;
+};
+
 // Options of a batch beyond its plans: the exact-decision check (guard bands and flags; term-by-term revaluation),
 // or the re-run of chosen paths (maps[i]: the paths of plan i, its header's path count their number; every plan its
 // own launch; term by term).
 struct BuildOpts {
   bool exact = false;
   const std::vector<std::vector<uint32_t>>* maps = nullptr;
+  const Presim* presim = nullptr;  // the first plan's scenario already simulated (single precision, counter normals)
 };
 
 template <typename R>
@@ -829,20 +869,11 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
                P.rowTrades == kNoRow;
     }
     const Plan<R>& P0 = B->plans[L.planIdx.front()];
-    ScenarioArgs<R>& sc = L.sc;
-    sc.nP = P0.nP, sc.nT = P0.nT, sc.nA = P0.nA, sc.nC = P0.nC, sc.substeps = P0.sub, sc.nNormals = P0.nNormals;
-    sc.nCorr = P0.nCorr, sc.seed = P0.seed, sc.antithetic = P0.anti, sc.nStreams = static_cast<uint32_t>(streams);
-    sc.nF = P0.nF, sc.stepStride = P0.stepStride;
-    sc.steps = nullptr, sc.normals = nullptr, sc.pathMap = nullptr;
-    for (int k = 0; k < 8; ++k) sc.cir[k] = P0.v.params[k];
-    for (int k = 0; k < 4; ++k) sc.spots[k] = P0.v.params[12 + k];
-    for (int k = 0; k < 64; ++k) sc.chol[k] = P0.v.params[16 + k];
-    CubeArgs<R>& cb = L.cb;
-    cb.nP = P0.nP, cb.nT = P0.nT, cb.nA = P0.nA, cb.nC = P0.nC;
-    cb.fS = 2, cb.fQ = 2 + P0.nA, cb.fXf = 2 + P0.nA + P0.nC, cb.nF = P0.nF;
-    cb.fLnS = cb.fXf + P0.nF, cb.fY = cb.fLnS + P0.nA;
-    cb.probes = L.probes ? 1u : 0u;
-    L.numFields = (L.probes ? 2 + 2 * P0.nA + 2 * P0.nC : 2 + P0.nA + P0.nC) + P0.nF;
+    L.numFields = scenarioOf(P0, L.probes, streams, L.sc, L.cb);
+    if constexpr (sizeof(R) == 4)  // the launch of plan 0 finds its cube simulated when the probe fields agree
+      if (opts.presim && !sink && !normals && !opts.maps && opts.presim->probes == L.probes &&
+          std::find(L.planIdx.begin(), L.planIdx.end(), 0u) != L.planIdx.end())
+        L.presim = opts.presim->cube;
     if (revalueSmemBytes(L.stateWordsMax, L.perTrade, sizeof(R) == 8, 1) > 200 * 1024)
       throw fail(ZK_ERR_UNSUPPORTED, "a netting set needs more shared memory than a CTA has");
   }
@@ -898,7 +929,7 @@ std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, boo
   }
   B->inputBytes = off;
   for (auto& L : B->launches)
-    L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
+    if (!L.presim) L.cubeOff = take(static_cast<size_t>(L.numFields) * L.sc.nT * L.sc.nP * sizeof(R));
   // Rows and warp partials: one region per plan, or -- when they exceed the row budget -- waves of netting sets
   // (in each launch's order) that reuse one region, sized by the largest wave.
   auto rowsBytes = [&](const Plan<R>& P) {
@@ -1061,7 +1092,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
         A.imState = static_cast<R*>(dptr(D.imState));
         A.imWords = 5 + P.nSlots;
         ImArgs<R> M{};
-        M.cube = static_cast<const R*>(dptr(L.cubeOff));
+        M.cube = L.presim ? L.presim : static_cast<const R*>(dptr(L.cubeOff));
         M.dates = A.dates, M.table = A.table, M.steps = A.steps;
         M.model = static_cast<const R*>(dptr(D.imModel));
         M.slots = static_cast<const uint32_t*>(dptr(D.imSlots));
@@ -1090,7 +1121,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
         if (!I.blob.empty()) std::memcpy(img + G.blob, I.blob.data(), I.blob.size() * 2);
         std::memcpy(img + G.scale, I.scale.data(), I.scale.size() * 4);
         BasisArgs a{};
-        a.cube = static_cast<const float*>(dptr(L.cubeOff));
+        a.cube = L.presim ? reinterpret_cast<const float*>(L.presim) : static_cast<const float*>(dptr(L.cubeOff));
         a.nP = L.sc.nP, a.nT = L.sc.nT, a.nA = L.cb.nA, a.nC = L.cb.nC, a.nF = L.cb.nF;
         a.fS = L.cb.fS, a.fQ = L.cb.fQ, a.fXf = L.cb.fXf;
         a.dates = static_cast<const uint32_t*>(dptr(G.dates));
@@ -1109,7 +1140,7 @@ void fillImage(Batch<R>& B, const double* normals, size_t streams, unsigned char
     L.sc.steps = static_cast<const R*>(dptr(B.dev[L.planIdx.front()].steps));
     L.sc.normals = normals ? static_cast<const R*>(dptr(B.normalsOff)) : nullptr;
     L.sc.pathMap = P0.pathMap.empty() ? nullptr : static_cast<const uint32_t*>(dptr(B.dev[L.planIdx.front()].pathMap));
-    L.cb.data = static_cast<R*>(dptr(L.cubeOff));
+    L.cb.data = L.presim ? L.presim : static_cast<R*>(dptr(L.cubeOff));
     (void)P0;
   }
   std::vector<ReduceJob<R>> red(B.plans.size());
@@ -1297,6 +1328,7 @@ void execute(Batch<R>& B, bool capturing = false) {
     ZK_CUDA(recordEvent(B.ev[1], s, capturing));
   } else {
     for (auto& L : B.launches) {
+      if (L.presim) continue;  // simulated ahead of the host work
       injectPoint(ctx);
       ZK_CUDA(launchSimulate<R>(L.sc, L.cb, s));
     }
@@ -1831,6 +1863,8 @@ void zk_context_destroy(zk_context* ctx) {
     cudaStreamDestroy(ctx->side);
   }
   for (auto& blk : ctx->spareBlocks) cudaFree(blk.first);
+  if (ctx->cube) cudaFree(ctx->cube);
+  if (ctx->presimSteps) cudaFree(ctx->presimSteps);
   for (auto w : ctx->workers) {
     cudaStreamSynchronize(w);
     cudaStreamDestroy(w);
@@ -1872,6 +1906,12 @@ zk_status zk_context_set_exact_decisions(zk_context* ctx, double guard) {
   return ZK_OK;
 }
 
+zk_status zk_context_call_timings(const zk_context* ctx, double* ms5) {
+  if (!ctx || !ms5) return ZK_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 5; ++k) ms5[k] = ctx->callMs[k];
+  return ZK_OK;
+}
+
 zk_status zk_context_exact_stats(zk_context* ctx, uint64_t* flagged_paths, uint64_t* checked_paths) {
   if (!ctx || !flagged_paths || !checked_paths) return ZK_ERR_INVALID_ARGUMENT;
   *flagged_paths = ctx->exactFlagged, *checked_paths = ctx->exactPaths;
@@ -1908,6 +1948,44 @@ zk_status zk_debug_basis(const zk_plan_view* plans, size_t n, const double* x, c
   }
 }
 
+namespace {
+// The first plan's scenario simulated on the context's stream into the context's cube buffer, so that the factor
+// cube is being written while the host validates and lowers the plans; build() hands it to the launch that holds
+// plan 0 when that launch needs the same fields (else the launch simulates again).  The step table goes up first;
+// the buffers are reused by later calls, which synchronise before they return.
+Presim presimulate(zk_context* ctx, const zk_plan_view& v0) {
+  Presim pre;
+  const Plan<float> P0 = parse(viewOf(v0), 0);
+  ScenarioArgs<float> sc;
+  CubeArgs<float> cb;
+  const uint32_t fields = scenarioOf(P0, P0.probes, 0, sc, cb);
+  const size_t cubeBytes = static_cast<size_t>(fields) * P0.nT * P0.nP * 4, stepBytes = static_cast<size_t>(P0.nT) * P0.stepStride * 4;
+  if (ctx->cubeBytes < cubeBytes) {
+    if (ctx->cube) ZK_CUDA(cudaFree(ctx->cube));
+    ctx->cube = nullptr, ctx->cubeBytes = 0;
+    if (cudaMalloc(&ctx->cube, cubeBytes) != cudaSuccess) {
+      cudaGetLastError();
+      return pre;  // no room beside the arena: the batch simulates inside its own
+    }
+    ctx->cubeBytes = cubeBytes;
+  }
+  if (ctx->presimStepsBytes < stepBytes) {
+    if (ctx->presimSteps) ZK_CUDA(cudaFree(ctx->presimSteps));
+    ctx->presimSteps = nullptr, ctx->presimStepsBytes = 0;
+    ZK_CUDA(cudaMalloc(&ctx->presimSteps, stepBytes));
+    ctx->presimStepsBytes = stepBytes;
+  }
+  ZK_CUDA(cudaMemcpyAsync(ctx->presimSteps, P0.v.steps, stepBytes, cudaMemcpyHostToDevice, ctx->stream));
+  sc.steps = static_cast<const float*>(ctx->presimSteps);
+  cb.data = static_cast<float*>(ctx->cube);
+  injectPoint(ctx);
+  ZK_CUDA(launchSimulate<float>(sc, cb, ctx->stream));
+  pre.cube = static_cast<float*>(ctx->cube);
+  pre.probes = P0.probes;
+  return pre;
+}
+}  // namespace
+
 zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_output* outs) {
   try {
     requireCtx(ctx);
@@ -1916,13 +1994,27 @@ zk_status zk_run_plans(zk_context* ctx, const zk_plan_view* plans, size_t n, zk_
     for (size_t i = 0; i < n; ++i) views.push_back(viewOf(plans[i]));
     BuildOpts bo;
     bo.exact = ctx->exactGuard > 0.0;
+    using Clock = std::chrono::steady_clock;
+    auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    const auto t0 = Clock::now();
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));  // a failed earlier call may have left work on the buffers
+    const Presim pre = presimulate(ctx, plans[0]);
+    bo.presim = &pre;
     auto B = build<float>(ctx, views, false, nullptr, 0, bo);
     checkOutputs(*B, outs, false);
+    const auto t1 = Clock::now();
     upload(*B, ctx, true, nullptr, 0);
+    const auto t2 = Clock::now();
     execute(*B);
+    ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+    const auto t3 = Clock::now();
     const auto patches = exactCheck(*B);
+    const auto t4 = Clock::now();
     readOutputs(*B, outs);
     applyPatches(patches, outs);
+    const auto t5 = Clock::now();
+    ctx->callMs[0] = ms(t0, t1), ctx->callMs[1] = ms(t1, t2), ctx->callMs[2] = ms(t2, t3), ctx->callMs[3] = ms(t3, t4);
+    ctx->callMs[4] = ms(t4, t5);
     return ZK_OK;
   } catch (const Failure& f) {
     return record(ctx, f);

@@ -313,6 +313,12 @@ class Context:
         check(lib().zk_context_exact_stats(self.handle, C.byref(f), C.byref(n)), self.handle)
         return int(f.value), int(n.value)
 
+    def call_timings(self) -> dict:
+        """zk_context_call_timings: host wall milliseconds of the last run / run_many call by phase."""
+        ms = (C.c_double * 5)()
+        check(lib().zk_context_call_timings(self.handle, ms), self.handle)
+        return dict(zip(("lower", "upload", "device", "exact_check", "read"), [float(v) for v in ms]))
+
     INJECT_FAIL_LAUNCH, INJECT_ROW_ROUNDS = 1, 2
 
     def inject(self, what: int, value: int) -> None:
