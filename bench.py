@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--tile-paths", type=int, default=0, help="pin the tile shape (128/256/512) instead of the autotuned one")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate leg")
     ap.add_argument("--surrogate-paths", type=int, default=65_536)
-    ap.add_argument("--surrogate-train-paths", type=int, default=384)
+    ap.add_argument("--surrogate-train-paths", type=int, default=512)
     ap.add_argument("--no-amc", action="store_true", help="skip the Bermudan (AMC) leg")
     ap.add_argument("--amc-paths", type=int, default=200_000)
     ap.add_argument("--no-amc-surrogate", action="store_true", help="skip the AMC continuation surrogate leg")
@@ -295,8 +295,9 @@ def surrogate_leg(ctx, a):
     per-netting-set fallback, against the plain GPU pricer on the same paths: device time of each, the CVA difference
     and the fallbacks.  The surrogate revalues every simulation date (the margin-call dates included) and the GPU
     applies the collateral rule per path.  The network is trained on the per-trade values the plain pricer itself
-    produces on --surrogate-train-paths paths (every live trade and reporting date: about 40M revaluations for this
-    book); training is reported apart, it runs once per book."""
+    produces on --surrogate-train-paths paths (every live trade and reporting date: about 53M revaluations for this
+    book at 512 paths, the 50M the surrogate configuration asks for); training is reported apart, it runs once per
+    book."""
     from zlatko_b200 import surrogate_book as SB
     from zlatko_b200 import workloads
     from zlatko_b200.surrogate import Surrogate
