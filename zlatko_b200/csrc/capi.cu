@@ -498,8 +498,38 @@ void lowerTerms(Plan<R>& p) {
     for (const R* r = first; r < last; r += kTermStride)
       if (isAsset(r)) push4(r[2], r[3], r[1], 0.0);
     d[3] = units();
-    for (const R* r = first; r < last; r += kTermStride)
-      if (!isFloat(r) && !isBond(r) && !isFixing(r) && !isAsset(r)) p.table.insert(p.table.end(), r, r + kTermStride);
+    // Generic records in plan order.  A run of two or more Bermudan bonds (kBermBond) of one Bermudan and trade group
+    // becomes a block: a header record (the run's code with extra 0, -count, the largest exercise index) and two
+    // bonds (c, A, B, exercise index) per record; the kernel skips the block in a warp none of whose paths has
+    // exercised that Bermudan by then, and otherwise adds each bond as the record would.
+    auto bermBond = [&](const R* r) { return (static_cast<uint32_t>(r[0]) & 15u) == static_cast<uint32_t>(kBermBond); };
+    for (const R* r = first; r < last;) {
+      if (isFloat(r) || isBond(r) || isFixing(r) || isAsset(r)) {
+        r += kTermStride;
+        continue;
+      }
+      const uint32_t low = static_cast<uint32_t>(r[0]) & 0xFFFu;
+      const R* e = r;
+      if (bermBond(r))
+        while (e < last && bermBond(e) && (static_cast<uint32_t>(e[0]) & 0xFFFu) == low) e += kTermStride;
+      const size_t n = static_cast<size_t>(e - r) / kTermStride;
+      if (n < 2) {
+        p.table.insert(p.table.end(), r, r + kTermStride);
+        r += kTermStride;
+        continue;
+      }
+      double maxEx = 0.0;
+      for (const R* q = r; q < e; q += kTermStride) maxEx = std::max(maxEx, static_cast<double>(static_cast<uint32_t>(q[0]) >> 12u));
+      push4(static_cast<double>(low), -static_cast<double>(n), maxEx, 0.0);
+      push4(0.0, 0.0, 0.0, 0.0);
+      for (size_t q = 0; q < n; ++q) {
+        const R* b = r + q * kTermStride;
+        p.table.push_back(b[2]), p.table.push_back(b[3]), p.table.push_back(b[4]);
+        p.table.push_back(static_cast<R>(static_cast<uint32_t>(b[0]) >> 12u));
+      }
+      if (n % 2) push4(0.0, 0.0, 0.0, -1.0);
+      r = e;
+    }
     d[4] = units();
     for (const R* r = first; r < last; r += kTermStride)
       if (isFixing(r)) push4(r[3], -static_cast<double>(r[4]) * bScale, 1.0 / static_cast<double>(r[2]), r[1]);

@@ -536,8 +536,31 @@ __global__ void __launch_bounds__(kTile, (revalueMinBlocks<PPT, kLean, kSmallSta
       loadTerm(table + 4 * u, rec);
       const uint32_t code = static_cast<uint32_t>(rec[0]);
       const uint32_t kind = code & 15u, bm = bermudanOf(code, manyBerm), extra = code >> 12u;
-      const uint32_t slot = static_cast<uint32_t>(rec[1]);
       const uint32_t grp = min((code >> 4u) & 15u, 15u);
+      if (!kLean && kind == kBermBond && rec[1] < R(0)) {
+        // A block of nb bonds of Bermudan bm (the lowering's run of its kBermBond records): each counts on a path
+        // that exercised at or before the bond's exercise index; a warp with no such path skips the block.
+        const uint32_t nb = static_cast<uint32_t>(-rec[1]);
+        R exi[PPT];
+        bool live = false;
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) exi[i] = exOf(bm, i), live = live || (exi[i] >= R(0) && exi[i] <= rec[2]);
+        if (__any_sync(0xFFFFFFFFu, live))
+          for (uint32_t q = 0; q < nb; ++q) {
+            const R4 b = ld4(table + 4 * (u + 2 + q));
+            const R nBq = -b.z;
+#pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              R term = R(0);
+              if (exi[i] >= R(0) && exi[i] <= b.w) term = b.x * (b.y * fastExp(nBq * x[i]));
+              if (kPerTrade && A.nTr > 0) vt(grp, i) += term;
+              else value[i] += term;
+            }
+          }
+        u += 2 * ((nb + 1) / 2);
+        continue;
+      }
+      const uint32_t slot = static_cast<uint32_t>(rec[1]);
       const R c = rec[2], nB = -rec[4];
       R term[PPT];
 #pragma unroll
@@ -898,6 +921,17 @@ __device__ R innerDateValue(const ImArgs<R>& M, uint32_t jj, R x, const R (&S)[4
     loadTerm(table + 4 * u, rec);
     const uint32_t code = static_cast<uint32_t>(rec[0]);
     const uint32_t kind = code & 15u, bm = min((code >> 8u) & 15u, 3u), extra = code >> 12u;
+    if (kind == kBermBond && rec[1] < R(0)) {  // a block of the Bermudan's bonds (see the outer kernel)
+      const uint32_t nb = static_cast<uint32_t>(-rec[1]);
+      const R e = sel4(ex, bm);
+      if (e >= R(0) && e <= rec[2])
+        for (uint32_t q = 0; q < nb; ++q) {
+          const R4 b = ld4(table + 4 * (u + 2 + q));
+          if (e <= b.w) value += b.x * (b.y * fastExp(-b.z * x));
+        }
+      u += 2 * ((nb + 1) / 2);
+      continue;
+    }
     const uint32_t slot = static_cast<uint32_t>(rec[1]);
     const R c = rec[2];
     switch (kind) {
