@@ -29,6 +29,7 @@ constexpr int kBins = 4096;
 constexpr int kCap = 4096;
 constexpr int kMaxRounds = 16;
 constexpr int kHistBins = 3072;  // the reference's histogram-request limit (kPfeBins)
+constexpr int kGather = 4096;    // values of the first histogram pass kept from the bins the sample points at
 
 template <typename R>
 struct RowSmem {
@@ -36,6 +37,8 @@ struct RowSmem {
     uint32_t hist[kBins];
     R cand[kCap];
   };
+  R gath[kGather];
+  uint32_t gathCount;
   double dsum[kRowWarps];
   R rmin[kRowWarps], rmax[kRowWarps];
   uint32_t candCount;
@@ -70,14 +73,27 @@ __device__ __forceinline__ void blockMinMax(R& lo, R& hi, R* smin, R* smax) {
   __syncthreads();
 }
 
-__device__ __forceinline__ uint32_t binOf(double v, double lo, double invw) {
-  const double f = (v - lo) * invw;
+// The bin of a value over a range starting at lo, `scale` bins per unit: any non-decreasing map of the values to the
+// bins serves the rank search, as long as every pass of a round uses the same one.  Double rows: floor((v - lo)
+// scale) in double.  Single-precision rows: (v - lo) scale in float, clamped, rounded to an integer by adding 2^23
+// (an FMA-pipe add and an integer subtract instead of two conversions per value); scaleOf gives the float scale.
+__device__ __forceinline__ uint32_t binOf(double v, double lo, double scale) {
+  const double f = (v - lo) * scale;
   const uint32_t b = f <= 0.0 ? 0u : (f >= static_cast<double>(kBins) ? static_cast<uint32_t>(kBins) : static_cast<uint32_t>(f));
   return min(b, static_cast<uint32_t>(kBins - 1));
 }
+__device__ __forceinline__ uint32_t binOf(float v, double lo, double scale) {
+  const float f = fminf(fmaxf((v - static_cast<float>(lo)) * static_cast<float>(scale), 0.0f), static_cast<float>(kBins - 1));
+  return __float_as_uint(f + 8388608.0f) - 0x4B000000u;
+}
+template <typename R>
+__device__ __forceinline__ double scaleOf(R lo, R hi) {
+  const double sc = static_cast<double>(kBins) / (static_cast<double>(hi) - static_cast<double>(lo));
+  return sizeof(R) == 4 ? static_cast<double>(static_cast<float>(sc)) : sc;
+}
 
 template <typename R>
-__device__ __forceinline__ bool passes(const RowSmem<R>& s, int rounds, double v) {
+__device__ __forceinline__ bool passes(const RowSmem<R>& s, int rounds, R v) {
   for (int r = 0; r < rounds; ++r) {
     const uint32_t b = binOf(v, s.flo[r], s.finvw[r]);
     if (b < s.fb0[r] || b > s.fb1[r]) return false;
@@ -148,6 +164,34 @@ __device__ __forceinline__ void sampleMinMax(const R* X, uint32_t nP, bool pos, 
   }
 }
 
+// The histogram of the same sample as sampleMinMax over the bins of (dlo, invw), bin 0's votes per warp as in the
+// full pass; returns the number of values sampled.
+template <typename R>
+__device__ __forceinline__ uint32_t sampleHistogram(const R* X, uint32_t nP, bool pos, double dlo, double invw, uint32_t* hist) {
+  constexpr uint32_t kVec = 16 / sizeof(R);
+  const uint32_t nv = nP / kVec, blocks = nv / 32, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t zero = 0;  // this lane's values in bin 0, summed over the warp at the end
+  auto put = [&](R x) {
+    x = pos ? fmax(x, R(0)) : x;
+    const uint32_t b = binOf(x, dlo, invw);
+    zero += b == 0 ? 1u : 0u;
+    if (b != 0) atomicAdd(&hist[b], 1u);
+  };
+  for (uint32_t b = warp * kSampleStride; b < blocks; b += kRowWarps * kSampleStride) {
+    const uint32_t i = b * 32 + lane;
+    if constexpr (sizeof(R) == 4) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(X) + i);
+      put(q.x), put(q.y), put(q.z), put(q.w);
+    } else {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(X) + i);
+      put(q.x), put(q.y);
+    }
+  }
+  zero = __reduce_add_sync(0xFFFFFFFFu, zero);
+  if (lane == 0 && zero) atomicAdd(&hist[0], zero);
+  return (blocks + kSampleStride - 1) / kSampleStride * 32u * kVec;
+}
+
 // The bins of ranks k and k1 >= k among the candidates counted in s.hist, `below` values ranking under bin 0:
 // pick = {bin of k, bin of k1, values under k's bin, count of k's bin}, as a walk over the bins in order would
 // find them.  One warp: lane l owns bins [128 l, 128 l + 128) (read skewed by l, free of bank conflicts), a
@@ -213,7 +257,7 @@ __device__ void bitonicSort(R* a, uint32_t n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err,
+__global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>* __restrict__ jobs, uint32_t* __restrict__ err,
                                                                  uint32_t maxRounds) {
   extern __shared__ __align__(16) unsigned char raw[];
   RowSmem<R>& s = *reinterpret_cast<RowSmem<R>*>(raw);
@@ -304,6 +348,24 @@ __global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>
   int rounds = 0;
   R vk = lo, vk1 = lo;
   bool done = false;
+  // On a sampled row the sample's own histogram (same bins as round 0's) says where ranks k, k1 lie to within the
+  // sample's rank error: round 0 then keeps the row's values of the bins holding sample ranks k_s -+ (3 sd + 4) and,
+  // when those hold every value of the bins of k and k1, the quantile is read from them without another pass.
+  uint32_t winLo = 1, winHi = 0;
+  if (sampled) {
+    const double dlo0 = static_cast<double>(lo), invw0 = scaleOf(lo, hi);
+    for (uint32_t b = tid; b < kBins; b += kRowThreads) s.hist[b] = 0;
+    if (tid == 0) s.gathCount = 0;
+    __syncthreads();
+    const uint32_t ns = sampleHistogram(X, nP, pos, dlo0, invw0, s.hist);
+    __syncthreads();
+    const double q = static_cast<double>(k) / static_cast<double>(nP), ks = q * static_cast<double>(ns);
+    const double sd = sqrt(static_cast<double>(ns) * q * (1.0 - q)) * 3.0 + 4.0;
+    const uint32_t rlo = static_cast<uint32_t>(fmax(ks - sd, 0.0)), rhi = static_cast<uint32_t>(fmin(ks + sd + 1.0, ns - 1.0));
+    if (tid < 32) locateRanks(s, 0u, rlo, rhi, tid);
+    __syncthreads();
+    winLo = s.pick[0], winHi = s.pick[1];
+  }
   while (!done) {
     if (rounds >= static_cast<int>(maxRounds)) {
       if (tid == 0) atomicExch(err, kDevBadTerm), out[0] = R(NAN);
@@ -313,7 +375,7 @@ __global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>
     if (rounds > 0) {
       lo = R(INFINITY), hi = R(-INFINITY);
       forEachValue(X, nP, pos, [&](R v, bool ok) {
-        if (ok && passes(s, rounds, static_cast<double>(v))) lo = fmin(lo, v), hi = fmax(hi, v);
+        if (ok && passes(s, rounds, v)) lo = fmin(lo, v), hi = fmax(hi, v);
       });
       blockMinMax(lo, hi, s.rmin, s.rmax);
       if (!(lo < hi)) {  // every candidate has the same value
@@ -321,31 +383,59 @@ __global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>
         break;
       }
     }
-    const double dlo = static_cast<double>(lo), invw = static_cast<double>(kBins) / (static_cast<double>(hi) - dlo);
+    const double dlo = static_cast<double>(lo), invw = scaleOf(lo, hi);
     for (uint32_t b = tid; b < kBins; b += kRowThreads) s.hist[b] = 0;
     __syncthreads();
-    // Bin 0 holds the row's minimum, the dominant duplicate of exposure rows (exact zeros): its lanes are
-    // counted with one vote per warp instead of contended shared-memory atomics.
+    // Bin 0 holds the row's minimum, the dominant duplicate of exposure rows (exact zeros): each lane counts its own
+    // and the warp adds them once, instead of contended shared-memory atomics.
     uint32_t zeroBin = 0;
+    const bool gather = rounds == 0 && winLo <= winHi;
     forEachValue(X, nP, pos, [&](R x, bool ok) {
-      const double v = static_cast<double>(x);
-      const bool in = ok && passes(s, rounds, v);
-      const uint32_t b = binOf(v, dlo, invw);
-      zeroBin += __popc(__ballot_sync(0xFFFFFFFFu, in && b == 0));
+      const bool in = ok && passes(s, rounds, x);
+      const uint32_t b = binOf(x, dlo, invw);
+      zeroBin += in && b == 0 ? 1u : 0u;
       if (in && b != 0) atomicAdd(&s.hist[b], 1u);
+      if (gather && in && b >= winLo && b <= winHi) {
+        const uint32_t at = atomicAdd(&s.gathCount, 1u);
+        if (at < static_cast<uint32_t>(kGather)) s.gath[at] = x;
+      }
     });
+    zeroBin = __reduce_add_sync(0xFFFFFFFFu, zeroBin);
     if ((tid & 31u) == 0 && zeroBin) atomicAdd(&s.hist[0], zeroBin);
     __syncthreads();
     if (tid < 32) locateRanks(s, below, k, k1, tid);
     __syncthreads();
     const uint32_t b0 = s.pick[0], b1 = s.pick[1], below0 = s.pick[2], c0 = s.pick[3];
+    if (gather && winLo <= b0 && b1 <= winHi && s.gathCount <= static_cast<uint32_t>(kGather)) {
+      // Every value of bins b0..b1 was kept (no bin between them holds one): sort them, read ranks k and k1.
+      if (tid == 0) s.candCount = 0;
+      __syncthreads();
+      const uint32_t ng = s.gathCount;
+      for (uint32_t i = tid; i < ng; i += kRowThreads) {
+        const R v = s.gath[i];
+        const uint32_t b = binOf(v, dlo, invw);
+        if (b >= b0 && b <= b1) {
+          const uint32_t at = atomicAdd(&s.candCount, 1u);
+          if (at < static_cast<uint32_t>(kCap)) s.cand[at] = v;
+        }
+      }
+      __syncthreads();
+      const uint32_t n = s.candCount;
+      if (n <= static_cast<uint32_t>(kCap) && k1 - below0 < n) {
+        bitonicSort(s.cand, n);
+        vk = s.cand[k - below0];
+        vk1 = s.cand[k1 - below0];
+        done = true;
+        continue;
+      }
+      // more than kCap values: the passes below
+    }
     if (b0 != b1) {
       // k is the largest value of bin b0, k + 1 the smallest of bin b1.
       R mx = R(-INFINITY), mn = R(INFINITY);
       forEachValue(X, nP, pos, [&](R v, bool ok) {
-        const double dv = static_cast<double>(v);
-        if (!ok || !passes(s, rounds, dv)) return;
-        const uint32_t b = binOf(dv, dlo, invw);
+        if (!ok || !passes(s, rounds, v)) return;
+        const uint32_t b = binOf(v, dlo, invw);
         if (b == b0) mx = fmax(mx, v);
         if (b == b1) mn = fmin(mn, v);
       });
@@ -356,8 +446,7 @@ __global__ void __launch_bounds__(kRowThreads, 8) rowStatsKernel(const RowJob<R>
       if (tid == 0) s.candCount = 0;
       __syncthreads();
       forEachValue(X, nP, pos, [&](R v, bool ok) {
-        const double dv = static_cast<double>(v);
-        if (ok && passes(s, rounds, dv) && binOf(dv, dlo, invw) == b0) s.cand[atomicAdd(&s.candCount, 1u)] = v;
+        if (ok && passes(s, rounds, v) && binOf(v, dlo, invw) == b0) s.cand[atomicAdd(&s.candCount, 1u)] = v;
       });
       __syncthreads();
       const uint32_t n = s.candCount;
