@@ -816,6 +816,8 @@ def main():
         try:
             if a.no_cpu:
                 raise RuntimeError("skipped (--no-cpu)")
+            if world > 1:
+                raise RuntimeError("measured with --gpus 1 only")
             r = reference_arm(replace_args(a, steps=1, warmup=0, cpu_seconds=a.cpu_seconds / 2))
             if "unavailable" in r:  # the reference library is absent: the plain-C restatement of its kernels, on the
                 # book in the reference's model family (the restatement has no stochastic foreign rates)
@@ -872,6 +874,10 @@ def main():
             "plan_compile_s": compile_s,
             "cpu_baseline": cpu,
         }
+        if world > 1:  # the other ranks wait at the closing barrier: the legs run in the one-GPU line only
+            a.no_precision = a.no_exact = a.no_surrogate = a.no_amc = a.no_amc_surrogate = True
+            a.no_im = a.no_xva_batch = a.no_nest = True
+            line["legs"] = "run with --gpus 1 only"
         if not a.no_precision:
             line["fp32_vs_fp64"] = guarded(precision_leg, ctx, a)
         if not a.no_exact:
