@@ -29,7 +29,7 @@ typedef enum zk_status {
   ZK_OK = 0,
   ZK_ERR_INVALID_ARGUMENT = 1, /* null pointer, wrong buffer length */
   ZK_ERR_INVALID_PLAN = 2,     /* malformed or inconsistent plan tables */
-  ZK_ERR_UNSUPPORTED = 3,      /* a plan feature this build does not run (message says which) */
+  ZK_ERR_UNSUPPORTED = 3,      /* a plan feature this library does not run (message says which) */
   ZK_ERR_OUT_OF_MEMORY = 4,
   ZK_ERR_CUDA = 5,             /* a CUDA runtime error (launch failure, ...) */
   ZK_ERR_DEVICE_TIMEOUT = 6,   /* a bounded wait inside a kernel gave up; the context stays usable */

@@ -3,7 +3,7 @@
 The oracle is the plain-C restatement of the reference's path (oracle/restated.py), which is pinned bit for bit
 to the reference itself (tests/test_oracle_pins.py), plus the golden fixtures the reference computed
 (tests/golden/).  Plans come from this package's compiler (pinned table-for-table to the reference's
-gpu::compile by tests/test_compiler.py) or, where the reference fits something this build does not (the AMC
+gpu::compile by tests/test_compiler.py) or, where the reference fits something this package does not (the AMC
 regression of a Bermudan), from the reference's own tables stored in a fixture.
 
 Tolerances.  The FP32 kernels draw the same counter-based normals as the reference; the two differ only by the

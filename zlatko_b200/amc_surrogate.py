@@ -9,7 +9,7 @@ src/gpu/fused_exposure.cpp:145-154; evaluated by amcPoly, src/gpu/fused_kernels.
 pos * max(poly(x), 0)).  Here one perceptron for every date and every Bermudan of a book learns it from the
 realised values the plain method itself generates: the AMC pass of the fused kernels (zk_amc_states: the state
 x, the deflator D and the exercise values on every path) under the policy the Longstaff-Schwartz fit chose
-(zk_fit_amc).  The policy stays the judge of exercise; only the continuation values change.
+(zk_fit_amc).  The policy still decides exercise; only the continuation values change.
 
 Inputs (16): x, the co-terminal swap rate of the next exercise and its annuity, the intrinsic value of the
 underlying from that exercise, t, the times to the next exercise and to the final maturity, the strike, the
