@@ -838,13 +838,15 @@ struct BuildOpts {
   const Presim* presim = nullptr;  // the first plan's scenario already simulated (single precision, counter normals)
 };
 
+// parsed: the plans already validated and lowered (their views' tables stay the caller's), else parsed from views.
 template <typename R>
 std::unique_ptr<Batch<R>> build(zk_context* ctx, std::vector<View<R>> views, bool sink, const double* normals, size_t streams,
-                                const BuildOpts& opts = BuildOpts()) {
+                                const BuildOpts& opts = BuildOpts(), std::vector<Plan<R>>* parsed = nullptr) {
   auto B = std::make_unique<Batch<R>>();
   B->ctx = ctx;
   B->sink = sink;
-  parseAll(views, B->plans, hostPool(ctx, views.size()));
+  if (parsed) B->plans = std::move(*parsed);
+  else parseAll(views, B->plans, hostPool(ctx, views.size()));
   const size_t nPlans = B->plans.size();
   if (opts.maps) {
     for (size_t i = 0; i < nPlans; ++i) {
@@ -1332,7 +1334,7 @@ void execute(Batch<R>& B, bool capturing = false) {
   // each its simulation then its revaluation, joined before the reduce.
   const bool fan = !capturing && !B.waved && B.launches.size() > 1 && !B.plans[B.launches[0].planIdx[0]].pathMap.empty();
   if (fan) {
-    const size_t k = std::min<size_t>(B.launches.size(), 8);
+    const size_t k = std::min<size_t>(B.launches.size(), 16);
     while (ctx->workers.size() < k) {
       cudaStream_t w = nullptr;
       cudaEvent_t e = nullptr;
@@ -1478,8 +1480,8 @@ std::vector<SumPatch> exactCheck(Batch<float>& B) {
     if (P.guard.empty()) continue;
     const uint32_t* w = bits.data() + (B.dev[i].flags - B.flagsOff) / 4;
     std::vector<uint32_t> paths;
-    for (uint32_t p = 0; p < P.nP; ++p)
-      if (w[p >> 5] >> (p & 31u) & 1u) paths.push_back(p);
+    for (uint32_t k = 0; k < (P.nP + 31) / 32; ++k)
+      for (uint32_t m = w[k]; m; m &= m - 1) paths.push_back(32 * k + static_cast<uint32_t>(__builtin_ctz(m)));
     ctx->exactPaths += P.nP;
     ctx->exactFlagged += paths.size();
     if (paths.empty()) continue;
@@ -1515,7 +1517,14 @@ std::vector<SumPatch> exactCheck(Batch<float>& B) {
   }
   BuildOpts ro;
   ro.maps = &maps;
-  auto B32 = build<float>(ctx, v32, false, nullptr, 0, ro);
+  // The single-precision re-run takes the batch's parsed and lowered plans, with the re-run's path count.
+  std::vector<Plan<float>> p32(n);
+  for (size_t k = 0; k < n; ++k) {
+    p32[k] = B.plans[which[k]];
+    p32[k].v = v32[k], p32[k].H = headers[k].data(), p32[k].nP = static_cast<uint32_t>(maps[k].size());
+    p32[k].guard.clear(), p32[k].pathMap.clear();
+  }
+  auto B32 = build<float>(ctx, v32, false, nullptr, 0, ro, &p32);
   auto B64 = build<double>(ctx, v64, false, nullptr, 0, ro);
   for (size_t k = 0; k < n; ++k) {
     SumPatch sp;
