@@ -42,6 +42,7 @@ struct RowSmem {
   double dsum[kRowWarps];
   R rmin[kRowWarps], rmax[kRowWarps];
   uint32_t candCount;
+  uint32_t usum[kRowWarps];
   uint32_t pick[4];
   double flo[kMaxRounds], finvw[kMaxRounds];
   uint32_t fb0[kMaxRounds], fb1[kMaxRounds];
@@ -57,6 +58,23 @@ __device__ __forceinline__ double blockSum(double v, double* scratch) {
     for (int w = 0; w < kRowWarps; ++w) s += scratch[w];
   __syncthreads();
   return s;  // valid in thread 0
+}
+
+// Bin 0 holds the row's minimum, the dominant duplicate of exposure rows (exact zeros): instead of counting it value
+// by value, its count is the values binned less the other bins' counts, summed here over the CTA.
+__device__ __forceinline__ void fillBinZero(uint32_t* hist, uint32_t binned, uint32_t* scratch) {
+  uint32_t v = 0;
+  for (uint32_t b = threadIdx.x; b < static_cast<uint32_t>(kBins); b += kRowThreads)
+    if (b != 0) v += hist[b];
+  v = __reduce_add_sync(0xFFFFFFFFu, v);
+  if ((threadIdx.x & 31u) == 0) scratch[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kRowWarps; ++w) t += scratch[w];
+    hist[0] = binned - t;
+  }
+  __syncthreads();
 }
 
 template <typename R>
@@ -170,11 +188,9 @@ template <typename R>
 __device__ __forceinline__ uint32_t sampleHistogram(const R* X, uint32_t nP, bool pos, double dlo, double invw, uint32_t* hist) {
   constexpr uint32_t kVec = 16 / sizeof(R);
   const uint32_t nv = nP / kVec, blocks = nv / 32, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  uint32_t zero = 0;  // this lane's values in bin 0, summed over the warp at the end
-  auto put = [&](R x) {
+  auto put = [&](R x) {  // bin 0 is filled afterwards (fillBinZero)
     x = pos ? fmax(x, R(0)) : x;
     const uint32_t b = binOf(x, dlo, invw);
-    zero += b == 0 ? 1u : 0u;
     if (b != 0) atomicAdd(&hist[b], 1u);
   };
   for (uint32_t b = warp * kSampleStride; b < blocks; b += kRowWarps * kSampleStride) {
@@ -187,8 +203,6 @@ __device__ __forceinline__ uint32_t sampleHistogram(const R* X, uint32_t nP, boo
       put(q.x), put(q.y);
     }
   }
-  zero = __reduce_add_sync(0xFFFFFFFFu, zero);
-  if (lane == 0 && zero) atomicAdd(&hist[0], zero);
   return (blocks + kSampleStride - 1) / kSampleStride * 32u * kVec;
 }
 
@@ -344,7 +358,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
     if (tid == 0) out[0] = lo;
     return;
   }
-  uint32_t below = 0;
+  uint32_t below = 0, binned = nP;  // the values each round bins: the row, then the previous round's bin
   int rounds = 0;
   R vk = lo, vk1 = lo;
   bool done = false;
@@ -359,6 +373,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
     __syncthreads();
     const uint32_t ns = sampleHistogram(X, nP, pos, dlo0, invw0, s.hist);
     __syncthreads();
+    fillBinZero(s.hist, ns, s.usum);
     const double q = static_cast<double>(k) / static_cast<double>(nP), ks = q * static_cast<double>(ns);
     const double sd = sqrt(static_cast<double>(ns) * q * (1.0 - q)) * 3.0 + 4.0;
     const uint32_t rlo = static_cast<uint32_t>(fmax(ks - sd, 0.0)), rhi = static_cast<uint32_t>(fmin(ks + sd + 1.0, ns - 1.0));
@@ -386,23 +401,19 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
     const double dlo = static_cast<double>(lo), invw = scaleOf(lo, hi);
     for (uint32_t b = tid; b < kBins; b += kRowThreads) s.hist[b] = 0;
     __syncthreads();
-    // Bin 0 holds the row's minimum, the dominant duplicate of exposure rows (exact zeros): each lane counts its own
-    // and the warp adds them once, instead of contended shared-memory atomics.
-    uint32_t zeroBin = 0;
     const bool gather = rounds == 0 && winLo <= winHi;
+    const uint32_t winSpan = winHi - winLo;
     forEachValue(X, nP, pos, [&](R x, bool ok) {
       const bool in = ok && passes(s, rounds, x);
       const uint32_t b = binOf(x, dlo, invw);
-      zeroBin += in && b == 0 ? 1u : 0u;
-      if (in && b != 0) atomicAdd(&s.hist[b], 1u);
-      if (gather && in && b >= winLo && b <= winHi) {
+      if (in && b != 0) atomicAdd(&s.hist[b], 1u);  // bin 0 is filled afterwards (fillBinZero)
+      if (gather && in && b - winLo <= winSpan) {
         const uint32_t at = atomicAdd(&s.gathCount, 1u);
         if (at < static_cast<uint32_t>(kGather)) s.gath[at] = x;
       }
     });
-    zeroBin = __reduce_add_sync(0xFFFFFFFFu, zeroBin);
-    if ((tid & 31u) == 0 && zeroBin) atomicAdd(&s.hist[0], zeroBin);
     __syncthreads();
+    fillBinZero(s.hist, binned, s.usum);
     if (tid < 32) locateRanks(s, below, k, k1, tid);
     __syncthreads();
     const uint32_t b0 = s.pick[0], b1 = s.pick[1], below0 = s.pick[2], c0 = s.pick[3];
@@ -457,7 +468,7 @@ __global__ void __launch_bounds__(kRowThreads, 6) rowStatsKernel(const RowJob<R>
     } else {
       if (tid == 0) s.flo[rounds] = dlo, s.finvw[rounds] = invw, s.fb0[rounds] = b0, s.fb1[rounds] = b0;
       __syncthreads();
-      below = below0;
+      below = below0, binned = c0;
       ++rounds;
     }
   }
